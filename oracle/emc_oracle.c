@@ -1,0 +1,474 @@
+/* CPU oracle for one EMC iteration. TEST INFRASTRUCTURE ONLY (see emc_oracle.h).
+ *
+ * Written from the algorithm of duaneloh/Dragonfly's packaged engine; each
+ * function names the reference lines it restates. The data structures are our
+ * own (flat arrays instead of the reference's linked dataset list and per-thread
+ * max_data), but arithmetic follows the reference's operation order so that a
+ * build without FMA contraction is bit-identical to the one-thread reference.
+ */
+#include "emc_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_PROB_MIN 1.e-6         /* max_internal.h:6 */
+#define ORC_PDIFF_THRESH 14.       /* max_internal.h:7 */
+#define ORC_MAX_EXP_START -1.e100  /* max_internal.h:8 */
+
+void orc_make_rot_quat(const double *q, double rot[3][3]) {
+	/* model.c:759-786 */
+	double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+	double q01 = q0 * q1, q02 = q0 * q2, q03 = q0 * q3;
+	double q11 = q1 * q1, q12 = q1 * q2, q13 = q1 * q3;
+	double q22 = q2 * q2, q23 = q2 * q3, q33 = q3 * q3;
+	rot[0][0] = (1. - 2. * (q22 + q33));
+	rot[0][1] = 2. * (q12 + q03);
+	rot[0][2] = 2. * (q13 - q02);
+	rot[1][0] = 2. * (q12 - q03);
+	rot[1][1] = (1. - 2. * (q11 + q33));
+	rot[1][2] = 2. * (q01 + q23);
+	rot[2][0] = 2. * (q02 + q13);
+	rot[2][1] = 2. * (q23 - q01);
+	rot[2][2] = (1. - 2. * (q11 + q22));
+}
+
+/* Rotated voxel position of pixel t: sum_j rot[i][j] q_j, then + center,
+ * accumulated from 0 in j order (model.c:19-25). */
+static void rotate_pixel(double rot[3][3], const double *qv, double center, double pos[3]) {
+	int i, j;
+	for (i = 0; i < 3; ++i) {
+		double acc = 0.;
+		for (j = 0; j < 3; ++j)
+			acc += rot[i][j] * qv[j];
+		acc += center;
+		pos[i] = acc;
+	}
+}
+
+void orc_slice_gen3d(const double *quat, int mode, double *slice, int num_pix, const double *qvals,
+                     const double *corr, long size, long center, const double *model1) {
+	/* model.c:11-59 */
+	long t, x, y, z, vol = size * size * size;
+	double rot[3][3], pos[3], fx, fy, fz, cx, cy, cz;
+	const double *m = &model1[(long)mode * vol];
+	orc_make_rot_quat(quat, rot);
+	for (t = 0; t < num_pix; ++t) {
+		rotate_pixel(rot, &qvals[t * 3], (double)center, pos);
+		x = (long)pos[0];  /* truncation toward zero, as the reference's assignment */
+		y = (long)pos[1];
+		z = (long)pos[2];
+		if (x < 0 || x > size - 2 || y < 0 || y > size - 2 || z < 0 || z > size - 2) {
+			slice[t] = DBL_MIN;
+			continue;
+		}
+		fx = pos[0] - x; fy = pos[1] - y; fz = pos[2] - z;
+		cx = 1. - fx; cy = 1. - fy; cz = 1. - fz;
+		{
+			long x1 = (x + 1) % size, y1 = (y + 1) % size, z1 = (z + 1) % size;
+			long s2 = size * size;
+			double v = cx * cy * cz * m[x * s2 + y * size + z] +
+			           cx * cy * fz * m[x * s2 + y * size + z1] +
+			           cx * fy * cz * m[x * s2 + y1 * size + z] +
+			           cx * fy * fz * m[x * s2 + y1 * size + z1] +
+			           fx * cy * cz * m[x1 * s2 + y * size + z] +
+			           fx * cy * fz * m[x1 * s2 + y * size + z1] +
+			           fx * fy * cz * m[x1 * s2 + y1 * size + z] +
+			           fx * fy * fz * m[x1 * s2 + y1 * size + z1];
+			slice[t] = v * corr[t];
+		}
+	}
+}
+
+void orc_slice_merge3d(const double *quat, int mode, const double *slice, double *model2, double *weight,
+                       long size, int num_pix, const double *qvals, const double *corr, const uint8_t *mask) {
+	/* model.c:171-244 */
+	long t, x, y, z, vol = size * size * size, s2 = size * size;
+	double rot[3][3], pos[3], fx, fy, fz, cx, cy, cz, w, f;
+	double *m = &model2[(long)mode * vol], *wt = &weight[(long)mode * vol];
+	orc_make_rot_quat(quat, rot);
+	for (t = 0; t < num_pix; ++t) {
+		if (mask[t] > 1)
+			continue;
+		rotate_pixel(rot, &qvals[t * 3], (double)(size / 2), pos);
+		x = (long)pos[0];
+		y = (long)pos[1];
+		z = (long)pos[2];
+		if (x < 0 || x > size - 2 || y < 0 || y > size - 2 || z < 0 || z > size - 2)
+			continue;
+		fx = pos[0] - x; fy = pos[1] - y; fz = pos[2] - z;
+		cx = 1. - fx; cy = 1. - fy; cz = 1. - fz;
+		w = slice[t] / corr[t];
+		{
+			long x1 = (x + 1) % size, y1 = (y + 1) % size, z1 = (z + 1) % size;
+			long idx[8] = {x * s2 + y * size + z, x * s2 + y * size + z1, x * s2 + y1 * size + z,
+			               x * s2 + y1 * size + z1, x1 * s2 + y * size + z, x1 * s2 + y * size + z1,
+			               x1 * s2 + y1 * size + z, x1 * s2 + y1 * size + z1};
+			double fw[8] = {cx * cy * cz, cx * cy * fz, cx * fy * cz, cx * fy * fz,
+			                fx * cy * cz, fx * cy * fz, fx * fy * cz, fx * fy * fz};
+			int k;
+			for (k = 0; k < 8; ++k) {
+				f = fw[k];
+				wt[idx[k]] += f;
+				m[idx[k]] += f * w;
+			}
+		}
+	}
+}
+
+void orc_symmetrize_friedel(double *array, const double *weights, int size) {
+	/* model.c:470-490: visits z <= center, so pairs inside the z == center plane
+	 * are averaged twice, the second time from the other member of the pair. */
+	int x, y, z, v1, v2, lo = (size % 2 == 0) ? 1 : 0, c = size / 2;
+	double a, wsum;
+	for (x = lo; x < size; ++x)
+		for (y = lo; y < size; ++y)
+			for (z = lo; z <= c; ++z) {
+				v1 = x * size * size + y * size + z;
+				v2 = (2 * c - x) * size * size + (2 * c - y) * size + (2 * c - z);
+				a = 0.5 * (array[v1] * weights[v1] + array[v2] * weights[v2]);
+				wsum = 0.5 * (weights[v1] + weights[v2]);
+				a = (wsum > 0) ? a / wsum : 0.;
+				array[v1] = a;
+				array[v2] = a;
+			}
+}
+
+void orc_frame_stats(int num_data, const int *ones, const int *multi, const int *place_ones,
+                     const int *place_multi, const int *count_multi, const uint8_t *mask,
+                     int *fcounts, double *sum_fact, double *mean_count) {
+	/* iterate.c:3-64 (calc_frame_counts) and 85-117 (calc_sum_fact) */
+	long d, t, o = 0, mo = 0;
+	double mc = 0.;
+	for (d = 0; d < num_data; ++d) {
+		int fc = 0;
+		double sf = 0.;
+		for (t = 0; t < ones[d]; ++t)
+			if (mask[place_ones[o + t]] < 1)
+				fc++;
+		for (t = 0; t < multi[d]; ++t)
+			if (mask[place_multi[mo + t]] < 1) {
+				fc += count_multi[mo + t];
+				sf += lgamma((double)count_multi[mo + t] + 1.0);
+			}
+		fcounts[d] = fc;
+		sum_fact[d] = sf;
+		mc += fc;
+		o += ones[d];
+		mo += multi[d];
+	}
+	*mean_count = mc / num_data;
+}
+
+void orc_calc_beta(int num_data, double start, int need_scaling, double mean_count, const int *fcounts,
+                   double *beta_start) {
+	/* iterate.c:66-83 */
+	int d;
+	if (!need_scaling && start < 0)
+		start = exp(-6.5 * pow(mean_count * 1.e-5, 0.15));
+	for (d = 0; d < num_data; ++d)
+		beta_start[d] = start > 0 ? start : exp(-6.5 * pow(fcounts[d] * 1.e-5, 0.15));
+}
+
+/* Per-frame list of kept (orientation, log-probability) pairs, in the order
+ * the orientations were visited (max_prob.c:184-203, resparsify 429-448).
+ * Orientations are visited in ascending order, so each list stays sorted by
+ * orientation and can be searched by bisection. */
+typedef struct {
+	int n, cap;
+	int *pos;
+	double *val;
+} kept_list;
+
+static void list_push(kept_list *l, int r, double v) {
+	if (l->n == l->cap) {
+		l->cap = l->cap ? 2 * l->cap : 8;
+		l->pos = realloc(l->pos, (size_t)l->cap * sizeof(int));
+		l->val = realloc(l->val, (size_t)l->cap * sizeof(double));
+	}
+	l->pos[l->n] = r;
+	l->val[l->n] = v;
+	l->n++;
+}
+
+/* Drops entries <= thresh, keeping order (max_prob.c:429-448). */
+static void list_prune(kept_list *l, double thresh) {
+	int i, k = 0;
+	for (i = 0; i < l->n; ++i)
+		if (!(l->val[i] <= thresh)) {
+			l->pos[k] = l->pos[i];
+			l->val[k] = l->val[i];
+			k++;
+		}
+	l->n = k;
+}
+
+/* Index of orientation r in the sorted list, or -1 (the lookup that
+ * max_update.c:86-93 does by linear search). */
+static int list_find(const kept_list *l, int r) {
+	int lo = 0, hi = l->n - 1;
+	while (lo <= hi) {
+		int mid = (lo + hi) / 2;
+		if (l->pos[mid] == r)
+			return mid;
+		if (l->pos[mid] < r)
+			lo = mid + 1;
+		else
+			hi = mid - 1;
+	}
+	return -1;
+}
+
+/* Orientations are processed in blocks whose slices fit in this many doubles. */
+#define ORC_BLOCK_DOUBLES (1L << 27)
+
+/* The reference visits orientations in an outer loop and frames in an inner
+ * loop. Every quantity it accumulates is either per frame (summed over
+ * orientations in ascending order) or per orientation (summed over frames in
+ * ascending order); this restatement keeps each of those orders and
+ * parallelises only across independent frames or orientations, so its results
+ * do not depend on the thread count. The merge into model2 is sequential in
+ * orientation order, as with one reference thread. */
+double orc_maximize(int num_pix, const double *qvals, const double *corr, const uint8_t *mask,
+                    int num_data, const int *ones, const int *multi, const int *place_ones,
+                    const int *place_multi, const int *count_multi,
+                    int num_rot, int num_modes, const double *quats,
+                    long size, const double *model1,
+                    double *scale, const double *beta, const double *sum_fact, const int *fcounts,
+                    const uint8_t *blacklist, double mean_count,
+                    int need_scaling, int update_scale, int known_scale, int iteration,
+                    double *model2, double *weight, double *u, double *psum_r,
+                    int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
+                    double *psum_d, double *quat_norm, int *num_prob, double *scalars_out) {
+	const int M = num_modes, R = num_modes * num_rot;
+	const long vol = size * size * size, center = size / 2;
+	long *ones_off = malloc((size_t)(num_data + 1) * sizeof(long));
+	long *multi_off = malloc((size_t)(num_data + 1) * sizeof(long));
+	long blk = ORC_BLOCK_DOUBLES / (num_pix > 0 ? num_pix : 1);
+	double *views;
+	kept_list *lists = calloc((size_t)num_data, sizeof(kept_list));
+	double total = 0., rescale, avg_ll = 0., mutual_info = 0.;
+	const int use_scale = need_scaling && (iteration > 1 || known_scale);
+	int d, r, r0;
+
+	if (blk < 1)
+		blk = 1;
+	if (blk > R)
+		blk = R;
+	views = malloc((size_t)blk * num_pix * sizeof(double));
+	ones_off[0] = multi_off[0] = 0;
+	for (d = 0; d < num_data; ++d) {
+		ones_off[d + 1] = ones_off[d] + ones[d];
+		multi_off[d + 1] = multi_off[d] + multi[d];
+	}
+	memset(model2, 0, (size_t)M * vol * sizeof(double));
+	memset(weight, 0, (size_t)M * vol * sizeof(double));
+	for (d = 0; d < num_data; ++d) {
+		rmax[d] = 0;
+		info[d] = likelihood[d] = p_norm[d] = psum_d[d] = 0.;
+		max_exp[d] = ORC_MAX_EXP_START;
+	}
+	if (M > 1)
+		memset(quat_norm, 0, (size_t)num_data * M * sizeof(double));
+
+	/* Orientation index r -> (rotation, mode) (max_prob.c:80-85 for one rank) */
+#define ROTIND(r) ((r) / M)
+#define MODE(r) ((r) % M)
+
+	/* calculate_rescale (max_prob.c:3-64): u_r = sum of W over mask==0 pixels */
+	#pragma omp parallel for schedule(dynamic, 4)
+	for (r = 0; r < R; ++r) {
+		int t;
+		double *view = malloc((size_t)num_pix * sizeof(double)), acc = 0.;
+		orc_slice_gen3d(&quats[ROTIND(r) * 5], MODE(r), view, num_pix, qvals, corr, size, center, model1);
+		for (t = 0; t < num_pix; ++t)
+			if (mask[t] < 1)
+				acc += view[t];
+		u[r] = acc;
+		free(view);
+	}
+	for (r = 0; r < R; ++r)
+		total += quats[ROTIND(r) * 5 + 4] * u[r];
+	rescale = mean_count / total * M;
+
+	/* calculate_prob (max_prob.c:66-213): per frame, orientations in order */
+	for (r0 = 0; r0 < R; r0 += (int)blk) {
+		int r1 = r0 + (int)blk < R ? r0 + (int)blk : R;
+		#pragma omp parallel for schedule(dynamic, 1)
+		for (r = r0; r < r1; ++r) {
+			int t;
+			double *view = &views[(long)(r - r0) * num_pix];
+			orc_slice_gen3d(&quats[ROTIND(r) * 5], MODE(r), view, num_pix, qvals, corr, size, center, model1);
+			for (t = 0; t < num_pix; ++t)
+				view[t] = log(view[t]);
+		}
+		#pragma omp parallel for schedule(dynamic, 16)
+		for (d = 0; d < num_data; ++d) {
+			int rr;
+			long i;
+			if (blacklist[d])
+				continue;
+			for (rr = r0; rr < r1; ++rr) {
+				const double *view = &views[(long)(rr - r0) * num_pix];
+				const double w = quats[ROTIND(rr) * 5 + 4];
+				double pval, thr;
+				if (use_scale)
+					pval = log(w) - u[rr] * scale[d];
+				else
+					pval = log(w) - u[rr] * rescale;
+				for (i = ones_off[d]; i < ones_off[d + 1]; ++i)
+					if (mask[place_ones[i]] < 1)
+						pval += view[place_ones[i]];
+				for (i = multi_off[d]; i < multi_off[d + 1]; ++i)
+					if (mask[place_multi[i]] < 1)
+						pval += count_multi[i] * view[place_multi[i]];
+				thr = ORC_PDIFF_THRESH / beta[d];
+				if (pval + thr > max_exp[d])
+					list_push(&lists[d], rr, pval);
+				if (pval > max_exp[d]) {
+					max_exp[d] = pval;
+					rmax[d] = rr;
+					list_prune(&lists[d], pval - thr);
+				}
+			}
+		}
+	}
+
+	/* normalize_prob (max_prob.c:215-265) and the per-frame half of calc_psum_r
+	 * (max_update.c:95-130): P, likelihood, psum_d, quat_norm, info, each summed
+	 * over the frame's kept orientations in ascending order. */
+	#pragma omp parallel for schedule(dynamic, 16)
+	for (d = 0; d < num_data; ++d) {
+		int k;
+		double s = 0.;
+		kept_list *l = &lists[d];
+		if (max_exp[d] == ORC_MAX_EXP_START)
+			rmax[d] = -1;
+		for (k = 0; k < l->n; ++k)
+			s += exp(beta[d] * (l->val[k] - max_exp[d]));
+		p_norm[d] = s;
+		if (blacklist[d])
+			continue;
+		for (k = 0; k < l->n; ++k) {
+			const int rr = l->pos[k];
+			const double w = quats[ROTIND(rr) * 5 + 4];
+			double temp = l->val[k];
+			double P = exp(beta[d] * (temp - max_exp[d])) / p_norm[d];
+			l->val[k] = P;
+			likelihood[d] += P * (temp - sum_fact[d]);
+			if (need_scaling && update_scale)
+				psum_d[d] += P * u[rr] * rescale;
+			if (P < ORC_PROB_MIN)
+				continue;
+			if (M > 1)
+				quat_norm[d * M + MODE(rr)] += P;
+			info[d] += P * log(P / w * M);
+		}
+	}
+
+	/* Per-orientation half of calc_psum_r (max_update.c:108-116), then
+	 * update_tomogram_nobg (max_update.c:142-230) and merge_tomogram
+	 * (max_update.c:18-40), block by block; merges run in orientation order. */
+	for (r0 = 0; r0 < R; r0 += (int)blk) {
+		int r1 = r0 + (int)blk < R ? r0 + (int)blk : R;
+		#pragma omp parallel for schedule(dynamic, 1)
+		for (r = r0; r < r1; ++r) {
+			double *view = &views[(long)(r - r0) * num_pix], pr = 0.;
+			int dd, t;
+			long i;
+			for (dd = 0; dd < num_data; ++dd) {
+				int ind;
+				if (blacklist[dd])
+					continue;
+				ind = list_find(&lists[dd], r);
+				if (ind < 0)
+					continue;
+				pr += need_scaling ? lists[dd].val[ind] * scale[dd] : lists[dd].val[ind];
+			}
+			psum_r[r] = pr;
+			memset(view, 0, (size_t)num_pix * sizeof(double));
+			for (dd = 0; dd < num_data; ++dd) {
+				int ind;
+				double P;
+				if (blacklist[dd])
+					continue;
+				ind = list_find(&lists[dd], r);
+				if (ind < 0)
+					continue;
+				P = lists[dd].val[ind];
+				if (!(P > ORC_PROB_MIN))
+					continue;
+				for (i = ones_off[dd]; i < ones_off[dd + 1]; ++i)
+					if (mask[place_ones[i]] < 2)
+						view[place_ones[i]] += P;
+				for (i = multi_off[dd]; i < multi_off[dd + 1]; ++i)
+					if (mask[place_multi[i]] < 2)
+						view[place_multi[i]] += count_multi[i] * P;
+			}
+			if (pr > 0.)
+				for (t = 0; t < num_pix; ++t)
+					view[t] /= pr;
+		}
+		for (r = r0; r < r1; ++r)
+			if (psum_r[r] > 0.)
+				orc_slice_merge3d(&quats[ROTIND(r) * 5], MODE(r), &views[(long)(r - r0) * num_pix], model2,
+				                  weight, size, num_pix, qvals, corr, mask);
+	}
+
+	/* combine_information_mpi (max_prob.c:344-427). The packaged Iterate never
+	 * sets num_blacklist (iterate.pyx:35, 317-359), so averages divide by N. */
+	for (d = 0; d < num_data; ++d)
+		if (!blacklist[d]) {
+			mutual_info += info[d];
+			avg_ll += likelihood[d];
+		}
+	mutual_info /= num_data;
+	avg_ll /= num_data;
+
+	/* update_scale (max_scale.c:3-19) */
+	if (need_scaling && update_scale)
+		for (d = 0; d < num_data; ++d)
+			if (!blacklist[d])
+				scale[d] = fcounts[d] / psum_d[d];
+
+	if (num_prob != NULL)
+		for (d = 0; d < num_data; ++d)
+			num_prob[d] = lists[d].n;
+	scalars_out[0] = rescale;
+	scalars_out[1] = mutual_info;
+	scalars_out[2] = avg_ll;
+
+	for (d = 0; d < num_data; ++d) {
+		free(lists[d].pos);
+		free(lists[d].val);
+	}
+	free(lists);
+	free(views);
+	free(ones_off);
+	free(multi_off);
+#undef ROTIND
+#undef MODE
+	return avg_ll;
+}
+
+double orc_update_model(long size, int num_modes, double *model1, double *model2, double *weight,
+                        double alpha) {
+	/* recon.pyx:112-149, RECON3D branch with Friedel symmetry (recon.pyx:128-130) */
+	long x, vol = size * size * size, n = vol * num_modes;
+	double diff, change = 0.;
+	for (x = 0; x < num_modes; ++x)
+		orc_symmetrize_friedel(&model2[x * vol], &weight[x * vol], (int)size);
+	for (x = 0; x < n; ++x)
+		if (weight[x] > 0.)
+			model2[x] /= weight[x];
+	for (x = 0; x < n; ++x) {
+		diff = model2[x] - model1[x];
+		change += diff * diff;
+		if (alpha > 0.)
+			model1[x] = alpha * model1[x] + (1 - alpha) * model2[x];
+		else
+			model1[x] = model2[x];
+	}
+	return sqrt(change / num_modes / vol);
+}

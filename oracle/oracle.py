@@ -1,0 +1,329 @@
+"""ctypes front end of the CPU oracle. TEST INFRASTRUCTURE ONLY.
+
+Two engines with one interface:
+
+* ``OracleEngine`` -- our own single-threaded C restatement (``liboracle.so``,
+  source ``emc_oracle.c``) of duaneloh/Dragonfly's packaged EMC engine;
+* ``ReferenceEngine`` -- the reference's own C engine compiled from its sources
+  (``_ref/libdragonfly_ref.so``, driver ``ref_driver.c``).
+
+Both run ``run_iteration`` the way ``EMCRecon.run_iteration`` does
+(dragonfly/recon.pyx:72-110): update_beta, maximize, update_model and, when
+need_scaling is set, Iterate.normalize_scale (dragonfly/iterate.pyx:361-384,
+restated here in numpy as in the reference).
+
+Only tests/, ``__graft_entry__.smoke`` and bench.py's CPU-baseline leg import
+this module; the product never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_ORACLE = os.path.join(HERE, "liboracle.so")
+LIB_REF = os.path.join(HERE, "_ref", "libdragonfly_ref.so")
+LIB_REF_FAST = os.path.join(HERE, "_ref", "libdragonfly_ref_fast.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def build_oracle():
+    """Builds liboracle.so (and the reference libraries when the reference
+    sources are present) with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load(path):
+    if not os.path.exists(path):
+        build_oracle()
+    return C.CDLL(path)
+
+
+def reference_available(fast=False):
+    return os.path.exists(LIB_REF_FAST if fast else LIB_REF)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class EMCProblem:
+    """Inputs of an EMC reconstruction in the reference's layouts.
+
+    Attributes mirror the reference structs: detector (``qvals [P,3]``, ``corr``,
+    ``mask``), sparse frames (``ones``, ``multi``, ``place_ones``,
+    ``place_multi``, ``count_multi``), ``quats [R,5]``, model1
+    ``[M, S, S, S]`` and the [emc] parameters used by the iteration.
+    """
+
+    def __init__(self, qvals, corr, mask, ones, multi, place_ones, place_multi, count_multi,
+                 quats, model1, need_scaling=0, update_scale=1, known_scale=0, alpha=0.,
+                 beta=1., beta_jump=1., beta_period=100, beta_factor=1., scale=None,
+                 blacklist=None):
+        self.qvals = _c(qvals, np.float64).reshape(-1, 3)
+        self.corr = _c(corr, np.float64)
+        self.mask = _c(mask, np.uint8)
+        self.ones = _c(ones, np.int32)
+        self.multi = _c(multi, np.int32)
+        self.place_ones = _c(place_ones, np.int32)
+        self.place_multi = _c(place_multi, np.int32)
+        self.count_multi = _c(count_multi, np.int32)
+        self.quats = _c(quats, np.float64).reshape(-1, 5)
+        m = _c(model1, np.float64)
+        self.model1 = m.reshape((-1,) + m.shape[-3:]) if m.ndim >= 3 else m
+        self.need_scaling = int(need_scaling)
+        self.update_scale = int(update_scale)
+        self.known_scale = int(known_scale)
+        self.alpha = float(alpha)
+        self.beta = float(beta)
+        self.beta_jump = float(beta_jump)
+        self.beta_period = int(beta_period)
+        self.beta_factor = float(beta_factor)
+        self.scale = None if scale is None else _c(scale, np.float64)
+        self.blacklist = None if blacklist is None else _c(blacklist, np.uint8)
+
+    @property
+    def num_pix(self):
+        return self.corr.shape[0]
+
+    @property
+    def num_data(self):
+        return self.ones.shape[0]
+
+    @property
+    def num_rot(self):
+        return self.quats.shape[0]
+
+    @property
+    def num_modes(self):
+        return self.model1.shape[0]
+
+    @property
+    def size(self):
+        return self.model1.shape[-1]
+
+
+def normalize_scale(scale, blacklist, model1, rms):
+    """Iterate.normalize_scale (dragonfly/iterate.pyx:361-384): numpy mean of
+    the good frames' scale, model1 of mode 0 multiplied by it, scale divided."""
+    if blacklist is None:
+        mean_scale = scale.mean()
+        scale /= mean_scale
+    else:
+        mean_scale = scale[blacklist == 0].mean()
+        scale[blacklist == 0] /= mean_scale
+    vol = model1[0].size
+    model1.reshape(-1)[:vol] *= mean_scale
+    return rms * mean_scale, mean_scale
+
+
+class IterationResult(dict):
+    """Outputs of one iteration, keyed like the reference's properties."""
+    __getattr__ = dict.__getitem__
+
+
+class ReferenceEngine:
+    """The reference C engine (dragonfly/src) driven through ref_driver.c."""
+
+    def __init__(self, prob, num_threads=1, fast=False):
+        self.lib = _load(LIB_REF_FAST if fast else LIB_REF)
+        L = self.lib
+        L.ref_create.restype = C.c_void_p
+        L.ref_create.argtypes = [C.c_int, _dp, _dp, _up, C.c_int, _ip, _ip, _ip, _ip, _ip,
+                                 C.c_int, _dp, C.c_long, C.c_int, _dp,
+                                 C.c_int, C.c_int, C.c_int, C.c_double,
+                                 C.c_double, C.c_double, C.c_int, C.c_double,
+                                 C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_maximize.restype = C.c_double
+        L.ref_maximize.argtypes = [C.c_void_p, C.c_int]
+        L.ref_update_model.restype = C.c_double
+        L.ref_update_model.argtypes = [C.c_void_p]
+        for n in ("ref_get_model1", "ref_set_model1", "ref_get_model2", "ref_get_weight",
+                  "ref_get_quat_norm", "ref_get_u", "ref_set_scale", "ref_get_scalars"):
+            getattr(L, n).argtypes = [C.c_void_p, _dp]
+        L.ref_get_frame_arrays.argtypes = [C.c_void_p, _ip, _dp, _dp, _dp, _dp, _dp]
+        L.ref_get_iter_arrays.argtypes = [C.c_void_p, _ip, _dp, _dp, _dp, _dp]
+        L.ref_set_rms.argtypes = [C.c_void_p, C.c_double]
+        L.ref_slice_gen.argtypes = [C.c_void_p, _dp, C.c_int, _dp]
+        L.ref_slice_merge.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _dp, _dp]
+        L.ref_destroy.argtypes = [C.c_void_p]
+        self.prob = p = prob
+        self._scale_buf = p.scale
+        self._bl_buf = p.blacklist
+        self.h = L.ref_create(
+            p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, p.num_data, p.ones, p.multi,
+            p.place_ones, p.place_multi, p.count_multi, p.num_rot, p.quats.reshape(-1),
+            p.size, p.num_modes, p.model1.reshape(-1), p.need_scaling, p.update_scale,
+            p.known_scale, p.alpha, p.beta, p.beta_jump, p.beta_period, p.beta_factor,
+            None if p.scale is None else p.scale.ctypes.data,
+            None if p.blacklist is None else p.blacklist.ctypes.data, int(num_threads))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _arr(self, fn, shape, dt=np.float64):
+        out = np.zeros(shape, dtype=dt)
+        fn(self.h, out.reshape(-1))
+        return out
+
+    def model1(self):
+        p = self.prob
+        return self._arr(self.lib.ref_get_model1, p.model1.shape)
+
+    def iter_arrays(self):
+        n = self.prob.num_data
+        fc = np.zeros(n, np.int32)
+        sf, sc, be, bs = (np.zeros(n) for _ in range(4))
+        self.lib.ref_get_iter_arrays(self.h, fc, sf, sc, be, bs)
+        return dict(fcounts=fc, sum_fact=sf, scale=sc, beta=be, beta_start=bs)
+
+    def slice_gen(self, quat, mode=0):
+        out = np.zeros(self.prob.num_pix)
+        self.lib.ref_slice_gen(self.h, _c(quat, np.float64), int(mode), out)
+        return out
+
+    def run_iteration(self, iteration):
+        p = self.prob
+        L = self.lib
+        avg_ll = L.ref_maximize(self.h, int(iteration))
+        n = p.num_data
+        res = IterationResult()
+        rmax = np.zeros(n, np.int32)
+        info, ll, mx, pn, pd = (np.zeros(n) for _ in range(5))
+        L.ref_get_frame_arrays(self.h, rmax, info, ll, mx, pn, pd)
+        res.update(rmax=rmax, info=info, likelihood=ll, max_exp=mx, p_norm=pn, psum_d=pd)
+        res["u"] = self._arr(L.ref_get_u, p.num_modes * p.num_rot)
+        res["quat_norm"] = self._arr(L.ref_get_quat_norm, (n, p.num_modes))
+        sc = np.zeros(5)
+        L.ref_get_scalars(self.h, sc)
+        res["rescale"], res["mean_count"], res["mutual_info"] = sc[0], sc[1], sc[2]
+        res["avg_likelihood"] = avg_ll
+        res["model2_sum"] = self._arr(L.ref_get_model2, p.model1.shape)
+        res["inter_weight"] = self._arr(L.ref_get_weight, p.model1.shape)
+        rms = L.ref_update_model(self.h)
+        res["model2"] = self._arr(L.ref_get_model2, p.model1.shape)
+        it = self.iter_arrays()
+        res["beta"] = it["beta"]
+        if p.need_scaling:
+            scale = it["scale"]
+            model1 = self.model1()
+            rms, _ = normalize_scale(scale, p.blacklist, model1, rms)
+            L.ref_set_scale(self.h, scale)
+            L.ref_set_model1(self.h, model1.reshape(-1))
+            L.ref_set_rms(self.h, rms)
+            res["scale"] = scale
+        res["rms_change"] = rms
+        res["model1"] = self.model1()
+        return res
+
+
+class OracleEngine:
+    """Our own C restatement (emc_oracle.c), same interface as ReferenceEngine."""
+
+    def __init__(self, prob):
+        self.lib = L = _load(LIB_ORACLE)
+        L.orc_maximize.restype = C.c_double
+        L.orc_maximize.argtypes = [C.c_int, _dp, _dp, _up, C.c_int, _ip, _ip, _ip, _ip, _ip,
+                                   C.c_int, C.c_int, _dp, C.c_long, _dp,
+                                   _dp, _dp, _dp, _ip, _up, C.c_double,
+                                   C.c_int, C.c_int, C.c_int, C.c_int,
+                                   _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _dp]
+        L.orc_update_model.restype = C.c_double
+        L.orc_update_model.argtypes = [C.c_long, C.c_int, _dp, _dp, _dp, C.c_double]
+        L.orc_frame_stats.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _ip, _up, _ip, _dp,
+                                      C.POINTER(C.c_double)]
+        L.orc_calc_beta.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp]
+        L.orc_slice_gen3d.argtypes = [_dp, C.c_int, _dp, C.c_int, _dp, _dp, C.c_long, C.c_long, _dp]
+        L.orc_slice_merge3d.argtypes = [_dp, C.c_int, _dp, _dp, _dp, C.c_long, C.c_int, _dp, _dp, _up]
+        self.prob = p = prob
+        n = p.num_data
+        self.fcounts = np.zeros(n, np.int32)
+        self.sum_fact = np.zeros(n)
+        mc = C.c_double(0.)
+        L.orc_frame_stats(n, p.ones, p.multi, p.place_ones, p.place_multi, p.count_multi,
+                          p.mask, self.fcounts, self.sum_fact, C.byref(mc))
+        self.mean_count = mc.value
+        self.beta_start = np.zeros(n)
+        L.orc_calc_beta(n, p.beta, p.need_scaling, self.mean_count, self.fcounts, self.beta_start)
+        self.beta = np.zeros(n)
+        self.blacklist = p.blacklist if p.blacklist is not None else np.zeros(n, np.uint8)
+        self.scale = (p.scale.copy() if p.scale is not None else np.ones(n)) if p.need_scaling \
+            else np.ones(n)
+        self._model1 = p.model1.copy()
+
+    def model1(self):
+        return self._model1.copy()
+
+    def slice_gen(self, quat, mode=0):
+        p = self.prob
+        out = np.zeros(p.num_pix)
+        self.lib.orc_slice_gen3d(_c(quat, np.float64), int(mode), out, p.num_pix,
+                                 p.qvals.reshape(-1), p.corr, p.size, p.size // 2,
+                                 self._model1.reshape(-1))
+        return out
+
+    def update_beta(self, iteration):
+        """recon.pyx:151-174"""
+        p = self.prob
+        factor = p.beta_jump ** ((iteration - 1) // p.beta_period)
+        factor *= p.beta_factor
+        good = self.blacklist != 1
+        self.beta[good] = np.minimum(self.beta_start[good] * factor, 1.)
+
+    def run_iteration(self, iteration):
+        p = self.prob
+        L = self.lib
+        n, M = p.num_data, p.num_modes
+        self.update_beta(iteration)
+        shape = self._model1.shape
+        model2 = np.zeros(shape)
+        weight = np.zeros(shape)
+        u = np.zeros(M * p.num_rot)
+        psum_r = np.zeros(M * p.num_rot)
+        rmax = np.zeros(n, np.int32)
+        info, ll, mx, pn, pd = (np.zeros(n) for _ in range(5))
+        qn = np.zeros((n, M))
+        nprob = np.zeros(n, np.int32)
+        sc = np.zeros(3)
+        avg_ll = L.orc_maximize(
+            p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, n, p.ones, p.multi, p.place_ones,
+            p.place_multi, p.count_multi, p.num_rot, M, p.quats.reshape(-1), p.size,
+            self._model1.reshape(-1), self.scale, self.beta, self.sum_fact, self.fcounts,
+            self.blacklist, self.mean_count, p.need_scaling, p.update_scale, p.known_scale,
+            int(iteration), model2.reshape(-1), weight.reshape(-1), u, psum_r, rmax, info, ll,
+            mx, pn, pd, qn.reshape(-1), nprob, sc)
+        res = IterationResult(rmax=rmax, info=info, likelihood=ll, max_exp=mx, p_norm=pn,
+                              psum_d=pd, u=u, psum_r=psum_r, quat_norm=qn, num_prob=nprob,
+                              rescale=sc[0], mutual_info=sc[1], avg_likelihood=avg_ll,
+                              mean_count=self.mean_count, beta=self.beta.copy())
+        res["model2_sum"] = model2.copy()
+        res["inter_weight"] = weight
+        rms = L.orc_update_model(p.size, M, self._model1.reshape(-1), model2.reshape(-1),
+                                 weight.reshape(-1), p.alpha)
+        res["model2"] = model2
+        if p.need_scaling:
+            rms, _ = normalize_scale(self.scale, p.blacklist, self._model1, rms)
+            res["scale"] = self.scale.copy()
+        res["rms_change"] = rms
+        res["model1"] = self.model1()
+        return res
+
+
+def quat_gen_reference(num_div):
+    """Quaternions from the reference's quat_gen (quaternion.c:811-842)."""
+    L = _load(LIB_REF)
+    L.ref_quat_gen.restype = C.c_int
+    L.ref_quat_gen.argtypes = [C.c_int, C.c_void_p]
+    n = L.ref_quat_gen(int(num_div), None)
+    out = np.zeros((n, 5))
+    L.ref_quat_gen(int(num_div), out.ctypes.data)
+    return out

@@ -1,0 +1,320 @@
+/* Driver for the reference's own packaged C engine, built from its unmodified
+ * sources (dragonfly/src/{maximize,max_prob,max_update,max_scale,model,iterate,
+ * quaternion}.c) into oracle/_ref/. TEST INFRASTRUCTURE ONLY: tests/, the smoke
+ * check and bench.py's CPU-baseline leg use it as the checker and as the timed
+ * reference arm; the product never links it.
+ *
+ * The reference's Python layer (dragonfly/recon.pyx, iterate.pyx) cannot be
+ * built here (no mpi4py/h5py), so this file takes its place around the C engine:
+ *   - it fills the reference structs the way Iterate.set_data / set_quat /
+ *     set_model / calc_beta do (dragonfly/iterate.pyx:241-266, 386-402),
+ *   - ref_maximize() runs EMCRecon.run_iteration's compute steps
+ *     (dragonfly/recon.pyx:86-99): select slice_gen3d/slice_merge3d, update_beta
+ *     (recon.pyx:151-174), then the reference's maximize() (maximize.c:8-56),
+ *   - ref_update_model() restates EMCRecon.update_model (recon.pyx:112-149) for
+ *     the 3-D Friedel case, calling the reference's symmetrize_friedel.
+ * Iterate.normalize_scale (iterate.pyx:361-384) is numpy code in the reference
+ * and is restated in numpy by oracle/oracle.py.
+ */
+#include <math.h>
+#include <omp.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "max_internal.h"
+
+typedef struct ref_engine {
+	struct detector det;
+	struct dataset dset;
+	struct quaternion quat;
+	struct model mod;
+	struct params par;
+	struct iterate iter;
+	struct max_data *mdata;
+	int det_mapping[1];
+	double avg_likelihood;
+} ref_engine;
+
+static void *dup_mem(const void *src, size_t bytes) {
+	void *dst = malloc(bytes > 0 ? bytes : 1);
+	if (src != NULL && bytes > 0)
+		memcpy(dst, src, bytes);
+	return dst;
+}
+
+/* Frees the per-call arrays that maximize() allocates on the common struct
+ * (maximize.c:58-97). The reference itself leaks them on every call. */
+static void free_common(struct max_data *c, int num_data) {
+	int d;
+	if (c->rmax == NULL)
+		return;
+	free(c->rmax); free(c->info); free(c->likelihood); free(c->max_exp_p);
+	free(c->quat_norm); free(c->num_prob); free(c->psum_d);
+	if (c->prob != NULL) {
+		for (d = 0; d < num_data; ++d) {
+			free(c->prob[d]);
+			free(c->place_prob[d]);
+		}
+	}
+	free(c->prob); free(c->place_prob);
+	if (c->u != NULL) {
+		free(c->u[0]);
+		free(c->u);
+	}
+	free(c->max_exp); free(c->p_norm); free(c->offset_prob);
+	memset(c, 0, sizeof(*c));
+}
+
+ref_engine *ref_create(int num_pix, const double *qvals, const double *corr, const uint8_t *mask,
+                       int num_data, const int *ones, const int *multi, const int *place_ones,
+                       const int *place_multi, const int *count_multi,
+                       int num_rot, const double *quats,
+                       long size, int num_modes, const double *model1,
+                       int need_scaling, int update_scale, int known_scale, double alpha,
+                       double beta_start, double beta_jump, int beta_period, double beta_factor,
+                       const double *scale, const uint8_t *blacklist, int num_threads) {
+	long d, ones_total = 0, multi_total = 0;
+	ref_engine *e = calloc(1, sizeof(ref_engine));
+	if (num_threads > 0)
+		omp_set_num_threads(num_threads);
+
+	/* Detector (detector.pyx:61-74) */
+	e->det.num_pix = num_pix;
+	e->det.qvals = dup_mem(qvals, (size_t)num_pix * 3 * sizeof(double));
+	e->det.corr = dup_mem(corr, (size_t)num_pix * sizeof(double));
+	e->det.raw_mask = dup_mem(mask, (size_t)num_pix);
+	e->det.with_bg = 0;
+
+	/* Sparse dataset, as parse_binarydataset lays it out (emcfile.c:15-37) */
+	e->dset.ftype = SPARSE;
+	e->dset.num_data = num_data;
+	e->dset.num_pix = num_pix;
+	e->dset.det = &e->det;
+	e->dset.next = NULL;
+	e->dset.num_offset = 0;
+	e->dset.ones = dup_mem(ones, (size_t)num_data * sizeof(int));
+	e->dset.multi = dup_mem(multi, (size_t)num_data * sizeof(int));
+	e->dset.ones_accum = malloc((size_t)(num_data > 0 ? num_data : 1) * sizeof(long));
+	e->dset.multi_accum = malloc((size_t)(num_data > 0 ? num_data : 1) * sizeof(long));
+	for (d = 0; d < num_data; ++d) {
+		e->dset.ones_accum[d] = ones_total;
+		e->dset.multi_accum[d] = multi_total;
+		ones_total += ones[d];
+		multi_total += multi[d];
+	}
+	e->dset.ones_total = ones_total;
+	e->dset.multi_total = multi_total;
+	e->dset.place_ones = dup_mem(place_ones, (size_t)ones_total * sizeof(int));
+	e->dset.place_multi = dup_mem(place_multi, (size_t)multi_total * sizeof(int));
+	e->dset.count_multi = dup_mem(count_multi, (size_t)multi_total * sizeof(int));
+
+	/* Parameters (params.pyx:13-46 defaults, then the values we are given) */
+	e->par.rank = 0;
+	e->par.num_proc = 1;
+	e->par.rtype = RECON3D;
+	e->par.verbosity = 0;
+	e->par.need_scaling = need_scaling;
+	e->par.update_scale = update_scale;
+	e->par.known_scale = known_scale;
+	e->par.alpha = alpha;
+	e->par.beta_jump = beta_jump;
+	e->par.beta_period = beta_period;
+	e->par.beta_factor = beta_factor;
+	e->par.num_modes = num_modes;
+	e->par.nonrot_modes = 0;
+	e->par.axial_sym = 1;
+	e->par.iteration = 1;
+
+	/* Orientations; Quaternion.divide for one rank (quaternion.pyx:156-175) */
+	e->quat.num_rot = num_rot;
+	e->quat.quats = dup_mem(quats, (size_t)num_rot * 5 * sizeof(double));
+	e->quat.num_rot_p = num_modes * num_rot;
+
+	/* Model (model.pyx:57-63, 280-284) */
+	e->mod.mtype = MODEL_3D;
+	e->mod.size = size;
+	e->mod.center = size / 2;
+	e->mod.vol = size * size * size;
+	e->mod.num_modes = num_modes;
+	e->mod.model1 = dup_mem(model1, (size_t)num_modes * e->mod.vol * sizeof(double));
+	e->mod.model2 = calloc((size_t)num_modes * e->mod.vol, sizeof(double));
+	e->mod.inter_weight = calloc((size_t)num_modes * e->mod.vol, sizeof(double));
+
+	/* Iterate.set_data (iterate.pyx:241-266) with one detector and one file */
+	e->iter.det = &e->det;
+	e->iter.mod = &e->mod;
+	e->iter.dset = &e->dset;
+	e->iter.quat = &e->quat;
+	e->iter.par = &e->par;
+	e->iter.tot_num_data = num_data;
+	e->iter.num_det = 1;
+	e->iter.num_dfiles = 1;
+	e->det_mapping[0] = 0;
+	e->iter.det_mapping = e->det_mapping;
+	calc_frame_counts(&e->iter);
+	/* Iterate.parse_blacklist copies the flags but never sets num_blacklist
+	 * (iterate.pyx:317-359), so it stays 0 as calloc left it. */
+	e->iter.blacklist = calloc((size_t)(num_data > 0 ? num_data : 1), 1);
+	if (blacklist != NULL)
+		memcpy(e->iter.blacklist, blacklist, (size_t)num_data);
+	calc_sum_fact(&e->iter);
+	if (need_scaling) {
+		e->iter.scale = malloc((size_t)(num_data > 0 ? num_data : 1) * sizeof(double));
+		for (d = 0; d < num_data; ++d)
+			e->iter.scale[d] = scale != NULL ? scale[d] : 1.;
+	}
+	calc_beta(beta_start, &e->iter);
+
+	e->mdata = calloc(1, sizeof(struct max_data));
+	e->mdata->iter = &e->iter;
+	return e;
+}
+
+/* recon.pyx:151-174 (update_beta) followed by recon.pyx:86-99 (maximize). */
+double ref_maximize(ref_engine *e, int iteration) {
+	int d;
+	struct iterate *it = &e->iter;
+	double factor;
+
+	e->par.iteration = iteration;
+	factor = pow(e->par.beta_jump, (double)((iteration - 1) / e->par.beta_period));
+	factor *= e->par.beta_factor;
+	for (d = 0; d < it->tot_num_data; ++d) {
+		if (it->blacklist[d] == 1)
+			continue;
+		it->beta[d] = it->beta_start[d] * factor;
+		if (it->beta[d] > 1.)
+			it->beta[d] = 1.;
+	}
+
+	slice_gen = &slice_gen3d;
+	slice_merge = &slice_merge3d;
+	free_common(e->mdata, it->tot_num_data);
+	e->mdata->iter = it;
+	e->mdata->within_openmp = 0;
+	e->avg_likelihood = maximize(e->mdata);
+	return e->avg_likelihood;
+}
+
+/* recon.pyx:112-149 for RECON3D without point-group or axial symmetry. */
+double ref_update_model(ref_engine *e) {
+	long x;
+	double diff, change = 0.;
+	struct model *mod = &e->mod;
+
+	for (x = 0; x < mod->num_modes; ++x)
+		symmetrize_friedel(&mod->model2[x * mod->vol], &mod->inter_weight[x * mod->vol], (int)mod->size);
+	for (x = 0; x < mod->num_modes * mod->vol; ++x)
+		if (mod->inter_weight[x] > 0.)
+			mod->model2[x] /= mod->inter_weight[x];
+	for (x = 0; x < mod->num_modes * mod->vol; ++x) {
+		diff = mod->model2[x] - mod->model1[x];
+		change += diff * diff;
+		if (e->par.alpha > 0.)
+			mod->model1[x] = e->par.alpha * mod->model1[x] + (1 - e->par.alpha) * mod->model2[x];
+		else
+			mod->model1[x] = mod->model2[x];
+	}
+	e->iter.rms_change = sqrt(change / mod->num_modes / mod->vol);
+	return e->iter.rms_change;
+}
+
+void ref_destroy(ref_engine *e) {
+	if (e == NULL)
+		return;
+	free_common(e->mdata, e->iter.tot_num_data);
+	free(e->mdata);
+	free(e->det.qvals); free(e->det.corr); free(e->det.raw_mask);
+	free(e->dset.ones); free(e->dset.multi); free(e->dset.ones_accum); free(e->dset.multi_accum);
+	free(e->dset.place_ones); free(e->dset.place_multi); free(e->dset.count_multi);
+	free(e->quat.quats);
+	free(e->mod.model1); free(e->mod.model2); free(e->mod.inter_weight);
+	free(e->iter.fcounts); free(e->iter.mean_count); free(e->iter.rescale);
+	free(e->iter.blacklist); free(e->iter.sum_fact); free(e->iter.scale);
+	free(e->iter.beta); free(e->iter.beta_start);
+	free(e);
+}
+
+/* ---- accessors (copies; arrays that a call did not produce are zero-filled) ---- */
+
+static void copy_or_zero(void *dst, const void *src, size_t bytes) {
+	if (src != NULL)
+		memcpy(dst, src, bytes);
+	else
+		memset(dst, 0, bytes);
+}
+
+long ref_model_len(ref_engine *e) { return e->mod.num_modes * e->mod.vol; }
+void ref_get_model1(ref_engine *e, double *o) { memcpy(o, e->mod.model1, ref_model_len(e) * sizeof(double)); }
+void ref_set_model1(ref_engine *e, const double *i) { memcpy(e->mod.model1, i, ref_model_len(e) * sizeof(double)); }
+void ref_get_model2(ref_engine *e, double *o) { memcpy(o, e->mod.model2, ref_model_len(e) * sizeof(double)); }
+void ref_get_weight(ref_engine *e, double *o) { memcpy(o, e->mod.inter_weight, ref_model_len(e) * sizeof(double)); }
+
+void ref_get_frame_arrays(ref_engine *e, int *rmax, double *info, double *likelihood, double *max_exp,
+                          double *p_norm, double *psum_d) {
+	size_t n = (size_t)e->iter.tot_num_data;
+	struct max_data *c = e->mdata;
+	copy_or_zero(rmax, c->rmax, n * sizeof(int));
+	copy_or_zero(info, c->info, n * sizeof(double));
+	copy_or_zero(likelihood, c->likelihood, n * sizeof(double));
+	copy_or_zero(max_exp, c->max_exp, n * sizeof(double));
+	copy_or_zero(p_norm, c->p_norm, n * sizeof(double));
+	copy_or_zero(psum_d, c->psum_d, n * sizeof(double));
+}
+
+void ref_get_quat_norm(ref_engine *e, double *o) {
+	size_t n = (size_t)e->iter.tot_num_data * e->mod.num_modes;
+	copy_or_zero(o, e->mod.num_modes > 1 ? e->mdata->quat_norm : NULL, n * sizeof(double));
+}
+
+void ref_get_u(ref_engine *e, double *o) {
+	copy_or_zero(o, e->mdata->u != NULL ? e->mdata->u[0] : NULL, (size_t)e->quat.num_rot_p * sizeof(double));
+}
+
+void ref_get_iter_arrays(ref_engine *e, int *fcounts, double *sum_fact, double *scale, double *beta,
+                         double *beta_start) {
+	size_t n = (size_t)e->iter.tot_num_data;
+	copy_or_zero(fcounts, e->iter.fcounts, n * sizeof(int));
+	copy_or_zero(sum_fact, e->iter.sum_fact, n * sizeof(double));
+	copy_or_zero(scale, e->iter.scale, n * sizeof(double));
+	copy_or_zero(beta, e->iter.beta, n * sizeof(double));
+	copy_or_zero(beta_start, e->iter.beta_start, n * sizeof(double));
+}
+
+void ref_set_scale(ref_engine *e, const double *scale) {
+	if (e->iter.scale != NULL)
+		memcpy(e->iter.scale, scale, (size_t)e->iter.tot_num_data * sizeof(double));
+}
+
+void ref_get_scalars(ref_engine *e, double *out) {
+	out[0] = e->iter.rescale[0];
+	out[1] = e->iter.mean_count[0];
+	out[2] = e->iter.mutual_info;
+	out[3] = e->avg_likelihood;
+	out[4] = e->iter.rms_change;
+}
+
+void ref_set_rms(ref_engine *e, double rms) { e->iter.rms_change = rms; }
+
+/* Model.slice_gen / slice_merge (model.pyx:105-151) on this engine's detector. */
+void ref_slice_gen(ref_engine *e, const double *quat, int mode, double *out) {
+	slice_gen3d((double *)quat, mode, out, &e->det, &e->mod);
+}
+
+void ref_slice_merge(ref_engine *e, const double *quat, int mode, const double *view, double *model2,
+                     double *weight) {
+	slice_merge3d((double *)quat, mode, (double *)view, model2, weight, e->mod.size, &e->det);
+}
+
+/* Quaternion.generate_3d (quaternion.pyx:94-102): count, and the list if out != NULL. */
+int ref_quat_gen(int num_div, double *out) {
+	struct quaternion q;
+	int n;
+	memset(&q, 0, sizeof(q));
+	n = quat_gen(num_div, &q);
+	if (out != NULL)
+		memcpy(out, q.quats, (size_t)n * 5 * sizeof(double));
+	free(q.quats);
+	return n;
+}
