@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of one EMC iteration (expand -> maximize -> compress).
+
+A step is one iteration -- maximize (slices, E-step with pruning, per-frame
+normalisation, M-step, merge, scale update) + update_model + normalize_scale --
+on the production-size plain workload:
+
+  260 x 257 flat pnCCD-like detector, 6-row panel gap (rows 127-132), radius-10
+  central hole; 201^3 model from 2000 Gaussian atoms in a radius-30 sphere;
+  num_div = 10 (50100 orientations); 200000 frames with lognormal fluence
+  (median 300 photons, sigma 0.5); scale update on; beta from 0.01, x sqrt(2)
+  every 5 iterations, capped at 1.
+
+Data are seeded synthetic inputs of that shape (no dataset is involved);
+frames are simulated on the GPU by the library. Every input (frames, log-slices,
+per-pair buffers) is far larger than the 126 MB L2, so no flush is needed
+between iterations.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU engine (dragonfly/src compiled
+into oracle/_ref) on the host cores, on a bounded frame sample of the same
+workload. With N > 1 each rank runs an independent replica (the iteration
+needs no collective); rank 0 prints the JSON line.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="plain EMC: 260x257 pnCCD-like detector, 201^3 model, 50100 orientations, "
+                     "200000 frames, median 300 photons, scale update, beta 0.01 x sqrt2 / 5",
+                det=(260, 257), gap_rows=list(range(127, 133)), hole=10., size=201, qmax=100.,
+                n_atoms=2000, atom_radius=30., num_div=10, n_frames=200000, median_photons=300.,
+                fluence_sigma=0.5, beta=0.01, beta_jump=math.sqrt(2.), beta_period=5)
+METRIC = "frame x orientation pairs per second of one plain EMC iteration"
+UNIT = "pairs/s"
+
+
+# ---------------------------------------------------------------------------
+# inputs
+# ---------------------------------------------------------------------------
+def build_inputs(w, seed=1234):
+    """Host-side inputs: detector, intensity model, orientations, per-frame
+    orientations and fluence, start model."""
+    from dragonfly_b200 import synth
+    from dragonfly_b200.quatgen import quat_gen
+    rng = np.random.default_rng(seed)
+    intens = synth.gaussian_atom_intensity(w["n_atoms"], w["atom_radius"], w["size"], rng)
+    qvals, corr, mask, detd, ewald = synth.flat_detector(w["det"][0], w["det"][1], w["qmax"], w["size"],
+                                                         hole_radius=w["hole"], gap_rows=w["gap_rows"])
+    intens *= w["median_photons"] / synth.model_mean_count(intens, qvals, corr, mask, rng, n_orient=48)
+    quats = quat_gen(w["num_div"])
+    n = w["n_frames"]
+    frame_q = synth.random_quaternions(n, rng)
+    phi = np.exp(rng.normal(0., w["fluence_sigma"], n))
+    model_mean = w["median_photons"] * math.exp(w["fluence_sigma"] ** 2 / 2) / (mask == 0).sum() * 2.
+    start = rng.random((1,) + (w["size"],) * 3) * model_mean
+    return dict(qvals=qvals, corr=corr, mask=mask, intens=intens, quats=quats, frame_q=frame_q, phi=phi,
+                start=start)
+
+
+def clock_sampler(device_index):
+    """Starts nvidia-smi sampling clocks every 200 ms; returns (proc, path)."""
+    fd, path = tempfile.mkstemp(suffix=".csv")
+    os.close(fd)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        proc = subprocess.Popen(["nvidia-smi", "--id=%d" % device_index, "--query-gpu=" + q,
+                                 "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except OSError:
+        proc = None
+    return proc, path
+
+
+def clock_summary(proc, path):
+    if proc is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    proc.terminate()
+    proc.wait()
+    sm, smax, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in open(path):
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            smax.append(float(f[2]))
+        except ValueError:
+            continue
+        for k, v in zip(names, f[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(k)
+    os.unlink(path)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "of measured"
+    except Exception:
+        return 6650., "of fallback"
+
+
+def roofline_traffic(kernel, units):
+    """DRAM traffic per launch from the committed ncu summary (bytes per unit
+    of work, scaled to this launch), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_per_unit.json")) as f:
+            t = json.load(f)
+        return t[kernel]["bytes_per_unit"] * units
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# reference engine on the host cores
+# ---------------------------------------------------------------------------
+def reference_threads(w):
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        per_thread = 2 * w["size"] ** 3 * 8 * 1.3  # private model + weight copies (maximize.c:103-104)
+        n = max(1, min(n, int(avail * 0.5 // per_thread)))
+    except Exception:
+        pass
+    return n
+
+
+def reference_step(w, inp, n_frames, seed, threads):
+    """One reference iteration (maximize + update_model + normalize_scale) on
+    n_frames frames at the full orientation set. Returns seconds."""
+    from dragonfly_b200 import synth
+    from oracle.oracle import EMCProblem, ReferenceEngine
+    rng = np.random.default_rng(seed)
+    phi = np.exp(rng.normal(0., w["fluence_sigma"], n_frames))
+    fr = synth.sample_frames(inp["intens"], inp["qvals"], inp["corr"], inp["mask"], n_frames, rng, phi=phi)
+    prob = EMCProblem(inp["qvals"], inp["corr"], inp["mask"], fr["ones"], fr["multi"], fr["place_ones"],
+                      fr["place_multi"], fr["count_multi"], inp["quats"], inp["start"], need_scaling=1,
+                      update_scale=1, beta=w["beta"], beta_jump=w["beta_jump"], beta_period=w["beta_period"])
+    eng = ReferenceEngine(prob, num_threads=threads, fast=True)
+    t0 = time.perf_counter()
+    eng.run_iteration(1)
+    t = time.perf_counter() - t0
+    eng.close()
+    return t
+
+
+def reference_throughput(w, inp, threads, budget_s=40., steps=2):
+    """Reference pairs/s at the full frame count, extrapolated from frame
+    samples: t(n) = a + b n fitted on samples of n and 4 n frames."""
+    R = inp["quats"].shape[0]
+    n1 = 64
+    t1 = reference_step(w, inp, n1, 11, threads)
+    # grow the sample while a step stays well inside the budget
+    while t1 < budget_s / 10 and n1 < 4096:
+        n1 *= 2
+        t1 = reference_step(w, inp, n1, 11, threads)
+    n2 = 4 * n1
+    times = {n1: [t1]}
+    for k in range(max(1, steps - 1)):
+        times.setdefault(n2, []).append(reference_step(w, inp, n2, 12 + k, threads))
+    t2 = float(np.mean(times[n2]))
+    b = max((t2 - t1) / (n2 - n1), 1e-12)
+    a = max(t1 - b * n1, 0.)
+    N = w["n_frames"]
+    t_full = a + b * N
+    return dict(value=R * N / t_full, t_full=t_full, fixed_s=a, per_frame_s=b, samples={n1: t1, n2: t2},
+                raw_sample_pairs_s=R * n2 / t2, cores=threads)
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    from dragonfly_b200._lib import Context
+    import torch
+    w = dict(WORKLOAD)
+    if args.frames:
+        w["n_frames"] = args.frames
+    if args.num_div:
+        w["num_div"] = args.num_div
+    t_setup = time.perf_counter()
+    inp = build_inputs(w)
+    ctx = Context(local_rank)
+    ctx.set_detector(inp["qvals"], inp["corr"], inp["mask"])
+    tot = ctx.simulate_frames(inp["intens"], inp["frame_q"], inp["phi"], seed=777 + rank)
+    ctx.set_quaternions(inp["quats"])
+    ctx.set_model(inp["start"])
+    ctx.calc_beta(w["beta"], 1)
+    R = inp["quats"].shape[0]
+    N = w["n_frames"]
+    setup_s = time.perf_counter() - t_setup
+
+    def params(it):
+        return ctx.params(it, need_scaling=1, update_scale=1, known_scale=0, beta_jump=w["beta_jump"],
+                          beta_period=w["beta_period"], beta_factor=1.)
+
+    def step(it):
+        ctx.maximize(params(it))
+        ctx.update_model(0.)
+        ctx.normalize_scale()
+
+    it = 1
+    for _ in range(args.warmup):
+        step(it)
+        it += 1
+    wl = ctx.workload()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # timed region: K iterations bracketed by events on the library's stream
+    ctx.set_option("timing", 1)
+    ctx.reset_phase_times()
+    launches0 = ctx.workload()["launches"]
+    proc, cpath = clock_sampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    ctx.event_record(0)
+    for _ in range(args.steps):
+        step(it)
+        it += 1
+    ctx.event_record(1)
+    total_ms = ctx.event_elapsed_ms(0, 1)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clock_summary(proc, cpath)
+    launches = ctx.workload()["launches"] - launches0
+    phases = ctx.phase_times()
+    ctx.set_option("timing", 0)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda:%d" % local_rank, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * R * N / (ms_per_step / 1e3)
+
+    # end to end through the host-buffer entry point: model in pinned host
+    # memory uploaded, iteration, model + rmax + likelihood read back, per step
+    model_h = torch.empty(inp["start"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    rmax_h = torch.empty(N, dtype=torch.int32, pin_memory=True).numpy()
+    ll_h = torch.empty(N, dtype=torch.float64, pin_memory=True).numpy()
+    m1, _, _ = ctx.model()
+    model_h[...] = m1
+    barrier()
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.run_iteration_host(params(it), model_h, 0., rmax_h, ll_h)
+        e2e.append(time.perf_counter() - t0)
+        it += 1
+    e2e_s = float(np.mean(e2e))
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda:%d" % local_rank, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    # roofline of the dominant kernel (per-launch CUDA-event durations)
+    dom = max(phases, key=lambda k: phases[k][0])
+    ms, nl = phases[dom]
+    peak, peak_src = measured_peaks()
+    E, EM = wl["estep_entries"], wl["mstep_entries"]
+    chunks = max(wl["chunks"], 1)
+    algo = {  # algorithmic bytes per launch
+        "estep": 4. * R * E / chunks,             # one FP32 log-slice value per orientation x photon entry
+        "mstep": 4. * R * EM / chunks,            # one FP32 probability per orientation x photon entry
+        "slice": (4. * R * inp["qvals"].shape[0]) / 3,  # log-slice output, over 3 launches
+        "norm": 3 * 8. * R * N / chunks,          # three passes over FP64 log-likelihoods
+        "psum": 4. * R * N / chunks / 2,
+        "merge": 8. * inp["start"].size,
+        "update": 8. * inp["start"].size,
+    }
+    per_launch_s = (ms / 1e3) / max(nl, 1)
+    achieved = algo[dom] / per_launch_s / 1e9
+    units = R * (E if dom == "estep" else EM) / chunks
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_src,
+            "traffic": roofline_traffic(dom, units),
+            "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64 accumulate / f32 log-slices",
+           "data": "synthetic (seeded; frames simulated on the GPU)",
+           "config": {"workload": w["name"], "num_orientations": R, "num_frames": N,
+                      "photons_per_frame_mean": tot[2] / N, "detector_pixels": int(inp["qvals"].shape[0]),
+                      "model": "%d^3 x %d mode" % (w["size"], 1), "frame_chunks": wl["chunks"],
+                      "l2": "inputs larger than L2 (no flush needed)",
+                      "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
+                      "setup_s": setup_s},
+           "s_per_iteration": ms_per_step / 1e3,
+           "clocks": clocks,
+           "e2e": {"value": world * R * N / e2e_s, "unit": UNIT,
+                   "h2d_bytes_per_step": int(model_h.nbytes),
+                   "d2h_bytes_per_step": int(model_h.nbytes + rmax_h.nbytes + ll_h.nbytes),
+                   "s_per_iteration": e2e_s},
+           "gpu_launches": int(launches),
+           "roofline": roof}
+    ctx.close()
+    return out, inp, w
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=0, help="override the frame count (testing)")
+    ap.add_argument("--num-div", type=int, default=0, help="override num_div (testing)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w = dict(WORKLOAD)
+        if args.frames:
+            w["n_frames"] = args.frames
+        if args.num_div:
+            w["num_div"] = args.num_div
+        from oracle.oracle import reference_available, build_oracle
+        if not reference_available(fast=True):
+            try:
+                build_oracle()
+            except Exception:
+                pass
+        if not reference_available(fast=True):
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "reference engine library oracle/_ref/libdragonfly_ref_fast.so not built"}))
+            return
+        inp = build_inputs(w)
+        threads = reference_threads(w)
+        for _ in range(args.warmup):
+            pass  # every reference step builds its own engine; nothing to warm
+        res = reference_throughput(w, inp, threads, steps=max(2, args.steps))
+        sample = ("reference engine (dragonfly/src, -O3 -march=native, OpenMP %d threads) on %s frames at "
+                  "all %d orientations; t(n) = a + b n fitted, extrapolated to %d frames"
+                  % (threads, "/".join(str(k) for k in res["samples"]), inp["quats"].shape[0], w["n_frames"]))
+        out = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["t_full"] * 1e3,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (seeded)", "impl": "reference",
+               "config": {"workload": w["name"], "num_orientations": int(inp["quats"].shape[0]),
+                          "num_frames": w["n_frames"], "parallelism": "host cores"},
+               "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+                                "sample": sample, "fixed_s": res["fixed_s"], "per_frame_s": res["per_frame_s"]},
+               "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
+
+    import torch
+    if world > 1:
+        torch.cuda.set_device(local_rank)
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    out, inp, w = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.oracle import reference_available
+        if reference_available(fast=True):
+            threads = reference_threads(w)
+            res = reference_throughput(w, inp, threads, budget_s=30., steps=2)
+            out["cpu_baseline"] = {
+                "value": res["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": "reference engine (dragonfly/src) on %s frames at all orientations, OpenMP %d threads; "
+                          "extrapolated to %d frames by t(n) = a + b n" % (
+                              "/".join(str(k) for k in res["samples"]), threads, w["n_frames"]),
+                "raw_sample_pairs_s": res["raw_sample_pairs_s"]}
+        else:
+            out["cpu_baseline"] = None
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

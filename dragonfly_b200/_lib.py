@@ -1,0 +1,326 @@
+"""ctypes binding of libdfgpu.so, the C ABI in include/dragonfly_b200.h.
+
+The library is the only compute path of this package: if it cannot be loaded
+(not built, or no CUDA driver) every call raises; there is no CPU fallback.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdfgpu.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "dragonfly_b200.h")
+
+DFG_OK, DFG_ERR_ARG, DFG_ERR_CUDA, DFG_ERR_STATE, DFG_ERR_NOMEM = range(5)
+PHASES = ("slice", "estep", "norm", "psum", "mstep", "merge", "update")
+
+
+class DFGError(RuntimeError):
+    """A call into libdfgpu.so returned an error code."""
+
+    def __init__(self, code, msg):
+        super().__init__("dragonfly_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class IterParams(C.Structure):
+    _fields_ = [("iteration", C.c_int), ("need_scaling", C.c_int), ("update_scale", C.c_int),
+                ("known_scale", C.c_int), ("beta_jump", C.c_double), ("beta_period", C.c_int),
+                ("beta_factor", C.c_double)]
+
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_U8 = C.POINTER(C.c_uint8)
+_V = C.c_void_p
+
+_SIGS = {
+    "dfg_version": (C.c_char_p, []),
+    "dfg_create": (C.c_int, [C.c_int, C.POINTER(_V)]),
+    "dfg_destroy": (None, [_V]),
+    "dfg_last_error": (C.c_char_p, [_V]),
+    "dfg_set_detector": (C.c_int, [_V, C.c_int, _D, _D, _U8]),
+    "dfg_set_frames": (C.c_int, [_V, C.c_int, _I, _I, _I, _I, _I]),
+    "dfg_set_quaternions": (C.c_int, [_V, C.c_int, _D]),
+    "dfg_set_model": (C.c_int, [_V, C.c_long, C.c_int, _D]),
+    "dfg_set_scale": (C.c_int, [_V, _D]),
+    "dfg_set_blacklist": (C.c_int, [_V, _U8]),
+    "dfg_set_beta_start": (C.c_int, [_V, _D]),
+    "dfg_calc_beta": (C.c_int, [_V, C.c_double, C.c_int]),
+    "dfg_maximize": (C.c_int, [_V, C.POINTER(IterParams), _D]),
+    "dfg_update_model": (C.c_int, [_V, C.c_double, _D]),
+    "dfg_normalize_scale": (C.c_int, [_V, _D]),
+    "dfg_get_frame_results": (C.c_int, [_V, _I, _D, _D, _D, _D, _D]),
+    "dfg_get_quat_norm": (C.c_int, [_V, _D]),
+    "dfg_get_orientation_results": (C.c_int, [_V, _D, _D]),
+    "dfg_get_model": (C.c_int, [_V, _D, _D, _D]),
+    "dfg_get_frame_params": (C.c_int, [_V, _D, _D, _D, _I, _D, _U8]),
+    "dfg_get_scalars": (C.c_int, [_V, _D]),
+    "dfg_get_num_prob": (C.c_int, [_V, _I]),
+    "dfg_slice_gen": (C.c_int, [_V, _D, C.c_int, _D]),
+    "dfg_slice_merge": (C.c_int, [_V, _D, C.c_int, _D, _D, _D]),
+    "dfg_run_iteration_host": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D, _I, _D, _D, _D]),
+    "dfg_set_option": (C.c_int, [_V, C.c_char_p, C.c_double]),
+    "dfg_get_phase_times": (C.c_int, [_V, _D, C.POINTER(C.c_long), C.c_int]),
+    "dfg_phase_name": (C.c_char_p, [C.c_int]),
+    "dfg_reset_phase_times": (C.c_int, [_V]),
+    "dfg_get_workload": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
+    "dfg_simulate_frames": (C.c_int, [_V, C.c_long, _D, C.c_int, _D, _D, C.c_ulonglong,
+                                      C.POINTER(C.c_longlong)]),
+    "dfg_get_frames": (C.c_int, [_V, _I, _I, _I, _I, _I]),
+    "dfg_event_record": (C.c_int, [_V, C.c_int]),
+    "dfg_event_elapsed": (C.c_int, [_V, C.c_int, C.c_int, _D]),
+}
+
+_lib = None
+
+
+def header_symbols():
+    """Entry points declared in include/dragonfly_b200.h."""
+    with open(HEADER) as f:
+        return re.findall(r"^DFG_API[^(]*?\b(dfg_\w+)\s*\(", f.read(), flags=re.M)
+
+
+def load():
+    """Loads libdfgpu.so (raises OSError if it is missing or does not load)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libdfgpu.so is not built (run python -m dragonfly_b200.build): %s" % LIB_PATH)
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def ptr(a, ctype):
+    """Pointer to a C-contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Context:
+    """Owner of one dfg_ctx (one GPU's resident inputs and work buffers)."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = _V()
+        rc = self.lib.dfg_create(int(device), C.byref(h))
+        if rc != DFG_OK:
+            raise DFGError(rc, "dfg_create(device=%d) failed (no usable CUDA device?)" % device)
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dfg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != DFG_OK:
+            raise DFGError(rc, self.lib.dfg_last_error(self.h).decode())
+        return rc
+
+    def call(self, name, *args):
+        return self.check(getattr(self.lib, name)(self.h, *args))
+
+    # -- inputs ------------------------------------------------------------
+    def set_detector(self, qvals, corr, mask):
+        q = np.ascontiguousarray(qvals, np.float64).reshape(-1)
+        c = np.ascontiguousarray(corr, np.float64)
+        m = np.ascontiguousarray(mask, np.uint8)
+        if q.size != 3 * c.size or m.size != c.size:
+            raise ValueError("qvals must be [P,3], corr and mask [P]")
+        self.call("dfg_set_detector", c.size, ptr(q, C.c_double), ptr(c, C.c_double), ptr(m, C.c_uint8))
+        self.num_pix = c.size
+
+    def set_frames(self, ones, multi, place_ones, place_multi, count_multi):
+        a = [np.ascontiguousarray(x, np.int32) for x in (ones, multi, place_ones, place_multi, count_multi)]
+        if a[1].size != a[0].size or a[4].size != a[3].size:
+            raise ValueError("ones/multi and place_multi/count_multi lengths differ")
+        if a[2].size != int(a[0].sum()) or a[3].size != int(a[1].sum()):
+            raise ValueError("place arrays do not match the per-frame counts")
+        self.call("dfg_set_frames", a[0].size, *[ptr(x, C.c_int) for x in a])
+        self.num_data = a[0].size
+
+    def set_quaternions(self, quats):
+        q = np.ascontiguousarray(quats, np.float64).reshape(-1, 5)
+        self.call("dfg_set_quaternions", q.shape[0], ptr(q, C.c_double))
+        self.num_rot = q.shape[0]
+
+    def set_model(self, model1):
+        m = np.ascontiguousarray(model1, np.float64)
+        if m.ndim == 3:
+            m = m[None]
+        self.call("dfg_set_model", m.shape[-1], m.shape[0], ptr(m, C.c_double))
+        self.model_shape = m.shape
+
+    def set_scale(self, scale):
+        s = np.ascontiguousarray(scale, np.float64)
+        self.call("dfg_set_scale", ptr(s, C.c_double))
+
+    def set_blacklist(self, blacklist):
+        b = np.ascontiguousarray(blacklist, np.uint8)
+        self.call("dfg_set_blacklist", ptr(b, C.c_uint8))
+
+    def set_beta_start(self, beta_start):
+        b = np.ascontiguousarray(beta_start, np.float64)
+        self.call("dfg_set_beta_start", ptr(b, C.c_double))
+
+    def calc_beta(self, start, need_scaling):
+        self.call("dfg_calc_beta", float(start), int(need_scaling))
+
+    def set_option(self, key, value):
+        self.call("dfg_set_option", key.encode(), float(value))
+
+    # -- iteration ---------------------------------------------------------
+    @staticmethod
+    def params(iteration, need_scaling=0, update_scale=1, known_scale=0, beta_jump=1.,
+               beta_period=100, beta_factor=1.):
+        return IterParams(int(iteration), int(need_scaling), int(update_scale), int(known_scale),
+                          float(beta_jump), int(beta_period), float(beta_factor))
+
+    def maximize(self, par):
+        ll = C.c_double(0.)
+        self.call("dfg_maximize", C.byref(par), C.byref(ll))
+        return ll.value
+
+    def update_model(self, alpha=0.):
+        rms = C.c_double(0.)
+        self.call("dfg_update_model", float(alpha), C.byref(rms))
+        return rms.value
+
+    def normalize_scale(self):
+        m = C.c_double(0.)
+        self.call("dfg_normalize_scale", C.byref(m))
+        return m.value
+
+    def run_iteration_host(self, par, model1, alpha=0., rmax=None, likelihood=None):
+        """model1 (float64, C order) is updated in place."""
+        ll = C.c_double(0.)
+        rms = C.c_double(0.)
+        self.call("dfg_run_iteration_host", C.byref(par), float(alpha), ptr(model1, C.c_double),
+                  ptr(rmax, C.c_int), ptr(likelihood, C.c_double), C.byref(ll), C.byref(rms))
+        return ll.value, rms.value
+
+    # -- results -----------------------------------------------------------
+    def frame_results(self):
+        n = self.num_data
+        rmax = np.zeros(n, np.int32)
+        info, ll, mx, pn, pd = (np.zeros(n) for _ in range(5))
+        self.call("dfg_get_frame_results", ptr(rmax, C.c_int), ptr(info, C.c_double), ptr(ll, C.c_double),
+                  ptr(mx, C.c_double), ptr(pn, C.c_double), ptr(pd, C.c_double))
+        return dict(rmax=rmax, info=info, likelihood=ll, max_exp=mx, p_norm=pn, psum_d=pd)
+
+    def num_prob(self):
+        out = np.zeros(self.num_data, np.int32)
+        self.call("dfg_get_num_prob", ptr(out, C.c_int))
+        return out
+
+    def quat_norm(self):
+        out = np.zeros((self.num_data, self.model_shape[0]))
+        self.call("dfg_get_quat_norm", ptr(out, C.c_double))
+        return out
+
+    def orientation_results(self):
+        R = self.model_shape[0] * self.num_rot
+        u, pr = np.zeros(R), np.zeros(R)
+        self.call("dfg_get_orientation_results", ptr(u, C.c_double), ptr(pr, C.c_double))
+        return u, pr
+
+    def model(self):
+        m1, m2, w = (np.zeros(self.model_shape) for _ in range(3))
+        self.call("dfg_get_model", ptr(m1, C.c_double), ptr(m2, C.c_double), ptr(w, C.c_double))
+        return m1, m2, w
+
+    def frame_params(self):
+        n = self.num_data
+        sc, be, bs, sf = (np.zeros(n) for _ in range(4))
+        fc = np.zeros(n, np.int32)
+        bl = np.zeros(n, np.uint8)
+        self.call("dfg_get_frame_params", ptr(sc, C.c_double), ptr(be, C.c_double), ptr(bs, C.c_double),
+                  ptr(fc, C.c_int), ptr(sf, C.c_double), ptr(bl, C.c_uint8))
+        return dict(scale=sc, beta=be, beta_start=bs, fcounts=fc, sum_fact=sf, blacklist=bl)
+
+    def scalars(self):
+        out = np.zeros(5)
+        self.call("dfg_get_scalars", ptr(out, C.c_double))
+        return dict(rescale=out[0], mutual_info=out[1], avg_likelihood=out[2], mean_count=out[3],
+                    rms_change=out[4])
+
+    def slice_gen(self, quat, mode=0):
+        q = np.ascontiguousarray(quat, np.float64)
+        if q.size == 4:
+            q = np.append(q, 1.)
+        out = np.zeros(self.num_pix)
+        self.call("dfg_slice_gen", ptr(q, C.c_double), int(mode), ptr(out, C.c_double))
+        return out
+
+    def slice_merge(self, quat, view, model2, inter_weight, mode=0):
+        q = np.ascontiguousarray(quat, np.float64)
+        if q.size == 4:
+            q = np.append(q, 1.)
+        v = np.ascontiguousarray(view, np.float64)
+        self.call("dfg_slice_merge", ptr(q, C.c_double), int(mode), ptr(v, C.c_double),
+                  ptr(model2, C.c_double), ptr(inter_weight, C.c_double))
+
+    def phase_times(self):
+        ms = np.zeros(len(PHASES))
+        la = (C.c_long * len(PHASES))()
+        self.check(0 if self.lib.dfg_get_phase_times(self.h, ptr(ms, C.c_double), la, len(PHASES)) >= 0 else 1)
+        return {PHASES[i]: (ms[i], la[i]) for i in range(len(PHASES))}
+
+    def reset_phase_times(self):
+        self.call("dfg_reset_phase_times")
+
+    def simulate_frames(self, intens, quats4, phi, seed):
+        """Poisson frames of intens at quats4 [N,4] times phi [N]; they become
+        this context's frames. Returns (ones_total, multi_total, photons)."""
+        m = np.ascontiguousarray(intens, np.float64)
+        q = np.ascontiguousarray(np.asarray(quats4)[:, :4], np.float64)
+        f = np.ascontiguousarray(phi, np.float64)
+        tot = (C.c_longlong * 3)()
+        self.call("dfg_simulate_frames", m.shape[-1], ptr(m, C.c_double), q.shape[0], ptr(q, C.c_double),
+                  ptr(f, C.c_double), int(seed), tot)
+        self.num_data = q.shape[0]
+        self._frame_totals = (tot[0], tot[1])
+        return tuple(tot)
+
+    def get_frames(self):
+        """The context's sparse frames (ones, multi, place_ones, place_multi, count_multi)."""
+        n = self.num_data
+        ones, multi = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self.call("dfg_get_frames", ptr(ones, C.c_int), ptr(multi, C.c_int), None, None, None)
+        po = np.zeros(int(ones.sum()), np.int32)
+        pm = np.zeros(int(multi.sum()), np.int32)
+        cm = np.zeros(int(multi.sum()), np.int32)
+        self.call("dfg_get_frames", None, None, ptr(po, C.c_int), ptr(pm, C.c_int), ptr(cm, C.c_int))
+        return ones, multi, po, pm, cm
+
+    def event_record(self, slot):
+        self.call("dfg_event_record", int(slot))
+
+    def event_elapsed_ms(self, a, b):
+        ms = C.c_double(0.)
+        self.call("dfg_event_elapsed", int(a), int(b), C.byref(ms))
+        return ms.value
+
+    def workload(self):
+        out = (C.c_longlong * 7)()
+        self.call("dfg_get_workload", out)
+        keys = ("num_orient", "num_data", "estep_entries", "mstep_entries", "chunks", "chunk_frames",
+                "launches")
+        return dict(zip(keys, list(out)))

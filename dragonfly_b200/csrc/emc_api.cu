@@ -1,0 +1,858 @@
+// C ABI of the B200 EMC iteration (declared in include/dragonfly_b200.h).
+//
+// The context keeps every input resident in HBM and re-uses its work buffers
+// across iterations. One iteration (dfg_maximize) is a fixed sequence of
+// kernels on the context's stream:
+//   slice_log -> u_reduce -> rescale                   (calculate_rescale + slices)
+//   for each frame chunk:
+//       estep -> norm -> psum_r -> mstep               (calculate_prob .. update_tomogram)
+//   merge -> unpack -> [scale]                          (merge_tomogram, update_scale)
+// The frame chunk bounds the per-pair buffers (12 bytes per orientation x frame).
+
+#include "emc_ctx.cuh"
+#include "emc_device.cuh"
+
+using namespace dfg;
+
+// ---------------------------------------------------------------------------
+// phase timing
+// ---------------------------------------------------------------------------
+static void phase_begin(dfg_ctx *ctx, int ph) {
+	if (ctx->timing)
+		cudaEventRecord(ctx->ev[2 * ph], ctx->stream);
+}
+static void phase_end(dfg_ctx *ctx, int ph, long launches) {
+	if (!ctx->timing)
+		return;
+	cudaEventRecord(ctx->ev[2 * ph + 1], ctx->stream);
+	cudaEventSynchronize(ctx->ev[2 * ph + 1]);
+	float ms = 0.f;
+	cudaEventElapsedTime(&ms, ctx->ev[2 * ph], ctx->ev[2 * ph + 1]);
+	ctx->phase_ms[ph] += ms;
+	ctx->phase_launches[ph] += launches;
+}
+
+// ---------------------------------------------------------------------------
+// lifetime
+// ---------------------------------------------------------------------------
+extern "C" const char *dfg_version(void) { return "dragonfly_b200 0.1 (sm_100a)"; }
+
+extern "C" int dfg_create(int device, dfg_ctx **out) {
+	if (out == nullptr)
+		return DFG_ERR_ARG;
+	*out = nullptr;
+	int n = 0;
+	if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+		return DFG_ERR_CUDA;
+	if (cudaSetDevice(device) != cudaSuccess)
+		return DFG_ERR_CUDA;
+	dfg_ctx *ctx = new dfg_ctx();
+	ctx->device = device;
+	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+		delete ctx;
+		return DFG_ERR_CUDA;
+	}
+	for (auto &e : ctx->ev)
+		cudaEventCreate(&e);
+	for (auto &e : ctx->user_ev)
+		cudaEventCreate(&e);
+	*out = ctx;
+	return DFG_OK;
+}
+
+extern "C" void dfg_destroy(dfg_ctx *ctx) {
+	if (ctx == nullptr)
+		return;
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	for (auto &e : ctx->ev)
+		if (e)
+			cudaEventDestroy(e);
+	for (auto &e : ctx->user_ev)
+		if (e)
+			cudaEventDestroy(e);
+	ctx->chunks.clear();
+	cudaStreamDestroy(ctx->stream);
+	delete ctx;
+}
+
+extern "C" const char *dfg_last_error(const dfg_ctx *ctx) {
+	return ctx == nullptr ? "null context" : ctx->err.c_str();
+}
+
+// ---------------------------------------------------------------------------
+// inputs
+// ---------------------------------------------------------------------------
+extern "C" int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, const double *corr,
+                                const uint8_t *raw_mask) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(num_pix > 0 && qvals && corr && raw_mask, DFG_ERR_ARG, "detector: need num_pix > 0 and arrays");
+	NEED((uint32_t)num_pix <= IDX_MASK + 1u, DFG_ERR_ARG, "detector: at most %u pixels", IDX_MASK + 1u);
+	for (long long i = 0; i < 3LL * num_pix; ++i)
+		NEED(std::isfinite(qvals[i]), DFG_ERR_ARG, "detector: qvals[%lld] is not finite", i);
+	for (int i = 0; i < num_pix; ++i)
+		NEED(std::isfinite(corr[i]), DFG_ERR_ARG, "detector: corr[%d] is not finite", i);
+	CK(cudaSetDevice(ctx->device));
+	if (ctx->P != 0 && ctx->P != num_pix)
+		ctx->chunks_R = -1;
+	ctx->P = num_pix;
+	ctx->h_mask.assign(raw_mask, raw_mask + num_pix);
+	CK(upload(ctx->qvals, qvals, 3 * (size_t)num_pix, ctx->stream));
+	CK(upload(ctx->corr, corr, (size_t)num_pix, ctx->stream));
+	CK(upload(ctx->mask, raw_mask, (size_t)num_pix, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->chunks_R = -1;  // photon lists depend on the mask
+	if (ctx->N > 0) {
+		int rc = dfg_set_frames(ctx, ctx->N, ctx->h_ones.data(), ctx->h_multi.data(), ctx->h_place_ones.data(),
+		                        ctx->h_place_multi.data(), ctx->h_count_multi.data());
+		if (rc != DFG_OK)
+			return rc;
+	}
+	return DFG_OK;
+}
+
+// Packs (index, count) words, splitting counts above MAX_COUNT.
+static inline void push_word(std::vector<uint32_t> &v, uint32_t idx, long long count) {
+	while (count > 0) {
+		uint32_t c = (uint32_t)std::min<long long>(count, MAX_COUNT);
+		v.push_back(idx | (c << IDX_BITS));
+		count -= c;
+	}
+}
+
+extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const int *multi,
+                              const int *place_ones, const int *place_multi, const int *count_multi) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->P > 0, DFG_ERR_STATE, "frames: set the detector first");
+	NEED(num_data > 0 && ones && multi, DFG_ERR_ARG, "frames: need num_data > 0, ones and multi");
+	NEED((uint32_t)num_data <= IDX_MASK + 1u, DFG_ERR_ARG, "frames: at most %u frames", IDX_MASK + 1u);
+	CK(cudaSetDevice(ctx->device));
+	const int N = num_data, P = ctx->P;
+	std::vector<long long> oo(N + 1, 0), mo(N + 1, 0);
+	for (int d = 0; d < N; ++d) {
+		NEED(ones[d] >= 0 && multi[d] >= 0, DFG_ERR_ARG, "frames: negative ones/multi at frame %d", d);
+		oo[d + 1] = oo[d] + ones[d];
+		mo[d + 1] = mo[d] + multi[d];
+	}
+	NEED(oo[N] == 0 || place_ones, DFG_ERR_ARG, "frames: place_ones missing");
+	NEED(mo[N] == 0 || (place_multi && count_multi), DFG_ERR_ARG, "frames: place_multi/count_multi missing");
+	for (long long i = 0; i < oo[N]; ++i)
+		NEED(place_ones[i] >= 0 && place_ones[i] < P, DFG_ERR_ARG, "frames: place_ones[%lld] = %d out of [0, %d)",
+		     i, place_ones[i], P);
+	for (long long i = 0; i < mo[N]; ++i) {
+		NEED(place_multi[i] >= 0 && place_multi[i] < P, DFG_ERR_ARG,
+		     "frames: place_multi[%lld] = %d out of [0, %d)", i, place_multi[i], P);
+		NEED(count_multi[i] >= 1, DFG_ERR_ARG, "frames: count_multi[%lld] = %d < 1", i, count_multi[i]);
+	}
+	// host copies (the M-step index is rebuilt per frame chunk)
+	if (ones != ctx->h_ones.data()) {
+		ctx->h_ones.assign(ones, ones + N);
+		ctx->h_multi.assign(multi, multi + N);
+		ctx->h_place_ones.assign(place_ones, place_ones + oo[N]);
+		ctx->h_place_multi.assign(place_multi, place_multi + mo[N]);
+		ctx->h_count_multi.assign(count_multi, count_multi + mo[N]);
+	}
+	ctx->h_ones_off = oo;
+	ctx->h_multi_off = mo;
+	ctx->N = N;
+
+	// E-step lists: photons on mask == 0 pixels, ones then multi, per frame;
+	// fcounts, sum_fact, mean_count as calc_frame_counts / calc_sum_fact
+	// (iterate.c:3-117).
+	const uint8_t *mk = ctx->h_mask.data();
+	std::vector<uint32_t> words;
+	words.reserve((size_t)(oo[N] + mo[N]));
+	std::vector<long long> off(N + 1, 0);
+	std::vector<int> fc(N, 0);
+	std::vector<double> sf(N, 0.);
+	double mc = 0.;
+	for (int d = 0; d < N; ++d) {
+		for (long long i = oo[d]; i < oo[d + 1]; ++i) {
+			int p = ctx->h_place_ones[i];
+			if (mk[p] < 1) {
+				push_word(words, (uint32_t)p, 1);
+				fc[d]++;
+			}
+		}
+		for (long long i = mo[d]; i < mo[d + 1]; ++i) {
+			int p = ctx->h_place_multi[i], c = ctx->h_count_multi[i];
+			if (mk[p] < 1) {
+				push_word(words, (uint32_t)p, c);
+				fc[d] += c;
+				sf[d] += std::lgamma((double)c + 1.0);
+			}
+		}
+		off[d + 1] = (long long)words.size();
+		mc += fc[d];
+	}
+	ctx->mean_count = mc / N;
+	ctx->n_ph = (long long)words.size();
+	CK(upload(ctx->ph, words.data(), words.size(), ctx->stream));
+	CK(upload(ctx->ph_off, off.data(), off.size(), ctx->stream));
+	CK(upload(ctx->fcounts, fc.data(), (size_t)N, ctx->stream));
+	CK(upload(ctx->sum_fact, sf.data(), (size_t)N, ctx->stream));
+	std::vector<double> ones_d(N, 1.);
+	std::vector<uint8_t> zeros(N, 0);
+	CK(upload(ctx->scale, ones_d.data(), (size_t)N, ctx->stream));
+	CK(upload(ctx->blacklist, zeros.data(), (size_t)N, ctx->stream));
+	CK(ctx->beta.ensure((size_t)N));
+	CK(ctx->beta_start.ensure((size_t)N));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->beta_set = false;
+	ctx->chunks_R = -1;
+	ctx->have_results = false;
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quats) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(num_rot > 0 && quats, DFG_ERR_ARG, "quaternions: need num_rot > 0");
+	for (long long i = 0; i < 5LL * num_rot; ++i)
+		NEED(std::isfinite(quats[i]), DFG_ERR_ARG, "quaternions: entry %lld is not finite", i);
+	CK(cudaSetDevice(ctx->device));
+	ctx->num_rot = num_rot;
+	CK(upload(ctx->quats, quats, 5 * (size_t)num_rot, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const double *model1) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(size >= 3 && num_modes >= 1 && model1, DFG_ERR_ARG, "model: need size >= 3, num_modes >= 1");
+	NEED(num_modes <= MAX_MODES, DFG_ERR_ARG, "model: at most %d modes", MAX_MODES);
+	CK(cudaSetDevice(ctx->device));
+	ctx->S = size;
+	ctx->V = (long long)size * size * size;
+	ctx->M = num_modes;
+	const size_t n = (size_t)num_modes * ctx->V;
+	CK(upload(ctx->model1, model1, n, ctx->stream));
+	CK(ctx->model2.ensure(n));
+	CK(ctx->weight.ensure(n));
+	CK(ctx->accum.ensure(n));
+	CK(cudaMemsetAsync(ctx->model2.p, 0, n * sizeof(double), ctx->stream));
+	CK(cudaMemsetAsync(ctx->weight.p, 0, n * sizeof(double), ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+static int need_frames(dfg_ctx *ctx) {
+	NEED(ctx->N > 0, DFG_ERR_STATE, "set the frames first");
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_scale(dfg_ctx *ctx, const double *scale) {
+	if (!ctx || !scale)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->scale, scale, (size_t)ctx->N, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_blacklist(dfg_ctx *ctx, const uint8_t *blacklist) {
+	if (!ctx || !blacklist)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->blacklist, blacklist, (size_t)ctx->N, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_beta_start(dfg_ctx *ctx, const double *beta_start) {
+	if (!ctx || !beta_start)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	for (int d = 0; d < ctx->N; ++d)
+		NEED(beta_start[d] > 0. && std::isfinite(beta_start[d]), DFG_ERR_ARG, "beta_start[%d] must be > 0", d);
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->beta_start, beta_start, (size_t)ctx->N, ctx->stream));
+	CK(cudaMemcpyAsync(ctx->beta.p, beta_start, (size_t)ctx->N * sizeof(double), cudaMemcpyHostToDevice,
+	                   ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->beta_set = true;
+	return DFG_OK;
+}
+
+extern "C" int dfg_calc_beta(dfg_ctx *ctx, double start, int need_scaling) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	// iterate.c:66-83
+	std::vector<int> fc(ctx->N);
+	CK(cudaSetDevice(ctx->device));
+	CK(cudaMemcpy(fc.data(), ctx->fcounts.p, (size_t)ctx->N * sizeof(int), cudaMemcpyDeviceToHost));
+	if (!need_scaling && start < 0)
+		start = std::exp(-6.5 * std::pow(ctx->mean_count * 1.e-5, 0.15));
+	std::vector<double> b(ctx->N);
+	for (int d = 0; d < ctx->N; ++d)
+		b[d] = start > 0 ? start : std::exp(-6.5 * std::pow(fc[d] * 1.e-5, 0.15));
+	return dfg_set_beta_start(ctx, b.data());
+}
+
+// ---------------------------------------------------------------------------
+// work buffers and the frame chunks
+// ---------------------------------------------------------------------------
+static int build_chunks(dfg_ctx *ctx) {
+	const int N = ctx->N, P = ctx->P;
+	const size_t pair_bytes = (size_t)ctx->RT * TILE * (sizeof(double) + sizeof(float));
+	size_t budget;
+	if (ctx->pair_budget_mb > 0.) {
+		budget = (size_t)(ctx->pair_budget_mb * 1048576.);
+	} else {
+		size_t fr = 0, tot = 0;
+		CK(cudaMemGetInfo(&fr, &tot));
+		budget = (size_t)(0.6 * (double)fr);
+	}
+	long long nc = (long long)(budget / pair_bytes);
+	NEED(nc >= 1, DFG_ERR_NOMEM, "pair buffers: %zu bytes per frame exceed the budget", pair_bytes);
+	nc = std::min<long long>(nc, N);
+	const int n_chunks = (int)((N + nc - 1) / nc);
+	nc = (N + n_chunks - 1) / n_chunks;  // even chunks
+	ctx->chunk_frames = (int)nc;
+	ctx->chunks.clear();
+	ctx->chunks.resize(n_chunks);
+
+	// M-step index per chunk: photons on mask < 2 pixels, grouped by pixel
+	// (counting sort), frames ascending inside a pixel.
+	const uint8_t *mk = ctx->h_mask.data();
+	std::vector<long long> cnt(P + 1);
+	std::vector<uint32_t> words;
+	for (int k = 0; k < n_chunks; ++k) {
+		Chunk &ch = ctx->chunks[k];
+		ch.d0 = (int)(k * nc);
+		ch.nc = (int)std::min<long long>(nc, N - ch.d0);
+		std::fill(cnt.begin(), cnt.end(), 0);
+		auto each = [&](auto fn) {
+			for (int dl = 0; dl < ch.nc; ++dl) {
+				int d = ch.d0 + dl;
+				for (long long i = ctx->h_ones_off[d]; i < ctx->h_ones_off[d + 1]; ++i) {
+					int p = ctx->h_place_ones[i];
+					if (mk[p] < 2)
+						fn(p, dl, 1LL);
+				}
+				for (long long i = ctx->h_multi_off[d]; i < ctx->h_multi_off[d + 1]; ++i) {
+					int p = ctx->h_place_multi[i];
+					if (mk[p] < 2)
+						fn(p, dl, (long long)ctx->h_count_multi[i]);
+				}
+			}
+		};
+		each([&](int p, int, long long c) { cnt[p + 1] += (c + MAX_COUNT - 1) / MAX_COUNT; });
+		for (int p = 0; p < P; ++p)
+			cnt[p + 1] += cnt[p];
+		words.assign((size_t)cnt[P], 0u);
+		std::vector<long long> fill(cnt.begin(), cnt.end() - 1);
+		each([&](int p, int dl, long long c) {
+			while (c > 0) {
+				uint32_t cc = (uint32_t)std::min<long long>(c, MAX_COUNT);
+				words[(size_t)fill[p]++] = (uint32_t)dl | (cc << IDX_BITS);
+				c -= cc;
+			}
+		});
+		std::vector<int> pix;
+		for (int p = 0; p < P; ++p)
+			if (cnt[p + 1] > cnt[p])
+				pix.push_back(p);
+		std::stable_sort(pix.begin(), pix.end(),
+		                 [&](int a, int b) { return cnt[a + 1] - cnt[a] > cnt[b + 1] - cnt[b]; });
+		ch.npix = (int)pix.size();
+		ch.entries = cnt[P];
+		CK(upload(ch.cs, words.data(), words.size(), ctx->stream));
+		CK(upload(ch.cs_off, cnt.data(), cnt.size(), ctx->stream));
+		CK(upload(ch.pix, pix.data(), pix.size(), ctx->stream));
+		CK(cudaStreamSynchronize(ctx->stream));
+	}
+	ctx->chunks_R = ctx->R;
+	return DFG_OK;
+}
+
+static int ensure_buffers(dfg_ctx *ctx) {
+	NEED(ctx->P > 0, DFG_ERR_STATE, "detector not set");
+	NEED(ctx->N > 0, DFG_ERR_STATE, "frames not set");
+	NEED(ctx->num_rot > 0, DFG_ERR_STATE, "quaternions not set");
+	NEED(ctx->S > 0, DFG_ERR_STATE, "model not set");
+	NEED(ctx->beta_set, DFG_ERR_STATE, "beta not set (dfg_calc_beta or dfg_set_beta_start)");
+	ctx->R = ctx->M * ctx->num_rot;
+	ctx->RT = (ctx->R + TILE - 1) / TILE;
+	ctx->R_pad = ctx->RT * TILE;
+	const size_t tiles_px = (size_t)ctx->RT * ctx->P * TILE;
+	const int nblk = (ctx->P + PB - 1) / PB;
+	CK(ctx->logW.ensure(tiles_px));
+	CK(ctx->T.ensure(tiles_px));
+	CK(ctx->upart.ensure((size_t)nblk * ctx->R_pad));
+	CK(ctx->u.ensure((size_t)ctx->R_pad));
+	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
+	CK(ctx->scalars.ensure(8));
+	CK(ctx->red_part.ensure(std::max<size_t>(blocks_for((long long)ctx->M * ctx->V, 256), 1024)));
+	const size_t N = (size_t)ctx->N;
+	CK(ctx->rmax.ensure(N));
+	CK(ctx->num_prob.ensure(N));
+	CK(ctx->info.ensure(N));
+	CK(ctx->likelihood.ensure(N));
+	CK(ctx->max_exp.ensure(N));
+	CK(ctx->p_norm.ensure(N));
+	CK(ctx->psum_d.ensure(N));
+	CK(ctx->quat_norm.ensure(N * ctx->M));
+	if (ctx->chunks_R != ctx->R) {
+		ctx->pval.release();
+		ctx->Pst.release();
+		if (int rc = build_chunks(ctx))
+			return rc;
+	}
+	const size_t pairs = (size_t)ctx->R_pad * ctx->chunk_frames;
+	CK(ctx->pval.ensure(pairs));
+	CK(ctx->Pst.ensure(pairs));
+	const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
+	CK(ctx->psum_part.ensure((size_t)nsplit * ctx->R_pad));
+	return DFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the iteration
+// ---------------------------------------------------------------------------
+extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_likelihood) {
+	if (!ctx || !par)
+		return DFG_ERR_ARG;
+	NEED(par->beta_period > 0, DFG_ERR_ARG, "beta_period must be > 0");
+	CK(cudaSetDevice(ctx->device));
+	if (int rc = ensure_buffers(ctx))
+		return rc;
+	cudaStream_t st = ctx->stream;
+	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
+	const long long S = ctx->S, V = ctx->V;
+	const int nblk = (P + PB - 1) / PB;
+
+	// update_beta (recon.pyx:161-171)
+	{
+		double factor = std::pow(par->beta_jump, (double)((par->iteration - 1) / par->beta_period));
+		factor *= par->beta_factor;
+		beta_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->beta_start.p, ctx->blacklist.p, N, factor,
+		                                                 ctx->beta.p);
+		CKL("beta_kernel");
+	}
+
+	// slices, u_r, rescale (calculate_rescale, max_prob.c:3-64)
+	phase_begin(ctx, PH_SLICE);
+	slice_log_kernel<double><<<dim3(nblk, RT), 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p,
+	                                                         ctx->mask.p, P, ctx->model1.p, S, V, ctx->logW.p,
+	                                                         ctx->upart.p, R_pad);
+	CKL("slice_log_kernel");
+	u_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->upart.p, nblk, R, R_pad, ctx->u.p);
+	CKL("u_reduce_kernel");
+	rescale_kernel<<<1, 1024, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
+	CKL("rescale_kernel");
+	phase_end(ctx, PH_SLICE, 3);
+
+	CK(cudaMemsetAsync(ctx->T.p, 0, (size_t)RT * P * TILE * sizeof(float), st));
+	CK(cudaMemsetAsync(ctx->psum_r.p, 0, (size_t)R_pad * sizeof(double), st));
+	CK(cudaMemsetAsync(ctx->accum.p, 0, (size_t)M * V * sizeof(float2), st));
+	const int use_scale = par->need_scaling && (par->iteration > 1 || par->known_scale);
+	const int psum_d_on = par->need_scaling && par->update_scale;
+
+	for (Chunk &ch : ctx->chunks) {
+		const int Nc = ch.nc;
+		// E-step (calculate_prob, max_prob.c:66-213)
+		phase_begin(ctx, PH_ESTEP);
+		{
+			long long warps = (long long)RT * Nc;
+			estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
+			    ctx->logW.p, ctx->u.p, ctx->quats.p, M, R, ctx->ph.p, ctx->ph_off.p, ctx->scale.p,
+			    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p);
+			CKL("estep_kernel");
+		}
+		phase_end(ctx, PH_ESTEP, 1);
+		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
+		phase_begin(ctx, PH_NORM);
+		norm_kernel<<<blocks_for(Nc, 8), 256, 0, st>>>(
+		    ctx->pval.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p, ctx->sum_fact.p,
+		    ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p, ctx->max_exp.p, ctx->p_norm.p,
+		    ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p, ctx->num_prob.p);
+		CKL("norm_kernel");
+		phase_end(ctx, PH_NORM, 1);
+		// psum_r (calc_psum_r, max_update.c:108-116)
+		phase_begin(ctx, PH_PSUM);
+		{
+			const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
+			const int fps = (Nc + nsplit - 1) / nsplit;
+			psum_r_kernel<<<dim3(RT, nsplit), 256, 0, st>>>(ctx->Pst.p, Nc, ch.d0, fps, ctx->scale.p,
+			                                                par->need_scaling, ctx->psum_part.p, R_pad);
+			CKL("psum_r_kernel");
+			psum_r_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->psum_part.p, nsplit, R, R_pad,
+			                                                          ctx->psum_r.p);
+			CKL("psum_r_reduce_kernel");
+		}
+		phase_end(ctx, PH_PSUM, 2);
+		// tomograms (update_tomogram_nobg, max_update.c:142-230)
+		phase_begin(ctx, PH_MSTEP);
+		if (ch.npix > 0) {
+			long long warps = (long long)RT * ch.npix;
+			mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.pix.p,
+			                                                    ch.npix, P, RT, ctx->T.p);
+			CKL("mstep_kernel");
+		}
+		phase_end(ctx, PH_MSTEP, ch.npix > 0 ? 1 : 0);
+	}
+
+	// merge (merge_tomogram -> slice_merge3d)
+	phase_begin(ctx, PH_MERGE);
+	merge_kernel<<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
+	                                              ctx->corr.p, ctx->mask.p, P, S, V, ctx->accum.p);
+	CKL("merge_kernel");
+	phase_end(ctx, PH_MERGE, 1);
+
+	phase_begin(ctx, PH_UPDATE);
+	unpack_accum_kernel<<<blocks_for((long long)M * V, 256), 256, 0, st>>>(ctx->accum.p, (long long)M * V,
+	                                                                       ctx->model2.p, ctx->weight.p);
+	CKL("unpack_accum_kernel");
+	// averages over good frames; the packaged Iterate never sets num_blacklist,
+	// so they divide by N (max_prob.c:373-374, iterate.pyx:35)
+	frame_totals_kernel<<<1, 1024, 0, st>>>(ctx->info.p, ctx->likelihood.p, ctx->blacklist.p, N,
+	                                        ctx->scalars.p + 1);
+	CKL("frame_totals_kernel");
+	if (par->need_scaling && par->update_scale) {
+		scale_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->fcounts.p, ctx->psum_d.p, ctx->blacklist.p, N,
+		                                                  ctx->scale.p);
+		CKL("scale_kernel");
+	}
+	phase_end(ctx, PH_UPDATE, par->need_scaling && par->update_scale ? 3 : 2);
+
+	double h[3];
+	CK(cudaMemcpyAsync(h, ctx->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	ctx->rescale = h[0];
+	ctx->mutual_info = h[1] / N;
+	ctx->avg_ll = h[2] / N;
+	ctx->have_results = true;
+	if (avg_likelihood)
+		*avg_likelihood = ctx->avg_ll;
+	return DFG_OK;
+}
+
+extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "update_model: run dfg_maximize first");
+	CK(cudaSetDevice(ctx->device));
+	cudaStream_t st = ctx->stream;
+	const long long n = (long long)ctx->M * ctx->V;
+	const int S = (int)ctx->S, lo = (S % 2 == 0) ? 1 : 0;
+	const long long pairs = (long long)ctx->M * (S - lo) * (S - lo) * (S / 2 - lo + 1);
+	phase_begin(ctx, PH_UPDATE);
+	friedel_kernel<<<blocks_for(pairs, 256), 256, 0, st>>>(ctx->model2.p, ctx->weight.p, S, ctx->M);
+	CKL("friedel_kernel");
+	const unsigned nb = blocks_for(n, 256);
+	divide_update_kernel<float><<<nb, 256, 0, st>>>(ctx->model2.p, ctx->weight.p, ctx->model1.p, nullptr, n,
+	                                                alpha, ctx->red_part.p);
+	CKL("divide_update_kernel");
+	sum_kernel<<<1, 1024, 0, st>>>(ctx->red_part.p, nb, ctx->scalars.p + 3);
+	CKL("sum_kernel");
+	phase_end(ctx, PH_UPDATE, 3);
+	double change = 0.;
+	CK(cudaMemcpyAsync(&change, ctx->scalars.p + 3, sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	ctx->rms = std::sqrt(change / ctx->M / (double)ctx->V);
+	if (rms_change)
+		*rms_change = ctx->rms;
+	return DFG_OK;
+}
+
+extern "C" int dfg_normalize_scale(dfg_ctx *ctx, double *mean_scale) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	NEED(ctx->S > 0, DFG_ERR_STATE, "model not set");
+	CK(cudaSetDevice(ctx->device));
+	cudaStream_t st = ctx->stream;
+	CK(ctx->scalars.ensure(8));
+	scale_sum_kernel<<<1, 1024, 0, st>>>(ctx->scale.p, ctx->blacklist.p, ctx->N, ctx->scalars.p + 4);
+	CKL("scale_sum_kernel");
+	double h[2];
+	CK(cudaMemcpyAsync(h, ctx->scalars.p + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	NEED(h[1] > 0, DFG_ERR_STATE, "normalize_scale: no good frames");
+	const double mean = h[0] / h[1];
+	CK(cudaMemcpyAsync(ctx->scalars.p + 6, &mean, sizeof(double), cudaMemcpyHostToDevice, st));
+	const long long n = std::max<long long>(ctx->V, ctx->N);
+	apply_scale_norm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(ctx->scale.p, ctx->blacklist.p, ctx->N,
+	                                                             ctx->model1.p, nullptr, ctx->V,
+	                                                             ctx->scalars.p + 6);
+	CKL("apply_scale_norm_kernel");
+	CK(cudaStreamSynchronize(st));
+	ctx->rms *= mean;
+	if (mean_scale)
+		*mean_scale = mean;
+	return DFG_OK;
+}
+
+extern "C" int dfg_run_iteration_host(dfg_ctx *ctx, const dfg_iter_params *par, double alpha,
+                                      double *model1_inout, int *rmax, double *likelihood,
+                                      double *avg_likelihood, double *rms_change) {
+	if (!ctx || !par || !model1_inout)
+		return DFG_ERR_ARG;
+	NEED(ctx->S > 0, DFG_ERR_STATE, "model not set");
+	CK(cudaSetDevice(ctx->device));
+	const size_t n = (size_t)ctx->M * ctx->V;
+	CK(cudaMemcpyAsync(ctx->model1.p, model1_inout, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+	double ll = 0., rms = 0.;
+	if (int rc = dfg_maximize(ctx, par, &ll))
+		return rc;
+	if (int rc = dfg_update_model(ctx, alpha, &rms))
+		return rc;
+	if (par->need_scaling) {
+		double m;
+		if (int rc = dfg_normalize_scale(ctx, &m))
+			return rc;
+		rms = ctx->rms;
+	}
+	CK(cudaMemcpyAsync(model1_inout, ctx->model1.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	if (rmax)
+		CK(cudaMemcpyAsync(rmax, ctx->rmax.p, (size_t)ctx->N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+	if (likelihood)
+		CK(cudaMemcpyAsync(likelihood, ctx->likelihood.p, (size_t)ctx->N * sizeof(double), cudaMemcpyDeviceToHost,
+		                   ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	if (avg_likelihood)
+		*avg_likelihood = ll;
+	if (rms_change)
+		*rms_change = rms;
+	return DFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// results
+// ---------------------------------------------------------------------------
+template <typename T>
+static cudaError_t fetch(T *h, const DevBuf<T> &b, size_t n, cudaStream_t s) {
+	if (h == nullptr || n == 0)
+		return cudaSuccess;
+	return cudaMemcpyAsync(h, b.p, n * sizeof(T), cudaMemcpyDeviceToHost, s);
+}
+
+extern "C" int dfg_get_frame_results(dfg_ctx *ctx, int *rmax, double *info, double *likelihood,
+                                     double *max_exp, double *p_norm, double *psum_d) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
+	CK(cudaSetDevice(ctx->device));
+	const size_t N = (size_t)ctx->N;
+	CK(fetch(rmax, ctx->rmax, N, ctx->stream));
+	CK(fetch(info, ctx->info, N, ctx->stream));
+	CK(fetch(likelihood, ctx->likelihood, N, ctx->stream));
+	CK(fetch(max_exp, ctx->max_exp, N, ctx->stream));
+	CK(fetch(p_norm, ctx->p_norm, N, ctx->stream));
+	CK(fetch(psum_d, ctx->psum_d, N, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_num_prob(dfg_ctx *ctx, int *num_prob) {
+	if (!ctx || !num_prob)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
+	CK(cudaSetDevice(ctx->device));
+	CK(fetch(num_prob, ctx->num_prob, (size_t)ctx->N, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_quat_norm(dfg_ctx *ctx, double *quat_norm) {
+	if (!ctx || !quat_norm)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
+	const size_t n = (size_t)ctx->N * ctx->M;
+	if (ctx->M == 1) {
+		memset(quat_norm, 0, n * sizeof(double));
+		return DFG_OK;
+	}
+	CK(cudaSetDevice(ctx->device));
+	CK(fetch(quat_norm, ctx->quat_norm, n, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_orientation_results(dfg_ctx *ctx, double *u, double *psum_r) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
+	CK(cudaSetDevice(ctx->device));
+	CK(fetch(u, ctx->u, (size_t)ctx->R, ctx->stream));
+	CK(fetch(psum_r, ctx->psum_r, (size_t)ctx->R, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_model(dfg_ctx *ctx, double *model1, double *model2, double *inter_weight) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->S > 0, DFG_ERR_STATE, "model not set");
+	CK(cudaSetDevice(ctx->device));
+	const size_t n = (size_t)ctx->M * ctx->V;
+	CK(fetch(model1, ctx->model1, n, ctx->stream));
+	CK(fetch(model2, ctx->model2, n, ctx->stream));
+	CK(fetch(inter_weight, ctx->weight, n, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_frame_params(dfg_ctx *ctx, double *scale, double *beta, double *beta_start, int *fcounts,
+                                    double *sum_fact, uint8_t *blacklist) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	CK(cudaSetDevice(ctx->device));
+	const size_t N = (size_t)ctx->N;
+	CK(fetch(scale, ctx->scale, N, ctx->stream));
+	if (ctx->beta_set) {
+		CK(fetch(beta, ctx->beta, N, ctx->stream));
+		CK(fetch(beta_start, ctx->beta_start, N, ctx->stream));
+	}
+	CK(fetch(fcounts, ctx->fcounts, N, ctx->stream));
+	CK(fetch(sum_fact, ctx->sum_fact, N, ctx->stream));
+	CK(fetch(blacklist, ctx->blacklist, N, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_scalars(dfg_ctx *ctx, double *out) {
+	if (!ctx || !out)
+		return DFG_ERR_ARG;
+	out[0] = ctx->rescale;
+	out[1] = ctx->mutual_info;
+	out[2] = ctx->avg_ll;
+	out[3] = ctx->mean_count;
+	out[4] = ctx->rms;
+	return DFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one-slice operations
+// ---------------------------------------------------------------------------
+extern "C" int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double *out) {
+	if (!ctx || !quat || !out)
+		return DFG_ERR_ARG;
+	NEED(ctx->P > 0 && ctx->S > 0, DFG_ERR_STATE, "slice_gen: detector and model must be set");
+	NEED(mode >= 0 && mode < ctx->M, DFG_ERR_ARG, "slice_gen: mode %d out of range", mode);
+	CK(cudaSetDevice(ctx->device));
+	CK(ctx->scalars.ensure(8));
+	DevBuf<double> q, o;
+	CK(upload(q, quat, 5, ctx->stream));
+	CK(o.ensure((size_t)ctx->P));
+	slice_one_kernel<<<blocks_for(ctx->P, 256), 256, 0, ctx->stream>>>(q.p, mode, ctx->qvals.p, ctx->corr.p, ctx->P,
+	                                                                    ctx->model1.p, ctx->S, ctx->V, o.p);
+	CKL("slice_one_kernel");
+	CK(cudaMemcpyAsync(out, o.p, (size_t)ctx->P * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const double *view, double *model2,
+                               double *inter_weight) {
+	if (!ctx || !quat || !view || !model2 || !inter_weight)
+		return DFG_ERR_ARG;
+	NEED(ctx->P > 0 && ctx->S > 0, DFG_ERR_STATE, "slice_merge: detector and model must be set");
+	NEED(mode >= 0 && mode < ctx->M, DFG_ERR_ARG, "slice_merge: mode %d out of range", mode);
+	CK(cudaSetDevice(ctx->device));
+	const size_t n = (size_t)ctx->M * ctx->V;
+	DevBuf<double> q, v, m2, w;
+	CK(upload(q, quat, 5, ctx->stream));
+	CK(upload(v, view, (size_t)ctx->P, ctx->stream));
+	CK(upload(m2, model2, n, ctx->stream));
+	CK(upload(w, inter_weight, n, ctx->stream));
+	merge_one_kernel<<<blocks_for(ctx->P, 256), 256, 0, ctx->stream>>>(q.p, mode, v.p, ctx->qvals.p, ctx->corr.p,
+	                                                                    ctx->mask.p, ctx->P, ctx->S, ctx->V, m2.p, w.p);
+	CKL("merge_one_kernel");
+	CK(cudaMemcpyAsync(model2, m2.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaMemcpyAsync(inter_weight, w.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// options and instrumentation
+// ---------------------------------------------------------------------------
+extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
+	if (!ctx || !key)
+		return DFG_ERR_ARG;
+	if (!strcmp(key, "pair_budget_mb")) {
+		NEED(value >= 0., DFG_ERR_ARG, "pair_budget_mb must be >= 0");
+		ctx->pair_budget_mb = value;
+		ctx->chunks_R = -1;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "timing")) {
+		ctx->timing = value != 0.;
+		return DFG_OK;
+	}
+	return ctx->fail(DFG_ERR_ARG, "unknown option '%s'", key);
+}
+
+extern "C" int dfg_get_phase_times(dfg_ctx *ctx, double *ms, long *launches, int n) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	for (int i = 0; i < n && i < PH_COUNT; ++i) {
+		if (ms)
+			ms[i] = ctx->phase_ms[i];
+		if (launches)
+			launches[i] = ctx->phase_launches[i];
+	}
+	return PH_COUNT;
+}
+
+extern "C" const char *dfg_phase_name(int i) { return (i >= 0 && i < PH_COUNT) ? kPhaseNames[i] : ""; }
+
+extern "C" int dfg_reset_phase_times(dfg_ctx *ctx) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	for (int i = 0; i < PH_COUNT; ++i) {
+		ctx->phase_ms[i] = 0.;
+		ctx->phase_launches[i] = 0;
+	}
+	return DFG_OK;
+}
+
+extern "C" int dfg_event_record(dfg_ctx *ctx, int slot) {
+	if (!ctx || slot < 0 || slot >= 8)
+		return DFG_ERR_ARG;
+	CK(cudaSetDevice(ctx->device));
+	CK(cudaEventRecord(ctx->user_ev[slot], ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_event_elapsed(dfg_ctx *ctx, int a, int b, double *ms) {
+	if (!ctx || !ms || a < 0 || a >= 8 || b < 0 || b >= 8)
+		return DFG_ERR_ARG;
+	CK(cudaSetDevice(ctx->device));
+	CK(cudaEventSynchronize(ctx->user_ev[b]));
+	float f = 0.f;
+	CK(cudaEventElapsedTime(&f, ctx->user_ev[a], ctx->user_ev[b]));
+	*ms = f;
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_workload(dfg_ctx *ctx, long long *out) {
+	if (!ctx || !out)
+		return DFG_ERR_ARG;
+	long long ms = 0;
+	for (auto &c : ctx->chunks)
+		ms += c.entries;
+	out[0] = ctx->R;
+	out[1] = ctx->N;
+	out[2] = ctx->n_ph;
+	out[3] = ms;
+	out[4] = (long long)ctx->chunks.size();
+	out[5] = ctx->chunk_frames;
+	out[6] = ctx->launches;
+	return DFG_OK;
+}

@@ -1,0 +1,129 @@
+// Constants and inline device helpers of the EMC iteration for sm_100a (B200).
+//
+// Layout conventions (all in HBM, owned by the context in emc_api.cu):
+//   R        = num_modes * num_rot orientations, processed in tiles of 32
+//              (one warp's lanes); RT = ceil(R / 32) tiles, orientation
+//              r = tile * 32 + lane, r -> (rotation r / M, mode r % M) as in
+//              dragonfly/src/max_prob.c:80-85.
+//   logW     [RT][P][32] float   log of the slice W_r[p], pixel-major inside a
+//                                tile so that every photon gather reads one
+//                                coalesced 128-byte row (32 orientations).
+//   pval     [RT][Nc][32] double log-likelihood of (orientation, frame) pairs
+//                                of the current frame chunk.
+//   Pst      [RT][Nc][32] float  normalised probability of kept pairs; the sign
+//                                carries the reference's PROB_MIN gate: P > 1e-6
+//                                stored as +P, kept but <= 1e-6 as -P, pruned 0.
+//   T        [RT][P][32] float   photon tomograms sum_d P_dr * K_d[p].
+//   accum    [M*V] float2        (model2 sum, weight) merge accumulators.
+// Photon lists are packed 32-bit words: low 22 bits a pixel (E-step, per
+// frame) or a chunk-local frame (M-step, per pixel), high 10 bits the count;
+// counts above 1023 are split over several words (all uses are linear in it).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+namespace dfg {
+
+constexpr int TILE = 32;
+constexpr int IDX_BITS = 22;
+constexpr uint32_t IDX_MASK = (1u << IDX_BITS) - 1u;
+constexpr uint32_t MAX_COUNT = (1u << (32 - IDX_BITS)) - 1u;
+constexpr double PROB_MIN = 1.e-6;          // dragonfly/src/max_internal.h:6
+constexpr double PDIFF_THRESH = 14.;        // dragonfly/src/max_internal.h:7
+constexpr double MAX_EXP_START = -1.e100;   // dragonfly/src/max_internal.h:8
+constexpr int PB = 64;                      // pixels per block in slice / merge kernels
+constexpr int MAX_MODES = 16;
+constexpr unsigned FULL = 0xffffffffu;
+
+// FP64 arithmetic in the reference's operation order: these intrinsics are
+// never contracted into fused multiply-adds, so geometry (cell index, OOB
+// test, interpolation weights) is bit-identical to the C engine.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// Rotation matrix of a quaternion (dragonfly/src/model.c:759-786), row-major.
+__device__ inline void rot_from_quat(const double *q, double *rot) {
+	double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+	double q01 = dmul(q0, q1), q02 = dmul(q0, q2), q03 = dmul(q0, q3);
+	double q11 = dmul(q1, q1), q12 = dmul(q1, q2), q13 = dmul(q1, q3);
+	double q22 = dmul(q2, q2), q23 = dmul(q2, q3), q33 = dmul(q3, q3);
+	rot[0] = dsub(1., dmul(2., dadd(q22, q33)));
+	rot[1] = dmul(2., dadd(q12, q03));
+	rot[2] = dmul(2., dsub(q13, q02));
+	rot[3] = dmul(2., dsub(q12, q03));
+	rot[4] = dsub(1., dmul(2., dadd(q11, q33)));
+	rot[5] = dmul(2., dadd(q01, q23));
+	rot[6] = dmul(2., dadd(q02, q13));
+	rot[7] = dmul(2., dsub(q23, q01));
+	rot[8] = dsub(1., dmul(2., dadd(q11, q22)));
+}
+
+// Trilinear cell of a detector pixel rotated into the model grid, computed as
+// slice_gen3d / slice_merge3d do (model.c:19-44, 177-201): position
+// sum_j rot[i][j] q_j + center, integer part by truncation toward zero,
+// in bounds iff 0 <= x <= size-2 on every axis.
+struct Cell {
+	long long i000;  // x*S*S + y*S + z
+	double fx, fy, fz;
+	bool ok;
+};
+
+__device__ __forceinline__ Cell locate(const double *rot, double qx, double qy, double qz, double center,
+                                       long long S) {
+	Cell c;
+	double px = dadd(dadd(dadd(dmul(rot[0], qx), dmul(rot[1], qy)), dmul(rot[2], qz)), center);
+	double py = dadd(dadd(dadd(dmul(rot[3], qx), dmul(rot[4], qy)), dmul(rot[5], qz)), center);
+	double pz = dadd(dadd(dadd(dmul(rot[6], qx), dmul(rot[7], qy)), dmul(rot[8], qz)), center);
+	long long x = (long long)px, y = (long long)py, z = (long long)pz;
+	c.ok = !(x < 0 || x > S - 2 || y < 0 || y > S - 2 || z < 0 || z > S - 2);
+	c.fx = dsub(px, (double)x);
+	c.fy = dsub(py, (double)y);
+	c.fz = dsub(pz, (double)z);
+	c.i000 = c.ok ? (x * S + y) * S + z : 0;
+	return c;
+}
+
+// The 8 corner weights in the reference's order (000, 001, 010, 011, 100, ...).
+__device__ __forceinline__ void corner_weights(const Cell &c, double *w) {
+	double cx = dsub(1., c.fx), cy = dsub(1., c.fy), cz = dsub(1., c.fz);
+	double cxcy = dmul(cx, cy), cxfy = dmul(cx, c.fy), fxcy = dmul(c.fx, cy), fxfy = dmul(c.fx, c.fy);
+	w[0] = dmul(cxcy, cz); w[1] = dmul(cxcy, c.fz);
+	w[2] = dmul(cxfy, cz); w[3] = dmul(cxfy, c.fz);
+	w[4] = dmul(fxcy, cz); w[5] = dmul(fxcy, c.fz);
+	w[6] = dmul(fxfy, cz); w[7] = dmul(fxfy, c.fz);
+}
+
+__device__ __forceinline__ void corner_offsets(long long S, long long *o) {
+	// +z, +y, +x neighbours; (x+1) % S == x+1 inside bounds
+	o[0] = 0; o[1] = 1; o[2] = S; o[3] = S + 1;
+	o[4] = S * S; o[5] = S * S + 1; o[6] = S * S + S; o[7] = S * S + S + 1;
+}
+
+// W = corr * sum_k w_k m_k, summed left to right; DBL_MIN outside the model
+// (model.c:33-57).
+template <typename MT>
+__device__ __forceinline__ double interp(const Cell &c, const MT *__restrict__ m, long long S, double corr) {
+	if (!c.ok)
+		return DBL_MIN;
+	double w[8];
+	long long o[8];
+	corner_weights(c, w);
+	corner_offsets(S, o);
+	double v = dmul(w[0], (double)__ldg(m + c.i000));
+#pragma unroll
+	for (int k = 1; k < 8; ++k)
+		v = dadd(v, dmul(w[k], (double)__ldg(m + c.i000 + o[k])));
+	return dmul(v, corr);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_xor_sync(FULL, v, o);
+	return v;
+}
+
+}  // namespace dfg

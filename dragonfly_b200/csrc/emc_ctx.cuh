@@ -1,0 +1,166 @@
+// Context of the B200 EMC iteration: resident inputs, work buffers and the
+// error/instrumentation state behind the C ABI (include/dragonfly_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dragonfly_b200.h"
+#include "emc_common.cuh"
+
+namespace dfg {
+
+enum Phase { PH_SLICE, PH_ESTEP, PH_NORM, PH_PSUM, PH_MSTEP, PH_MERGE, PH_UPDATE, PH_COUNT };
+static const char *kPhaseNames[PH_COUNT] = {"slice", "estep", "norm", "psum", "mstep", "merge", "update"};
+
+// Owning device buffer; move-only.
+template <typename T>
+struct DevBuf {
+	T *p = nullptr;
+	size_t n = 0;
+	DevBuf() = default;
+	DevBuf(const DevBuf &) = delete;
+	DevBuf &operator=(const DevBuf &) = delete;
+	DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+	DevBuf &operator=(DevBuf &&o) noexcept {
+		if (this != &o) {
+			release();
+			p = o.p; n = o.n;
+			o.p = nullptr; o.n = 0;
+		}
+		return *this;
+	}
+	~DevBuf() { release(); }
+	void release() {
+		if (p)
+			cudaFree(p);
+		p = nullptr;
+		n = 0;
+	}
+	cudaError_t ensure(size_t count) {
+		if (count <= n && p)
+			return cudaSuccess;
+		release();
+		cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+		if (e == cudaSuccess)
+			n = std::max<size_t>(count, 1);
+		else
+			p = nullptr;
+		return e;
+	}
+};
+
+struct Chunk {
+	int d0 = 0, nc = 0;
+	DevBuf<uint32_t> cs;       // (chunk-local frame | count << 22), grouped by pixel
+	DevBuf<long long> cs_off;  // [P + 1]
+	DevBuf<int> pix;           // pixels with non-empty lists, longest first
+	int npix = 0;
+	long long entries = 0;
+};
+
+}  // namespace dfg
+
+using namespace dfg;
+
+struct dfg_ctx {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	std::string err;
+
+	// detector
+	int P = 0;
+	DevBuf<double> qvals, corr;
+	DevBuf<uint8_t> mask;
+	std::vector<uint8_t> h_mask;
+
+	// frames
+	int N = 0;
+	std::vector<int> h_ones, h_multi, h_place_ones, h_place_multi, h_count_multi;
+	std::vector<long long> h_ones_off, h_multi_off;
+	DevBuf<uint32_t> ph;
+	DevBuf<long long> ph_off;
+	long long n_ph = 0;
+	DevBuf<double> scale, beta, beta_start, sum_fact;
+	DevBuf<int> fcounts;
+	DevBuf<uint8_t> blacklist;
+	double mean_count = 0.;
+	bool beta_set = false;
+
+	// orientations and model
+	int num_rot = 0, M = 1, R = 0, RT = 0, R_pad = 0;
+	DevBuf<double> quats;
+	long long S = 0, V = 0;
+	DevBuf<double> model1, model2, weight;
+	DevBuf<float2> accum;
+
+	// work buffers
+	DevBuf<float> logW, Pst, T;
+	DevBuf<double> upart, u, pval, psum_r, psum_part, scalars, red_part;
+	DevBuf<int> rmax, num_prob;
+	DevBuf<double> info, likelihood, max_exp, p_norm, psum_d, quat_norm;
+	std::vector<Chunk> chunks;
+	int chunk_frames = 0;
+	int chunks_R = -1;  // R the chunk layout was built for
+
+	// options and results
+	double pair_budget_mb = 0.;
+	bool timing = false;
+	cudaEvent_t ev[2 * PH_COUNT] = {};
+	cudaEvent_t user_ev[8] = {};
+	long long launches = 0;  // kernels launched by this context
+	double phase_ms[PH_COUNT] = {};
+	long phase_launches[PH_COUNT] = {};
+	double rescale = 0., mutual_info = 0., avg_ll = 0., rms = 0.;
+	bool have_results = false;
+
+	int fail(int code, const char *fmt, ...) {
+		char buf[1024];
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(buf, sizeof(buf), fmt, ap);
+		va_end(ap);
+		err = buf;
+		return code;
+	}
+};
+
+#define CK(call)                                                                                  \
+	do {                                                                                          \
+		cudaError_t e_ = (call);                                                                  \
+		if (e_ != cudaSuccess)                                                                    \
+			return ctx->fail(e_ == cudaErrorMemoryAllocation ? DFG_ERR_NOMEM : DFG_ERR_CUDA,      \
+			                 "%s failed: %s", #call, cudaGetErrorString(e_));                    \
+	} while (0)
+
+#define CKL(name)                                                                                 \
+	do {                                                                                          \
+		ctx->launches++;                                                                          \
+		cudaError_t e_ = cudaGetLastError();                                                      \
+		if (e_ != cudaSuccess)                                                                    \
+			return ctx->fail(DFG_ERR_CUDA, "launch of %s failed: %s", name, cudaGetErrorString(e_)); \
+	} while (0)
+
+#define NEED(cond, code, ...)                                                                     \
+	do {                                                                                          \
+		if (!(cond))                                                                              \
+			return ctx->fail(code, __VA_ARGS__);                                                  \
+	} while (0)
+
+static inline unsigned blocks_for(long long n, int per) { return (unsigned)((n + per - 1) / per); }
+
+template <typename T>
+static cudaError_t upload(DevBuf<T> &b, const T *h, size_t n, cudaStream_t s) {
+	cudaError_t e = b.ensure(n);
+	if (e != cudaSuccess || n == 0)
+		return e;
+	return cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+

@@ -1,0 +1,682 @@
+// Kernels of one EMC iteration for sm_100a (B200); layouts in emc_common.cuh.
+// Included by emc_api.cu only (one definition of each kernel).
+#pragma once
+
+#include "emc_common.cuh"
+
+namespace dfg {
+
+// ---------------------------------------------------------------------------
+// (a) slice generation: logW[tile][p][lane] = log(W), u partial sums
+// ---------------------------------------------------------------------------
+// Block = one orientation tile x PB pixels, 256 threads: thread (i = t % 64,
+// g = t / 64) computes pixel i for orientations g, g+4, ..., g+28, so a warp
+// walks 32 neighbouring pixels of one orientation (neighbouring model reads).
+// u_r (sum of un-logged W over mask == 0 pixels, max_prob.c:32-40) is reduced
+// per block in a fixed order into upart[block][r].
+template <typename MT>
+__global__ void __launch_bounds__(256) slice_log_kernel(
+    const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
+    const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
+    long long S, long long V, float *__restrict__ logW, double *__restrict__ upart, int R_pad) {
+	__shared__ double s_rot[TILE][9];
+	__shared__ int s_mode[TILE];
+	__shared__ float s_tile[PB][TILE + 1];
+	__shared__ double s_u[2][TILE];
+	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
+	if (t < TILE) {
+		int r = rt * TILE + t;
+		int rr = r < R ? r : 0;
+		rot_from_quat(&quats[(rr / M) * 5], s_rot[t]);
+		s_mode[t] = rr % M;
+	}
+	__syncthreads();
+	const int i = t & (PB - 1), g = t >> 6, p = p0 + i;
+	const bool pix = p < P;
+	double qx = 0., qy = 0., qz = 0., cr = 1.;
+	bool good = false;
+	if (pix) {
+		qx = qvals[3 * (size_t)p]; qy = qvals[3 * (size_t)p + 1]; qz = qvals[3 * (size_t)p + 2];
+		cr = corr[p];
+		good = mask[p] < 1;
+	}
+	const double center = (double)(S / 2);
+#pragma unroll 2
+	for (int k = 0; k < 8; ++k) {
+		const int j = g + 4 * k;
+		double W = 0.;
+		if (pix) {
+			Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+			W = interp(c, model + (size_t)s_mode[j] * V, S, cr);
+			s_tile[i][j] = (float)log(W);
+		}
+		double uw = warp_sum((pix && good) ? W : 0.);
+		if ((t & 31) == 0)
+			s_u[i >> 5][j] = uw;
+	}
+	__syncthreads();
+	if (t < TILE) {
+		int r = rt * TILE + t;
+		upart[(size_t)blockIdx.x * R_pad + r] = s_u[0][t] + s_u[1][t];
+	}
+	// coalesced store: warp w writes rows w, w+8, ...
+	const int w = t >> 5, lane = t & 31;
+	for (int row = w; row < PB; row += 8) {
+		int pp = p0 + row;
+		if (pp < P)
+			logW[((size_t)rt * P + pp) * TILE + lane] = s_tile[row][lane];
+	}
+}
+
+// u_r = sum over pixel blocks in block order (deterministic)
+__global__ void u_reduce_kernel(const double *__restrict__ upart, int nblk, int R, int R_pad,
+                                double *__restrict__ u) {
+	int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r >= R)
+		return;
+	double s = 0.;
+	for (int b = 0; b < nblk; ++b)
+		s += upart[(size_t)b * R_pad + r];
+	u[r] = s;
+}
+
+// rescale = mean_count / sum_r w_r u_r * M (max_prob.c:40, 55-60); one block.
+__global__ void __launch_bounds__(1024) rescale_kernel(const double *__restrict__ u,
+                                                       const double *__restrict__ quats, int M, int R,
+                                                       double mean_count, double *__restrict__ scalars) {
+	__shared__ double s[32];
+	double acc = 0.;
+	for (int r = threadIdx.x; r < R; r += blockDim.x)
+		acc += quats[(r / M) * 5 + 4] * u[r];
+	acc = warp_sum(acc);
+	if ((threadIdx.x & 31) == 0)
+		s[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		double v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.;
+		v = warp_sum(v);
+		if (threadIdx.x == 0)
+			scalars[0] = mean_count / v * M;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// (b) E-step: pval[tile][d][lane] = log w_r - u_r * s_d + sum_k c_k logW_r[p_k]
+// ---------------------------------------------------------------------------
+// One warp per (orientation tile, frame), tiles outermost so that resident
+// warps share one tile's log-slices in L2. Photon words are fetched 32 at a
+// time and broadcast by shuffle; each photon costs one coalesced 128-byte row
+// read. FP64 accumulation of FP32 log-slice values (c * v is exact in FP64).
+// s_d = phi_d when need_scaling && (iteration > 1 || known_scale), else the
+// rescale factor (max_prob.c:122-128).
+__global__ void __launch_bounds__(256) estep_kernel(
+    const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ quats, int M,
+    int R, const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
+    const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
+    const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval) {
+	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (warp >= (long long)RT * Nc)
+		return;
+	const int rt = (int)(warp / Nc), dl = (int)(warp - (long long)rt * Nc), d = d0 + dl;
+	if (blacklist[d])
+		return;
+	const int r = rt * TILE + lane;
+	const double s = use_scale ? scale[d] : scalars[0];
+	double acc = 0.;
+	if (r < R)
+		acc = dsub(log(quats[(r / M) * 5 + 4]), dmul(u[r], s));
+	const float *L = logW + (size_t)rt * P * TILE + lane;
+	const long long beg = ph_off[d], end = ph_off[d + 1];
+	for (long long j0 = beg; j0 < end; j0 += 32) {
+		const uint32_t e = (j0 + lane < end) ? __ldg(ph + j0 + lane) : 0u;
+		const int n = (int)min(32LL, end - j0);
+		for (int k = 0; k < n; k += 8) {
+			uint32_t ek[8];
+			float v[8];
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				ek[q] = __shfl_sync(FULL, e, k + q);
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				v[q] = (k + q < n) ? __ldg(L + (size_t)(ek[q] & IDX_MASK) * TILE) : 0.f;
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				acc = fma((double)(ek[q] >> IDX_BITS), (double)v[q], acc);
+		}
+	}
+	pval[((size_t)rt * Nc + dl) * TILE + lane] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// (c) per-frame maximum, pruning, normalisation and frame reductions
+// ---------------------------------------------------------------------------
+// One warp per frame. The reference visits orientations in ascending order
+// with a running maximum m (max_prob.c:184-203): a pair enters the kept list
+// when pval + 14/beta > m and, when pval > m, the list is pruned to entries
+// > pval - 14/beta. With one thread the final list is: every r up to the first
+// maximiser r* with pval > max - 14/beta, and every r after r* with
+// pval + 14/beta > max. The maximiser is the lowest index reaching the maximum.
+// P_dr = exp(beta (pval - max)) / p_norm (max_update.c:96-98); likelihood,
+// psum_d, info and quat_norm follow max_update.c:105-130.
+__global__ void __launch_bounds__(256) norm_kernel(
+    const double *__restrict__ pval, int RT, int Nc, int d0, int R, int M, const double *__restrict__ quats,
+    const double *__restrict__ u, const double *__restrict__ beta, const double *__restrict__ sum_fact,
+    const uint8_t *__restrict__ blacklist, int psum_d_on, const double *__restrict__ scalars,
+    float *__restrict__ Pst, int *__restrict__ rmax, double *__restrict__ max_exp,
+    double *__restrict__ p_norm, double *__restrict__ info, double *__restrict__ likelihood,
+    double *__restrict__ psum_d, double *__restrict__ quat_norm, int *__restrict__ num_prob) {
+	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (warp >= Nc)
+		return;
+	const int dl = warp, d = d0 + dl;
+	const double *pv = pval + (size_t)dl * TILE + lane;
+	float *ps = Pst + (size_t)dl * TILE + lane;
+	const size_t tstride = (size_t)Nc * TILE;
+
+	double m = MAX_EXP_START;
+	int am = 0;
+	if (!blacklist[d]) {
+		for (int rt = 0; rt < RT; ++rt) {
+			int r = rt * TILE + lane;
+			if (r < R) {
+				double v = pv[rt * tstride];
+				if (v > m) {
+					m = v;
+					am = r;
+				}
+			}
+		}
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		double om = __shfl_xor_sync(FULL, m, o);
+		int oa = __shfl_xor_sync(FULL, am, o);
+		if (om > m || (om == m && oa < am)) {
+			m = om;
+			am = oa;
+		}
+	}
+	const bool any = !blacklist[d] && m != MAX_EXP_START;
+	if (!any) {
+		for (int rt = 0; rt < RT; ++rt)
+			ps[rt * tstride] = 0.f;
+		if (lane == 0) {
+			rmax[d] = -1;
+			max_exp[d] = MAX_EXP_START;
+			p_norm[d] = 0.;
+			info[d] = 0.;
+			likelihood[d] = 0.;
+			psum_d[d] = 0.;
+			num_prob[d] = 0;
+		}
+		if (M > 1 && lane < M)
+			quat_norm[(size_t)d * M + lane] = 0.;
+		return;
+	}
+	const double b = beta[d];
+	const double thr = PDIFF_THRESH / b;
+	const double lo = dsub(m, thr);
+	const int rstar = am;
+
+	double s = 0.;
+	int cnt = 0;
+	for (int rt = 0; rt < RT; ++rt) {
+		int r = rt * TILE + lane;
+		if (r < R) {
+			double v = pv[rt * tstride];
+			bool kept = (r <= rstar) ? (v > lo) : (dadd(v, thr) > m);
+			if (kept) {
+				s += exp(dmul(b, dsub(v, m)));
+				cnt++;
+			}
+		}
+	}
+	s = warp_sum(s);
+	for (int o = 16; o > 0; o >>= 1)
+		cnt += __shfl_xor_sync(FULL, cnt, o);
+
+	const double rescale = scalars[0], sf = sum_fact[d];
+	double ll = 0., pd = 0., inf = 0.;
+	double qn[MAX_MODES];
+#pragma unroll
+	for (int k = 0; k < MAX_MODES; ++k)
+		qn[k] = 0.;
+	for (int rt = 0; rt < RT; ++rt) {
+		int r = rt * TILE + lane;
+		float out = 0.f;
+		if (r < R) {
+			double v = pv[rt * tstride];
+			bool kept = (r <= rstar) ? (v > lo) : (dadd(v, thr) > m);
+			if (kept) {
+				double P = exp(dmul(b, dsub(v, m))) / s;
+				ll += P * (v - sf);
+				if (psum_d_on)
+					pd += P * u[r] * rescale;
+				if (!(P < PROB_MIN)) {
+					double w = quats[(r / M) * 5 + 4];
+					inf += P * log(P / w * M);
+					if (M > 1) {
+						int mode = r % M;
+#pragma unroll
+						for (int k = 0; k < MAX_MODES; ++k)
+							if (k == mode)
+								qn[k] += P;
+					}
+				}
+				out = (P > PROB_MIN) ? (float)P : -(float)P;
+			}
+		}
+		ps[rt * tstride] = out;
+	}
+	ll = warp_sum(ll);
+	pd = warp_sum(pd);
+	inf = warp_sum(inf);
+	if (M > 1) {
+		for (int k = 0; k < M && k < MAX_MODES; ++k) {
+			double v = warp_sum(qn[k]);
+			if (lane == 0)
+				quat_norm[(size_t)d * M + k] = v;
+		}
+	}
+	if (lane == 0) {
+		rmax[d] = rstar;
+		max_exp[d] = m;
+		p_norm[d] = s;
+		likelihood[d] = ll;
+		info[d] = inf;
+		psum_d[d] = pd;
+		num_prob[d] = cnt;
+	}
+}
+
+// psum_r partials: sum over a frame range of |Pst| * (phi_d or 1)
+// (max_update.c:108-116). Grid (RT, splits), 8 warps per block; fixed order.
+__global__ void __launch_bounds__(256) psum_r_kernel(const float *__restrict__ Pst, int Nc, int d0,
+                                                      int frames_per_split, const double *__restrict__ scale,
+                                                      int need_scaling, double *__restrict__ part, int R_pad) {
+	__shared__ double s[8][TILE];
+	const int rt = blockIdx.x, split = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int beg = split * frames_per_split, end = min(Nc, beg + frames_per_split);
+	double acc = 0.;
+	const float *p = Pst + (size_t)rt * Nc * TILE + lane;
+	for (int dl = beg + w; dl < end; dl += 8) {
+		double v = fabs((double)p[(size_t)dl * TILE]);
+		acc += need_scaling ? v * scale[d0 + dl] : v;
+	}
+	s[w][lane] = acc;
+	__syncthreads();
+	if (w == 0) {
+		double t = 0.;
+#pragma unroll
+		for (int k = 0; k < 8; ++k)
+			t += s[k][lane];
+		part[(size_t)split * R_pad + rt * TILE + lane] = t;
+	}
+}
+
+__global__ void psum_r_reduce_kernel(const double *__restrict__ part, int nsplit, int R, int R_pad,
+                                     double *__restrict__ psum_r) {
+	int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r >= R)
+		return;
+	double s = 0.;
+	for (int k = 0; k < nsplit; ++k)
+		s += part[(size_t)k * R_pad + r];
+	psum_r[r] += s;
+}
+
+// ---------------------------------------------------------------------------
+// (e1) M-step back-projection: T[tile][p][lane] += sum_(d,c) c * P_dr
+// ---------------------------------------------------------------------------
+// Gather form of update_tomogram_nobg (max_update.c:142-230): one warp per
+// (orientation tile, pixel), walking the pixel's list of (frame, count) words
+// (pixels with mask < 2 only) and reading one 128-byte row of P per entry.
+// No atomics; pixels are visited heaviest first for balance.
+__global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Pst, int Nc,
+                                                     const uint32_t *__restrict__ cs,
+                                                     const long long *__restrict__ cs_off,
+                                                     const int *__restrict__ pix, int npix, int P, int RT,
+                                                     float *__restrict__ T) {
+	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (warp >= (long long)RT * npix)
+		return;
+	const int rt = (int)(warp / npix), k = (int)(warp - (long long)rt * npix);
+	const int p = pix[k];
+	const float *Pr = Pst + (size_t)rt * Nc * TILE + lane;
+	const long long beg = cs_off[p], end = cs_off[p + 1];
+	double acc = 0.;
+	for (long long j0 = beg; j0 < end; j0 += 32) {
+		const uint32_t e = (j0 + lane < end) ? __ldg(cs + j0 + lane) : 0u;
+		const int n = (int)min(32LL, end - j0);
+		for (int q0 = 0; q0 < n; q0 += 8) {
+			uint32_t ek[8];
+			float v[8];
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				ek[q] = __shfl_sync(FULL, e, q0 + q);
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				v[q] = (q0 + q < n) ? __ldg(Pr + (size_t)(ek[q] & IDX_MASK) * TILE) : 0.f;
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				acc = fma((double)(ek[q] >> IDX_BITS), (double)fmaxf(v[q], 0.f), acc);
+		}
+	}
+	float *out = T + ((size_t)rt * P + p) * TILE + lane;
+	*out = (float)((double)*out + acc);
+}
+
+// ---------------------------------------------------------------------------
+// (e2) merge: slice_merge3d of tomo_r / psum_r for every r with psum_r > 0
+// ---------------------------------------------------------------------------
+// Block = orientation tile x PB pixels (same thread layout as slice_log_kernel).
+// The tile's tomogram rows are staged through shared memory; each
+// (pixel, orientation) with mask <= 1 and in bounds adds (f * w, f) to its 8
+// corners with float2 vector atomics (model.c:171-244, max_update.c:33-36).
+__global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
+                                                     const double *__restrict__ psum_r,
+                                                     const double *__restrict__ quats, int M, int R,
+                                                     const double *__restrict__ qvals,
+                                                     const double *__restrict__ corr,
+                                                     const uint8_t *__restrict__ mask, int P, long long S,
+                                                     long long V, float2 *__restrict__ accum) {
+	__shared__ double s_rot[TILE][9];
+	__shared__ int s_mode[TILE];
+	__shared__ double s_ps[TILE];
+	__shared__ float s_tile[PB][TILE + 1];
+	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
+	if (t < TILE) {
+		int r = rt * TILE + t;
+		int rr = r < R ? r : 0;
+		rot_from_quat(&quats[(rr / M) * 5], s_rot[t]);
+		s_mode[t] = rr % M;
+		s_ps[t] = r < R ? psum_r[r] : 0.;
+	}
+	{
+		const int w = t >> 5, lane = t & 31;
+		for (int row = w; row < PB; row += 8) {
+			int pp = p0 + row;
+			s_tile[row][lane] = pp < P ? T[((size_t)rt * P + pp) * TILE + lane] : 0.f;
+		}
+	}
+	__syncthreads();
+	const int i = t & (PB - 1), g = t >> 6, p = p0 + i;
+	if (p >= P || mask[p] > 1)
+		return;
+	const double qx = qvals[3 * (size_t)p], qy = qvals[3 * (size_t)p + 1], qz = qvals[3 * (size_t)p + 2];
+	const double cr = corr[p];
+	const double center = (double)(S / 2);
+	long long o[8];
+	corner_offsets(S, o);
+	for (int k = 0; k < 8; ++k) {
+		const int j = g + 4 * k;
+		const double ps = s_ps[j];
+		if (!(ps > 0.))
+			continue;
+		Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+		if (!c.ok)
+			continue;
+		const double wv = ((double)s_tile[i][j] / ps) / cr;
+		double fw[8];
+		corner_weights(c, fw);
+		float2 *a = accum + (size_t)s_mode[j] * V + c.i000;
+#pragma unroll
+		for (int q = 0; q < 8; ++q)
+			atomicAdd(a + o[q], make_float2((float)(fw[q] * wv), (float)fw[q]));
+	}
+}
+
+// ---------------------------------------------------------------------------
+// model update (recon.pyx:112-149) and small per-frame kernels
+// ---------------------------------------------------------------------------
+__global__ void unpack_accum_kernel(const float2 *__restrict__ accum, long long n, double *__restrict__ model2,
+                                    double *__restrict__ weight) {
+	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	float2 a = accum[i];
+	model2[i] = (double)a.x;
+	weight[i] = (double)a.y;
+}
+
+__device__ __forceinline__ double friedel_avg(double a1, double w1, double a2, double w2) {
+	double a = dmul(0.5, dadd(dmul(a1, w1), dmul(a2, w2)));
+	double ws = dmul(0.5, dadd(w1, w2));
+	return ws > 0 ? a / ws : 0.;
+}
+
+// symmetrize_friedel (model.c:470-490) over every mode. The reference visits
+// (x, y, z) for x, y in [lo, S), z in [lo, c] sequentially; pairs with z < c
+// are touched once, pairs inside the z == c plane twice (the second visit
+// starts from the first member's result with the roles swapped). Each thread
+// owns one pair and replays exactly those visits.
+__global__ void friedel_kernel(double *__restrict__ model2, const double *__restrict__ weight, int S, int M) {
+	const int c = S / 2, lo = (S % 2 == 0) ? 1 : 0, n = S - lo, nz = c - lo + 1;
+	const long long per_mode = (long long)n * n * nz;
+	long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= per_mode * M)
+		return;
+	const int mode = (int)(id / per_mode);
+	long long k = id - (long long)mode * per_mode;
+	const int z = lo + (int)(k % nz);
+	k /= nz;
+	const int y = lo + (int)(k % n);
+	const int x = lo + (int)(k / n);
+	const long long V = (long long)S * S * S;
+	double *a = model2 + (size_t)mode * V;
+	const double *w = weight + (size_t)mode * V;
+	const long long v1 = ((long long)x * S + y) * S + z;
+	const long long v2 = ((long long)(2 * c - x) * S + (2 * c - y)) * S + (2 * c - z);
+	if (z < c) {
+		double A = friedel_avg(a[v1], w[v1], a[v2], w[v2]);
+		a[v1] = A;
+		a[v2] = A;
+		return;
+	}
+	// z == c: the member visited first owns the pair
+	const int mx = 2 * c - x, my = 2 * c - y;
+	const bool first = (x < mx) || (x == mx && y <= my);
+	if (!first)
+		return;
+	double A = friedel_avg(a[v1], w[v1], a[v2], w[v2]);
+	if (v1 != v2)
+		A = friedel_avg(A, w[v2], A, w[v1]);
+	a[v1] = A;
+	a[v2] = A;
+}
+
+// model2 /= weight where weight > 0; squared change against model1; model1
+// <- model2 or the alpha mix (recon.pyx:136-147). Block partial sums of the
+// squared change go to part[blockIdx.x] for a fixed-order reduction.
+template <typename MT>
+__global__ void __launch_bounds__(256) divide_update_kernel(double *__restrict__ model2,
+                                                            const double *__restrict__ weight,
+                                                            double *__restrict__ model1, MT *__restrict__ model1_copy,
+                                                            long long n, double alpha, double *__restrict__ part) {
+	__shared__ double s[8];
+	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	double d2 = 0.;
+	if (i < n) {
+		double m2 = model2[i];
+		if (weight[i] > 0.)
+			m2 = m2 / weight[i];
+		model2[i] = m2;
+		double m1 = model1[i];
+		double diff = m2 - m1;
+		d2 = diff * diff;
+		double nm = alpha > 0. ? alpha * m1 + (1 - alpha) * m2 : m2;
+		model1[i] = nm;
+		if (model1_copy != nullptr)
+			model1_copy[i] = (MT)nm;
+	}
+	d2 = warp_sum(d2);
+	if ((threadIdx.x & 31) == 0)
+		s[threadIdx.x >> 5] = d2;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.;
+		for (int k = 0; k < 8; ++k)
+			t += s[k];
+		part[blockIdx.x] = t;
+	}
+}
+
+// Fixed-order sum of n doubles by one block (second stage of reductions).
+__global__ void __launch_bounds__(1024) sum_kernel(const double *__restrict__ x, long long n,
+                                                   double *__restrict__ out) {
+	__shared__ double s[32];
+	double acc = 0.;
+	for (long long i = threadIdx.x; i < n; i += blockDim.x)
+		acc += x[i];
+	acc = warp_sum(acc);
+	if ((threadIdx.x & 31) == 0)
+		s[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		double v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.;
+		v = warp_sum(v);
+		if (threadIdx.x == 0)
+			*out = v;
+	}
+}
+
+// Sums of info / likelihood over good frames, and count of good frames:
+// out[0] = sum info, out[1] = sum likelihood (max_prob.c:367-371); one block.
+__global__ void __launch_bounds__(1024) frame_totals_kernel(const double *__restrict__ info,
+                                                            const double *__restrict__ ll,
+                                                            const uint8_t *__restrict__ blacklist, int N,
+                                                            double *__restrict__ out) {
+	__shared__ double s[2][32];
+	double a = 0., b = 0.;
+	for (int d = threadIdx.x; d < N; d += blockDim.x)
+		if (!blacklist[d]) {
+			a += info[d];
+			b += ll[d];
+		}
+	a = warp_sum(a);
+	b = warp_sum(b);
+	if ((threadIdx.x & 31) == 0) {
+		s[0][threadIdx.x >> 5] = a;
+		s[1][threadIdx.x >> 5] = b;
+	}
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		int nw = blockDim.x >> 5;
+		double x = threadIdx.x < nw ? s[0][threadIdx.x] : 0., y = threadIdx.x < nw ? s[1][threadIdx.x] : 0.;
+		x = warp_sum(x);
+		y = warp_sum(y);
+		if (threadIdx.x == 0) {
+			out[0] = x;
+			out[1] = y;
+		}
+	}
+}
+
+// beta_d = min(1, beta_start_d * factor) for good frames (recon.pyx:165-171)
+__global__ void beta_kernel(const double *__restrict__ beta_start, const uint8_t *__restrict__ blacklist,
+                            int N, double factor, double *__restrict__ beta) {
+	int d = blockIdx.x * blockDim.x + threadIdx.x;
+	if (d >= N || blacklist[d] == 1)
+		return;
+	double b = beta_start[d] * factor;
+	beta[d] = b > 1. ? 1. : b;
+}
+
+// phi_d = fcounts_d / psum_d for good frames (max_scale.c:13-15)
+__global__ void scale_kernel(const int *__restrict__ fcounts, const double *__restrict__ psum_d,
+                             const uint8_t *__restrict__ blacklist, int N, double *__restrict__ scale) {
+	int d = blockIdx.x * blockDim.x + threadIdx.x;
+	if (d >= N || blacklist[d])
+		return;
+	scale[d] = fcounts[d] / psum_d[d];
+}
+
+// Good-frame sum of phi and count, for normalize_scale (one block).
+__global__ void __launch_bounds__(1024) scale_sum_kernel(const double *__restrict__ scale,
+                                                         const uint8_t *__restrict__ blacklist, int N,
+                                                         double *__restrict__ out) {
+	__shared__ double s[2][32];
+	double a = 0., c = 0.;
+	for (int d = threadIdx.x; d < N; d += blockDim.x)
+		if (!blacklist[d]) {
+			a += scale[d];
+			c += 1.;
+		}
+	a = warp_sum(a);
+	c = warp_sum(c);
+	if ((threadIdx.x & 31) == 0) {
+		s[0][threadIdx.x >> 5] = a;
+		s[1][threadIdx.x >> 5] = c;
+	}
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		int nw = blockDim.x >> 5;
+		double x = threadIdx.x < nw ? s[0][threadIdx.x] : 0., y = threadIdx.x < nw ? s[1][threadIdx.x] : 0.;
+		x = warp_sum(x);
+		y = warp_sum(y);
+		if (threadIdx.x == 0) {
+			out[0] = x;
+			out[1] = y;
+		}
+	}
+}
+
+// phi /= mean for good frames; model1 of mode 0 *= mean (iterate.pyx:372-382)
+__global__ void apply_scale_norm_kernel(double *__restrict__ scale, const uint8_t *__restrict__ blacklist,
+                                        int N, double *__restrict__ model1, float *__restrict__ model1f,
+                                        long long V, const double *__restrict__ mean) {
+	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	const double m = *mean;
+	if (i < V) {
+		double v = model1[i] * m;
+		model1[i] = v;
+		if (model1f != nullptr)
+			model1f[i] = (float)v;
+	}
+	if (i < N && !blacklist[i])
+		scale[i] /= m;
+}
+
+// One slice, un-logged (Model.slice_gen, model.c:11-59)
+__global__ void slice_one_kernel(const double *__restrict__ quat, int mode, const double *__restrict__ qvals,
+                                 const double *__restrict__ corr, int P, const double *__restrict__ model,
+                                 long long S, long long V, double *__restrict__ out) {
+	int p = blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= P)
+		return;
+	double rot[9];
+	rot_from_quat(quat, rot);
+	Cell c = locate(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2],
+	                (double)(S / 2), S);
+	out[p] = interp(c, model + (size_t)mode * V, S, corr[p]);
+}
+
+// One merge in FP64 (Model.slice_merge, model.c:171-244)
+__global__ void merge_one_kernel(const double *__restrict__ quat, int mode, const double *__restrict__ view,
+                                 const double *__restrict__ qvals, const double *__restrict__ corr,
+                                 const uint8_t *__restrict__ mask, int P, long long S, long long V,
+                                 double *__restrict__ model2, double *__restrict__ weight) {
+	int p = blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= P || mask[p] > 1)
+		return;
+	double rot[9];
+	rot_from_quat(quat, rot);
+	Cell c = locate(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2],
+	                (double)(S / 2), S);
+	if (!c.ok)
+		return;
+	double fw[8];
+	long long o[8];
+	corner_weights(c, fw);
+	corner_offsets(S, o);
+	const double w = view[p] / corr[p];
+	for (int q = 0; q < 8; ++q) {
+		atomicAdd(weight + (size_t)mode * V + c.i000 + o[q], fw[q]);
+		atomicAdd(model2 + (size_t)mode * V + c.i000 + o[q], fw[q] * w);
+	}
+}
+
+}  // namespace dfg

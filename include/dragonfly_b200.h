@@ -1,0 +1,184 @@
+/* dragonfly_b200: one EMC iteration (expand -> maximize -> compress) of
+ * duaneloh/Dragonfly on an NVIDIA B200 (sm_100a), behind a plain C ABI.
+ *
+ * A context owns one GPU's copies of the detector, the sparse photon frames,
+ * the orientation list, the model and the per-frame parameters, plus all work
+ * buffers. Arguments are plain host pointers and sizes in the reference's own
+ * layouts; nothing in this header needs CUDA or torch types.
+ *
+ * Every function returns DFG_OK (0) or an error code; dfg_last_error() gives a
+ * readable message. A context is not re-entrant: calls on one context must not
+ * overlap (the reference's maximize() has the same rule, recon.pyx:99).
+ *
+ * Library: dragonfly_b200/libdfgpu.so. Python binding: dragonfly_b200/_lib.py.
+ */
+#ifndef DRAGONFLY_B200_H
+#define DRAGONFLY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DFG_API __attribute__((visibility("default")))
+#else
+#define DFG_API
+#endif
+
+#define DFG_OK 0
+#define DFG_ERR_ARG 1      /* invalid argument (message says which) */
+#define DFG_ERR_CUDA 2     /* a CUDA call failed */
+#define DFG_ERR_STATE 3    /* required input not set yet */
+#define DFG_ERR_NOMEM 4    /* device allocation failed */
+
+typedef struct dfg_ctx dfg_ctx;
+
+/* Per-call parameters of one iteration. Mirrors the struct params fields that
+ * maximize() and EMCRecon.update_beta read (dragonfly/src/params.h:6-34). */
+typedef struct dfg_iter_params {
+	int iteration;     /* params.iteration, 1-based */
+	int need_scaling;  /* per-frame scale factors phi_d in the likelihood */
+	int update_scale;  /* update phi_d = fcounts_d / psum_d after the M-step */
+	int known_scale;   /* use phi_d in the likelihood from iteration 1 */
+	double beta_jump;  /* beta schedule: beta_d = min(1, beta_start_d * */
+	int beta_period;   /*   beta_jump^((iteration-1)/beta_period) * beta_factor) */
+	double beta_factor;
+} dfg_iter_params;
+
+/* ---- lifetime -------------------------------------------------------------
+ * Replaces EMCRecon.__init__ / free (dragonfly/recon.pyx:37-46, 176-180). */
+DFG_API int dfg_create(int device, dfg_ctx **out);
+DFG_API void dfg_destroy(dfg_ctx *ctx);
+DFG_API const char *dfg_last_error(const dfg_ctx *ctx);
+/* Version string of the library. */
+DFG_API const char *dfg_version(void);
+
+/* ---- inputs ---------------------------------------------------------------
+ * Detector: qvals [num_pix][3] (voxel units), corr [num_pix], raw_mask
+ * [num_pix] (0 good, 1 merge only, 2 bad). Replaces CDetector.parse / setters
+ * (dragonfly/detector.pyx:31-74, 161-206) and struct detector
+ * (dragonfly/src/detector.h:6-16). */
+DFG_API int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, const double *corr,
+                     const uint8_t *raw_mask);
+
+/* Sparse photon frames in the .emc layout: ones[num_data], multi[num_data],
+ * place_ones[sum ones], place_multi[sum multi], count_multi[sum multi]
+ * (dragonfly/src/emcfile.h:12-32, parse_binarydataset emcfile.c:3-57). Also
+ * computes fcounts, sum_fact and mean_count (calc_frame_counts and
+ * calc_sum_fact, dragonfly/src/iterate.c:3-117; ln c! as lgamma(c + 1)),
+ * resets the blacklist to all-good and phi_d to 1. Replaces Iterate.set_data
+ * (dragonfly/iterate.pyx:241-266). */
+DFG_API int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const int *multi,
+                   const int *place_ones, const int *place_multi, const int *count_multi);
+
+/* Orientations quats [num_rot][5] = (q0, q1, q2, q3, weight). Replaces
+ * Iterate.set_quat (dragonfly/iterate.pyx:268-274), struct quaternion
+ * (dragonfly/src/quaternion.h:11-15). */
+DFG_API int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quats);
+
+/* Model model1 [num_modes][size][size][size] (C order), centre size / 2.
+ * Replaces Iterate.set_model / Model.allocate (dragonfly/iterate.pyx:184-190,
+ * dragonfly/model.pyx:43-103). */
+DFG_API int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const double *model1);
+
+/* Per-frame arrays (num_data entries). Replace the Iterate.scale setter,
+ * parse_blacklist and calc_beta (dragonfly/iterate.pyx:284-402;
+ * dragonfly/src/iterate.c:66-83). dfg_calc_beta: start > 0 sets every
+ * beta_start_d = start; start <= 0 selects the reference's empirical rule. */
+DFG_API int dfg_set_scale(dfg_ctx *ctx, const double *scale);
+DFG_API int dfg_set_blacklist(dfg_ctx *ctx, const uint8_t *blacklist);
+DFG_API int dfg_set_beta_start(dfg_ctx *ctx, const double *beta_start);
+DFG_API int dfg_calc_beta(dfg_ctx *ctx, double start, int need_scaling);
+
+/* ---- the iteration --------------------------------------------------------
+ * update_beta (recon.pyx:151-174) then maximize (dragonfly/src/maximize.c:8-56):
+ * rescale, E-step with the reference's pruning rule, normalisation, M-step,
+ * merge into model2 / inter_weight and, when need_scaling && update_scale, the
+ * phi update (dragonfly/src/max_scale.c:3-19). Writes the average
+ * log-likelihood to *avg_likelihood. Replaces `maximize(struct max_data*)`
+ * (dragonfly/src/maximize.h:45, called at recon.pyx:99). */
+DFG_API int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_likelihood);
+
+/* EMCRecon.update_model for 3-D reconstructions with Friedel symmetry
+ * (recon.pyx:112-149 with model.c:470-490): symmetrise the merged sums,
+ * divide by inter_weight, rms change against model1, model1 <- model2
+ * (alpha = 0) or alpha * model1 + (1 - alpha) * model2. */
+DFG_API int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change);
+
+/* Iterate.normalize_scale (dragonfly/iterate.pyx:361-384): mean phi over
+ * good frames, mode-0 model1 *= mean, phi /= mean. Writes the mean. */
+DFG_API int dfg_normalize_scale(dfg_ctx *ctx, double *mean_scale);
+
+/* ---- results (host copies; NULL pointers are skipped) ---------------------
+ * The read-only properties of EMCRecon / Iterate / Model
+ * (dragonfly/recon.pyx:306-415, iterate.pyx:470-592, model.pyx:295-313). */
+DFG_API int dfg_get_frame_results(dfg_ctx *ctx, int *rmax, double *info, double *likelihood,
+                          double *max_exp, double *p_norm, double *psum_d);
+DFG_API int dfg_get_quat_norm(dfg_ctx *ctx, double *quat_norm);             /* [num_data][num_modes] */
+DFG_API int dfg_get_orientation_results(dfg_ctx *ctx, double *u, double *psum_r); /* [modes*num_rot] */
+DFG_API int dfg_get_model(dfg_ctx *ctx, double *model1, double *model2, double *inter_weight);
+DFG_API int dfg_get_frame_params(dfg_ctx *ctx, double *scale, double *beta, double *beta_start,
+                         int *fcounts, double *sum_fact, uint8_t *blacklist);
+/* out[0..4] = rescale, mutual_info, average log-likelihood, mean_count, rms_change */
+DFG_API int dfg_get_scalars(dfg_ctx *ctx, double *out);
+DFG_API int dfg_get_num_prob(dfg_ctx *ctx, int *num_prob);  /* kept pairs per frame */
+
+/* ---- one-slice operations -------------------------------------------------
+ * Model.slice_gen (dragonfly/model.pyx:105-132 -> model.c:11-59): slice of
+ * model1 at one quaternion, out[num_pix]. */
+DFG_API int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double *out);
+/* Model.slice_merge (dragonfly/model.pyx:134-151 -> model.c:171-244): merges
+ * view[num_pix] into the host arrays model2 / inter_weight [modes][size^3]. */
+DFG_API int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const double *view,
+                    double *model2, double *inter_weight);
+
+/* ---- end to end from host buffers ----------------------------------------
+ * EMCRecon.run_iteration's compute (recon.pyx:93-104): model1_inout (host,
+ * [modes][size^3]) is uploaded, maximize + update_model (+ normalize_scale
+ * when need_scaling) run, and the new model1, rmax[num_data] and
+ * likelihood[num_data] come back to host memory. */
+DFG_API int dfg_run_iteration_host(dfg_ctx *ctx, const dfg_iter_params *par, double alpha,
+                           double *model1_inout, int *rmax, double *likelihood,
+                           double *avg_likelihood, double *rms_change);
+
+/* ---- synthetic data -------------------------------------------------------
+ * GPU counterpart of the reference simulator's gen_and_save_dataset
+ * (dragonfly/utils/src/make_data.c:115-326): for each frame d, the slice of
+ * intens [size^3] (centre size / 2) at quats4[d] (q0..q3) on the context's
+ * detector, times phi[d], Poisson-sampled on pixels with mask <= 1. The frames
+ * become the context's frames (as dfg_set_frames). totals[0..2] = ones total,
+ * multi total, photons. dfg_get_frames copies the context's frames out
+ * (arrays sized from dfg_set_frames / the totals). */
+DFG_API int dfg_simulate_frames(dfg_ctx *ctx, long size, const double *intens, int num_data,
+                                const double *quats4, const double *phi, unsigned long long seed,
+                                long long *totals);
+DFG_API int dfg_get_frames(dfg_ctx *ctx, int *ones, int *multi, int *place_ones, int *place_multi,
+                           int *count_multi);
+
+/* ---- tuning and instrumentation ------------------------------------------
+ * Options: "pair_budget_mb" (device memory for the per-pair buffers, which
+ * sets the frame chunk), "timing" (1: record per-phase CUDA-event times). */
+DFG_API int dfg_set_option(dfg_ctx *ctx, const char *key, double value);
+/* Phase times in ms summed since the last reset, and launch counts:
+ * names[i] = "slice", "estep", "norm", "psum", "mstep", "merge", "update".
+ * n = number of slots provided. Returns the number of phases. */
+DFG_API int dfg_get_phase_times(dfg_ctx *ctx, double *ms, long *launches, int n);
+DFG_API const char *dfg_phase_name(int i);
+/* Device timing on the context's stream: dfg_event_record puts a CUDA event
+ * (slot 0..7) on the stream; dfg_event_elapsed waits for slot b and writes the
+ * milliseconds from slot a to slot b. */
+DFG_API int dfg_event_record(dfg_ctx *ctx, int slot);
+DFG_API int dfg_event_elapsed(dfg_ctx *ctx, int a, int b, double *ms);
+DFG_API int dfg_reset_phase_times(dfg_ctx *ctx);
+/* Sizes of the last iteration: out[0] = R (modes * num_rot), out[1] = frames,
+ * out[2] = photon entries in the E-step lists, out[3] = M-step entries,
+ * out[4] = frame chunks, out[5] = frames per chunk, out[6] = kernels launched
+ * by this context so far. */
+DFG_API int dfg_get_workload(dfg_ctx *ctx, long long *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,19 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libdfgpu.so")
+
+
+@pytest.fixture(scope="session")
+def oracle_built():
+    from oracle.oracle import build_oracle
+    build_oracle()
+    return True

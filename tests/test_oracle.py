@@ -1,0 +1,100 @@
+"""The CPU oracle, pinned against the reference engine.
+
+* golden vectors (tests/golden/*.npz, produced by the reference's own C engine
+  with one thread by tests/golden/make_golden.py): the oracle must reproduce
+  them bit for bit;
+* where the reference sources were compiled here (oracle/_ref), a live
+  comparison on fresh seeded inputs, also bit for bit.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from common import CASES, load_case
+from oracle.oracle import EMCProblem, OracleEngine, ReferenceEngine, reference_available
+
+
+def sha(m):
+    return hashlib.sha256(np.ascontiguousarray(m, np.float64).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_golden(name, oracle_built):
+    prob, g = load_case(name)
+    eng = OracleEngine(prob)
+    np.testing.assert_array_equal(eng.fcounts, g["fcounts"])
+    np.testing.assert_array_equal(eng.sum_fact, g["sum_fact"])
+    np.testing.assert_array_equal(eng.beta_start, g["beta_start"])
+    for it in range(1, int(g["iters"]) + 1):
+        r = eng.run_iteration(it)
+        k = "it%d_" % it
+        sc = g[k + "scalars"]
+        assert r["avg_likelihood"] == sc[0]
+        assert r["mutual_info"] == sc[1]
+        assert r["rms_change"] == sc[2]
+        assert r["rescale"] == sc[3]
+        for key in ("rmax", "info", "likelihood", "max_exp", "p_norm", "psum_d", "u"):
+            np.testing.assert_array_equal(r[key], g[k + key], err_msg=key)
+        # the reference never writes beta of blacklisted frames (malloc'd,
+        # iterate.c:70; skipped at recon.pyx:166-167)
+        good = g["blacklist"] == 0
+        np.testing.assert_array_equal(r["beta"][good], g[k + "beta"][good])
+        if prob.num_modes > 1:
+            np.testing.assert_array_equal(r["quat_norm"], g[k + "quat_norm"])
+        if prob.need_scaling:
+            np.testing.assert_array_equal(r["scale"], g[k + "scale"])
+        assert sha(r["model2_sum"]) == str(g[k + "model2_sum_sha256"])
+        assert sha(r["inter_weight"]) == str(g[k + "weight_sha256"])
+        assert sha(r["model1"]) == str(g[k + "model_sha256"])
+    np.testing.assert_array_equal(r["model1"], g["final_model1"])
+
+
+def test_golden_edge_case_contents():
+    """The edge case really exercises what it claims to."""
+    prob, g = load_case("edge")
+    assert prob.num_pix % 64 != 0 and prob.num_rot % 32 != 0
+    assert (g["blacklist"] == 1).sum() == 10
+    assert (prob.ones == 0).sum() >= 2
+    assert prob.count_multi.max() > 1023
+    rmax = g["it1_rmax"]
+    assert ((rmax == -1) & (g["blacklist"] == 0)).sum() > 0  # frames with every pval = -inf
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference sources not compiled here")
+@pytest.mark.parametrize("seed,prob_kw", [
+    (11, dict(beta=1.)),
+    (12, dict(beta=0.02, beta_jump=2., beta_period=1, need_scaling=1, update_scale=1)),
+    (13, dict(beta=0.3, need_scaling=1, update_scale=0, known_scale=1, alpha=0.25)),
+])
+def test_oracle_matches_live_reference(seed, prob_kw, oracle_built):
+    from dragonfly_b200 import synth
+    d = synth.small_problem(seed=seed, det_side=28, size=33, qmax=15., n_atoms=80, atom_radius=6.,
+                            num_div=2, n_frames=160, mean_count=40.)
+    scale = None
+    if prob_kw.get("known_scale"):
+        scale = np.random.default_rng(seed).uniform(0.5, 1.5, d["ones"].size)
+    p = EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"],
+                   d["place_multi"], d["count_multi"], d["quats"], d["model_start"], scale=scale, **prob_kw)
+    ref = ReferenceEngine(p, num_threads=1)
+    orc = OracleEngine(p)
+    for it in (1, 2, 3):
+        a = ref.run_iteration(it)
+        b = orc.run_iteration(it)
+        for k in ("avg_likelihood", "mutual_info", "rms_change", "rescale"):
+            assert a[k] == b[k], k
+        for k in ("rmax", "info", "likelihood", "max_exp", "p_norm", "psum_d", "u", "model1", "model2"):
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+        if p.need_scaling:
+            np.testing.assert_array_equal(a["scale"], b["scale"])
+    ref.close()
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference sources not compiled here")
+def test_oracle_slice_ops_match_reference(oracle_built):
+    prob, _ = load_case("beta1")
+    ref = ReferenceEngine(prob, num_threads=1)
+    orc = OracleEngine(prob)
+    for r in (0, 17, 200, 419):
+        np.testing.assert_array_equal(ref.slice_gen(prob.quats[r]), orc.slice_gen(prob.quats[r]))
+    ref.close()
