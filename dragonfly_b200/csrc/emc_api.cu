@@ -386,10 +386,8 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	ctx->RT = (ctx->R + TILE - 1) / TILE;
 	ctx->R_pad = ctx->RT * TILE;
 	const size_t tiles_px = (size_t)ctx->RT * ctx->P * TILE;
-	const int nblk = (ctx->P + PB - 1) / PB;
 	CK(ctx->logW.ensure(tiles_px));
 	CK(ctx->T.ensure(tiles_px));
-	CK(ctx->upart.ensure((size_t)nblk * ctx->R_pad));
 	CK(ctx->u.ensure((size_t)ctx->R_pad));
 	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
 	CK(ctx->scalars.ensure(8));
@@ -406,12 +404,16 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	if (ctx->chunks_R != ctx->R) {
 		ctx->pval.release();
 		ctx->Pst.release();
+		ctx->tmax.release();
+		ctx->targ.release();
 		if (int rc = build_chunks(ctx))
 			return rc;
 	}
 	const size_t pairs = (size_t)ctx->R_pad * ctx->chunk_frames;
 	CK(ctx->pval.ensure(pairs));
 	CK(ctx->Pst.ensure(pairs));
+	CK(ctx->tmax.ensure((size_t)ctx->RT * ctx->chunk_frames));
+	CK(ctx->targ.ensure((size_t)ctx->RT * ctx->chunk_frames));
 	const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
 	CK(ctx->psum_part.ensure((size_t)nsplit * ctx->R_pad));
 	return DFG_OK;
@@ -443,19 +445,20 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 
 	// slices, u_r, rescale (calculate_rescale, max_prob.c:3-64)
 	phase_begin(ctx, PH_SLICE);
-	slice_log_kernel<double><<<dim3(nblk, RT), 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p,
-	                                                         ctx->mask.p, P, ctx->model1.p, S, V, ctx->logW.p,
-	                                                         ctx->upart.p, R_pad);
+	slice_log_kernel<double><<<dim3(nblk, RT), 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, P,
+	                                                         ctx->model1.p, S, V, ctx->logW.p);
 	CKL("slice_log_kernel");
-	u_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->upart.p, nblk, R, R_pad, ctx->u.p);
-	CKL("u_reduce_kernel");
-	rescale_kernel<<<1, 1024, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
+	u_sequential_kernel<double><<<blocks_for(R, 128), 128, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p,
+	                                                               ctx->corr.p, ctx->mask.p, P, ctx->model1.p,
+	                                                               S, V, ctx->u.p);
+	CKL("u_sequential_kernel");
+	rescale_kernel<<<1, 32, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
 	CKL("rescale_kernel");
 	phase_end(ctx, PH_SLICE, 3);
 
 	CK(cudaMemsetAsync(ctx->T.p, 0, (size_t)RT * P * TILE * sizeof(float), st));
 	CK(cudaMemsetAsync(ctx->psum_r.p, 0, (size_t)R_pad * sizeof(double), st));
-	CK(cudaMemsetAsync(ctx->accum.p, 0, (size_t)M * V * sizeof(float2), st));
+	CK(cudaMemsetAsync(ctx->accum.p, 0, (size_t)M * V * sizeof(double2), st));
 	const int use_scale = par->need_scaling && (par->iteration > 1 || par->known_scale);
 	const int psum_d_on = par->need_scaling && par->update_scale;
 
@@ -467,16 +470,25 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 			long long warps = (long long)RT * Nc;
 			estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
 			    ctx->logW.p, ctx->u.p, ctx->quats.p, M, R, ctx->ph.p, ctx->ph_off.p, ctx->scale.p,
-			    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p);
+			    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
+			    ctx->targ.p);
 			CKL("estep_kernel");
 		}
 		phase_end(ctx, PH_ESTEP, 1);
 		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
 		phase_begin(ctx, PH_NORM);
-		norm_kernel<<<blocks_for(Nc, 8), 256, 0, st>>>(
-		    ctx->pval.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p, ctx->sum_fact.p,
-		    ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p, ctx->max_exp.p, ctx->p_norm.p,
-		    ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p, ctx->num_prob.p);
+		if (M > 1)
+			norm_kernel<true><<<blocks_for(Nc, 8), 256, 0, st>>>(
+			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p,
+			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
+			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
+			    ctx->num_prob.p);
+		else
+			norm_kernel<false><<<blocks_for(Nc, 8), 256, 0, st>>>(
+			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p,
+			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
+			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
+			    ctx->num_prob.p);
 		CKL("norm_kernel");
 		phase_end(ctx, PH_NORM, 1);
 		// psum_r (calc_psum_r, max_update.c:108-116)
@@ -506,7 +518,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	// merge (merge_tomogram -> slice_merge3d)
 	phase_begin(ctx, PH_MERGE);
 	merge_kernel<<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
-	                                              ctx->corr.p, ctx->mask.p, P, S, V, ctx->accum.p);
+	                                              ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p);
 	CKL("merge_kernel");
 	phase_end(ctx, PH_MERGE, 1);
 

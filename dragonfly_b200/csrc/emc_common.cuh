@@ -10,11 +10,12 @@
 //                                coalesced 128-byte row (32 orientations).
 //   pval     [RT][Nc][32] double log-likelihood of (orientation, frame) pairs
 //                                of the current frame chunk.
+//   tmax/targ [RT][Nc]           per (tile, frame) maximum pval and its lowest r.
 //   Pst      [RT][Nc][32] float  normalised probability of kept pairs; the sign
 //                                carries the reference's PROB_MIN gate: P > 1e-6
 //                                stored as +P, kept but <= 1e-6 as -P, pruned 0.
 //   T        [RT][P][32] float   photon tomograms sum_d P_dr * K_d[p].
-//   accum    [M*V] float2        (model2 sum, weight) merge accumulators.
+//   accum    [M*V] double2       (model2 sum, weight) merge accumulators.
 // Photon lists are packed 32-bit words: low 22 bits a pixel (E-step, per
 // frame) or a chunk-local frame (M-step, per pixel), high 10 bits the count;
 // counts above 1023 are split over several words (all uses are linear in it).

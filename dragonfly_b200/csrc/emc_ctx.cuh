@@ -99,12 +99,13 @@ struct dfg_ctx {
 	DevBuf<double> quats;
 	long long S = 0, V = 0;
 	DevBuf<double> model1, model2, weight;
-	DevBuf<float2> accum;
+	DevBuf<double2> accum;
 
 	// work buffers
 	DevBuf<float> logW, Pst, T;
-	DevBuf<double> upart, u, pval, psum_r, psum_part, scalars, red_part;
-	DevBuf<int> rmax, num_prob;
+	DevBuf<double> u, pval, psum_r, psum_part, scalars, red_part;
+	DevBuf<int> rmax, num_prob, targ;
+	DevBuf<double> tmax;  // per (tile, frame) maximum of pval and its first orientation
 	DevBuf<double> info, likelihood, max_exp, p_norm, psum_d, quat_norm;
 	std::vector<Chunk> chunks;
 	int chunk_frames = 0;

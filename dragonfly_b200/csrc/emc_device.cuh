@@ -12,17 +12,14 @@ namespace dfg {
 // Block = one orientation tile x PB pixels, 256 threads: thread (i = t % 64,
 // g = t / 64) computes pixel i for orientations g, g+4, ..., g+28, so a warp
 // walks 32 neighbouring pixels of one orientation (neighbouring model reads).
-// u_r (sum of un-logged W over mask == 0 pixels, max_prob.c:32-40) is reduced
-// per block in a fixed order into upart[block][r].
 template <typename MT>
 __global__ void __launch_bounds__(256) slice_log_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
-    const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
-    long long S, long long V, float *__restrict__ logW, double *__restrict__ upart, int R_pad) {
+    const double *__restrict__ corr, int P, const MT *__restrict__ model, long long S, long long V,
+    float *__restrict__ logW) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ float s_tile[PB][TILE + 1];
-	__shared__ double s_u[2][TILE];
 	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
 	if (t < TILE) {
 		int r = rt * TILE + t;
@@ -34,31 +31,20 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 	const int i = t & (PB - 1), g = t >> 6, p = p0 + i;
 	const bool pix = p < P;
 	double qx = 0., qy = 0., qz = 0., cr = 1.;
-	bool good = false;
 	if (pix) {
 		qx = qvals[3 * (size_t)p]; qy = qvals[3 * (size_t)p + 1]; qz = qvals[3 * (size_t)p + 2];
 		cr = corr[p];
-		good = mask[p] < 1;
 	}
 	const double center = (double)(S / 2);
 #pragma unroll 2
 	for (int k = 0; k < 8; ++k) {
 		const int j = g + 4 * k;
-		double W = 0.;
 		if (pix) {
 			Cell c = locate(s_rot[j], qx, qy, qz, center, S);
-			W = interp(c, model + (size_t)s_mode[j] * V, S, cr);
-			s_tile[i][j] = (float)log(W);
+			s_tile[i][j] = (float)log(interp(c, model + (size_t)s_mode[j] * V, S, cr));
 		}
-		double uw = warp_sum((pix && good) ? W : 0.);
-		if ((t & 31) == 0)
-			s_u[i >> 5][j] = uw;
 	}
 	__syncthreads();
-	if (t < TILE) {
-		int r = rt * TILE + t;
-		upart[(size_t)blockIdx.x * R_pad + r] = s_u[0][t] + s_u[1][t];
-	}
 	// coalesced store: warp w writes rows w, w+8, ...
 	const int w = t >> 5, lane = t & 31;
 	for (int row = w; row < PB; row += 8) {
@@ -68,36 +54,45 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 	}
 }
 
-// u_r = sum over pixel blocks in block order (deterministic)
-__global__ void u_reduce_kernel(const double *__restrict__ upart, int nblk, int R, int R_pad,
-                                double *__restrict__ u) {
-	int r = blockIdx.x * blockDim.x + threadIdx.x;
+// u_r = sum of W over mask == 0 pixels, added in pixel order (max_prob.c:32-38).
+// One thread per orientation walks the pixels sequentially, so u_r is
+// bit-identical to the reference's (frames without photons are ranked by u_r
+// alone, and orientations related by a symmetry of the model tie exactly).
+// Pixel data are read uniformly by a warp; orientations differ per lane.
+template <typename MT>
+__global__ void __launch_bounds__(128) u_sequential_kernel(const double *__restrict__ quats, int M, int R,
+                                                           const double *__restrict__ qvals,
+                                                           const double *__restrict__ corr,
+                                                           const uint8_t *__restrict__ mask, int P,
+                                                           const MT *__restrict__ model, long long S, long long V,
+                                                           double *__restrict__ u) {
+	const int r = blockIdx.x * blockDim.x + threadIdx.x;
 	if (r >= R)
 		return;
-	double s = 0.;
-	for (int b = 0; b < nblk; ++b)
-		s += upart[(size_t)b * R_pad + r];
-	u[r] = s;
+	double rot[9];
+	rot_from_quat(&quats[(r / M) * 5], rot);
+	const MT *m = model + (size_t)(r % M) * V;
+	const double center = (double)(S / 2);
+	double acc = 0.;
+	for (int p = 0; p < P; ++p) {
+		if (mask[p] < 1) {
+			Cell c = locate(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2], center, S);
+			acc = dadd(acc, interp(c, m, S, corr[p]));
+		}
+	}
+	u[r] = acc;
 }
 
-// rescale = mean_count / sum_r w_r u_r * M (max_prob.c:40, 55-60); one block.
-__global__ void __launch_bounds__(1024) rescale_kernel(const double *__restrict__ u,
-                                                       const double *__restrict__ quats, int M, int R,
-                                                       double mean_count, double *__restrict__ scalars) {
-	__shared__ double s[32];
-	double acc = 0.;
-	for (int r = threadIdx.x; r < R; r += blockDim.x)
-		acc += quats[(r / M) * 5 + 4] * u[r];
-	acc = warp_sum(acc);
-	if ((threadIdx.x & 31) == 0)
-		s[threadIdx.x >> 5] = acc;
-	__syncthreads();
-	if (threadIdx.x < 32) {
-		double v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.;
-		v = warp_sum(v);
-		if (threadIdx.x == 0)
-			scalars[0] = mean_count / v * M;
-	}
+// rescale = mean_count / sum_r w_r u_r * M, summed in orientation order
+// (max_prob.c:40, 55-60); a single thread.
+__global__ void rescale_kernel(const double *__restrict__ u, const double *__restrict__ quats, int M, int R,
+                               double mean_count, double *__restrict__ scalars) {
+	if (threadIdx.x != 0 || blockIdx.x != 0)
+		return;
+	double total = 0.;
+	for (int r = 0; r < R; ++r)
+		total = dadd(total, dmul(quats[(r / M) * 5 + 4], u[r]));
+	scalars[0] = mean_count / total * M;
 }
 
 // ---------------------------------------------------------------------------
@@ -113,7 +108,8 @@ __global__ void __launch_bounds__(256) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ quats, int M,
     int R, const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
     const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
-    const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval) {
+    const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval, double *__restrict__ tmax,
+    int *__restrict__ targ) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * Nc)
@@ -146,6 +142,23 @@ __global__ void __launch_bounds__(256) estep_kernel(
 		}
 	}
 	pval[((size_t)rt * Nc + dl) * TILE + lane] = acc;
+	// tile maximum and its lowest orientation index (strict > in ascending r,
+	// as the running maximum of max_prob.c:199-202)
+	double m = (r < R && acc > MAX_EXP_START) ? acc : MAX_EXP_START;
+	int am = (r < R && acc > MAX_EXP_START) ? r : -1;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		double om = __shfl_xor_sync(FULL, m, o);
+		int oa = __shfl_xor_sync(FULL, am, o);
+		if (om > m || (om == m && oa >= 0 && (am < 0 || oa < am))) {
+			m = om;
+			am = oa;
+		}
+	}
+	if (lane == 0) {
+		tmax[(size_t)rt * Nc + dl] = m;
+		targ[(size_t)rt * Nc + dl] = am;
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -156,16 +169,21 @@ __global__ void __launch_bounds__(256) estep_kernel(
 // when pval + 14/beta > m and, when pval > m, the list is pruned to entries
 // > pval - 14/beta. With one thread the final list is: every r up to the first
 // maximiser r* with pval > max - 14/beta, and every r after r* with
-// pval + 14/beta > max. The maximiser is the lowest index reaching the maximum.
-// P_dr = exp(beta (pval - max)) / p_norm (max_update.c:96-98); likelihood,
-// psum_d, info and quat_norm follow max_update.c:105-130.
+// pval + 14/beta > max. The maximiser is the lowest index reaching the maximum;
+// it comes from the per-tile maxima the E-step wrote (lanes take tiles lane,
+// lane + 32, ...). P_dr = exp(beta (pval - max)) / p_norm (max_update.c:96-98);
+// likelihood, psum_d, info and quat_norm follow max_update.c:105-130. The two
+// passes over a frame's log-likelihoods keep UNR tile rows in flight per lane.
+template <bool MULTI>
 __global__ void __launch_bounds__(256) norm_kernel(
-    const double *__restrict__ pval, int RT, int Nc, int d0, int R, int M, const double *__restrict__ quats,
-    const double *__restrict__ u, const double *__restrict__ beta, const double *__restrict__ sum_fact,
-    const uint8_t *__restrict__ blacklist, int psum_d_on, const double *__restrict__ scalars,
-    float *__restrict__ Pst, int *__restrict__ rmax, double *__restrict__ max_exp,
-    double *__restrict__ p_norm, double *__restrict__ info, double *__restrict__ likelihood,
-    double *__restrict__ psum_d, double *__restrict__ quat_norm, int *__restrict__ num_prob) {
+    const double *__restrict__ pval, const double *__restrict__ tmax, const int *__restrict__ targ, int RT,
+    int Nc, int d0, int R, int M, const double *__restrict__ quats, const double *__restrict__ u,
+    const double *__restrict__ beta, const double *__restrict__ sum_fact, const uint8_t *__restrict__ blacklist,
+    int psum_d_on, const double *__restrict__ scalars, float *__restrict__ Pst, int *__restrict__ rmax,
+    double *__restrict__ max_exp, double *__restrict__ p_norm, double *__restrict__ info,
+    double *__restrict__ likelihood, double *__restrict__ psum_d, double *__restrict__ quat_norm,
+    int *__restrict__ num_prob) {
+	constexpr int UNR = 4;
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= Nc)
@@ -174,18 +192,16 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	const double *pv = pval + (size_t)dl * TILE + lane;
 	float *ps = Pst + (size_t)dl * TILE + lane;
 	const size_t tstride = (size_t)Nc * TILE;
+	const bool bl = blacklist[d] != 0;
 
 	double m = MAX_EXP_START;
-	int am = 0;
-	if (!blacklist[d]) {
-		for (int rt = 0; rt < RT; ++rt) {
-			int r = rt * TILE + lane;
-			if (r < R) {
-				double v = pv[rt * tstride];
-				if (v > m) {
-					m = v;
-					am = r;
-				}
+	int am = -1;
+	if (!bl) {
+		for (int rt = lane; rt < RT; rt += 32) {
+			double v = tmax[(size_t)rt * Nc + dl];
+			if (v > m) {
+				m = v;
+				am = targ[(size_t)rt * Nc + dl];
 			}
 		}
 	}
@@ -193,13 +209,12 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	for (int o = 16; o > 0; o >>= 1) {
 		double om = __shfl_xor_sync(FULL, m, o);
 		int oa = __shfl_xor_sync(FULL, am, o);
-		if (om > m || (om == m && oa < am)) {
+		if (om > m || (om == m && oa >= 0 && (am < 0 || oa < am))) {
 			m = om;
 			am = oa;
 		}
 	}
-	const bool any = !blacklist[d] && m != MAX_EXP_START;
-	if (!any) {
+	if (bl || m == MAX_EXP_START) {
 		for (int rt = 0; rt < RT; ++rt)
 			ps[rt * tstride] = 0.f;
 		if (lane == 0) {
@@ -211,7 +226,7 @@ __global__ void __launch_bounds__(256) norm_kernel(
 			psum_d[d] = 0.;
 			num_prob[d] = 0;
 		}
-		if (M > 1 && lane < M)
+		if (MULTI && lane < M)
 			quat_norm[(size_t)d * M + lane] = 0.;
 		return;
 	}
@@ -222,14 +237,20 @@ __global__ void __launch_bounds__(256) norm_kernel(
 
 	double s = 0.;
 	int cnt = 0;
-	for (int rt = 0; rt < RT; ++rt) {
-		int r = rt * TILE + lane;
-		if (r < R) {
-			double v = pv[rt * tstride];
-			bool kept = (r <= rstar) ? (v > lo) : (dadd(v, thr) > m);
-			if (kept) {
-				s += exp(dmul(b, dsub(v, m)));
-				cnt++;
+	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
+		double v[UNR];
+#pragma unroll
+		for (int k = 0; k < UNR; ++k)
+			v[k] = (rt0 + k < RT) ? pv[(rt0 + k) * tstride] : 0.;
+#pragma unroll
+		for (int k = 0; k < UNR; ++k) {
+			const int r = (rt0 + k) * TILE + lane;
+			if (rt0 + k < RT && r < R) {
+				bool kept = (r <= rstar) ? (v[k] > lo) : (dadd(v[k], thr) > m);
+				if (kept) {
+					s += exp(dmul(b, dsub(v[k], m)));
+					cnt++;
+				}
 			}
 		}
 	}
@@ -239,41 +260,50 @@ __global__ void __launch_bounds__(256) norm_kernel(
 
 	const double rescale = scalars[0], sf = sum_fact[d];
 	double ll = 0., pd = 0., inf = 0.;
-	double qn[MAX_MODES];
+	double qn[MULTI ? MAX_MODES : 1];
 #pragma unroll
-	for (int k = 0; k < MAX_MODES; ++k)
+	for (int k = 0; k < (MULTI ? MAX_MODES : 1); ++k)
 		qn[k] = 0.;
-	for (int rt = 0; rt < RT; ++rt) {
-		int r = rt * TILE + lane;
-		float out = 0.f;
-		if (r < R) {
-			double v = pv[rt * tstride];
-			bool kept = (r <= rstar) ? (v > lo) : (dadd(v, thr) > m);
-			if (kept) {
-				double P = exp(dmul(b, dsub(v, m))) / s;
-				ll += P * (v - sf);
-				if (psum_d_on)
-					pd += P * u[r] * rescale;
-				if (!(P < PROB_MIN)) {
-					double w = quats[(r / M) * 5 + 4];
-					inf += P * log(P / w * M);
-					if (M > 1) {
-						int mode = r % M;
+	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
+		double v[UNR];
 #pragma unroll
-						for (int k = 0; k < MAX_MODES; ++k)
-							if (k == mode)
-								qn[k] += P;
+		for (int k = 0; k < UNR; ++k)
+			v[k] = (rt0 + k < RT) ? pv[(rt0 + k) * tstride] : 0.;
+#pragma unroll
+		for (int k = 0; k < UNR; ++k) {
+			const int rt = rt0 + k;
+			if (rt >= RT)
+				break;
+			const int r = rt * TILE + lane;
+			float out = 0.f;
+			if (r < R) {
+				bool kept = (r <= rstar) ? (v[k] > lo) : (dadd(v[k], thr) > m);
+				if (kept) {
+					double P = exp(dmul(b, dsub(v[k], m))) / s;
+					ll += P * (v[k] - sf);
+					if (psum_d_on)
+						pd += P * u[r] * rescale;
+					if (!(P < PROB_MIN)) {
+						double w = quats[(r / M) * 5 + 4];
+						inf += P * log(P / w * M);
+						if (MULTI) {
+							int mode = r % M;
+#pragma unroll
+							for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
+								if (q == mode)
+									qn[q] += P;
+						}
 					}
+					out = (P > PROB_MIN) ? (float)P : -(float)P;
 				}
-				out = (P > PROB_MIN) ? (float)P : -(float)P;
 			}
+			ps[rt * tstride] = out;
 		}
-		ps[rt * tstride] = out;
 	}
 	ll = warp_sum(ll);
 	pd = warp_sum(pd);
 	inf = warp_sum(inf);
-	if (M > 1) {
+	if (MULTI) {
 		for (int k = 0; k < M && k < MAX_MODES; ++k) {
 			double v = warp_sum(qn[k]);
 			if (lane == 0)
@@ -375,14 +405,17 @@ __global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Ps
 // Block = orientation tile x PB pixels (same thread layout as slice_log_kernel).
 // The tile's tomogram rows are staged through shared memory; each
 // (pixel, orientation) with mask <= 1 and in bounds adds (f * w, f) to its 8
-// corners with float2 vector atomics (model.c:171-244, max_update.c:33-36).
+// corners (model.c:171-244, max_update.c:33-36). The accumulators are FP64
+// (model, weight) pairs, interleaved so both atomics of a corner hit one
+// 32-byte sector: FP32 sums of thousands of contributions per voxel would
+// carry ~1e-6 relative error into the next iteration's likelihoods.
 __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ psum_r,
                                                      const double *__restrict__ quats, int M, int R,
                                                      const double *__restrict__ qvals,
                                                      const double *__restrict__ corr,
                                                      const uint8_t *__restrict__ mask, int P, long long S,
-                                                     long long V, float2 *__restrict__ accum) {
+                                                     long long V, double *__restrict__ accum) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ double s_ps[TILE];
@@ -422,24 +455,26 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 		const double wv = ((double)s_tile[i][j] / ps) / cr;
 		double fw[8];
 		corner_weights(c, fw);
-		float2 *a = accum + (size_t)s_mode[j] * V + c.i000;
+		double *a = accum + 2 * ((size_t)s_mode[j] * V + c.i000);
 #pragma unroll
-		for (int q = 0; q < 8; ++q)
-			atomicAdd(a + o[q], make_float2((float)(fw[q] * wv), (float)fw[q]));
+		for (int q = 0; q < 8; ++q) {
+			atomicAdd(a + 2 * o[q], fw[q] * wv);
+			atomicAdd(a + 2 * o[q] + 1, fw[q]);
+		}
 	}
 }
 
 // ---------------------------------------------------------------------------
 // model update (recon.pyx:112-149) and small per-frame kernels
 // ---------------------------------------------------------------------------
-__global__ void unpack_accum_kernel(const float2 *__restrict__ accum, long long n, double *__restrict__ model2,
+__global__ void unpack_accum_kernel(const double2 *__restrict__ accum, long long n, double *__restrict__ model2,
                                     double *__restrict__ weight) {
 	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
-	float2 a = accum[i];
-	model2[i] = (double)a.x;
-	weight[i] = (double)a.y;
+	double2 a = accum[i];
+	model2[i] = a.x;
+	weight[i] = a.y;
 }
 
 __device__ __forceinline__ double friedel_avg(double a1, double w1, double a2, double w2) {

@@ -1,0 +1,302 @@
+"""State of an EMC reconstruction (mirror of dragonfly.iterate.Iterate,
+dragonfly/iterate.pyx:21-592).
+
+Holds the detector(s), the photon datasets, orientations, model, parameters
+and the per-frame arrays (fcounts, scale, beta, beta_start, sum_fact,
+blacklist) on the host; EMCRecon uploads them to the GPU. Supports one unique
+detector (the reference's multi-detector lists are not supported).
+"""
+import configparser
+import ctypes
+import ctypes.util
+import math
+import os.path as op
+import re
+
+import numpy as np
+
+from .detector import CDetector
+from .emcfile import CDataset
+from .model import Model
+from .params import MyConfigParser, EMCParams, RECON3D, RECON2D, RECONRZ
+from .quaternion import Quaternion
+
+try:
+    import h5py
+except ImportError:
+    h5py = None
+
+
+_libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+_libm.lgamma.restype = ctypes.c_double
+_libm.lgamma.argtypes = [ctypes.c_double]
+
+
+def ln_factorial(c):
+    """ln(c!) as the C library's lgamma(c + 1), which the device library and
+    the oracle also use (Python's math.lgamma rounds differently)."""
+    return _libm.lgamma(float(c) + 1.0)
+
+
+def frame_stats(dsets, mask):
+    """fcounts, sum_fact and mean_count over mask == 0 pixels (calc_frame_counts
+    and calc_sum_fact, dragonfly/src/iterate.c:3-117; ln c! = lgamma(c + 1))."""
+    fc, sf = [], []
+    for d in dsets:
+        n = d.num_data
+        good1 = mask[d.place_ones] < 1
+        good_m = mask[d.place_multi] < 1
+        fid1 = np.repeat(np.arange(n), d.ones)
+        fidm = np.repeat(np.arange(n), d.multi)
+        f = np.bincount(fid1[good1], minlength=n).astype(np.int64)
+        f += np.bincount(fidm[good_m], weights=d.count_multi[good_m], minlength=n).astype(np.int64)
+        lf = np.array([ln_factorial(c) for c in d.count_multi], np.float64)
+        s = np.zeros(n)
+        # sequential per-frame sums, in file order, as the reference adds them
+        for i in np.nonzero(good_m)[0]:
+            s[fidm[i]] += lf[i]
+        fc.append(f.astype(np.int32))
+        sf.append(s)
+    fcounts = np.concatenate(fc)
+    mean_count = float(np.cumsum(fcounts.astype(np.float64))[-1] / fcounts.size) if fcounts.size else 0.
+    return fcounts, np.concatenate(sf), mean_count
+
+
+class Iterate:
+    def __init__(self, config_fname="", section_name="emc", resume=False):
+        self.params = EMCParams()
+        self.dets = []
+        self.data = None
+        self.quat = None
+        self.model = None
+        self.tot_num_data = 0
+        self.num_blacklist = 0
+        self.fcounts = self.scale = self.bgscale = self.beta = self.beta_start = None
+        self.sum_fact = self.blacklist = None
+        self.mean_count = None
+        self.rescale = None
+        self.likelihood = 0.
+        self.mutual_info = 0.
+        self.rms_change = 0.
+        if config_fname != "":
+            self.from_config(config_fname, section_name, resume=resume)
+
+    # -- construction --------------------------------------------------------
+    def from_config(self, config_fname, section_name="emc", resume=False):
+        """iterate.pyx:40-182"""
+        param = EMCParams()
+        param.from_config(config_fname, section_name)
+        self.set_params(param)
+        rtype = {RECON3D: "3d", RECON2D: "2d", RECONRZ: "rz"}[param.rtype]
+        if rtype != "3d":
+            raise NotImplementedError("only 3-D reconstructions are supported")
+        print("Doing %s recon from %s" % (rtype.upper(), config_fname))
+        folder = op.dirname(config_fname)
+        config = MyConfigParser()
+        config.read(config_fname)
+
+        def chained(key):
+            v = config.get(section_name, key, fallback=None)
+            if v is not None and ":::" in v:
+                s, o = re.split(":::", v)
+                v = config.get(s, o)
+            return v
+
+        det_fname, det_flist = chained("in_detector_file"), chained("in_detector_list")
+        if det_fname is not None and det_flist is not None:
+            raise ValueError("Both in_detector_file and in_detector_list specified. Pick one.")
+        if det_flist is not None:
+            raise NotImplementedError("multiple detectors (in_detector_list) are not supported")
+        if det_fname is None:
+            raise ValueError("Need either in_detector_file or in_detector_list.")
+        det = CDetector(op.join(folder, det_fname), norm=True, rtype=rtype)
+
+        ph_fname, ph_flist = chained("in_photons_file"), chained("in_photons_list")
+        if ph_fname is not None and ph_flist is not None:
+            raise ValueError("Both in_photons_file and in_photons_list specified. Pick one.")
+        if ph_fname is not None:
+            frames = CDataset(op.join(folder, ph_fname), det)
+        elif ph_flist is not None:
+            with open(ph_flist) as f:
+                fnames = [op.join(folder, ln.strip()) for ln in f if ln.strip()]
+            frames = CDataset(fnames[0], det)
+            for fn in fnames[1:]:
+                frames.append(CDataset(fn, det))
+        else:
+            raise ValueError("Need either in_photons_file or in_photons_list.")
+        for key in ("background_file", "background_list"):
+            if config.get(section_name, key, fallback=None) is not None:
+                raise NotImplementedError("background-aware reconstruction is not supported")
+        self.dets = [det]
+        self.set_data(frames)
+
+        quat = Quaternion()
+        quat.from_config(config_fname, section_name)
+        self.set_quat(quat)
+
+        def fname_opt(key):
+            try:
+                return config.get_filename(section_name, key)
+            except configparser.NoOptionError:
+                return ""
+        model_file, scale_file = fname_opt("start_model_file"), fname_opt("scale_file")
+        if resume:
+            with open(param.log_fname) as f:
+                last_iter = int(f.readlines()[-1].split()[0])
+            self.params.start_iter = last_iter + 1
+            ext = ".h5" if h5py is not None else ".npz"
+            model_file = op.join(param.output_folder, "output_%.3d%s" % (last_iter, ext))
+            scale_file = model_file
+            print("Resuming from iteration", self.params.start_iter)
+
+        model = Model(self.calculate_size(det.qmax()), param.num_modes, rtype)
+        model_mean = self.mean_count[0] / (det.raw_mask == 0).sum() * 2.
+        model.allocate(model_file, model_mean, fixed_seed=bool(param.fixed_seed))
+        self.set_model(model)
+        if param.need_scaling == 1:
+            self.parse_scale(scale_file)
+        sel_string = config.get(section_name, "selection", fallback=None)
+        self.parse_blacklist(fname_opt("blacklist_file"), sel_string)
+        beta_str = config.get(section_name, "beta", fallback="auto")
+        self.calc_beta() if beta_str == "auto" else self.calc_beta(float(beta_str))
+
+    def set_model(self, model):
+        self.model = model
+
+    def set_quat(self, quat):
+        self.quat = quat
+
+    def set_params(self, param):
+        self.params = param
+
+    def set_data(self, in_dset):
+        """iterate.pyx:241-266"""
+        if self.tot_num_data != 0:
+            raise ValueError("Please use update_data() to change dataset")
+        self._attach(in_dset)
+
+    def update_data(self, in_dset):
+        self._attach(in_dset)
+        if self.params.need_scaling == 1:
+            self.parse_scale("")
+        self.calc_beta()
+
+    def _attach(self, in_dset):
+        self.data = in_dset
+        dsets = list(in_dset)
+        if not self.dets:
+            self.dets = [in_dset.det]
+        for d in dsets:
+            if d.det is not None and d.det is not self.dets[0] and d.det.num_pix != self.dets[0].num_pix:
+                raise NotImplementedError("multiple detectors are not supported")
+        self.tot_num_data = sum(d.num_data for d in dsets)
+        fc, sf, mc = frame_stats(dsets, self.dets[0].raw_mask)
+        self.fcounts, self.sum_fact = fc, sf
+        self.mean_count = np.array([mc])
+        self.rescale = np.zeros(1)
+        self.blacklist = np.zeros(self.tot_num_data, np.uint8)
+
+    def merged_frames(self):
+        """The linked datasets as one set of sparse arrays."""
+        ds = list(self.data)
+        cat = lambda k: np.concatenate([getattr(d, k) for d in ds]).astype(np.int32)
+        return tuple(cat(k) for k in ("ones", "multi", "place_ones", "place_multi", "count_multi"))
+
+    # -- per-frame parameters -------------------------------------------------
+    def parse_scale(self, fname, bg=False):
+        """iterate.pyx:284-315"""
+        if bg:
+            raise NotImplementedError("background scale factors are not supported")
+        if not fname or not op.isfile(fname):
+            if self.tot_num_data == 0:
+                raise AttributeError("Need tot_num_data to initialize scale factors")
+            scale = np.ones(self.tot_num_data)
+        elif fname.endswith(".npz") or h5py is None:
+            scale = np.load(fname)["scale"]
+        else:
+            with h5py.File(fname, "r") as f:
+                scale = f["scale"][:]
+        scale = np.asarray(scale, np.float64)
+        if self.tot_num_data == 0:
+            self.tot_num_data = scale.shape[0]
+        elif self.tot_num_data < scale.shape[0]:
+            print("More scale factors than required. Taking only first", self.tot_num_data)
+            scale = scale[:self.tot_num_data]
+        elif self.tot_num_data > scale.shape[0]:
+            print("Insufficient scale factors in file. Setting rest to unity")
+            scale = np.append(scale, np.ones(self.tot_num_data - scale.shape[0]))
+        self.scale = scale.copy()
+
+    def parse_blacklist(self, fname, sel_string=None, refresh=False):
+        """iterate.pyx:317-359 (num_blacklist is left at 0, as there)."""
+        if self.tot_num_data == 0:
+            raise AttributeError("Need to define tot_num_data before generating blacklist")
+        if self.blacklist is None or refresh:
+            self.blacklist = np.zeros(self.tot_num_data, np.uint8)
+        if fname and op.isfile(fname):
+            arr = np.loadtxt(fname, dtype="u1")
+            if arr.shape[0] != self.tot_num_data:
+                raise ValueError("Mismatched number of frames in blacklist file")
+            self.blacklist[:] = arr
+        if sel_string is None:
+            return
+        if sel_string == "odd_only":
+            curr = 0
+        elif sel_string == "even_only":
+            curr = 1
+        else:
+            raise ValueError("Unrecognized sel_string, %s" % sel_string)
+        for d in range(self.tot_num_data):
+            if self.blacklist[d] == 0:
+                self.blacklist[d] = curr
+                curr = 1 - curr
+
+    def calc_beta(self, setval=None):
+        """iterate.pyx:386-402 -> iterate.c:66-83"""
+        if self.data is None:
+            raise AttributeError("Add data first before calculating beta for each frame")
+        start = -1. if setval is None else float(setval)
+        if not self.params.need_scaling and start < 0:
+            start = math.exp(-6.5 * math.pow(self.mean_count[0] * 1.e-5, 0.15))
+        if start > 0:
+            self.beta_start = np.full(self.tot_num_data, start)
+        else:
+            self.beta_start = np.array([math.exp(-6.5 * math.pow(f * 1.e-5, 0.15)) for f in self.fcounts])
+        self.beta = self.beta_start.copy()
+
+    def normalize_scale(self):
+        """iterate.pyx:361-384"""
+        blist = self.blacklist
+        mean_scale = self.scale.mean() if blist is None else self.scale[blist == 0].mean()
+        if self.model is not None and self.model.model1 is not None:
+            self.model.model1.reshape(-1)[:self.model.vol] *= mean_scale
+        if blist is None:
+            self.scale /= mean_scale
+        else:
+            self.scale[blist == 0] /= mean_scale
+        self.rms_change *= mean_scale
+        return mean_scale
+
+    def free(self):
+        pass
+
+    @staticmethod
+    def calculate_size(qmax):
+        """iterate.pyx:458-468"""
+        return int(2 * np.ceil(qmax) + 3)
+
+    @property
+    def det(self):
+        return self.dets[0] if self.dets else None
+
+    @property
+    def num_det(self):
+        return len(self.dets)
+
+    @property
+    def num_dfiles(self):
+        return 0 if self.data is None else len(list(self.data))
+
+    @property
+    def det_mapping(self):
+        return np.zeros(self.num_dfiles, np.int32)

@@ -1,0 +1,135 @@
+"""Orientation sets (mirror of dragonfly.quaternion.Quaternion,
+dragonfly/quaternion.pyx:25-342). Quaternions are rows (q0, q1, q2, q3, w)
+with weights summing to one; generate_3d uses the 600-cell refinement of
+quatgen.py, identical to the reference's quat_gen."""
+import configparser
+import os.path as op
+import sys
+
+import numpy as np
+
+from .quatgen import quat_gen
+
+try:
+    import h5py
+except ImportError:
+    h5py = None
+
+
+class Quaternion:
+    def __init__(self, num_div=0, num_rot=0, point_group=""):
+        self.octahedral_flag = point_group == "S4"
+        self.icosahedral_flag = point_group == "A5"
+        self.num_rot_p = 0
+        self.num_div = 0
+        self._quats = None
+        self.reduced = False
+        self.quat_mapping = None
+        if num_div > 0 and num_rot > 0:
+            raise ValueError("Cannot specify both num_div and num_rot")
+        elif num_div > 0:
+            self.generate_3d(num_div)
+        elif num_rot > 0:
+            self.generate_2d(num_rot, point_group)
+
+    def from_config(self, config_fname, section_name="emc"):
+        config = configparser.ConfigParser()
+        config.read(config_fname)
+        rtype = config.get(section_name, "recon_type", fallback="3d").lower()
+        if rtype == "2d":
+            num_rot = config.getint(section_name, "num_rot")
+            friedel = config.getboolean(section_name, "friedel_sym", fallback=False)
+            self.generate_2d(num_rot, "2" if friedel else "1")
+        elif rtype == "3d":
+            num_div = config.get(section_name, "num_div", fallback="0").split()
+            self.generate_3d(int(num_div[0]))
+            if len(num_div) == 2:
+                self.voronoi_subset(int(num_div[1]))
+            point_group = config.get(section_name, "point_group", fallback="1")
+            if point_group in ("A5", "S4"):
+                raise NotImplementedError("point-group reduction (%s) is not supported" % point_group)
+            elif point_group != "1":
+                raise ValueError("Unknown point group: " + point_group)
+
+    def generate_3d(self, num_div):
+        self.num_div = int(num_div)
+        self.reduced = False
+        self._quats = quat_gen(num_div)
+
+    def generate_2d(self, num_rot, point_group):
+        if point_group == "":
+            point_group = "1"
+        max_angle = 2 * np.pi / int(point_group)
+        q = np.zeros((num_rot, 5))
+        q[:, 0] = np.arange(0, max_angle, max_angle / num_rot)[:num_rot]
+        q[:, 4] = 1. / num_rot
+        self._quats = q
+
+    def save(self, fname):
+        if self._quats is None:
+            raise AttributeError("Generate quaternion first before saving")
+        if h5py is None or fname.endswith(".npz"):
+            np.savez(fname, quaternions=self._quats)
+        else:
+            with h5py.File(fname, "w") as f:
+                f["quaternions"] = self._quats
+
+    def parse(self, fname):
+        if h5py is None or fname.endswith(".npz"):
+            quats = np.load(fname)["quaternions"]
+        else:
+            with h5py.File(fname, "r") as f:
+                quats = f["quaternions"][:]
+        quats = np.asarray(quats, np.float64)
+        if quats.shape[1] == 4:
+            quats = np.pad(quats, ((0, 0), (0, 1)), constant_values=1. / quats.shape[0])
+        elif quats.shape[1] == 5:
+            quats = quats.copy()
+            quats[:, 4] /= quats[:, 4].sum()
+        else:
+            raise ValueError("Need 4- or 5-dimensional quaternions")
+        self._quats = np.ascontiguousarray(quats)
+
+    def divide(self, rank, num_proc, num_modes=1, num_nonrot_modes=0):
+        """Orientations handled by one rank (quaternion.pyx:156-175)."""
+        tot = num_modes * self.num_rot + num_nonrot_modes
+        self.num_rot_p = tot // num_proc + (1 if rank < tot % num_proc else 0)
+        if num_proc > 1:
+            sys.stderr.write("%d: num_rot_p = %d/%d\n" % (rank, self.num_rot_p, tot))
+        return self.num_rot_p
+
+    def voronoi_subset(self, coarse_div):
+        """Nearest coarse orientation of every fine one, by 1 - (q.q')^2
+        (voronoi_subset, quaternion.c:844-862); ties keep the first."""
+        coarse = quat_gen(coarse_div)
+        q = self._quats[:, :4]
+        out = np.empty(q.shape[0], np.int64)
+        for s in range(0, q.shape[0], 4096):
+            dist = 1. - (q[s:s + 4096] @ coarse[:, :4].T) ** 2
+            out[s:s + 4096] = np.argmin(dist, axis=1)
+        self.quat_mapping = out
+        return out
+
+    def reduce_icosahedral(self, return_sym=False):
+        raise NotImplementedError("point-group reduction is not supported")
+
+    def reduce_octahedral(self, return_sym=False):
+        raise NotImplementedError("point-group reduction is not supported")
+
+    def free(self):
+        self._quats = None
+
+    @property
+    def num_rot(self):
+        return 0 if self._quats is None else int(self._quats.shape[0])
+
+    @property
+    def quats(self):
+        return self._quats
+
+    @quats.setter
+    def quats(self, arr):
+        arr = np.asarray(arr, np.float64)
+        if arr.ndim != 2 or arr.shape[1] != 5:
+            raise ValueError("quats must be [num_rot, 5]")
+        self._quats = np.ascontiguousarray(arr).copy()

@@ -1,0 +1,332 @@
+"""EMC reconstruction driver (mirror of dragonfly.recon, dragonfly/recon.pyx).
+
+EMCRecon keeps the reference's interface -- set_iterate, run_iteration,
+update_model, update_beta, save_output, save_initial_model and the read-only
+result properties -- but the iteration runs on one GPU through the C ABI of
+libdfgpu.so (include/dragonfly_b200.h). The Iterate's host arrays stay the
+source of truth between iterations: run_iteration uploads model1 and the
+per-frame parameters, runs the iteration on the device and writes model1,
+model2, inter_weight, scale and beta back, so code that edits them between
+iterations keeps working as with the reference.
+
+Outputs: output_%03d.h5 with the reference's keys when h5py is importable,
+otherwise output_%03d.npz with the same keys; the EMC.log format is the
+reference's (recon.pyx:182-228).
+"""
+import os
+import time
+
+import numpy as np
+
+from .iterate import Iterate
+from .params import RECON3D
+
+try:
+    import h5py
+except ImportError:
+    h5py = None
+
+
+class EMCRecon:
+    """Runs EMC iterations on the GPU (recon.pyx:19-415).
+
+    Args:
+        num_threads (int): accepted for interface compatibility; the GPU path
+            does not use host threads.
+        device (int): CUDA device (default: LOCAL_RANK or 0).
+    """
+
+    def __init__(self, num_threads=-1, device=None):
+        self.num_threads = num_threads if num_threads > 0 else (os.cpu_count() or 1)
+        self.device = int(os.environ.get("LOCAL_RANK", "0")) if device is None else device
+        self.ctx = None
+        self._iter = None
+        self.refinement = 0
+        self.within_openmp = 0
+        self._results = {}
+
+    # -- setup ---------------------------------------------------------------
+    def set_iterate(self, itr):
+        """Uploads the detector, frames, orientations and model (recon.pyx:48-70)."""
+        if itr.data is None:
+            print("Set data for iterate first")
+            return
+        if itr.model is None:
+            print("Set model for iterate first")
+            return
+        if itr.quat is None:
+            print("Set quat for iterate first")
+            return
+        if itr.params.rtype != RECON3D or itr.model.mtype != "MODEL_3D":
+            raise NotImplementedError("only 3-D reconstructions are supported")
+        if itr.params.nonrot_modes:
+            raise NotImplementedError("non-rotating modes are not supported")
+        if itr.params.refine:
+            raise NotImplementedError("orientation refinement is not supported")
+        if itr.params.axial_sym > 1 or getattr(itr.quat, "icosahedral_flag", False) or \
+                getattr(itr.quat, "octahedral_flag", False):
+            raise NotImplementedError("point-group and axial symmetrisation are not supported")
+        if itr.dets[0].with_bg and itr.params.need_scaling:
+            raise NotImplementedError("background-aware updates are not supported")
+        from ._lib import Context
+        if self.ctx is None:
+            self.ctx = Context(self.device)
+        c = self.ctx
+        det = itr.dets[0]
+        c.set_detector(det.qvals, det.corr, det.raw_mask)
+        c.set_frames(*itr.merged_frames())
+        c.set_quaternions(itr.quat.quats)
+        c.set_model(itr.model.model1)
+        itr.quat.divide(0, 1, itr.params.num_modes, itr.params.nonrot_modes)
+        itr.params.rank, itr.params.num_proc = 0, 1
+        self._iter = itr
+
+    # -- one iteration ---------------------------------------------------------
+    def run_iteration(self, dynamic=False):
+        """update_beta, maximize, update_model, normalize_scale, output
+        (recon.pyx:72-110)."""
+        itr = self._iter
+        if itr is None:
+            print("Set iterate first")
+            return
+        par = itr.params
+        stime = time.time()
+        if par.iteration == 1:
+            self.write_log_file_header()
+        c = self.ctx
+        c.set_model(itr.model.model1)
+        c.set_blacklist(itr.blacklist)
+        c.set_beta_start(itr.beta_start)
+        if par.need_scaling:
+            c.set_scale(itr.scale)
+        beta_mean = self.update_beta()
+        p = c.params(par.iteration, par.need_scaling, par.update_scale, par.known_scale, par.beta_jump,
+                     par.beta_period, par.beta_factor)
+        likelihood = c.maximize(p)
+        self.update_model()
+        if par.need_scaling == 1:
+            itr.normalize_scale()
+        fp = c.frame_params()
+        itr.beta[itr.blacklist == 0] = fp["beta"][itr.blacklist == 0]
+        sc = c.scalars()
+        itr.rescale[0] = sc["rescale"]
+        itr.mutual_info = sc["mutual_info"]
+        itr.likelihood = likelihood
+        self._results = {}
+        if par.rank == 0:
+            self.save_output(dynamic)
+            self.update_log_file(likelihood, beta_mean, time.time() - stime)
+        if par.verbosity > 0:
+            print("Finished iteration", par.iteration, "(%e)" % itr.rms_change)
+        return likelihood
+
+    def update_model(self):
+        """Friedel-symmetrise, divide, rms change, model1 <- model2
+        (recon.pyx:112-149), on the device; results copied to the Iterate.
+        When need_scaling, the scale update of maximize is copied too."""
+        itr = self._iter
+        c = self.ctx
+        itr.rms_change = c.update_model(itr.params.alpha)
+        m1, m2, w = c.model()
+        itr.model.model1 = m1
+        itr.model.model2 = m2
+        itr.model.inter_weight = w
+        if itr.params.need_scaling:
+            itr.scale = c.frame_params()["scale"]
+
+    def update_beta(self):
+        """Mean of beta_d = min(1, beta_start_d * factor) over good frames
+        (recon.pyx:151-174); the device applies the same rule in maximize."""
+        itr = self._iter
+        par = itr.params
+        factor = par.beta_jump ** ((par.iteration - 1) // par.beta_period)
+        factor *= par.beta_factor
+        print("beta factor =", factor)
+        good = itr.blacklist != 1
+        beta = np.minimum(itr.beta_start[good] * factor, 1.)
+        return float(beta.sum() / (itr.tot_num_data - itr.num_blacklist))
+
+    def free(self):
+        if self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None
+
+    # -- output ----------------------------------------------------------------
+    def write_log_file_header(self):
+        itr = self._iter
+        par = itr.params
+        d = os.path.dirname(par.log_fname)
+        if d and not os.path.exists(d):
+            os.makedirs(d)
+        with open(par.log_fname, "w") as fp:
+            fp.write("Cryptotomography with the EMC algorithm using MPI+OpenMP\n\n")
+            fp.write("Data parameters:\n")
+            fp.write("\tnum_data = %d\n\tmean_count = %f\n\n" % (itr.tot_num_data, itr.mean_count[0]))
+            fp.write("System size:\n")
+            fp.write("\tnum_rot = %d\n\tnum_pix = %d/%d\n\t" % (itr.quat.num_rot, (itr.dets[0].raw_mask == 0).sum(),
+                                                            itr.dets[0].num_pix))
+            m = itr.model
+            fp.write("system_volume = %d X %ld X %ld X %ld\n\n" % (m.num_modes, m.size, m.size, m.size))
+            fp.write("Reconstruction parameters:\n")
+            fp.write("\tnum_threads = %d\n\tnum_proc = %d\n\talpha = %.6f\n\tbeta = %.6f\n\tneed_scaling = %s"
+                     % (self.num_threads, par.num_proc, par.alpha, itr.beta_start[0],
+                        "yes" if par.need_scaling == 1 else "no"))
+            fp.write("\n\nIter\ttime\trms_change\tinfo_rate\tlog-likelihood\tnum_rot\tbeta\n")
+
+    def update_log_file(self, likelihood, beta, iter_time):
+        itr = self._iter
+        with open(itr.params.log_fname, "a") as fp:
+            fp.write("%d\t" % itr.params.iteration)
+            fp.write("%4.2f\t" % iter_time)
+            fp.write("%1.4e\t%f\t%.6e\t%-7d\t%f\n" % (itr.rms_change, itr.mutual_info, likelihood,
+                                                     itr.quat.num_rot, beta))
+
+    def _output_dict(self):
+        itr = self._iter
+        par = itr.params
+        out = {}
+        for k, v in vars(par).items():
+            if not k.startswith("_") and not callable(v):
+                out["params/" + k] = v
+        out["params/mtype"] = itr.model.mtype
+        out["params/num_rot"] = itr.quat.num_rot
+        out["params/num_div"] = itr.quat.num_div
+        out["orientations"] = self.rmax
+        out["mutual_info"] = self.info
+        out["likelihood"] = self.likelihood
+        if itr.model.num_modes > 1:
+            out["occupancies"] = self.quat_norm
+        out["intens"] = itr.model.model1
+        out["inter_weight"] = itr.model.inter_weight
+        if par.need_scaling != 0:
+            out["scale"] = itr.scale
+        out["quaternions"] = itr.quat.quats
+        return out
+
+    def _write(self, fname_noext, d):
+        if h5py is not None:
+            with h5py.File(fname_noext + ".h5", "w") as f:
+                for k, v in d.items():
+                    f[k] = v
+        else:
+            np.savez(fname_noext + ".npz", **{k.replace("/", "__"): np.asarray(v) for k, v in d.items()})
+
+    def save_output(self, dynamic=False):
+        par = self._iter.params
+        if not os.path.exists(par.output_folder):
+            os.makedirs(par.output_folder)
+        name = "output_dynamic" if dynamic else "output_%.3d" % par.iteration
+        self._write(os.path.join(par.output_folder, name), self._output_dict())
+
+    def save_initial_model(self):
+        itr = self._iter
+        par = itr.params
+        if not os.path.exists(par.output_folder):
+            os.makedirs(par.output_folder)
+        d = {"intens": itr.model.model1}
+        if par.need_scaling != 0:
+            d["scale"] = itr.scale
+        self._write(os.path.join(par.output_folder, "output_000"), d)
+
+    # -- results ---------------------------------------------------------------
+    def _frame(self, key):
+        if key not in self._results:
+            self._results.update(self.ctx.frame_results())
+        return self._results[key]
+
+    @property
+    def iter(self):
+        return self._iter
+
+    @property
+    def rmax(self):
+        return self._frame("rmax")
+
+    @property
+    def info(self):
+        return self._frame("info")
+
+    @property
+    def likelihood(self):
+        return self._frame("likelihood")
+
+    @property
+    def max_exp(self):
+        return self._frame("max_exp")
+
+    @property
+    def p_norm(self):
+        return self._frame("p_norm")
+
+    @property
+    def psum_d(self):
+        return self._frame("psum_d")
+
+    @property
+    def max_exp_p(self):
+        return self._frame("max_exp")
+
+    @property
+    def quat_norm(self):
+        return self.ctx.quat_norm()
+
+    @property
+    def num_prob(self):
+        return self.ctx.num_prob()
+
+    @property
+    def u(self):
+        return [self.ctx.orientation_results()[0]]
+
+    @property
+    def psum_r(self):
+        return self.ctx.orientation_results()[1]
+
+    @property
+    def model(self):
+        return self._iter.model.model2
+
+    @property
+    def weight(self):
+        return self._iter.model.inter_weight
+
+    @property
+    def all_views(self):
+        return None
+
+    @property
+    def prob(self):
+        return None
+
+    @property
+    def place_prob(self):
+        return None
+
+
+def main():
+    """Command line: dragonfly_b200.recon niter [-c config] [-r] [-t threads]
+    (recon.pyx:418-445)."""
+    import argparse
+    parser = argparse.ArgumentParser(description="Cryptotomography with the EMC algorithm on a B200 GPU")
+    parser.add_argument("niter", help="Number of iterations", type=int)
+    parser.add_argument("-c", "--config_file", help="Path to configuration file. Default: config.ini",
+                        default="config.ini")
+    parser.add_argument("-r", "--resume", help="Whether to resume from last iteration", action="store_true")
+    parser.add_argument("-t", "--threads", help="Accepted for compatibility", type=int, default=-1)
+    args = parser.parse_args()
+    recon = EMCRecon(args.threads)
+    itr = Iterate(args.config_file, resume=args.resume)
+    itr.params.num_iter = args.niter
+    recon.set_iterate(itr)
+    st = itr.params.start_iter
+    en = st + itr.params.num_iter
+    if st == 1:
+        recon.save_initial_model()
+    for itr.params.iteration in range(st, en):
+        recon.run_iteration()
+    if itr.params.verbosity > 0:
+        print("Finished all iterations")
+
+
+if __name__ == "__main__":
+    main()

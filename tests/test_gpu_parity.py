@@ -29,12 +29,15 @@ def test_gpu_matches_oracle_on_golden_cases(name, oracle_built):
         assert np.mean(a["rmax"][good] == g[k + "rmax"][good]) >= 0.999
         assert np.all(a["rmax"][~good] == -1)
         assert abs(a["avg_likelihood"] - g[k + "scalars"][0]) <= 1e-6 * abs(g[k + "scalars"][0])
-        # u_r and the rescale factor are sums of FP64 slices: exact up to
-        # summation order on the shared start model; afterwards the model
-        # carries the FP32 merge accumulation (within the model tolerance)
-        tol = 1e-12 if it == 1 else 1e-5
-        np.testing.assert_allclose(a["u"], b["u"], rtol=tol)
-        assert abs(a["rescale"] - b["rescale"]) <= tol * abs(b["rescale"])
+        # u_r and the rescale factor are FP64 sums in the reference's order:
+        # bit-identical on the shared start model; afterwards the models differ
+        # within the model tolerance
+        if it == 1:
+            np.testing.assert_array_equal(a["u"], b["u"])
+            assert a["rescale"] == b["rescale"]
+        else:
+            np.testing.assert_allclose(a["u"], b["u"], rtol=1e-6)
+            assert abs(a["rescale"] - b["rescale"]) <= 1e-6 * abs(b["rescale"])
         # kept-set sizes: the pruning rule of max_prob.c:184-203
         assert np.mean(a["num_prob"] == b["num_prob"]) >= 0.999
         if prob.num_modes > 1:
@@ -70,7 +73,6 @@ def test_gpu_frame_chunks_agree(oracle_built):
     prob, _ = load_case("scaling")
     one = GPUEngine(prob)
     many = GPUEngine(prob, pair_budget_mb=0.05)
-    assert many.ctx.workload()["chunks"] == 1 or True
     for it in (1, 2):
         a = one.run_iteration(it)
         b = many.run_iteration(it)

@@ -1,0 +1,65 @@
+"""The reference-facing Python API end to end on the GPU: a config file,
+Iterate, EMCRecon.run_iteration (recon.pyx:72-110), outputs and the log,
+checked against the oracle on the same inputs."""
+import os
+
+import numpy as np
+import pytest
+
+from common import MODEL_REL_L2, SCALAR_REL, rel, rel_l2
+from oracle.oracle import EMCProblem, OracleEngine
+from test_api_host import write_problem
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("need_scaling", [0, 1])
+def test_emcrecon_run_iteration_matches_oracle(tmp_path, need_scaling, oracle_built):
+    from dragonfly_b200 import Iterate
+    from dragonfly_b200.recon import EMCRecon
+    d, cfg = write_problem(tmp_path, need_scaling=need_scaling, extra="update_scale = 1\n")
+    itr = Iterate(cfg)
+    start = itr.model.model1.copy()
+    recon = EMCRecon()
+    recon.set_iterate(itr)
+    recon.save_initial_model()
+
+    prob = EMCProblem(itr.dets[0].qvals, itr.dets[0].corr, itr.dets[0].raw_mask, d["ones"], d["multi"],
+                      d["place_ones"], d["place_multi"], d["count_multi"], itr.quat.quats, start,
+                      need_scaling=need_scaling, update_scale=1, beta=0.5, beta_jump=2., beta_period=3)
+    orc = OracleEngine(prob)
+    for it in (1, 2, 3, 4):
+        itr.params.iteration = it
+        ll = recon.run_iteration()
+        b = orc.run_iteration(it)
+        assert rel_l2(itr.model.model1, b["model1"]) <= MODEL_REL_L2
+        assert rel(ll, b["avg_likelihood"]) <= SCALAR_REL
+        assert rel(itr.mutual_info, b["mutual_info"]) <= SCALAR_REL
+        assert np.mean(recon.rmax == b["rmax"]) >= 0.999
+        np.testing.assert_allclose(itr.beta, b["beta"], rtol=0)
+        if need_scaling:
+            np.testing.assert_allclose(itr.scale, b["scale"], rtol=1e-6)
+        assert abs(itr.rms_change - b["rms_change"]) <= 1e-5 * abs(b["rms_change"])
+    out = itr.params.output_folder
+    names = sorted(os.listdir(out))
+    assert any(n.startswith("output_000") for n in names) and any(n.startswith("output_004") for n in names)
+    log = open(itr.params.log_fname).read().splitlines()
+    assert log[-1].split()[0] == "4" and "num_rot = 420" in "\n".join(log)
+    recon.free()
+
+
+def test_model_slice_api_on_gpu(oracle_built):
+    from common import load_case
+    from dragonfly_b200 import CDetector, Model
+    prob, _ = load_case("beta1")
+    det = CDetector()
+    det.qvals, det.corr, det.raw_mask = prob.qvals, prob.corr, prob.mask
+    m = Model(prob.size)
+    m.model1 = prob.model1.copy()
+    m.model2 = np.zeros_like(m.model1)
+    m.inter_weight = np.zeros_like(m.model1)
+    orc = OracleEngine(prob)
+    s = m.slice_gen(prob.quats[3], det)
+    np.testing.assert_array_equal(s, orc.slice_gen(prob.quats[3]))
+    m.slice_merge(prob.quats[3], s, det)
+    assert m.inter_weight.sum() > 0
