@@ -61,6 +61,7 @@ _SIGS = {
     "dfg_get_num_prob": (C.c_int, [_V, _I]),
     "dfg_slice_gen": (C.c_int, [_V, _D, C.c_int, _D]),
     "dfg_slice_merge": (C.c_int, [_V, _D, C.c_int, _D, _D, _D]),
+    "dfg_slice_gen_noalloc": (C.c_int, [_V, _D, C.c_int, _D]),
     "dfg_run_iteration_host": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D, _I, _D, _D, _D]),
     "dfg_set_option": (C.c_int, [_V, C.c_char_p, C.c_double]),
     "dfg_get_phase_times": (C.c_int, [_V, _D, C.POINTER(C.c_long), C.c_int]),
@@ -267,6 +268,16 @@ class Context:
             q = np.append(q, 1.)
         out = np.zeros(self.num_pix)
         self.call("dfg_slice_gen", ptr(q, C.c_double), int(mode), ptr(out, C.c_double))
+        return out
+
+    def slice_gen_noalloc(self, quat, mode=0):
+        """slice_gen through the entry point that allocates no device memory
+        (its scratch is a fixed device array of DFG_NOALLOC_MAX_PIXELS)."""
+        q = np.ascontiguousarray(quat, np.float64)
+        if q.size == 4:
+            q = np.append(q, 1.)
+        out = np.zeros(self.num_pix)
+        self.call("dfg_slice_gen_noalloc", ptr(q, C.c_double), int(mode), ptr(out, C.c_double))
         return out
 
     def slice_merge(self, quat, view, model2, inter_weight, mode=0):

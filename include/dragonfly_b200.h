@@ -134,6 +134,19 @@ DFG_API int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double *ou
 DFG_API int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const double *view,
                     double *model2, double *inter_weight);
 
+/* dfg_slice_gen without any device allocation. No counterpart in the
+ * reference: it is for callers that cannot allocate device memory while they
+ * run -- an application whose own pool allocator owns the device memory
+ * budget, or a real-time loop where a cudaMalloc / cudaFree would synchronise
+ * the device. The scratch (quaternion and output slice) is a fixed file-scope
+ * device array of DFG_NOALLOC_MAX_PIXELS doubles (2 MiB plus 64 bytes) that
+ * each GPU loading the library holds until exit; detectors with more pixels
+ * are rejected with DFG_ERR_ARG. The first call on a device looks the array's
+ * address up (make it before any stream capture). All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+#define DFG_NOALLOC_MAX_PIXELS 262144
+DFG_API int dfg_slice_gen_noalloc(dfg_ctx *ctx, const double *quat, int mode, double *out);
+
 /* ---- end to end from host buffers ----------------------------------------
  * EMCRecon.run_iteration's compute (recon.pyx:93-104): model1_inout (host,
  * [modes][size^3]) is uploaded, maximize + update_model (+ normalize_scale
