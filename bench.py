@@ -129,6 +129,18 @@ def roofline_traffic(kernel, units):
         return None
 
 
+def max_over_ranks(x, world, device):
+    """Maximum of a per-rank number over all ranks (the slowest replica sets
+    the job time). device: where the collective's tensor lives ("cpu" for
+    gloo, "cuda:i" for nccl)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------
 # reference engine on the host cores
 # ---------------------------------------------------------------------------
@@ -247,10 +259,7 @@ def run_ours(args, rank, world, local_rank):
     launches = ctx.workload()["launches"] - launches0
     phases = ctx.phase_times()
     ctx.set_option("timing", 0)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda:%d" % local_rank, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world, "cuda:%d" % local_rank)
     ms_per_step = total_ms / args.steps
     value = world * R * N / (ms_per_step / 1e3)
 
@@ -268,11 +277,7 @@ def run_ours(args, rank, world, local_rank):
         ctx.run_iteration_host(params(it), model_h, 0., rmax_h, ll_h)
         e2e.append(time.perf_counter() - t0)
         it += 1
-    e2e_s = float(np.mean(e2e))
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda:%d" % local_rank, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(float(np.mean(e2e)), world, "cuda:%d" % local_rank)
 
     # roofline of the dominant kernel (per-launch CUDA-event durations)
     dom = max(phases, key=lambda k: phases[k][0])

@@ -88,11 +88,12 @@ extern "C" int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, 
 	if (!ctx)
 		return DFG_ERR_ARG;
 	NEED(num_pix > 0 && qvals && corr && raw_mask, DFG_ERR_ARG, "detector: need num_pix > 0 and arrays");
-	NEED((uint32_t)num_pix <= IDX_MASK + 1u, DFG_ERR_ARG, "detector: at most %u pixels", IDX_MASK + 1u);
+	NEED((uint32_t)num_pix <= IDX_MASK, DFG_ERR_ARG, "detector: at most %u pixels", IDX_MASK);
 	for (long long i = 0; i < 3LL * num_pix; ++i)
 		NEED(std::isfinite(qvals[i]), DFG_ERR_ARG, "detector: qvals[%lld] is not finite", i);
 	for (int i = 0; i < num_pix; ++i)
 		NEED(std::isfinite(corr[i]), DFG_ERR_ARG, "detector: corr[%d] is not finite", i);
+	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
 	if (ctx->P != 0 && ctx->P != num_pix)
 		ctx->chunks_R = -1;
@@ -101,6 +102,15 @@ extern "C" int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, 
 	CK(upload(ctx->qvals, qvals, 3 * (size_t)num_pix, ctx->stream));
 	CK(upload(ctx->corr, corr, (size_t)num_pix, ctx->stream));
 	CK(upload(ctx->mask, raw_mask, (size_t)num_pix, ctx->stream));
+	{
+		std::vector<double4> g;
+		for (int t = 0; t < num_pix; ++t)
+			if (raw_mask[t] < 1)
+				g.push_back(make_double4(qvals[3 * (size_t)t], qvals[3 * (size_t)t + 1], qvals[3 * (size_t)t + 2],
+				                         corr[t]));
+		ctx->n_good = (int)g.size();
+		CK(upload(ctx->good, g.data(), g.size(), ctx->stream));
+	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->chunks_R = -1;  // photon lists depend on the mask
 	if (ctx->N > 0) {
@@ -119,6 +129,13 @@ static inline void push_word(std::vector<uint32_t> &v, uint32_t idx, long long c
 		v.push_back(idx | (c << IDX_BITS));
 		count -= c;
 	}
+}
+
+// Pads a segment that started at `start` to a multiple of 8 words with `pad`
+// (an index whose row is all zero, count 0).
+static inline void pad8(std::vector<uint32_t> &v, size_t start, uint32_t pad) {
+	while ((v.size() - start) % 8)
+		v.push_back(pad);
 }
 
 extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const int *multi,
@@ -162,35 +179,46 @@ extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const
 	// fcounts, sum_fact, mean_count as calc_frame_counts / calc_sum_fact
 	// (iterate.c:3-117).
 	const uint8_t *mk = ctx->h_mask.data();
+	const uint32_t pad = (uint32_t)P;  // zero row of logW
 	std::vector<uint32_t> words;
-	words.reserve((size_t)(oo[N] + mo[N]));
-	std::vector<long long> off(N + 1, 0);
+	words.reserve((size_t)(oo[N] + mo[N] + 16 * (size_t)N));
+	std::vector<long long> off(N + 1, 0), midv(N, 0);
 	std::vector<int> fc(N, 0);
 	std::vector<double> sf(N, 0.);
 	double mc = 0.;
+	long long real = 0;
 	for (int d = 0; d < N; ++d) {
+		size_t st = words.size();
 		for (long long i = oo[d]; i < oo[d + 1]; ++i) {
 			int p = ctx->h_place_ones[i];
 			if (mk[p] < 1) {
-				push_word(words, (uint32_t)p, 1);
+				words.push_back((uint32_t)p);
 				fc[d]++;
+				real++;
 			}
 		}
+		pad8(words, st, pad);
+		midv[d] = (long long)words.size();
+		st = words.size();
 		for (long long i = mo[d]; i < mo[d + 1]; ++i) {
 			int p = ctx->h_place_multi[i], c = ctx->h_count_multi[i];
 			if (mk[p] < 1) {
+				size_t before = words.size();
 				push_word(words, (uint32_t)p, c);
+				real += (long long)(words.size() - before);
 				fc[d] += c;
 				sf[d] += std::lgamma((double)c + 1.0);
 			}
 		}
+		pad8(words, st, pad);
 		off[d + 1] = (long long)words.size();
 		mc += fc[d];
 	}
 	ctx->mean_count = mc / N;
-	ctx->n_ph = (long long)words.size();
+	ctx->n_ph = real;
 	CK(upload(ctx->ph, words.data(), words.size(), ctx->stream));
 	CK(upload(ctx->ph_off, off.data(), off.size(), ctx->stream));
+	CK(upload(ctx->ph_mid, midv.data(), midv.size(), ctx->stream));
 	CK(upload(ctx->fcounts, fc.data(), (size_t)N, ctx->stream));
 	CK(upload(ctx->sum_fact, sf.data(), (size_t)N, ctx->stream));
 	std::vector<double> ones_d(N, 1.);
@@ -212,6 +240,7 @@ extern "C" int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quat
 	NEED(num_rot > 0 && quats, DFG_ERR_ARG, "quaternions: need num_rot > 0");
 	for (long long i = 0; i < 5LL * num_rot; ++i)
 		NEED(std::isfinite(quats[i]), DFG_ERR_ARG, "quaternions: entry %lld is not finite", i);
+	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
 	ctx->num_rot = num_rot;
 	CK(upload(ctx->quats, quats, 5 * (size_t)num_rot, ctx->stream));
@@ -224,6 +253,7 @@ extern "C" int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const doubl
 		return DFG_ERR_ARG;
 	NEED(size >= 3 && num_modes >= 1 && model1, DFG_ERR_ARG, "model: need size >= 3, num_modes >= 1");
 	NEED(num_modes <= MAX_MODES, DFG_ERR_ARG, "model: at most %d modes", MAX_MODES);
+	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
 	ctx->S = size;
 	ctx->V = (long long)size * size * size;
@@ -322,16 +352,21 @@ static int build_chunks(dfg_ctx *ctx) {
 	ctx->chunks.clear();
 	ctx->chunks.resize(n_chunks);
 
-	// M-step index per chunk: photons on mask < 2 pixels, grouped by pixel
-	// (counting sort), frames ascending inside a pixel.
+	// M-step index per chunk: photons on mask < 2 pixels grouped by pixel
+	// (two counting sorts), frames ascending; per pixel a count-1 segment and
+	// a multi-photon segment, each padded to 8 words with the chunk's zero
+	// row Nc.
+	NEED(nc <= (long long)IDX_MASK, DFG_ERR_ARG, "frame chunk of %lld frames exceeds %u", nc, IDX_MASK);
 	const uint8_t *mk = ctx->h_mask.data();
-	std::vector<long long> cnt(P + 1);
+	std::vector<long long> c1(P + 1), cm(P + 1);
 	std::vector<uint32_t> words;
 	for (int k = 0; k < n_chunks; ++k) {
 		Chunk &ch = ctx->chunks[k];
 		ch.d0 = (int)(k * nc);
 		ch.nc = (int)std::min<long long>(nc, N - ch.d0);
-		std::fill(cnt.begin(), cnt.end(), 0);
+		const uint32_t pad = (uint32_t)ch.nc;
+		std::fill(c1.begin(), c1.end(), 0);
+		std::fill(cm.begin(), cm.end(), 0);
 		auto each = [&](auto fn) {
 			for (int dl = 0; dl < ch.nc; ++dl) {
 				int d = ch.d0 + dl;
@@ -347,28 +382,45 @@ static int build_chunks(dfg_ctx *ctx) {
 				}
 			}
 		};
-		each([&](int p, int, long long c) { cnt[p + 1] += (c + MAX_COUNT - 1) / MAX_COUNT; });
-		for (int p = 0; p < P; ++p)
-			cnt[p + 1] += cnt[p];
-		words.assign((size_t)cnt[P], 0u);
-		std::vector<long long> fill(cnt.begin(), cnt.end() - 1);
+		each([&](int p, int, long long c) {
+			if (c == 1)
+				c1[p]++;
+			else
+				cm[p] += (c + MAX_COUNT - 1) / MAX_COUNT;
+		});
+		std::vector<long long> off(P + 1, 0), midv(P, 0), f1(P), fm(P);
+		long long real = 0;
+		for (int p = 0; p < P; ++p) {
+			const long long a = (c1[p] + 7) / 8 * 8, b = (cm[p] + 7) / 8 * 8;
+			f1[p] = off[p];
+			midv[p] = off[p] + a;
+			fm[p] = midv[p];
+			off[p + 1] = off[p] + a + b;
+			real += c1[p] + cm[p];
+		}
+		words.assign((size_t)off[P], pad);
 		each([&](int p, int dl, long long c) {
+			if (c == 1) {
+				words[(size_t)f1[p]++] = (uint32_t)dl;
+				return;
+			}
 			while (c > 0) {
 				uint32_t cc = (uint32_t)std::min<long long>(c, MAX_COUNT);
-				words[(size_t)fill[p]++] = (uint32_t)dl | (cc << IDX_BITS);
+				words[(size_t)fm[p]++] = (uint32_t)dl | (cc << IDX_BITS);
 				c -= cc;
 			}
 		});
 		std::vector<int> pix;
 		for (int p = 0; p < P; ++p)
-			if (cnt[p + 1] > cnt[p])
+			if (off[p + 1] > off[p])
 				pix.push_back(p);
 		std::stable_sort(pix.begin(), pix.end(),
-		                 [&](int a, int b) { return cnt[a + 1] - cnt[a] > cnt[b + 1] - cnt[b]; });
+		                 [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
 		ch.npix = (int)pix.size();
-		ch.entries = cnt[P];
+		ch.entries = real;
 		CK(upload(ch.cs, words.data(), words.size(), ctx->stream));
-		CK(upload(ch.cs_off, cnt.data(), cnt.size(), ctx->stream));
+		CK(upload(ch.cs_off, off.data(), off.size(), ctx->stream));
+		CK(upload(ch.cs_mid, midv.data(), midv.size(), ctx->stream));
 		CK(upload(ch.pix, pix.data(), pix.size(), ctx->stream));
 		CK(cudaStreamSynchronize(ctx->stream));
 	}
@@ -386,7 +438,14 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	ctx->RT = (ctx->R + TILE - 1) / TILE;
 	ctx->R_pad = ctx->RT * TILE;
 	const size_t tiles_px = (size_t)ctx->RT * ctx->P * TILE;
-	CK(ctx->logW.ensure(tiles_px));
+	const size_t logw_n = (size_t)ctx->RT * (ctx->P + 1) * TILE;
+	if (ctx->logW.n < logw_n || ctx->logW_P != ctx->P) {
+		CK(ctx->logW.ensure(logw_n));
+		// the zero rows (pixel P of every tile) stay zero: the slice kernel
+		// writes rows 0..P-1 only
+		CK(cudaMemsetAsync(ctx->logW.p, 0, logw_n * sizeof(float), ctx->stream));
+		ctx->logW_P = ctx->P;
+	}
 	CK(ctx->T.ensure(tiles_px));
 	CK(ctx->u.ensure((size_t)ctx->R_pad));
 	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
@@ -411,7 +470,7 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	}
 	const size_t pairs = (size_t)ctx->R_pad * ctx->chunk_frames;
 	CK(ctx->pval.ensure(pairs));
-	CK(ctx->Pst.ensure(pairs));
+	CK(ctx->Pst.ensure((size_t)ctx->R_pad * (ctx->chunk_frames + 1)));
 	CK(ctx->tmax.ensure((size_t)ctx->RT * ctx->chunk_frames));
 	CK(ctx->targ.ensure((size_t)ctx->RT * ctx->chunk_frames));
 	const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
@@ -448,9 +507,8 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	slice_log_kernel<double><<<dim3(nblk, RT), 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, P,
 	                                                         ctx->model1.p, S, V, ctx->logW.p);
 	CKL("slice_log_kernel");
-	u_sequential_kernel<double><<<blocks_for(R, 128), 128, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p,
-	                                                               ctx->corr.p, ctx->mask.p, P, ctx->model1.p,
-	                                                               S, V, ctx->u.p);
+	u_sequential_kernel<double><<<blocks_for(R, 128), 128, 0, st>>>(ctx->quats.p, M, R, ctx->good.p, ctx->n_good,
+	                                                               ctx->model1.p, S, V, ctx->u.p);
 	CKL("u_sequential_kernel");
 	rescale_kernel<<<1, 32, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
 	CKL("rescale_kernel");
@@ -469,7 +527,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		{
 			long long warps = (long long)RT * Nc;
 			estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
-			    ctx->logW.p, ctx->u.p, ctx->quats.p, M, R, ctx->ph.p, ctx->ph_off.p, ctx->scale.p,
+			    ctx->logW.p, ctx->u.p, ctx->quats.p, M, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
 			    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
 			    ctx->targ.p);
 			CKL("estep_kernel");
@@ -478,13 +536,13 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
 		phase_begin(ctx, PH_NORM);
 		if (M > 1)
-			norm_kernel<true><<<blocks_for(Nc, 8), 256, 0, st>>>(
+			norm_kernel<true><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
 			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p,
 			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
 			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
 			    ctx->num_prob.p);
 		else
-			norm_kernel<false><<<blocks_for(Nc, 8), 256, 0, st>>>(
+			norm_kernel<false><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
 			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p,
 			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
 			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
@@ -508,23 +566,38 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		phase_begin(ctx, PH_MSTEP);
 		if (ch.npix > 0) {
 			long long warps = (long long)RT * ch.npix;
-			mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.pix.p,
-			                                                    ch.npix, P, RT, ctx->T.p);
+			mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p,
+			                                                    ch.pix.p, ch.npix, P, RT, ctx->T.p);
 			CKL("mstep_kernel");
 		}
 		phase_end(ctx, PH_MSTEP, ch.npix > 0 ? 1 : 0);
 	}
 
-	// merge (merge_tomogram -> slice_merge3d)
+	// merge (merge_tomogram -> slice_merge3d); the weight grid is rebuilt only
+	// when the set of orientations with psum_r > 0 changed
+	int with_weight = 1;
+	{
+		std::vector<double> pr(R);
+		CK(cudaMemcpyAsync(pr.data(), ctx->psum_r.p, (size_t)R * sizeof(double), cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		std::vector<uint8_t> pattern(R);
+		for (int r = 0; r < R; ++r)
+			pattern[r] = pr[r] > 0.;
+		if (ctx->weight_cache_valid && pattern == ctx->weight_pattern)
+			with_weight = 0;
+		ctx->weight_pattern.swap(pattern);
+		CK(ctx->weight_cache.ensure((size_t)M * V));
+	}
 	phase_begin(ctx, PH_MERGE);
 	merge_kernel<<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
-	                                              ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p);
+	                                              ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
+	                                              with_weight);
 	CKL("merge_kernel");
 	phase_end(ctx, PH_MERGE, 1);
 
 	phase_begin(ctx, PH_UPDATE);
-	unpack_accum_kernel<<<blocks_for((long long)M * V, 256), 256, 0, st>>>(ctx->accum.p, (long long)M * V,
-	                                                                       ctx->model2.p, ctx->weight.p);
+	unpack_accum_kernel<<<blocks_for((long long)M * V, 256), 256, 0, st>>>(
+	    ctx->accum.p, (long long)M * V, ctx->model2.p, ctx->weight.p, ctx->weight_cache.p, with_weight);
 	CKL("unpack_accum_kernel");
 	// averages over good frames; the packaged Iterate never sets num_blacklist,
 	// so they divide by N (max_prob.c:373-374, iterate.pyx:35)
@@ -541,6 +614,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	double h[3];
 	CK(cudaMemcpyAsync(h, ctx->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
+	ctx->weight_cache_valid = true;
 	ctx->rescale = h[0];
 	ctx->mutual_info = h[1] / N;
 	ctx->avg_ll = h[2] / N;

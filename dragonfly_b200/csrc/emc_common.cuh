@@ -5,20 +5,25 @@
 //              (one warp's lanes); RT = ceil(R / 32) tiles, orientation
 //              r = tile * 32 + lane, r -> (rotation r / M, mode r % M) as in
 //              dragonfly/src/max_prob.c:80-85.
-//   logW     [RT][P][32] float   log of the slice W_r[p], pixel-major inside a
+//   logW     [RT][P+1][32] float log of the slice W_r[p], pixel-major inside a
 //                                tile so that every photon gather reads one
-//                                coalesced 128-byte row (32 orientations).
+//                                coalesced 128-byte row (32 orientations); row
+//                                P is all zero (target of padding words).
 //   pval     [RT][Nc][32] double log-likelihood of (orientation, frame) pairs
 //                                of the current frame chunk.
 //   tmax/targ [RT][Nc]           per (tile, frame) maximum pval and its lowest r.
-//   Pst      [RT][Nc][32] float  normalised probability of kept pairs; the sign
-//                                carries the reference's PROB_MIN gate: P > 1e-6
-//                                stored as +P, kept but <= 1e-6 as -P, pruned 0.
+//   Pst      [RT][Nc+1][32] float normalised probability of kept pairs; the
+//                                sign carries the reference's PROB_MIN gate:
+//                                P > 1e-6 stored as +P, kept but <= 1e-6 as -P,
+//                                pruned 0; row Nc is all zero.
 //   T        [RT][P][32] float   photon tomograms sum_d P_dr * K_d[p].
 //   accum    [M*V] double2       (model2 sum, weight) merge accumulators.
-// Photon lists are packed 32-bit words: low 22 bits a pixel (E-step, per
-// frame) or a chunk-local frame (M-step, per pixel), high 10 bits the count;
-// counts above 1023 are split over several words (all uses are linear in it).
+// Photon lists: per frame (E-step) or per pixel (M-step) a segment of
+// count-1 photons followed by a segment of multi-photon words, each padded to
+// a multiple of 8 with words that point at the zero row. Count-1 words hold
+// the pixel (E-step) or chunk-local frame (M-step); multi words hold that
+// index in the low 22 bits and the count in the high 10 bits (counts above
+// 1023 are split over several words; every use is linear in the count).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -118,6 +123,33 @@ __device__ __forceinline__ double interp(const Cell &c, const MT *__restrict__ m
 	for (int k = 1; k < 8; ++k)
 		v = dadd(v, dmul(w[k], (double)__ldg(m + c.i000 + o[k])));
 	return dmul(v, corr);
+}
+
+// Compensated FP32 summation (Kahan): the represented sum is s - comp, with
+// an error of order n u^2 sum|x| (u = 2^-24), i.e. far below FP32 rounding.
+// Intrinsics keep the compiler from simplifying (t - s) - y.
+__device__ __forceinline__ void kahan_add(float &s, float &comp, float x) {
+	const float y = __fsub_rn(x, comp);
+	const float t = __fadd_rn(s, y);
+	comp = __fsub_rn(__fsub_rn(t, s), y);
+	s = t;
+}
+
+// Adds count * v exactly: the product's rounding error (from an FMA) goes
+// into the compensation. The count is converted through the bits of
+// 2^23 + c, without a conversion instruction.
+__device__ __forceinline__ void kahan_add_count(float &s, float &comp, uint32_t count, float v) {
+	const float c = __fsub_rn(__int_as_float(0x4B000000u | count), 8388608.f);
+	const float p = __fmul_rn(c, v);
+	const float e = __fmaf_rn(c, v, -p);
+	kahan_add(s, comp, p);
+	comp = __fsub_rn(comp, e);
+}
+
+// The compensated sum in FP64; -inf (a photon on a zero slice value) and NaN
+// pass through (the compensation is NaN then).
+__device__ __forceinline__ double kahan_value(float s, float comp) {
+	return isinf(s) ? (double)s : (double)s - (double)comp;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

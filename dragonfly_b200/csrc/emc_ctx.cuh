@@ -59,8 +59,9 @@ struct DevBuf {
 
 struct Chunk {
 	int d0 = 0, nc = 0;
-	DevBuf<uint32_t> cs;       // (chunk-local frame | count << 22), grouped by pixel
+	DevBuf<uint32_t> cs;       // per pixel: count-1 frames, then (frame | count << 22), padded
 	DevBuf<long long> cs_off;  // [P + 1]
+	DevBuf<long long> cs_mid;  // [P] start of the multi-photon segment
 	DevBuf<int> pix;           // pixels with non-empty lists, longest first
 	int npix = 0;
 	long long entries = 0;
@@ -80,14 +81,18 @@ struct dfg_ctx {
 	DevBuf<double> qvals, corr;
 	DevBuf<uint8_t> mask;
 	std::vector<uint8_t> h_mask;
+	DevBuf<double4> good;  // (qx, qy, qz, corr) of mask == 0 pixels, in pixel order
+	int n_good = 0;
 
 	// frames
 	int N = 0;
 	std::vector<int> h_ones, h_multi, h_place_ones, h_place_multi, h_count_multi;
 	std::vector<long long> h_ones_off, h_multi_off;
-	DevBuf<uint32_t> ph;
-	DevBuf<long long> ph_off;
-	long long n_ph = 0;
+	DevBuf<uint32_t> ph;       // per frame: count-1 pixels, then (pixel | count << 22), padded
+	DevBuf<long long> ph_off;  // [N + 1]
+	DevBuf<long long> ph_mid;  // [N] start of the multi-photon segment
+	long long n_ph = 0;        // photon words without padding
+	int logW_P = -1;           // detector size the zero row of logW was written for
 	DevBuf<double> scale, beta, beta_start, sum_fact;
 	DevBuf<int> fcounts;
 	DevBuf<uint8_t> blacklist;
@@ -100,6 +105,11 @@ struct dfg_ctx {
 	long long S = 0, V = 0;
 	DevBuf<double> model1, model2, weight;
 	DevBuf<double2> accum;
+	// inter_weight of the last merge and the psum_r > 0 pattern it was built
+	// for (the weights depend on nothing else once geometry is fixed)
+	DevBuf<double> weight_cache;
+	std::vector<uint8_t> weight_pattern;
+	bool weight_cache_valid = false;
 
 	// work buffers
 	DevBuf<float> logW, Pst, T;

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 	for (int row = w; row < PB; row += 8) {
 		int pp = p0 + row;
 		if (pp < P)
-			logW[((size_t)rt * P + pp) * TILE + lane] = s_tile[row][lane];
+			logW[((size_t)rt * (P + 1) + pp) * TILE + lane] = s_tile[row][lane];
 	}
 }
 
@@ -58,12 +58,11 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 // One thread per orientation walks the pixels sequentially, so u_r is
 // bit-identical to the reference's (frames without photons are ranked by u_r
 // alone, and orientations related by a symmetry of the model tie exactly).
-// Pixel data are read uniformly by a warp; orientations differ per lane.
+// The mask-0 pixels come packed as (qx, qy, qz, corr), in pixel order; four
+// interpolations are in flight while the additions stay sequential.
 template <typename MT>
 __global__ void __launch_bounds__(128) u_sequential_kernel(const double *__restrict__ quats, int M, int R,
-                                                           const double *__restrict__ qvals,
-                                                           const double *__restrict__ corr,
-                                                           const uint8_t *__restrict__ mask, int P,
+                                                           const double4 *__restrict__ good, int n_good,
                                                            const MT *__restrict__ model, long long S, long long V,
                                                            double *__restrict__ u) {
 	const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -74,11 +73,21 @@ __global__ void __launch_bounds__(128) u_sequential_kernel(const double *__restr
 	const MT *m = model + (size_t)(r % M) * V;
 	const double center = (double)(S / 2);
 	double acc = 0.;
-	for (int p = 0; p < P; ++p) {
-		if (mask[p] < 1) {
-			Cell c = locate(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2], center, S);
-			acc = dadd(acc, interp(c, m, S, corr[p]));
+	int k = 0;
+	for (; k + 4 <= n_good; k += 4) {
+		double w[4];
+#pragma unroll
+		for (int q = 0; q < 4; ++q) {
+			const double4 g = good[k + q];
+			w[q] = interp(locate(rot, g.x, g.y, g.z, center, S), m, S, g.w);
 		}
+#pragma unroll
+		for (int q = 0; q < 4; ++q)
+			acc = dadd(acc, w[q]);
+	}
+	for (; k < n_good; ++k) {
+		const double4 g = good[k];
+		acc = dadd(acc, interp(locate(rot, g.x, g.y, g.z, center, S), m, S, g.w));
 	}
 	u[r] = acc;
 }
@@ -99,17 +108,18 @@ __global__ void rescale_kernel(const double *__restrict__ u, const double *__res
 // (b) E-step: pval[tile][d][lane] = log w_r - u_r * s_d + sum_k c_k logW_r[p_k]
 // ---------------------------------------------------------------------------
 // One warp per (orientation tile, frame), tiles outermost so that resident
-// warps share one tile's log-slices in L2. Photon words are fetched 32 at a
-// time and broadcast by shuffle; each photon costs one coalesced 128-byte row
-// read. FP64 accumulation of FP32 log-slice values (c * v is exact in FP64).
-// s_d = phi_d when need_scaling && (iteration > 1 || known_scale), else the
-// rescale factor (max_prob.c:122-128).
+// warps share one tile's log-slices in L2. Each photon costs one coalesced
+// 128-byte row read and a compensated FP32 addition (no conversion
+// instructions in the loop; two interleaved accumulators halve the dependency
+// chain); padded segments need no per-photon bounds test. The photon sum is
+// formed in FP64 once per pair. s_d = phi_d when need_scaling &&
+// (iteration > 1 || known_scale), else the rescale factor (max_prob.c:122-128).
 __global__ void __launch_bounds__(256) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ quats, int M,
     int R, const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
-    const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
-    const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval, double *__restrict__ tmax,
-    int *__restrict__ targ) {
+    const long long *__restrict__ ph_mid, const double *__restrict__ scale, const uint8_t *__restrict__ blacklist,
+    int d0, int Nc, int use_scale, const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval,
+    double *__restrict__ tmax, int *__restrict__ targ) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * Nc)
@@ -118,28 +128,45 @@ __global__ void __launch_bounds__(256) estep_kernel(
 	if (blacklist[d])
 		return;
 	const int r = rt * TILE + lane;
-	const double s = use_scale ? scale[d] : scalars[0];
-	double acc = 0.;
-	if (r < R)
-		acc = dsub(log(quats[(r / M) * 5 + 4]), dmul(u[r], s));
-	const float *L = logW + (size_t)rt * P * TILE + lane;
-	const long long beg = ph_off[d], end = ph_off[d + 1];
-	for (long long j0 = beg; j0 < end; j0 += 32) {
-		const uint32_t e = (j0 + lane < end) ? __ldg(ph + j0 + lane) : 0u;
-		const int n = (int)min(32LL, end - j0);
-		for (int k = 0; k < n; k += 8) {
-			uint32_t ek[8];
-			float v[8];
+	const float *L = logW + (size_t)rt * (P + 1) * TILE + lane;
+	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
+	// segments start at multiples of 8 words: two 16-byte loads, identical for
+	// every lane (broadcast), bring 8 photon words
+	const uint4 *w4 = reinterpret_cast<const uint4 *>(ph);
+	float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
+#pragma unroll 2
+	for (long long j = beg; j < mid; j += 8) {
+		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
+		const float v0 = __ldg(L + a.x * TILE), v1 = __ldg(L + a.y * TILE), v2 = __ldg(L + a.z * TILE),
+		            v3 = __ldg(L + a.w * TILE), v4 = __ldg(L + b.x * TILE), v5 = __ldg(L + b.y * TILE),
+		            v6 = __ldg(L + b.z * TILE), v7 = __ldg(L + b.w * TILE);
+		kahan_add(s0, c0, v0);
+		kahan_add(s1, c1, v1);
+		kahan_add(s0, c0, v2);
+		kahan_add(s1, c1, v3);
+		kahan_add(s0, c0, v4);
+		kahan_add(s1, c1, v5);
+		kahan_add(s0, c0, v6);
+		kahan_add(s1, c1, v7);
+	}
+	for (long long j = mid; j < end; j += 8) {
+		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
+		const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+		float v[8];
 #pragma unroll
-			for (int q = 0; q < 8; ++q)
-				ek[q] = __shfl_sync(FULL, e, k + q);
+		for (int q = 0; q < 8; ++q)
+			v[q] = __ldg(L + (e[q] & IDX_MASK) * TILE);
 #pragma unroll
-			for (int q = 0; q < 8; ++q)
-				v[q] = (k + q < n) ? __ldg(L + (size_t)(ek[q] & IDX_MASK) * TILE) : 0.f;
-#pragma unroll
-			for (int q = 0; q < 8; ++q)
-				acc = fma((double)(ek[q] >> IDX_BITS), (double)v[q], acc);
+		for (int q = 0; q < 8; q += 2) {
+			kahan_add_count(s0, c0, e[q] >> IDX_BITS, v[q]);
+			kahan_add_count(s1, c1, e[q + 1] >> IDX_BITS, v[q + 1]);
 		}
+	}
+	double acc = 0.;
+	if (r < R) {
+		const double sd = use_scale ? scale[d] : scalars[0];
+		acc = dadd(dsub(log(quats[(r / M) * 5 + 4]), dmul(u[r], sd)),
+		           dadd(kahan_value(s0, c0), kahan_value(s1, c1)));
 	}
 	pval[((size_t)rt * Nc + dl) * TILE + lane] = acc;
 	// tile maximum and its lowest orientation index (strict > in ascending r,
@@ -186,12 +213,17 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	constexpr int UNR = 4;
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
-	if (warp >= Nc)
+	const size_t tstride = (size_t)Nc * TILE, pstride = (size_t)(Nc + 1) * TILE;
+	if (warp == Nc) {  // the zero row that padding words of the M-step point at
+		for (int rt = 0; rt < RT; ++rt)
+			Pst[rt * pstride + (size_t)Nc * TILE + lane] = 0.f;
+		return;
+	}
+	if (warp > Nc)
 		return;
 	const int dl = warp, d = d0 + dl;
 	const double *pv = pval + (size_t)dl * TILE + lane;
 	float *ps = Pst + (size_t)dl * TILE + lane;
-	const size_t tstride = (size_t)Nc * TILE;
 	const bool bl = blacklist[d] != 0;
 
 	double m = MAX_EXP_START;
@@ -216,7 +248,7 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	}
 	if (bl || m == MAX_EXP_START) {
 		for (int rt = 0; rt < RT; ++rt)
-			ps[rt * tstride] = 0.f;
+			ps[rt * pstride] = 0.f;
 		if (lane == 0) {
 			rmax[d] = -1;
 			max_exp[d] = MAX_EXP_START;
@@ -297,7 +329,7 @@ __global__ void __launch_bounds__(256) norm_kernel(
 					out = (P > PROB_MIN) ? (float)P : -(float)P;
 				}
 			}
-			ps[rt * tstride] = out;
+			ps[rt * pstride] = out;
 		}
 	}
 	ll = warp_sum(ll);
@@ -330,7 +362,7 @@ __global__ void __launch_bounds__(256) psum_r_kernel(const float *__restrict__ P
 	const int rt = blockIdx.x, split = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int beg = split * frames_per_split, end = min(Nc, beg + frames_per_split);
 	double acc = 0.;
-	const float *p = Pst + (size_t)rt * Nc * TILE + lane;
+	const float *p = Pst + (size_t)rt * (Nc + 1) * TILE + lane;
 	for (int dl = beg + w; dl < end; dl += 8) {
 		double v = fabs((double)p[(size_t)dl * TILE]);
 		acc += need_scaling ? v * scale[d0 + dl] : v;
@@ -361,12 +393,14 @@ __global__ void psum_r_reduce_kernel(const double *__restrict__ part, int nsplit
 // (e1) M-step back-projection: T[tile][p][lane] += sum_(d,c) c * P_dr
 // ---------------------------------------------------------------------------
 // Gather form of update_tomogram_nobg (max_update.c:142-230): one warp per
-// (orientation tile, pixel), walking the pixel's list of (frame, count) words
-// (pixels with mask < 2 only) and reading one 128-byte row of P per entry.
-// No atomics; pixels are visited heaviest first for balance.
+// (orientation tile, pixel), walking the pixel's list of frames (pixels with
+// mask < 2 only) and reading one 128-byte row of P per entry; count-1 and
+// multi-photon segments as in the E-step, compensated FP32 sums. No atomics;
+// pixels are visited heaviest first for balance.
 __global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Pst, int Nc,
                                                      const uint32_t *__restrict__ cs,
                                                      const long long *__restrict__ cs_off,
+                                                     const long long *__restrict__ cs_mid,
                                                      const int *__restrict__ pix, int npix, int P, int RT,
                                                      float *__restrict__ T) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -375,28 +409,40 @@ __global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Ps
 		return;
 	const int rt = (int)(warp / npix), k = (int)(warp - (long long)rt * npix);
 	const int p = pix[k];
-	const float *Pr = Pst + (size_t)rt * Nc * TILE + lane;
-	const long long beg = cs_off[p], end = cs_off[p + 1];
-	double acc = 0.;
-	for (long long j0 = beg; j0 < end; j0 += 32) {
-		const uint32_t e = (j0 + lane < end) ? __ldg(cs + j0 + lane) : 0u;
-		const int n = (int)min(32LL, end - j0);
-		for (int q0 = 0; q0 < n; q0 += 8) {
-			uint32_t ek[8];
-			float v[8];
+	const float *Pr = Pst + (size_t)rt * (Nc + 1) * TILE + lane;
+	const long long beg = cs_off[p], mid = cs_mid[p], end = cs_off[p + 1];
+	const uint4 *w4 = reinterpret_cast<const uint4 *>(cs);
+	float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
+#pragma unroll 2
+	for (long long j = beg; j < mid; j += 8) {
+		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
+		const float v0 = __ldg(Pr + a.x * TILE), v1 = __ldg(Pr + a.y * TILE), v2 = __ldg(Pr + a.z * TILE),
+		            v3 = __ldg(Pr + a.w * TILE), v4 = __ldg(Pr + b.x * TILE), v5 = __ldg(Pr + b.y * TILE),
+		            v6 = __ldg(Pr + b.z * TILE), v7 = __ldg(Pr + b.w * TILE);
+		kahan_add(s0, c0, fmaxf(v0, 0.f));
+		kahan_add(s1, c1, fmaxf(v1, 0.f));
+		kahan_add(s0, c0, fmaxf(v2, 0.f));
+		kahan_add(s1, c1, fmaxf(v3, 0.f));
+		kahan_add(s0, c0, fmaxf(v4, 0.f));
+		kahan_add(s1, c1, fmaxf(v5, 0.f));
+		kahan_add(s0, c0, fmaxf(v6, 0.f));
+		kahan_add(s1, c1, fmaxf(v7, 0.f));
+	}
+	for (long long j = mid; j < end; j += 8) {
+		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
+		const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+		float v[8];
 #pragma unroll
-			for (int q = 0; q < 8; ++q)
-				ek[q] = __shfl_sync(FULL, e, q0 + q);
+		for (int q = 0; q < 8; ++q)
+			v[q] = fmaxf(__ldg(Pr + (e[q] & IDX_MASK) * TILE), 0.f);
 #pragma unroll
-			for (int q = 0; q < 8; ++q)
-				v[q] = (q0 + q < n) ? __ldg(Pr + (size_t)(ek[q] & IDX_MASK) * TILE) : 0.f;
-#pragma unroll
-			for (int q = 0; q < 8; ++q)
-				acc = fma((double)(ek[q] >> IDX_BITS), (double)fmaxf(v[q], 0.f), acc);
+		for (int q = 0; q < 8; q += 2) {
+			kahan_add_count(s0, c0, e[q] >> IDX_BITS, v[q]);
+			kahan_add_count(s1, c1, e[q + 1] >> IDX_BITS, v[q + 1]);
 		}
 	}
 	float *out = T + ((size_t)rt * P + p) * TILE + lane;
-	*out = (float)((double)*out + acc);
+	*out = (float)((double)*out + dadd(kahan_value(s0, c0), kahan_value(s1, c1)));
 }
 
 // ---------------------------------------------------------------------------
@@ -409,13 +455,16 @@ __global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Ps
 // (model, weight) pairs, interleaved so both atomics of a corner hit one
 // 32-byte sector: FP32 sums of thousands of contributions per voxel would
 // carry ~1e-6 relative error into the next iteration's likelihoods.
+// The weight sum depends only on which orientations have psum_r > 0; when
+// that set is the one of a cached weight grid, with_weight is 0 and only the
+// model sums are accumulated.
 __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ psum_r,
                                                      const double *__restrict__ quats, int M, int R,
                                                      const double *__restrict__ qvals,
                                                      const double *__restrict__ corr,
                                                      const uint8_t *__restrict__ mask, int P, long long S,
-                                                     long long V, double *__restrict__ accum) {
+                                                     long long V, double *__restrict__ accum, int with_weight) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ double s_ps[TILE];
@@ -456,10 +505,16 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 		double fw[8];
 		corner_weights(c, fw);
 		double *a = accum + 2 * ((size_t)s_mode[j] * V + c.i000);
+		if (with_weight) {
 #pragma unroll
-		for (int q = 0; q < 8; ++q) {
-			atomicAdd(a + 2 * o[q], fw[q] * wv);
-			atomicAdd(a + 2 * o[q] + 1, fw[q]);
+			for (int q = 0; q < 8; ++q) {
+				atomicAdd(a + 2 * o[q], fw[q] * wv);
+				atomicAdd(a + 2 * o[q] + 1, fw[q]);
+			}
+		} else {
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				atomicAdd(a + 2 * o[q], fw[q] * wv);
 		}
 	}
 }
@@ -467,14 +522,22 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 // ---------------------------------------------------------------------------
 // model update (recon.pyx:112-149) and small per-frame kernels
 // ---------------------------------------------------------------------------
+// model2 / inter_weight from the accumulators; the weights either come from
+// this merge (and are kept in weight_cache) or from weight_cache.
 __global__ void unpack_accum_kernel(const double2 *__restrict__ accum, long long n, double *__restrict__ model2,
-                                    double *__restrict__ weight) {
+                                    double *__restrict__ weight, double *__restrict__ weight_cache,
+                                    int with_weight) {
 	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
 	double2 a = accum[i];
 	model2[i] = a.x;
-	weight[i] = a.y;
+	if (with_weight) {
+		weight[i] = a.y;
+		weight_cache[i] = a.y;
+	} else {
+		weight[i] = weight_cache[i];
+	}
 }
 
 __device__ __forceinline__ double friedel_avg(double a1, double w1, double a2, double w2) {

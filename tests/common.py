@@ -86,9 +86,56 @@ class GPUEngine:
         self.ctx.close()
 
 
-def compare_iteration(a, b, prob, it, check_model=True):
+def pair_loglik(prob, model, r, d, u_r, s_d):
+    """FP64 log-likelihood of frame d at orientation r under model, in the
+    reference's order (max_prob.c:122-171), from the oracle's slice."""
+    M = prob.num_modes
+    orc = OracleEngine(prob)
+    orc._model1 = np.ascontiguousarray(model)
+    logw = np.log(orc.slice_gen(prob.quats[r // M], r % M))
+    oo = int(prob.ones[:d].sum())
+    mo = int(prob.multi[:d].sum())
+    pval = np.log(prob.quats[r // M, 4]) - u_r * s_d
+    for p in prob.place_ones[oo:oo + prob.ones[d]]:
+        if prob.mask[p] < 1:
+            pval += logw[p]
+    for p, c in zip(prob.place_multi[mo:mo + prob.multi[d]], prob.count_multi[mo:mo + prob.multi[d]]):
+        if prob.mask[p] < 1:
+            pval += c * logw[p]
+    return pval
+
+
+def rmax_agreement(a, b, prob, model_before, it, scale_before=None):
+    """Fraction of good frames whose most likely orientation is the oracle's,
+    counting as agreeing the frames where the two choices are exact ties: the
+    oracle's log-likelihoods of both orientations equal within 1e-9 relative
+    (e.g. frames without photons, ranked by u_r alone, when a symmetry of the
+    detector and the Friedel-symmetric model maps one orientation onto the
+    other -- the reference then picks by rounding noise). Returns
+    (agreement, number of tie frames)."""
+    good = np.ones(prob.num_data, bool) if prob.blacklist is None else prob.blacklist == 0
+    if not good.any():
+        return 1., 0
+    mism = np.nonzero((a["rmax"] != b["rmax"]) & good)[0]
+    ties = 0
+    use_scale = prob.need_scaling and (it > 1 or prob.known_scale)
+    for d in mism:
+        ra, rb = int(a["rmax"][d]), int(b["rmax"][d])
+        if ra < 0 or rb < 0:
+            continue
+        s_d = scale_before[d] if use_scale else b["rescale"]
+        la = pair_loglik(prob, model_before, ra, d, b["u"][ra], s_d)
+        lb = pair_loglik(prob, model_before, rb, d, b["u"][rb], s_d)
+        if abs(la - lb) <= 1e-9 * max(1., abs(lb)):
+            ties += 1
+    return float(1. - (len(mism) - ties) / good.sum()), ties
+
+
+def compare_iteration(a, b, prob, it, check_model=True, model_before=None, scale_before=None):
     """Checks GPU result a against oracle result b; returns a dict of the
-    measured deviations (asserts the parity bar)."""
+    measured deviations (asserts the parity bar). model_before / scale_before
+    (the oracle's inputs of this iteration) let exact ties of the most likely
+    orientation be recognised."""
     good = np.ones(prob.num_data, bool) if prob.blacklist is None else prob.blacklist == 0
     out = {}
     out["model_rel_l2"] = rel_l2(a["model1"], b["model1"])
@@ -96,6 +143,9 @@ def compare_iteration(a, b, prob, it, check_model=True):
     out["mi_rel"] = rel(a["mutual_info"], b["mutual_info"]) if b["mutual_info"] != 0 else \
         abs(a["mutual_info"])
     out["rmax_agree"] = float(np.mean(a["rmax"][good] == b["rmax"][good])) if good.any() else 1.
+    out["rmax_ties"] = 0
+    if out["rmax_agree"] < RMAX_AGREE and model_before is not None:
+        out["rmax_agree"], out["rmax_ties"] = rmax_agreement(a, b, prob, model_before, it, scale_before)
     out["rmax_blacklisted_equal"] = bool(np.all(a["rmax"][~good] == b["rmax"][~good]))
     if prob.need_scaling:
         sa, sb = a["scale"][good], b["scale"][good]

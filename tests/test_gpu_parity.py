@@ -20,13 +20,14 @@ def test_gpu_matches_oracle_on_golden_cases(name, oracle_built):
     gpu = GPUEngine(prob)
     orc = OracleEngine(prob)
     for it in range(1, int(g["iters"]) + 1):
+        model_before, scale_before = orc.model1(), orc.scale.copy()
         a = gpu.run_iteration(it)
         b = orc.run_iteration(it)
-        compare_iteration(a, b, prob, it)
+        dev = compare_iteration(a, b, prob, it, model_before=model_before, scale_before=scale_before)
         # the golden vectors of the reference itself
         k = "it%d_" % it
         good = g["blacklist"] == 0
-        assert np.mean(a["rmax"][good] == g[k + "rmax"][good]) >= 0.999
+        assert np.mean(a["rmax"][good] == g[k + "rmax"][good]) >= 0.999 - dev["rmax_ties"] / good.sum()
         assert np.all(a["rmax"][~good] == -1)
         assert abs(a["avg_likelihood"] - g[k + "scalars"][0]) <= 1e-6 * abs(g[k + "scalars"][0])
         # u_r and the rescale factor are FP64 sums in the reference's order:
@@ -57,9 +58,10 @@ def test_gpu_small_config_ten_iterations(oracle_built):
     orc = OracleEngine(prob)
     worst = {}
     for it in range(1, 11):
+        model_before = orc.model1()
         a = gpu.run_iteration(it)
         b = orc.run_iteration(it)
-        dev = compare_iteration(a, b, prob, it)
+        dev = compare_iteration(a, b, prob, it, model_before=model_before)
         for k, v in dev.items():
             if isinstance(v, float):
                 worst[k] = max(worst.get(k, 0.), v) if k != "rmax_agree" else min(worst.get(k, 1.), v)
