@@ -114,7 +114,7 @@ __global__ void rescale_kernel(const double *__restrict__ u, const double *__res
 // chain); padded segments need no per-photon bounds test. The photon sum is
 // formed in FP64 once per pair. s_d = phi_d when need_scaling &&
 // (iteration > 1 || known_scale), else the rescale factor (max_prob.c:122-128).
-__global__ void __launch_bounds__(256) estep_kernel(
+__global__ void __launch_bounds__(256, 6) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ quats, int M,
     int R, const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
     const long long *__restrict__ ph_mid, const double *__restrict__ scale, const uint8_t *__restrict__ blacklist,
@@ -134,12 +134,20 @@ __global__ void __launch_bounds__(256) estep_kernel(
 	// every lane (broadcast), bring 8 photon words
 	const uint4 *w4 = reinterpret_cast<const uint4 *>(ph);
 	float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
-#pragma unroll 2
+	// the next 8 words are fetched while the current 8 rows are in flight
+	uint4 a = make_uint4(P, P, P, P), b = a;
+	if (beg < mid) {
+		a = __ldg(w4 + (beg >> 2));
+		b = __ldg(w4 + (beg >> 2) + 1);
+	}
 	for (long long j = beg; j < mid; j += 8) {
-		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
 		const float v0 = __ldg(L + a.x * TILE), v1 = __ldg(L + a.y * TILE), v2 = __ldg(L + a.z * TILE),
 		            v3 = __ldg(L + a.w * TILE), v4 = __ldg(L + b.x * TILE), v5 = __ldg(L + b.y * TILE),
 		            v6 = __ldg(L + b.z * TILE), v7 = __ldg(L + b.w * TILE);
+		if (j + 8 < mid) {
+			a = __ldg(w4 + ((j + 8) >> 2));
+			b = __ldg(w4 + ((j + 8) >> 2) + 1);
+		}
 		kahan_add(s0, c0, v0);
 		kahan_add(s1, c1, v1);
 		kahan_add(s0, c0, v2);
