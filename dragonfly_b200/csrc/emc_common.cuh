@@ -1,22 +1,24 @@
 // Constants and inline device helpers of the EMC iteration for sm_100a (B200).
 //
 // Layout conventions (all in HBM, owned by the context in emc_api.cu):
-//   R        = num_modes * num_rot orientations, processed in tiles of 32
-//              (one warp's lanes); RT = ceil(R / 32) tiles, orientation
-//              r = tile * 32 + lane, r -> (rotation r / M, mode r % M) as in
-//              dragonfly/src/max_prob.c:80-85.
-//   logW     [RT][P+1][32] float log of the slice W_r[p], pixel-major inside a
-//                                tile so that every photon gather reads one
-//                                coalesced 128-byte row (32 orientations); row
-//                                P is all zero (target of padding words).
-//   pval     [RT][Nc][32] double log-likelihood of (orientation, frame) pairs
-//                                of the current frame chunk.
+//   R        = num_modes * num_rot orientations, processed in tiles of
+//              TILE = 32 * LW (one warp; each lane owns LW consecutive
+//              orientations, so a row of a tile is one vector load per lane);
+//              RT = ceil(R / TILE) tiles, orientation
+//              r = tile * TILE + lane * LW + k, r -> (rotation r / M, mode r % M)
+//              as in dragonfly/src/max_prob.c:80-85.
+//   logW     [RT][P+1][TILE] float log of the slice W_r[p], pixel-major inside
+//                                a tile so that every photon gather reads one
+//                                coalesced row (4 * TILE bytes); row P is all
+//                                zero (target of padding words).
+//   pval     [RT][Nc][TILE] double log-likelihood of (orientation, frame)
+//                                pairs of the current frame chunk.
 //   tmax/targ [RT][Nc]           per (tile, frame) maximum pval and its lowest r.
-//   Pst      [RT][Nc+1][32] float normalised probability of kept pairs; the
+//   Pst      [RT][Nc+1][TILE] float normalised probability of kept pairs; the
 //                                sign carries the reference's PROB_MIN gate:
 //                                P > 1e-6 stored as +P, kept but <= 1e-6 as -P,
 //                                pruned 0; row Nc is all zero.
-//   T        [RT][P][32] float   photon tomograms sum_d P_dr * K_d[p].
+//   T        [RT][P][TILE] float  photon tomograms sum_d P_dr * K_d[p].
 //   accum    [M*V] double2       (model2 sum, weight) merge accumulators.
 // Photon lists: per frame (E-step) or per pixel (M-step) a segment of
 // count-1 photons followed by a segment of multi-photon words, each padded to
@@ -30,9 +32,18 @@
 #include <float.h>
 #include <stdint.h>
 
+// Orientations per lane: 4 makes every photon gather one 16-byte load per
+// lane (a 512-byte row per warp), which moves four times the bytes per load
+// instruction and per photon-word fetch of a one-orientation lane.
+#ifndef DFG_LANE_W
+#define DFG_LANE_W 4
+#endif
+
 namespace dfg {
 
-constexpr int TILE = 32;
+constexpr int LW = DFG_LANE_W;
+static_assert(LW == 1 || LW == 2 || LW == 4, "lane width must be 1, 2 or 4");
+constexpr int TILE = 32 * LW;
 constexpr int IDX_BITS = 22;
 constexpr uint32_t IDX_MASK = (1u << IDX_BITS) - 1u;
 constexpr uint32_t MAX_COUNT = (1u << (32 - IDX_BITS)) - 1u;
@@ -150,6 +161,65 @@ __device__ __forceinline__ void kahan_add_count(float &s, float &comp, uint32_t 
 // pass through (the compensation is NaN then).
 __device__ __forceinline__ double kahan_value(float s, float comp) {
 	return isinf(s) ? (double)s : (double)s - (double)comp;
+}
+
+// LW consecutive values of one lane as a single vector access (p aligned to
+// LW elements). Read-only loads go through the non-coherent path.
+__device__ __forceinline__ void ld_row(const float *__restrict__ p, float (&v)[LW]) {
+	if constexpr (LW == 4) {
+		const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
+		v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+	} else if constexpr (LW == 2) {
+		const float2 x = __ldg(reinterpret_cast<const float2 *>(p));
+		v[0] = x.x; v[1] = x.y;
+	} else {
+		v[0] = __ldg(p);
+	}
+}
+
+// Same, for rows the calling kernel may have written (plain loads).
+__device__ __forceinline__ void ld_row_rw(const float *p, float (&v)[LW]) {
+	if constexpr (LW == 4) {
+		const float4 x = *reinterpret_cast<const float4 *>(p);
+		v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+	} else if constexpr (LW == 2) {
+		const float2 x = *reinterpret_cast<const float2 *>(p);
+		v[0] = x.x; v[1] = x.y;
+	} else {
+		v[0] = *p;
+	}
+}
+
+__device__ __forceinline__ void st_row(float *p, const float (&v)[LW]) {
+	if constexpr (LW == 4)
+		*reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+	else if constexpr (LW == 2)
+		*reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+	else
+		*p = v[0];
+}
+
+__device__ __forceinline__ void ld_row(const double *__restrict__ p, double (&v)[LW]) {
+	if constexpr (LW == 1) {
+		v[0] = __ldg(p);
+	} else {
+#pragma unroll
+		for (int k = 0; k < LW; k += 2) {
+			const double2 x = __ldg(reinterpret_cast<const double2 *>(p + k));
+			v[k] = x.x;
+			v[k + 1] = x.y;
+		}
+	}
+}
+
+__device__ __forceinline__ void st_row(double *p, const double (&v)[LW]) {
+	if constexpr (LW == 1) {
+		*p = v[0];
+	} else {
+#pragma unroll
+		for (int k = 0; k < LW; k += 2)
+			*reinterpret_cast<double2 *>(p + k) = make_double2(v[k], v[k + 1]);
+	}
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -7,11 +7,12 @@
 namespace dfg {
 
 // ---------------------------------------------------------------------------
-// (a) slice generation: logW[tile][p][lane] = log(W), u partial sums
+// (a) slice generation: logW[tile][p][j] = log(W_r), r = tile * TILE + j
 // ---------------------------------------------------------------------------
 // Block = one orientation tile x PB pixels, 256 threads: thread (i = t % 64,
-// g = t / 64) computes pixel i for orientations g, g+4, ..., g+28, so a warp
-// walks 32 neighbouring pixels of one orientation (neighbouring model reads).
+// g = t / 64) computes pixel i for orientations g, g+4, ..., so a warp walks
+// 32 neighbouring pixels of one orientation (neighbouring model reads).
+// The tile is staged in shared memory and stored as coalesced rows.
 template <typename MT>
 __global__ void __launch_bounds__(256) slice_log_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
@@ -21,11 +22,11 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 	__shared__ int s_mode[TILE];
 	__shared__ float s_tile[PB][TILE + 1];
 	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
-	if (t < TILE) {
-		int r = rt * TILE + t;
+	for (int j = t; j < TILE; j += blockDim.x) {
+		int r = rt * TILE + j;
 		int rr = r < R ? r : 0;
-		rot_from_quat(&quats[(rr / M) * 5], s_rot[t]);
-		s_mode[t] = rr % M;
+		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
+		s_mode[j] = rr % M;
 	}
 	__syncthreads();
 	const int i = t & (PB - 1), g = t >> 6, p = p0 + i;
@@ -37,7 +38,7 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 	}
 	const double center = (double)(S / 2);
 #pragma unroll 2
-	for (int k = 0; k < 8; ++k) {
+	for (int k = 0; k < TILE / 4; ++k) {
 		const int j = g + 4 * k;
 		if (pix) {
 			Cell c = locate(s_rot[j], qx, qy, qz, center, S);
@@ -45,12 +46,17 @@ __global__ void __launch_bounds__(256) slice_log_kernel(
 		}
 	}
 	__syncthreads();
-	// coalesced store: warp w writes rows w, w+8, ...
+	// coalesced store: warp w writes rows w, w+8, ...; a lane its LW values
 	const int w = t >> 5, lane = t & 31;
 	for (int row = w; row < PB; row += 8) {
 		int pp = p0 + row;
-		if (pp < P)
-			logW[((size_t)rt * (P + 1) + pp) * TILE + lane] = s_tile[row][lane];
+		if (pp < P) {
+			float v[LW];
+#pragma unroll
+			for (int k = 0; k < LW; ++k)
+				v[k] = s_tile[row][lane * LW + k];
+			st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + lane * LW, v);
+		}
 	}
 }
 
@@ -105,16 +111,20 @@ __global__ void rescale_kernel(const double *__restrict__ u, const double *__res
 }
 
 // ---------------------------------------------------------------------------
-// (b) E-step: pval[tile][d][lane] = log w_r - u_r * s_d + sum_k c_k logW_r[p_k]
+// (b) E-step: pval[tile][d][j] = log w_r - u_r * s_d + sum_k c_k logW_r[p_k]
 // ---------------------------------------------------------------------------
 // One warp per (orientation tile, frame), tiles outermost so that resident
 // warps share one tile's log-slices in L2. Each photon costs one coalesced
-// 128-byte row read and a compensated FP32 addition (no conversion
-// instructions in the loop; two interleaved accumulators halve the dependency
+// row read (one LW-wide vector load per lane) and a compensated FP32
+// addition per orientation (no conversion instructions in the loop; with one
+// orientation per lane two interleaved accumulators halve the dependency
 // chain); padded segments need no per-photon bounds test. The photon sum is
 // formed in FP64 once per pair. s_d = phi_d when need_scaling &&
 // (iteration > 1 || known_scale), else the rescale factor (max_prob.c:122-128).
-__global__ void __launch_bounds__(256, 6) estep_kernel(
+constexpr int ECH = LW == 1 ? 2 : 1;  // accumulator chains per orientation
+constexpr int ESTEP_MINB = LW == 1 ? 6 : (LW == 2 ? 4 : 3);
+
+__global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ quats, int M,
     int R, const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
     const long long *__restrict__ ph_mid, const double *__restrict__ scale, const uint8_t *__restrict__ blacklist,
@@ -127,13 +137,18 @@ __global__ void __launch_bounds__(256, 6) estep_kernel(
 	const int rt = (int)(warp / Nc), dl = (int)(warp - (long long)rt * Nc), d = d0 + dl;
 	if (blacklist[d])
 		return;
-	const int r = rt * TILE + lane;
-	const float *L = logW + (size_t)rt * (P + 1) * TILE + lane;
+	const int r0 = rt * TILE + lane * LW;
+	const float *L = logW + (size_t)rt * (P + 1) * TILE + lane * LW;
 	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
 	// segments start at multiples of 8 words: two 16-byte loads, identical for
 	// every lane (broadcast), bring 8 photon words
 	const uint4 *w4 = reinterpret_cast<const uint4 *>(ph);
-	float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
+	float s[ECH][LW], c[ECH][LW];
+#pragma unroll
+	for (int h = 0; h < ECH; ++h)
+#pragma unroll
+		for (int k = 0; k < LW; ++k)
+			s[h][k] = c[h][k] = 0.f;
 	// the next 8 words are fetched while the current 8 rows are in flight
 	uint4 a = make_uint4(P, P, P, P), b = a;
 	if (beg < mid) {
@@ -141,46 +156,60 @@ __global__ void __launch_bounds__(256, 6) estep_kernel(
 		b = __ldg(w4 + (beg >> 2) + 1);
 	}
 	for (long long j = beg; j < mid; j += 8) {
-		const float v0 = __ldg(L + a.x * TILE), v1 = __ldg(L + a.y * TILE), v2 = __ldg(L + a.z * TILE),
-		            v3 = __ldg(L + a.w * TILE), v4 = __ldg(L + b.x * TILE), v5 = __ldg(L + b.y * TILE),
-		            v6 = __ldg(L + b.z * TILE), v7 = __ldg(L + b.w * TILE);
+		float v[8][LW];
+		ld_row(L + a.x * TILE, v[0]);
+		ld_row(L + a.y * TILE, v[1]);
+		ld_row(L + a.z * TILE, v[2]);
+		ld_row(L + a.w * TILE, v[3]);
+		ld_row(L + b.x * TILE, v[4]);
+		ld_row(L + b.y * TILE, v[5]);
+		ld_row(L + b.z * TILE, v[6]);
+		ld_row(L + b.w * TILE, v[7]);
 		if (j + 8 < mid) {
 			a = __ldg(w4 + ((j + 8) >> 2));
 			b = __ldg(w4 + ((j + 8) >> 2) + 1);
 		}
-		kahan_add(s0, c0, v0);
-		kahan_add(s1, c1, v1);
-		kahan_add(s0, c0, v2);
-		kahan_add(s1, c1, v3);
-		kahan_add(s0, c0, v4);
-		kahan_add(s1, c1, v5);
-		kahan_add(s0, c0, v6);
-		kahan_add(s1, c1, v7);
+#pragma unroll
+		for (int q = 0; q < 8; ++q)
+#pragma unroll
+			for (int k = 0; k < LW; ++k)
+				kahan_add(s[q % ECH][k], c[q % ECH][k], v[q][k]);
 	}
 	for (long long j = mid; j < end; j += 8) {
 		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
 		const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-		float v[8];
+		float v[8][LW];
 #pragma unroll
 		for (int q = 0; q < 8; ++q)
-			v[q] = __ldg(L + (e[q] & IDX_MASK) * TILE);
+			ld_row(L + (e[q] & IDX_MASK) * TILE, v[q]);
 #pragma unroll
-		for (int q = 0; q < 8; q += 2) {
-			kahan_add_count(s0, c0, e[q] >> IDX_BITS, v[q]);
-			kahan_add_count(s1, c1, e[q + 1] >> IDX_BITS, v[q + 1]);
-		}
+		for (int q = 0; q < 8; ++q)
+#pragma unroll
+			for (int k = 0; k < LW; ++k)
+				kahan_add_count(s[q % ECH][k], c[q % ECH][k], e[q] >> IDX_BITS, v[q][k]);
 	}
-	double acc = 0.;
-	if (r < R) {
-		const double sd = use_scale ? scale[d] : scalars[0];
-		acc = dadd(dsub(log(quats[(r / M) * 5 + 4]), dmul(u[r], sd)),
-		           dadd(kahan_value(s0, c0), kahan_value(s1, c1)));
-	}
-	pval[((size_t)rt * Nc + dl) * TILE + lane] = acc;
+	const double sd = use_scale ? scale[d] : scalars[0];
+	double acc[LW];
 	// tile maximum and its lowest orientation index (strict > in ascending r,
 	// as the running maximum of max_prob.c:199-202)
-	double m = (r < R && acc > MAX_EXP_START) ? acc : MAX_EXP_START;
-	int am = (r < R && acc > MAX_EXP_START) ? r : -1;
+	double m = MAX_EXP_START;
+	int am = -1;
+#pragma unroll
+	for (int k = 0; k < LW; ++k) {
+		const int r = r0 + k;
+		acc[k] = 0.;
+		if (r < R) {
+			double ph_sum = kahan_value(s[0][k], c[0][k]);
+			if (ECH == 2)
+				ph_sum = dadd(ph_sum, kahan_value(s[ECH - 1][k], c[ECH - 1][k]));
+			acc[k] = dadd(dsub(log(quats[(r / M) * 5 + 4]), dmul(u[r], sd)), ph_sum);
+			if (acc[k] > m) {
+				m = acc[k];
+				am = r;
+			}
+		}
+	}
+	st_row(pval + ((size_t)rt * Nc + dl) * TILE + lane * LW, acc);
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		double om = __shfl_xor_sync(FULL, m, o);
@@ -218,20 +247,24 @@ __global__ void __launch_bounds__(256) norm_kernel(
     double *__restrict__ max_exp, double *__restrict__ p_norm, double *__restrict__ info,
     double *__restrict__ likelihood, double *__restrict__ psum_d, double *__restrict__ quat_norm,
     int *__restrict__ num_prob) {
-	constexpr int UNR = 4;
+	constexpr int UNR = LW == 1 ? 4 : 2;
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	const size_t tstride = (size_t)Nc * TILE, pstride = (size_t)(Nc + 1) * TILE;
+	float zero[LW];
+#pragma unroll
+	for (int k = 0; k < LW; ++k)
+		zero[k] = 0.f;
 	if (warp == Nc) {  // the zero row that padding words of the M-step point at
 		for (int rt = 0; rt < RT; ++rt)
-			Pst[rt * pstride + (size_t)Nc * TILE + lane] = 0.f;
+			st_row(Pst + rt * pstride + (size_t)Nc * TILE + lane * LW, zero);
 		return;
 	}
 	if (warp > Nc)
 		return;
 	const int dl = warp, d = d0 + dl;
-	const double *pv = pval + (size_t)dl * TILE + lane;
-	float *ps = Pst + (size_t)dl * TILE + lane;
+	const double *pv = pval + (size_t)dl * TILE + lane * LW;
+	float *ps = Pst + (size_t)dl * TILE + lane * LW;
 	const bool bl = blacklist[d] != 0;
 
 	double m = MAX_EXP_START;
@@ -256,7 +289,7 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	}
 	if (bl || m == MAX_EXP_START) {
 		for (int rt = 0; rt < RT; ++rt)
-			ps[rt * pstride] = 0.f;
+			st_row(ps + rt * pstride, zero);
 		if (lane == 0) {
 			rmax[d] = -1;
 			max_exp[d] = MAX_EXP_START;
@@ -278,18 +311,24 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	double s = 0.;
 	int cnt = 0;
 	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
-		double v[UNR];
+		double v[UNR][LW];
 #pragma unroll
 		for (int k = 0; k < UNR; ++k)
-			v[k] = (rt0 + k < RT) ? pv[(rt0 + k) * tstride] : 0.;
+			if (rt0 + k < RT)
+				ld_row(pv + (rt0 + k) * tstride, v[k]);
 #pragma unroll
 		for (int k = 0; k < UNR; ++k) {
-			const int r = (rt0 + k) * TILE + lane;
-			if (rt0 + k < RT && r < R) {
-				bool kept = (r <= rstar) ? (v[k] > lo) : (dadd(v[k], thr) > m);
-				if (kept) {
-					s += exp(dmul(b, dsub(v[k], m)));
-					cnt++;
+			if (rt0 + k >= RT)
+				break;
+#pragma unroll
+			for (int e = 0; e < LW; ++e) {
+				const int r = (rt0 + k) * TILE + lane * LW + e;
+				if (r < R) {
+					bool kept = (r <= rstar) ? (v[k][e] > lo) : (dadd(v[k][e], thr) > m);
+					if (kept) {
+						s += exp(dmul(b, dsub(v[k][e], m)));
+						cnt++;
+					}
 				}
 			}
 		}
@@ -305,39 +344,45 @@ __global__ void __launch_bounds__(256) norm_kernel(
 	for (int k = 0; k < (MULTI ? MAX_MODES : 1); ++k)
 		qn[k] = 0.;
 	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
-		double v[UNR];
+		double v[UNR][LW];
 #pragma unroll
 		for (int k = 0; k < UNR; ++k)
-			v[k] = (rt0 + k < RT) ? pv[(rt0 + k) * tstride] : 0.;
+			if (rt0 + k < RT)
+				ld_row(pv + (rt0 + k) * tstride, v[k]);
 #pragma unroll
 		for (int k = 0; k < UNR; ++k) {
 			const int rt = rt0 + k;
 			if (rt >= RT)
 				break;
-			const int r = rt * TILE + lane;
-			float out = 0.f;
-			if (r < R) {
-				bool kept = (r <= rstar) ? (v[k] > lo) : (dadd(v[k], thr) > m);
-				if (kept) {
-					double P = exp(dmul(b, dsub(v[k], m))) / s;
-					ll += P * (v[k] - sf);
-					if (psum_d_on)
-						pd += P * u[r] * rescale;
-					if (!(P < PROB_MIN)) {
-						double w = quats[(r / M) * 5 + 4];
-						inf += P * log(P / w * M);
-						if (MULTI) {
-							int mode = r % M;
+			float out[LW];
 #pragma unroll
-							for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
-								if (q == mode)
-									qn[q] += P;
+			for (int e = 0; e < LW; ++e) {
+				const int r = rt * TILE + lane * LW + e;
+				out[e] = 0.f;
+				if (r < R) {
+					const double x = v[k][e];
+					bool kept = (r <= rstar) ? (x > lo) : (dadd(x, thr) > m);
+					if (kept) {
+						double P = exp(dmul(b, dsub(x, m))) / s;
+						ll += P * (x - sf);
+						if (psum_d_on)
+							pd += P * u[r] * rescale;
+						if (!(P < PROB_MIN)) {
+							double w = quats[(r / M) * 5 + 4];
+							inf += P * log(P / w * M);
+							if (MULTI) {
+								int mode = r % M;
+#pragma unroll
+								for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
+									if (q == mode)
+										qn[q] += P;
+							}
 						}
+						out[e] = (P > PROB_MIN) ? (float)P : -(float)P;
 					}
-					out = (P > PROB_MIN) ? (float)P : -(float)P;
 				}
 			}
-			ps[rt * pstride] = out;
+			st_row(ps + rt * pstride, out);
 		}
 	}
 	ll = warp_sum(ll);
@@ -369,20 +414,29 @@ __global__ void __launch_bounds__(256) psum_r_kernel(const float *__restrict__ P
 	__shared__ double s[8][TILE];
 	const int rt = blockIdx.x, split = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int beg = split * frames_per_split, end = min(Nc, beg + frames_per_split);
-	double acc = 0.;
-	const float *p = Pst + (size_t)rt * (Nc + 1) * TILE + lane;
+	double acc[LW];
+#pragma unroll
+	for (int k = 0; k < LW; ++k)
+		acc[k] = 0.;
+	const float *p = Pst + (size_t)rt * (Nc + 1) * TILE + lane * LW;
 	for (int dl = beg + w; dl < end; dl += 8) {
-		double v = fabs((double)p[(size_t)dl * TILE]);
-		acc += need_scaling ? v * scale[d0 + dl] : v;
+		float v[LW];
+		ld_row(p + (size_t)dl * TILE, v);
+		const double f = need_scaling ? scale[d0 + dl] : 1.;
+#pragma unroll
+		for (int k = 0; k < LW; ++k)
+			acc[k] += need_scaling ? fabs((double)v[k]) * f : fabs((double)v[k]);
 	}
-	s[w][lane] = acc;
+#pragma unroll
+	for (int k = 0; k < LW; ++k)
+		s[w][lane * LW + k] = acc[k];
 	__syncthreads();
-	if (w == 0) {
+	for (int j = threadIdx.x; j < TILE; j += blockDim.x) {
 		double t = 0.;
 #pragma unroll
 		for (int k = 0; k < 8; ++k)
-			t += s[k][lane];
-		part[(size_t)split * R_pad + rt * TILE + lane] = t;
+			t += s[k][j];
+		part[(size_t)split * R_pad + rt * TILE + j] = t;
 	}
 }
 
@@ -398,14 +452,16 @@ __global__ void psum_r_reduce_kernel(const double *__restrict__ part, int nsplit
 }
 
 // ---------------------------------------------------------------------------
-// (e1) M-step back-projection: T[tile][p][lane] += sum_(d,c) c * P_dr
+// (e1) M-step back-projection: T[tile][p][j] += sum_(d,c) c * P_dr
 // ---------------------------------------------------------------------------
 // Gather form of update_tomogram_nobg (max_update.c:142-230): one warp per
 // (orientation tile, pixel), walking the pixel's list of frames (pixels with
-// mask < 2 only) and reading one 128-byte row of P per entry; count-1 and
-// multi-photon segments as in the E-step, compensated FP32 sums. No atomics;
-// pixels are visited heaviest first for balance.
-__global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Pst, int Nc,
+// mask < 2 only) and reading one row of P per entry (one LW-wide vector load
+// per lane); count-1 and multi-photon segments as in the E-step, compensated
+// FP32 sums. No atomics; pixels are visited heaviest first for balance.
+constexpr int MSTEP_MINB = LW == 4 ? 4 : 6;
+
+__global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__restrict__ Pst, int Nc,
                                                      const uint32_t *__restrict__ cs,
                                                      const long long *__restrict__ cs_off,
                                                      const long long *__restrict__ cs_mid,
@@ -415,42 +471,59 @@ __global__ void __launch_bounds__(256) mstep_kernel(const float *__restrict__ Ps
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * npix)
 		return;
-	const int rt = (int)(warp / npix), k = (int)(warp - (long long)rt * npix);
-	const int p = pix[k];
-	const float *Pr = Pst + (size_t)rt * (Nc + 1) * TILE + lane;
+	const int rt = (int)(warp / npix), kp = (int)(warp - (long long)rt * npix);
+	const int p = pix[kp];
+	const float *Pr = Pst + (size_t)rt * (Nc + 1) * TILE + lane * LW;
 	const long long beg = cs_off[p], mid = cs_mid[p], end = cs_off[p + 1];
 	const uint4 *w4 = reinterpret_cast<const uint4 *>(cs);
-	float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
-#pragma unroll 2
+	float s[ECH][LW], c[ECH][LW];
+#pragma unroll
+	for (int h = 0; h < ECH; ++h)
+#pragma unroll
+		for (int k = 0; k < LW; ++k)
+			s[h][k] = c[h][k] = 0.f;
+#pragma unroll(LW == 1 ? 2 : 1)
 	for (long long j = beg; j < mid; j += 8) {
 		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
-		const float v0 = __ldg(Pr + a.x * TILE), v1 = __ldg(Pr + a.y * TILE), v2 = __ldg(Pr + a.z * TILE),
-		            v3 = __ldg(Pr + a.w * TILE), v4 = __ldg(Pr + b.x * TILE), v5 = __ldg(Pr + b.y * TILE),
-		            v6 = __ldg(Pr + b.z * TILE), v7 = __ldg(Pr + b.w * TILE);
-		kahan_add(s0, c0, fmaxf(v0, 0.f));
-		kahan_add(s1, c1, fmaxf(v1, 0.f));
-		kahan_add(s0, c0, fmaxf(v2, 0.f));
-		kahan_add(s1, c1, fmaxf(v3, 0.f));
-		kahan_add(s0, c0, fmaxf(v4, 0.f));
-		kahan_add(s1, c1, fmaxf(v5, 0.f));
-		kahan_add(s0, c0, fmaxf(v6, 0.f));
-		kahan_add(s1, c1, fmaxf(v7, 0.f));
+		float v[8][LW];
+		ld_row(Pr + a.x * TILE, v[0]);
+		ld_row(Pr + a.y * TILE, v[1]);
+		ld_row(Pr + a.z * TILE, v[2]);
+		ld_row(Pr + a.w * TILE, v[3]);
+		ld_row(Pr + b.x * TILE, v[4]);
+		ld_row(Pr + b.y * TILE, v[5]);
+		ld_row(Pr + b.z * TILE, v[6]);
+		ld_row(Pr + b.w * TILE, v[7]);
+#pragma unroll
+		for (int q = 0; q < 8; ++q)
+#pragma unroll
+			for (int k = 0; k < LW; ++k)
+				kahan_add(s[q % ECH][k], c[q % ECH][k], fmaxf(v[q][k], 0.f));
 	}
 	for (long long j = mid; j < end; j += 8) {
 		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
 		const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-		float v[8];
+		float v[8][LW];
 #pragma unroll
 		for (int q = 0; q < 8; ++q)
-			v[q] = fmaxf(__ldg(Pr + (e[q] & IDX_MASK) * TILE), 0.f);
+			ld_row(Pr + (e[q] & IDX_MASK) * TILE, v[q]);
 #pragma unroll
-		for (int q = 0; q < 8; q += 2) {
-			kahan_add_count(s0, c0, e[q] >> IDX_BITS, v[q]);
-			kahan_add_count(s1, c1, e[q + 1] >> IDX_BITS, v[q + 1]);
-		}
+		for (int q = 0; q < 8; ++q)
+#pragma unroll
+			for (int k = 0; k < LW; ++k)
+				kahan_add_count(s[q % ECH][k], c[q % ECH][k], e[q] >> IDX_BITS, fmaxf(v[q][k], 0.f));
 	}
-	float *out = T + ((size_t)rt * P + p) * TILE + lane;
-	*out = (float)((double)*out + dadd(kahan_value(s0, c0), kahan_value(s1, c1)));
+	float *out = T + ((size_t)rt * P + p) * TILE + lane * LW;
+	float o[LW];
+	ld_row_rw(out, o);
+#pragma unroll
+	for (int k = 0; k < LW; ++k) {
+		double t = kahan_value(s[0][k], c[0][k]);
+		if (ECH == 2)
+			t = dadd(t, kahan_value(s[ECH - 1][k], c[ECH - 1][k]));
+		o[k] = (float)((double)o[k] + t);
+	}
+	st_row(out, o);
 }
 
 // ---------------------------------------------------------------------------
@@ -478,18 +551,28 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 	__shared__ double s_ps[TILE];
 	__shared__ float s_tile[PB][TILE + 1];
 	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
-	if (t < TILE) {
-		int r = rt * TILE + t;
+	for (int j = t; j < TILE; j += blockDim.x) {
+		int r = rt * TILE + j;
 		int rr = r < R ? r : 0;
-		rot_from_quat(&quats[(rr / M) * 5], s_rot[t]);
-		s_mode[t] = rr % M;
-		s_ps[t] = r < R ? psum_r[r] : 0.;
+		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
+		s_mode[j] = rr % M;
+		s_ps[j] = r < R ? psum_r[r] : 0.;
 	}
 	{
 		const int w = t >> 5, lane = t & 31;
 		for (int row = w; row < PB; row += 8) {
 			int pp = p0 + row;
-			s_tile[row][lane] = pp < P ? T[((size_t)rt * P + pp) * TILE + lane] : 0.f;
+			float v[LW];
+			if (pp < P) {
+				ld_row(T + ((size_t)rt * P + pp) * TILE + lane * LW, v);
+			} else {
+#pragma unroll
+				for (int k = 0; k < LW; ++k)
+					v[k] = 0.f;
+			}
+#pragma unroll
+			for (int k = 0; k < LW; ++k)
+				s_tile[row][lane * LW + k] = v[k];
 		}
 	}
 	__syncthreads();
@@ -501,7 +584,7 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 	const double center = (double)(S / 2);
 	long long o[8];
 	corner_offsets(S, o);
-	for (int k = 0; k < 8; ++k) {
+	for (int k = 0; k < TILE / 4; ++k) {
 		const int j = g + 4 * k;
 		const double ps = s_ps[j];
 		if (!(ps > 0.))
