@@ -48,7 +48,9 @@ extern "C" int dfg_create(int device, dfg_ctx **out) {
 		return DFG_ERR_CUDA;
 	dfg_ctx *ctx = new dfg_ctx();
 	ctx->device = device;
-	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+	if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+	    ctx->num_sms < 1 ||
+	    cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
 		delete ctx;
 		return DFG_ERR_CUDA;
 	}
@@ -102,15 +104,6 @@ extern "C" int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, 
 	CK(upload(ctx->qvals, qvals, 3 * (size_t)num_pix, ctx->stream));
 	CK(upload(ctx->corr, corr, (size_t)num_pix, ctx->stream));
 	CK(upload(ctx->mask, raw_mask, (size_t)num_pix, ctx->stream));
-	{
-		std::vector<double4> g;
-		for (int t = 0; t < num_pix; ++t)
-			if (raw_mask[t] < 1)
-				g.push_back(make_double4(qvals[3 * (size_t)t], qvals[3 * (size_t)t + 1], qvals[3 * (size_t)t + 2],
-				                         corr[t]));
-		ctx->n_good = (int)g.size();
-		CK(upload(ctx->good, g.data(), g.size(), ctx->stream));
-	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->chunks_R = -1;  // photon lists depend on the mask
 	if (ctx->N > 0) {
@@ -448,6 +441,7 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	}
 	CK(ctx->T.ensure(tiles_px));
 	CK(ctx->u.ensure((size_t)ctx->R_pad));
+	CK(ctx->logw.ensure((size_t)ctx->R_pad));
 	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
 	CK(ctx->scalars.ensure(8));
 	CK(ctx->red_part.ensure(std::max<size_t>(blocks_for((long long)ctx->M * ctx->V, 256), 1024)));
@@ -504,14 +498,13 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 
 	// slices, u_r, rescale (calculate_rescale, max_prob.c:3-64)
 	phase_begin(ctx, PH_SLICE);
-	slice_log_kernel<double><<<dim3(nblk, RT), 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, P,
-	                                                         ctx->model1.p, S, V, ctx->logW.p);
-	CKL("slice_log_kernel");
-	u_sequential_kernel<double><<<blocks_for(R, 128), 128, 0, st>>>(ctx->quats.p, M, R, ctx->good.p, ctx->n_good,
-	                                                               ctx->model1.p, S, V, ctx->u.p);
-	CKL("u_sequential_kernel");
-	rescale_kernel<<<1, 32, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
+	slice_u_kernel<double><<<RT, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
+	                                           ctx->model1.p, S, V, ctx->logW.p, ctx->u.p);
+	CKL("slice_u_kernel");
+	rescale_kernel<<<1, 256, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
 	CKL("rescale_kernel");
+	logw_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->quats.p, M, R, ctx->logw.p);
+	CKL("logw_kernel");
 	phase_end(ctx, PH_SLICE, 3);
 
 	CK(cudaMemsetAsync(ctx->T.p, 0, (size_t)RT * P * TILE * sizeof(float), st));
@@ -527,7 +520,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		{
 			long long warps = (long long)RT * Nc;
 			estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
-			    ctx->logW.p, ctx->u.p, ctx->quats.p, M, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
+			    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
 			    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
 			    ctx->targ.p);
 			CKL("estep_kernel");
@@ -537,13 +530,13 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		phase_begin(ctx, PH_NORM);
 		if (M > 1)
 			norm_kernel<true><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
-			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p,
+			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
 			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
 			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
 			    ctx->num_prob.p);
 		else
 			norm_kernel<false><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
-			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->quats.p, ctx->u.p, ctx->beta.p,
+			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
 			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
 			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
 			    ctx->num_prob.p);

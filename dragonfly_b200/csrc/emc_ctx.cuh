@@ -73,6 +73,7 @@ using namespace dfg;
 
 struct dfg_ctx {
 	int device = 0;
+	int num_sms = 0;  // streaming multiprocessors of the device (persistent grids)
 	cudaStream_t stream = nullptr;
 	std::string err;
 
@@ -81,8 +82,6 @@ struct dfg_ctx {
 	DevBuf<double> qvals, corr;
 	DevBuf<uint8_t> mask;
 	std::vector<uint8_t> h_mask;
-	DevBuf<double4> good;  // (qx, qy, qz, corr) of mask == 0 pixels, in pixel order
-	int n_good = 0;
 
 	// frames
 	int N = 0;
@@ -114,6 +113,7 @@ struct dfg_ctx {
 	// work buffers
 	DevBuf<float> logW, Pst, T;
 	DevBuf<double> u, pval, psum_r, psum_part, scalars, red_part;
+	DevBuf<double> logw;  // log w_r per orientation
 	DevBuf<int> rmax, num_prob, targ;
 	DevBuf<double> tmax;  // per (tile, frame) maximum of pval and its first orientation
 	DevBuf<double> info, likelihood, max_exp, p_norm, psum_d, quat_norm;

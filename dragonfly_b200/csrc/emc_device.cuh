@@ -7,107 +7,112 @@
 namespace dfg {
 
 // ---------------------------------------------------------------------------
-// (a) slice generation: logW[tile][p][j] = log(W_r), r = tile * TILE + j
+// (a) slice generation: logW[tile][p][j] = log(W_r[p]) and u_r, r = tile * TILE + j
 // ---------------------------------------------------------------------------
-// Block = one orientation tile x PB pixels, 256 threads: thread (i = t % 64,
-// g = t / 64) computes pixel i for orientations g, g+4, ..., so a warp walks
-// 32 neighbouring pixels of one orientation (neighbouring model reads).
-// The tile is staged in shared memory and stored as coalesced rows.
+// Block = one orientation tile; it walks every pixel in chunks of SB pixels,
+// in pixel order. Per chunk the 256 threads compute W for SB pixels x TILE
+// orientations into shared memory (thread (i = t % SB, g = t / SB) takes
+// pixel i of orientations g, g + 256/SB, ..., so a warp walks 32 neighbouring
+// pixels of one orientation); then thread j < TILE adds the chunk's mask-0
+// values of orientation j to u_j in pixel order, which keeps u_r
+// bit-identical to the reference's sequential sum (max_prob.c:32-38), while
+// the warps store log W as coalesced rows (max_prob.c:94-97).
+constexpr int SB = 32;
+
 template <typename MT>
-__global__ void __launch_bounds__(256) slice_log_kernel(
+__global__ void __launch_bounds__(256) slice_u_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
-    const double *__restrict__ corr, int P, const MT *__restrict__ model, long long S, long long V,
-    float *__restrict__ logW) {
+    const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
+    long long S, long long V, float *__restrict__ logW, double *__restrict__ u) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
-	__shared__ float s_tile[PB][TILE + 1];
-	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
+	__shared__ double s_w[SB][TILE + 1];
+	__shared__ double s_q[SB][4];
+	__shared__ int s_m[SB];
+	const int t = threadIdx.x, rt = blockIdx.x;
 	for (int j = t; j < TILE; j += blockDim.x) {
 		int r = rt * TILE + j;
 		int rr = r < R ? r : 0;
 		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
 		s_mode[j] = rr % M;
 	}
-	__syncthreads();
-	const int i = t & (PB - 1), g = t >> 6, p = p0 + i;
-	const bool pix = p < P;
-	double qx = 0., qy = 0., qz = 0., cr = 1.;
-	if (pix) {
-		qx = qvals[3 * (size_t)p]; qy = qvals[3 * (size_t)p + 1]; qz = qvals[3 * (size_t)p + 2];
-		cr = corr[p];
-	}
 	const double center = (double)(S / 2);
+	const int i = t % SB, g = t / SB, w = t >> 5, lane = t & 31;
+	double acc = 0.;
+	for (int p0 = 0; p0 < P; p0 += SB) {
+		if (t < SB) {
+			const int p = p0 + t;
+			if (p < P) {
+				s_q[t][0] = qvals[3 * (size_t)p];
+				s_q[t][1] = qvals[3 * (size_t)p + 1];
+				s_q[t][2] = qvals[3 * (size_t)p + 2];
+				s_q[t][3] = corr[p];
+				s_m[t] = mask[p];
+			} else {
+				s_m[t] = -1;
+			}
+		}
+		__syncthreads();
+		if (s_m[i] >= 0) {
+			const double qx = s_q[i][0], qy = s_q[i][1], qz = s_q[i][2], cr = s_q[i][3];
 #pragma unroll 2
-	for (int k = 0; k < TILE / 4; ++k) {
-		const int j = g + 4 * k;
-		if (pix) {
-			Cell c = locate(s_rot[j], qx, qy, qz, center, S);
-			s_tile[i][j] = (float)log(interp(c, model + (size_t)s_mode[j] * V, S, cr));
+			for (int j = g; j < TILE; j += 256 / SB) {
+				Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+				s_w[i][j] = interp(c, model + (size_t)s_mode[j] * V, S, cr);
+			}
 		}
-	}
-	__syncthreads();
-	// coalesced store: warp w writes rows w, w+8, ...; a lane its LW values
-	const int w = t >> 5, lane = t & 31;
-	for (int row = w; row < PB; row += 8) {
-		int pp = p0 + row;
-		if (pp < P) {
-			float v[LW];
+		__syncthreads();
+		if (t < TILE) {
+#pragma unroll 8
+			for (int k = 0; k < SB; ++k)
+				if (s_m[k] == 0)
+					acc = dadd(acc, s_w[k][t]);
+		}
+		for (int row = w; row < SB; row += 8) {
+			const int pp = p0 + row;
+			if (pp < P) {
+				float v[LW];
 #pragma unroll
-			for (int k = 0; k < LW; ++k)
-				v[k] = s_tile[row][lane * LW + k];
-			st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + lane * LW, v);
+				for (int k = 0; k < LW; ++k)
+					v[k] = (float)log(s_w[row][lane * LW + k]);
+				st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + lane * LW, v);
+			}
 		}
+		__syncthreads();
 	}
+	if (t < TILE && rt * TILE + t < R)
+		u[rt * TILE + t] = acc;
 }
 
-// u_r = sum of W over mask == 0 pixels, added in pixel order (max_prob.c:32-38).
-// One thread per orientation walks the pixels sequentially, so u_r is
-// bit-identical to the reference's (frames without photons are ranked by u_r
-// alone, and orientations related by a symmetry of the model tie exactly).
-// The mask-0 pixels come packed as (qx, qy, qz, corr), in pixel order; four
-// interpolations are in flight while the additions stay sequential.
-template <typename MT>
-__global__ void __launch_bounds__(128) u_sequential_kernel(const double *__restrict__ quats, int M, int R,
-                                                           const double4 *__restrict__ good, int n_good,
-                                                           const MT *__restrict__ model, long long S, long long V,
-                                                           double *__restrict__ u) {
+// log w_r per orientation, so that no pair evaluates a logarithm of its
+// orientation weight (max_prob.c:122).
+__global__ void logw_kernel(const double *__restrict__ quats, int M, int R, double *__restrict__ logw) {
 	const int r = blockIdx.x * blockDim.x + threadIdx.x;
-	if (r >= R)
-		return;
-	double rot[9];
-	rot_from_quat(&quats[(r / M) * 5], rot);
-	const MT *m = model + (size_t)(r % M) * V;
-	const double center = (double)(S / 2);
-	double acc = 0.;
-	int k = 0;
-	for (; k + 4 <= n_good; k += 4) {
-		double w[4];
-#pragma unroll
-		for (int q = 0; q < 4; ++q) {
-			const double4 g = good[k + q];
-			w[q] = interp(locate(rot, g.x, g.y, g.z, center, S), m, S, g.w);
-		}
-#pragma unroll
-		for (int q = 0; q < 4; ++q)
-			acc = dadd(acc, w[q]);
-	}
-	for (; k < n_good; ++k) {
-		const double4 g = good[k];
-		acc = dadd(acc, interp(locate(rot, g.x, g.y, g.z, center, S), m, S, g.w));
-	}
-	u[r] = acc;
+	if (r < R)
+		logw[r] = log(quats[(r / M) * 5 + 4]);
 }
 
 // rescale = mean_count / sum_r w_r u_r * M, summed in orientation order
-// (max_prob.c:40, 55-60); a single thread.
-__global__ void rescale_kernel(const double *__restrict__ u, const double *__restrict__ quats, int M, int R,
-                               double mean_count, double *__restrict__ scalars) {
-	if (threadIdx.x != 0 || blockIdx.x != 0)
-		return;
+// (max_prob.c:40, 55-60): the block stages 256 products at a time in shared
+// memory and one thread adds them in order.
+__global__ void __launch_bounds__(256) rescale_kernel(const double *__restrict__ u, const double *__restrict__ quats,
+                                                      int M, int R, double mean_count, double *__restrict__ scalars) {
+	__shared__ double s_p[256];
 	double total = 0.;
-	for (int r = 0; r < R; ++r)
-		total = dadd(total, dmul(quats[(r / M) * 5 + 4], u[r]));
-	scalars[0] = mean_count / total * M;
+	for (int r0 = 0; r0 < R; r0 += 256) {
+		const int r = r0 + threadIdx.x;
+		s_p[threadIdx.x] = r < R ? dmul(quats[(r / M) * 5 + 4], u[r]) : 0.;
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			const int n = min(256, R - r0);
+#pragma unroll 8
+			for (int k = 0; k < n; ++k)
+				total = dadd(total, s_p[k]);
+		}
+		__syncthreads();
+	}
+	if (threadIdx.x == 0)
+		scalars[0] = mean_count / total * M;
 }
 
 // ---------------------------------------------------------------------------
@@ -125,11 +130,11 @@ constexpr int ECH = LW == 1 ? 2 : 1;  // accumulator chains per orientation
 constexpr int ESTEP_MINB = LW == 1 ? 6 : (LW == 2 ? 4 : 3);
 
 __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
-    const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ quats, int M,
-    int R, const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
-    const long long *__restrict__ ph_mid, const double *__restrict__ scale, const uint8_t *__restrict__ blacklist,
-    int d0, int Nc, int use_scale, const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval,
-    double *__restrict__ tmax, int *__restrict__ targ) {
+    const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ logw, int R,
+    const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off, const long long *__restrict__ ph_mid,
+    const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
+    const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval, double *__restrict__ tmax,
+    int *__restrict__ targ) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * Nc)
@@ -202,7 +207,7 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 			double ph_sum = kahan_value(s[0][k], c[0][k]);
 			if (ECH == 2)
 				ph_sum = dadd(ph_sum, kahan_value(s[ECH - 1][k], c[ECH - 1][k]));
-			acc[k] = dadd(dsub(log(quats[(r / M) * 5 + 4]), dmul(u[r], sd)), ph_sum);
+			acc[k] = dadd(dsub(logw[r], dmul(u[r], sd)), ph_sum);
 			if (acc[k] > m) {
 				m = acc[k];
 				am = r;
@@ -235,13 +240,16 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 // maximiser r* with pval > max - 14/beta, and every r after r* with
 // pval + 14/beta > max. The maximiser is the lowest index reaching the maximum;
 // it comes from the per-tile maxima the E-step wrote (lanes take tiles lane,
-// lane + 32, ...). P_dr = exp(beta (pval - max)) / p_norm (max_update.c:96-98);
-// likelihood, psum_d, info and quat_norm follow max_update.c:105-130. The two
-// passes over a frame's log-likelihoods keep UNR tile rows in flight per lane.
+// lane + 32, ...). P_dr = exp(beta (pval - max)) / p_norm (max_update.c:96-98),
+// formed as a product with 1 / p_norm; likelihood, psum_d, info and quat_norm
+// follow max_update.c:105-130, with log(P / w_r * M) written as
+// beta (pval - max) - log p_norm + log M - log w_r so that no pair evaluates a
+// logarithm. The two passes over a frame's log-likelihoods keep UNR tile rows
+// in flight per lane.
 template <bool MULTI>
-__global__ void __launch_bounds__(256) norm_kernel(
+__global__ void __launch_bounds__(256, 3) norm_kernel(
     const double *__restrict__ pval, const double *__restrict__ tmax, const int *__restrict__ targ, int RT,
-    int Nc, int d0, int R, int M, const double *__restrict__ quats, const double *__restrict__ u,
+    int Nc, int d0, int R, int M, const double *__restrict__ logw, const double *__restrict__ u,
     const double *__restrict__ beta, const double *__restrict__ sum_fact, const uint8_t *__restrict__ blacklist,
     int psum_d_on, const double *__restrict__ scalars, float *__restrict__ Pst, int *__restrict__ rmax,
     double *__restrict__ max_exp, double *__restrict__ p_norm, double *__restrict__ info,
@@ -338,6 +346,7 @@ __global__ void __launch_bounds__(256) norm_kernel(
 		cnt += __shfl_xor_sync(FULL, cnt, o);
 
 	const double rescale = scalars[0], sf = sum_fact[d];
+	const double inv_s = 1. / s, cinf = log((double)M) - log(s);
 	double ll = 0., pd = 0., inf = 0.;
 	double qn[MULTI ? MAX_MODES : 1];
 #pragma unroll
@@ -363,13 +372,13 @@ __global__ void __launch_bounds__(256) norm_kernel(
 					const double x = v[k][e];
 					bool kept = (r <= rstar) ? (x > lo) : (dadd(x, thr) > m);
 					if (kept) {
-						double P = exp(dmul(b, dsub(x, m))) / s;
+						const double y = dmul(b, dsub(x, m));
+						const double P = exp(y) * inv_s;
 						ll += P * (x - sf);
 						if (psum_d_on)
 							pd += P * u[r] * rescale;
 						if (!(P < PROB_MIN)) {
-							double w = quats[(r / M) * 5 + 4];
-							inf += P * log(P / w * M);
+							inf += P * (y + cinf - logw[r]);
 							if (MULTI) {
 								int mode = r % M;
 #pragma unroll
