@@ -498,9 +498,35 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 
 	// slices, u_r, rescale (calculate_rescale, max_prob.c:3-64)
 	phase_begin(ctx, PH_SLICE);
-	slice_u_kernel<double><<<RT, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
-	                                           ctx->model1.p, S, V, ctx->logW.p, ctx->u.p);
-	CKL("slice_u_kernel");
+	{
+		// whole tiles when they give every SM two blocks; else the largest
+		// orientation block that does (16 at least)
+		int ob = ctx->slice_block;
+		if (ob == 0) {
+			ob = 16;
+			for (int c : {TILE, 64, 32})
+				if (c <= TILE && R_pad / c >= 2 * ctx->num_sms) {
+					ob = c;
+					break;
+				}
+		}
+		const int nb = R_pad / ob;
+#define DFG_SLICE(OBV)                                                                                        \
+	slice_u_kernel<double, OBV><<<nb, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, \
+	                                                ctx->model1.p, S, V, ctx->logW.p, ctx->u.p)
+		if (ob == TILE)
+			slice_u_tile_kernel<double><<<RT, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p,
+			                                                ctx->mask.p, P, ctx->model1.p, S, V, ctx->logW.p,
+			                                                ctx->u.p);
+		else if (ob == 64)
+			DFG_SLICE(TILE >= 64 ? 64 : 16);
+		else if (ob == 32)
+			DFG_SLICE(32);
+		else
+			DFG_SLICE(16);
+#undef DFG_SLICE
+		CKL("slice_u_kernel");
+	}
 	rescale_kernel<<<1, 256, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
 	CKL("rescale_kernel");
 	logw_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->quats.p, M, R, ctx->logw.p);
@@ -872,6 +898,13 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 	}
 	if (!strcmp(key, "timing")) {
 		ctx->timing = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "slice_block")) {
+		const int v = (int)value;
+		NEED(v == 0 || ((v == 16 || v == 32 || v == 64 || v == TILE) && v <= TILE), DFG_ERR_ARG,
+		     "slice_block must be 0 (automatic), 16, 32, 64 (at most %d) or %d", TILE, TILE);
+		ctx->slice_block = v;
 		return DFG_OK;
 	}
 	return ctx->fail(DFG_ERR_ARG, "unknown option '%s'", key);

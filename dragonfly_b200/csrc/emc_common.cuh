@@ -163,6 +163,70 @@ __device__ __forceinline__ double kahan_value(float s, float comp) {
 	return isinf(s) ? (double)s : (double)s - (double)comp;
 }
 
+// Pairs of FP32 values in one 64-bit register, for the paired FP32
+// instructions of sm_100 (add/sub/fma/mul.f32x2, round to nearest per
+// component): a compensated addition of two orientations costs four
+// instructions instead of eight, with results identical to the scalar form.
+typedef unsigned long long f32x2;
+constexpr int NPAIR = LW / 2 > 0 ? LW / 2 : 1;  // pairs per lane
+
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+	f32x2 d;
+	asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+	return d;
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+	f32x2 d;
+	asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+	return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+	f32x2 d;
+	asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+	return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+	f32x2 d;
+	asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+	return d;
+}
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
+	f32x2 d;
+	asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+	return d;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 a, float &lo, float &hi) {
+	asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+}
+
+__device__ __forceinline__ void kahan_add2(f32x2 &s, f32x2 &comp, f32x2 x) {
+	const f32x2 y = f2_sub(x, comp);
+	const f32x2 t = f2_add(s, y);
+	comp = f2_sub(f2_sub(t, s), y);
+	s = t;
+}
+
+// count * v added exactly, as kahan_add_count, for a pair of orientations
+__device__ __forceinline__ void kahan_add_count2(f32x2 &s, f32x2 &comp, uint32_t count, f32x2 v) {
+	const float c = __fsub_rn(__int_as_float(0x4B000000u | count), 8388608.f);
+	const f32x2 cc = f2_pack(c, c);
+	const f32x2 p = f2_mul(cc, v);
+	const f32x2 e = f2_fma(cc, v, p ^ 0x8000000080000000ull);  // c v - p
+	kahan_add2(s, comp, p);
+	comp = f2_sub(comp, e);
+}
+
+// LW consecutive floats of one lane as LW / 2 pairs (16- or 8-byte load)
+__device__ __forceinline__ void ld_pairs(const float *__restrict__ p, f32x2 (&v)[NPAIR]) {
+	if constexpr (LW == 4) {
+		const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2 *>(p));
+		v[0] = x.x;
+		v[1] = x.y;
+	} else {
+		v[0] = __ldg(reinterpret_cast<const unsigned long long *>(p));
+	}
+}
+
 // LW consecutive values of one lane as a single vector access (p aligned to
 // LW elements). Read-only loads go through the non-coherent path.
 __device__ __forceinline__ void ld_row(const float *__restrict__ p, float (&v)[LW]) {

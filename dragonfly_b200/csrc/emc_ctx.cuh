@@ -123,6 +123,7 @@ struct dfg_ctx {
 
 	// options and results
 	double pair_budget_mb = 0.;
+	int slice_block = 0;  // orientations per slice block; 0 = automatic
 	bool timing = false;
 	cudaEvent_t ev[2 * PH_COUNT] = {};
 	cudaEvent_t user_ev[8] = {};

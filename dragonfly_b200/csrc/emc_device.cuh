@@ -20,7 +20,7 @@ namespace dfg {
 constexpr int SB = 32;
 
 template <typename MT>
-__global__ void __launch_bounds__(256) slice_u_kernel(
+__global__ void __launch_bounds__(256) slice_u_tile_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
     const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
     long long S, long long V, float *__restrict__ logW, double *__restrict__ u) {
@@ -82,6 +82,88 @@ __global__ void __launch_bounds__(256) slice_u_kernel(
 	}
 	if (t < TILE && rt * TILE + t < R)
 		u[rt * TILE + t] = acc;
+}
+
+// Block = OB consecutive orientations (OB divides TILE); it walks every pixel
+// in chunks of 4096 / OB pixels, in pixel order. Per chunk the 256 threads
+// compute W for the chunk's pixels x OB orientations into shared memory
+// (consecutive threads take consecutive pixels of one orientation, so a warp
+// reads neighbouring model voxels); then thread j < OB adds the chunk's
+// mask-0 values of its orientation to u in pixel order, which keeps u_r
+// bit-identical to the reference's sequential sum (max_prob.c:32-38), while
+// all threads store log W as coalesced row segments (max_prob.c:94-97). The
+// host uses it when whole tiles would give the SMs too few blocks.
+template <typename MT, int OB>
+__global__ void __launch_bounds__(256) slice_u_kernel(
+    const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
+    const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
+    long long S, long long V, float *__restrict__ logW, double *__restrict__ u) {
+	static_assert(TILE % OB == 0 && OB % LW == 0, "orientation block must divide the tile");
+	constexpr int CB = 4096 / OB;  // pixels per chunk
+	static_assert(256 % CB == 0, "a thread keeps one pixel of the chunk");
+	constexpr int SEG = OB / LW;   // vector stores per row segment
+	__shared__ double s_rot[OB][9];
+	__shared__ int s_mode[OB];
+	__shared__ double s_w[CB][OB + 1];
+	__shared__ double s_q[CB][4];
+	__shared__ int s_m[CB];
+	const int t = threadIdx.x, r0 = blockIdx.x * OB, rt = r0 / TILE, jj0 = r0 % TILE;
+	for (int j = t; j < OB; j += blockDim.x) {
+		const int r = r0 + j;
+		const int rr = r < R ? r : 0;
+		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
+		s_mode[j] = rr % M;
+	}
+	const double center = (double)(S / 2);
+	double acc = 0.;
+	for (int p0 = 0; p0 < P; p0 += CB) {
+		for (int k = t; k < CB; k += blockDim.x) {
+			const int p = p0 + k;
+			if (p < P) {
+				s_q[k][0] = qvals[3 * (size_t)p];
+				s_q[k][1] = qvals[3 * (size_t)p + 1];
+				s_q[k][2] = qvals[3 * (size_t)p + 2];
+				s_q[k][3] = corr[p];
+				s_m[k] = mask[p];
+			} else {
+				s_m[k] = -1;
+			}
+		}
+		__syncthreads();
+		{
+			// 256 is a multiple of CB: thread t keeps pixel t % CB in registers
+			// and takes orientations t / CB, t / CB + 256 / CB, ...
+			const int i = t % CB;
+			if (s_m[i] >= 0) {
+				const double qx = s_q[i][0], qy = s_q[i][1], qz = s_q[i][2], cr = s_q[i][3];
+#pragma unroll 2
+				for (int j = t / CB; j < OB; j += 256 / CB) {
+					Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+					s_w[i][j] = interp(c, model + (size_t)s_mode[j] * V, S, cr);
+				}
+			}
+		}
+		__syncthreads();
+		if (t < OB) {
+#pragma unroll 8
+			for (int k = 0; k < CB; ++k)
+				if (s_m[k] == 0)
+					acc = dadd(acc, s_w[k][t]);
+		}
+		for (int idx = t; idx < CB * SEG; idx += blockDim.x) {
+			const int row = idx / SEG, seg = idx % SEG, pp = p0 + row;
+			if (pp < P) {
+				float v[LW];
+#pragma unroll
+				for (int k = 0; k < LW; ++k)
+					v[k] = (float)log(s_w[row][seg * LW + k]);
+				st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + jj0 + seg * LW, v);
+			}
+		}
+		__syncthreads();
+	}
+	if (t < OB && r0 + t < R)
+		u[r0 + t] = acc;
 }
 
 // log w_r per orientation, so that no pair evaluates a logarithm of its
@@ -246,8 +328,11 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 // beta (pval - max) - log p_norm + log M - log w_r so that no pair evaluates a
 // logarithm. The two passes over a frame's log-likelihoods keep UNR tile rows
 // in flight per lane.
+#ifndef DFG_NORM_MINB
+#define DFG_NORM_MINB 4
+#endif
 template <bool MULTI>
-__global__ void __launch_bounds__(256, 3) norm_kernel(
+__global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
     const double *__restrict__ pval, const double *__restrict__ tmax, const int *__restrict__ targ, int RT,
     int Nc, int d0, int R, int M, const double *__restrict__ logw, const double *__restrict__ u,
     const double *__restrict__ beta, const double *__restrict__ sum_fact, const uint8_t *__restrict__ blacklist,
@@ -467,7 +552,9 @@ __global__ void psum_r_reduce_kernel(const double *__restrict__ part, int nsplit
 // (orientation tile, pixel), walking the pixel's list of frames (pixels with
 // mask < 2 only) and reading one row of P per entry (one LW-wide vector load
 // per lane); count-1 and multi-photon segments as in the E-step, compensated
-// FP32 sums. No atomics; pixels are visited heaviest first for balance.
+// FP32 sums, two orientations per paired FP32 instruction (this kernel is
+// bound by instruction issue; the E-step, bound by L2, gains nothing from
+// pairing). No atomics; pixels are visited heaviest first for balance.
 constexpr int MSTEP_MINB = LW == 4 ? 4 : 6;
 
 __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__restrict__ Pst, int Nc,
@@ -491,7 +578,65 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 #pragma unroll
 		for (int k = 0; k < LW; ++k)
 			s[h][k] = c[h][k] = 0.f;
-#pragma unroll(LW == 1 ? 2 : 1)
+	if constexpr (LW >= 2) {
+		// orientations in pairs: paired FP32 compensated additions; the next
+		// 8 words are fetched while the current 8 rows are in flight
+		constexpr int NP = NPAIR;
+		f32x2 s2[NP], c2[NP];
+#pragma unroll
+		for (int h = 0; h < NP; ++h)
+			s2[h] = c2[h] = 0ull;
+		uint4 a = make_uint4(Nc, Nc, Nc, Nc), b = a;
+		if (beg < mid) {
+			a = __ldg(w4 + (beg >> 2));
+			b = __ldg(w4 + (beg >> 2) + 1);
+		}
+		for (long long j = beg; j < mid; j += 8) {
+			f32x2 v[8][NP];
+			ld_pairs(Pr + a.x * TILE, v[0]);
+			ld_pairs(Pr + a.y * TILE, v[1]);
+			ld_pairs(Pr + a.z * TILE, v[2]);
+			ld_pairs(Pr + a.w * TILE, v[3]);
+			ld_pairs(Pr + b.x * TILE, v[4]);
+			ld_pairs(Pr + b.y * TILE, v[5]);
+			ld_pairs(Pr + b.z * TILE, v[6]);
+			ld_pairs(Pr + b.w * TILE, v[7]);
+			if (j + 8 < mid) {
+				a = __ldg(w4 + ((j + 8) >> 2));
+				b = __ldg(w4 + ((j + 8) >> 2) + 1);
+			}
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+#pragma unroll
+				for (int h = 0; h < NP; ++h) {
+					float lo, hi;
+					f2_unpack(v[q][h], lo, hi);
+					kahan_add2(s2[h], c2[h], f2_pack(fmaxf(lo, 0.f), fmaxf(hi, 0.f)));
+				}
+		}
+		for (long long j = mid; j < end; j += 8) {
+			const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
+			const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+			f32x2 v[8][NP];
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+				ld_pairs(Pr + (e[q] & IDX_MASK) * TILE, v[q]);
+#pragma unroll
+			for (int q = 0; q < 8; ++q)
+#pragma unroll
+				for (int h = 0; h < NP; ++h) {
+					float lo, hi;
+					f2_unpack(v[q][h], lo, hi);
+					kahan_add_count2(s2[h], c2[h], e[q] >> IDX_BITS, f2_pack(fmaxf(lo, 0.f), fmaxf(hi, 0.f)));
+				}
+		}
+#pragma unroll
+		for (int h = 0; h < NP; ++h) {
+			f2_unpack(s2[h], s[0][2 * h], s[0][2 * h + 1]);
+			f2_unpack(c2[h], c[0][2 * h], c[0][2 * h + 1]);
+		}
+	} else {
+#pragma unroll 2
 	for (long long j = beg; j < mid; j += 8) {
 		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
 		float v[8][LW];
@@ -521,6 +666,7 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 #pragma unroll
 			for (int k = 0; k < LW; ++k)
 				kahan_add_count(s[q % ECH][k], c[q % ECH][k], e[q] >> IDX_BITS, fmaxf(v[q][k], 0.f));
+	}
 	}
 	float *out = T + ((size_t)rt * P + p) * TILE + lane * LW;
 	float o[LW];
