@@ -59,6 +59,9 @@ _SIGS = {
     "dfg_get_frame_params": (C.c_int, [_V, _D, _D, _D, _I, _D, _U8]),
     "dfg_get_scalars": (C.c_int, [_V, _D]),
     "dfg_get_num_prob": (C.c_int, [_V, _I]),
+    "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
+    "dfg_get_sparse_prob": (C.c_int, [_V, _I, _D]),
+    "dfg_get_tomograms": (C.c_int, [_V, C.c_int, C.c_int, _D]),
     "dfg_slice_gen": (C.c_int, [_V, _D, C.c_int, _D]),
     "dfg_slice_merge": (C.c_int, [_V, _D, C.c_int, _D, _D, _D]),
     "dfg_slice_gen_noalloc": (C.c_int, [_V, _D, C.c_int, _D]),
@@ -229,6 +232,25 @@ class Context:
     def num_prob(self):
         out = np.zeros(self.num_data, np.int32)
         self.call("dfg_get_num_prob", ptr(out, C.c_int))
+        return out
+
+    def sparse_prob(self):
+        """(offsets [N+1] int64, place_prob int32, prob float64) of the last
+        maximize run with option keep_prob: frame d's pairs with P > 1e-6 are
+        [offsets[d], offsets[d+1]) in orientation order."""
+        off = np.zeros(self.num_data + 1, np.int64)
+        self.call("dfg_get_sparse_prob_offsets", ptr(off, C.c_longlong))
+        place = np.zeros(max(int(off[-1]), 1), np.int32)
+        prob = np.zeros(max(int(off[-1]), 1), np.float64)
+        self.call("dfg_get_sparse_prob", ptr(place, C.c_int), ptr(prob, C.c_double))
+        n = int(off[-1])
+        return off, place[:n], prob[:n]
+
+    def tomograms(self, r0, n):
+        """Photon tomograms of orientations r0 .. r0+n-1 (each / psum_r where
+        positive) as [n, num_pix] float64."""
+        out = np.zeros((n, self.num_pix))
+        self.call("dfg_get_tomograms", int(r0), int(n), ptr(out, C.c_double))
         return out
 
     def quat_norm(self):

@@ -475,6 +475,44 @@ static int ensure_buffers(dfg_ctx *ctx) {
 // ---------------------------------------------------------------------------
 // the iteration
 // ---------------------------------------------------------------------------
+// Sparse probabilities of one frame chunk, copied to the host lists: the
+// pairs with P > PROB_MIN of every frame, in orientation order, as the
+// reference's combined and resparsified prob / place_prob (max_prob.c:294-325).
+// Runs after the chunk's normalisation, while its log-likelihoods are held.
+static int collect_prob(dfg_ctx *ctx, const Chunk &ch) {
+	cudaStream_t st = ctx->stream;
+	const int Nc = ch.nc, RT = ctx->RT;
+	CK(ctx->prob_count.ensure((size_t)Nc));
+	count_prob_kernel<<<blocks_for(Nc, 8), 256, 0, st>>>(ctx->Pst.p, RT, Nc, ctx->prob_count.p);
+	CKL("count_prob_kernel");
+	std::vector<int> cnt(Nc);
+	CK(cudaMemcpyAsync(cnt.data(), ctx->prob_count.p, (size_t)Nc * sizeof(int), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	std::vector<long long> off((size_t)Nc + 1, 0);
+	for (int k = 0; k < Nc; ++k)
+		off[k + 1] = off[k] + cnt[k];
+	const long long total = off[Nc], base = ctx->h_prob_off[ch.d0];
+	for (int k = 0; k < Nc; ++k)
+		ctx->h_prob_off[(size_t)ch.d0 + k + 1] = base + off[k + 1];
+	if (total == 0)
+		return DFG_OK;
+	CK(upload(ctx->d_prob_off, off.data(), off.size(), st));
+	CK(ctx->d_place.ensure((size_t)total));
+	CK(ctx->d_prob.ensure((size_t)total));
+	compact_prob_kernel<<<blocks_for(Nc, 8), 256, 0, st>>>(ctx->pval.p, ctx->Pst.p, RT, Nc, ch.d0, ctx->beta.p,
+	                                                        ctx->max_exp.p, ctx->p_norm.p, ctx->d_prob_off.p,
+	                                                        ctx->d_place.p, ctx->d_prob.p);
+	CKL("compact_prob_kernel");
+	ctx->h_place_prob.resize((size_t)(base + total));
+	ctx->h_prob.resize((size_t)(base + total));
+	CK(cudaMemcpyAsync(ctx->h_place_prob.data() + base, ctx->d_place.p, (size_t)total * sizeof(int),
+	                   cudaMemcpyDeviceToHost, st));
+	CK(cudaMemcpyAsync(ctx->h_prob.data() + base, ctx->d_prob.p, (size_t)total * sizeof(double),
+	                   cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	return DFG_OK;
+}
+
 extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_likelihood) {
 	if (!ctx || !par)
 		return DFG_ERR_ARG;
@@ -539,6 +577,12 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	const int use_scale = par->need_scaling && (par->iteration > 1 || par->known_scale);
 	const int psum_d_on = par->need_scaling && par->update_scale;
 
+	if (ctx->keep_prob) {
+		ctx->h_prob_off.assign((size_t)N + 1, 0);
+		ctx->h_place_prob.clear();
+		ctx->h_prob.clear();
+	}
+	ctx->have_prob = false;
 	for (Chunk &ch : ctx->chunks) {
 		const int Nc = ch.nc;
 		// E-step (calculate_prob, max_prob.c:66-213)
@@ -568,6 +612,9 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 			    ctx->num_prob.p);
 		CKL("norm_kernel");
 		phase_end(ctx, PH_NORM, 1);
+		if (ctx->keep_prob)
+			if (int rc = collect_prob(ctx, ch))
+				return rc;
 		// psum_r (calc_psum_r, max_update.c:108-116)
 		phase_begin(ctx, PH_PSUM);
 		{
@@ -638,6 +685,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	ctx->mutual_info = h[1] / N;
 	ctx->avg_ll = h[2] / N;
 	ctx->have_results = true;
+	ctx->have_prob = ctx->keep_prob;
 	if (avg_likelihood)
 		*avg_likelihood = ctx->avg_ll;
 	return DFG_OK;
@@ -771,6 +819,42 @@ extern "C" int dfg_get_num_prob(dfg_ctx *ctx, int *num_prob) {
 	return DFG_OK;
 }
 
+extern "C" int dfg_get_sparse_prob_offsets(dfg_ctx *ctx, long long *offsets) {
+	if (!ctx || !offsets)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_prob, DFG_ERR_STATE, "no sparse probabilities: set option keep_prob and run dfg_maximize");
+	std::memcpy(offsets, ctx->h_prob_off.data(), ctx->h_prob_off.size() * sizeof(long long));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_sparse_prob(dfg_ctx *ctx, int *place_prob, double *prob) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_prob, DFG_ERR_STATE, "no sparse probabilities: set option keep_prob and run dfg_maximize");
+	if (place_prob)
+		std::memcpy(place_prob, ctx->h_place_prob.data(), ctx->h_place_prob.size() * sizeof(int));
+	if (prob)
+		std::memcpy(prob, ctx->h_prob.data(), ctx->h_prob.size() * sizeof(double));
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_tomograms(dfg_ctx *ctx, int r0, int n, double *out) {
+	if (!ctx || !out)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
+	NEED(r0 >= 0 && n >= 1 && (long long)r0 + n <= ctx->R, DFG_ERR_ARG,
+	     "orientations %d..%lld outside 0..%d", r0, (long long)r0 + n - 1, ctx->R - 1);
+	CK(cudaSetDevice(ctx->device));
+	const size_t count = (size_t)n * ctx->P;
+	CK(ctx->tomo_out.ensure(count));
+	tomogram_kernel<<<blocks_for((long long)count, 256), 256, 0, ctx->stream>>>(ctx->T.p, ctx->psum_r.p, ctx->P, r0, n,
+	                                                                             ctx->tomo_out.p);
+	CKL("tomogram_kernel");
+	CK(fetch(out, ctx->tomo_out, count, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
 extern "C" int dfg_get_quat_norm(dfg_ctx *ctx, double *quat_norm) {
 	if (!ctx || !quat_norm)
 		return DFG_ERR_ARG;
@@ -898,6 +982,10 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 	}
 	if (!strcmp(key, "timing")) {
 		ctx->timing = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "keep_prob")) {
+		ctx->keep_prob = value != 0.;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "slice_block")) {

@@ -124,6 +124,15 @@ struct dfg_ctx {
 	// options and results
 	double pair_budget_mb = 0.;
 	int slice_block = 0;  // orientations per slice block; 0 = automatic
+	// sparse probabilities of the last maximize (option keep_prob): per frame
+	// the pairs with P > PROB_MIN in orientation order, host-resident
+	bool keep_prob = false, have_prob = false;
+	std::vector<long long> h_prob_off;  // [N + 1]
+	std::vector<int> h_place_prob;
+	std::vector<double> h_prob;
+	DevBuf<int> prob_count, d_place;
+	DevBuf<long long> d_prob_off;
+	DevBuf<double> d_prob, tomo_out;
 	bool timing = false;
 	cudaEvent_t ev[2 * PH_COUNT] = {};
 	cudaEvent_t user_ev[8] = {};

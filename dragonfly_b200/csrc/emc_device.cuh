@@ -1023,4 +1023,95 @@ __global__ void merge_one_kernel(const double *__restrict__ quat, int mode, cons
 	}
 }
 
+// ---------------------------------------------------------------------------
+// sparse probabilities and tomograms for the result getters
+// ---------------------------------------------------------------------------
+// Per frame of the chunk: the number of pairs with P > PROB_MIN (positive
+// Pst), i.e. the length of the frame's list after resparsify
+// (max_prob.c:321-325, 429-448). One warp per frame.
+__global__ void __launch_bounds__(256) count_prob_kernel(const float *__restrict__ Pst, int RT, int Nc,
+                                                         int *__restrict__ count) {
+	const int dl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (dl >= Nc)
+		return;
+	const size_t pstride = (size_t)(Nc + 1) * TILE;
+	int c = 0;
+	for (int rt = 0; rt < RT; ++rt) {
+		float v[LW];
+		ld_row(Pst + rt * pstride + (size_t)dl * TILE + lane * LW, v);
+#pragma unroll
+		for (int e = 0; e < LW; ++e)
+			c += v[e] > 0.f;
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		c += __shfl_xor_sync(FULL, c, o);
+	if (lane == 0)
+		count[dl] = c;
+}
+
+// The frame's list in ascending orientation order, as the reference's
+// combined and resparsified prob / place_prob (max_prob.c:306-325): P is
+// formed again in FP64 from the log-likelihood exactly as the normalisation
+// formed it. off [Nc + 1] holds the chunk-local list offsets. One warp per
+// frame; lanes own LW consecutive orientations, so a warp-wide exclusive scan
+// of the per-lane counts orders each row.
+__global__ void __launch_bounds__(256) compact_prob_kernel(
+    const double *__restrict__ pval, const float *__restrict__ Pst, int RT, int Nc, int d0,
+    const double *__restrict__ beta, const double *__restrict__ max_exp, const double *__restrict__ p_norm,
+    const long long *__restrict__ off, int *__restrict__ place, double *__restrict__ prob) {
+	const int dl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (dl >= Nc)
+		return;
+	long long base = off[dl];
+	if (off[dl + 1] == base)
+		return;
+	const int d = d0 + dl;
+	const double m = max_exp[d], inv_s = 1. / p_norm[d], b = beta[d];
+	const size_t pstride = (size_t)(Nc + 1) * TILE, tstride = (size_t)Nc * TILE;
+	for (int rt = 0; rt < RT; ++rt) {
+		float pv[LW];
+		ld_row(Pst + rt * pstride + (size_t)dl * TILE + lane * LW, pv);
+		int c = 0;
+#pragma unroll
+		for (int e = 0; e < LW; ++e)
+			c += pv[e] > 0.f;
+		int incl = c;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int y = __shfl_up_sync(FULL, incl, o);
+			if (lane >= o)
+				incl += y;
+		}
+		const int total = __shfl_sync(FULL, incl, 31);
+		if (c > 0) {
+			double x[LW];
+			ld_row(pval + rt * tstride + (size_t)dl * TILE + lane * LW, x);
+			long long pos = base + incl - c;
+#pragma unroll
+			for (int e = 0; e < LW; ++e)
+				if (pv[e] > 0.f) {
+					place[pos] = rt * TILE + lane * LW + e;
+					prob[pos] = exp(dmul(b, dsub(x[e], m))) * inv_s;
+					++pos;
+				}
+		}
+		base += total;
+	}
+}
+
+// Tomograms of orientations r0 .. r0 + n - 1 divided by psum_r where it is
+// positive (update_tomogram_nobg's final step, max_update.c:226-229), as
+// out [n][P] FP64.
+__global__ void tomogram_kernel(const float *__restrict__ T, const double *__restrict__ psum_r, int P, int r0,
+                                int n, double *__restrict__ out) {
+	const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= (long long)n * P)
+		return;
+	const int k = (int)(idx / P), p = (int)(idx - (long long)k * P), r = r0 + k;
+	const double v = T[((size_t)(r / TILE) * P + p) * TILE + r % TILE];
+	const double ps = psum_r[r];
+	out[idx] = ps > 0. ? v / ps : v;
+}
+
 }  // namespace dfg

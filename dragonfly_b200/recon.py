@@ -102,6 +102,9 @@ class EMCRecon:
         beta_mean = self.update_beta()
         p = c.params(par.iteration, par.need_scaling, par.update_scale, par.known_scale, par.beta_jump,
                      par.beta_period, par.beta_factor)
+        # the per-frame probability lists are formed only when they are saved
+        # (combine_information_omp, max_prob.c:294-325)
+        c.set_option("keep_prob", 1 if par.save_prob else 0)
         likelihood = c.maximize(p)
         self.update_model()
         if par.need_scaling == 1:
@@ -201,6 +204,14 @@ class EMCRecon:
         if par.need_scaling != 0:
             out["scale"] = itr.scale
         out["quaternions"] = itr.quat.quats
+        if par.save_prob != 0:
+            # vlen datasets in the reference (recon.pyx:270-279): stored here as
+            # flat arrays with per-frame offsets
+            off, place, prob = self._sparse()
+            out["probabilities/num_rot"] = [itr.quat.num_rot]
+            out["probabilities/offsets"] = off
+            out["probabilities/place"] = place
+            out["probabilities/prob"] = prob
         return out
 
     def _write(self, fname_noext, d):
@@ -272,7 +283,13 @@ class EMCRecon:
 
     @property
     def num_prob(self):
-        return self.ctx.num_prob()
+        """Length of each frame's probability list: the pairs with P > 1e-6
+        when save_prob is set, zeros otherwise (the reference forms the lists
+        only to save them, max_prob.c:294-325)."""
+        if self._iter is not None and self._iter.params.save_prob:
+            off = self._sparse()[0]
+            return np.diff(off).astype(np.int32)
+        return np.zeros(self.ctx.num_data, np.int32)
 
     @property
     def u(self):
@@ -290,17 +307,42 @@ class EMCRecon:
     def weight(self):
         return self._iter.model.inter_weight
 
+    def _sparse(self):
+        if "sparse" not in self._results:
+            self._results["sparse"] = self.ctx.sparse_prob()
+        return self._results["sparse"]
+
     @property
     def all_views(self):
-        return None
+        """Photon tomogram of every orientation (divided by psum_r where it is
+        positive) as [num_rot * num_modes, num_pix]; see tomograms() for a
+        range of orientations."""
+        c = self.ctx
+        n = c.num_rot * c.model_shape[0]
+        if n * c.num_pix * 8 > (2 << 30):
+            raise MemoryError("all_views of %d orientations x %d pixels exceeds 2 GiB; use tomograms(r0, n)"
+                              % (n, c.num_pix))
+        return c.tomograms(0, n)
+
+    def tomograms(self, r0, n):
+        return self.ctx.tomograms(r0, n)
 
     @property
     def prob(self):
-        return None
+        """Per-frame probabilities P > 1e-6 in orientation order (save_prob
+        runs only, as in recon.pyx:409-411)."""
+        if self._iter is None or not self._iter.params.save_prob:
+            return None
+        off, _, prob = self._sparse()
+        return [prob[off[d]:off[d + 1]] if off[d + 1] > off[d] else None for d in range(len(off) - 1)]
 
     @property
     def place_prob(self):
-        return None
+        """Orientation indices of prob (recon.pyx:412-415)."""
+        if self._iter is None or not self._iter.params.save_prob:
+            return None
+        off, place, _ = self._sparse()
+        return [place[off[d]:off[d + 1]] for d in range(len(off) - 1)]
 
 
 def main():

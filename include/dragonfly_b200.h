@@ -125,6 +125,23 @@ DFG_API int dfg_get_frame_params(dfg_ctx *ctx, double *scale, double *beta, doub
 DFG_API int dfg_get_scalars(dfg_ctx *ctx, double *out);
 DFG_API int dfg_get_num_prob(dfg_ctx *ctx, int *num_prob);  /* kept pairs per frame */
 
+/* Sparse probabilities of the last dfg_maximize, present when the option
+ * "keep_prob" was set before it (replaces EMCRecon.prob / place_prob,
+ * recon.pyx:409-415, which the reference fills when save_prob is set:
+ * combine_information_omp, max_prob.c:294-325). For every frame, the pairs
+ * with P > 1e-6 in ascending orientation order; frame d's entries are
+ * [offsets[d], offsets[d + 1]) of place_prob (orientation index) and prob
+ * (P, FP64). offsets has num_data + 1 entries; DFG_ERR_STATE without them. */
+DFG_API int dfg_get_sparse_prob_offsets(dfg_ctx *ctx, long long *offsets);
+DFG_API int dfg_get_sparse_prob(dfg_ctx *ctx, int *place_prob, double *prob);
+
+/* Photon tomograms of orientations r0 .. r0 + n - 1 of the last dfg_maximize,
+ * each divided by its psum_r where that is positive, as out[n][num_pix] FP64
+ * (the views update_tomogram_nobg forms per orientation, max_update.c:142-230,
+ * exposed by the reference only as the per-thread EMCRecon.all_views,
+ * recon.pyx:342-351). */
+DFG_API int dfg_get_tomograms(dfg_ctx *ctx, int r0, int n, double *out);
+
 /* ---- one-slice operations -------------------------------------------------
  * Model.slice_gen (dragonfly/model.pyx:105-132 -> model.c:11-59): slice of
  * model1 at one quaternion, out[num_pix]. */

@@ -151,6 +151,10 @@ class ReferenceEngine:
         L.ref_slice_gen.argtypes = [C.c_void_p, _dp, C.c_int, _dp]
         L.ref_slice_merge.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _dp, _dp]
         L.ref_destroy.argtypes = [C.c_void_p]
+        L.ref_set_save_prob.argtypes = [C.c_void_p, C.c_int]
+        L.ref_get_frame_prob.restype = C.c_int
+        L.ref_get_frame_prob.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        self.save_prob = False
         self.prob = p = prob
         self._scale_buf = p.scale
         self._bl_buf = p.blacklist
@@ -191,12 +195,33 @@ class ReferenceEngine:
         self.lib.ref_slice_gen(self.h, _c(quat, np.float64), int(mode), out)
         return out
 
+    def set_save_prob(self, on):
+        """Makes maximize form the combined per-frame probability lists
+        (save_prob path, max_prob.c:294-325); run_iteration then returns them
+        as res["sparse_prob"] = (offsets, place, prob)."""
+        self.save_prob = bool(on)
+        self.lib.ref_set_save_prob(self.h, int(bool(on)))
+
+    def _sparse_prob(self):
+        n = self.prob.num_data
+        counts = np.array([self.lib.ref_get_frame_prob(self.h, d, None, None) for d in range(n)], np.int64)
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum(counts)
+        place = np.zeros(int(off[-1]), np.int32)
+        prob = np.zeros(int(off[-1]))
+        for d in range(n):
+            if counts[d]:
+                self.lib.ref_get_frame_prob(self.h, d, place[off[d]:].ctypes.data, prob[off[d]:].ctypes.data)
+        return off, place, prob
+
     def run_iteration(self, iteration):
         p = self.prob
         L = self.lib
         avg_ll = L.ref_maximize(self.h, int(iteration))
         n = p.num_data
         res = IterationResult()
+        if self.save_prob:
+            res["sparse_prob"] = self._sparse_prob()
         rmax = np.zeros(n, np.int32)
         info, ll, mx, pn, pd = (np.zeros(n) for _ in range(5))
         L.ref_get_frame_arrays(self.h, rmax, info, ll, mx, pn, pd)

@@ -263,6 +263,25 @@ void ref_get_frame_arrays(ref_engine *e, int *rmax, double *info, double *likeli
 	copy_or_zero(psum_d, c->psum_d, n * sizeof(double));
 }
 
+/* Asks the reference to form the combined per-frame probability lists (the
+ * save_prob path of combine_information_omp, max_prob.c:294-325). */
+void ref_set_save_prob(ref_engine *e, int on) { e->par.save_prob = on; }
+
+/* Frame d's combined list after ref_maximize with save_prob: copies
+ * num_prob[d] entries (orientation index, P) when the pointers are non-NULL
+ * and returns the count (0 without lists). */
+int ref_get_frame_prob(ref_engine *e, int d, int *place, double *prob) {
+	struct max_data *c = e->mdata;
+	if (c == NULL || c->num_prob == NULL || c->prob == NULL || c->prob[d] == NULL)
+		return 0;
+	int n = c->num_prob[d];
+	if (place != NULL)
+		memcpy(place, c->place_prob[d], (size_t)n * sizeof(int));
+	if (prob != NULL)
+		memcpy(prob, c->prob[d], (size_t)n * sizeof(double));
+	return n;
+}
+
 void ref_get_quat_norm(ref_engine *e, double *o) {
 	size_t n = (size_t)e->iter.tot_num_data * e->mod.num_modes;
 	copy_or_zero(o, e->mod.num_modes > 1 ? e->mdata->quat_norm : NULL, n * sizeof(double));
