@@ -59,6 +59,8 @@ _SIGS = {
     "dfg_get_frame_params": (C.c_int, [_V, _D, _D, _D, _I, _D, _U8]),
     "dfg_get_scalars": (C.c_int, [_V, _D]),
     "dfg_get_num_prob": (C.c_int, [_V, _I]),
+    "dfg_set_background": (C.c_int, [_V, _D]),
+    "dfg_set_bgscale": (C.c_int, [_V, _D]),
     "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
     "dfg_get_sparse_prob": (C.c_int, [_V, _I, _D]),
     "dfg_get_tomograms": (C.c_int, [_V, C.c_int, C.c_int, _D]),
@@ -171,6 +173,17 @@ class Context:
             m = m[None]
         self.call("dfg_set_model", m.shape[-1], m.shape[0], ptr(m, C.c_double))
         self.model_shape = m.shape
+
+    def set_background(self, background):
+        """Per-pixel background (None: none); with need_scaling the iteration
+        then takes the background-aware updates."""
+        b = None if background is None else np.ascontiguousarray(background, np.float64).ravel()
+        self.call("dfg_set_background", ptr(b, C.c_double))
+
+    def set_bgscale(self, bgscale):
+        """Per-frame background scales (None: ones)."""
+        b = None if bgscale is None else np.ascontiguousarray(bgscale, np.float64).ravel()
+        self.call("dfg_set_bgscale", ptr(b, C.c_double))
 
     def set_scale(self, scale):
         s = np.ascontiguousarray(scale, np.float64)

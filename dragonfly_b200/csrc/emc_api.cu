@@ -11,6 +11,7 @@
 
 #include "emc_ctx.cuh"
 #include "emc_device.cuh"
+#include "emc_bg.cuh"
 
 using namespace dfg;
 
@@ -166,6 +167,9 @@ extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const
 	}
 	ctx->h_ones_off = oo;
 	ctx->h_multi_off = mo;
+	ctx->powder_valid = false;
+	if ((int)ctx->h_bgscale.size() != N)
+		ctx->h_bgscale.clear();
 	ctx->N = N;
 
 	// E-step lists: photons on mask == 0 pixels, ones then multi, per frame;
@@ -275,6 +279,78 @@ extern "C" int dfg_set_scale(dfg_ctx *ctx, const double *scale) {
 	CK(cudaSetDevice(ctx->device));
 	CK(upload(ctx->scale, scale, (size_t)ctx->N, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_background(dfg_ctx *ctx, const double *background) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->P > 0, DFG_ERR_STATE, "background: set the detector first");
+	if (background == nullptr) {
+		ctx->with_bg = false;
+		return DFG_OK;
+	}
+	const int P = ctx->P;
+	for (int t = 0; t < P; ++t)
+		NEED(std::isfinite(background[t]), DFG_ERR_ARG, "background[%d] is not finite", t);
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->background, background, (size_t)P, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->with_bg = true;
+	ctx->powder_valid = false;
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_bgscale(dfg_ctx *ctx, const double *bgscale) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->N > 0, DFG_ERR_STATE, "bgscale: set the frames first");
+	if (bgscale == nullptr) {
+		ctx->h_bgscale.clear();
+		return DFG_OK;
+	}
+	for (int d = 0; d < ctx->N; ++d)
+		NEED(std::isfinite(bgscale[d]), DFG_ERR_ARG, "bgscale[%d] is not finite", d);
+	ctx->h_bgscale.assign(bgscale, bgscale + ctx->N);
+	return DFG_OK;
+}
+
+// Powder sum and per-frame background scales for the background-aware path:
+// powder[t] = photons on mask-0 pixel t summed over all frames / num_data
+// (calc_powder, iterate.c:119-177); bgscale defaults to ones (iterate.pyx:290-296).
+static int ensure_bg(dfg_ctx *ctx) {
+	const int N = ctx->N, P = ctx->P;
+	cudaStream_t st = ctx->stream;
+	if (!ctx->powder_valid) {
+		std::vector<double> pw(P, 0.);
+		const uint8_t *mk = ctx->h_mask.data();
+		for (int d = 0; d < N; ++d) {
+			for (long long i = ctx->h_ones_off[d]; i < ctx->h_ones_off[d + 1]; ++i)
+				if (mk[ctx->h_place_ones[i]] < 1)
+					pw[ctx->h_place_ones[i]] += 1.;
+			for (long long i = ctx->h_multi_off[d]; i < ctx->h_multi_off[d + 1]; ++i)
+				if (mk[ctx->h_place_multi[i]] < 1)
+					pw[ctx->h_place_multi[i]] += ctx->h_count_multi[i];
+		}
+		for (int t = 0; t < P; ++t)
+			pw[t] /= N;
+		CK(upload(ctx->powder, pw.data(), pw.size(), st));
+		ctx->powder_valid = true;
+	}
+	std::vector<double> bs = ctx->h_bgscale;
+	if ((int)bs.size() != N)
+		bs.assign(N, 1.);
+	CK(upload(ctx->bgscale, bs.data(), bs.size(), st));
+	const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
+	CK(ctx->scalemax.ensure((size_t)ctx->R_pad));
+	CK(ctx->smax_part.ensure((size_t)nsplit * ctx->R_pad));
+	CK(ctx->gd_part.ensure((size_t)ctx->RT * ctx->chunk_frames));
+	CK(ctx->gd_G.ensure((size_t)N));
+	CK(ctx->gd_s.ensure((size_t)N));
+	CK(ctx->gd_active.ensure((size_t)N));
+	CK(ctx->Wd.ensure((size_t)ctx->RT * (P + 1) * TILE));
+	CK(ctx->Pd.ensure((size_t)ctx->R_pad * (ctx->chunk_frames + 1)));
+	CK(cudaStreamSynchronize(st));
 	return DFG_OK;
 }
 
@@ -513,6 +589,147 @@ static int collect_prob(dfg_ctx *ctx, const Chunk &ch) {
 	return DFG_OK;
 }
 
+// G_d(phi) for the frames with mask 0 (gradient_d, max_scale.c:21-127); the
+// other entries of G keep their values, as in the reference.
+static int grad_d(dfg_ctx *ctx, const Chunk &ch, const std::vector<uint8_t> &mask, const std::vector<double> &phi,
+                  std::vector<double> &G) {
+	cudaStream_t st = ctx->stream;
+	const int N = ctx->N, Nc = ch.nc, RT = ctx->RT;
+	std::vector<uint8_t> active(N);
+	for (int d = 0; d < N; ++d)
+		active[d] = mask[d] == 0;
+	CK(cudaMemcpyAsync(ctx->gd_active.p, active.data(), (size_t)N, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(ctx->gd_s.p, phi.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, st));
+	grad_d_kernel<<<blocks_for((long long)RT * Nc, 8), 256, 0, st>>>(
+	    ctx->Wd.p, ctx->Pd.p, Nc, ch.d0, RT, ctx->P, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scalars.p,
+	    ctx->gd_s.p, ctx->bgscale.p, ctx->background.p, ctx->gd_active.p, ctx->gd_part.p);
+	CKL("grad_d_kernel");
+	grad_d_reduce_kernel<<<blocks_for(Nc, 256), 256, 0, st>>>(ctx->gd_part.p, RT, Nc, ch.d0, ctx->psum_d.p,
+	                                                          ctx->gd_active.p, ctx->gd_G.p);
+	CKL("grad_d_reduce_kernel");
+	std::vector<double> g(N);
+	CK(cudaMemcpyAsync(g.data(), ctx->gd_G.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	for (int d = 0; d < N; ++d)
+		if (active[d])
+			G[d] = g[d];
+	return DFG_OK;
+}
+
+// Background-aware scale update (update_scale_bg, max_scale.c:129-288): per
+// frame, bracket phi (start 4 phi or 32, x4 up to 5 times) and refine by
+// Ridder's method (50 rounds; converged when the bracket is < 1e-5 wide or
+// |G| < 1e-3); blacklisted frames get phi = -1, frames with G(0) < 1e-6 get
+// 0.001. The per-frame rules run here; the sums run on the device.
+static int update_scale_bg(dfg_ctx *ctx, const Chunk &ch, const dfg_iter_params *par) {
+	const int N = ctx->N;
+	cudaStream_t st = ctx->stream;
+	std::vector<double> scale(N), so(N, 0.), sn(N, 0.), sm(N, 0.), sl(N, 0.), Go(N, 0.), Gn(N, 0.), Gm(N, 0.),
+	    Gl(N, 0.);
+	std::vector<uint8_t> bl(N), mask(N, 0);
+	CK(cudaMemcpyAsync(scale.data(), ctx->scale.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaMemcpyAsync(bl.data(), ctx->blacklist.p, (size_t)N, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	for (int d = 0; d < N; ++d) {
+		if (bl[d]) {
+			mask[d] = 255;
+			scale[d] = -1.;
+			continue;
+		}
+		sn[d] = (par->iteration > 1 || par->known_scale) ? 4. * scale[d] : 32.;
+	}
+	if (int rc = grad_d(ctx, ch, mask, so, Go))
+		return rc;
+	for (int d = 0; d < N; ++d)
+		if (mask[d] != 255 && Go[d] < 1.e-6) {
+			scale[d] = 0.001;
+			mask[d] = 255;
+		}
+	for (int i = 0; i < 5; ++i) {
+		if (int rc = grad_d(ctx, ch, mask, sn, Gn))
+			return rc;
+		int nm = 0;
+		for (int d = 0; d < N; ++d) {
+			if (mask[d] != 0)
+				nm++;
+			else if (Gn[d] < 0.) {
+				mask[d] = 192;
+				nm++;
+			} else
+				sn[d] *= 4.;
+		}
+		if (nm > 0.99 * N)
+			break;
+	}
+	for (int i = 0; i < 50; ++i) {
+		int nm = 0;
+		for (int d = 0; d < N; ++d) {
+			if (mask[d] == 255) {
+				nm++;
+			} else if (std::fabs(so[d] - sn[d]) < 1.e-5) {
+				mask[d] = 255;
+				scale[d] = 0.5 * (so[d] + sn[d]);
+				nm++;
+			} else {
+				mask[d] = 0;
+				sm[d] = 0.5 * (so[d] + sn[d]);
+			}
+		}
+		if (nm == N)
+			break;
+		if (int rc = grad_d(ctx, ch, mask, sm, Gm))
+			return rc;
+		for (int d = 0; d < N; ++d) {
+			if (mask[d] == 255)
+				continue;
+			if (std::fabs(Gm[d]) < BG_SCALE_TOL) {
+				scale[d] = sm[d];
+				mask[d] = 255;
+				nm++;
+				continue;
+			}
+			const double s = std::sqrt(Gm[d] * Gm[d] - Go[d] * Gn[d]);
+			if (s < 1.e-15) {
+				sl[d] = sm[d];
+			} else {
+				sl[d] = sm[d] + (sm[d] - so[d]) * std::copysign(1.0, Go[d]) * Gm[d] / s;
+				const double lo = std::fmin(so[d], sn[d]), hi = std::fmax(so[d], sn[d]);
+				if (sl[d] <= lo || sl[d] >= hi)
+					sl[d] = sm[d];
+			}
+		}
+		if (nm == N)
+			break;
+		if (int rc = grad_d(ctx, ch, mask, sl, Gl))
+			return rc;
+		for (int d = 0; d < N; ++d) {
+			if (mask[d] >= 255)
+				continue;
+			if (std::fabs(Gl[d]) < BG_SCALE_TOL) {
+				scale[d] = sl[d];
+				mask[d] = 255;
+				nm++;
+			} else if (Gm[d] * Gl[d] < 0.) {
+				so[d] = sm[d];
+				Go[d] = Gm[d];
+				sn[d] = sl[d];
+				Gn[d] = Gl[d];
+			} else if (Go[d] * Gl[d] < 0.) {
+				sn[d] = sl[d];
+				Gn[d] = Gl[d];
+			} else {
+				so[d] = sl[d];
+				Go[d] = Gl[d];
+			}
+		}
+		if (nm == N)
+			break;
+	}
+	CK(cudaMemcpyAsync(ctx->scale.p, scale.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CK(cudaStreamSynchronize(st));
+	return DFG_OK;
+}
+
 extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_likelihood) {
 	if (!ctx || !par)
 		return DFG_ERR_ARG;
@@ -524,6 +741,17 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
 	const long long S = ctx->S, V = ctx->V;
 	const int nblk = (P + PB - 1) / PB;
+	// background-aware path (max_prob.c:134, max_update.c:10-14, max_scale.c:8-10)
+	const bool bg = ctx->with_bg && par->need_scaling;
+	if (bg) {
+		NEED(ctx->chunks.size() == 1, DFG_ERR_NOMEM,
+		     "background-aware updates need all %d frames in one chunk (%d chunks at the pair budget; raise "
+		     "option pair_budget_mb)",
+		     N, (int)ctx->chunks.size());
+		if (int rc = ensure_bg(ctx))
+			return rc;
+	}
+	double *const Wd = bg ? ctx->Wd.p : nullptr;  // FP64 slices for the background path
 
 	// update_beta (recon.pyx:161-171)
 	{
@@ -551,11 +779,11 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		const int nb = R_pad / ob;
 #define DFG_SLICE(OBV)                                                                                        \
 	slice_u_kernel<double, OBV><<<nb, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, \
-	                                                ctx->model1.p, S, V, ctx->logW.p, ctx->u.p)
+	                                                ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd)
 		if (ob == TILE)
 			slice_u_tile_kernel<double><<<RT, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p,
 			                                                ctx->mask.p, P, ctx->model1.p, S, V, ctx->logW.p,
-			                                                ctx->u.p);
+			                                                ctx->u.p, Wd);
 		else if (ob == 64)
 			DFG_SLICE(TILE >= 64 ? 64 : 16);
 		else if (ob == 32)
@@ -589,11 +817,19 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		phase_begin(ctx, PH_ESTEP);
 		{
 			long long warps = (long long)RT * Nc;
-			estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
-			    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
-			    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
-			    ctx->targ.p);
-			CKL("estep_kernel");
+			if (bg) {
+				estep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
+				    ctx->Wd.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
+				    ctx->bgscale.p, ctx->background.p, ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT,
+				    ctx->pval.p, ctx->tmax.p, ctx->targ.p);
+				CKL("estep_bg_kernel");
+			} else {
+				estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
+				    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
+				    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
+				    ctx->targ.p);
+				CKL("estep_kernel");
+			}
 		}
 		phase_end(ctx, PH_ESTEP, 1);
 		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
@@ -603,13 +839,13 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
 			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
 			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
-			    ctx->num_prob.p);
+			    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
 		else
 			norm_kernel<false><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
 			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
 			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
 			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
-			    ctx->num_prob.p);
+			    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
 		CKL("norm_kernel");
 		phase_end(ctx, PH_NORM, 1);
 		if (ctx->keep_prob)
@@ -626,15 +862,33 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 			psum_r_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->psum_part.p, nsplit, R, R_pad,
 			                                                          ctx->psum_r.p);
 			CKL("psum_r_reduce_kernel");
+			if (bg) {
+				scalemax_kernel<<<dim3(RT, nsplit), 256, 0, st>>>(ctx->Pd.p, Nc, ch.d0, fps, ctx->scale.p,
+				                                                  ctx->smax_part.p, R_pad);
+				CKL("scalemax_kernel");
+				scalemax_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->smax_part.p, nsplit, R, R_pad,
+				                                                            ctx->scalemax.p);
+				CKL("scalemax_reduce_kernel");
+			}
 		}
-		phase_end(ctx, PH_PSUM, 2);
+		phase_end(ctx, PH_PSUM, bg ? 4 : 2);
 		// tomograms (update_tomogram_nobg, max_update.c:142-230)
 		phase_begin(ctx, PH_MSTEP);
 		if (ch.npix > 0) {
 			long long warps = (long long)RT * ch.npix;
-			mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p,
-			                                                    ch.pix.p, ch.npix, P, RT, ctx->T.p);
-			CKL("mstep_kernel");
+			if (bg) {
+				// update_tomogram_bg (max_update.c:343-543); the mean photons per
+				// pixel bound the first search window (:397-400)
+				mstep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
+				    ctx->Pd.p, Nc, ch.d0, ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, R,
+				    ctx->psum_r.p, ctx->scalemax.p, ctx->scale.p, ctx->bgscale.p, ctx->background.p, ctx->powder.p,
+				    ctx->mean_count / P, ctx->T.p);
+				CKL("mstep_bg_kernel");
+			} else {
+				mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p,
+				                                                    ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p);
+				CKL("mstep_kernel");
+			}
 		}
 		phase_end(ctx, PH_MSTEP, ch.npix > 0 ? 1 : 0);
 	}
@@ -657,7 +911,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	phase_begin(ctx, PH_MERGE);
 	merge_kernel<<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
 	                                              ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
-	                                              with_weight);
+	                                              with_weight, bg ? 1 : 0);
 	CKL("merge_kernel");
 	phase_end(ctx, PH_MERGE, 1);
 
@@ -671,9 +925,14 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	                                        ctx->scalars.p + 1);
 	CKL("frame_totals_kernel");
 	if (par->need_scaling && par->update_scale) {
-		scale_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->fcounts.p, ctx->psum_d.p, ctx->blacklist.p, N,
-		                                                  ctx->scale.p);
-		CKL("scale_kernel");
+		if (bg) {
+			if (int rc = update_scale_bg(ctx, ctx->chunks[0], par))
+				return rc;
+		} else {
+			scale_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->fcounts.p, ctx->psum_d.p, ctx->blacklist.p, N,
+			                                                  ctx->scale.p);
+			CKL("scale_kernel");
+		}
 	}
 	phase_end(ctx, PH_UPDATE, par->need_scaling && par->update_scale ? 3 : 2);
 
@@ -686,6 +945,7 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	ctx->avg_ll = h[2] / N;
 	ctx->have_results = true;
 	ctx->have_prob = ctx->keep_prob;
+	ctx->views_final = bg;
 	if (avg_likelihood)
 		*avg_likelihood = ctx->avg_ll;
 	return DFG_OK;
@@ -847,8 +1107,8 @@ extern "C" int dfg_get_tomograms(dfg_ctx *ctx, int r0, int n, double *out) {
 	CK(cudaSetDevice(ctx->device));
 	const size_t count = (size_t)n * ctx->P;
 	CK(ctx->tomo_out.ensure(count));
-	tomogram_kernel<<<blocks_for((long long)count, 256), 256, 0, ctx->stream>>>(ctx->T.p, ctx->psum_r.p, ctx->P, r0, n,
-	                                                                             ctx->tomo_out.p);
+	tomogram_kernel<<<blocks_for((long long)count, 256), 256, 0, ctx->stream>>>(
+	    ctx->T.p, ctx->views_final ? nullptr : ctx->psum_r.p, ctx->P, r0, n, ctx->tomo_out.p);
 	CKL("tomogram_kernel");
 	CK(fetch(out, ctx->tomo_out, count, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));

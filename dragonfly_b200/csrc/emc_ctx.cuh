@@ -124,6 +124,16 @@ struct dfg_ctx {
 	// options and results
 	double pair_budget_mb = 0.;
 	int slice_block = 0;  // orientations per slice block; 0 = automatic
+	// background-aware model (per-pixel background with need_scaling):
+	// background [P], powder [P] (mean mask-0 photons per frame and pixel),
+	// bgscale [N], scalemax [R] and the work buffers of the scale search
+	bool with_bg = false, powder_valid = false;
+	bool views_final = false;  // T holds the final views (background path), not sums
+	std::vector<double> h_bgscale;
+	DevBuf<double> background, powder, bgscale, scalemax, smax_part, gd_part, gd_G, gd_s;
+	DevBuf<double> Wd;  // slices W [RT][P+1][TILE] in FP64 (background-aware E-step)
+	DevBuf<double> Pd;  // probabilities [RT][Nc+1][TILE] in FP64, sign as Pst
+	DevBuf<uint8_t> gd_active;
 	// sparse probabilities of the last maximize (option keep_prob): per frame
 	// the pairs with P > PROB_MIN in orientation order, host-resident
 	bool keep_prob = false, have_prob = false;

@@ -16,14 +16,15 @@ namespace dfg {
 // pixels of one orientation); then thread j < TILE adds the chunk's mask-0
 // values of orientation j to u_j in pixel order, which keeps u_r
 // bit-identical to the reference's sequential sum (max_prob.c:32-38), while
-// the warps store log W as coalesced rows (max_prob.c:94-97).
+// the warps store log W as coalesced rows (max_prob.c:94-97); with Wd given
+// (background-aware path, max_prob.c:94) they store W itself in FP64 there.
 constexpr int SB = 32;
 
 template <typename MT>
 __global__ void __launch_bounds__(256) slice_u_tile_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
     const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
-    long long S, long long V, float *__restrict__ logW, double *__restrict__ u) {
+    long long S, long long V, float *__restrict__ logW, double *__restrict__ u, double *__restrict__ Wd) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ double s_w[SB][TILE + 1];
@@ -71,11 +72,19 @@ __global__ void __launch_bounds__(256) slice_u_tile_kernel(
 		for (int row = w; row < SB; row += 8) {
 			const int pp = p0 + row;
 			if (pp < P) {
-				float v[LW];
+				if (Wd != nullptr) {
+					double v[LW];
 #pragma unroll
-				for (int k = 0; k < LW; ++k)
-					v[k] = (float)log(s_w[row][lane * LW + k]);
-				st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + lane * LW, v);
+					for (int k = 0; k < LW; ++k)
+						v[k] = s_w[row][lane * LW + k];
+					st_row(Wd + ((size_t)rt * (P + 1) + pp) * TILE + lane * LW, v);
+				} else {
+					float v[LW];
+#pragma unroll
+					for (int k = 0; k < LW; ++k)
+						v[k] = (float)log(s_w[row][lane * LW + k]);
+					st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + lane * LW, v);
+				}
 			}
 		}
 		__syncthreads();
@@ -97,7 +106,7 @@ template <typename MT, int OB>
 __global__ void __launch_bounds__(256) slice_u_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
     const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
-    long long S, long long V, float *__restrict__ logW, double *__restrict__ u) {
+    long long S, long long V, float *__restrict__ logW, double *__restrict__ u, double *__restrict__ Wd) {
 	static_assert(TILE % OB == 0 && OB % LW == 0, "orientation block must divide the tile");
 	constexpr int CB = 4096 / OB;  // pixels per chunk
 	static_assert(256 % CB == 0, "a thread keeps one pixel of the chunk");
@@ -153,11 +162,19 @@ __global__ void __launch_bounds__(256) slice_u_kernel(
 		for (int idx = t; idx < CB * SEG; idx += blockDim.x) {
 			const int row = idx / SEG, seg = idx % SEG, pp = p0 + row;
 			if (pp < P) {
-				float v[LW];
+				if (Wd != nullptr) {
+					double v[LW];
 #pragma unroll
-				for (int k = 0; k < LW; ++k)
-					v[k] = (float)log(s_w[row][seg * LW + k]);
-				st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + jj0 + seg * LW, v);
+					for (int k = 0; k < LW; ++k)
+						v[k] = s_w[row][seg * LW + k];
+					st_row(Wd + ((size_t)rt * (P + 1) + pp) * TILE + jj0 + seg * LW, v);
+				} else {
+					float v[LW];
+#pragma unroll
+					for (int k = 0; k < LW; ++k)
+						v[k] = (float)log(s_w[row][seg * LW + k]);
+					st_row(logW + ((size_t)rt * (P + 1) + pp) * TILE + jj0 + seg * LW, v);
+				}
 			}
 		}
 		__syncthreads();
@@ -327,7 +344,8 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 // follow max_update.c:105-130, with log(P / w_r * M) written as
 // beta (pval - max) - log p_norm + log M - log w_r so that no pair evaluates a
 // logarithm. The two passes over a frame's log-likelihoods keep UNR tile rows
-// in flight per lane.
+// in flight per lane. With Pd given (background-aware path) P is also stored
+// in FP64, with the same sign convention as Pst.
 #ifndef DFG_NORM_MINB
 #define DFG_NORM_MINB 4
 #endif
@@ -339,7 +357,7 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
     int psum_d_on, const double *__restrict__ scalars, float *__restrict__ Pst, int *__restrict__ rmax,
     double *__restrict__ max_exp, double *__restrict__ p_norm, double *__restrict__ info,
     double *__restrict__ likelihood, double *__restrict__ psum_d, double *__restrict__ quat_norm,
-    int *__restrict__ num_prob) {
+    int *__restrict__ num_prob, double *__restrict__ Pd) {
 	constexpr int UNR = LW == 1 ? 4 : 2;
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
@@ -348,9 +366,16 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 #pragma unroll
 	for (int k = 0; k < LW; ++k)
 		zero[k] = 0.f;
+	double zerod[LW];
+#pragma unroll
+	for (int k = 0; k < LW; ++k)
+		zerod[k] = 0.;
 	if (warp == Nc) {  // the zero row that padding words of the M-step point at
-		for (int rt = 0; rt < RT; ++rt)
+		for (int rt = 0; rt < RT; ++rt) {
 			st_row(Pst + rt * pstride + (size_t)Nc * TILE + lane * LW, zero);
+			if (Pd != nullptr)
+				st_row(Pd + rt * pstride + (size_t)Nc * TILE + lane * LW, zerod);
+		}
 		return;
 	}
 	if (warp > Nc)
@@ -381,8 +406,11 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 		}
 	}
 	if (bl || m == MAX_EXP_START) {
-		for (int rt = 0; rt < RT; ++rt)
+		for (int rt = 0; rt < RT; ++rt) {
 			st_row(ps + rt * pstride, zero);
+			if (Pd != nullptr)
+				st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, zerod);
+		}
 		if (lane == 0) {
 			rmax[d] = -1;
 			max_exp[d] = MAX_EXP_START;
@@ -449,10 +477,12 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 			if (rt >= RT)
 				break;
 			float out[LW];
+			double outd[LW];
 #pragma unroll
 			for (int e = 0; e < LW; ++e) {
 				const int r = rt * TILE + lane * LW + e;
 				out[e] = 0.f;
+				outd[e] = 0.;
 				if (r < R) {
 					const double x = v[k][e];
 					bool kept = (r <= rstar) ? (x > lo) : (dadd(x, thr) > m);
@@ -473,10 +503,13 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 							}
 						}
 						out[e] = (P > PROB_MIN) ? (float)P : -(float)P;
+						outd[e] = (P > PROB_MIN) ? P : -P;
 					}
 				}
 			}
 			st_row(ps + rt * pstride, out);
+			if (Pd != nullptr)
+				st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, outd);
 		}
 	}
 	ll = warp_sum(ll);
@@ -693,14 +726,16 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 // carry ~1e-6 relative error into the next iteration's likelihoods.
 // The weight sum depends only on which orientations have psum_r > 0; when
 // that set is the one of a cached weight grid, with_weight is 0 and only the
-// model sums are accumulated.
+// model sums are accumulated. With views_final the tomograms already are the
+// views (background-aware update) and are not divided by psum_r.
 __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ psum_r,
                                                      const double *__restrict__ quats, int M, int R,
                                                      const double *__restrict__ qvals,
                                                      const double *__restrict__ corr,
                                                      const uint8_t *__restrict__ mask, int P, long long S,
-                                                     long long V, double *__restrict__ accum, int with_weight) {
+                                                     long long V, double *__restrict__ accum, int with_weight,
+                                                     int views_final) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ double s_ps[TILE];
@@ -747,7 +782,7 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 		Cell c = locate(s_rot[j], qx, qy, qz, center, S);
 		if (!c.ok)
 			continue;
-		const double wv = ((double)s_tile[i][j] / ps) / cr;
+		const double wv = views_final ? (double)s_tile[i][j] / cr : ((double)s_tile[i][j] / ps) / cr;
 		double fw[8];
 		corner_weights(c, fw);
 		double *a = accum + 2 * ((size_t)s_mode[j] * V + c.i000);
@@ -1102,7 +1137,7 @@ __global__ void __launch_bounds__(256) compact_prob_kernel(
 
 // Tomograms of orientations r0 .. r0 + n - 1 divided by psum_r where it is
 // positive (update_tomogram_nobg's final step, max_update.c:226-229), as
-// out [n][P] FP64.
+// out [n][P] FP64; with psum_r null (background path) T already holds them.
 __global__ void tomogram_kernel(const float *__restrict__ T, const double *__restrict__ psum_r, int P, int r0,
                                 int n, double *__restrict__ out) {
 	const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1110,7 +1145,7 @@ __global__ void tomogram_kernel(const float *__restrict__ T, const double *__res
 		return;
 	const int k = (int)(idx / P), p = (int)(idx - (long long)k * P), r = r0 + k;
 	const double v = T[((size_t)(r / TILE) * P + p) * TILE + r % TILE];
-	const double ps = psum_r[r];
+	const double ps = psum_r != nullptr ? psum_r[r] : 0.;
 	out[idx] = ps > 0. ? v / ps : v;
 }
 

@@ -124,9 +124,21 @@ class Iterate:
                 frames.append(CDataset(fn, det))
         else:
             raise ValueError("Need either in_photons_file or in_photons_list.")
-        for key in ("background_file", "background_list"):
-            if config.get(section_name, key, fallback=None) is not None:
-                raise NotImplementedError("background-aware reconstruction is not supported")
+        # per-pixel background (iterate.pyx:109-127); one detector here, so a
+        # background list must have one entry
+        bg_file = config.get(section_name, "background_file", fallback=None)
+        bg_list = config.get(section_name, "background_list", fallback=None)
+        if bg_file is not None and bg_list is not None:
+            raise ValueError("Both background_file and background_list specified. Pick one.")
+        if bg_list is not None:
+            bg_list = op.join(folder, bg_list)
+            with open(bg_list) as f:
+                lines = [ln.strip() for ln in f if ln.strip()]
+            if len(lines) != 1:
+                raise ValueError("Background list has %d entries but there are 1 unique detectors" % len(lines))
+            det.parse_background(op.join(op.dirname(bg_list), lines[0]))
+        elif bg_file is not None:
+            det.parse_background(op.join(folder, bg_file))
         self.dets = [det]
         self.set_data(frames)
 
@@ -140,6 +152,7 @@ class Iterate:
             except configparser.NoOptionError:
                 return ""
         model_file, scale_file = fname_opt("start_model_file"), fname_opt("scale_file")
+        bgscale_file = fname_opt("bgscale_file")
         if resume:
             with open(param.log_fname) as f:
                 last_iter = int(f.readlines()[-1].split()[0])
@@ -155,6 +168,7 @@ class Iterate:
         self.set_model(model)
         if param.need_scaling == 1:
             self.parse_scale(scale_file)
+            self.parse_scale(bgscale_file, bg=True)
         sel_string = config.get(section_name, "selection", fallback=None)
         self.parse_blacklist(fname_opt("blacklist_file"), sel_string)
         beta_str = config.get(section_name, "beta", fallback="auto")
@@ -204,9 +218,7 @@ class Iterate:
 
     # -- per-frame parameters -------------------------------------------------
     def parse_scale(self, fname, bg=False):
-        """iterate.pyx:284-315"""
-        if bg:
-            raise NotImplementedError("background scale factors are not supported")
+        """iterate.pyx:284-315; bg selects the per-frame background scales."""
         if not fname or not op.isfile(fname):
             if self.tot_num_data == 0:
                 raise AttributeError("Need tot_num_data to initialize scale factors")
@@ -225,7 +237,10 @@ class Iterate:
         elif self.tot_num_data > scale.shape[0]:
             print("Insufficient scale factors in file. Setting rest to unity")
             scale = np.append(scale, np.ones(self.tot_num_data - scale.shape[0]))
-        self.scale = scale.copy()
+        if bg:
+            self.bgscale = scale.copy()
+        else:
+            self.scale = scale.copy()
 
     def parse_blacklist(self, fname, sel_string=None, refresh=False):
         """iterate.pyx:317-359 (num_blacklist is left at 0, as there)."""

@@ -66,8 +66,6 @@ class EMCRecon:
         if itr.params.axial_sym > 1 or getattr(itr.quat, "icosahedral_flag", False) or \
                 getattr(itr.quat, "octahedral_flag", False):
             raise NotImplementedError("point-group and axial symmetrisation are not supported")
-        if itr.dets[0].with_bg and itr.params.need_scaling:
-            raise NotImplementedError("background-aware updates are not supported")
         from ._lib import Context
         if self.ctx is None:
             self.ctx = Context(self.device)
@@ -75,6 +73,8 @@ class EMCRecon:
         det = itr.dets[0]
         c.set_detector(det.qvals, det.corr, det.raw_mask)
         c.set_frames(*itr.merged_frames())
+        # background-aware updates (max_update.c:232-543, max_scale.c:21-288)
+        c.set_background(det.background if det.with_bg else None)
         c.set_quaternions(itr.quat.quats)
         c.set_model(itr.model.model1)
         itr.quat.divide(0, 1, itr.params.num_modes, itr.params.nonrot_modes)
@@ -99,6 +99,8 @@ class EMCRecon:
         c.set_beta_start(itr.beta_start)
         if par.need_scaling:
             c.set_scale(itr.scale)
+            if itr.dets[0].with_bg:
+                c.set_bgscale(itr.bgscale)
         beta_mean = self.update_beta()
         p = c.params(par.iteration, par.need_scaling, par.update_scale, par.known_scale, par.beta_jump,
                      par.beta_period, par.beta_factor)

@@ -92,6 +92,18 @@ DFG_API int dfg_set_blacklist(dfg_ctx *ctx, const uint8_t *blacklist);
 DFG_API int dfg_set_beta_start(dfg_ctx *ctx, const double *beta_start);
 DFG_API int dfg_calc_beta(dfg_ctx *ctx, double start, int need_scaling);
 
+/* Per-pixel background [num_pix] of the detector (CDetector.parse_background,
+ * detector.pyx:100-104; NULL removes it) and per-frame background scales
+ * [num_data] (Iterate.parse_scale(bg=True), iterate.pyx:146-171, 311-312; NULL
+ * means ones). With a background and need_scaling, dfg_maximize takes the
+ * background-aware E-step (max_prob.c:134-156), tomogram update by bracketed
+ * root finding (update_tomogram_bg, max_update.c:232-543) and scale update
+ * (update_scale_bg, max_scale.c:21-288); the powder sum it needs is formed
+ * from the frames (calc_powder, iterate.c:119-177). That path needs all frames
+ * in one chunk (DFG_ERR_NOMEM otherwise; see option pair_budget_mb). */
+DFG_API int dfg_set_background(dfg_ctx *ctx, const double *background);
+DFG_API int dfg_set_bgscale(dfg_ctx *ctx, const double *bgscale);
+
 /* ---- the iteration --------------------------------------------------------
  * update_beta (recon.pyx:151-174) then maximize (dragonfly/src/maximize.c:8-56):
  * rescale, E-step with the reference's pruning rule, normalisation, M-step,

@@ -152,6 +152,8 @@ class ReferenceEngine:
         L.ref_slice_merge.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _dp, _dp]
         L.ref_destroy.argtypes = [C.c_void_p]
         L.ref_set_save_prob.argtypes = [C.c_void_p, C.c_int]
+        L.ref_set_background.argtypes = [C.c_void_p, _dp, _dp]
+        L.ref_get_powder.argtypes = [C.c_void_p, _dp]
         L.ref_get_frame_prob.restype = C.c_int
         L.ref_get_frame_prob.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         self.save_prob = False
@@ -194,6 +196,17 @@ class ReferenceEngine:
         out = np.zeros(self.prob.num_pix)
         self.lib.ref_slice_gen(self.h, _c(quat, np.float64), int(mode), out)
         return out
+
+    def set_background(self, background, bgscale=None):
+        """Background-aware model (see ref_set_background); bgscale defaults
+        to ones (iterate.pyx:290-296)."""
+        p = self.prob
+        bg = _c(background, np.float64)
+        bs = _c(np.ones(p.num_data) if bgscale is None else bgscale, np.float64)
+        self.lib.ref_set_background(self.h, bg, bs)
+
+    def powder(self):
+        return self._arr(self.lib.ref_get_powder, self.prob.num_pix)
 
     def set_save_prob(self, on):
         """Makes maximize form the combined per-frame probability lists

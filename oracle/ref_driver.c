@@ -233,7 +233,22 @@ void ref_destroy(ref_engine *e) {
 	free(e->iter.fcounts); free(e->iter.mean_count); free(e->iter.rescale);
 	free(e->iter.blacklist); free(e->iter.sum_fact); free(e->iter.scale);
 	free(e->iter.beta); free(e->iter.beta_start);
+	free(e->det.background); free(e->det.powder); free(e->iter.bgscale);
 	free(e);
+}
+
+/* Background-aware model: per-pixel background (detector.pyx:100-104), per-frame
+ * background scale (iterate.pyx:146-171, 311-312) and the powder sum that the
+ * reference derives from the frames (calc_powder, iterate.c:119-177). With
+ * need_scaling, maximize then takes the background-aware E-step, tomogram and
+ * scale updates (max_prob.c:134-156, max_update.c:232-543, max_scale.c:21-288). */
+void ref_set_background(ref_engine *e, const double *background, const double *bgscale) {
+	free(e->det.background);
+	free(e->iter.bgscale);
+	e->det.background = dup_mem(background, (size_t)e->det.num_pix * sizeof(double));
+	e->iter.bgscale = dup_mem(bgscale, (size_t)e->iter.tot_num_data * sizeof(double));
+	e->det.with_bg = 1;
+	calc_powder(&e->iter);
 }
 
 /* ---- accessors (copies; arrays that a call did not produce are zero-filled) ---- */
@@ -246,6 +261,9 @@ static void copy_or_zero(void *dst, const void *src, size_t bytes) {
 }
 
 long ref_model_len(ref_engine *e) { return e->mod.num_modes * e->mod.vol; }
+void ref_get_powder(ref_engine *e, double *o) {
+	copy_or_zero(o, e->det.powder, (size_t)e->det.num_pix * sizeof(double));
+}
 void ref_get_model1(ref_engine *e, double *o) { memcpy(o, e->mod.model1, ref_model_len(e) * sizeof(double)); }
 void ref_set_model1(ref_engine *e, const double *i) { memcpy(e->mod.model1, i, ref_model_len(e) * sizeof(double)); }
 void ref_get_model2(ref_engine *e, double *o) { memcpy(o, e->mod.model2, ref_model_len(e) * sizeof(double)); }
