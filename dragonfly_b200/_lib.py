@@ -60,6 +60,7 @@ _SIGS = {
     "dfg_get_scalars": (C.c_int, [_V, _D]),
     "dfg_get_num_prob": (C.c_int, [_V, _I]),
     "dfg_set_background": (C.c_int, [_V, _D]),
+    "dfg_set_symmetry": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
     "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
     "dfg_get_sparse_prob": (C.c_int, [_V, _I, _D]),
@@ -173,6 +174,11 @@ class Context:
             m = m[None]
         self.call("dfg_set_model", m.shape[-1], m.shape[0], ptr(m, C.c_double))
         self.model_shape = m.shape
+
+    def set_symmetry(self, point_group=0, axial_order=0):
+        """Model symmetries of update_model: point_group 0 (Friedel only),
+        1 (S4) or 2 (A5); axial_order > 1 adds the axial symmetry."""
+        self.call("dfg_set_symmetry", int(point_group), int(axial_order))
 
     def set_background(self, background):
         """Per-pixel background (None: none); with need_scaling the iteration

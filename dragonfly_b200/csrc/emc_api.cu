@@ -951,6 +951,118 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	return DFG_OK;
 }
 
+// Rotation lists of the model symmetries, row-major 3x3 each.
+// S4 (octahedral, symmetrize_octahedral model.c:636-729): the 48 signed
+// permutation matrices. A5 (icosahedral, symmetrize_icosahedral model.c:573-757):
+// the 60 rotations of the icosahedron whose vertices are the cyclic
+// permutations of (0, +-tau, +-1), the one the reference's table preserves,
+// generated by the cyclic axis permutation, diag(-1, -1, 1) and the 72-degree
+// rotation about the vertex axis (0, tau, 1), entries snapped to their exact
+// values (the reference's table gives them to 11 decimals). Axial (symmetrize_axial model.c:527-571): rotations by
+// 2 pi i / order about z, from cos / sin as the reference forms them.
+static std::vector<double> octahedral_rotations() {
+	std::vector<double> out;
+	const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+	for (const auto &pm : perms)
+		for (int sg = 0; sg < 8; ++sg) {
+			double R[9] = {0};
+			for (int i = 0; i < 3; ++i)
+				R[3 * i + pm[i]] = (sg >> (2 - i)) & 1 ? -1. : 1.;
+			out.insert(out.end(), R, R + 9);
+		}
+	return out;
+}
+
+static std::vector<double> icosahedral_rotations() {
+	const double t = (1. + std::sqrt(5.)) / 2.;
+	const double exact[5] = {0., 0.5, 1., t / 2., 1. / (2. * t)};
+	auto snap = [&](double x) {
+		double best = x, bd = 1e300;
+		for (double e : exact)
+			for (double sg : {1., -1.})
+				if (std::fabs(x - sg * e) < bd) {
+					bd = std::fabs(x - sg * e);
+					best = sg * e;
+				}
+		return best;
+	};
+	auto mul = [&](const double *A, const double *B, double *C) {
+		for (int i = 0; i < 3; ++i)
+			for (int j = 0; j < 3; ++j) {
+				double v = 0.;
+				for (int k = 0; k < 3; ++k)
+					v += A[3 * i + k] * B[3 * k + j];
+				C[3 * i + j] = snap(v);
+			}
+	};
+	// 72-degree rotation about the unit axis along (0, tau, 1) (Rodrigues)
+	const double nrm = std::sqrt(1. + t * t), ax[3] = {0., t / nrm, 1. / nrm};
+	const double c5 = std::cos(2. * M_PI / 5.), s5 = std::sin(2. * M_PI / 5.);
+	double F[9];
+	for (int i = 0; i < 3; ++i)
+		for (int j = 0; j < 3; ++j) {
+			double v = (i == j ? c5 : 0.) + (1. - c5) * ax[i] * ax[j];
+			const int k = 3 - i - j;  // the remaining axis for the cross-product term
+			if (i != j) {
+				const double sgn = ((i + 1) % 3 == j) ? -1. : 1.;
+				v += sgn * s5 * ax[k];
+			}
+			F[3 * i + j] = snap(v);
+		}
+	const double P[9] = {0, 0, 1, 1, 0, 0, 0, 1, 0}, D[9] = {-1, 0, 0, 0, -1, 0, 0, 0, 1};
+	std::vector<std::vector<double>> group = {{1, 0, 0, 0, 1, 0, 0, 0, 1}};
+	const double *gens[3] = {P, D, F};
+	for (size_t i = 0; i < group.size() && group.size() < 60; ++i)
+		for (const double *g : gens) {
+			std::vector<double> C(9);
+			mul(group[i].data(), g, C.data());
+			bool found = false;
+			for (const auto &h : group) {
+				double d = 0.;
+				for (int k = 0; k < 9; ++k)
+					d += std::fabs(h[k] - C[k]);
+				if (d < 1e-9) {
+					found = true;
+					break;
+				}
+			}
+			if (!found)
+				group.push_back(C);
+		}
+	std::vector<double> out;
+	for (const auto &g : group)
+		out.insert(out.end(), g.begin(), g.end());
+	return out;
+}
+
+extern "C" int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(point_group >= 0 && point_group <= 2, DFG_ERR_ARG, "point_group must be 0 (none), 1 (S4) or 2 (A5)");
+	NEED(axial_order >= 0, DFG_ERR_ARG, "axial_order must be >= 0");
+	CK(cudaSetDevice(ctx->device));
+	ctx->n_group_rots = 0;
+	if (point_group > 0) {
+		std::vector<double> r = point_group == 1 ? octahedral_rotations() : icosahedral_rotations();
+		NEED(r.size() == (point_group == 1 ? 48u : 60u) * 9u, DFG_ERR_STATE, "symmetry group generation failed");
+		CK(upload(ctx->group_rots, r.data(), r.size(), ctx->stream));
+		ctx->n_group_rots = (int)(r.size() / 9);
+	}
+	ctx->n_axial_rots = 0;
+	if (axial_order > 1) {
+		std::vector<double> r;
+		for (int i = 0; i < axial_order; ++i) {
+			const double angle = 2. * M_PI * i / axial_order, c = std::cos(angle), s = std::sin(angle);
+			const double R[9] = {c, -s, 0., s, c, 0., 0., 0., 1.};
+			r.insert(r.end(), R, R + 9);
+		}
+		CK(upload(ctx->axial_rots, r.data(), r.size(), ctx->stream));
+		ctx->n_axial_rots = axial_order;
+	}
+	CK(cudaStreamSynchronize(ctx->stream));
+	return DFG_OK;
+}
+
 extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) {
 	if (!ctx)
 		return DFG_ERR_ARG;
@@ -961,15 +1073,38 @@ extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) 
 	const int S = (int)ctx->S, lo = (S % 2 == 0) ? 1 : 0;
 	const long long pairs = (long long)ctx->M * (S - lo) * (S - lo) * (S / 2 - lo + 1);
 	phase_begin(ctx, PH_UPDATE);
-	friedel_kernel<<<blocks_for(pairs, 256), 256, 0, st>>>(ctx->model2.p, ctx->weight.p, S, ctx->M);
-	CKL("friedel_kernel");
+	int launched = 3;
+	// recon.pyx:120-134: the point group replaces the Friedel average; the
+	// axial symmetry applies after either
+	auto symmetrize = [&](const DevBuf<double> &rots, int nrot) -> int {
+		for (int mode = 0; mode < ctx->M; ++mode) {
+			double *m2 = ctx->model2.p + (size_t)mode * ctx->V, *w = ctx->weight.p + (size_t)mode * ctx->V;
+			symmetrize_kernel<<<blocks_for(ctx->V, 256), 256, 0, st>>>(m2, w, S, rots.p, nrot, ctx->accum.p);
+			CKL("symmetrize_kernel");
+			symmetrize_finish_kernel<<<blocks_for(ctx->V, 256), 256, 0, st>>>(ctx->accum.p, ctx->V, m2, w);
+			CKL("symmetrize_finish_kernel");
+			launched += 2;
+		}
+		return DFG_OK;
+	};
+	if (ctx->n_group_rots > 0) {
+		if (int rc = symmetrize(ctx->group_rots, ctx->n_group_rots))
+			return rc;
+	} else {
+		friedel_kernel<<<blocks_for(pairs, 256), 256, 0, st>>>(ctx->model2.p, ctx->weight.p, S, ctx->M);
+		CKL("friedel_kernel");
+		launched++;
+	}
+	if (ctx->n_axial_rots > 1)
+		if (int rc = symmetrize(ctx->axial_rots, ctx->n_axial_rots))
+			return rc;
 	const unsigned nb = blocks_for(n, 256);
 	divide_update_kernel<float><<<nb, 256, 0, st>>>(ctx->model2.p, ctx->weight.p, ctx->model1.p, nullptr, n,
 	                                                alpha, ctx->red_part.p);
 	CKL("divide_update_kernel");
 	sum_kernel<<<1, 1024, 0, st>>>(ctx->red_part.p, nb, ctx->scalars.p + 3);
 	CKL("sum_kernel");
-	phase_end(ctx, PH_UPDATE, 3);
+	phase_end(ctx, PH_UPDATE, launched - 1);
 	double change = 0.;
 	CK(cudaMemcpyAsync(&change, ctx->scalars.p + 3, sizeof(double), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));

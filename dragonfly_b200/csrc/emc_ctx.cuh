@@ -129,6 +129,10 @@ struct dfg_ctx {
 	// bgscale [N], scalemax [R] and the work buffers of the scale search
 	bool with_bg = false, powder_valid = false;
 	bool views_final = false;  // T holds the final views (background path), not sums
+	// model symmetries applied by update_model: a point group (S4 / A5) in
+	// place of the Friedel average, then an axial symmetry
+	DevBuf<double> group_rots, axial_rots;
+	int n_group_rots = 0, n_axial_rots = 0;
 	std::vector<double> h_bgscale;
 	DevBuf<double> background, powder, bgscale, scalemax, smax_part, gd_part, gd_G, gd_s;
 	DevBuf<double> Wd;  // slices W [RT][P+1][TILE] in FP64 (background-aware E-step)

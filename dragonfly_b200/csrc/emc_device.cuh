@@ -903,6 +903,69 @@ __global__ void __launch_bounds__(256) divide_update_kernel(double *__restrict__
 	}
 }
 
+// Point-group and axial symmetrisation (symmetrize_octahedral /
+// symmetrize_icosahedral / symmetrize_axial, model.c:527-757, with
+// rotate_model_openmp :423-468): for every voxel v = (vx, vy, vz) - c with
+// vx, vy, vz in [0, S-2], sum over the n rotations g, in list order, of the
+// trilinear sample of model2 * weight and of weight at g v + c (samples
+// outside [0, S-1) are skipped); out = (sum A, sum W). One thread per voxel,
+// FP64 in the reference's operation order. The plane index S-1 stays zero,
+// as in the reference.
+__global__ void symmetrize_kernel(const double *__restrict__ model2, const double *__restrict__ weight, int S,
+                                  const double *__restrict__ rots, int n, double2 *__restrict__ out) {
+	const long long V = (long long)S * S * S;
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= V)
+		return;
+	const int iz = (int)(i % S), iy = (int)((i / S) % S), ix = (int)(i / ((long long)S * S));
+	double sa = 0., sw = 0.;
+	if (ix < S - 1 && iy < S - 1 && iz < S - 1) {
+		const int c = S / 2;
+		const double vx = (double)(ix - c), vy = (double)(iy - c), vz = (double)(iz - c), cd = (double)c;
+		const long long SS = (long long)S * S;
+		for (int g = 0; g < n; ++g) {
+			const double *R = rots + 9 * g;
+			double rv[3];
+#pragma unroll
+			for (int k = 0; k < 3; ++k)
+				rv[k] = dadd(dadd(dadd(dmul(R[3 * k], vx), dmul(R[3 * k + 1], vy)), dmul(R[3 * k + 2], vz)), cd);
+			if (rv[0] < 0. || rv[0] >= S - 1 || rv[1] < 0. || rv[1] >= S - 1 || rv[2] < 0. || rv[2] >= S - 1)
+				continue;
+			const int x = (int)rv[0], y = (int)rv[1], z = (int)rv[2];
+			const double fx = dsub(rv[0], (double)x), fy = dsub(rv[1], (double)y), fz = dsub(rv[2], (double)z);
+			const double cx = dsub(1., fx), cy = dsub(1., fy), cz = dsub(1., fz);
+			const double wts[8] = {dmul(dmul(cx, cy), cz), dmul(dmul(cx, cy), fz), dmul(dmul(cx, fy), cz),
+			                       dmul(dmul(cx, fy), fz), dmul(dmul(fx, cy), cz), dmul(dmul(fx, cy), fz),
+			                       dmul(dmul(fx, fy), cz), dmul(dmul(fx, fy), fz)};
+			const long long b = x * SS + (long long)y * S + z;
+			const long long o[8] = {0, 1, S, S + 1, SS, SS + 1, SS + S, SS + S + 1};
+			double ta = 0., tw = 0.;
+#pragma unroll
+			for (int q = 0; q < 8; ++q) {
+				const double w = __ldg(weight + b + o[q]);
+				const double a = dmul(__ldg(model2 + b + o[q]), w);
+				ta = q == 0 ? dmul(wts[q], a) : dadd(ta, dmul(wts[q], a));
+				tw = q == 0 ? dmul(wts[q], w) : dadd(tw, dmul(wts[q], w));
+			}
+			sa = dadd(sa, ta);
+			sw = dadd(sw, tw);
+		}
+	}
+	out[i] = make_double2(sa, sw);
+}
+
+// model2 = sum A / sum W where sum W > 0 (else 0), weight = sum W
+// (model.c:553-569, 715-729, 751-756).
+__global__ void symmetrize_finish_kernel(const double2 *__restrict__ in, long long n, double *__restrict__ model2,
+                                         double *__restrict__ weight) {
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const double2 v = in[i];
+	model2[i] = v.y > 0. ? v.x / v.y : 0.;
+	weight[i] = v.y;
+}
+
 // Fixed-order sum of n doubles by one block (second stage of reductions).
 __global__ void __launch_bounds__(1024) sum_kernel(const double *__restrict__ x, long long n,
                                                    double *__restrict__ out) {

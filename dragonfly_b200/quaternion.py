@@ -46,8 +46,14 @@ class Quaternion:
             if len(num_div) == 2:
                 self.voronoi_subset(int(num_div[1]))
             point_group = config.get(section_name, "point_group", fallback="1")
-            if point_group in ("A5", "S4"):
-                raise NotImplementedError("point-group reduction (%s) is not supported" % point_group)
+            if point_group == "A5":
+                print("Reducing to A5 sub-group")
+                self.reduce_icosahedral()
+                self.icosahedral_flag = True
+            elif point_group == "S4":
+                print("Reducing to S4 sub-group")
+                self.reduce_octahedral()
+                self.octahedral_flag = True
             elif point_group != "1":
                 raise ValueError("Unknown point group: " + point_group)
 
@@ -111,10 +117,58 @@ class Quaternion:
         return out
 
     def reduce_icosahedral(self, return_sym=False):
-        raise NotImplementedError("point-group reduction is not supported")
+        """Keep the orientations whose nearest (Euclidean, first on ties) of
+        the 60 vertex quaternions of the 600-cell is vertex 8, the identity;
+        it goes first, and weights are kept (quaternion.pyx:177-209)."""
+        from scipy.spatial import distance
+        if self._quats is None:
+            raise AttributeError("Generate quaternion first before reducing")
+        if self.reduced:
+            print("Already reduced")
+            return self.num_rot
+        quats = self._quats
+        sel = np.where(distance.cdist(quats[:60, :4], quats[60:, :4]).argmin(axis=0) == 8)[0]
+        self._quats = np.ascontiguousarray(np.concatenate([quats[8:9], quats[60 + sel]]))
+        self.reduced = True
+        return quats[:60, :4].copy() if return_sym else self.num_rot
+
+    @staticmethod
+    def octahedral_quaternions():
+        """The 24 unit quaternions of the octahedral rotation group, with the
+        signs and order of quaternion.pyx:227-241 (the identity first): the
+        four axes, (1, +-1, +-1, +-1) / 2, the 90-degree turns
+        (1, +-e_i) / sqrt 2 and the six edge turns (0, e_i +- e_j) / sqrt 2."""
+        q = np.zeros((24, 4))
+        q[:4] = np.identity(4)
+        v = np.sqrt(0.5)
+        for k, (a, b, c) in enumerate(np.ndindex(2, 2, 2)):
+            q[4 + k] = [0.5, (a * 2 - 1) * 0.5, (b * 2 - 1) * 0.5, (c * 2 - 1) * 0.5]
+        for i in range(3):
+            q[12 + i, 0] = q[12 + i, 1 + i] = v
+            q[15 + i, 0], q[15 + i, 1 + i] = v, -v
+        k = 18
+        for i in range(3):
+            for j in range(3):
+                if i != j:
+                    q[k, 1 + i], q[k, 1 + j] = v, (-v if i < j else v)
+                    k += 1
+        return q
 
     def reduce_octahedral(self, return_sym=False):
-        raise NotImplementedError("point-group reduction is not supported")
+        """Keep the orientations whose nearest (Euclidean, first on ties) of
+        the 24 octahedral-group quaternions is the identity; weights are
+        kept (quaternion.pyx:211-255)."""
+        from scipy.spatial import distance
+        if self._quats is None:
+            raise AttributeError("Generate quaternion first before reducing")
+        if self.reduced:
+            print("Already reduced")
+            return self.num_rot
+        cube = self.octahedral_quaternions()
+        sel = np.where(distance.cdist(cube, self._quats[:, :4]).argmin(axis=0) == 0)[0]
+        self._quats = np.ascontiguousarray(self._quats[sel])
+        self.reduced = True
+        return cube if return_sym else self.num_rot
 
     def free(self):
         self._quats = None

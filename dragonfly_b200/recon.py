@@ -63,9 +63,6 @@ class EMCRecon:
             raise NotImplementedError("non-rotating modes are not supported")
         if itr.params.refine:
             raise NotImplementedError("orientation refinement is not supported")
-        if itr.params.axial_sym > 1 or getattr(itr.quat, "icosahedral_flag", False) or \
-                getattr(itr.quat, "octahedral_flag", False):
-            raise NotImplementedError("point-group and axial symmetrisation are not supported")
         from ._lib import Context
         if self.ctx is None:
             self.ctx = Context(self.device)
@@ -77,6 +74,9 @@ class EMCRecon:
         c.set_background(det.background if det.with_bg else None)
         c.set_quaternions(itr.quat.quats)
         c.set_model(itr.model.model1)
+        # update_model's symmetries (recon.pyx:120-134)
+        pg = 2 if itr.quat.icosahedral_flag else (1 if itr.quat.octahedral_flag else 0)
+        c.set_symmetry(pg, itr.params.axial_sym if itr.params.axial_sym > 1 else 0)
         itr.quat.divide(0, 1, itr.params.num_modes, itr.params.nonrot_modes)
         itr.params.rank, itr.params.num_proc = 0, 1
         self._iter = itr

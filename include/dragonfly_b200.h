@@ -119,6 +119,16 @@ DFG_API int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_l
  * (alpha = 0) or alpha * model1 + (1 - alpha) * model2. */
 DFG_API int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change);
 
+/* Model symmetries applied by dfg_update_model, as EMCRecon.update_model
+ * (recon.pyx:120-134): point_group 1 (S4, Quaternion point_group 'S4') or 2
+ * (A5, 'A5') replaces the Friedel average by symmetrize_octahedral /
+ * symmetrize_icosahedral (model.c:636-757); axial_order > 1 then applies
+ * symmetrize_axial (params.axial_sym, model.c:527-571). 0 and 0 restore the
+ * default (Friedel only). The orientation list is reduced to the group's
+ * asymmetric unit on the host (Quaternion.reduce_octahedral /
+ * reduce_icosahedral, quaternion.pyx:177-255). */
+DFG_API int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order);
+
 /* Iterate.normalize_scale (dragonfly/iterate.pyx:361-384): mean phi over
  * good frames, mode-0 model1 *= mean, phi /= mean. Writes the mean. */
 DFG_API int dfg_normalize_scale(dfg_ctx *ctx, double *mean_scale);

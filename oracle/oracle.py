@@ -152,6 +152,7 @@ class ReferenceEngine:
         L.ref_slice_merge.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _dp, _dp]
         L.ref_destroy.argtypes = [C.c_void_p]
         L.ref_set_save_prob.argtypes = [C.c_void_p, C.c_int]
+        L.ref_set_symmetry.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.ref_set_background.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_get_powder.argtypes = [C.c_void_p, _dp]
         L.ref_get_frame_prob.restype = C.c_int
@@ -207,6 +208,10 @@ class ReferenceEngine:
 
     def powder(self):
         return self._arr(self.lib.ref_get_powder, self.prob.num_pix)
+
+    def set_symmetry(self, point_group=0, axial_order=0):
+        """Model symmetries of update_model: point_group 1 = S4, 2 = A5."""
+        self.lib.ref_set_symmetry(self.h, int(point_group), int(axial_order))
 
     def set_save_prob(self, on):
         """Makes maximize form the combined per-frame probability lists

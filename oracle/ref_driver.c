@@ -197,14 +197,27 @@ double ref_maximize(ref_engine *e, int iteration) {
 	return e->avg_likelihood;
 }
 
-/* recon.pyx:112-149 for RECON3D without point-group or axial symmetry. */
+/* recon.pyx:112-149 for RECON3D: the icosahedral or octahedral point group
+ * (Quaternion.icosahedral_flag / octahedral_flag) in place of the Friedel
+ * average, then the axial symmetry (params.axial_sym), then the division. */
 double ref_update_model(ref_engine *e) {
 	long x;
 	double diff, change = 0.;
 	struct model *mod = &e->mod;
 
-	for (x = 0; x < mod->num_modes; ++x)
-		symmetrize_friedel(&mod->model2[x * mod->vol], &mod->inter_weight[x * mod->vol], (int)mod->size);
+	for (x = 0; x < mod->num_modes; ++x) {
+		double *m2 = &mod->model2[x * mod->vol], *w = &mod->inter_weight[x * mod->vol];
+		if (e->quat.icosahedral_flag)
+			symmetrize_icosahedral(m2, w, (int)mod->size);
+		else if (e->quat.octahedral_flag)
+			symmetrize_octahedral(m2, w, (int)mod->size);
+		else
+			symmetrize_friedel(m2, w, (int)mod->size);
+	}
+	if (e->par.axial_sym > 1)
+		for (x = 0; x < mod->num_modes; ++x)
+			symmetrize_axial(&mod->model2[x * mod->vol], &mod->inter_weight[x * mod->vol], (int)mod->size,
+			                 e->par.axial_sym);
 	for (x = 0; x < mod->num_modes * mod->vol; ++x)
 		if (mod->inter_weight[x] > 0.)
 			mod->model2[x] /= mod->inter_weight[x];
@@ -279,6 +292,14 @@ void ref_get_frame_arrays(ref_engine *e, int *rmax, double *info, double *likeli
 	copy_or_zero(max_exp, c->max_exp, n * sizeof(double));
 	copy_or_zero(p_norm, c->p_norm, n * sizeof(double));
 	copy_or_zero(psum_d, c->psum_d, n * sizeof(double));
+}
+
+/* Model symmetries of update_model: point_group 1 = S4 (octahedral_flag),
+ * 2 = A5 (icosahedral_flag), 0 = none; axial_order = params.axial_sym. */
+void ref_set_symmetry(ref_engine *e, int point_group, int axial_order) {
+	e->quat.octahedral_flag = point_group == 1;
+	e->quat.icosahedral_flag = point_group == 2;
+	e->par.axial_sym = axial_order > 1 ? axial_order : 1;
 }
 
 /* Asks the reference to form the combined per-frame probability lists (the
