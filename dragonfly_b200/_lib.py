@@ -60,6 +60,8 @@ _SIGS = {
     "dfg_get_scalars": (C.c_int, [_V, _D]),
     "dfg_get_num_prob": (C.c_int, [_V, _I]),
     "dfg_set_background": (C.c_int, [_V, _D]),
+    "dfg_load_emc": (C.c_int, [_V, C.c_int, C.POINTER(C.c_char_p)]),
+    "dfg_save_emc": (C.c_int, [_V, C.c_char_p]),
     "dfg_set_symmetry": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
     "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
@@ -174,6 +176,18 @@ class Context:
             m = m[None]
         self.call("dfg_set_model", m.shape[-1], m.shape[0], ptr(m, C.c_double))
         self.model_shape = m.shape
+
+    def load_emc(self, paths):
+        """Frames from binary .emc files (sparse, or dense integer made
+        sparse), concatenated in order; replaces set_frames."""
+        paths = [paths] if isinstance(paths, (str, bytes, os.PathLike)) else list(paths)
+        arr = (C.c_char_p * len(paths))(*[os.fsencode(p) for p in paths])
+        self.call("dfg_load_emc", len(paths), arr)
+        self.num_data = int(self.workload()["num_data"])
+
+    def save_emc(self, path):
+        """The context's frames as one sparse binary .emc file."""
+        self.call("dfg_save_emc", os.fsencode(path))
 
     def set_symmetry(self, point_group=0, axial_order=0):
         """Model symmetries of update_model: point_group 0 (Friedel only),

@@ -164,3 +164,88 @@ extern "C" int dfg_get_frames(dfg_ctx *ctx, int *ones, int *multi, int *place_on
 	cp(count_multi, ctx->h_count_multi);
 	return DFG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// .emc files (binary): a 1024-byte header of int32 num_data, num_pix, ftype,
+// then for ftype 0 (sparse) int32 ones[num_data], multi[num_data],
+// place_ones[], place_multi[], count_multi[] (emcfile.c:3-57,
+// emcfile.pyx:491-532); for ftype 1 int32 frames [num_data][num_pix].
+// ---------------------------------------------------------------------------
+extern "C" int dfg_load_emc(dfg_ctx *ctx, int num_files, const char *const *paths) {
+	if (!ctx || num_files < 1 || !paths)
+		return DFG_ERR_ARG;
+	NEED(ctx->P > 0, DFG_ERR_STATE, "load_emc: set the detector first");
+	std::vector<int> ones, multi, po, pm, cm;
+	for (int f = 0; f < num_files; ++f) {
+		FILE *fp = fopen(paths[f], "rb");
+		NEED(fp != nullptr, DFG_ERR_ARG, "load_emc: cannot open %s", paths[f]);
+		int hdr[3] = {0, 0, -1};
+		bool ok = fread(hdr, sizeof(int), 3, fp) == 3 && fseek(fp, 1024, SEEK_SET) == 0;
+		const int nd = hdr[0], npx = hdr[1], ftype = hdr[2];
+		if (!ok || nd < 0 || npx != ctx->P || (ftype != 0 && ftype != 1)) {
+			fclose(fp);
+			return ctx->fail(DFG_ERR_ARG,
+			                 "load_emc: %s: %d frames x %d pixels, type %d (need %d pixels, type 0 sparse or 1 "
+			                 "dense integer)",
+			                 paths[f], nd, npx, ftype, ctx->P);
+		}
+		auto rd = [&](std::vector<int> &v, size_t n) {
+			const size_t o = v.size();
+			v.resize(o + n);
+			return n == 0 || fread(v.data() + o, sizeof(int), n, fp) == n;
+		};
+		if (ftype == 0) {
+			const size_t o0 = ones.size(), m0 = multi.size();
+			ok = rd(ones, (size_t)nd) && rd(multi, (size_t)nd);
+			long long so = 0, sm = 0;
+			for (int d = 0; ok && d < nd; ++d) {
+				so += ones[o0 + d];
+				sm += multi[m0 + d];
+			}
+			ok = ok && rd(po, (size_t)so) && rd(pm, (size_t)sm) && rd(cm, (size_t)sm);
+		} else {
+			// dense integer frames become sparse (count 1 -> ones, > 1 -> multi)
+			std::vector<int> fr((size_t)npx);
+			for (int d = 0; ok && d < nd; ++d) {
+				ok = fread(fr.data(), sizeof(int), (size_t)npx, fp) == (size_t)npx;
+				int n1 = 0, nm = 0;
+				for (int t = 0; ok && t < npx; ++t) {
+					if (fr[t] == 1) {
+						po.push_back(t);
+						n1++;
+					} else if (fr[t] > 1) {
+						pm.push_back(t);
+						cm.push_back(fr[t]);
+						nm++;
+					}
+				}
+				ones.push_back(n1);
+				multi.push_back(nm);
+			}
+		}
+		fclose(fp);
+		NEED(ok, DFG_ERR_ARG, "load_emc: %s is truncated", paths[f]);
+	}
+	NEED(!ones.empty(), DFG_ERR_ARG, "load_emc: no frames");
+	return dfg_set_frames(ctx, (int)ones.size(), ones.data(), multi.data(), po.data(), pm.data(), cm.data());
+}
+
+extern "C" int dfg_save_emc(dfg_ctx *ctx, const char *path) {
+	if (!ctx || !path)
+		return DFG_ERR_ARG;
+	NEED(ctx->N > 0, DFG_ERR_STATE, "save_emc: no frames set");
+	FILE *fp = fopen(path, "wb");
+	NEED(fp != nullptr, DFG_ERR_ARG, "save_emc: cannot create %s", path);
+	std::vector<char> hdr(1024, 0);
+	const int h[3] = {ctx->N, ctx->P, 0};
+	memcpy(hdr.data(), h, sizeof(h));
+	auto wr = [&](const void *p, size_t bytes) { return bytes == 0 || fwrite(p, 1, bytes, fp) == bytes; };
+	const bool ok = wr(hdr.data(), hdr.size()) && wr(ctx->h_ones.data(), ctx->h_ones.size() * sizeof(int)) &&
+	                wr(ctx->h_multi.data(), ctx->h_multi.size() * sizeof(int)) &&
+	                wr(ctx->h_place_ones.data(), ctx->h_place_ones.size() * sizeof(int)) &&
+	                wr(ctx->h_place_multi.data(), ctx->h_place_multi.size() * sizeof(int)) &&
+	                wr(ctx->h_count_multi.data(), ctx->h_count_multi.size() * sizeof(int));
+	const bool closed = fclose(fp) == 0;
+	NEED(ok && closed, DFG_ERR_ARG, "save_emc: writing %s failed", path);
+	return DFG_OK;
+}

@@ -209,6 +209,14 @@ DFG_API int dfg_simulate_frames(dfg_ctx *ctx, long size, const double *intens, i
 DFG_API int dfg_get_frames(dfg_ctx *ctx, int *ones, int *multi, int *place_ones, int *place_multi,
                            int *count_multi);
 
+/* Binary .emc files (1024-byte header of int32 num_data, num_pix, type): load
+ * one or more (type 0 sparse, or type 1 dense integer, turned sparse) into the
+ * context as dfg_set_frames would; save the context's frames as one sparse
+ * file. Replace CDataset / EMCReader parsing (parse_binarydataset,
+ * emcfile.c:3-57; emcfile.pyx:200-330) and EMCWriter (emcfile.pyx:420-532). */
+DFG_API int dfg_load_emc(dfg_ctx *ctx, int num_files, const char *const *paths);
+DFG_API int dfg_save_emc(dfg_ctx *ctx, const char *path);
+
 /* ---- tuning and instrumentation ------------------------------------------
  * Options: "pair_budget_mb" (device memory for the per-pair buffers, which
  * sets the frame chunk), "timing" (1: record per-phase CUDA-event times). */
