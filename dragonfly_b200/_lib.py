@@ -63,6 +63,8 @@ _SIGS = {
     "dfg_load_emc": (C.c_int, [_V, C.c_int, C.POINTER(C.c_char_p)]),
     "dfg_save_emc": (C.c_int, [_V, C.c_char_p]),
     "dfg_set_symmetry": (C.c_int, [_V, C.c_int, C.c_int]),
+    "dfg_set_refinement": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_longlong), _I]),
+    "dfg_voronoi_subset": (C.c_int, [_V, C.c_int, _D, C.c_int, _D, _I]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
     "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
     "dfg_get_sparse_prob": (C.c_int, [_V, _I, _D]),
@@ -193,6 +195,31 @@ class Context:
         """Model symmetries of update_model: point_group 0 (Friedel only),
         1 (S4) or 2 (A5); axial_order > 1 adds the axial symmetry."""
         self.call("dfg_set_symmetry", int(point_group), int(axial_order))
+
+    def set_refinement(self, num_coarse=0, quat_mapping=None, rel_quat=None):
+        """Coarse-to-fine refinement: frame d evaluates orientation r only
+        when quat_mapping[r] is in rel_quat[d] (a sequence of per-frame
+        coarse-orientation lists). quat_mapping None switches it off."""
+        if quat_mapping is None:
+            self.call("dfg_set_refinement", 0, None, None, None)
+            return
+        qm = np.ascontiguousarray(quat_mapping, np.int32).ravel()
+        lens = np.array([len(x) for x in rel_quat], np.int64)
+        off = np.zeros(len(lens) + 1, np.int64)
+        np.cumsum(lens, out=off[1:])
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in rel_quat])
+                                    if len(lens) else np.zeros(0, np.int32), np.int32)
+        self.call("dfg_set_refinement", int(num_coarse), ptr(qm, C.c_int), ptr(off, C.c_longlong),
+                  ptr(flat, C.c_int))
+
+    def voronoi_subset(self, coarse, fine):
+        """Nearest coarse orientation of every fine one (rows of five)."""
+        c = np.ascontiguousarray(coarse, np.float64)
+        f = np.ascontiguousarray(fine, np.float64)
+        out = np.empty(f.shape[0], np.int32)
+        self.call("dfg_voronoi_subset", c.shape[0], ptr(c, C.c_double), f.shape[0], ptr(f, C.c_double),
+                  ptr(out, C.c_int))
+        return out
 
     def set_background(self, background):
         """Per-pixel background (None: none); with need_scaling the iteration

@@ -228,6 +228,7 @@ extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const
 	ctx->beta_set = false;
 	ctx->chunks_R = -1;
 	ctx->have_results = false;
+	ctx->refine = false;  // relevant orientations are per frame
 	return DFG_OK;
 }
 
@@ -239,6 +240,8 @@ extern "C" int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quat
 		NEED(std::isfinite(quats[i]), DFG_ERR_ARG, "quaternions: entry %lld is not finite", i);
 	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
+	if (num_rot != ctx->num_rot)
+		ctx->refine = false;  // the coarse map was made for the previous set
 	ctx->num_rot = num_rot;
 	CK(upload(ctx->quats, quats, 5 * (size_t)num_rot, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
@@ -268,6 +271,66 @@ extern "C" int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const doubl
 
 static int need_frames(dfg_ctx *ctx) {
 	NEED(ctx->N > 0, DFG_ERR_STATE, "set the frames first");
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
+                                  const long long *rel_off, const int *rel_quat) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	if (quat_mapping == nullptr) {
+		ctx->refine = false;
+		return DFG_OK;
+	}
+	if (int rc = need_frames(ctx))
+		return rc;
+	NEED(ctx->num_rot > 0, DFG_ERR_STATE, "refinement: set the quaternions first");
+	NEED(num_coarse > 0 && rel_off && (rel_quat || rel_off[ctx->N] == 0), DFG_ERR_ARG,
+	     "refinement: need num_coarse > 0 and the per-frame lists");
+	const int N = ctx->N, rw = (num_coarse + 31) / 32;
+	for (int r = 0; r < ctx->num_rot; ++r)
+		NEED(quat_mapping[r] >= 0 && quat_mapping[r] < num_coarse, DFG_ERR_ARG,
+		     "refinement: quat_mapping[%d] = %d outside [0, %d)", r, quat_mapping[r], num_coarse);
+	NEED(rel_off[0] == 0, DFG_ERR_ARG, "refinement: rel_off[0] must be 0");
+	std::vector<uint32_t> bits((size_t)N * rw, 0u);
+	for (int d = 0; d < N; ++d) {
+		NEED(rel_off[d + 1] >= rel_off[d], DFG_ERR_ARG, "refinement: rel_off decreases at frame %d", d);
+		for (long long t = rel_off[d]; t < rel_off[d + 1]; ++t) {
+			const int c = rel_quat[t];
+			NEED(c >= 0 && c < num_coarse, DFG_ERR_ARG, "refinement: frame %d lists coarse orientation %d", d, c);
+			bits[(size_t)d * rw + (c >> 5)] |= 1u << (c & 31);
+		}
+	}
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->h_qmap.assign(quat_mapping, quat_mapping + ctx->num_rot);
+	ctx->num_coarse = num_coarse;
+	ctx->rwords = rw;
+	ctx->refine = true;
+	ctx->qmap_valid = false;
+	return DFG_OK;
+}
+
+extern "C" int dfg_voronoi_subset(dfg_ctx *ctx, int num_coarse, const double *coarse, int num_fine,
+                                  const double *fine, int *nearest) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(num_coarse > 0 && num_fine >= 0 && coarse && (fine && nearest || num_fine == 0), DFG_ERR_ARG,
+	     "voronoi_subset: need coarse and fine quaternions");
+	if (num_fine == 0)
+		return DFG_OK;
+	CK(cudaSetDevice(ctx->device));
+	cudaStream_t st = ctx->stream;
+	DevBuf<double> c, f;
+	DevBuf<int> o;
+	CK(upload(c, coarse, 5 * (size_t)num_coarse, st));
+	CK(upload(f, fine, 5 * (size_t)num_fine, st));
+	CK(o.ensure((size_t)num_fine));
+	voronoi_kernel<<<blocks_for(num_fine, 256), 256, 0, st>>>(c.p, num_coarse, f.p, num_fine, o.p);
+	CKL("voronoi_kernel");
+	CK(cudaMemcpyAsync(nearest, o.p, (size_t)num_fine * sizeof(int), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
 	return DFG_OK;
 }
 
@@ -752,6 +815,19 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 			return rc;
 	}
 	double *const Wd = bg ? ctx->Wd.p : nullptr;  // FP64 slices for the background path
+	// refinement: the reference indexes quat_mapping by the flat orientation
+	// index over all modes (max_prob.c:114), which only covers one mode
+	RefineMask rm{nullptr, nullptr, 0};
+	if (ctx->refine) {
+		NEED(M == 1, DFG_ERR_ARG, "refinement needs num_modes == 1");
+		if (!ctx->qmap_valid || ctx->qmap.n < (size_t)R_pad) {
+			std::vector<int> q((size_t)R_pad, -1);
+			std::copy(ctx->h_qmap.begin(), ctx->h_qmap.end(), q.begin());
+			CK(upload(ctx->qmap, q.data(), q.size(), st));
+			ctx->qmap_valid = true;
+		}
+		rm = RefineMask{ctx->qmap.p, ctx->rel_bits.p, ctx->rwords};
+	}
 
 	// update_beta (recon.pyx:161-171)
 	{
@@ -821,13 +897,13 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 				estep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
 				    ctx->Wd.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
 				    ctx->bgscale.p, ctx->background.p, ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT,
-				    ctx->pval.p, ctx->tmax.p, ctx->targ.p);
+				    ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm);
 				CKL("estep_bg_kernel");
 			} else {
 				estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
 				    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
 				    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
-				    ctx->targ.p);
+				    ctx->targ.p, rm);
 				CKL("estep_kernel");
 			}
 		}

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(256, 3) estep_bg_kernel(
     const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off, const long long *__restrict__ ph_mid,
     const double *__restrict__ scale, const double *__restrict__ bgscale, const double *__restrict__ bg,
     const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale, const double *__restrict__ scalars,
-    int P, int RT, double *__restrict__ pval, double *__restrict__ tmax, int *__restrict__ targ) {
+    int P, int RT, double *__restrict__ pval, double *__restrict__ tmax, int *__restrict__ targ, RefineMask rm) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * Nc)
@@ -37,6 +37,11 @@ __global__ void __launch_bounds__(256, 3) estep_bg_kernel(
 	if (blacklist[d])
 		return;
 	const int r0 = rt * TILE + lane * LW;
+	const unsigned live = refine_live(rm, d, r0);
+	if (rm.qmap != nullptr && !__any_sync(FULL, live)) {
+		refine_skip_tile(pval, tmax, targ, rt, Nc, dl, lane);
+		return;
+	}
 	const double *L = Wsl + (size_t)rt * (P + 1) * TILE + lane * LW;
 	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
 	const uint4 *w4 = reinterpret_cast<const uint4 *>(ph);
@@ -78,7 +83,9 @@ __global__ void __launch_bounds__(256, 3) estep_bg_kernel(
 		acc[k] = 0.;
 		if (r < R) {
 			acc[k] = dadd(dsub(logw[r], dmul(u[r], su)), kahan_value(s[k], c[k]));
-			if (acc[k] > m) {
+			if (!(live >> k & 1u))
+				acc[k] = -INFINITY;
+			else if (acc[k] > m) {
 				m = acc[k];
 				am = r;
 			}

@@ -147,6 +147,14 @@ struct dfg_ctx {
 	DevBuf<int> prob_count, d_place;
 	DevBuf<long long> d_prob_off;
 	DevBuf<double> d_prob, tomo_out;
+	// coarse-to-fine refinement: coarse cell of every orientation (qmap,
+	// [R_pad], -1 past R) and per frame one bit per relevant coarse
+	// orientation (rel_bits, [N][rwords])
+	bool refine = false, qmap_valid = false;
+	int num_coarse = 0, rwords = 0;
+	std::vector<int> h_qmap;
+	DevBuf<int> qmap;
+	DevBuf<uint32_t> rel_bits;
 	bool timing = false;
 	cudaEvent_t ev[2 * PH_COUNT] = {};
 	cudaEvent_t user_ev[8] = {};

@@ -228,12 +228,55 @@ __global__ void __launch_bounds__(256) rescale_kernel(const double *__restrict__
 constexpr int ECH = LW == 1 ? 2 : 1;  // accumulator chains per orientation
 constexpr int ESTEP_MINB = LW == 1 ? 6 : (LW == 2 ? 4 : 3);
 
+// Coarse-to-fine refinement (param->refine, max_prob.c:110-120): frame d
+// evaluates orientation r only when r's coarse cell qmap[r] is one of the
+// frame's relevant coarse orientations, held as one bit per coarse
+// orientation in rel[d * rwords ...]. A pair that is not evaluated never
+// enters the frame's list; its log-likelihood is stored as -inf, which the
+// normalisation neither keeps nor takes as a maximum. qmap == nullptr: every
+// pair is evaluated.
+struct RefineMask {
+	const int *qmap;      // [R_pad] coarse cell per orientation, -1 past R
+	const uint32_t *rel;  // [N][rwords]
+	int rwords;
+};
+
+// Bit k set when orientation r0 + k (k < LW) is evaluated for frame d.
+__device__ __forceinline__ unsigned refine_live(const RefineMask &rm, int d, int r0) {
+	if (rm.qmap == nullptr)
+		return (1u << LW) - 1u;
+	const uint32_t *bits = rm.rel + (size_t)d * rm.rwords;
+	unsigned live = 0;
+#pragma unroll
+	for (int k = 0; k < LW; ++k) {
+		const int c = __ldg(rm.qmap + r0 + k);
+		if (c >= 0 && (__ldg(bits + (c >> 5)) >> (c & 31) & 1u))
+			live |= 1u << k;
+	}
+	return live;
+}
+
+// A (tile, frame) task with no evaluated pair: -inf log-likelihoods and an
+// empty tile maximum.
+__device__ __forceinline__ void refine_skip_tile(double *__restrict__ pval, double *__restrict__ tmax,
+                                                 int *__restrict__ targ, int rt, int Nc, int dl, int lane) {
+	double ninf[LW];
+#pragma unroll
+	for (int k = 0; k < LW; ++k)
+		ninf[k] = -INFINITY;
+	st_row(pval + ((size_t)rt * Nc + dl) * TILE + lane * LW, ninf);
+	if (lane == 0) {
+		tmax[(size_t)rt * Nc + dl] = MAX_EXP_START;
+		targ[(size_t)rt * Nc + dl] = -1;
+	}
+}
+
 __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ logw, int R,
     const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off, const long long *__restrict__ ph_mid,
     const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
     const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval, double *__restrict__ tmax,
-    int *__restrict__ targ) {
+    int *__restrict__ targ, RefineMask rm) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * Nc)
@@ -242,6 +285,11 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 	if (blacklist[d])
 		return;
 	const int r0 = rt * TILE + lane * LW;
+	const unsigned live = refine_live(rm, d, r0);
+	if (rm.qmap != nullptr && !__any_sync(FULL, live)) {
+		refine_skip_tile(pval, tmax, targ, rt, Nc, dl, lane);
+		return;
+	}
 	const float *L = logW + (size_t)rt * (P + 1) * TILE + lane * LW;
 	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
 	// segments start at multiples of 8 words: two 16-byte loads, identical for
@@ -307,7 +355,9 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 			if (ECH == 2)
 				ph_sum = dadd(ph_sum, kahan_value(s[ECH - 1][k], c[ECH - 1][k]));
 			acc[k] = dadd(dsub(logw[r], dmul(u[r], sd)), ph_sum);
-			if (acc[k] > m) {
+			if (!(live >> k & 1u))
+				acc[k] = -INFINITY;
+			else if (acc[k] > m) {
 				m = acc[k];
 				am = r;
 			}
@@ -1080,6 +1130,44 @@ __global__ void apply_scale_norm_kernel(double *__restrict__ scale, const uint8_
 	}
 	if (i < N && !blacklist[i])
 		scale[i] /= m;
+}
+
+// Nearest coarse orientation of every fine one (voronoi_subset,
+// quaternion.c:844-862): distance 1 - (q . q')^2 with the dot product summed
+// in component order, first coarse index on ties (strict <). One thread per
+// fine orientation; the coarse list is staged through shared memory.
+__global__ void __launch_bounds__(256) voronoi_kernel(const double *__restrict__ coarse, int nc,
+                                                      const double *__restrict__ fine, int nf,
+                                                      int *__restrict__ nearest) {
+	__shared__ double cq[256][4];
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	double q[4] = {0., 0., 0., 0.};
+	if (i < nf)
+		for (int k = 0; k < 4; ++k)
+			q[k] = fine[(size_t)i * 5 + k];
+	double dmin = 2.;
+	int best = -1;
+	for (int j0 = 0; j0 < nc; j0 += 256) {
+		const int n = min(256, nc - j0);
+		__syncthreads();
+		if (threadIdx.x < n)
+			for (int k = 0; k < 4; ++k)
+				cq[threadIdx.x][k] = coarse[(size_t)(j0 + threadIdx.x) * 5 + k];
+		__syncthreads();
+		for (int j = 0; j < n; ++j) {
+			double dot = 0.;
+#pragma unroll
+			for (int k = 0; k < 4; ++k)
+				dot = dadd(dot, dmul(q[k], cq[j][k]));
+			const double dist = dsub(1., dmul(dot, dot));
+			if (dist < dmin) {
+				dmin = dist;
+				best = j0 + j;
+			}
+		}
+	}
+	if (i < nf)
+		nearest[i] = best;
 }
 
 // One slice, un-logged (Model.slice_gen, model.c:11-59)

@@ -73,6 +73,7 @@ class Iterate:
         self.num_blacklist = 0
         self.fcounts = self.scale = self.bgscale = self.beta = self.beta_start = None
         self.sum_fact = self.blacklist = None
+        self.rel_quat = None  # relevant coarse orientations per frame (refinement)
         self.mean_count = None
         self.rescale = None
         self.likelihood = 0.
@@ -153,6 +154,7 @@ class Iterate:
                 return ""
         model_file, scale_file = fname_opt("start_model_file"), fname_opt("scale_file")
         bgscale_file = fname_opt("bgscale_file")
+        probs_file = fname_opt("probs_file")
         if resume:
             with open(param.log_fname) as f:
                 last_iter = int(f.readlines()[-1].split()[0])
@@ -160,7 +162,18 @@ class Iterate:
             ext = ".h5" if h5py is not None else ".npz"
             model_file = op.join(param.output_folder, "output_%.3d%s" % (last_iter, ext))
             scale_file = model_file
+            if param.refine and not probs_file:
+                probs_file = model_file
             print("Resuming from iteration", self.params.start_iter)
+        # refinement (src/iterate.c:103-130): fine orientations mapped to their
+        # nearest coarse one, relevant coarse orientations per frame from an
+        # earlier coarse run
+        if param.refine:
+            if not probs_file:
+                raise ValueError("Need coarse probabilities in probs_file to do refinement")
+            if quat.quat_mapping is None:
+                quat.voronoi_subset(param.coarse_div)
+            self.parse_rel_quat(probs_file, quat.num_rot_coarse)
 
         model = Model(self.calculate_size(det.qmax()), param.num_modes, rtype)
         model_mean = self.mean_count[0] / (det.raw_mask == 0).sum() * 2.
@@ -241,6 +254,61 @@ class Iterate:
             self.bgscale = scale.copy()
         else:
             self.scale = scale.copy()
+
+    def parse_rel_quat(self, fname, num_rot_coarse):
+        """Relevant coarse orientations per frame for refinement
+        (parse_rel_quat, src/iterate.c:364-527). From an output file of an
+        earlier (coarse) run: the saved probability lists when there are any
+        (their orientation count must be num_rot_coarse), else the most
+        likely orientation of each frame. From a binary file: int32 num_data
+        and num_rot at the start, then from byte 1024 int32 counts [num_data]
+        followed by each frame's list. Sets ``rel_quat`` (list of int32
+        arrays)."""
+        if fname.endswith(".npz") or fname.endswith(".h5"):
+            if fname.endswith(".npz"):
+                f = np.load(fname)
+                get = lambda k: f[k.replace("/", "__")] if k.replace("/", "__") in f.files else None
+            else:
+                if h5py is None:
+                    raise ImportError("h5py is needed to read " + fname)
+                h = h5py.File(fname, "r")
+                get = lambda k: h[k][()] if k in h else None
+            num_rot = get("probabilities/num_rot")
+            if num_rot is None:
+                print("No probabilities saved. Using most likely orientations")
+                rmax = np.asarray(get("orientations"), np.int32)
+                if rmax.shape[0] != self.tot_num_data:
+                    raise ValueError("num_data of orientations (%d) does not match %d"
+                                     % (rmax.shape[0], self.tot_num_data))
+                rel = [rmax[d:d + 1] for d in range(rmax.shape[0])]
+            else:
+                if int(np.ravel(num_rot)[0]) != num_rot_coarse:
+                    raise ValueError("Rotation sampling in probs file does not match num_rot_coarse: %d vs %d"
+                                     % (int(np.ravel(num_rot)[0]), num_rot_coarse))
+                off = np.asarray(get("probabilities/offsets"), np.int64)
+                place = np.asarray(get("probabilities/place"), np.int32)
+                if off.shape[0] - 1 != self.tot_num_data:
+                    raise ValueError("num_data of rel_quat (%d) does not match %d"
+                                     % (off.shape[0] - 1, self.tot_num_data))
+                rel = [place[off[d]:off[d + 1]] for d in range(off.shape[0] - 1)]
+            if not fname.endswith(".npz"):
+                h.close()
+        else:
+            with open(fname, "rb") as f:
+                num_data, num_rot = np.fromfile(f, np.int32, 2)
+                if num_data != self.tot_num_data:
+                    raise ValueError("num_data of rel_quat (%d) does not match" % num_data)
+                if num_rot != num_rot_coarse:
+                    raise ValueError("Rotation sampling in probs file does not match num_rot_coarse: %d vs %d"
+                                     % (num_rot, num_rot_coarse))
+                f.seek(1024)
+                counts = np.fromfile(f, np.int32, num_data)
+                flat = np.fromfile(f, np.int32, int(counts.sum()))
+            off = np.zeros(num_data + 1, np.int64)
+            np.cumsum(counts, out=off[1:])
+            rel = [flat[off[d]:off[d + 1]] for d in range(num_data)]
+        self.rel_quat = rel
+        return rel
 
     def parse_blacklist(self, fname, sel_string=None, refresh=False):
         """iterate.pyx:317-359 (num_blacklist is left at 0, as there)."""

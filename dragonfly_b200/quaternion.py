@@ -24,7 +24,9 @@ class Quaternion:
         self.num_div = 0
         self._quats = None
         self.reduced = False
-        self.quat_mapping = None
+        self.quat_mapping = None  # nearest coarse orientation (voronoi_subset)
+        self.coarse_div = 0
+        self.num_rot_coarse = 0
         if num_div > 0 and num_rot > 0:
             raise ValueError("Cannot specify both num_div and num_rot")
         elif num_div > 0:
@@ -104,16 +106,28 @@ class Quaternion:
             sys.stderr.write("%d: num_rot_p = %d/%d\n" % (rank, self.num_rot_p, tot))
         return self.num_rot_p
 
-    def voronoi_subset(self, coarse_div):
-        """Nearest coarse orientation of every fine one, by 1 - (q.q')^2
-        (voronoi_subset, quaternion.c:844-862); ties keep the first."""
+    def voronoi_subset(self, coarse_div, ctx=None):
+        """Nearest coarse (num_div = coarse_div) orientation of every fine one,
+        by 1 - (q.q')^2 with ties to the first (voronoi_subset,
+        quaternion.c:844-862; Quaternion.voronoi_subset, quaternion.pyx:257-281),
+        computed on the GPU (dfg_voronoi_subset) of ``ctx`` or of a temporary
+        context on device 0. The result is kept as ``quat_mapping`` with
+        ``coarse_div`` and ``num_rot_coarse`` for refinement."""
+        if self._quats is None:
+            print("Generate fine quaternions first")
+            return None
+        from ._lib import Context
         coarse = quat_gen(coarse_div)
-        q = self._quats[:, :4]
-        out = np.empty(q.shape[0], np.int64)
-        for s in range(0, q.shape[0], 4096):
-            dist = 1. - (q[s:s + 4096] @ coarse[:, :4].T) ** 2
-            out[s:s + 4096] = np.argmin(dist, axis=1)
+        own = ctx is None
+        c = Context(0) if own else ctx
+        try:
+            out = c.voronoi_subset(coarse, self._quats)
+        finally:
+            if own:
+                c.close()
         self.quat_mapping = out
+        self.coarse_div = int(coarse_div)
+        self.num_rot_coarse = coarse.shape[0]
         return out
 
     def reduce_icosahedral(self, return_sym=False):
@@ -129,6 +143,8 @@ class Quaternion:
         quats = self._quats
         sel = np.where(distance.cdist(quats[:60, :4], quats[60:, :4]).argmin(axis=0) == 8)[0]
         self._quats = np.ascontiguousarray(np.concatenate([quats[8:9], quats[60 + sel]]))
+        if self.quat_mapping is not None:
+            self.quat_mapping = np.concatenate([self.quat_mapping[8:9], self.quat_mapping[60 + sel]])
         self.reduced = True
         return quats[:60, :4].copy() if return_sym else self.num_rot
 
@@ -167,6 +183,8 @@ class Quaternion:
         cube = self.octahedral_quaternions()
         sel = np.where(distance.cdist(cube, self._quats[:, :4]).argmin(axis=0) == 0)[0]
         self._quats = np.ascontiguousarray(self._quats[sel])
+        if self.quat_mapping is not None:
+            self.quat_mapping = self.quat_mapping[sel]
         self.reduced = True
         return cube if return_sym else self.num_rot
 

@@ -61,8 +61,6 @@ class EMCRecon:
             raise NotImplementedError("only 3-D reconstructions are supported")
         if itr.params.nonrot_modes:
             raise NotImplementedError("non-rotating modes are not supported")
-        if itr.params.refine:
-            raise NotImplementedError("orientation refinement is not supported")
         from ._lib import Context
         if self.ctx is None:
             self.ctx = Context(self.device)
@@ -74,6 +72,12 @@ class EMCRecon:
         c.set_background(det.background if det.with_bg else None)
         c.set_quaternions(itr.quat.quats)
         c.set_model(itr.model.model1)
+        # refinement (max_prob.c:110-120 with src/iterate.c:103-130)
+        if itr.params.refine:
+            if itr.quat.quat_mapping is None or itr.rel_quat is None:
+                raise ValueError("refinement needs quat.voronoi_subset() and Iterate.parse_rel_quat()")
+            c.set_refinement(itr.quat.num_rot_coarse, itr.quat.quat_mapping, itr.rel_quat)
+            self.refinement = 1
         # update_model's symmetries (recon.pyx:120-134)
         pg = 2 if itr.quat.icosahedral_flag else (1 if itr.quat.octahedral_flag else 0)
         c.set_symmetry(pg, itr.params.axial_sym if itr.params.axial_sym > 1 else 0)

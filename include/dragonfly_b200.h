@@ -129,6 +129,24 @@ DFG_API int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change);
  * reduce_icosahedral, quaternion.pyx:177-255). */
 DFG_API int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order);
 
+/* Coarse-to-fine orientation refinement (params.refine with iterate.quat_mapping,
+ * rel_quat and num_rel_quat; maximize consults them at max_prob.c:110-120,
+ * max_update.c:73-83 / :170-180 and max_scale.c:69-79; the legacy engine fills
+ * them at src/iterate.c:103-130 and parse_rel_quat, src/iterate.c:364-527):
+ * frame d evaluates orientation r only when quat_mapping[r] (its nearest
+ * coarse orientation, [num_rot]) is one of rel_quat[rel_off[d] .. rel_off[d+1]).
+ * quat_mapping == NULL switches refinement off. Needs frames and quaternions;
+ * setting either again switches it off. One model mode only. */
+DFG_API int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
+                               const long long *rel_off, const int *rel_quat);
+
+/* voronoi_subset (quaternion.c:844-862, Quaternion.voronoi_subset
+ * quaternion.pyx:257-281): nearest[i] = the coarse orientation with the
+ * smallest 1 - (q_i . c_j)^2, first on ties. Quaternions are rows of five
+ * (q0..q3, weight). Runs on the context's device. */
+DFG_API int dfg_voronoi_subset(dfg_ctx *ctx, int num_coarse, const double *coarse, int num_fine,
+                               const double *fine, int *nearest);
+
 /* Iterate.normalize_scale (dragonfly/iterate.pyx:361-384): mean phi over
  * good frames, mode-0 model1 *= mean, phi /= mean. Writes the mean. */
 DFG_API int dfg_normalize_scale(dfg_ctx *ctx, double *mean_scale);

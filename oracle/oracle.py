@@ -157,6 +157,7 @@ class ReferenceEngine:
         L.ref_get_powder.argtypes = [C.c_void_p, _dp]
         L.ref_get_frame_prob.restype = C.c_int
         L.ref_get_frame_prob.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.ref_set_refinement.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         self.save_prob = False
         self.prob = p = prob
         self._scale_buf = p.scale
@@ -212,6 +213,22 @@ class ReferenceEngine:
     def set_symmetry(self, point_group=0, axial_order=0):
         """Model symmetries of update_model: point_group 1 = S4, 2 = A5."""
         self.lib.ref_set_symmetry(self.h, int(point_group), int(axial_order))
+
+    def set_refinement(self, quat_mapping=None, rel_quat=None):
+        """Coarse-to-fine refinement (see ref_set_refinement): quat_mapping
+        [num_rot] nearest coarse orientation, rel_quat a per-frame sequence of
+        relevant coarse orientations; None switches it off."""
+        if quat_mapping is None:
+            self.lib.ref_set_refinement(self.h, None, None, None)
+            return
+        self._qmap = _c(quat_mapping, np.int32)
+        lens = np.array([len(x) for x in rel_quat], np.int64)
+        self._rel_off = np.zeros(len(lens) + 1, np.int64)
+        np.cumsum(lens, out=self._rel_off[1:])
+        self._rel = _c(np.concatenate([np.asarray(x, np.int32).ravel() for x in rel_quat]) if lens.sum()
+                       else np.zeros(1, np.int32), np.int32)
+        self.lib.ref_set_refinement(self.h, self._qmap.ctypes.data, self._rel_off.ctypes.data,
+                                    self._rel.ctypes.data)
 
     def set_save_prob(self, on):
         """Makes maximize form the combined per-frame probability lists
@@ -369,4 +386,32 @@ def quat_gen_reference(num_div):
     n = L.ref_quat_gen(int(num_div), None)
     out = np.zeros((n, 5))
     L.ref_quat_gen(int(num_div), out.ctypes.data)
+    return out
+
+
+def voronoi_subset_reference(coarse_div, fine):
+    """Nearest coarse (num_div = coarse_div) orientation of every fine one,
+    from the reference's voronoi_subset (quaternion.c:844-862)."""
+    L = _load(LIB_REF)
+    L.ref_voronoi_subset.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    f = _c(fine, np.float64)
+    out = np.full(f.shape[0], -1, np.int32)
+    L.ref_voronoi_subset(int(coarse_div), f.shape[0], f.ctypes.data, out.ctypes.data)
+    return out
+
+
+def voronoi_subset_port(coarse, fine):
+    """Restatement of voronoi_subset (quaternion.c:844-862) in numpy: for each
+    fine orientation the coarse one with the smallest 1 - d^2, d the dot
+    product of (q0..q3) summed in component order without fused multiply-add
+    (numpy elementwise operations, no BLAS), first index on ties."""
+    c = np.asarray(coarse, np.float64)[:, :4]
+    f = np.asarray(fine, np.float64)[:, :4]
+    out = np.empty(f.shape[0], np.int32)
+    for s in range(0, f.shape[0], 2048):
+        q = f[s:s + 2048]
+        d = q[:, 0:1] * c[None, :, 0]
+        for k in range(1, 4):
+            d = d + q[:, k:k + 1] * c[None, :, k]
+        out[s:s + 2048] = np.argmin(1. - d * d, axis=1)
     return out

@@ -233,6 +233,8 @@ double ref_update_model(ref_engine *e) {
 	return e->iter.rms_change;
 }
 
+void ref_set_refinement(ref_engine *e, const int *quat_mapping, const long long *rel_off, const int *rel_quat);
+
 void ref_destroy(ref_engine *e) {
 	if (e == NULL)
 		return;
@@ -247,6 +249,7 @@ void ref_destroy(ref_engine *e) {
 	free(e->iter.blacklist); free(e->iter.sum_fact); free(e->iter.scale);
 	free(e->iter.beta); free(e->iter.beta_start);
 	free(e->det.background); free(e->det.powder); free(e->iter.bgscale);
+	ref_set_refinement(e, NULL, NULL, NULL);
 	free(e);
 }
 
@@ -375,4 +378,48 @@ int ref_quat_gen(int num_div, double *out) {
 		memcpy(out, q.quats, (size_t)n * 5 * sizeof(double));
 	free(q.quats);
 	return n;
+}
+
+/* Coarse-to-fine refinement: params.refine with iterate.quat_mapping, rel_quat
+ * and num_rel_quat filled as the legacy engine's setup does (src/iterate.c:
+ * 103-130: quat_mapping from voronoi_subset, rel_quat per frame from the
+ * coarse probabilities). The packaged engine consults them in max_prob.c:
+ * 110-120, max_update.c:73-83 / 170-180 and max_scale.c:69-79; its Python
+ * layer never fills them. quat_mapping == NULL switches refinement off. */
+void ref_set_refinement(ref_engine *e, const int *quat_mapping, const long long *rel_off, const int *rel_quat) {
+	int d, n = e->iter.tot_num_data;
+	if (e->iter.rel_quat != NULL) {
+		for (d = 0; d < n; ++d)
+			free(e->iter.rel_quat[d]);
+		free(e->iter.rel_quat);
+	}
+	free(e->iter.num_rel_quat);
+	free(e->iter.quat_mapping);
+	e->iter.rel_quat = NULL;
+	e->iter.num_rel_quat = NULL;
+	e->iter.quat_mapping = NULL;
+	e->par.refine = 0;
+	if (quat_mapping == NULL)
+		return;
+	e->iter.quat_mapping = dup_mem(quat_mapping, (size_t)e->quat.num_rot * sizeof(int));
+	e->iter.num_rel_quat = malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+	e->iter.rel_quat = malloc((size_t)(n > 0 ? n : 1) * sizeof(int *));
+	for (d = 0; d < n; ++d) {
+		e->iter.num_rel_quat[d] = (int)(rel_off[d + 1] - rel_off[d]);
+		e->iter.rel_quat[d] = dup_mem(rel_quat + rel_off[d], (size_t)e->iter.num_rel_quat[d] * sizeof(int));
+	}
+	e->par.refine = 1;
+}
+
+/* Quaternion.voronoi_subset (quaternion.pyx:257-281): the nearest of the
+ * num_div = coarse_div orientations for each of the fine ones. */
+void ref_voronoi_subset(int coarse_div, int num_fine, const double *fine, int *nearest) {
+	struct quaternion qc, qf;
+	memset(&qc, 0, sizeof(qc));
+	memset(&qf, 0, sizeof(qf));
+	quat_gen(coarse_div, &qc);
+	qf.num_rot = num_fine;
+	qf.quats = (double *)fine;
+	voronoi_subset(&qc, &qf, nearest);
+	free(qc.quats);
 }

@@ -63,3 +63,55 @@ def test_model_slice_api_on_gpu(oracle_built):
     np.testing.assert_array_equal(s, orc.slice_gen(prob.quats[3]))
     m.slice_merge(prob.quats[3], s, det)
     assert m.inter_weight.sum() > 0
+
+
+def test_emcrecon_refinement_from_a_coarse_run(tmp_path, oracle_built):
+    """num_div = "2 1" with probs_file naming a coarse run's output: the fine
+    orientations map to their nearest coarse one (voronoi_subset) and each
+    frame evaluates those whose coarse cell carries probability in the
+    coarse run (src/iterate.c:103-130), checked against the reference engine
+    with the same lists."""
+    from dragonfly_b200 import Iterate
+    from dragonfly_b200.recon import EMCRecon
+    from oracle.oracle import ReferenceEngine, reference_available, voronoi_subset_reference
+    if not reference_available():
+        pytest.skip("reference engine library not built")
+    d, cfg = write_problem(tmp_path, extra="save_prob = 1\n")
+    text = open(cfg).read()
+    open(cfg, "w").write(text.replace("num_div = 2", "num_div = 1"))
+    itr = Iterate(cfg)
+    recon = EMCRecon()
+    recon.set_iterate(itr)
+    for it in (1, 2):
+        itr.params.iteration = it
+        recon.run_iteration()
+    coarse_out = [n for n in os.listdir(itr.params.output_folder) if n.startswith("output_002")][0]
+    recon.free()
+
+    fine_cfg = tmp_path / "fine.ini"
+    fine_cfg.write_text(text.replace("num_div = 2", "num_div = 2 1").replace("save_prob = 1", "")
+                        .replace("output_folder = out/", "output_folder = fine/")
+                        .replace("log_file = out/EMC.log", "log_file = fine/EMC.log")
+                        + "probs_file = out/%s\n" % coarse_out)
+    itr = Iterate(str(fine_cfg))
+    assert itr.params.refine and itr.quat.num_rot == 420 and itr.quat.num_rot_coarse == 60
+    np.testing.assert_array_equal(itr.quat.quat_mapping, voronoi_subset_reference(1, itr.quat.quats))
+    assert len(itr.rel_quat) == d["ones"].size and sum(len(x) for x in itr.rel_quat) > d["ones"].size
+    start = itr.model.model1.copy()
+    recon = EMCRecon()
+    recon.set_iterate(itr)
+    prob = EMCProblem(itr.dets[0].qvals, itr.dets[0].corr, itr.dets[0].raw_mask, d["ones"], d["multi"],
+                      d["place_ones"], d["place_multi"], d["count_multi"], itr.quat.quats, start,
+                      beta=0.5, beta_jump=2., beta_period=3)
+    ref = ReferenceEngine(prob)
+    ref.set_refinement(itr.quat.quat_mapping, itr.rel_quat)
+    for it in (1, 2):
+        itr.params.iteration = it
+        ll = recon.run_iteration()
+        b = ref.run_iteration(it)
+        assert rel_l2(itr.model.model1, b["model1"]) <= MODEL_REL_L2
+        assert rel(ll, b["avg_likelihood"]) <= SCALAR_REL
+        assert np.mean(recon.rmax == b["rmax"]) >= 0.999
+        assert all(r < 0 or itr.quat.quat_mapping[r] in itr.rel_quat[i] for i, r in enumerate(recon.rmax))
+    recon.free()
+    ref.close()
