@@ -64,6 +64,8 @@ _SIGS = {
     "dfg_save_emc": (C.c_int, [_V, C.c_char_p]),
     "dfg_set_symmetry": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_set_refinement": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_longlong), _I]),
+    "dfg_set_model_type": (C.c_int, [_V, C.c_int, C.c_int]),
+    "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
     "dfg_voronoi_subset": (C.c_int, [_V, C.c_int, _D, C.c_int, _D, _I]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
     "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
@@ -173,8 +175,10 @@ class Context:
         self.num_rot = q.shape[0]
 
     def set_model(self, model1):
+        """model1 [modes, S, S, S] (3-D) or [modes, S, S] (2-D / RZ); one
+        mode may omit the leading axis."""
         m = np.ascontiguousarray(model1, np.float64)
-        if m.ndim == 3:
+        if m.ndim == (3 if getattr(self, "model_type", 0) == 0 else 2):
             m = m[None]
         self.call("dfg_set_model", m.shape[-1], m.shape[0], ptr(m, C.c_double))
         self.model_shape = m.shape
@@ -195,6 +199,17 @@ class Context:
         """Model symmetries of update_model: point_group 0 (Friedel only),
         1 (S4) or 2 (A5); axial_order > 1 adds the axial symmetry."""
         self.call("dfg_set_symmetry", int(point_group), int(axial_order))
+
+    def set_model_type(self, model_type, friedel_sym=0):
+        """0 / "3d" (volume), 1 / "2d" (stack of images, angle orientations)
+        or 2 / "rz"; friedel_sym: 2-D Friedel average in update_model. Call
+        set_model afterwards."""
+        mt = {"3d": 0, "2d": 1, "rz": 2}.get(str(model_type).lower(), model_type)
+        self.call("dfg_set_model_type", int(mt), int(friedel_sym))
+        self.model_type = int(mt)
+
+    def set_detector_distance(self, detd):
+        self.call("dfg_set_detector_distance", float(detd))
 
     def set_refinement(self, num_coarse=0, quat_mapping=None, rel_quat=None):
         """Coarse-to-fine refinement: frame d evaluates orientation r only
@@ -345,7 +360,8 @@ class Context:
                     rms_change=out[4])
 
     def slice_gen(self, quat, mode=0):
-        q = np.ascontiguousarray(quat, np.float64)
+        """Slice at a quaternion (3-D), an angle (2-D) or (phi, beta) (RZ)."""
+        q = np.ascontiguousarray(np.atleast_1d(quat), np.float64)
         if q.size == 4:
             q = np.append(q, 1.)
         out = np.zeros(self.num_pix)
@@ -363,7 +379,7 @@ class Context:
         return out
 
     def slice_merge(self, quat, view, model2, inter_weight, mode=0):
-        q = np.ascontiguousarray(quat, np.float64)
+        q = np.ascontiguousarray(np.atleast_1d(quat), np.float64)
         if q.size == 4:
             q = np.append(q, 1.)
         v = np.ascontiguousarray(view, np.float64)

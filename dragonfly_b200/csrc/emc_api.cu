@@ -244,6 +244,12 @@ extern "C" int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quat
 		ctx->refine = false;  // the coarse map was made for the previous set
 	ctx->num_rot = num_rot;
 	CK(upload(ctx->quats, quats, 5 * (size_t)num_rot, ctx->stream));
+	std::vector<double> cs(2 * (size_t)num_rot);
+	for (int r = 0; r < num_rot; ++r) {
+		cs[2 * (size_t)r] = std::cos(quats[5 * (size_t)r]);
+		cs[2 * (size_t)r + 1] = std::sin(quats[5 * (size_t)r]);
+	}
+	CK(upload(ctx->cs2d, cs.data(), cs.size(), ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
 	return DFG_OK;
 }
@@ -256,7 +262,7 @@ extern "C" int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const doubl
 	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
 	ctx->S = size;
-	ctx->V = (long long)size * size * size;
+	ctx->V = ctx->model_type == MT_3D ? (long long)size * size * size : (long long)size * size;
 	ctx->M = num_modes;
 	const size_t n = (size_t)num_modes * ctx->V;
 	CK(upload(ctx->model1, model1, n, ctx->stream));
@@ -271,6 +277,29 @@ extern "C" int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const doubl
 
 static int need_frames(dfg_ctx *ctx) {
 	NEED(ctx->N > 0, DFG_ERR_STATE, "set the frames first");
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_model_type(dfg_ctx *ctx, int model_type, int friedel_sym) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(model_type == MT_3D || model_type == MT_2D || model_type == MT_RZ, DFG_ERR_ARG,
+	     "model_type must be 0 (3-D), 1 (2-D) or 2 (RZ)");
+	if (model_type != ctx->model_type) {
+		ctx->S = 0;  // the model must be set again with its new shape
+		ctx->V = 0;
+		ctx->weight_cache_valid = false;
+	}
+	ctx->model_type = model_type;
+	ctx->friedel2d = friedel_sym != 0;
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_detector_distance(dfg_ctx *ctx, double detd) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(std::isfinite(detd), DFG_ERR_ARG, "detector distance must be finite");
+	ctx->detd = detd;
 	return DFG_OK;
 }
 
@@ -815,6 +844,10 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 			return rc;
 	}
 	double *const Wd = bg ? ctx->Wd.p : nullptr;  // FP64 slices for the background path
+	// recon.pyx:86-91 selects the 3-D or the 2-D slice functions; an RZ
+	// iteration has none there
+	NEED(ctx->model_type != MT_RZ, DFG_ERR_ARG, "RZ models: slice_gen / slice_merge only, no iteration");
+	const bool two_d = ctx->model_type == MT_2D;
 	// refinement: the reference indexes quat_mapping by the flat orientation
 	// index over all modes (max_prob.c:114), which only covers one mode
 	RefineMask rm{nullptr, nullptr, 0};
@@ -853,19 +886,27 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 				}
 		}
 		const int nb = R_pad / ob;
-#define DFG_SLICE(OBV)                                                                                        \
-	slice_u_kernel<double, OBV><<<nb, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, \
-	                                                ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd)
-		if (ob == TILE)
-			slice_u_tile_kernel<double><<<RT, 256, 0, st>>>(ctx->quats.p, M, R, ctx->qvals.p, ctx->corr.p,
-			                                                ctx->mask.p, P, ctx->model1.p, S, V, ctx->logW.p,
-			                                                ctx->u.p, Wd);
-		else if (ob == 64)
-			DFG_SLICE(TILE >= 64 ? 64 : 16);
-		else if (ob == 32)
-			DFG_SLICE(32);
-		else
-			DFG_SLICE(16);
+		// orientation parameters: quaternions (3-D) or (cos, sin) of the angles (2-D)
+		const double *geo = two_d ? ctx->cs2d.p : ctx->quats.p;
+#define DFG_SLICE(OBV, G)                                                                                     \
+	slice_u_kernel<double, OBV, G><<<nb, 256, 0, st>>>(geo, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,     \
+	                                                   ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd)
+#define DFG_SLICE_ALL(G)                                                                                      \
+	if (ob == TILE)                                                                                           \
+		slice_u_tile_kernel<double, G><<<RT, 256, 0, st>>>(geo, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, \
+		                                                   ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd);     \
+	else if (ob == 64)                                                                                        \
+		DFG_SLICE(TILE >= 64 ? 64 : 16, G);                                                                   \
+	else if (ob == 32)                                                                                        \
+		DFG_SLICE(32, G);                                                                                     \
+	else                                                                                                      \
+		DFG_SLICE(16, G)
+		if (two_d) {
+			DFG_SLICE_ALL(MT_2D);
+		} else {
+			DFG_SLICE_ALL(MT_3D);
+		}
+#undef DFG_SLICE_ALL
 #undef DFG_SLICE
 		CKL("slice_u_kernel");
 	}
@@ -985,9 +1026,14 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		CK(ctx->weight_cache.ensure((size_t)M * V));
 	}
 	phase_begin(ctx, PH_MERGE);
-	merge_kernel<<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
-	                                              ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
-	                                              with_weight, bg ? 1 : 0);
+	if (two_d)
+		merge_kernel<MT_2D><<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->cs2d.p, M, R, ctx->qvals.p,
+		                                                     ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
+		                                                     with_weight, bg ? 1 : 0);
+	else
+		merge_kernel<MT_3D><<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
+		                                                     ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
+		                                                     with_weight, bg ? 1 : 0);
 	CKL("merge_kernel");
 	phase_end(ctx, PH_MERGE, 1);
 
@@ -1163,7 +1209,18 @@ extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) 
 		}
 		return DFG_OK;
 	};
-	if (ctx->n_group_rots > 0) {
+	if (ctx->model_type != MT_3D) {
+		// image stacks: the 2-D Friedel average for RZ, or for 2-D with
+		// params.friedel_sym (recon.pyx:118-119); no volume symmetries
+		NEED(ctx->n_group_rots == 0 && ctx->n_axial_rots <= 1, DFG_ERR_ARG,
+		     "point-group and axial symmetries apply to 3-D models only");
+		if (ctx->model_type == MT_RZ || ctx->friedel2d) {
+			const long long pairs2 = (long long)ctx->M * (S - lo) * (S / 2 - lo + 1);
+			friedel2d_kernel<<<blocks_for(pairs2, 256), 256, 0, st>>>(ctx->model2.p, ctx->weight.p, S, ctx->M);
+			CKL("friedel2d_kernel");
+			launched++;
+		}
+	} else if (ctx->n_group_rots > 0) {
 		if (int rc = symmetrize(ctx->group_rots, ctx->n_group_rots))
 			return rc;
 	} else {
@@ -1171,7 +1228,7 @@ extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) 
 		CKL("friedel_kernel");
 		launched++;
 	}
-	if (ctx->n_axial_rots > 1)
+	if (ctx->model_type == MT_3D && ctx->n_axial_rots > 1)
 		if (int rc = symmetrize(ctx->axial_rots, ctx->n_axial_rots))
 			return rc;
 	const unsigned nb = blocks_for(n, 256);
@@ -1399,6 +1456,29 @@ extern "C" int dfg_get_scalars(dfg_ctx *ctx, double *out) {
 // ---------------------------------------------------------------------------
 // one-slice operations
 // ---------------------------------------------------------------------------
+// Orientation parameters of one slice for slice_one_kernel / merge_one_kernel:
+// the quaternion (3-D); cos, sin of the angle quat[0] (2-D); cos, sin of phi =
+// quat[0] and of beta = quat[1] and the detector distance (RZ). cos and sin
+// come from the host's libm, as make_rot_angle's (model.c:788-795).
+static int orientation_params(const dfg_ctx *ctx, const double *quat, double *g) {
+	if (ctx->model_type == MT_2D) {
+		g[0] = std::cos(quat[0]);
+		g[1] = std::sin(quat[0]);
+		return 2;
+	}
+	if (ctx->model_type == MT_RZ) {
+		g[0] = std::cos(quat[0]);
+		g[1] = std::sin(quat[0]);
+		g[2] = std::cos(quat[1]);
+		g[3] = std::sin(quat[1]);
+		g[4] = ctx->detd;
+		return 5;
+	}
+	for (int k = 0; k < 5; ++k)
+		g[k] = quat[k];
+	return 5;
+}
+
 extern "C" int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double *out) {
 	if (!ctx || !quat || !out)
 		return DFG_ERR_ARG;
@@ -1407,10 +1487,20 @@ extern "C" int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double 
 	CK(cudaSetDevice(ctx->device));
 	CK(ctx->scalars.ensure(8));
 	DevBuf<double> q, o;
-	CK(upload(q, quat, 5, ctx->stream));
+	double g[8];
+	const int ng = orientation_params(ctx, quat, g);
+	CK(upload(q, g, (size_t)ng, ctx->stream));
 	CK(o.ensure((size_t)ctx->P));
-	slice_one_kernel<<<blocks_for(ctx->P, 256), 256, 0, ctx->stream>>>(q.p, mode, ctx->qvals.p, ctx->corr.p, ctx->P,
-	                                                                    ctx->model1.p, ctx->S, ctx->V, o.p);
+	const unsigned nb = blocks_for(ctx->P, 256);
+	if (ctx->model_type == MT_2D)
+		slice_one_kernel<MT_2D><<<nb, 256, 0, ctx->stream>>>(q.p, mode, ctx->qvals.p, ctx->corr.p, ctx->P,
+		                                                     ctx->model1.p, ctx->S, ctx->V, o.p);
+	else if (ctx->model_type == MT_RZ)
+		slice_one_kernel<MT_RZ><<<nb, 256, 0, ctx->stream>>>(q.p, mode, ctx->qvals.p, ctx->corr.p, ctx->P,
+		                                                     ctx->model1.p, ctx->S, ctx->V, o.p);
+	else
+		slice_one_kernel<MT_3D><<<nb, 256, 0, ctx->stream>>>(q.p, mode, ctx->qvals.p, ctx->corr.p, ctx->P,
+		                                                     ctx->model1.p, ctx->S, ctx->V, o.p);
 	CKL("slice_one_kernel");
 	CK(cudaMemcpyAsync(out, o.p, (size_t)ctx->P * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
@@ -1426,12 +1516,23 @@ extern "C" int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const
 	CK(cudaSetDevice(ctx->device));
 	const size_t n = (size_t)ctx->M * ctx->V;
 	DevBuf<double> q, v, m2, w;
-	CK(upload(q, quat, 5, ctx->stream));
+	double g[8];
+	const int ng = orientation_params(ctx, quat, g);
+	CK(upload(q, g, (size_t)ng, ctx->stream));
 	CK(upload(v, view, (size_t)ctx->P, ctx->stream));
 	CK(upload(m2, model2, n, ctx->stream));
 	CK(upload(w, inter_weight, n, ctx->stream));
-	merge_one_kernel<<<blocks_for(ctx->P, 256), 256, 0, ctx->stream>>>(q.p, mode, v.p, ctx->qvals.p, ctx->corr.p,
-	                                                                    ctx->mask.p, ctx->P, ctx->S, ctx->V, m2.p, w.p);
+	const unsigned nb = blocks_for(ctx->P, 256);
+#define DFG_MERGE_ONE(G)                                                                                       \
+	merge_one_kernel<G><<<nb, 256, 0, ctx->stream>>>(q.p, mode, v.p, ctx->qvals.p, ctx->corr.p, ctx->mask.p, ctx->P, \
+	                                                 ctx->S, ctx->V, m2.p, w.p)
+	if (ctx->model_type == MT_2D)
+		DFG_MERGE_ONE(MT_2D);
+	else if (ctx->model_type == MT_RZ)
+		DFG_MERGE_ONE(MT_RZ);
+	else
+		DFG_MERGE_ONE(MT_3D);
+#undef DFG_MERGE_ONE
 	CKL("merge_one_kernel");
 	CK(cudaMemcpyAsync(model2, m2.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 	CK(cudaMemcpyAsync(inter_weight, w.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -136,6 +136,109 @@ __device__ __forceinline__ double interp(const Cell &c, const MT *__restrict__ m
 	return dmul(v, corr);
 }
 
+// Model types (enum model_type, model.h:13): a volume sampled trilinearly at
+// quaternion-rotated pixel positions, a stack of 2-D images sampled
+// bilinearly at in-plane-rotated positions (orientation = angle), or an RZ
+// image (orientation = (phi, beta)).
+enum ModelType { MT_3D = 0, MT_2D = 1, MT_RZ = 2 };
+
+// Bilinear cell in a 2-D image: integer part by truncation toward zero, in
+// bounds iff 0 <= x, y <= size-2 (model.c:85-99, 133-146, 280-290).
+struct Cell2 {
+	long long i00;  // x*S + y
+	double fx, fy;
+	bool ok;
+};
+
+__device__ __forceinline__ Cell2 cell2_at(double px, double py, long long S) {
+	Cell2 c;
+	const long long x = (long long)px, y = (long long)py;
+	c.ok = !(x < 0 || x > S - 2 || y < 0 || y > S - 2);
+	c.fx = dsub(px, (double)x);
+	c.fy = dsub(py, (double)y);
+	c.i00 = c.ok ? x * S + y : 0;
+	return c;
+}
+
+// slice_gen2d / slice_merge2d (model.c:65-99, 254-280): the pixel's (qx, qy)
+// rotated by rot = [[c, -s], [s, c]] (make_rot_angle, model.c:788-795; c and
+// s come from the host's libm), plus the center.
+__device__ __forceinline__ Cell2 locate2d(const double *cs, double qx, double qy, double center, long long S) {
+	const double px = dadd(dadd(dmul(cs[0], qx), dmul(-cs[1], qy)), center);
+	const double py = dadd(dadd(dmul(cs[1], qx), dmul(cs[0], qy)), center);
+	return cell2_at(px, py, S);
+}
+
+// slice_genrz / slice_mergerz (model.c:106-150, 305-340): g = (cos phi,
+// sin phi, cos beta, sin beta, detd). The pixel is projected with
+// fac = detd^2 + qx^2 + qy^2, rotated by phi in the detector plane, then the
+// (y, z) components by beta; the image coordinates are the radius in the
+// (x, z) plane and y, scaled by the center.
+__device__ __forceinline__ Cell2 locate_rz(const double *g, double qx, double qy, double center, long long S) {
+	const double detd = g[4];
+	const double fac = dadd(dmul(detd, detd), dadd(dmul(qx, qx), dmul(qy, qy)));
+	const double q0 = __ddiv_rn(dadd(dmul(qx, g[0]), dmul(qy, -g[1])), fac);
+	const double q1 = __ddiv_rn(dadd(dmul(qx, g[1]), dmul(qy, g[0])), fac);
+	const double q2 = dsub(__ddiv_rn(detd, fac), 1.);
+	const double b1 = dadd(dmul(q1, g[2]), dmul(q2, -g[3]));
+	const double b2 = dadd(dmul(q1, g[3]), dmul(q2, g[2]));
+	const double px = dmul(center, dadd(1., __dsqrt_rn(dadd(dmul(q0, q0), dmul(b2, b2)))));
+	const double py = dmul(center, dadd(1., b1));
+	return cell2_at(px, py, S);
+}
+
+// The 4 corner weights in the reference's order (00, 01, 10, 11).
+__device__ __forceinline__ void corner_weights2(const Cell2 &c, double *w) {
+	const double cx = dsub(1., c.fx), cy = dsub(1., c.fy);
+	w[0] = dmul(cx, cy);
+	w[1] = dmul(cx, c.fy);
+	w[2] = dmul(c.fx, cy);
+	w[3] = dmul(c.fx, c.fy);
+}
+
+// W = corr * sum_k w_k m_k, summed left to right; DBL_MIN outside the image
+// and where W <= 0 (model.c:88-99, 136-149).
+template <typename MT>
+__device__ __forceinline__ double interp2(const Cell2 &c, const MT *__restrict__ m, long long S, double corr) {
+	if (!c.ok)
+		return DBL_MIN;
+	double w[4];
+	corner_weights2(c, w);
+	double v = dmul(w[0], (double)__ldg(m + c.i00));
+	v = dadd(v, dmul(w[1], (double)__ldg(m + c.i00 + 1)));
+	v = dadd(v, dmul(w[2], (double)__ldg(m + c.i00 + S)));
+	v = dadd(v, dmul(w[3], (double)__ldg(m + c.i00 + S + 1)));
+	v = dmul(v, corr);
+	return v <= 0. ? DBL_MIN : v;
+}
+
+// Orientation parameters of orientation qi staged in rot[9]: the rotation
+// matrix of quaternion geo[qi * 5 ..] (3-D), or (cos, sin) of its angle from
+// the host-made table geo[qi * 2 ..] (2-D).
+template <int GEO>
+__device__ __forceinline__ void geo_setup(const double *__restrict__ geo, int qi, double *rot) {
+	if constexpr (GEO == MT_3D) {
+		rot_from_quat(geo + (size_t)qi * 5, rot);
+	} else {
+		rot[0] = geo[2 * (size_t)qi];
+		rot[1] = geo[2 * (size_t)qi + 1];
+	}
+}
+
+// W of one pixel under orientation parameters rot (see geo_setup; for RZ the
+// five values of locate_rz).
+template <int GEO, typename MT>
+__device__ __forceinline__ double geo_sample(const double *rot, double qx, double qy, double qz, double center,
+                                             long long S, const MT *__restrict__ m, double corr) {
+	if constexpr (GEO == MT_3D) {
+		return interp(locate(rot, qx, qy, qz, center, S), m, S, corr);
+	} else if constexpr (GEO == MT_2D) {
+		return interp2(locate2d(rot, qx, qy, center, S), m, S, corr);
+	} else {
+		return interp2(locate_rz(rot, qx, qy, center, S), m, S, corr);
+	}
+}
+
 // Compensated FP32 summation (Kahan): the represented sum is s - comp, with
 // an error of order n u^2 sum|x| (u = 2^-24), i.e. far below FP32 rounding.
 // Intrinsics keep the compiler from simplifying (t - s) - y.

@@ -98,9 +98,15 @@ struct dfg_ctx {
 	double mean_count = 0.;
 	bool beta_set = false;
 
-	// orientations and model
+	// orientations and model; model_type MT_2D / MT_RZ hold stacks of S x S
+	// images (V = S^2) and take an angle (2-D) or (phi, beta) (RZ) per
+	// orientation; cs2d [num_rot][2] = (cos, sin) of the 2-D angles, from the
+	// host's libm as the reference's make_rot_angle (model.c:788-795)
 	int num_rot = 0, M = 1, R = 0, RT = 0, R_pad = 0;
-	DevBuf<double> quats;
+	int model_type = MT_3D;
+	bool friedel2d = false;  // params.friedel_sym of a 2-D reconstruction
+	double detd = 0.;        // detector distance (RZ geometry)
+	DevBuf<double> quats, cs2d;
 	long long S = 0, V = 0;
 	DevBuf<double> model1, model2, weight;
 	DevBuf<double2> accum;

@@ -20,7 +20,7 @@ namespace dfg {
 // (background-aware path, max_prob.c:94) they store W itself in FP64 there.
 constexpr int SB = 32;
 
-template <typename MT>
+template <typename MT, int GEO>
 __global__ void __launch_bounds__(256) slice_u_tile_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
     const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(256) slice_u_tile_kernel(
 	for (int j = t; j < TILE; j += blockDim.x) {
 		int r = rt * TILE + j;
 		int rr = r < R ? r : 0;
-		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
+		geo_setup<GEO>(quats, rr / M, s_rot[j]);
 		s_mode[j] = rr % M;
 	}
 	const double center = (double)(S / 2);
@@ -57,10 +57,8 @@ __global__ void __launch_bounds__(256) slice_u_tile_kernel(
 		if (s_m[i] >= 0) {
 			const double qx = s_q[i][0], qy = s_q[i][1], qz = s_q[i][2], cr = s_q[i][3];
 #pragma unroll 2
-			for (int j = g; j < TILE; j += 256 / SB) {
-				Cell c = locate(s_rot[j], qx, qy, qz, center, S);
-				s_w[i][j] = interp(c, model + (size_t)s_mode[j] * V, S, cr);
-			}
+			for (int j = g; j < TILE; j += 256 / SB)
+				s_w[i][j] = geo_sample<GEO>(s_rot[j], qx, qy, qz, center, S, model + (size_t)s_mode[j] * V, cr);
 		}
 		__syncthreads();
 		if (t < TILE) {
@@ -102,7 +100,7 @@ __global__ void __launch_bounds__(256) slice_u_tile_kernel(
 // bit-identical to the reference's sequential sum (max_prob.c:32-38), while
 // all threads store log W as coalesced row segments (max_prob.c:94-97). The
 // host uses it when whole tiles would give the SMs too few blocks.
-template <typename MT, int OB>
+template <typename MT, int OB, int GEO>
 __global__ void __launch_bounds__(256) slice_u_kernel(
     const double *__restrict__ quats, int M, int R, const double *__restrict__ qvals,
     const double *__restrict__ corr, const uint8_t *__restrict__ mask, int P, const MT *__restrict__ model,
@@ -120,7 +118,7 @@ __global__ void __launch_bounds__(256) slice_u_kernel(
 	for (int j = t; j < OB; j += blockDim.x) {
 		const int r = r0 + j;
 		const int rr = r < R ? r : 0;
-		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
+		geo_setup<GEO>(quats, rr / M, s_rot[j]);
 		s_mode[j] = rr % M;
 	}
 	const double center = (double)(S / 2);
@@ -146,10 +144,8 @@ __global__ void __launch_bounds__(256) slice_u_kernel(
 			if (s_m[i] >= 0) {
 				const double qx = s_q[i][0], qy = s_q[i][1], qz = s_q[i][2], cr = s_q[i][3];
 #pragma unroll 2
-				for (int j = t / CB; j < OB; j += 256 / CB) {
-					Cell c = locate(s_rot[j], qx, qy, qz, center, S);
-					s_w[i][j] = interp(c, model + (size_t)s_mode[j] * V, S, cr);
-				}
+				for (int j = t / CB; j < OB; j += 256 / CB)
+					s_w[i][j] = geo_sample<GEO>(s_rot[j], qx, qy, qz, center, S, model + (size_t)s_mode[j] * V, cr);
 			}
 		}
 		__syncthreads();
@@ -778,6 +774,7 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 // that set is the one of a cached weight grid, with_weight is 0 and only the
 // model sums are accumulated. With views_final the tomograms already are the
 // views (background-aware update) and are not divided by psum_r.
+template <int GEO>
 __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ psum_r,
                                                      const double *__restrict__ quats, int M, int R,
@@ -794,7 +791,7 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 	for (int j = t; j < TILE; j += blockDim.x) {
 		int r = rt * TILE + j;
 		int rr = r < R ? r : 0;
-		rot_from_quat(&quats[(rr / M) * 5], s_rot[j]);
+		geo_setup<GEO>(quats, rr / M, s_rot[j]);
 		s_mode[j] = rr % M;
 		s_ps[j] = r < R ? psum_r[r] : 0.;
 	}
@@ -822,29 +819,44 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 	const double qx = qvals[3 * (size_t)p], qy = qvals[3 * (size_t)p + 1], qz = qvals[3 * (size_t)p + 2];
 	const double cr = corr[p];
 	const double center = (double)(S / 2);
+	constexpr int NC = GEO == MT_3D ? 8 : 4;  // corners
 	long long o[8];
-	corner_offsets(S, o);
+	if constexpr (GEO == MT_3D) {
+		corner_offsets(S, o);
+	} else {
+		o[0] = 0; o[1] = 1; o[2] = S; o[3] = S + 1;
+	}
 	for (int k = 0; k < TILE / 4; ++k) {
 		const int j = g + 4 * k;
 		const double ps = s_ps[j];
 		if (!(ps > 0.))
 			continue;
-		Cell c = locate(s_rot[j], qx, qy, qz, center, S);
-		if (!c.ok)
-			continue;
-		const double wv = views_final ? (double)s_tile[i][j] / cr : ((double)s_tile[i][j] / ps) / cr;
 		double fw[8];
-		corner_weights(c, fw);
-		double *a = accum + 2 * ((size_t)s_mode[j] * V + c.i000);
+		long long base;
+		if constexpr (GEO == MT_3D) {
+			Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+			if (!c.ok)
+				continue;
+			corner_weights(c, fw);
+			base = c.i000;
+		} else {
+			Cell2 c = locate2d(s_rot[j], qx, qy, center, S);
+			if (!c.ok)
+				continue;
+			corner_weights2(c, fw);
+			base = c.i00;
+		}
+		const double wv = views_final ? (double)s_tile[i][j] / cr : ((double)s_tile[i][j] / ps) / cr;
+		double *a = accum + 2 * ((size_t)s_mode[j] * V + base);
 		if (with_weight) {
 #pragma unroll
-			for (int q = 0; q < 8; ++q) {
+			for (int q = 0; q < NC; ++q) {
 				atomicAdd(a + 2 * o[q], fw[q] * wv);
 				atomicAdd(a + 2 * o[q] + 1, fw[q]);
 			}
 		} else {
 #pragma unroll
-			for (int q = 0; q < 8; ++q)
+			for (int q = 0; q < NC; ++q)
 				atomicAdd(a + 2 * o[q], fw[q] * wv);
 		}
 	}
@@ -909,6 +921,38 @@ __global__ void friedel_kernel(double *__restrict__ model2, const double *__rest
 	const int mx = 2 * c - x, my = 2 * c - y;
 	const bool first = (x < mx) || (x == mx && y <= my);
 	if (!first)
+		return;
+	double A = friedel_avg(a[v1], w[v1], a[v2], w[v2]);
+	if (v1 != v2)
+		A = friedel_avg(A, w[v2], A, w[v1]);
+	a[v1] = A;
+	a[v2] = A;
+}
+
+// symmetrize_friedel2d (model.c:495-515) over every layer: (y, z) and
+// (2c - y, 2c - z) for y in [lo, S), z in [lo, c], visited as friedel_kernel
+// visits its pairs (the z == c line holds the pairs touched twice).
+__global__ void friedel2d_kernel(double *__restrict__ model2, const double *__restrict__ weight, int S, int M) {
+	const int c = S / 2, lo = (S % 2 == 0) ? 1 : 0, n = S - lo, nz = c - lo + 1;
+	const long long per_layer = (long long)n * nz;
+	const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= per_layer * M)
+		return;
+	const int layer = (int)(id / per_layer);
+	const long long k = id - (long long)layer * per_layer;
+	const int z = lo + (int)(k % nz), y = lo + (int)(k / nz);
+	const long long A2 = (long long)S * S;
+	double *a = model2 + (size_t)layer * A2;
+	const double *w = weight + (size_t)layer * A2;
+	const long long v1 = (long long)y * S + z, v2 = (long long)(2 * c - y) * S + (2 * c - z);
+	if (z < c) {
+		const double A = friedel_avg(a[v1], w[v1], a[v2], w[v2]);
+		a[v1] = A;
+		a[v2] = A;
+		return;
+	}
+	// z == c: the member visited first owns the pair
+	if (y > 2 * c - y)
 		return;
 	double A = friedel_avg(a[v1], w[v1], a[v2], w[v2]);
 	if (v1 != v2)
@@ -1171,41 +1215,63 @@ __global__ void __launch_bounds__(256) voronoi_kernel(const double *__restrict__
 }
 
 // One slice, un-logged (Model.slice_gen, model.c:11-59)
-__global__ void slice_one_kernel(const double *__restrict__ quat, int mode, const double *__restrict__ qvals,
+// (slice_gen2d / slice_genrz, model.c:65-150, for 2-D and RZ models: g holds
+// the quaternion, or (cos, sin) of the angle, or the five RZ parameters)
+template <int GEO>
+__global__ void slice_one_kernel(const double *__restrict__ g, int mode, const double *__restrict__ qvals,
                                  const double *__restrict__ corr, int P, const double *__restrict__ model,
                                  long long S, long long V, double *__restrict__ out) {
 	int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= P)
 		return;
 	double rot[9];
-	rot_from_quat(quat, rot);
-	Cell c = locate(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2],
-	                (double)(S / 2), S);
-	out[p] = interp(c, model + (size_t)mode * V, S, corr[p]);
+	if constexpr (GEO == MT_3D)
+		rot_from_quat(g, rot);
+	else
+		for (int k = 0; k < 5; ++k)
+			rot[k] = g[k];
+	out[p] = geo_sample<GEO>(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2],
+	                         (double)(S / 2), S, model + (size_t)mode * V, corr[p]);
 }
 
 // One merge in FP64 (Model.slice_merge, model.c:171-244)
-__global__ void merge_one_kernel(const double *__restrict__ quat, int mode, const double *__restrict__ view,
+// (slice_merge2d / slice_mergerz, model.c:254-340, for 2-D and RZ models)
+template <int GEO>
+__global__ void merge_one_kernel(const double *__restrict__ g, int mode, const double *__restrict__ view,
                                  const double *__restrict__ qvals, const double *__restrict__ corr,
                                  const uint8_t *__restrict__ mask, int P, long long S, long long V,
                                  double *__restrict__ model2, double *__restrict__ weight) {
 	int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= P || mask[p] > 1)
 		return;
-	double rot[9];
-	rot_from_quat(quat, rot);
-	Cell c = locate(rot, qvals[3 * (size_t)p], qvals[3 * (size_t)p + 1], qvals[3 * (size_t)p + 2],
-	                (double)(S / 2), S);
-	if (!c.ok)
-		return;
+	const double qx = qvals[3 * (size_t)p], qy = qvals[3 * (size_t)p + 1], qz = qvals[3 * (size_t)p + 2];
+	const double center = (double)(S / 2);
 	double fw[8];
-	long long o[8];
-	corner_weights(c, fw);
-	corner_offsets(S, o);
+	long long o[8], base;
+	int nc;
+	if constexpr (GEO == MT_3D) {
+		double rot[9];
+		rot_from_quat(g, rot);
+		Cell c = locate(rot, qx, qy, qz, center, S);
+		if (!c.ok)
+			return;
+		corner_weights(c, fw);
+		corner_offsets(S, o);
+		base = c.i000;
+		nc = 8;
+	} else {
+		Cell2 c = GEO == MT_2D ? locate2d(g, qx, qy, center, S) : locate_rz(g, qx, qy, center, S);
+		if (!c.ok)
+			return;
+		corner_weights2(c, fw);
+		o[0] = 0; o[1] = 1; o[2] = S; o[3] = S + 1;
+		base = c.i00;
+		nc = 4;
+	}
 	const double w = view[p] / corr[p];
-	for (int q = 0; q < 8; ++q) {
-		atomicAdd(weight + (size_t)mode * V + c.i000 + o[q], fw[q]);
-		atomicAdd(model2 + (size_t)mode * V + c.i000 + o[q], fw[q] * w);
+	for (int q = 0; q < nc; ++q) {
+		atomicAdd(weight + (size_t)mode * V + base + o[q], fw[q]);
+		atomicAdd(model2 + (size_t)mode * V + base + o[q], fw[q] * w);
 	}
 }
 

@@ -66,6 +66,7 @@ extern "C" int dfg_slice_gen_noalloc(dfg_ctx *ctx, const double *quat, int mode,
 		return DFG_ERR_ARG;
 	NEED(ctx->P > 0 && ctx->S > 0, DFG_ERR_STATE, "slice_gen_noalloc: detector and model must be set");
 	NEED(mode >= 0 && mode < ctx->M, DFG_ERR_ARG, "slice_gen_noalloc: mode %d out of range", mode);
+	NEED(ctx->model_type == MT_3D, DFG_ERR_ARG, "slice_gen_noalloc: 3-D models only");
 	NEED(ctx->P <= DFG_NOALLOC_MAX_PIXELS, DFG_ERR_ARG,
 	     "slice_gen_noalloc: the detector has %d pixels, more than the maximum of %d", ctx->P,
 	     DFG_NOALLOC_MAX_PIXELS);

@@ -89,8 +89,9 @@ class Iterate:
         param.from_config(config_fname, section_name)
         self.set_params(param)
         rtype = {RECON3D: "3d", RECON2D: "2d", RECONRZ: "rz"}[param.rtype]
-        if rtype != "3d":
-            raise NotImplementedError("only 3-D reconstructions are supported")
+        if rtype == "rz":
+            # recon.pyx:86-91 selects no slice functions for RZ iterations
+            raise NotImplementedError("RZ reconstructions: Model.slice_gen / slice_merge only")
         print("Doing %s recon from %s" % (rtype.upper(), config_fname))
         folder = op.dirname(config_fname)
         config = MyConfigParser()

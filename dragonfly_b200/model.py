@@ -1,9 +1,11 @@
 """Intensity model (mirror of dragonfly.model.Model, dragonfly/model.pyx:18-313).
 
-model1 is the current 3-D intensity [num_modes, size, size, size] (float64,
-C order, centre size // 2); model2 / inter_weight hold the last iteration's
-merged model and interpolation weights. slice_gen / slice_merge run on the
-GPU through the C ABI (dfg_slice_gen / dfg_slice_merge).
+model1 is the current intensity [num_modes, size, size, size] (MODEL_3D) or
+[num_modes, size, size] (MODEL_2D, MODEL_RZ) (float64, C order, centre
+size // 2); model2 / inter_weight hold the last iteration's merged model and
+interpolation weights. slice_gen / slice_merge run on the GPU through the C
+ABI (dfg_slice_gen / dfg_slice_merge); the orientation is a quaternion (3-D),
+an angle (2-D) or (phi, beta) (RZ, which uses the detector's detd).
 """
 import os
 
@@ -18,8 +20,12 @@ _MODEL_TYPES = {"3d": "MODEL_3D", "2d": "MODEL_2D", "rz": "MODEL_RZ"}
 _slice_ctx = None
 
 
+_TYPE_CODES = {"MODEL_3D": 0, "MODEL_2D": 1, "MODEL_RZ": 2}
+
+
 def _slice_context(det, model):
-    """A shared GPU context holding det and this model, for one-slice calls."""
+    """A shared GPU context holding det and this Model's model1, for
+    one-slice calls."""
     global _slice_ctx
     from ._lib import Context
     if _slice_ctx is None:
@@ -30,7 +36,9 @@ def _slice_context(det, model):
     if c._det_id != key:
         c.set_detector(det.qvals, det.corr, det.raw_mask)
         c._det_id = key
-    c.set_model(model)
+    c.set_model_type(_TYPE_CODES[model.mtype])
+    c.set_detector_distance(getattr(det, "detd", 0.))
+    c.set_model(model.model1)
     return c
 
 
@@ -103,24 +111,22 @@ class Model:
             self.model1 = np.random.random(shape) * model_mean
 
     def slice_gen(self, quat, det, mode=0, view=None):
-        """Slice of model1 at quat on det (model.c:11-59), on the GPU."""
+        """Slice of model1 at quat on det (slice_gen3d / slice_gen2d /
+        slice_genrz, model.c:11-150), on the GPU."""
         if self.model1 is None:
             raise AttributeError("Allocate model1 first")
-        if self.mtype != "MODEL_3D":
-            raise NotImplementedError("only 3-D models are supported")
-        out = _slice_context(det, self.model1).slice_gen(quat, mode)
+        out = _slice_context(det, self).slice_gen(quat, mode)
         if view is not None:
             view[...] = out
             return view
         return out
 
     def slice_merge(self, quat, view, det, mode=0):
-        """Merges view into model2 / inter_weight (model.c:171-244), on the GPU."""
+        """Merges view into model2 / inter_weight (slice_merge3d / 2d / rz,
+        model.c:171-340), on the GPU."""
         if self.model2 is None:
             raise AttributeError("Allocate model2 first")
-        if self.mtype != "MODEL_3D":
-            raise NotImplementedError("only 3-D models are supported")
-        _slice_context(det, self.model1).slice_merge(quat, view, self.model2, self.inter_weight, mode)
+        _slice_context(det, self).slice_merge(quat, view, self.model2, self.inter_weight, mode)
 
     def free(self):
         self.model1 = self.model2 = self.inter_weight = None
@@ -169,11 +175,39 @@ class Model:
         m[xm, ym, c] = a
 
     @staticmethod
+    def symmetrize_friedel2d(model, weights):
+        """In-place Friedel average of every layer of a [layers, S, S] stack
+        (model.c:495-515), visiting z <= centre like the reference (pairs on
+        the z = centre line are averaged twice)."""
+        size = model.shape[-1]
+        c = size // 2
+        lo = 1 if size % 2 == 0 else 0
+
+        def avg(a1, w1, a2, w2):
+            a = 0.5 * (a1 * w1 + a2 * w2)
+            ws = 0.5 * (w1 + w2)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                return np.where(ws > 0, a / np.where(ws > 0, ws, 1.), 0.)
+
+        r = np.arange(lo, size)
+        for m, w in zip(model.reshape(-1, size, size), weights.reshape(-1, size, size)):
+            y, z = np.meshgrid(r, np.arange(lo, c), indexing="ij")
+            a = avg(m[y, z], w[y, z], m[2 * c - y, 2 * c - z], w[2 * c - y, 2 * c - z])
+            m[y, z] = a
+            m[2 * c - y, 2 * c - z] = a
+            y = r[r <= 2 * c - r]
+            ym = 2 * c - y
+            w1, w2 = w[y, c], w[ym, c]
+            a = avg(m[y, c], w1, m[ym, c], w2)
+            a = np.where(y == ym, a, avg(a, w2, a, w1))
+            m[y, c] = a
+            m[ym, c] = a
+
+    @staticmethod
     def _unsupported(*args, **kwargs):
         raise NotImplementedError("point-group / axial symmetrisation and model rotation are not supported")
 
     symmetrize_octahedral = _unsupported
     symmetrize_icosahedral = _unsupported
     symmetrize_axial = _unsupported
-    symmetrize_friedel2d = _unsupported
     rotate_model = _unsupported

@@ -19,7 +19,7 @@ import time
 import numpy as np
 
 from .iterate import Iterate
-from .params import RECON3D
+from .params import RECON2D, RECON3D
 
 try:
     import h5py
@@ -57,8 +57,14 @@ class EMCRecon:
         if itr.quat is None:
             print("Set quat for iterate first")
             return
-        if itr.params.rtype != RECON3D or itr.model.mtype != "MODEL_3D":
-            raise NotImplementedError("only 3-D reconstructions are supported")
+        two_d = itr.params.rtype == RECON2D
+        if not ((itr.params.rtype == RECON3D and itr.model.mtype == "MODEL_3D")
+                or (two_d and itr.model.mtype == "MODEL_2D")):
+            # recon.pyx:86-91 selects slice functions for 3-D and 2-D only
+            raise NotImplementedError("3-D and 2-D reconstructions are supported (RZ: Model.slice_gen / "
+                                      "slice_merge only)")
+        if two_d and (itr.params.axial_sym > 1 or itr.quat.icosahedral_flag or itr.quat.octahedral_flag):
+            raise NotImplementedError("point-group and axial symmetries apply to 3-D models")
         if itr.params.nonrot_modes:
             raise NotImplementedError("non-rotating modes are not supported")
         from ._lib import Context
@@ -71,6 +77,9 @@ class EMCRecon:
         # background-aware updates (max_update.c:232-543, max_scale.c:21-288)
         c.set_background(det.background if det.with_bg else None)
         c.set_quaternions(itr.quat.quats)
+        # 2-D: angles in quats[:, 0], images [modes, S, S], Friedel average
+        # when params.friedel_sym (recon.pyx:118-119)
+        c.set_model_type(1 if two_d else 0, itr.params.friedel_sym if two_d else 0)
         c.set_model(itr.model.model1)
         # refinement (max_prob.c:110-120 with src/iterate.c:103-130)
         if itr.params.refine:
@@ -80,7 +89,8 @@ class EMCRecon:
             self.refinement = 1
         # update_model's symmetries (recon.pyx:120-134)
         pg = 2 if itr.quat.icosahedral_flag else (1 if itr.quat.octahedral_flag else 0)
-        c.set_symmetry(pg, itr.params.axial_sym if itr.params.axial_sym > 1 else 0)
+        if not two_d:
+            c.set_symmetry(pg, itr.params.axial_sym if itr.params.axial_sym > 1 else 0)
         itr.quat.divide(0, 1, itr.params.num_modes, itr.params.nonrot_modes)
         itr.params.rank, itr.params.num_proc = 0, 1
         self._iter = itr
@@ -113,7 +123,8 @@ class EMCRecon:
         c.set_option("keep_prob", 1 if par.save_prob else 0)
         likelihood = c.maximize(p)
         self.update_model()
-        if par.need_scaling == 1:
+        # recon.pyx:102-103: volumes only
+        if par.need_scaling == 1 and itr.model.mtype == "MODEL_3D":
             itr.normalize_scale()
         fp = c.frame_params()
         itr.beta[itr.blacklist == 0] = fp["beta"][itr.blacklist == 0]

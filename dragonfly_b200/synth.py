@@ -157,13 +157,34 @@ def model_mean_count(model, qvals, corr, mask, rng, n_orient=256):
     return w[:, mask <= 1].sum(1).mean()
 
 
-def sample_frames(model, qvals, corr, mask, n_frames, rng, phi=None, chunk=256):
-    """Poisson frames at random orientations, in the sparse .emc layout.
+def slices2d(model, angles, qvals, corr):
+    """Bilinear slices W[n, P] of a 2-D image at in-plane angles: pixel
+    (qx, qy) rotated by [[c, -s], [s, c]] plus the centre, times corr; zero
+    outside the image (vectorised; used only to simulate data)."""
+    size = model.shape[0]
+    c, s = np.cos(angles)[:, None], np.sin(angles)[:, None]
+    px = c * qvals[None, :, 0] - s * qvals[None, :, 1] + size // 2
+    py = s * qvals[None, :, 0] + c * qvals[None, :, 1] + size // 2
+    x0, y0 = np.floor(px).astype(np.int64), np.floor(py).astype(np.int64)
+    fx, fy = px - x0, py - y0
+    ok = (x0 >= 0) & (x0 <= size - 2) & (y0 >= 0) & (y0 <= size - 2)
+    x0, y0 = np.where(ok, x0, 0), np.where(ok, y0, 0)
+    out = ((1 - fx) * (1 - fy) * model[x0, y0] + (1 - fx) * fy * model[x0, y0 + 1]
+           + fx * (1 - fy) * model[x0 + 1, y0] + fx * fy * model[x0 + 1, y0 + 1])
+    return np.where(ok, out, 0.) * corr[None, :]
+
+
+def sample_frames(model, qvals, corr, mask, n_frames, rng, phi=None, chunk=256, two_d=False):
+    """Poisson frames at random orientations (quaternions, or angles in
+    [0, 2 pi) for a 2-D image), in the sparse .emc layout.
 
     Returns dict(ones, multi, place_ones, place_multi, count_multi, quats, phi).
     Pixels with mask == 2 never receive photons."""
     good = mask <= 1
-    quats = random_quaternions(n_frames, rng)
+    if two_d:
+        quats = rng.random(n_frames) * 2. * np.pi
+    else:
+        quats = random_quaternions(n_frames, rng)
     if phi is None:
         phi = np.ones(n_frames)
     ones = np.zeros(n_frames, np.int32)
@@ -171,7 +192,8 @@ def sample_frames(model, qvals, corr, mask, n_frames, rng, phi=None, chunk=256):
     po, pm, cm = [], [], []
     for s in range(0, n_frames, chunk):
         e = min(n_frames, s + chunk)
-        lam = slices(model, quats[s:e], qvals, corr) * phi[s:e, None]
+        sl = slices2d if two_d else slices
+        lam = sl(model, quats[s:e], qvals, corr) * phi[s:e, None]
         lam[:, ~good] = 0.
         counts = rng.poisson(np.maximum(lam, 0.))
         for i in range(e - s):
@@ -211,3 +233,40 @@ def small_problem(seed=0, det_side=64, size=75, qmax=37., n_atoms=300, atom_radi
                 model_start=model_start, model_true=intens, **{k: fr[k] for k in
                 ('ones', 'multi', 'place_ones', 'place_multi', 'count_multi')},
                 frame_quats=fr['quats'])
+
+
+def small_problem_2d(seed=0, det_side=48, n_blobs=30, num_rot=90, n_frames=600, mean_count=80.,
+                     hole_radius=3.):
+    """A 2-D reconstruction (recon_type = 2d): a det_side^2 flat detector in
+    pixel units (qz = 0), an image of n_blobs Gaussian blobs on the
+    Iterate.calculate_size grid, num_rot equal-weight in-plane angles
+    (Quaternion.generate_2d) and Poisson frames at random angles. Mask: 2
+    inside hole_radius, 1 beyond size / 2 - 2 (merged, not in the likelihood)."""
+    rng = np.random.default_rng(seed)
+    c = (det_side - 1) / 2.
+    ix, iy = np.meshgrid(np.arange(det_side) - c, np.arange(det_side) - c, indexing="ij")
+    qvals = np.stack([ix.ravel(), iy.ravel(), np.zeros(ix.size)], 1)
+    r = np.hypot(qvals[:, 0], qvals[:, 1])
+    size = int(2 * np.ceil(r.max()) + 3)
+    mask = np.zeros(r.size, np.uint8)
+    mask[r > size / 2 - 2] = 1
+    mask[r < hole_radius] = 2
+    corr = 1. + 0.1 * rng.random(r.size)
+    corr /= corr.mean()
+    x = np.arange(size) - size // 2
+    gx, gy = np.meshgrid(x, x, indexing="ij")
+    img = np.zeros((size, size))
+    for _ in range(n_blobs):
+        cx, cy = rng.normal(0., size / 6., 2)
+        sg = 1.5 + 2. * rng.random()
+        img += rng.random() * np.exp(-((gx - cx) ** 2 + (gy - cy) ** 2) / (2 * sg * sg))
+    lam = slices2d(img, rng.random(64) * 2 * np.pi, qvals, corr)
+    img *= mean_count / lam[:, mask <= 1].sum(1).mean()
+    fr = sample_frames(img, qvals, corr, mask, n_frames, rng, two_d=True)
+    quats = np.zeros((num_rot, 5))
+    quats[:, 0] = np.arange(num_rot) * (2 * np.pi / num_rot)
+    quats[:, 4] = 1. / num_rot
+    model_start = rng.random((1, size, size))
+    return dict(qvals=qvals, corr=corr, mask=mask, quats=quats, model_start=model_start, model_true=img,
+                **{k: fr[k] for k in ('ones', 'multi', 'place_ones', 'place_multi', 'count_multi')},
+                frame_angles=fr['quats'])

@@ -78,10 +78,27 @@ DFG_API int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const in
  * (dragonfly/src/quaternion.h:11-15). */
 DFG_API int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quats);
 
-/* Model model1 [num_modes][size][size][size] (C order), centre size / 2.
+/* Model model1 [num_modes][size][size][size] (C order), centre size / 2;
+ * [num_modes][size][size] for 2-D and RZ models (dfg_set_model_type).
  * Replaces Iterate.set_model / Model.allocate (dragonfly/iterate.pyx:184-190,
  * dragonfly/model.pyx:43-103). */
 DFG_API int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const double *model1);
+
+/* Model type, as struct model's mtype (model.h:13-17) and params.rtype:
+ * 0 = 3-D volume (quaternion orientations; the default), 1 = stack of 2-D
+ * images (orientation = the in-plane angle quats[r][0]; slice_gen2d /
+ * slice_merge2d, model.c:65-99, 254-290), 2 = RZ image (orientation =
+ * (phi, beta); slice_genrz / slice_mergerz, model.c:106-150, 299-340; the one-
+ * slice operations only, as the reference's run_iteration selects no RZ slice
+ * functions, recon.pyx:86-91). friedel_sym: update_model applies the 2-D
+ * Friedel average (symmetrize_friedel2d, model.c:495-515) to 2-D models
+ * (params.friedel_sym, recon.pyx:118-119); RZ models always get it. Changing
+ * the type clears the model: call dfg_set_model afterwards. */
+DFG_API int dfg_set_model_type(dfg_ctx *ctx, int model_type, int friedel_sym);
+
+/* Detector distance in pixels (struct detector's detd, detector.h:15), used by
+ * the RZ geometry. */
+DFG_API int dfg_set_detector_distance(dfg_ctx *ctx, double detd);
 
 /* Per-frame arrays (num_data entries). Replace the Iterate.scale setter,
  * parse_blacklist and calc_beta (dragonfly/iterate.pyx:284-402;
@@ -183,11 +200,13 @@ DFG_API int dfg_get_sparse_prob(dfg_ctx *ctx, int *place_prob, double *prob);
 DFG_API int dfg_get_tomograms(dfg_ctx *ctx, int r0, int n, double *out);
 
 /* ---- one-slice operations -------------------------------------------------
- * Model.slice_gen (dragonfly/model.pyx:105-132 -> model.c:11-59): slice of
- * model1 at one quaternion, out[num_pix]. */
+ * Model.slice_gen (dragonfly/model.pyx:105-132 -> model.c:11-59, 65-150):
+ * slice of model1 at one orientation, out[num_pix]; quat is a quaternion (5
+ * values), an angle (2-D) or (phi, beta) (RZ) by the model type. */
 DFG_API int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double *out);
-/* Model.slice_merge (dragonfly/model.pyx:134-151 -> model.c:171-244): merges
- * view[num_pix] into the host arrays model2 / inter_weight [modes][size^3]. */
+/* Model.slice_merge (dragonfly/model.pyx:134-151 -> model.c:171-340): merges
+ * view[num_pix] into the host arrays model2 / inter_weight [modes][size^3]
+ * ([modes][size^2] for 2-D and RZ models). */
 DFG_API int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const double *view,
                     double *model2, double *inter_weight);
 

@@ -51,19 +51,27 @@ def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
 
 
+MODEL_TYPES = {"3d": 0, "2d": 1, "rz": 2}   # enum model_type, model.h:13
+
+
 class EMCProblem:
     """Inputs of an EMC reconstruction in the reference's layouts.
 
     Attributes mirror the reference structs: detector (``qvals [P,3]``, ``corr``,
     ``mask``), sparse frames (``ones``, ``multi``, ``place_ones``,
     ``place_multi``, ``count_multi``), ``quats [R,5]``, model1
-    ``[M, S, S, S]`` and the [emc] parameters used by the iteration.
+    ``[M, S, S, S]`` (``model_type`` "3d") or ``[M, S, S]`` ("2d", "rz"; the
+    orientation is then the angle in column 0, or (phi, beta) for RZ) and the
+    [emc] parameters used by the iteration.
     """
 
     def __init__(self, qvals, corr, mask, ones, multi, place_ones, place_multi, count_multi,
                  quats, model1, need_scaling=0, update_scale=1, known_scale=0, alpha=0.,
                  beta=1., beta_jump=1., beta_period=100, beta_factor=1., scale=None,
-                 blacklist=None):
+                 blacklist=None, model_type="3d", friedel_sym=0, detd=0.):
+        self.model_type = model_type
+        self.friedel_sym = int(friedel_sym)
+        self.detd = float(detd)
         self.qvals = _c(qvals, np.float64).reshape(-1, 3)
         self.corr = _c(corr, np.float64)
         self.mask = _c(mask, np.uint8)
@@ -74,7 +82,8 @@ class EMCProblem:
         self.count_multi = _c(count_multi, np.int32)
         self.quats = _c(quats, np.float64).reshape(-1, 5)
         m = _c(model1, np.float64)
-        self.model1 = m.reshape((-1,) + m.shape[-3:]) if m.ndim >= 3 else m
+        nd = 3 if model_type == "3d" else 2
+        self.model1 = m.reshape((-1,) + m.shape[-nd:]) if m.ndim >= nd else m
         self.need_scaling = int(need_scaling)
         self.update_scale = int(update_scale)
         self.known_scale = int(known_scale)
@@ -134,7 +143,7 @@ class ReferenceEngine:
         L = self.lib
         L.ref_create.restype = C.c_void_p
         L.ref_create.argtypes = [C.c_int, _dp, _dp, _up, C.c_int, _ip, _ip, _ip, _ip, _ip,
-                                 C.c_int, _dp, C.c_long, C.c_int, _dp,
+                                 C.c_int, _dp, C.c_long, C.c_int, C.c_int, _dp,
                                  C.c_int, C.c_int, C.c_int, C.c_double,
                                  C.c_double, C.c_double, C.c_int, C.c_double,
                                  C.c_void_p, C.c_void_p, C.c_int]
@@ -158,6 +167,7 @@ class ReferenceEngine:
         L.ref_get_frame_prob.restype = C.c_int
         L.ref_get_frame_prob.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.ref_set_refinement.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_set_friedel_detd.argtypes = [C.c_void_p, C.c_int, C.c_double]
         self.save_prob = False
         self.prob = p = prob
         self._scale_buf = p.scale
@@ -165,10 +175,11 @@ class ReferenceEngine:
         self.h = L.ref_create(
             p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, p.num_data, p.ones, p.multi,
             p.place_ones, p.place_multi, p.count_multi, p.num_rot, p.quats.reshape(-1),
-            p.size, p.num_modes, p.model1.reshape(-1), p.need_scaling, p.update_scale,
+            p.size, p.num_modes, MODEL_TYPES[p.model_type], p.model1.reshape(-1), p.need_scaling, p.update_scale,
             p.known_scale, p.alpha, p.beta, p.beta_jump, p.beta_period, p.beta_factor,
             None if p.scale is None else p.scale.ctypes.data,
             None if p.blacklist is None else p.blacklist.ctypes.data, int(num_threads))
+        L.ref_set_friedel_detd(self.h, int(p.friedel_sym), float(p.detd))
 
     def close(self):
         if getattr(self, "h", None):
@@ -273,7 +284,8 @@ class ReferenceEngine:
         res["model2"] = self._arr(L.ref_get_model2, p.model1.shape)
         it = self.iter_arrays()
         res["beta"] = it["beta"]
-        if p.need_scaling:
+        res["scale"] = it["scale"]
+        if p.need_scaling and p.model_type == "3d":   # recon.pyx:102-103
             scale = it["scale"]
             model1 = self.model1()
             rms, _ = normalize_scale(scale, p.blacklist, model1, rms)

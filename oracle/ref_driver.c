@@ -70,7 +70,7 @@ ref_engine *ref_create(int num_pix, const double *qvals, const double *corr, con
                        int num_data, const int *ones, const int *multi, const int *place_ones,
                        const int *place_multi, const int *count_multi,
                        int num_rot, const double *quats,
-                       long size, int num_modes, const double *model1,
+                       long size, int num_modes, int mtype, const double *model1,
                        int need_scaling, int update_scale, int known_scale, double alpha,
                        double beta_start, double beta_jump, int beta_period, double beta_factor,
                        const double *scale, const uint8_t *blacklist, int num_threads) {
@@ -112,7 +112,7 @@ ref_engine *ref_create(int num_pix, const double *qvals, const double *corr, con
 	/* Parameters (params.pyx:13-46 defaults, then the values we are given) */
 	e->par.rank = 0;
 	e->par.num_proc = 1;
-	e->par.rtype = RECON3D;
+	e->par.rtype = mtype == MODEL_2D ? RECON2D : (mtype == MODEL_RZ ? RECONRZ : RECON3D);
 	e->par.verbosity = 0;
 	e->par.need_scaling = need_scaling;
 	e->par.update_scale = update_scale;
@@ -131,11 +131,12 @@ ref_engine *ref_create(int num_pix, const double *qvals, const double *corr, con
 	e->quat.quats = dup_mem(quats, (size_t)num_rot * 5 * sizeof(double));
 	e->quat.num_rot_p = num_modes * num_rot;
 
-	/* Model (model.pyx:57-63, 280-284) */
-	e->mod.mtype = MODEL_3D;
+	/* Model (model.pyx:24-63, 280-284): a volume, or a stack of 2-D images
+	 * (MODEL_2D, MODEL_RZ) */
+	e->mod.mtype = mtype;
 	e->mod.size = size;
 	e->mod.center = size / 2;
-	e->mod.vol = size * size * size;
+	e->mod.vol = mtype == MODEL_3D ? size * size * size : size * size;
 	e->mod.num_modes = num_modes;
 	e->mod.model1 = dup_mem(model1, (size_t)num_modes * e->mod.vol * sizeof(double));
 	e->mod.model2 = calloc((size_t)num_modes * e->mod.vol, sizeof(double));
@@ -188,8 +189,15 @@ double ref_maximize(ref_engine *e, int iteration) {
 			it->beta[d] = 1.;
 	}
 
-	slice_gen = &slice_gen3d;
-	slice_merge = &slice_merge3d;
+	/* recon.pyx:86-91: 3-D or 2-D slice functions (none for RECONRZ there) */
+	if (e->par.rtype == RECON2D) {
+		slice_gen = &slice_gen2d;
+		slice_merge = &slice_merge2d;
+	}
+	else {
+		slice_gen = &slice_gen3d;
+		slice_merge = &slice_merge3d;
+	}
 	free_common(e->mdata, it->tot_num_data);
 	e->mdata->iter = it;
 	e->mdata->within_openmp = 0;
@@ -197,15 +205,19 @@ double ref_maximize(ref_engine *e, int iteration) {
 	return e->avg_likelihood;
 }
 
-/* recon.pyx:112-149 for RECON3D: the icosahedral or octahedral point group
- * (Quaternion.icosahedral_flag / octahedral_flag) in place of the Friedel
- * average, then the axial symmetry (params.axial_sym), then the division. */
+/* recon.pyx:112-149: for RECONRZ, or RECON2D with params.friedel_sym, the
+ * 2-D Friedel average of every layer; for RECON3D the icosahedral or
+ * octahedral point group (Quaternion.icosahedral_flag / octahedral_flag) in
+ * place of the Friedel average, then the axial symmetry (params.axial_sym,
+ * volumes only); then the division. */
 double ref_update_model(ref_engine *e) {
 	long x;
 	double diff, change = 0.;
 	struct model *mod = &e->mod;
 
-	for (x = 0; x < mod->num_modes; ++x) {
+	if (e->par.rtype == RECONRZ || (e->par.rtype == RECON2D && e->par.friedel_sym))
+		symmetrize_friedel2d(mod->model2, mod->inter_weight, mod->num_modes, (int)mod->size);
+	for (x = 0; x < mod->num_modes && e->par.rtype == RECON3D; ++x) {
 		double *m2 = &mod->model2[x * mod->vol], *w = &mod->inter_weight[x * mod->vol];
 		if (e->quat.icosahedral_flag)
 			symmetrize_icosahedral(m2, w, (int)mod->size);
@@ -214,7 +226,7 @@ double ref_update_model(ref_engine *e) {
 		else
 			symmetrize_friedel(m2, w, (int)mod->size);
 	}
-	if (e->par.axial_sym > 1)
+	if (e->par.axial_sym > 1 && e->par.rtype == RECON3D)
 		for (x = 0; x < mod->num_modes; ++x)
 			symmetrize_axial(&mod->model2[x * mod->vol], &mod->inter_weight[x * mod->vol], (int)mod->size,
 			                 e->par.axial_sym);
@@ -358,14 +370,32 @@ void ref_get_scalars(ref_engine *e, double *out) {
 
 void ref_set_rms(ref_engine *e, double rms) { e->iter.rms_change = rms; }
 
-/* Model.slice_gen / slice_merge (model.pyx:105-151) on this engine's detector. */
+/* Model.slice_gen / slice_merge (model.pyx:105-151) on this engine's detector,
+ * by model type: quat is a quaternion (3-D), an angle (2-D) or (phi, beta) (RZ). */
 void ref_slice_gen(ref_engine *e, const double *quat, int mode, double *out) {
-	slice_gen3d((double *)quat, mode, out, &e->det, &e->mod);
+	if (e->mod.mtype == MODEL_2D)
+		slice_gen2d((double *)quat, mode, out, &e->det, &e->mod);
+	else if (e->mod.mtype == MODEL_RZ)
+		slice_genrz((double *)quat, mode, out, &e->det, &e->mod);
+	else
+		slice_gen3d((double *)quat, mode, out, &e->det, &e->mod);
 }
 
 void ref_slice_merge(ref_engine *e, const double *quat, int mode, const double *view, double *model2,
                      double *weight) {
-	slice_merge3d((double *)quat, mode, (double *)view, model2, weight, e->mod.size, &e->det);
+	if (e->mod.mtype == MODEL_2D)
+		slice_merge2d((double *)quat, mode, (double *)view, model2, weight, e->mod.size, &e->det);
+	else if (e->mod.mtype == MODEL_RZ)
+		slice_mergerz((double *)quat, mode, (double *)view, model2, weight, e->mod.size, &e->det);
+	else
+		slice_merge3d((double *)quat, mode, (double *)view, model2, weight, e->mod.size, &e->det);
+}
+
+/* params.friedel_sym (2-D Friedel average in update_model) and the detector
+ * distance detd that the RZ geometry uses (detector.pyx:50). */
+void ref_set_friedel_detd(ref_engine *e, int friedel_sym, double detd) {
+	e->par.friedel_sym = friedel_sym;
+	e->det.detd = detd;
 }
 
 /* Quaternion.generate_3d (quaternion.pyx:94-102): count, and the list if out != NULL. */

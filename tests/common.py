@@ -51,6 +51,9 @@ class GPUEngine:
         c.set_detector(p.qvals, p.corr, p.mask)
         c.set_frames(p.ones, p.multi, p.place_ones, p.place_multi, p.count_multi)
         c.set_quaternions(p.quats)
+        if p.model_type != "3d":
+            c.set_model_type(p.model_type, p.friedel_sym)
+            c.set_detector_distance(p.detd)
         c.set_model(p.model1)
         if p.scale is not None:
             c.set_scale(p.scale)
@@ -72,7 +75,7 @@ class GPUEngine:
         _, m2, w = c.model()
         res["model2_sum"], res["inter_weight"] = m2, w
         rms = c.update_model(p.alpha)
-        if p.need_scaling:
+        if p.need_scaling and p.model_type == "3d":   # recon.pyx:102-103
             c.normalize_scale()
             rms = c.scalars()["rms_change"]
         fp = c.frame_params()

@@ -115,3 +115,36 @@ def test_emcrecon_refinement_from_a_coarse_run(tmp_path, oracle_built):
         assert all(r < 0 or itr.quat.quat_mapping[r] in itr.rel_quat[i] for i, r in enumerate(recon.rmax))
     recon.free()
     ref.close()
+
+
+def test_emcrecon_2d_from_config(tmp_path, oracle_built):
+    """recon_type = 2d: the detector's q vectors projected to the detector
+    plane (CDetector._convert_2d, detector.pyx:128-134), num_rot in-plane
+    angles over [0, pi) with friedel_sym (quaternion.pyx:70-74), a
+    [modes, S, S] image, and the iteration against the reference engine."""
+    from dragonfly_b200 import Iterate
+    from dragonfly_b200.recon import EMCRecon
+    from oracle.oracle import ReferenceEngine, reference_available
+    if not reference_available():
+        pytest.skip("reference engine library not built")
+    d, cfg = write_problem(tmp_path, extra="recon_type = 2d\nnum_rot = 48\nfriedel_sym = 1\n")
+    itr = Iterate(cfg)
+    assert itr.model.mtype == "MODEL_2D" and itr.model.model1.ndim == 3
+    assert itr.quat.num_rot == 48 and itr.quat.quats[:, 0].max() < np.pi
+    assert np.abs(itr.dets[0].qvals[:, :2]).max() > np.abs(d["qvals"][:, :2]).max()   # pixel units
+    start = itr.model.model1.copy()
+    recon = EMCRecon()
+    recon.set_iterate(itr)
+    prob = EMCProblem(itr.dets[0].qvals, itr.dets[0].corr, itr.dets[0].raw_mask, d["ones"], d["multi"],
+                      d["place_ones"], d["place_multi"], d["count_multi"], itr.quat.quats, start,
+                      beta=0.5, beta_jump=2., beta_period=3, model_type="2d", friedel_sym=1)
+    ref = ReferenceEngine(prob)
+    for it in (1, 2, 3):
+        itr.params.iteration = it
+        ll = recon.run_iteration()
+        b = ref.run_iteration(it)
+        assert rel_l2(itr.model.model1, b["model1"]) <= MODEL_REL_L2
+        assert rel(ll, b["avg_likelihood"]) <= SCALAR_REL
+        assert np.mean(recon.rmax == b["rmax"]) >= 0.999
+    recon.free()
+    ref.close()
