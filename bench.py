@@ -2,8 +2,9 @@
 """Benchmark of one EMC iteration (expand -> maximize -> compress).
 
 A step is one iteration -- maximize (slices, E-step with pruning, per-frame
-normalisation, M-step, merge, scale update) + update_model + normalize_scale --
-on the production-size plain workload:
+normalisation, M-step, merge, scale update) + update_model + normalize_scale,
+launched as one CUDA graph (dfg_run_iteration) -- on the production-size plain
+workload:
 
   260 x 257 flat pnCCD-like detector, 6-row panel gap (rows 127-132), radius-10
   central hole; 201^3 model from 2000 Gaussian atoms in a radius-30 sphere;
@@ -237,9 +238,8 @@ def run_ours(args, rank, world, local_rank):
                           beta_period=w["beta_period"], beta_factor=1.)
 
     def step(it):
-        ctx.maximize(params(it))
-        ctx.update_model(0.)
-        ctx.normalize_scale()
+        # maximize + update_model + normalize_scale, captured as one CUDA graph
+        ctx.run_iteration(params(it), 0.)
 
     it = 1
     for _ in range(args.warmup):

@@ -65,6 +65,8 @@ _SIGS = {
     "dfg_set_symmetry": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_set_refinement": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_longlong), _I]),
     "dfg_set_model_type": (C.c_int, [_V, C.c_int, C.c_int]),
+    "dfg_run_iteration": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D]),
+    "dfg_get_graph_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
     "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
     "dfg_voronoi_subset": (C.c_int, [_V, C.c_int, _D, C.c_int, _D, _I]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
@@ -286,6 +288,20 @@ class Context:
         m = C.c_double(0.)
         self.call("dfg_normalize_scale", C.byref(m))
         return m.value
+
+    def run_iteration(self, par, alpha=0.):
+        """maximize + update_model (+ normalize_scale for need_scaling and
+        volumes) with one synchronisation, as a CUDA graph where possible.
+        Returns dict(avg_likelihood, rms_change, mutual_info, rescale,
+        mean_scale)."""
+        out = np.zeros(5)
+        self.call("dfg_run_iteration", C.byref(par), float(alpha), ptr(out, C.c_double))
+        return dict(zip(("avg_likelihood", "rms_change", "mutual_info", "rescale", "mean_scale"), out.tolist()))
+
+    def graph_stats(self):
+        out = (C.c_long * 3)()
+        self.call("dfg_get_graph_stats", out)
+        return dict(launches=out[0], instantiations=out[1], updates=out[2])
 
     def run_iteration_host(self, par, model1, alpha=0., rmax=None, likelihood=None):
         """model1 (float64, C order) is updated in place."""

@@ -18,19 +18,39 @@ using namespace dfg;
 // ---------------------------------------------------------------------------
 // phase timing
 // ---------------------------------------------------------------------------
+// With option timing, each phase instance records a begin and an end event
+// from a pool (no synchronisation, so the records can sit inside a captured
+// graph); phase_collect adds the elapsed times up once the stream has
+// synchronised. A pool that runs out leaves the rest of the call untimed.
 static void phase_begin(dfg_ctx *ctx, int ph) {
-	if (ctx->timing)
-		cudaEventRecord(ctx->ev[2 * ph], ctx->stream);
+	if (!ctx->timing || ctx->ev_next + 2 > (int)ctx->ev_pool.size())
+		return;
+	ctx->ev_open[ph] = ctx->ev_next;
+	// under stream capture, external records become event-record nodes (the
+	// flag is refused outside a capture)
+	cudaEventRecordWithFlags(ctx->ev_pool[ctx->ev_next], ctx->stream,
+	                         ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+	ctx->ev_next += 2;
 }
 static void phase_end(dfg_ctx *ctx, int ph, long launches) {
-	if (!ctx->timing)
+	if (!ctx->timing || ctx->ev_open[ph] < 0)
 		return;
-	cudaEventRecord(ctx->ev[2 * ph + 1], ctx->stream);
-	cudaEventSynchronize(ctx->ev[2 * ph + 1]);
-	float ms = 0.f;
-	cudaEventElapsedTime(&ms, ctx->ev[2 * ph], ctx->ev[2 * ph + 1]);
-	ctx->phase_ms[ph] += ms;
-	ctx->phase_launches[ph] += launches;
+	const int b = ctx->ev_open[ph];
+	cudaEventRecordWithFlags(ctx->ev_pool[b + 1], ctx->stream,
+	                         ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+	ctx->ev_pending.push_back({ph, b, launches});
+	ctx->ev_open[ph] = -1;
+}
+static void phase_collect(dfg_ctx *ctx) {
+	for (const auto &q : ctx->ev_pending) {
+		float ms = 0.f;
+		if (cudaEventElapsedTime(&ms, ctx->ev_pool[q.ev], ctx->ev_pool[q.ev + 1]) == cudaSuccess)
+			ctx->phase_ms[q.phase] += ms;
+		ctx->phase_launches[q.phase] += q.launches;
+	}
+	cudaGetLastError();
+	ctx->ev_pending.clear();
+	ctx->ev_next = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -55,7 +75,8 @@ extern "C" int dfg_create(int device, dfg_ctx **out) {
 		delete ctx;
 		return DFG_ERR_CUDA;
 	}
-	for (auto &e : ctx->ev)
+	ctx->ev_pool.assign(kTimingEvents, nullptr);
+	for (auto &e : ctx->ev_pool)
 		cudaEventCreate(&e);
 	for (auto &e : ctx->user_ev)
 		cudaEventCreate(&e);
@@ -68,12 +89,14 @@ extern "C" void dfg_destroy(dfg_ctx *ctx) {
 		return;
 	cudaSetDevice(ctx->device);
 	cudaStreamSynchronize(ctx->stream);
-	for (auto &e : ctx->ev)
+	for (auto &e : ctx->ev_pool)
 		if (e)
 			cudaEventDestroy(e);
 	for (auto &e : ctx->user_ev)
 		if (e)
 			cudaEventDestroy(e);
+	if (ctx->graph_exec)
+		cudaGraphExecDestroy(ctx->graph_exec);
 	ctx->chunks.clear();
 	cudaStreamDestroy(ctx->stream);
 	delete ctx;
@@ -822,7 +845,10 @@ static int update_scale_bg(dfg_ctx *ctx, const Chunk &ch, const dfg_iter_params 
 	return DFG_OK;
 }
 
-extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_likelihood) {
+// The part of maximize that allocates, uploads or checks on the host, done
+// before any of its kernels is queued (so that the queued part can be
+// captured into a CUDA graph).
+static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 	if (!ctx || !par)
 		return DFG_ERR_ARG;
 	NEED(par->beta_period > 0, DFG_ERR_ARG, "beta_period must be > 0");
@@ -830,37 +856,61 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	if (int rc = ensure_buffers(ctx))
 		return rc;
 	cudaStream_t st = ctx->stream;
-	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
-	const long long S = ctx->S, V = ctx->V;
-	const int nblk = (P + PB - 1) / PB;
-	// background-aware path (max_prob.c:134, max_update.c:10-14, max_scale.c:8-10)
-	const bool bg = ctx->with_bg && par->need_scaling;
-	if (bg) {
-		NEED(ctx->chunks.size() == 1, DFG_ERR_NOMEM,
-		     "background-aware updates need all %d frames in one chunk (%d chunks at the pair budget; raise "
-		     "option pair_budget_mb)",
-		     N, (int)ctx->chunks.size());
-		if (int rc = ensure_bg(ctx))
-			return rc;
-	}
-	double *const Wd = bg ? ctx->Wd.p : nullptr;  // FP64 slices for the background path
 	// recon.pyx:86-91 selects the 3-D or the 2-D slice functions; an RZ
 	// iteration has none there
 	NEED(ctx->model_type != MT_RZ, DFG_ERR_ARG, "RZ models: slice_gen / slice_merge only, no iteration");
-	const bool two_d = ctx->model_type == MT_2D;
+	// background-aware path (max_prob.c:134, max_update.c:10-14, max_scale.c:8-10)
+	if (ctx->with_bg && par->need_scaling) {
+		NEED(ctx->chunks.size() == 1, DFG_ERR_NOMEM,
+		     "background-aware updates need all %d frames in one chunk (%d chunks at the pair budget; raise "
+		     "option pair_budget_mb)",
+		     ctx->N, (int)ctx->chunks.size());
+		if (int rc = ensure_bg(ctx))
+			return rc;
+	}
 	// refinement: the reference indexes quat_mapping by the flat orientation
 	// index over all modes (max_prob.c:114), which only covers one mode
-	RefineMask rm{nullptr, nullptr, 0};
 	if (ctx->refine) {
-		NEED(M == 1, DFG_ERR_ARG, "refinement needs num_modes == 1");
-		if (!ctx->qmap_valid || ctx->qmap.n < (size_t)R_pad) {
-			std::vector<int> q((size_t)R_pad, -1);
+		NEED(ctx->M == 1, DFG_ERR_ARG, "refinement needs num_modes == 1");
+		if (!ctx->qmap_valid || ctx->qmap.n < (size_t)ctx->R_pad) {
+			std::vector<int> q((size_t)ctx->R_pad, -1);
 			std::copy(ctx->h_qmap.begin(), ctx->h_qmap.end(), q.begin());
 			CK(upload(ctx->qmap, q.data(), q.size(), st));
+			CK(cudaStreamSynchronize(st));
 			ctx->qmap_valid = true;
 		}
-		rm = RefineMask{ctx->qmap.p, ctx->rel_bits.p, ctx->rwords};
 	}
+	// merge weight cache: grid, psum_r > 0 pattern and flags (on the device)
+	CK(ctx->weight_cache.ensure((size_t)ctx->M * ctx->V));
+	CK(ctx->wpattern.ensure((size_t)ctx->R_pad));
+	CK(ctx->wflags.ensure(2));
+	if (!ctx->weight_cache_valid) {
+		CK(cudaMemsetAsync(ctx->wflags.p, 0, 2 * sizeof(int), st));
+		CK(cudaMemsetAsync(ctx->wpattern.p, 0, (size_t)ctx->R_pad, st));
+		ctx->weight_cache_valid = true;  // from here on the device tracks it
+	}
+	return DFG_OK;
+}
+
+// Whether one iteration queues its kernels without waiting on the host: the
+// sparse-probability lists (keep_prob) and the background-aware scale search
+// do host work between kernels.
+static bool graphable(const dfg_ctx *ctx, const dfg_iter_params *par) {
+	return !ctx->keep_prob && !(ctx->with_bg && par->need_scaling && par->update_scale);
+}
+
+// Queues maximize's kernels (after max_prepare). Synchronises only where
+// graphable() is false.
+static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
+	cudaStream_t st = ctx->stream;
+	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
+	const long long S = ctx->S, V = ctx->V;
+	const int nblk = (P + PB - 1) / PB;
+	const bool bg = ctx->with_bg && par->need_scaling;
+	double *const Wd = bg ? ctx->Wd.p : nullptr;  // FP64 slices for the background path
+	const bool two_d = ctx->model_type == MT_2D;
+	const RefineMask rm = ctx->refine ? RefineMask{ctx->qmap.p, ctx->rel_bits.p, ctx->rwords}
+	                                  : RefineMask{nullptr, nullptr, 0};
 
 	// update_beta (recon.pyx:161-171)
 	{
@@ -941,10 +991,15 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 				    ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm);
 				CKL("estep_bg_kernel");
 			} else {
-				estep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
-				    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
-				    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p,
-				    ctx->targ.p, rm);
+#define DFG_ESTEP(REF)                                                                                        \
+	estep_kernel<REF><<<blocks_for(warps, 8), 256, 0, st>>>(                                                  \
+	    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,          \
+	    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm)
+				if (rm.qmap != nullptr)
+					DFG_ESTEP(true);
+				else
+					DFG_ESTEP(false);
+#undef DFG_ESTEP
 				CKL("estep_kernel");
 			}
 		}
@@ -1011,35 +1066,24 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	}
 
 	// merge (merge_tomogram -> slice_merge3d); the weight grid is rebuilt only
-	// when the set of orientations with psum_r > 0 changed
-	int with_weight = 1;
-	{
-		std::vector<double> pr(R);
-		CK(cudaMemcpyAsync(pr.data(), ctx->psum_r.p, (size_t)R * sizeof(double), cudaMemcpyDeviceToHost, st));
-		CK(cudaStreamSynchronize(st));
-		std::vector<uint8_t> pattern(R);
-		for (int r = 0; r < R; ++r)
-			pattern[r] = pr[r] > 0.;
-		if (ctx->weight_cache_valid && pattern == ctx->weight_pattern)
-			with_weight = 0;
-		ctx->weight_pattern.swap(pattern);
-		CK(ctx->weight_cache.ensure((size_t)M * V));
-	}
+	// when the set of orientations with psum_r > 0 changed (decided on the device)
+	weight_pattern_kernel<<<1, 1024, 0, st>>>(ctx->psum_r.p, R, ctx->wpattern.p, ctx->wflags.p);
+	CKL("weight_pattern_kernel");
 	phase_begin(ctx, PH_MERGE);
 	if (two_d)
 		merge_kernel<MT_2D><<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->cs2d.p, M, R, ctx->qvals.p,
 		                                                     ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
-		                                                     with_weight, bg ? 1 : 0);
+		                                                     ctx->wflags.p, bg ? 1 : 0);
 	else
 		merge_kernel<MT_3D><<<dim3(nblk, RT), 256, 0, st>>>(ctx->T.p, ctx->psum_r.p, ctx->quats.p, M, R, ctx->qvals.p,
 		                                                     ctx->corr.p, ctx->mask.p, P, S, V, (double *)ctx->accum.p,
-		                                                     with_weight, bg ? 1 : 0);
+		                                                     ctx->wflags.p, bg ? 1 : 0);
 	CKL("merge_kernel");
 	phase_end(ctx, PH_MERGE, 1);
 
 	phase_begin(ctx, PH_UPDATE);
 	unpack_accum_kernel<<<blocks_for((long long)M * V, 256), 256, 0, st>>>(
-	    ctx->accum.p, (long long)M * V, ctx->model2.p, ctx->weight.p, ctx->weight_cache.p, with_weight);
+	    ctx->accum.p, (long long)M * V, ctx->model2.p, ctx->weight.p, ctx->weight_cache.p, ctx->wflags.p);
 	CKL("unpack_accum_kernel");
 	// averages over good frames; the packaged Iterate never sets num_blacklist,
 	// so they divide by N (max_prob.c:373-374, iterate.pyx:35)
@@ -1057,17 +1101,30 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 		}
 	}
 	phase_end(ctx, PH_UPDATE, par->need_scaling && par->update_scale ? 3 : 2);
+	ctx->views_final = bg;
+	return DFG_OK;
+}
 
-	double h[3];
-	CK(cudaMemcpyAsync(h, ctx->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-	CK(cudaStreamSynchronize(st));
-	ctx->weight_cache_valid = true;
+// maximize's scalar results from h = scalars[0..2] (rescale, sum info, sum
+// log-likelihood), read back after its kernels completed.
+static void max_finish(dfg_ctx *ctx, const double *h) {
 	ctx->rescale = h[0];
-	ctx->mutual_info = h[1] / N;
-	ctx->avg_ll = h[2] / N;
+	ctx->mutual_info = h[1] / ctx->N;
+	ctx->avg_ll = h[2] / ctx->N;
 	ctx->have_results = true;
 	ctx->have_prob = ctx->keep_prob;
-	ctx->views_final = bg;
+}
+
+extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *avg_likelihood) {
+	if (int rc = max_prepare(ctx, par))
+		return rc;
+	if (int rc = max_enqueue(ctx, par))
+		return rc;
+	double h[3];
+	CK(cudaMemcpyAsync(h, ctx->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	phase_collect(ctx);
+	max_finish(ctx, h);
 	if (avg_likelihood)
 		*avg_likelihood = ctx->avg_ll;
 	return DFG_OK;
@@ -1185,11 +1242,8 @@ extern "C" int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order) 
 	return DFG_OK;
 }
 
-extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) {
-	if (!ctx)
-		return DFG_ERR_ARG;
-	NEED(ctx->have_results, DFG_ERR_STATE, "update_model: run dfg_maximize first");
-	CK(cudaSetDevice(ctx->device));
+// Queues update_model's kernels; the squared change lands in scalars[3].
+static int update_enqueue(dfg_ctx *ctx, double alpha) {
 	cudaStream_t st = ctx->stream;
 	const long long n = (long long)ctx->M * ctx->V;
 	const int S = (int)ctx->S, lo = (S % 2 == 0) ? 1 : 0;
@@ -1238,12 +1292,47 @@ extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) 
 	sum_kernel<<<1, 1024, 0, st>>>(ctx->red_part.p, nb, ctx->scalars.p + 3);
 	CKL("sum_kernel");
 	phase_end(ctx, PH_UPDATE, launched - 1);
+	return DFG_OK;
+}
+
+extern "C" int dfg_update_model(dfg_ctx *ctx, double alpha, double *rms_change) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	NEED(ctx->have_results, DFG_ERR_STATE, "update_model: run dfg_maximize first");
+	CK(cudaSetDevice(ctx->device));
+	if (int rc = update_enqueue(ctx, alpha))
+		return rc;
 	double change = 0.;
-	CK(cudaMemcpyAsync(&change, ctx->scalars.p + 3, sizeof(double), cudaMemcpyDeviceToHost, st));
-	CK(cudaStreamSynchronize(st));
+	CK(cudaMemcpyAsync(&change, ctx->scalars.p + 3, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	phase_collect(ctx);
 	ctx->rms = std::sqrt(change / ctx->M / (double)ctx->V);
 	if (rms_change)
 		*rms_change = ctx->rms;
+	return DFG_OK;
+}
+
+// Queues normalize_scale's kernels: sum and count of the good frames' phi
+// into scalars[4..5], then phi /= mean and model1 (mode 0) *= mean.
+static int normalize_enqueue(dfg_ctx *ctx) {
+	cudaStream_t st = ctx->stream;
+	scale_sum_kernel<<<1, 1024, 0, st>>>(ctx->scale.p, ctx->blacklist.p, ctx->N, ctx->scalars.p + 4);
+	CKL("scale_sum_kernel");
+	const long long n = std::max<long long>(ctx->V, ctx->N);
+	apply_scale_norm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(ctx->scale.p, ctx->blacklist.p, ctx->N,
+	                                                             ctx->model1.p, nullptr, ctx->V,
+	                                                             ctx->scalars.p + 4);
+	CKL("apply_scale_norm_kernel");
+	return DFG_OK;
+}
+
+// The mean from h = scalars[4..5], after normalize_enqueue's kernels ran.
+static int normalize_finish(dfg_ctx *ctx, const double *h, double *mean_scale) {
+	NEED(h[1] > 0, DFG_ERR_STATE, "normalize_scale: no good frames");
+	const double mean = h[0] / h[1];
+	ctx->rms *= mean;
+	if (mean_scale)
+		*mean_scale = mean;
 	return DFG_OK;
 }
 
@@ -1254,25 +1343,94 @@ extern "C" int dfg_normalize_scale(dfg_ctx *ctx, double *mean_scale) {
 		return rc;
 	NEED(ctx->S > 0, DFG_ERR_STATE, "model not set");
 	CK(cudaSetDevice(ctx->device));
-	cudaStream_t st = ctx->stream;
 	CK(ctx->scalars.ensure(8));
-	scale_sum_kernel<<<1, 1024, 0, st>>>(ctx->scale.p, ctx->blacklist.p, ctx->N, ctx->scalars.p + 4);
-	CKL("scale_sum_kernel");
+	if (int rc = normalize_enqueue(ctx))
+		return rc;
 	double h[2];
-	CK(cudaMemcpyAsync(h, ctx->scalars.p + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaMemcpyAsync(h, ctx->scalars.p + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return normalize_finish(ctx, h, mean_scale);
+}
+
+// One whole iteration (EMCRecon.run_iteration's compute, recon.pyx:94-104):
+// maximize, update_model and, when need_scaling (volumes only, recon.pyx:
+// 102-103), normalize_scale, with one synchronisation at the end. Where no
+// step needs the host in between (graphable) and option graph is on, the
+// queued kernels are captured into a CUDA graph and launched as one; the
+// graph of the previous iteration is updated in place when only kernel
+// arguments changed (beta factor, alpha), else instantiated again.
+static int iteration_enqueue(dfg_ctx *ctx, const dfg_iter_params *par, double alpha, bool normalize) {
+	if (int rc = max_enqueue(ctx, par))
+		return rc;
+	if (int rc = update_enqueue(ctx, alpha))
+		return rc;
+	if (normalize)
+		if (int rc = normalize_enqueue(ctx))
+			return rc;
+	return DFG_OK;
+}
+
+extern "C" int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double alpha, double *out) {
+	if (int rc = max_prepare(ctx, par))
+		return rc;
+	cudaStream_t st = ctx->stream;
+	const bool normalize = par->need_scaling && ctx->model_type == MT_3D;
+	if (ctx->use_graph && graphable(ctx, par)) {
+		CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		ctx->capturing = true;
+		const int rc = iteration_enqueue(ctx, par, alpha, normalize);
+		cudaGraph_t g = nullptr;
+		const cudaError_t e = cudaStreamEndCapture(st, &g);
+		ctx->capturing = false;
+		if (rc != DFG_OK || e != cudaSuccess) {
+			if (g)
+				cudaGraphDestroy(g);
+			cudaGetLastError();
+			return rc != DFG_OK ? rc : ctx->fail(DFG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+		}
+		if (ctx->graph_exec) {
+			cudaGraphExecUpdateResultInfo info;
+			if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) == cudaSuccess) {
+				ctx->graph_updates++;
+			} else {
+				cudaGetLastError();
+				cudaGraphExecDestroy(ctx->graph_exec);
+				ctx->graph_exec = nullptr;
+			}
+		}
+		if (!ctx->graph_exec) {
+			const cudaError_t ei = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+			if (ei != cudaSuccess) {
+				cudaGraphDestroy(g);
+				ctx->graph_exec = nullptr;
+				return ctx->fail(DFG_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ei));
+			}
+			ctx->graph_instantiations++;
+		}
+		cudaGraphDestroy(g);
+		CK(cudaGraphLaunch(ctx->graph_exec, st));
+		ctx->graph_launches++;
+	} else {
+		if (int rc = iteration_enqueue(ctx, par, alpha, normalize))
+			return rc;
+	}
+	double h[6];
+	CK(cudaMemcpyAsync(h, ctx->scalars.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
-	NEED(h[1] > 0, DFG_ERR_STATE, "normalize_scale: no good frames");
-	const double mean = h[0] / h[1];
-	CK(cudaMemcpyAsync(ctx->scalars.p + 6, &mean, sizeof(double), cudaMemcpyHostToDevice, st));
-	const long long n = std::max<long long>(ctx->V, ctx->N);
-	apply_scale_norm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(ctx->scale.p, ctx->blacklist.p, ctx->N,
-	                                                             ctx->model1.p, nullptr, ctx->V,
-	                                                             ctx->scalars.p + 6);
-	CKL("apply_scale_norm_kernel");
-	CK(cudaStreamSynchronize(st));
-	ctx->rms *= mean;
-	if (mean_scale)
-		*mean_scale = mean;
+	phase_collect(ctx);
+	max_finish(ctx, h);
+	ctx->rms = std::sqrt(h[3] / ctx->M / (double)ctx->V);
+	double mean = 1.;
+	if (normalize)
+		if (int rc = normalize_finish(ctx, h + 4, &mean))
+			return rc;
+	if (out) {
+		out[0] = ctx->avg_ll;
+		out[1] = ctx->rms;
+		out[2] = ctx->mutual_info;
+		out[3] = ctx->rescale;
+		out[4] = mean;
+	}
 	return DFG_OK;
 }
 
@@ -1285,17 +1443,10 @@ extern "C" int dfg_run_iteration_host(dfg_ctx *ctx, const dfg_iter_params *par, 
 	CK(cudaSetDevice(ctx->device));
 	const size_t n = (size_t)ctx->M * ctx->V;
 	CK(cudaMemcpyAsync(ctx->model1.p, model1_inout, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-	double ll = 0., rms = 0.;
-	if (int rc = dfg_maximize(ctx, par, &ll))
+	double out[5];
+	if (int rc = dfg_run_iteration(ctx, par, alpha, out))
 		return rc;
-	if (int rc = dfg_update_model(ctx, alpha, &rms))
-		return rc;
-	if (par->need_scaling) {
-		double m;
-		if (int rc = dfg_normalize_scale(ctx, &m))
-			return rc;
-		rms = ctx->rms;
-	}
+	const double ll = out[0], rms = out[1];
 	CK(cudaMemcpyAsync(model1_inout, ctx->model1.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 	if (rmax)
 		CK(cudaMemcpyAsync(rmax, ctx->rmax.p, (size_t)ctx->N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1560,6 +1711,10 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 		ctx->keep_prob = value != 0.;
 		return DFG_OK;
 	}
+	if (!strcmp(key, "graph")) {
+		ctx->use_graph = value != 0.;
+		return DFG_OK;
+	}
 	if (!strcmp(key, "slice_block")) {
 		const int v = (int)value;
 		NEED(v == 0 || ((v == 16 || v == 32 || v == 64 || v == TILE) && v <= TILE), DFG_ERR_ARG,
@@ -1568,6 +1723,15 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 		return DFG_OK;
 	}
 	return ctx->fail(DFG_ERR_ARG, "unknown option '%s'", key);
+}
+
+extern "C" int dfg_get_graph_stats(dfg_ctx *ctx, long *out) {
+	if (!ctx || !out)
+		return DFG_ERR_ARG;
+	out[0] = ctx->graph_launches;
+	out[1] = ctx->graph_instantiations;
+	out[2] = ctx->graph_updates;
+	return DFG_OK;
 }
 
 extern "C" int dfg_get_phase_times(dfg_ctx *ctx, double *ms, long *launches, int n) {

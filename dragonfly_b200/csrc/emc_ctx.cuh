@@ -18,6 +18,7 @@
 namespace dfg {
 
 enum Phase { PH_SLICE, PH_ESTEP, PH_NORM, PH_PSUM, PH_MSTEP, PH_MERGE, PH_UPDATE, PH_COUNT };
+constexpr int kTimingEvents = 2048;  // phase-timing events per context
 static const char *kPhaseNames[PH_COUNT] = {"slice", "estep", "norm", "psum", "mstep", "merge", "update"};
 
 // Owning device buffer; move-only.
@@ -111,10 +112,18 @@ struct dfg_ctx {
 	DevBuf<double> model1, model2, weight;
 	DevBuf<double2> accum;
 	// inter_weight of the last merge and the psum_r > 0 pattern it was built
-	// for (the weights depend on nothing else once geometry is fixed)
+	// for (the weights depend on nothing else once geometry is fixed); the
+	// pattern and the flags (accumulate weights, grid cached) live on the
+	// device; weight_cache_valid false makes the next maximize clear them
 	DevBuf<double> weight_cache;
-	std::vector<uint8_t> weight_pattern;
+	DevBuf<uint8_t> wpattern;
+	DevBuf<int> wflags;
 	bool weight_cache_valid = false;
+	// the iteration as a CUDA graph (dfg_run_iteration)
+	bool use_graph = true;
+	bool capturing = false;  // the stream is being captured into the graph
+	cudaGraphExec_t graph_exec = nullptr;
+	long graph_launches = 0, graph_updates = 0, graph_instantiations = 0;
 
 	// work buffers
 	DevBuf<float> logW, Pst, T;
@@ -162,7 +171,14 @@ struct dfg_ctx {
 	DevBuf<int> qmap;
 	DevBuf<uint32_t> rel_bits;
 	bool timing = false;
-	cudaEvent_t ev[2 * PH_COUNT] = {};
+	struct PhaseRec {
+		int phase, ev;  // phase, begin event (end = ev + 1) in ev_pool
+		long launches;
+	};
+	std::vector<cudaEvent_t> ev_pool;
+	std::vector<PhaseRec> ev_pending;
+	int ev_next = 0;
+	int ev_open[PH_COUNT] = {-1, -1, -1, -1, -1, -1, -1};
 	cudaEvent_t user_ev[8] = {};
 	long long launches = 0;  // kernels launched by this context
 	double phase_ms[PH_COUNT] = {};

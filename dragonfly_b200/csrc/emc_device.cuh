@@ -57,8 +57,14 @@ __global__ void __launch_bounds__(256) slice_u_tile_kernel(
 		if (s_m[i] >= 0) {
 			const double qx = s_q[i][0], qy = s_q[i][1], qz = s_q[i][2], cr = s_q[i][3];
 #pragma unroll 2
-			for (int j = g; j < TILE; j += 256 / SB)
-				s_w[i][j] = geo_sample<GEO>(s_rot[j], qx, qy, qz, center, S, model + (size_t)s_mode[j] * V, cr);
+			for (int j = g; j < TILE; j += 256 / SB) {
+				if constexpr (GEO == MT_3D) {
+					Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+					s_w[i][j] = interp(c, model + (size_t)s_mode[j] * V, S, cr);
+				} else {
+					s_w[i][j] = geo_sample<GEO>(s_rot[j], qx, qy, qz, center, S, model + (size_t)s_mode[j] * V, cr);
+				}
+			}
 		}
 		__syncthreads();
 		if (t < TILE) {
@@ -144,8 +150,15 @@ __global__ void __launch_bounds__(256) slice_u_kernel(
 			if (s_m[i] >= 0) {
 				const double qx = s_q[i][0], qy = s_q[i][1], qz = s_q[i][2], cr = s_q[i][3];
 #pragma unroll 2
-				for (int j = t / CB; j < OB; j += 256 / CB)
-					s_w[i][j] = geo_sample<GEO>(s_rot[j], qx, qy, qz, center, S, model + (size_t)s_mode[j] * V, cr);
+				for (int j = t / CB; j < OB; j += 256 / CB) {
+					if constexpr (GEO == MT_3D) {
+						Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+						s_w[i][j] = interp(c, model + (size_t)s_mode[j] * V, S, cr);
+					} else {
+						s_w[i][j] =
+						    geo_sample<GEO>(s_rot[j], qx, qy, qz, center, S, model + (size_t)s_mode[j] * V, cr);
+					}
+				}
 			}
 		}
 		__syncthreads();
@@ -267,6 +280,7 @@ __device__ __forceinline__ void refine_skip_tile(double *__restrict__ pval, doub
 	}
 }
 
+template <bool REFINE>
 __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ logw, int R,
     const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off, const long long *__restrict__ ph_mid,
@@ -281,10 +295,13 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 	if (blacklist[d])
 		return;
 	const int r0 = rt * TILE + lane * LW;
-	const unsigned live = refine_live(rm, d, r0);
-	if (rm.qmap != nullptr && !__any_sync(FULL, live)) {
-		refine_skip_tile(pval, tmax, targ, rt, Nc, dl, lane);
-		return;
+	unsigned live = (1u << LW) - 1u;
+	if constexpr (REFINE) {
+		live = refine_live(rm, d, r0);
+		if (!__any_sync(FULL, live)) {
+			refine_skip_tile(pval, tmax, targ, rt, Nc, dl, lane);
+			return;
+		}
 	}
 	const float *L = logW + (size_t)rt * (P + 1) * TILE + lane * LW;
 	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
@@ -351,7 +368,7 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 			if (ECH == 2)
 				ph_sum = dadd(ph_sum, kahan_value(s[ECH - 1][k], c[ECH - 1][k]));
 			acc[k] = dadd(dsub(logw[r], dmul(u[r], sd)), ph_sum);
-			if (!(live >> k & 1u))
+			if (REFINE && !(live >> k & 1u))
 				acc[k] = -INFINITY;
 			else if (acc[k] > m) {
 				m = acc[k];
@@ -781,13 +798,15 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ qvals,
                                                      const double *__restrict__ corr,
                                                      const uint8_t *__restrict__ mask, int P, long long S,
-                                                     long long V, double *__restrict__ accum, int with_weight,
+                                                     long long V, double *__restrict__ accum,
+                                                     const int *__restrict__ weight_flag,
                                                      int views_final) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ double s_ps[TILE];
 	__shared__ float s_tile[PB][TILE + 1];
 	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
+	const int with_weight = *weight_flag;
 	for (int j = t; j < TILE; j += blockDim.x) {
 		int r = rt * TILE + j;
 		int rr = r < R ? r : 0;
@@ -865,14 +884,37 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 // ---------------------------------------------------------------------------
 // model update (recon.pyx:112-149) and small per-frame kernels
 // ---------------------------------------------------------------------------
+// Whether the merge must accumulate weights: the set of orientations with
+// psum_r > 0 (the only input of the weight grid once the geometry is fixed)
+// differs from the one of the cached grid, or no grid is cached. flags[0] =
+// accumulate weights, flags[1] = a grid is cached (cleared by the host when
+// the geometry changes). One block; the pattern is updated in place.
+__global__ void __launch_bounds__(1024) weight_pattern_kernel(const double *__restrict__ psum_r, int R,
+                                                              uint8_t *__restrict__ pattern, int *__restrict__ flags) {
+	int changed = 0;
+	for (int r = threadIdx.x; r < R; r += blockDim.x) {
+		const uint8_t p = psum_r[r] > 0. ? 1 : 0;
+		if (p != pattern[r]) {
+			pattern[r] = p;
+			changed = 1;
+		}
+	}
+	changed = __syncthreads_or(changed);
+	if (threadIdx.x == 0) {
+		flags[0] = (changed || flags[1] == 0) ? 1 : 0;
+		flags[1] = 1;
+	}
+}
+
 // model2 / inter_weight from the accumulators; the weights either come from
 // this merge (and are kept in weight_cache) or from weight_cache.
 __global__ void unpack_accum_kernel(const double2 *__restrict__ accum, long long n, double *__restrict__ model2,
                                     double *__restrict__ weight, double *__restrict__ weight_cache,
-                                    int with_weight) {
+                                    const int *__restrict__ weight_flag) {
 	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
+	const int with_weight = *weight_flag;
 	double2 a = accum[i];
 	model2[i] = a.x;
 	if (with_weight) {
@@ -1160,12 +1202,16 @@ __global__ void __launch_bounds__(1024) scale_sum_kernel(const double *__restric
 	}
 }
 
-// phi /= mean for good frames; model1 of mode 0 *= mean (iterate.pyx:372-382)
+// phi /= mean for good frames; model1 of mode 0 *= mean (iterate.pyx:372-382);
+// mean = sums[0] / sums[1] (sum and count of good frames' phi); nothing
+// changes without good frames (the host reports that case).
 __global__ void apply_scale_norm_kernel(double *__restrict__ scale, const uint8_t *__restrict__ blacklist,
                                         int N, double *__restrict__ model1, float *__restrict__ model1f,
-                                        long long V, const double *__restrict__ mean) {
+                                        long long V, const double *__restrict__ sums) {
 	long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	const double m = *mean;
+	if (!(sums[1] > 0.))
+		return;
+	const double m = sums[0] / sums[1];
 	if (i < V) {
 		double v = model1[i] * m;
 		model1[i] = v;

@@ -223,11 +223,26 @@ DFG_API int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const do
 #define DFG_NOALLOC_MAX_PIXELS 262144
 DFG_API int dfg_slice_gen_noalloc(dfg_ctx *ctx, const double *quat, int mode, double *out);
 
+/* ---- one whole iteration --------------------------------------------------
+ * EMCRecon.run_iteration's compute (recon.pyx:93-104) on the resident inputs:
+ * dfg_maximize, dfg_update_model(alpha) and, when need_scaling and the model
+ * is a volume, dfg_normalize_scale, with one host synchronisation at the end.
+ * out[5] (may be NULL) = average log-likelihood, rms change (after the scale
+ * normalisation), mutual information, rescale, mean scale (1 without
+ * normalisation). Unless option keep_prob, timing or the background-aware
+ * scale search needs the host between kernels, the iteration's kernels are
+ * captured into a CUDA graph and launched as one (option graph, default 1);
+ * later iterations update that graph in place. */
+DFG_API int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double alpha, double *out);
+
+/* Graph use of dfg_run_iteration: out[0] = graph launches, out[1] =
+ * instantiations, out[2] = in-place updates. */
+DFG_API int dfg_get_graph_stats(dfg_ctx *ctx, long *out);
+
 /* ---- end to end from host buffers ----------------------------------------
  * EMCRecon.run_iteration's compute (recon.pyx:93-104): model1_inout (host,
- * [modes][size^3]) is uploaded, maximize + update_model (+ normalize_scale
- * when need_scaling) run, and the new model1, rmax[num_data] and
- * likelihood[num_data] come back to host memory. */
+ * [modes][size^3]) is uploaded, dfg_run_iteration runs, and the new model1,
+ * rmax[num_data] and likelihood[num_data] come back to host memory. */
 DFG_API int dfg_run_iteration_host(dfg_ctx *ctx, const dfg_iter_params *par, double alpha,
                            double *model1_inout, int *rmax, double *likelihood,
                            double *avg_likelihood, double *rms_change);
