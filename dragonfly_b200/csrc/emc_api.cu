@@ -9,9 +9,12 @@
 //   merge -> unpack -> [scale]                          (merge_tomogram, update_scale)
 // The frame chunk bounds the per-pair buffers (12 bytes per orientation x frame).
 
+#include <cudaTypedefs.h>
+
 #include "emc_ctx.cuh"
 #include "emc_device.cuh"
 #include "emc_bg.cuh"
+#include "emc_dense.cuh"
 
 using namespace dfg;
 
@@ -252,6 +255,7 @@ extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const
 	ctx->chunks_R = -1;
 	ctx->have_results = false;
 	ctx->refine = false;  // relevant orientations are per frame
+	ctx->max_count0 = -1;
 	return DFG_OK;
 }
 
@@ -518,7 +522,10 @@ extern "C" int dfg_calc_beta(dfg_ctx *ctx, double start, int need_scaling) {
 // ---------------------------------------------------------------------------
 static int build_chunks(dfg_ctx *ctx) {
 	const int N = ctx->N, P = ctx->P;
-	const size_t pair_bytes = (size_t)ctx->RT * TILE * (sizeof(double) + sizeof(float));
+	// per frame: pval and Pst of every orientation, plus its BF16 count row
+	// in the dense form
+	const size_t pair_bytes = (size_t)ctx->RT * TILE * (sizeof(double) + sizeof(float)) +
+	                          (ctx->dense_active ? (size_t)ctx->K_pad * 2 : 0);
 	size_t budget;
 	if (ctx->pair_budget_mb > 0.) {
 		budget = (size_t)(ctx->pair_budget_mb * 1048576.);
@@ -609,6 +616,7 @@ static int build_chunks(dfg_ctx *ctx) {
 		CK(cudaStreamSynchronize(ctx->stream));
 	}
 	ctx->chunks_R = ctx->R;
+	ctx->chunks_dense = ctx->dense_active;
 	return DFG_OK;
 }
 
@@ -645,7 +653,7 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	CK(ctx->p_norm.ensure(N));
 	CK(ctx->psum_d.ensure(N));
 	CK(ctx->quat_norm.ensure(N * ctx->M));
-	if (ctx->chunks_R != ctx->R) {
+	if (ctx->chunks_R != ctx->R || ctx->chunks_dense != ctx->dense_active) {
 		ctx->pval.release();
 		ctx->Pst.release();
 		ctx->tmax.release();
@@ -845,6 +853,115 @@ static int update_scale_bg(dfg_ctx *ctx, const Chunk &ch, const dfg_iter_params 
 	return DFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// dense form of the E-step photon term (emc_dense.cuh)
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	if (fn == nullptr) {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+		        cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+	}
+	return fn;
+}
+
+// Tensor map of a row-major BF16 matrix [rows][K_pad] read in boxes of
+// 64 columns x box_rows rows with the 128-byte swizzle.
+static int encode_bf16_map(dfg_ctx *ctx, CUtensorMap *map, const void *base, long long rows, int box_rows) {
+	auto fn = tensor_map_encoder();
+	NEED(fn != nullptr, DFG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+	cuuint64_t dims[2] = {(cuuint64_t)ctx->K_pad, (cuuint64_t)rows};
+	cuuint64_t strides[1] = {(cuuint64_t)ctx->K_pad * 2};
+	cuuint32_t box[2] = {(cuuint32_t)DK, (cuuint32_t)box_rows};
+	cuuint32_t estr[2] = {1, 1};
+	const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+	                      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+	                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	NEED(r == CUDA_SUCCESS, DFG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+	return DFG_OK;
+}
+
+// Whether this iteration may take the dense form, and why not (message).
+static const char *dense_refusal(dfg_ctx *ctx, const dfg_iter_params *par) {
+	if (TILE != 128)
+		return "the dense form needs 128-orientation tiles (lane width 4)";
+	if (ctx->with_bg && par->need_scaling)
+		return "the dense form does not take the background-aware E-step";
+	if (ctx->refine)
+		return "the dense form does not take refinement";
+	if (ctx->max_count0 < 0) {
+		int m = 1;
+		for (size_t i = 0; i < ctx->h_place_multi.size(); ++i)
+			if (ctx->h_mask[ctx->h_place_multi[i]] == 0)
+				m = std::max(m, ctx->h_count_multi[i]);
+		ctx->max_count0 = m;
+	}
+	if (ctx->max_count0 > 256)
+		return "the dense form needs photon counts of at most 256 (exact in BF16)";
+	return nullptr;
+}
+
+// Pixel columns and the hi / lo log-slice buffers, before the chunk layout
+// is sized (it counts the remaining memory).
+static int dense_prepare_slices(dfg_ctx *ctx) {
+	if (ctx->dense_P != ctx->P) {
+		std::vector<int> kp, pc((size_t)ctx->P, -1);
+		for (int p = 0; p < ctx->P; ++p)
+			if (ctx->h_mask[p] == 0) {
+				pc[p] = (int)kp.size();
+				kp.push_back(p);
+			}
+		ctx->K = (int)kp.size();
+		ctx->K_pad = std::max(DK, (ctx->K + DK - 1) / DK * DK);
+		CK(upload(ctx->kpix, kp.data(), kp.size(), ctx->stream));
+		CK(upload(ctx->pcol, pc.data(), pc.size(), ctx->stream));
+		CK(cudaStreamSynchronize(ctx->stream));
+		ctx->dense_P = ctx->P;
+		ctx->map_src[0] = ctx->map_src[1] = ctx->map_src[2] = nullptr;
+	}
+	const long long R_pad = (long long)(ctx->M * ctx->num_rot + TILE - 1) / TILE * TILE;
+	const size_t n = (size_t)R_pad * ctx->K_pad;
+	CK(ctx->Ahi.ensure(n));
+	CK(ctx->Alo.ensure(n));
+	if (ctx->map_src[0] != ctx->Ahi.p || ctx->map_src[1] != ctx->Alo.p) {
+		if (int rc = encode_bf16_map(ctx, &ctx->map_hi, ctx->Ahi.p, R_pad, 128))
+			return rc;
+		if (int rc = encode_bf16_map(ctx, &ctx->map_lo, ctx->Alo.p, R_pad, 128))
+			return rc;
+		ctx->map_src[0] = ctx->Ahi.p;
+		ctx->map_src[1] = ctx->Alo.p;
+	}
+	return DFG_OK;
+}
+
+// One chunk's count rows (after the chunk layout is known).
+static int dense_prepare_counts(dfg_ctx *ctx) {
+	const int rows = (ctx->chunk_frames + DN - 1) / DN * DN;
+	CK(ctx->cnt.ensure((size_t)rows * ctx->K_pad));
+	if (ctx->map_src[2] != ctx->cnt.p || ctx->cnt_rows != rows) {
+		if (int rc = encode_bf16_map(ctx, &ctx->map_cnt, ctx->cnt.p, rows, DN))
+			return rc;
+		ctx->map_src[2] = ctx->cnt.p;
+		ctx->cnt_rows = rows;
+	}
+	CK(ctx->derr.ensure(1));
+	CK(cudaMemsetAsync(ctx->derr.p, 0, sizeof(int), ctx->stream));
+	CK(cudaFuncSetAttribute(estep_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DSMEM_BYTES));
+	return DFG_OK;
+}
+
+// The dense buffers are freed when the sparse form is in use.
+static void dense_release(dfg_ctx *ctx) {
+	ctx->Ahi.release();
+	ctx->Alo.release();
+	ctx->cnt.release();
+	ctx->map_src[0] = ctx->map_src[1] = ctx->map_src[2] = nullptr;
+}
+
 // The part of maximize that allocates, uploads or checks on the host, done
 // before any of its kernels is queued (so that the queued part can be
 // captured into a CUDA graph).
@@ -853,8 +970,24 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 		return DFG_ERR_ARG;
 	NEED(par->beta_period > 0, DFG_ERR_ARG, "beta_period must be > 0");
 	CK(cudaSetDevice(ctx->device));
+	// E-step form: dense tensor-core products (option estep_form 1) where
+	// the inputs allow it
+	ctx->dense_active = false;
+	if (ctx->estep_form == 1) {
+		NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0, DFG_ERR_STATE, "set detector, frames and quaternions");
+		const char *why = dense_refusal(ctx, par);
+		NEED(why == nullptr, DFG_ERR_ARG, "%s", why);
+		ctx->dense_active = true;
+		if (int rc = dense_prepare_slices(ctx))
+			return rc;
+	} else if (ctx->Ahi.p != nullptr) {
+		dense_release(ctx);
+	}
 	if (int rc = ensure_buffers(ctx))
 		return rc;
+	if (ctx->dense_active)
+		if (int rc = dense_prepare_counts(ctx))
+			return rc;
 	cudaStream_t st = ctx->stream;
 	// recon.pyx:86-91 selects the 3-D or the 2-D slice functions; an RZ
 	// iteration has none there
@@ -964,7 +1097,13 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CKL("rescale_kernel");
 	logw_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->quats.p, M, R, ctx->logw.p);
 	CKL("logw_kernel");
-	phase_end(ctx, PH_SLICE, 3);
+	if (ctx->dense_active) {
+		split_logw_kernel<<<dim3(ctx->K_pad / DK, RT), 256, 0, st>>>(
+		    ctx->logW.p, P, ctx->kpix.p, ctx->K, ctx->K_pad, (__nv_bfloat16 *)ctx->Ahi.p,
+		    (__nv_bfloat16 *)ctx->Alo.p);
+		CKL("split_logw_kernel");
+	}
+	phase_end(ctx, PH_SLICE, ctx->dense_active ? 4 : 3);
 
 	CK(cudaMemsetAsync(ctx->T.p, 0, (size_t)RT * P * TILE * sizeof(float), st));
 	CK(cudaMemsetAsync(ctx->psum_r.p, 0, (size_t)R_pad * sizeof(double), st));
@@ -982,7 +1121,20 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 		const int Nc = ch.nc;
 		// E-step (calculate_prob, max_prob.c:66-213)
 		phase_begin(ctx, PH_ESTEP);
-		{
+		if (ctx->dense_active) {
+			// counts as BF16 rows, then the tensor-core products
+			CK(cudaMemsetAsync(ctx->cnt.p, 0, (size_t)ctx->cnt_rows * ctx->K_pad * 2, st));
+			densify_counts_kernel<<<blocks_for((long long)Nc * 32, 256), 256, 0, st>>>(
+			    ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->pcol.p, ch.d0, Nc, P, ctx->K_pad,
+			    (__nv_bfloat16 *)ctx->cnt.p);
+			CKL("densify_counts_kernel");
+			const int n_tiles = (Nc + DN - 1) / DN;
+			estep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
+			    ctx->map_hi, ctx->map_lo, ctx->map_cnt, ctx->K_pad / DK, RT, n_tiles, ctx->u.p, ctx->logw.p, R,
+			    ctx->scale.p, ch.d0, Nc, use_scale, ctx->scalars.p, ctx->pval.p, ctx->tmax.p, ctx->targ.p,
+			    ctx->derr.p);
+			CKL("estep_dense_kernel");
+		} else {
 			long long warps = (long long)RT * Nc;
 			if (bg) {
 				estep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
@@ -1003,7 +1155,7 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 				CKL("estep_kernel");
 			}
 		}
-		phase_end(ctx, PH_ESTEP, 1);
+		phase_end(ctx, PH_ESTEP, ctx->dense_active ? 2 : 1);
 		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
 		phase_begin(ctx, PH_NORM);
 		if (M > 1)
@@ -1121,9 +1273,13 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	if (int rc = max_enqueue(ctx, par))
 		return rc;
 	double h[3];
+	int derr = 0;
 	CK(cudaMemcpyAsync(h, ctx->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	if (ctx->dense_active)
+		CK(cudaMemcpyAsync(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
 	phase_collect(ctx);
+	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step: a pipeline wait gave up (results invalid)");
 	max_finish(ctx, h);
 	if (avg_likelihood)
 		*avg_likelihood = ctx->avg_ll;
@@ -1415,9 +1571,13 @@ extern "C" int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, doubl
 			return rc;
 	}
 	double h[6];
+	int derr = 0;
 	CK(cudaMemcpyAsync(h, ctx->scalars.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	if (ctx->dense_active)
+		CK(cudaMemcpyAsync(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
 	phase_collect(ctx);
+	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step: a pipeline wait gave up (results invalid)");
 	max_finish(ctx, h);
 	ctx->rms = std::sqrt(h[3] / ctx->M / (double)ctx->V);
 	double mean = 1.;
@@ -1713,6 +1873,12 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 	}
 	if (!strcmp(key, "graph")) {
 		ctx->use_graph = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "estep_form")) {
+		const int v = (int)value;
+		NEED(v == 0 || v == 1, DFG_ERR_ARG, "estep_form must be 0 (sparse) or 1 (dense)");
+		ctx->estep_form = v;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "slice_block")) {

@@ -2,6 +2,7 @@
 // error/instrumentation state behind the C ABI (include/dragonfly_b200.h).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -162,6 +163,21 @@ struct dfg_ctx {
 	DevBuf<int> prob_count, d_place;
 	DevBuf<long long> d_prob_off;
 	DevBuf<double> d_prob, tomo_out;
+	// dense (tensor-core) form of the E-step photon term. estep_form 0 =
+	// sparse gathers, 1 = dense, 2 = chosen by the autotuner; dense_active is
+	// this iteration's choice. K mask-0 pixels (kpix [K] their indices, pcol
+	// [P] the column of each, -1 elsewhere), K_pad = K rounded up to 64; hi / lo
+	// log-slices [R_pad][K_pad] and one chunk's counts [cnt_rows][K_pad] in
+	// BF16 (stored as 16-bit words); their TMA tensor maps; derr = the dense
+	// kernel's give-up flag
+	int estep_form = 0;
+	bool dense_active = false, chunks_dense = false;
+	int K = 0, K_pad = 0, dense_P = -1, cnt_rows = 0;
+	int max_count0 = -1;  // largest count on a mask-0 pixel; -1 = not known
+	DevBuf<int> kpix, pcol, derr;
+	DevBuf<uint16_t> Ahi, Alo, cnt;
+	CUtensorMap map_hi, map_lo, map_cnt;
+	const void *map_src[3] = {nullptr, nullptr, nullptr};
 	// coarse-to-fine refinement: coarse cell of every orientation (qmap,
 	// [R_pad], -1 past R) and per frame one bit per relevant coarse
 	// orientation (rel_bits, [N][rwords])

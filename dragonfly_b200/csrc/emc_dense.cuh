@@ -1,0 +1,359 @@
+// Dense form of the E-step photon term on the 5th-generation tensor cores
+// (sm_100a tcgen05 + TMA). Included by emc_api.cu only.
+//
+// The photon term of every (orientation r, frame d) pair is a product over the
+// mask-0 pixels: S[r][d] = sum_k count[d][k] * logW[r][k]. With photon counts
+// of at most 256 (exact in BF16) and log-slices split as hi + lo
+// (hi = bf16(x), lo = bf16(x - hi)), S = hi . count^T + lo . count^T is a pair
+// of BF16 matrix products with FP32 accumulation. One CTA computes a tile of
+// 128 orientations x 256 frames over all pixels:
+//   warp 0     TMA producer: per 64-pixel block, the 128 x 64 hi and lo tiles
+//              and the 256 x 64 count tile (128-byte swizzle) into one of
+//              three shared-memory stages;
+//   warp 1     one lane issues tcgen05.mma (M 128, N 256, K 16; hi then lo
+//              against the same count tile), accumulating in 256 TMEM columns,
+//              and releases each stage with tcgen05.commit;
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator (TMEM lane = orientation,
+//              column = frame), pval = log w_r - u_r s_d + S (FP64) stored in
+//              the sparse form's layout, and the tile maximum with its lowest
+//              orientation index.
+// Every wait on an mbarrier gives up after about a second of clock cycles,
+// sets the error flag and lets the CTA free its TMEM and exit.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "emc_common.cuh"
+
+namespace dfg {
+
+constexpr int DN = 256;      // frames per tile (UMMA N)
+constexpr int DK = 64;       // pixels per stage: one 128-byte swizzle row of BF16
+constexpr int DSTAGES = 3;
+constexpr int DA_BYTES = 128 * DK * 2;                 // one 128 x 64 BF16 tile
+constexpr int DB_BYTES = DN * DK * 2;                  // one 256 x 64 BF16 tile
+constexpr int DSTAGE_BYTES = 2 * DA_BYTES + DB_BYTES;  // 64 KB
+constexpr int DEPI_BYTES = 4 * DN * (8 + 4);            // per-warp column maxima
+constexpr int DSMEM_BYTES = 1024 + DSTAGES * DSTAGE_BYTES + DEPI_BYTES + 128;
+constexpr int DGROUP = 16;  // orientation tiles per rasterisation group
+constexpr long long DWAIT_CYCLES = 2000000000LL;  // about one second
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+	return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+	             : "memory");
+}
+
+// Waits for the phase of the given parity to complete; false after about a
+// second (the caller then gives up).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+	const long long t0 = clock64();
+	while (true) {
+		uint32_t done;
+		asm volatile(
+		    "{\n\t.reg .pred p;\n\t"
+		    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		    "selp.u32 %0, 1, 0, p;\n\t}"
+		    : "=r"(done)
+		    : "r"(smem_addr(bar)), "r"(parity)
+		    : "memory");
+		if (done)
+			return true;
+		if (clock64() - t0 > DWAIT_CYCLES)
+			return false;
+	}
+}
+
+// 2-D tiled TMA load into this CTA's shared memory, completing on bar.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+	asm volatile(
+	    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+	    "[%2];" ::"r"(smem_addr(dst)),
+	    "l"((uint64_t)map), "r"(smem_addr(bar)), "r"(x), "r"(y)
+	    : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile with 128-byte swizzle:
+// rows of 128 bytes, 8-row groups 1024 bytes apart (SBO), version 1,
+// layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+	return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+	       ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A
+// and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t DIDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(DN >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "setp.ne.b32 p, %4, 0;\n\t"
+	    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+	    "l"(adesc), "l"(bdesc), "r"(DIDESC), "r"(accumulate)
+	    : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+	                 smem_addr(bar))
+	             : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 16 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+	uint32_t r[16];
+	asm volatile(
+	    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+	    "%14, %15}, [%16];"
+	    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+	      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+	    : "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+	for (int k = 0; k < 16; ++k)
+		v[k] = __uint_as_float(r[k]);
+}
+
+// pval[tile][frame][j] for one frame chunk from the hi / lo log-slices
+// [R_pad][K_pad] and the chunk's counts [Nc_pad][K_pad] (tensor maps), plus
+// the per (tile, frame) maximum and its first orientation, as estep_kernel
+// writes them. Grid: RT x ceil(Nc / 256) tiles, grouped by DGROUP tiles of
+// orientations so that resident CTAs share operands in L2.
+__global__ void __launch_bounds__(192, 1) estep_dense_kernel(
+    const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+    const __grid_constant__ CUtensorMap map_cnt, int num_kb, int RT, int n_tiles, const double *__restrict__ u,
+    const double *__restrict__ logw, int R, const double *__restrict__ scale, int d0, int Nc, int use_scale,
+    const double *__restrict__ scalars, double *__restrict__ pval, double *__restrict__ tmax,
+    int *__restrict__ targ, int *__restrict__ err) {
+	extern __shared__ uint8_t dsm_raw[];
+	uint8_t *sm = (uint8_t *)(((uintptr_t)dsm_raw + 1023) & ~(uintptr_t)1023);
+	double *s_max = (double *)(sm + DSTAGES * DSTAGE_BYTES);
+	int *s_arg = (int *)(s_max + 4 * DN);
+	uint64_t *bars = (uint64_t *)(sm + DSTAGES * DSTAGE_BYTES + DEPI_BYTES);
+	uint64_t *full = bars, *empty = bars + DSTAGES, *accum = bars + 2 * DSTAGES;
+	uint32_t *tmem_slot = (uint32_t *)(bars + 2 * DSTAGES + 1);
+	volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	// grouped rasterisation of the (orientation tile, frame tile) grid
+	const int per_group = DGROUP * n_tiles;
+	const int grp = blockIdx.x / per_group, rem = blockIdx.x - grp * per_group;
+	const int rows = min(DGROUP, RT - grp * DGROUP);
+	const int rt = grp * DGROUP + rem % rows, nt = rem / rows;
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < DSTAGES; ++s) {
+			mbar_init(&full[s], 1);
+			mbar_init(&empty[s], 1);
+		}
+		mbar_init(accum, 1);
+		*abort_flag = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (warp == 1) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+		                 smem_addr(tmem_slot)),
+		             "r"(DN)
+		             : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = *tmem_slot;
+
+	if (warp == 0) {
+		if (lane == 0) {
+			int issued = 0;
+			for (int kb = 0; kb < num_kb; ++kb) {
+				const int s = kb % DSTAGES;
+				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
+				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u)) {
+					*abort_flag = 1;
+					atomicExch(err, 1);
+					break;
+				}
+				uint8_t *st = sm + s * DSTAGE_BYTES;
+				mbar_expect_tx(&full[s], DSTAGE_BYTES);
+				tma_load_2d(st, &map_hi, &full[s], kb * DK, rt * 128);
+				tma_load_2d(st + DA_BYTES, &map_lo, &full[s], kb * DK, rt * 128);
+				tma_load_2d(st + 2 * DA_BYTES, &map_cnt, &full[s], kb * DK, nt * DN);
+				issued = kb + 1;
+			}
+			// on a give-up, let the copies still in flight land before exiting
+			if (*abort_flag)
+				for (int kb = max(0, issued - DSTAGES); kb < issued; ++kb)
+					mbar_wait(&full[kb % DSTAGES], (uint32_t)(kb / DSTAGES) & 1u);
+		}
+		__syncwarp();
+	} else if (warp == 1) {
+		if (lane == 0) {
+			for (int kb = 0; kb < num_kb; ++kb) {
+				const int s = kb % DSTAGES;
+				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
+				if (*abort_flag || !mbar_wait(&full[s], ph)) {
+					*abort_flag = 1;
+					atomicExch(err, 1);
+					break;
+				}
+				tc_fence_after();
+				const uint32_t a_hi = smem_addr(sm + s * DSTAGE_BYTES);
+				const uint32_t a_lo = a_hi + DA_BYTES, b = a_hi + 2 * DA_BYTES;
+#pragma unroll
+				for (int k = 0; k < DK / 16; ++k) {
+					const uint64_t db = sw128_desc(b + 32 * k);
+					umma_bf16(tmem, sw128_desc(a_hi + 32 * k), db, (kb | k) != 0);
+					umma_bf16(tmem, sw128_desc(a_lo + 32 * k), db, 1u);
+				}
+				umma_commit(&empty[s]);
+			}
+			umma_commit(accum);
+		}
+		__syncwarp();
+	} else {
+		// epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+		const int q = warp & 3, i = q * 32 + lane, r = rt * 128 + i;
+		const bool valid_r = r < R;
+		const double lw = valid_r ? logw[r] : 0., ur = valid_r ? u[r] : 0.;
+		const bool ok = mbar_wait(accum, 0);
+		if (!ok) {
+			*abort_flag = 1;
+			atomicExch(err, 1);
+		}
+		tc_fence_after();
+		if (ok && !*abort_flag) {
+			for (int c = 0; c < DN / 16; ++c) {
+				float acc[16];
+				tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 16), acc);
+#pragma unroll
+				for (int j = 0; j < 16; ++j) {
+					const int col = c * 16 + j, dl = nt * DN + col;
+					double m = MAX_EXP_START;
+					int am = -1;
+					if (dl < Nc) {
+						const double sd = use_scale ? scale[d0 + dl] : scalars[0];
+						const double v = valid_r ? dadd(dsub(lw, dmul(ur, sd)), (double)acc[j]) : 0.;
+						pval[((size_t)rt * Nc + dl) * 128 + i] = v;
+						if (valid_r) {
+							m = v;
+							am = r;
+						}
+					}
+#pragma unroll
+					for (int o = 16; o > 0; o >>= 1) {
+						const double om = __shfl_xor_sync(FULL, m, o);
+						const int oa = __shfl_xor_sync(FULL, am, o);
+						if (om > m || (om == m && oa >= 0 && (am < 0 || oa < am))) {
+							m = om;
+							am = oa;
+						}
+					}
+					if (lane == 0) {
+						s_max[q * DN + col] = m;
+						s_arg[q * DN + col] = am;
+					}
+				}
+			}
+		}
+		asm volatile("bar.sync 1, 128;" ::: "memory");
+		if (ok && !*abort_flag) {
+			const int t = threadIdx.x - 64;
+			for (int col = t; col < DN; col += 128) {
+				const int dl = nt * DN + col;
+				if (dl >= Nc)
+					continue;
+				double m = MAX_EXP_START;
+				int am = -1;
+				for (int w = 0; w < 4; ++w) {  // lanes 0-31 first: lowest index wins ties
+					const double v = s_max[w * DN + col];
+					if (v > m) {
+						m = v;
+						am = s_arg[w * DN + col];
+					}
+				}
+				tmax[(size_t)rt * Nc + dl] = m;
+				targ[(size_t)rt * Nc + dl] = am;
+			}
+		}
+	}
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 1) {
+		tc_fence_after();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(DN) : "memory");
+	}
+}
+
+// hi / lo BF16 log-slices [R_pad][K_pad] (orientation rows, mask-0 pixels in
+// pixel order, zero past K) from the FP32 log-slice tiles [RT][P+1][TILE]:
+// x = hi + lo + O(2^-17 |x|), hi = bf16(x), lo = bf16(x - hi). A log of zero
+// (-inf) becomes -1e30 so that a zero count times it stays zero. Block = one
+// orientation tile x 64 pixels, transposed through shared memory.
+__global__ void __launch_bounds__(256) split_logw_kernel(const float *__restrict__ logW, int P,
+                                                         const int *__restrict__ kpix, int K, int K_pad,
+                                                         __nv_bfloat16 *__restrict__ hi,
+                                                         __nv_bfloat16 *__restrict__ lo) {
+	__shared__ float s[DK][128 + 1];
+	const int kb = blockIdx.x, rt = blockIdx.y, t = threadIdx.x;
+	for (int idx = t; idx < DK * 128; idx += 256) {
+		const int row = idx >> 7, col = idx & 127, k = kb * DK + row;
+		float v = 0.f;
+		if (k < K)
+			v = logW[((size_t)rt * (P + 1) + kpix[k]) * TILE + col];
+		s[row][col] = v;
+	}
+	__syncthreads();
+	for (int idx = t; idx < 128 * (DK / 8); idx += 256) {
+		const int col = idx >> 3, c8 = idx & 7;
+		__align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+		for (int e = 0; e < 8; ++e) {
+			float x = s[c8 * 8 + e][col];
+			x = fmaxf(x, -1e30f);
+			const __nv_bfloat16 xh = __float2bfloat16_rn(x);
+			h[e] = xh;
+			l[e] = __float2bfloat16_rn(x - __bfloat162float(xh));
+		}
+		const size_t o = ((size_t)rt * 128 + col) * K_pad + (size_t)kb * DK + c8 * 8;
+		*reinterpret_cast<uint4 *>(hi + o) = *reinterpret_cast<const uint4 *>(h);
+		*reinterpret_cast<uint4 *>(lo + o) = *reinterpret_cast<const uint4 *>(l);
+	}
+}
+
+// Counts of one frame chunk as BF16 rows [Nc_pad][K_pad] over the mask-0
+// pixels (the buffer is zeroed before): one warp per frame scatters its
+// E-step photon words (counts <= 256, one word per pixel).
+__global__ void densify_counts_kernel(const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
+                                      const long long *__restrict__ ph_mid, const int *__restrict__ pcol, int d0,
+                                      int Nc, int P, int K_pad, __nv_bfloat16 *__restrict__ cnt) {
+	const int dl = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+	if (dl >= Nc)
+		return;
+	const int d = d0 + dl;
+	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
+	for (long long j = beg + lane; j < end; j += 32) {
+		const uint32_t w = ph[j];
+		const uint32_t idx = j < mid ? w : (w & IDX_MASK);
+		if (idx >= (uint32_t)P)
+			continue;
+		const int k = pcol[idx];
+		if (k < 0)
+			continue;
+		const uint32_t c = j < mid ? 1u : (w >> IDX_BITS);
+		cnt[(size_t)dl * K_pad + k] = __float2bfloat16_rn((float)c);
+	}
+}
+
+}  // namespace dfg

@@ -1,0 +1,62 @@
+"""Dense (tensor-core) form of the E-step photon term against the sparse form
+and the FP64 oracle.
+
+The dense form computes sum_k count * logW as BF16 products of the hi / lo
+split of the log-slices (|x - hi - lo| <= 2^-17 |x|) with FP32 accumulation,
+so each log-likelihood carries an absolute error of order 1e-4 x the photon
+count; the bounds below state what that does to every reported result.
+"""
+import numpy as np
+import pytest
+
+from common import GPUEngine, load_case, rel_l2
+from oracle.oracle import EMCProblem, OracleEngine
+
+pytestmark = pytest.mark.gpu
+
+# measured on these cases: <= 5e-6 per photon, 8.5e-7, 6.3e-6, 1.0
+MAXEXP_ABS_PER_PHOTON = 2e-5   # |max_r pval| error per photon of the frame
+LL_REL = 5e-6                  # average log-likelihood
+MODEL_REL_L2 = 5e-5            # model after each iteration, against the oracle
+RMAX_AGREE = 0.999             # most likely orientation
+
+
+def _synth():
+    from dragonfly_b200 import synth
+    d = synth.small_problem(seed=21, det_side=48, size=41, qmax=19., n_atoms=120, atom_radius=7., num_div=4,
+                            n_frames=700, mean_count=300., hole_radius=3.)
+    return EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"], d["place_multi"],
+                      d["count_multi"], d["quats"], d["model_start"], beta=1.)
+
+
+@pytest.mark.parametrize("case", ["beta1", "scaling", "modes2", "synth300"])
+def test_dense_estep_matches_sparse_and_oracle(oracle_built, case):
+    prob = _synth() if case == "synth300" else load_case(case)[0]
+    sparse = GPUEngine(prob)
+    dense = GPUEngine(prob, estep_form=1)
+    orc = OracleEngine(prob)
+    mo = np.concatenate([[0], np.cumsum(prob.multi)])
+    cm = np.concatenate([[0], np.cumsum(prob.count_multi)])
+    photons = np.asarray(prob.ones, np.float64) + (cm[mo[1:]] - cm[mo[:-1]])
+    for it in (1, 2):
+        a = dense.run_iteration(it)
+        b = sparse.run_iteration(it)
+        o = orc.run_iteration(it)
+        good = np.asarray(b["rmax"]) >= 0
+        mx = np.abs(np.asarray(a["max_exp"]) - np.asarray(b["max_exp"]))[good]
+        per_photon = float((mx / np.maximum(photons[good], 1.)).max())
+        ll = abs(a["avg_likelihood"] - o["avg_likelihood"]) / abs(o["avg_likelihood"])
+        dev = rel_l2(a["model1"], o["model1"])
+        dev_sparse = rel_l2(b["model1"], o["model1"])
+        agree = float(np.mean(np.asarray(a["rmax"]) == np.asarray(o["rmax"])))
+        print("dense %s iteration %d: max_exp %.2e / photon, ll %.2e, model %.2e (sparse %.2e), rmax %.4f"
+              % (case, it, per_photon, ll, dev, dev_sparse, agree))
+        assert per_photon <= MAXEXP_ABS_PER_PHOTON, per_photon
+        assert ll <= LL_REL and dev <= MODEL_REL_L2 and agree >= RMAX_AGREE, (ll, dev, agree)
+        # both engines continue from the oracle's model, so the errors do not compound
+        for e in (dense, sparse):
+            e.ctx.set_model(o["model1"])
+            if prob.need_scaling:
+                e.ctx.set_scale(o["scale"])
+    for e in (dense, sparse):
+        e.close()
