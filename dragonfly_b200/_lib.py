@@ -67,6 +67,7 @@ _SIGS = {
     "dfg_set_model_type": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_run_iteration": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D]),
     "dfg_get_graph_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
+    "dfg_autotune": (C.c_int, [_V, C.POINTER(IterParams), _D]),
     "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
     "dfg_voronoi_subset": (C.c_int, [_V, C.c_int, _D, C.c_int, _D, _I]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
@@ -297,6 +298,16 @@ class Context:
         out = np.zeros(5)
         self.call("dfg_run_iteration", C.byref(par), float(alpha), ptr(out, C.c_double))
         return dict(zip(("avg_likelihood", "rms_change", "mutual_info", "rescale", "mean_scale"), out.tolist()))
+
+    def autotune(self, par):
+        """Times the slice blocks and both E-step forms on the current inputs
+        and keeps the fastest (used by later iterations with option
+        autotune). Returns the measurements and the choice."""
+        out = np.zeros(8)
+        self.call("dfg_autotune", C.byref(par), ptr(out, C.c_double))
+        return dict(slice_ms={b: out[i] for i, b in enumerate((128, 64, 32, 16)) if out[i] >= 0},
+                    estep_sparse_ms=out[4], estep_dense_ms=out[5] if out[5] >= 0 else None,
+                    slice_block=int(out[6]), estep_form=int(out[7]))
 
     def graph_stats(self):
         out = (C.c_long * 3)()

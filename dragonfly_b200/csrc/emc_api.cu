@@ -128,6 +128,8 @@ extern "C" int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, 
 		ctx->chunks_R = -1;
 	ctx->P = num_pix;
 	ctx->h_mask.assign(raw_mask, raw_mask + num_pix);
+	ctx->tuned = false;
+	ctx->dense_P = -1;  // pixel columns of the dense form follow the mask
 	CK(upload(ctx->qvals, qvals, 3 * (size_t)num_pix, ctx->stream));
 	CK(upload(ctx->corr, corr, (size_t)num_pix, ctx->stream));
 	CK(upload(ctx->mask, raw_mask, (size_t)num_pix, ctx->stream));
@@ -256,6 +258,7 @@ extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const
 	ctx->have_results = false;
 	ctx->refine = false;  // relevant orientations are per frame
 	ctx->max_count0 = -1;
+	ctx->tuned = false;
 	return DFG_OK;
 }
 
@@ -267,8 +270,10 @@ extern "C" int dfg_set_quaternions(dfg_ctx *ctx, int num_rot, const double *quat
 		NEED(std::isfinite(quats[i]), DFG_ERR_ARG, "quaternions: entry %lld is not finite", i);
 	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
-	if (num_rot != ctx->num_rot)
+	if (num_rot != ctx->num_rot) {
 		ctx->refine = false;  // the coarse map was made for the previous set
+		ctx->tuned = false;
+	}
 	ctx->num_rot = num_rot;
 	CK(upload(ctx->quats, quats, 5 * (size_t)num_rot, ctx->stream));
 	std::vector<double> cs(2 * (size_t)num_rot);
@@ -288,6 +293,8 @@ extern "C" int dfg_set_model(dfg_ctx *ctx, long size, int num_modes, const doubl
 	NEED(num_modes <= MAX_MODES, DFG_ERR_ARG, "model: at most %d modes", MAX_MODES);
 	ctx->weight_cache_valid = false;
 	CK(cudaSetDevice(ctx->device));
+	if (size != ctx->S || num_modes != ctx->M)
+		ctx->tuned = false;
 	ctx->S = size;
 	ctx->V = ctx->model_type == MT_3D ? (long long)size * size * size : (long long)size * size;
 	ctx->M = num_modes;
@@ -962,6 +969,8 @@ static void dense_release(dfg_ctx *ctx) {
 	ctx->map_src[0] = ctx->map_src[1] = ctx->map_src[2] = nullptr;
 }
 
+static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par);
+
 // The part of maximize that allocates, uploads or checks on the host, done
 // before any of its kernels is queued (so that the queued part can be
 // captured into a CUDA graph).
@@ -970,10 +979,14 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 		return DFG_ERR_ARG;
 	NEED(par->beta_period > 0, DFG_ERR_ARG, "beta_period must be > 0");
 	CK(cudaSetDevice(ctx->device));
-	// E-step form: dense tensor-core products (option estep_form 1) where
-	// the inputs allow it
+	// E-step form: dense tensor-core products (option estep_form 1, or the
+	// autotuner's choice) where the inputs allow it
+	if (ctx->autotune && !ctx->tuned && !ctx->tuning)
+		if (int rc = run_autotune(ctx, par))
+			return rc;
+	const int form = ctx->tuning ? ctx->tune_form : (ctx->autotune ? ctx->tuned_form : ctx->estep_form);
 	ctx->dense_active = false;
-	if (ctx->estep_form == 1) {
+	if (form == 1) {
 		NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0, DFG_ERR_STATE, "set detector, frames and quaternions");
 		const char *why = dense_refusal(ctx, par);
 		NEED(why == nullptr, DFG_ERR_ARG, "%s", why);
@@ -1032,6 +1045,95 @@ static bool graphable(const dfg_ctx *ctx, const dfg_iter_params *par) {
 	return !ctx->keep_prob && !(ctx->with_bg && par->need_scaling && par->update_scale);
 }
 
+// Orientations per slice block: the option, else whole tiles when they give
+// every SM two blocks, else the largest block that does (16 at least).
+static int slice_block_for(const dfg_ctx *ctx) {
+	int ob = (ctx->autotune && ctx->tuned && !ctx->tuning) ? ctx->tuned_ob : ctx->slice_block;
+	if (ob == 0) {
+		ob = 16;
+		for (int c : {TILE, 64, 32})
+			if (c <= TILE && ctx->R_pad / c >= 2 * ctx->num_sms) {
+				ob = c;
+				break;
+			}
+	}
+	return ob;
+}
+
+// Slices of every orientation with ob orientations per block: log W tiles (or
+// W in FP64 into Wd) and u_r.
+static int launch_slices(dfg_ctx *ctx, int ob, double *Wd) {
+	cudaStream_t st = ctx->stream;
+	const int M = ctx->M, R = ctx->R, RT = ctx->RT, P = ctx->P;
+	const long long S = ctx->S, V = ctx->V;
+	const int nb = ctx->R_pad / ob;
+	// orientation parameters: quaternions (3-D) or (cos, sin) of the angles (2-D)
+	const double *geo = ctx->model_type == MT_2D ? ctx->cs2d.p : ctx->quats.p;
+#define DFG_SLICE(OBV, G)                                                                                     \
+	slice_u_kernel<double, OBV, G><<<nb, 256, 0, st>>>(geo, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,     \
+	                                                   ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd)
+#define DFG_SLICE_ALL(G)                                                                                      \
+	if (ob == TILE)                                                                                           \
+		slice_u_tile_kernel<double, G><<<RT, 256, 0, st>>>(geo, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, \
+		                                                   ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd);     \
+	else if (ob == 64)                                                                                        \
+		DFG_SLICE(TILE >= 64 ? 64 : 16, G);                                                                   \
+	else if (ob == 32)                                                                                        \
+		DFG_SLICE(32, G);                                                                                     \
+	else                                                                                                      \
+		DFG_SLICE(16, G)
+	if (ctx->model_type == MT_2D) {
+		DFG_SLICE_ALL(MT_2D);
+	} else {
+		DFG_SLICE_ALL(MT_3D);
+	}
+#undef DFG_SLICE_ALL
+#undef DFG_SLICE
+	CKL("slice_u_kernel");
+	return DFG_OK;
+}
+
+// The E-step of one frame chunk: the tensor-core products (dense: counts
+// densified first) or the sparse gathers (background-aware with bg).
+static int launch_estep(dfg_ctx *ctx, const Chunk &ch, int use_scale, bool bg, const RefineMask &rm, bool dense) {
+	cudaStream_t st = ctx->stream;
+	const int Nc = ch.nc, P = ctx->P, R = ctx->R, RT = ctx->RT;
+	if (dense) {
+		CK(cudaMemsetAsync(ctx->cnt.p, 0, (size_t)ctx->cnt_rows * ctx->K_pad * 2, st));
+		densify_counts_kernel<<<blocks_for((long long)Nc * 32, 256), 256, 0, st>>>(
+		    ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->pcol.p, ch.d0, Nc, P, ctx->K_pad,
+		    (__nv_bfloat16 *)ctx->cnt.p);
+		CKL("densify_counts_kernel");
+		const int n_tiles = (Nc + DN - 1) / DN;
+		estep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
+		    ctx->map_hi, ctx->map_lo, ctx->map_cnt, ctx->K_pad / DK, RT, n_tiles, ctx->u.p, ctx->logw.p, R,
+		    ctx->scale.p, ch.d0, Nc, use_scale, ctx->scalars.p, ctx->pval.p, ctx->tmax.p, ctx->targ.p,
+		    ctx->derr.p);
+		CKL("estep_dense_kernel");
+		return DFG_OK;
+	}
+	const long long warps = (long long)RT * Nc;
+	if (bg) {
+		estep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
+		    ctx->Wd.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
+		    ctx->bgscale.p, ctx->background.p, ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT,
+		    ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm);
+		CKL("estep_bg_kernel");
+		return DFG_OK;
+	}
+#define DFG_ESTEP(REF)                                                                                        \
+	estep_kernel<REF><<<blocks_for(warps, 8), 256, 0, st>>>(                                                  \
+	    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,          \
+	    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm)
+	if (rm.qmap != nullptr)
+		DFG_ESTEP(true);
+	else
+		DFG_ESTEP(false);
+#undef DFG_ESTEP
+	CKL("estep_kernel");
+	return DFG_OK;
+}
+
 // Queues maximize's kernels (after max_prepare). Synchronises only where
 // graphable() is false.
 static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
@@ -1056,43 +1158,8 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 
 	// slices, u_r, rescale (calculate_rescale, max_prob.c:3-64)
 	phase_begin(ctx, PH_SLICE);
-	{
-		// whole tiles when they give every SM two blocks; else the largest
-		// orientation block that does (16 at least)
-		int ob = ctx->slice_block;
-		if (ob == 0) {
-			ob = 16;
-			for (int c : {TILE, 64, 32})
-				if (c <= TILE && R_pad / c >= 2 * ctx->num_sms) {
-					ob = c;
-					break;
-				}
-		}
-		const int nb = R_pad / ob;
-		// orientation parameters: quaternions (3-D) or (cos, sin) of the angles (2-D)
-		const double *geo = two_d ? ctx->cs2d.p : ctx->quats.p;
-#define DFG_SLICE(OBV, G)                                                                                     \
-	slice_u_kernel<double, OBV, G><<<nb, 256, 0, st>>>(geo, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,     \
-	                                                   ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd)
-#define DFG_SLICE_ALL(G)                                                                                      \
-	if (ob == TILE)                                                                                           \
-		slice_u_tile_kernel<double, G><<<RT, 256, 0, st>>>(geo, M, R, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, \
-		                                                   ctx->model1.p, S, V, ctx->logW.p, ctx->u.p, Wd);     \
-	else if (ob == 64)                                                                                        \
-		DFG_SLICE(TILE >= 64 ? 64 : 16, G);                                                                   \
-	else if (ob == 32)                                                                                        \
-		DFG_SLICE(32, G);                                                                                     \
-	else                                                                                                      \
-		DFG_SLICE(16, G)
-		if (two_d) {
-			DFG_SLICE_ALL(MT_2D);
-		} else {
-			DFG_SLICE_ALL(MT_3D);
-		}
-#undef DFG_SLICE_ALL
-#undef DFG_SLICE
-		CKL("slice_u_kernel");
-	}
+	if (int rc = launch_slices(ctx, slice_block_for(ctx), Wd))
+		return rc;
 	rescale_kernel<<<1, 256, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
 	CKL("rescale_kernel");
 	logw_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->quats.p, M, R, ctx->logw.p);
@@ -1121,40 +1188,8 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 		const int Nc = ch.nc;
 		// E-step (calculate_prob, max_prob.c:66-213)
 		phase_begin(ctx, PH_ESTEP);
-		if (ctx->dense_active) {
-			// counts as BF16 rows, then the tensor-core products
-			CK(cudaMemsetAsync(ctx->cnt.p, 0, (size_t)ctx->cnt_rows * ctx->K_pad * 2, st));
-			densify_counts_kernel<<<blocks_for((long long)Nc * 32, 256), 256, 0, st>>>(
-			    ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->pcol.p, ch.d0, Nc, P, ctx->K_pad,
-			    (__nv_bfloat16 *)ctx->cnt.p);
-			CKL("densify_counts_kernel");
-			const int n_tiles = (Nc + DN - 1) / DN;
-			estep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
-			    ctx->map_hi, ctx->map_lo, ctx->map_cnt, ctx->K_pad / DK, RT, n_tiles, ctx->u.p, ctx->logw.p, R,
-			    ctx->scale.p, ch.d0, Nc, use_scale, ctx->scalars.p, ctx->pval.p, ctx->tmax.p, ctx->targ.p,
-			    ctx->derr.p);
-			CKL("estep_dense_kernel");
-		} else {
-			long long warps = (long long)RT * Nc;
-			if (bg) {
-				estep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
-				    ctx->Wd.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
-				    ctx->bgscale.p, ctx->background.p, ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT,
-				    ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm);
-				CKL("estep_bg_kernel");
-			} else {
-#define DFG_ESTEP(REF)                                                                                        \
-	estep_kernel<REF><<<blocks_for(warps, 8), 256, 0, st>>>(                                                  \
-	    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,          \
-	    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm)
-				if (rm.qmap != nullptr)
-					DFG_ESTEP(true);
-				else
-					DFG_ESTEP(false);
-#undef DFG_ESTEP
-				CKL("estep_kernel");
-			}
-		}
+		if (int rc = launch_estep(ctx, ch, use_scale, bg, rm, ctx->dense_active))
+			return rc;
 		phase_end(ctx, PH_ESTEP, ctx->dense_active ? 2 : 1);
 		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
 		phase_begin(ctx, PH_NORM);
@@ -1254,6 +1289,107 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 	}
 	phase_end(ctx, PH_UPDATE, par->need_scaling && par->update_scale ? 3 : 2);
 	ctx->views_final = bg;
+	return DFG_OK;
+}
+
+// Project autotuner. On the context's own inputs it times (CUDA events, best
+// of two) the slice kernel with 128, 64, 32 and 16 orientations per block and
+// both forms of the E-step photon term (sparse gathers, dense tensor-core
+// products where the inputs allow them) on the first frame chunk, and keeps
+// the fastest of each. tune_report: slice ms per block size (-1 if not
+// tried), sparse and dense E-step ms (-1 if refused), the chosen block and
+// form.
+static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
+	NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0 && ctx->S > 0, DFG_ERR_STATE,
+	     "autotune: set detector, frames, quaternions and model first");
+	double rep[8] = {-1., -1., -1., -1., -1., -1., -1., -1.};
+	const bool dense_ok = dense_refusal(ctx, par) == nullptr;
+	const bool save_timing = ctx->timing;
+	ctx->timing = false;
+	ctx->tuning = true;
+	ctx->tune_form = dense_ok ? 1 : 0;
+	int rc = max_prepare(ctx, par);
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	if (rc == DFG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+		rc = ctx->fail(DFG_ERR_CUDA, "autotune: cudaEventCreate failed");
+	cudaStream_t st = ctx->stream;
+	auto timed = [&](auto &&launch, double &out) -> int {
+		float best = 1e30f;
+		for (int k = 0; k < 2; ++k) {
+			CK(cudaEventRecord(e0, st));
+			if (int r = launch())
+				return r;
+			CK(cudaEventRecord(e1, st));
+			CK(cudaEventSynchronize(e1));
+			float ms = 0.f;
+			CK(cudaEventElapsedTime(&ms, e0, e1));
+			best = std::min(best, ms);
+		}
+		out = best;
+		return DFG_OK;
+	};
+	const bool bg = ctx->with_bg && par->need_scaling;
+	double *const Wd = bg ? ctx->Wd.p : nullptr;
+	const RefineMask rm = ctx->refine ? RefineMask{ctx->qmap.p, ctx->rel_bits.p, ctx->rwords}
+	                                  : RefineMask{nullptr, nullptr, 0};
+	const int obs[4] = {128, 64, 32, 16};
+	int bi = -1;
+	for (int i = 0; i < 4 && rc == DFG_OK; ++i) {
+		const int ob = obs[i];
+		if (ob > TILE || TILE % ob != 0)
+			continue;
+		rc = timed([&] { return launch_slices(ctx, ob, Wd); }, rep[i]);
+		if (rc == DFG_OK && (bi < 0 || rep[i] < rep[bi]))
+			bi = i;
+	}
+	const int best_ob = bi >= 0 ? obs[bi] : 0;
+	const int use_scale = par->need_scaling && (par->iteration > 1 || par->known_scale);
+	if (rc == DFG_OK) {
+		// the E-step's other inputs
+		rescale_kernel<<<1, 256, 0, st>>>(ctx->u.p, ctx->quats.p, ctx->M, ctx->R, ctx->mean_count, ctx->scalars.p);
+		CKL("rescale_kernel");
+		logw_kernel<<<blocks_for(ctx->R, 256), 256, 0, st>>>(ctx->quats.p, ctx->M, ctx->R, ctx->logw.p);
+		CKL("logw_kernel");
+		rc = timed([&] { return launch_estep(ctx, ctx->chunks[0], use_scale, bg, rm, false); }, rep[4]);
+	}
+	if (rc == DFG_OK && dense_ok) {
+		split_logw_kernel<<<dim3(ctx->K_pad / DK, ctx->RT), 256, 0, st>>>(
+		    ctx->logW.p, ctx->P, ctx->kpix.p, ctx->K, ctx->K_pad, (__nv_bfloat16 *)ctx->Ahi.p,
+		    (__nv_bfloat16 *)ctx->Alo.p);
+		CKL("split_logw_kernel");
+		rc = timed([&] { return launch_estep(ctx, ctx->chunks[0], use_scale, bg, rm, true); }, rep[5]);
+		int derr = 0;
+		if (rc == DFG_OK) {
+			CK(cudaMemcpy(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+			if (derr)
+				rc = ctx->fail(DFG_ERR_CUDA, "autotune: the dense E-step gave up");
+		}
+	}
+	if (e0)
+		cudaEventDestroy(e0);
+	if (e1)
+		cudaEventDestroy(e1);
+	ctx->tuning = false;
+	ctx->timing = save_timing;
+	if (rc != DFG_OK)
+		return rc;
+	ctx->tuned_ob = best_ob;
+	ctx->tuned_form = (dense_ok && rep[5] >= 0. && rep[5] < rep[4]) ? 1 : 0;
+	ctx->tuned = true;
+	rep[6] = best_ob;
+	rep[7] = ctx->tuned_form;
+	std::copy(rep, rep + 8, ctx->tune_report);
+	return DFG_OK;
+}
+
+extern "C" int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *report) {
+	if (!ctx || !par)
+		return DFG_ERR_ARG;
+	CK(cudaSetDevice(ctx->device));
+	if (int rc = run_autotune(ctx, par))
+		return rc;
+	if (report)
+		std::copy(ctx->tune_report, ctx->tune_report + 8, report);
 	return DFG_OK;
 }
 
@@ -1873,6 +2009,10 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 	}
 	if (!strcmp(key, "graph")) {
 		ctx->use_graph = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "autotune")) {
+		ctx->autotune = value != 0.;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "estep_form")) {

@@ -172,6 +172,11 @@ struct dfg_ctx {
 	// kernel's give-up flag
 	int estep_form = 0;
 	bool dense_active = false, chunks_dense = false;
+	// autotuner (option autotune): the slice block and E-step form it chose
+	// for the current inputs; tuning / tune_form while it measures
+	bool autotune = false, tuned = false, tuning = false;
+	int tuned_ob = 0, tuned_form = 0, tune_form = 0;
+	double tune_report[8] = {};
 	int K = 0, K_pad = 0, dense_P = -1, cnt_rows = 0;
 	int max_count0 = -1;  // largest count on a mask-0 pixel; -1 = not known
 	DevBuf<int> kpix, pcol, derr;

@@ -235,6 +235,16 @@ DFG_API int dfg_slice_gen_noalloc(dfg_ctx *ctx, const double *quat, int mode, do
  * later iterations update that graph in place. */
 DFG_API int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double alpha, double *out);
 
+/* Autotuner: on the context's current inputs, times the slice kernel with
+ * 128, 64, 32 and 16 orientations per block and the E-step photon term in its
+ * sparse (gathers) and dense (tensor-core) forms on the first frame chunk, and
+ * keeps the fastest of each for later iterations when option autotune is 1
+ * (with option autotune, dfg_maximize / dfg_run_iteration tune by themselves
+ * whenever the inputs changed). report[8] (may be NULL): slice ms per block
+ * size (-1: not tried), sparse and dense E-step ms (-1: form refused), the
+ * chosen block and form (0 sparse, 1 dense). */
+DFG_API int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *report);
+
 /* Graph use of dfg_run_iteration: out[0] = graph launches, out[1] =
  * instantiations, out[2] = in-place updates. */
 DFG_API int dfg_get_graph_stats(dfg_ctx *ctx, long *out);

@@ -60,3 +60,28 @@ def test_dense_estep_matches_sparse_and_oracle(oracle_built, case):
                 e.ctx.set_scale(o["scale"])
     for e in (dense, sparse):
         e.close()
+
+
+@pytest.mark.parametrize("case", ["scaling", "synth300"])
+def test_autotuner_times_both_forms_and_keeps_the_fastest(oracle_built, case):
+    prob = _synth() if case == "synth300" else load_case(case)[0]
+    tuned = GPUEngine(prob, autotune=1)
+    c = tuned.ctx
+    par = c.params(1, prob.need_scaling, prob.update_scale, prob.known_scale, prob.beta_jump, prob.beta_period,
+                   prob.beta_factor)
+    rep = c.autotune(par)
+    print("autotune %s:" % case, rep)
+    assert set(rep["slice_ms"]) == {128, 64, 32, 16} and all(v > 0 for v in rep["slice_ms"].values())
+    assert rep["slice_block"] == min(rep["slice_ms"], key=rep["slice_ms"].get)
+    assert rep["estep_sparse_ms"] > 0 and rep["estep_dense_ms"] is not None and rep["estep_dense_ms"] > 0
+    assert rep["estep_form"] == int(rep["estep_dense_ms"] < rep["estep_sparse_ms"])
+    # iterations with the tuned choice agree with the plain sparse form
+    plain = GPUEngine(prob)
+    orc = OracleEngine(prob)
+    for it in (1, 2):
+        a = tuned.run_iteration(it)
+        b = orc.run_iteration(it)
+        assert rel_l2(a["model1"], b["model1"]) <= MODEL_REL_L2
+        assert np.mean(np.asarray(a["rmax"]) == np.asarray(b["rmax"])) >= RMAX_AGREE
+    tuned.close()
+    plain.close()
