@@ -129,6 +129,16 @@ def measured_peaks():
 TRAFFIC_FRACTIONS = {"estep": (0.85, 0.97), "mstep": (0.85, 0.72)}
 
 
+def measured_tensor_peak():
+    """Measured sustained dense BF16 rate (TFLOP/s) for a kernel timed inside a
+    long step, else the fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops_sustained"]), "of measured (sustained)"
+    except (OSError, KeyError, ValueError):
+        return 1400., "of fallback (sustained)"
+
+
 def roofline_traffic(kernel, R_pad, P, Nc):
     """Modelled DRAM bytes of one launch of `kernel` (None for other kernels)."""
     if kernel == "estep":
@@ -221,6 +231,14 @@ def run_ours(args, rank, world, local_rank):
         w["n_frames"] = args.frames
     if args.num_div:
         w["num_div"] = args.num_div
+    if args.median_photons > 0:
+        w["median_photons"] = args.median_photons
+    if args.fluence_sigma >= 0:
+        w["fluence_sigma"] = args.fluence_sigma
+    if w != WORKLOAD:
+        w["name"] = ("plain EMC: 260x257 pnCCD-like detector, 201^3 model, num_div %d, %d frames, median %g "
+                     "photons (sigma %g), scale update, beta 0.01 x sqrt2 / 5"
+                     % (w["num_div"], w["n_frames"], w["median_photons"], w["fluence_sigma"]))
     t_setup = time.perf_counter()
     inp = build_inputs(w)
     ctx = Context(local_rank)
@@ -233,9 +251,14 @@ def run_ours(args, rank, world, local_rank):
     N = w["n_frames"]
     # the library's autotuner picks the slice block and the E-step form
     # (sparse gathers or tensor-core products) on these inputs, before timing
-    ctx.set_option("autotune", 1)
-    tune = ctx.autotune(ctx.params(1, need_scaling=1, update_scale=1, beta_jump=w["beta_jump"],
-                                   beta_period=w["beta_period"]))
+    tpar = ctx.params(1, need_scaling=1, update_scale=1, beta_jump=w["beta_jump"], beta_period=w["beta_period"])
+    tune = ctx.autotune(tpar)
+    if args.estep_form == "auto":
+        ctx.set_option("autotune", 1)
+    else:
+        ctx.set_option("slice_block", tune["slice_block"])
+        ctx.set_option("estep_form", 1 if args.estep_form == "dense" else 0)
+        tune["estep_form"] = 1 if args.estep_form == "dense" else 0
     setup_s = time.perf_counter() - t_setup
 
     def params(it):
@@ -311,12 +334,22 @@ def run_ours(args, rank, world, local_rank):
         "update": 8. * inp["start"].size,
     }
     per_launch_s = (ms / 1e3) / max(nl, 1)
-    achieved = algo[dom] / per_launch_s / 1e9
-    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_src,
-            "traffic": roofline_traffic(dom, -(-R // 128) * 128, inp["qvals"].shape[0], wl["chunk_frames"]),
-            "traffic_note": "modelled from ncu DRAM bytes of a small capture (compulsory streams)",
-            "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
+    if dom == "estep" and wl["dense_estep"]:
+        # tensor-core E-step: 2 x R_pad x frames x K_pad x 2 (hi, lo) FLOP per
+        # chunk over the phase time per chunk (densification included)
+        tpeak, tsrc = measured_tensor_peak()
+        flop = 2. * (-(-R // 128) * 128) * wl["chunk_frames"] * wl["k_pad"] * 2
+        achieved = flop / ((ms / 1e3) / (args.steps * chunks)) / 1e12
+        roof = {"kernel": "estep (dense, tensor cores)", "bound": "tensor", "achieved": achieved, "peak": tpeak,
+                "unit": "TFLOP/s", "frac": achieved / tpeak, "peak_source": tsrc, "traffic": None,
+                "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
+    else:
+        achieved = algo[dom] / per_launch_s / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": roofline_traffic(dom, -(-R // 128) * 128, inp["qvals"].shape[0], wl["chunk_frames"]),
+                "traffic_note": "modelled from ncu DRAM bytes of a small capture (compulsory streams)",
+                "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -354,6 +387,10 @@ def main():
     ap.add_argument("--frames", type=int, default=0, help="override the frame count (testing)")
     ap.add_argument("--num-div", type=int, default=0, help="override num_div (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--median-photons", type=float, default=0., help="override the median photons per frame")
+    ap.add_argument("--fluence-sigma", type=float, default=-1., help="override the lognormal fluence sigma")
+    ap.add_argument("--estep-form", default="auto", choices=["auto", "sparse", "dense"],
+                    help="E-step photon term: autotuned (default), sparse gathers or tensor-core products")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -455,8 +455,8 @@ class Context:
         return ms.value
 
     def workload(self):
-        out = (C.c_longlong * 7)()
+        out = (C.c_longlong * 9)()
         self.call("dfg_get_workload", out)
         keys = ("num_orient", "num_data", "estep_entries", "mstep_entries", "chunks", "chunk_frames",
-                "launches")
+                "launches", "k_pad", "dense_estep")
         return dict(zip(keys, list(out)))

@@ -297,7 +297,9 @@ DFG_API int dfg_reset_phase_times(dfg_ctx *ctx);
 /* Sizes of the last iteration: out[0] = R (modes * num_rot), out[1] = frames,
  * out[2] = photon entries in the E-step lists, out[3] = M-step entries,
  * out[4] = frame chunks, out[5] = frames per chunk, out[6] = kernels launched
- * by this context so far. */
+ * by this context so far, out[7] = mask-0 pixel columns of the dense form
+ * (padded to 64; 0 before it is used), out[8] = 1 when the last iteration's
+ * E-step took the dense form. out must hold 9 values. */
 DFG_API int dfg_get_workload(dfg_ctx *ctx, long long *out);
 
 #ifdef __cplusplus
