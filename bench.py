@@ -378,6 +378,137 @@ def run_ours(args, rank, world, local_rank):
     return out, inp, w
 
 
+# ---------------------------------------------------------------------------
+# batched form: several reconstructions iterated together
+# ---------------------------------------------------------------------------
+# independent reconstructions: (model size, frames, num_div, median photons)
+BATCH_RECONS = [(51, 5000, 4, 50.), (65, 10000, 5, 100.), (81, 20000, 6, 150.), (95, 40000, 7, 200.),
+                (111, 80000, 8, 300.), (125, 60000, 6, 400.), (141, 30000, 5, 500.), (151, 15000, 4, 250.)]
+# four heterogeneous modes: a shared 1000-atom density with a 50-atom domain
+# shifted by 0, 2, 4 and 6 voxels; frames mixed 4:3:2:1
+BATCH_MODES = dict(size=125, atoms=1000, domain=50, shifts=(0, 2, 4, 6), frames=300000, mix=(4, 3, 2, 1),
+                   median=200., num_div=6)
+
+
+def _intensity(pos, size, sigma=1.0):
+    rho = np.zeros((size, size, size))
+    idx = np.rint(pos).astype(np.int64) % size
+    np.add.at(rho, (idx[:, 0], idx[:, 1], idx[:, 2]), 1.0)
+    f = np.fft.fftn(rho)
+    k = np.fft.fftfreq(size)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    f *= np.exp(-2. * np.pi ** 2 * sigma ** 2 * k2)
+    return np.fft.fftshift(np.abs(f) ** 2)
+
+
+def _batch_context(Context, device, size, num_div, models, frame_sets, budget_mb, seed):
+    """One reconstruction: flat size x size detector (edge |q| = (size - 3) / 2),
+    num_div orientations, frames simulated from models (one per mode, mode m
+    for frame_sets[m] frames) at lognormal fluence."""
+    from dragonfly_b200 import synth
+    from dragonfly_b200.quatgen import quat_gen
+    rng = np.random.default_rng(seed)
+    qmax = (size - 3) / 2.
+    qvals, corr, mask, _, _ = synth.flat_detector(size, size, qmax, size, hole_radius=size / 25.)
+    ctx = Context(device)
+    ctx.set_option("pair_budget_mb", budget_mb)
+    ctx.set_option("autotune", 1)
+    ctx.set_detector(qvals, corr, mask)
+    parts = []
+    for m, (intens, (n, median)) in enumerate(zip(models, frame_sets)):
+        intens = intens * (median / synth.model_mean_count(intens, qvals, corr, mask, rng, n_orient=32))
+        ctx.simulate_frames(intens, synth.random_quaternions(n, rng), np.exp(rng.normal(0., 0.3, n)), seed + m)
+        parts.append(ctx.get_frames())
+    if len(parts) > 1:
+        cat = [np.concatenate([p[k] for p in parts]) for k in range(5)]
+        ctx.set_frames(*cat)
+    quats = quat_gen(num_div)
+    ctx.set_quaternions(quats)
+    M = len(models)
+    ctx.set_model(rng.random((M, size, size, size)) * frame_sets[0][1] / (mask == 0).sum() * 2.)
+    ctx.calc_beta(0.01, 1)
+    n = sum(f[0] for f in frame_sets)
+    return ctx, M * quats.shape[0] * n
+
+
+def run_batched(args):
+    """The batched workload: the four-mode reconstruction and the eight
+    independent ones, one iteration each, as one batched graph launch
+    (dfg_batch_run) against the same iterations one reconstruction after
+    another (each its own graph); both timed on the device over the same
+    contexts. Prints one JSON line."""
+    from dragonfly_b200._lib import Batch, Context
+    from dragonfly_b200 import synth
+    import torch
+    rng = np.random.default_rng(4321)
+    t0 = time.perf_counter()
+    ctxs, pairs = [], []
+    B = BATCH_MODES
+    base = synth.atom_positions(B["atoms"], 0.15 * B["size"], rng)
+    dom = synth.atom_positions(B["domain"], 0.05 * B["size"], rng) + np.array([0.08 * B["size"], 0., 0.])
+    models = [_intensity(np.concatenate([base, dom + np.array([s, 0., 0.])]), B["size"]) for s in B["shifts"]]
+    tot = sum(B["mix"])
+    sets = [(B["frames"] * k // tot, B["median"]) for k in B["mix"]]
+    c, n = _batch_context(Context, 0, B["size"], B["num_div"], models, sets, 40000., 100)
+    ctxs.append(c)
+    pairs.append(n)
+    for i, (size, frames, nd, median) in enumerate(BATCH_RECONS):
+        intens = synth.gaussian_atom_intensity(1000, 0.15 * size, size, rng)
+        c, n = _batch_context(Context, 0, size, nd, [intens], [(frames, median)], 12000., 200 + i)
+        ctxs.append(c)
+        pairs.append(n)
+    setup_s = time.perf_counter() - t0
+    par = lambda c, it: c.params(it, need_scaling=1, update_scale=1, beta_jump=math.sqrt(2.), beta_period=5)
+    batch = Batch(ctxs)
+    it = 1
+    for _ in range(args.warmup):            # tunes every context, builds the graphs
+        batch.run([par(c, it) for c in ctxs])
+        for c in ctxs:
+            c.run_iteration(par(c, it), 0.)
+        it += 1
+    timer = ctxs[0]
+    torch.cuda.synchronize()
+    seq_ms, lane_ms = [], {1: [], len(ctxs): []}
+    for _ in range(args.steps):
+        timer.event_record(0)
+        for c in ctxs:
+            c.run_iteration(par(c, it), 0.)
+        timer.event_record(1)
+        seq_ms.append(timer.event_elapsed_ms(0, 1))
+        it += 1
+        for lanes in lane_ms:
+            batch.set_lanes(lanes)
+            timer.event_record(2)
+            batch.run([par(c, it) for c in ctxs])
+            timer.event_record(3)
+            lane_ms[lanes].append(timer.event_elapsed_ms(2, 3))
+            it += 1
+    total = float(sum(pairs))
+    seq = float(np.mean(seq_ms))
+    lane_mean = {k: float(np.mean(v)) for k, v in lane_ms.items()}
+    best_lanes = min(lane_mean, key=lane_mean.get)
+    bat = lane_mean[best_lanes]
+    out = {"metric": "frame x orientation pairs per second, batched reconstructions", "value": total / (bat / 1e3),
+           "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": bat,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 accumulate / f32 log-slices",
+           "data": "synthetic (seeded; frames simulated on the GPU)",
+           "config": {"workload": "batched: 4-mode 125^3 (shared 1000-atom density, 50-atom domain shifted 0/2/4/6 "
+                                  "voxels), 300000 frames mixed 4:3:2:1 at median 200, num_div 6; plus 8 independent "
+                                  "reconstructions " + ", ".join("%d^3/%d frames/num_div %d/median %g" % r
+                                                                for r in BATCH_RECONS),
+                      "pairs_per_step": total, "setup_s": setup_s,
+                      "autotuned": [c.tune_report() for c in ctxs]},
+           "sequential": {"ms_per_step": seq, "value": total / (seq / 1e3)},
+           "batch_lanes": {str(k): {"ms_per_step": v, "value": total / (v / 1e3)} for k, v in lane_mean.items()},
+           "lanes": best_lanes,
+           "speedup_vs_sequential": seq / bat,
+           "batch_graph": batch.stats()}
+    print(json.dumps(out))
+    batch.close()
+    for c in ctxs:
+        c.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -391,6 +522,9 @@ def main():
     ap.add_argument("--fluence-sigma", type=float, default=-1., help="override the lognormal fluence sigma")
     ap.add_argument("--estep-form", default="auto", choices=["auto", "sparse", "dense"],
                     help="E-step photon term: autotuned (default), sparse gathers or tensor-core products")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+                    help="plain: the production-size iteration (default); batched: nine reconstructions "
+                         "iterated together against one after another")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
@@ -398,6 +532,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "batched":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the batched workload has no counterpart in "
+                                  "the reference (one reconstruction per process)"}))
+            return
+        if rank == 0:
+            run_batched(args)
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -68,6 +68,13 @@ _SIGS = {
     "dfg_run_iteration": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D]),
     "dfg_get_graph_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
     "dfg_autotune": (C.c_int, [_V, C.POINTER(IterParams), _D]),
+    "dfg_get_autotune_report": (C.c_int, [_V, _D]),
+    "dfg_batch_create": (C.c_int, [C.POINTER(_V), C.c_int, C.POINTER(_V)]),
+    "dfg_batch_run": (C.c_int, [_V, C.POINTER(IterParams), _D, _D]),
+    "dfg_batch_last_error": (C.c_char_p, [_V]),
+    "dfg_batch_set_lanes": (C.c_int, [_V, C.c_int]),
+    "dfg_batch_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
+    "dfg_batch_destroy": (None, [_V]),
     "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
     "dfg_voronoi_subset": (C.c_int, [_V, C.c_int, _D, C.c_int, _D, _I]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
@@ -299,15 +306,26 @@ class Context:
         self.call("dfg_run_iteration", C.byref(par), float(alpha), ptr(out, C.c_double))
         return dict(zip(("avg_likelihood", "rms_change", "mutual_info", "rescale", "mean_scale"), out.tolist()))
 
+    @staticmethod
+    def _tune_dict(out):
+        return dict(slice_ms={b: float(out[i]) for i, b in enumerate((128, 64, 32, 16)) if out[i] >= 0},
+                    estep_sparse_ms=float(out[4]), estep_dense_ms=float(out[5]) if out[5] >= 0 else None,
+                    slice_block=int(out[6]), estep_form=int(out[7]))
+
     def autotune(self, par):
         """Times the slice blocks and both E-step forms on the current inputs
         and keeps the fastest (used by later iterations with option
         autotune). Returns the measurements and the choice."""
         out = np.zeros(8)
         self.call("dfg_autotune", C.byref(par), ptr(out, C.c_double))
-        return dict(slice_ms={b: out[i] for i, b in enumerate((128, 64, 32, 16)) if out[i] >= 0},
-                    estep_sparse_ms=out[4], estep_dense_ms=out[5] if out[5] >= 0 else None,
-                    slice_block=int(out[6]), estep_form=int(out[7]))
+        return self._tune_dict(out)
+
+    def tune_report(self):
+        """The autotuner's last report for the current inputs (None if not tuned)."""
+        out = np.zeros(8)
+        if self.lib.dfg_get_autotune_report(self.h, ptr(out, C.c_double)) != DFG_OK:
+            return None
+        return self._tune_dict(out)
 
     def graph_stats(self):
         out = (C.c_long * 3)()
@@ -460,3 +478,53 @@ class Context:
         keys = ("num_orient", "num_data", "estep_entries", "mstep_entries", "chunks", "chunk_frames",
                 "launches", "k_pad", "dense_estep")
         return dict(zip(keys, list(out)))
+
+
+class Batch:
+    """Independent reconstructions (Contexts on one GPU) iterated together as
+    one CUDA graph with a branch per reconstruction (dfg_batch_run)."""
+
+    def __init__(self, contexts):
+        self.lib = load()
+        self.contexts = list(contexts)
+        arr = (_V * len(self.contexts))(*[c.h for c in self.contexts])
+        h = _V()
+        rc = self.lib.dfg_batch_create(arr, len(self.contexts), C.byref(h))
+        if rc != DFG_OK:
+            raise DFGError(rc, "dfg_batch_create failed (contexts must be distinct and on one device)")
+        self.h = h
+
+    def run(self, pars, alphas=None):
+        """One iteration of every reconstruction; pars: one IterParams each.
+        Returns a list of dicts as Context.run_iteration's."""
+        n = len(self.contexts)
+        parr = (IterParams * n)(*pars)
+        al = None if alphas is None else np.ascontiguousarray(alphas, np.float64)
+        out = np.zeros((n, 5))
+        rc = self.lib.dfg_batch_run(self.h, parr, ptr(al, C.c_double), ptr(out, C.c_double))
+        if rc != DFG_OK:
+            raise DFGError(rc, self.lib.dfg_batch_last_error(self.h).decode())
+        keys = ("avg_likelihood", "rms_change", "mutual_info", "rescale", "mean_scale")
+        return [dict(zip(keys, row.tolist())) for row in out]
+
+    def set_lanes(self, lanes):
+        """Concurrent branches (1: one reconstruction after another)."""
+        rc = self.lib.dfg_batch_set_lanes(self.h, int(lanes))
+        if rc != DFG_OK:
+            raise DFGError(rc, "lanes must be >= 1")
+
+    def stats(self):
+        out = (C.c_long * 3)()
+        self.lib.dfg_batch_stats(self.h, out)
+        return dict(launches=out[0], instantiations=out[1], updates=out[2])
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dfg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

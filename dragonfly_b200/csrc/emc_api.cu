@@ -1386,6 +1386,14 @@ static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 	return DFG_OK;
 }
 
+extern "C" int dfg_get_autotune_report(dfg_ctx *ctx, double *report) {
+	if (!ctx || !report)
+		return DFG_ERR_ARG;
+	NEED(ctx->tuned, DFG_ERR_STATE, "not tuned for the current inputs");
+	std::copy(ctx->tune_report, ctx->tune_report + 8, report);
+	return DFG_OK;
+}
+
 extern "C" int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *report) {
 	if (!ctx || !par)
 		return DFG_ERR_ARG;
@@ -1666,11 +1674,64 @@ static int iteration_enqueue(dfg_ctx *ctx, const dfg_iter_params *par, double al
 	return DFG_OK;
 }
 
+// A captured graph replaces *exec in place when only kernel arguments
+// changed, else it is instantiated again.
+static cudaError_t graph_commit(cudaGraphExec_t *exec, cudaGraph_t g, long *updates, long *instantiations) {
+	if (*exec) {
+		cudaGraphExecUpdateResultInfo info;
+		if (cudaGraphExecUpdate(*exec, g, &info) == cudaSuccess) {
+			++*updates;
+			return cudaSuccess;
+		}
+		cudaGetLastError();
+		cudaGraphExecDestroy(*exec);
+		*exec = nullptr;
+	}
+	const cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+	if (e != cudaSuccess)
+		*exec = nullptr;
+	else
+		++*instantiations;
+	return e;
+}
+
+static bool iteration_normalizes(const dfg_ctx *ctx, const dfg_iter_params *par) {
+	return par->need_scaling && ctx->model_type == MT_3D;
+}
+
+// Reads an iteration's scalars back (the one synchronisation) and completes
+// its host-side results; out[5] as dfg_run_iteration.
+static int iteration_finish(dfg_ctx *ctx, const dfg_iter_params *par, double *out) {
+	cudaStream_t st = ctx->stream;
+	double h[6];
+	int derr = 0;
+	CK(cudaMemcpyAsync(h, ctx->scalars.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	if (ctx->dense_active)
+		CK(cudaMemcpyAsync(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	phase_collect(ctx);
+	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step: a pipeline wait gave up (results invalid)");
+	max_finish(ctx, h);
+	ctx->rms = std::sqrt(h[3] / ctx->M / (double)ctx->V);
+	double mean = 1.;
+	if (iteration_normalizes(ctx, par))
+		if (int rc = normalize_finish(ctx, h + 4, &mean))
+			return rc;
+	if (out) {
+		out[0] = ctx->avg_ll;
+		out[1] = ctx->rms;
+		out[2] = ctx->mutual_info;
+		out[3] = ctx->rescale;
+		out[4] = mean;
+	}
+	return DFG_OK;
+}
+
 extern "C" int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double alpha, double *out) {
 	if (int rc = max_prepare(ctx, par))
 		return rc;
 	cudaStream_t st = ctx->stream;
-	const bool normalize = par->need_scaling && ctx->model_type == MT_3D;
+	const bool normalize = iteration_normalizes(ctx, par);
 	if (ctx->use_graph && graphable(ctx, par)) {
 		CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
 		ctx->capturing = true;
@@ -1684,52 +1745,196 @@ extern "C" int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, doubl
 			cudaGetLastError();
 			return rc != DFG_OK ? rc : ctx->fail(DFG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
 		}
-		if (ctx->graph_exec) {
-			cudaGraphExecUpdateResultInfo info;
-			if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) == cudaSuccess) {
-				ctx->graph_updates++;
-			} else {
-				cudaGetLastError();
-				cudaGraphExecDestroy(ctx->graph_exec);
-				ctx->graph_exec = nullptr;
-			}
-		}
-		if (!ctx->graph_exec) {
-			const cudaError_t ei = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
-			if (ei != cudaSuccess) {
-				cudaGraphDestroy(g);
-				ctx->graph_exec = nullptr;
-				return ctx->fail(DFG_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ei));
-			}
-			ctx->graph_instantiations++;
-		}
+		const cudaError_t ei = graph_commit(&ctx->graph_exec, g, &ctx->graph_updates, &ctx->graph_instantiations);
 		cudaGraphDestroy(g);
+		NEED(ei == cudaSuccess, DFG_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ei));
 		CK(cudaGraphLaunch(ctx->graph_exec, st));
 		ctx->graph_launches++;
 	} else {
 		if (int rc = iteration_enqueue(ctx, par, alpha, normalize))
 			return rc;
 	}
-	double h[6];
-	int derr = 0;
-	CK(cudaMemcpyAsync(h, ctx->scalars.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
-	if (ctx->dense_active)
-		CK(cudaMemcpyAsync(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-	CK(cudaStreamSynchronize(st));
-	phase_collect(ctx);
-	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step: a pipeline wait gave up (results invalid)");
-	max_finish(ctx, h);
-	ctx->rms = std::sqrt(h[3] / ctx->M / (double)ctx->V);
-	double mean = 1.;
-	if (normalize)
-		if (int rc = normalize_finish(ctx, h + 4, &mean))
-			return rc;
-	if (out) {
-		out[0] = ctx->avg_ll;
-		out[1] = ctx->rms;
-		out[2] = ctx->mutual_info;
-		out[3] = ctx->rescale;
-		out[4] = mean;
+	return iteration_finish(ctx, par, out);
+}
+
+// ---------------------------------------------------------------------------
+// batches of independent reconstructions
+// ---------------------------------------------------------------------------
+struct dfg_batch {
+	std::vector<dfg_ctx *> ctxs;
+	int lanes = 1;  // concurrent branches; each runs its reconstructions in turn
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t fork = nullptr;
+	std::vector<cudaEvent_t> joins;
+	cudaGraphExec_t exec = nullptr;
+	long launches = 0, updates = 0, instantiations = 0;
+	std::string err;
+	int fail(int code, const char *fmt, ...) {
+		char buf[1024];
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(buf, sizeof(buf), fmt, ap);
+		va_end(ap);
+		err = buf;
+		return code;
+	}
+};
+
+extern "C" void dfg_batch_destroy(dfg_batch *b) {
+	if (!b)
+		return;
+	cudaSetDevice(b->device);
+	if (b->stream)
+		cudaStreamSynchronize(b->stream);
+	if (b->exec)
+		cudaGraphExecDestroy(b->exec);
+	for (auto e : b->joins)
+		if (e)
+			cudaEventDestroy(e);
+	if (b->fork)
+		cudaEventDestroy(b->fork);
+	if (b->stream)
+		cudaStreamDestroy(b->stream);
+	delete b;
+}
+
+extern "C" int dfg_batch_create(dfg_ctx *const *ctxs, int n, dfg_batch **out) {
+	if (!ctxs || n < 1 || !out)
+		return DFG_ERR_ARG;
+	*out = nullptr;
+	for (int i = 0; i < n; ++i) {
+		if (!ctxs[i] || ctxs[i]->device != ctxs[0]->device)
+			return DFG_ERR_ARG;
+		for (int j = 0; j < i; ++j)
+			if (ctxs[j] == ctxs[i])
+				return DFG_ERR_ARG;
+	}
+	dfg_batch *b = new dfg_batch();
+	b->ctxs.assign(ctxs, ctxs + n);
+	b->device = ctxs[0]->device;
+	b->joins.assign((size_t)n, nullptr);
+	b->lanes = 1;
+	bool ok = cudaSetDevice(b->device) == cudaSuccess &&
+	          cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+	          cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess;
+	for (int i = 0; i < n && ok; ++i)
+		ok = cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming) == cudaSuccess;
+	if (!ok) {
+		dfg_batch_destroy(b);
+		return DFG_ERR_CUDA;
+	}
+	*out = b;
+	return DFG_OK;
+}
+
+extern "C" const char *dfg_batch_last_error(const dfg_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+extern "C" int dfg_batch_set_lanes(dfg_batch *b, int lanes) {
+	if (!b || lanes < 1)
+		return DFG_ERR_ARG;
+	b->lanes = std::min<int>(lanes, (int)b->ctxs.size());
+	return DFG_OK;
+}
+
+extern "C" int dfg_batch_stats(dfg_batch *b, long *out) {
+	if (!b || !out)
+		return DFG_ERR_ARG;
+	out[0] = b->launches;
+	out[1] = b->instantiations;
+	out[2] = b->updates;
+	return DFG_OK;
+}
+
+extern "C" int dfg_batch_run(dfg_batch *b, const dfg_iter_params *pars, const double *alphas, double *out) {
+	if (!b || !pars)
+		return DFG_ERR_ARG;
+	const int n = (int)b->ctxs.size();
+	if (cudaSetDevice(b->device) != cudaSuccess)
+		return b->fail(DFG_ERR_CUDA, "cudaSetDevice failed");
+	bool graph = true;
+	for (int i = 0; i < n; ++i) {
+		dfg_ctx *c = b->ctxs[i];
+		if (int rc = max_prepare(c, &pars[i]))
+			return b->fail(rc, "reconstruction %d: %s", i, c->err.c_str());
+		graph = graph && c->use_graph && graphable(c, &pars[i]);
+	}
+	auto alpha = [&](int i) { return alphas ? alphas[i] : 0.; };
+	if (graph) {
+		// one graph: a branch per reconstruction on its own stream, forked
+		// from and joined back into the batch stream, so their kernels run
+		// side by side
+		if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+			return b->fail(DFG_ERR_CUDA, "cudaStreamBeginCapture failed");
+		// lanes: reconstructions dealt out in decreasing pair count to the
+		// least-loaded lane; within a lane each waits for the one before
+		std::vector<int> order(n), lane_of(n), prev(n, -1), last((size_t)b->lanes, -1);
+		std::vector<double> load((size_t)b->lanes, 0.);
+		for (int i = 0; i < n; ++i)
+			order[i] = i;
+		auto work = [&](int i) { return (double)b->ctxs[i]->R * b->ctxs[i]->N; };
+		std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
+		for (int i : order) {
+			const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+			lane_of[i] = l;
+			prev[i] = last[l];
+			last[l] = i;
+			load[l] += work(i);
+		}
+		int rc = DFG_OK, bad = -1;
+		cudaError_t e = cudaEventRecord(b->fork, b->stream);
+		for (int i : order) {
+			if (e != cudaSuccess)
+				break;
+			dfg_ctx *c = b->ctxs[i];
+			e = cudaStreamWaitEvent(c->stream, prev[i] < 0 ? b->fork : b->joins[prev[i]], 0);
+			if (e != cudaSuccess)
+				break;
+			if (rc == DFG_OK) {
+				c->capturing = true;
+				rc = iteration_enqueue(c, &pars[i], alpha(i), iteration_normalizes(c, &pars[i]));
+				c->capturing = false;
+				if (rc != DFG_OK)
+					bad = i;
+			}
+			e = cudaEventRecord(b->joins[i], c->stream);
+		}
+		for (int l = 0; l < b->lanes && e == cudaSuccess; ++l)
+			if (last[l] >= 0)
+				e = cudaStreamWaitEvent(b->stream, b->joins[last[l]], 0);
+		cudaGraph_t g = nullptr;
+		const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+		if (rc != DFG_OK || e != cudaSuccess || ee != cudaSuccess) {
+			if (g)
+				cudaGraphDestroy(g);
+			cudaGetLastError();
+			if (rc != DFG_OK)
+				return b->fail(rc, "reconstruction %d: %s", bad, b->ctxs[bad]->err.c_str());
+			return b->fail(DFG_ERR_CUDA, "batch capture failed: %s",
+			               cudaGetErrorString(e != cudaSuccess ? e : ee));
+		}
+		const cudaError_t ei = graph_commit(&b->exec, g, &b->updates, &b->instantiations);
+		cudaGraphDestroy(g);
+		if (ei != cudaSuccess)
+			return b->fail(DFG_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ei));
+		if (cudaGraphLaunch(b->exec, b->stream) != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess)
+			return b->fail(DFG_ERR_CUDA, "batch graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+		b->launches++;
+		for (int i = 0; i < n; ++i)
+			b->ctxs[i]->graph_launches++;
+	} else {
+		// some reconstruction needs the host between kernels: queue each on
+		// its own stream without a graph
+		for (int i = 0; i < n; ++i) {
+			dfg_ctx *c = b->ctxs[i];
+			if (int rc = iteration_enqueue(c, &pars[i], alpha(i), iteration_normalizes(c, &pars[i])))
+				return b->fail(rc, "reconstruction %d: %s", i, c->err.c_str());
+		}
+	}
+	for (int i = 0; i < n; ++i) {
+		dfg_ctx *c = b->ctxs[i];
+		if (int rc = iteration_finish(c, &pars[i], out ? out + 5 * (size_t)i : nullptr))
+			return b->fail(rc, "reconstruction %d: %s", i, c->err.c_str());
 	}
 	return DFG_OK;
 }

@@ -244,6 +244,33 @@ DFG_API int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double a
  * size (-1: not tried), sparse and dense E-step ms (-1: form refused), the
  * chosen block and form (0 sparse, 1 dense). */
 DFG_API int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *report);
+/* The last autotuner report for the current inputs (DFG_ERR_STATE if none). */
+DFG_API int dfg_get_autotune_report(dfg_ctx *ctx, double *report);
+
+/* ---- batches of independent reconstructions -------------------------------
+ * Several contexts on one GPU (different detectors, frames, orientation sets,
+ * models and modes) iterated together: dfg_batch_run runs dfg_run_iteration
+ * on every context with pars[i] and alphas[i] (NULL: 0), captured as one CUDA
+ * graph in which each reconstruction runs on its own stream, forked from and
+ * joined back into the batch's stream (see dfg_batch_set_lanes), with no host
+ * synchronisation between reconstructions. out
+ * (may be NULL) receives n x 5 values as dfg_run_iteration's. When a context
+ * needs the host between kernels (keep_prob, the background-aware scale
+ * search) the batch queues them without a graph. No counterpart in the
+ * reference (one reconstruction per process). */
+typedef struct dfg_batch dfg_batch;
+DFG_API int dfg_batch_create(dfg_ctx *const *ctxs, int n, dfg_batch **out);
+DFG_API int dfg_batch_run(dfg_batch *batch, const dfg_iter_params *pars, const double *alphas, double *out);
+DFG_API const char *dfg_batch_last_error(const dfg_batch *batch);
+/* Concurrent branches of the batch graph (default 1: the reconstructions run
+ * one after another inside one launch). With more lanes, reconstructions are
+ * dealt out by decreasing frame x orientation count to the least-loaded lane
+ * and the lanes run side by side (useful when single reconstructions leave
+ * SMs idle; concurrent reconstructions compete for L2). */
+DFG_API int dfg_batch_set_lanes(dfg_batch *batch, int lanes);
+/* out[0] = graph launches, out[1] = instantiations, out[2] = in-place updates. */
+DFG_API int dfg_batch_stats(dfg_batch *batch, long *out);
+DFG_API void dfg_batch_destroy(dfg_batch *batch);
 
 /* Graph use of dfg_run_iteration: out[0] = graph launches, out[1] =
  * instantiations, out[2] = in-place updates. */
