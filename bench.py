@@ -258,6 +258,7 @@ def run_ours(args, rank, world, local_rank):
     else:
         ctx.set_option("slice_block", tune["slice_block"])
         ctx.set_option("estep_form", 1 if args.estep_form == "dense" else 0)
+        ctx.set_option("mstep_form", tune["mstep_form"])
         tune["estep_form"] = 1 if args.estep_form == "dense" else 0
     setup_s = time.perf_counter() - t_setup
 
@@ -334,13 +335,16 @@ def run_ours(args, rank, world, local_rank):
         "update": 8. * inp["start"].size,
     }
     per_launch_s = (ms / 1e3) / max(nl, 1)
-    if dom == "estep" and wl["dense_estep"]:
-        # tensor-core E-step: 2 x R_pad x frames x K_pad x 2 (hi, lo) FLOP per
-        # chunk over the phase time per chunk (densification included)
+    dense_bits = {"estep": 1, "mstep": 2}.get(dom, 0)
+    if wl["dense_estep"] & dense_bits:
+        # tensor-core E-step or M-step: 2 x R_pad x frames x K_pad x 2 (hi, lo)
+        # FLOP per chunk over the phase time per chunk (the E-step phase
+        # includes the count densification, the M-step phase the probability
+        # split)
         tpeak, tsrc = measured_tensor_peak()
         flop = 2. * (-(-R // 128) * 128) * wl["chunk_frames"] * wl["k_pad"] * 2
         achieved = flop / ((ms / 1e3) / (args.steps * chunks)) / 1e12
-        roof = {"kernel": "estep (dense, tensor cores)", "bound": "tensor", "achieved": achieved, "peak": tpeak,
+        roof = {"kernel": dom + " (dense, tensor cores)", "bound": "tensor", "achieved": achieved, "peak": tpeak,
                 "unit": "TFLOP/s", "frac": achieved / tpeak, "peak_source": tsrc, "traffic": None,
                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
     else:
@@ -362,9 +366,10 @@ def run_ours(args, rank, world, local_rank):
                       "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
                       "autotuned": {"slice_block": tune["slice_block"],
                                     "estep_form": ["sparse", "dense"][tune["estep_form"]],
-                                    "estep_ms_first_chunk": {"sparse": round(float(tune["estep_sparse_ms"]), 2),
-                                                             "dense": None if tune["estep_dense_ms"] is None
-                                                             else round(float(tune["estep_dense_ms"]), 2)}},
+                                    "mstep_form": ["sparse", "dense"][tune["mstep_form"]],
+                                    "ms_first_chunk": {k: None if tune[k] is None else round(float(tune[k]), 2)
+                                                       for k in ("estep_sparse_ms", "estep_dense_ms",
+                                                                 "mstep_sparse_ms", "mstep_dense_ms")}},
                       "setup_s": setup_s},
            "s_per_iteration": ms_per_step / 1e3,
            "clocks": clocks,

@@ -310,19 +310,21 @@ class Context:
     def _tune_dict(out):
         return dict(slice_ms={b: float(out[i]) for i, b in enumerate((128, 64, 32, 16)) if out[i] >= 0},
                     estep_sparse_ms=float(out[4]), estep_dense_ms=float(out[5]) if out[5] >= 0 else None,
-                    slice_block=int(out[6]), estep_form=int(out[7]))
+                    slice_block=int(out[6]), estep_form=int(out[7]) & 1, mstep_form=int(out[7]) >> 1,
+                    mstep_sparse_ms=float(out[8]) if out[8] >= 0 else None,
+                    mstep_dense_ms=float(out[9]) if out[9] >= 0 else None)
 
     def autotune(self, par):
         """Times the slice blocks and both E-step forms on the current inputs
         and keeps the fastest (used by later iterations with option
         autotune). Returns the measurements and the choice."""
-        out = np.zeros(8)
+        out = np.zeros(10)
         self.call("dfg_autotune", C.byref(par), ptr(out, C.c_double))
         return self._tune_dict(out)
 
     def tune_report(self):
         """The autotuner's last report for the current inputs (None if not tuned)."""
-        out = np.zeros(8)
+        out = np.zeros(10)
         if self.lib.dfg_get_autotune_report(self.h, ptr(out, C.c_double)) != DFG_OK:
             return None
         return self._tune_dict(out)

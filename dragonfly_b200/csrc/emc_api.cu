@@ -531,8 +531,10 @@ static int build_chunks(dfg_ctx *ctx) {
 	const int N = ctx->N, P = ctx->P;
 	// per frame: pval and Pst of every orientation, plus its BF16 count row
 	// in the dense form
+	const bool any_dense = ctx->dense_active || ctx->m_dense_active;
 	const size_t pair_bytes = (size_t)ctx->RT * TILE * (sizeof(double) + sizeof(float)) +
-	                          (ctx->dense_active ? (size_t)ctx->K_pad * 2 : 0);
+	                          (any_dense ? (size_t)ctx->K_pad * 2 : 0) +
+	                          (ctx->m_dense_active ? (size_t)ctx->RT * TILE * 4 : 0);
 	size_t budget;
 	if (ctx->pair_budget_mb > 0.) {
 		budget = (size_t)(ctx->pair_budget_mb * 1048576.);
@@ -623,7 +625,7 @@ static int build_chunks(dfg_ctx *ctx) {
 		CK(cudaStreamSynchronize(ctx->stream));
 	}
 	ctx->chunks_R = ctx->R;
-	ctx->chunks_dense = ctx->dense_active;
+	ctx->chunks_dense = (ctx->dense_active ? 1 : 0) | (ctx->m_dense_active ? 2 : 0);
 	return DFG_OK;
 }
 
@@ -660,7 +662,8 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	CK(ctx->p_norm.ensure(N));
 	CK(ctx->psum_d.ensure(N));
 	CK(ctx->quat_norm.ensure(N * ctx->M));
-	if (ctx->chunks_R != ctx->R || ctx->chunks_dense != ctx->dense_active) {
+	if (ctx->chunks_R != ctx->R ||
+	    ctx->chunks_dense != ((ctx->dense_active ? 1 : 0) | (ctx->m_dense_active ? 2 : 0))) {
 		ctx->pval.release();
 		ctx->Pst.release();
 		ctx->tmax.release();
@@ -892,6 +895,22 @@ static int encode_bf16_map(dfg_ctx *ctx, CUtensorMap *map, const void *base, lon
 	return DFG_OK;
 }
 
+// Tensor map of the BF16 probability rows [rows][128] read in boxes of 64
+// orientations x 64 frames with the 128-byte swizzle.
+static int encode_rows_map(dfg_ctx *ctx, CUtensorMap *map, const void *base, long long rows) {
+	auto fn = tensor_map_encoder();
+	NEED(fn != nullptr, DFG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+	cuuint64_t dims[2] = {128, (cuuint64_t)rows};
+	cuuint64_t strides[1] = {256};
+	cuuint32_t box[2] = {64, (cuuint32_t)DK};
+	cuuint32_t estr[2] = {1, 1};
+	const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+	                      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+	                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	NEED(r == CUDA_SUCCESS, DFG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+	return DFG_OK;
+}
+
 // Whether this iteration may take the dense form, and why not (message).
 static const char *dense_refusal(dfg_ctx *ctx, const dfg_iter_params *par) {
 	if (TILE != 128)
@@ -903,7 +922,7 @@ static const char *dense_refusal(dfg_ctx *ctx, const dfg_iter_params *par) {
 	if (ctx->max_count0 < 0) {
 		int m = 1;
 		for (size_t i = 0; i < ctx->h_place_multi.size(); ++i)
-			if (ctx->h_mask[ctx->h_place_multi[i]] == 0)
+			if (ctx->h_mask[ctx->h_place_multi[i]] < 2)
 				m = std::max(m, ctx->h_count_multi[i]);
 		ctx->max_count0 = m;
 	}
@@ -918,7 +937,7 @@ static int dense_prepare_slices(dfg_ctx *ctx) {
 	if (ctx->dense_P != ctx->P) {
 		std::vector<int> kp, pc((size_t)ctx->P, -1);
 		for (int p = 0; p < ctx->P; ++p)
-			if (ctx->h_mask[p] == 0) {
+			if (ctx->h_mask[p] < 2) {
 				pc[p] = (int)kp.size();
 				kp.push_back(p);
 			}
@@ -928,7 +947,12 @@ static int dense_prepare_slices(dfg_ctx *ctx) {
 		CK(upload(ctx->pcol, pc.data(), pc.size(), ctx->stream));
 		CK(cudaStreamSynchronize(ctx->stream));
 		ctx->dense_P = ctx->P;
-		ctx->map_src[0] = ctx->map_src[1] = ctx->map_src[2] = nullptr;
+		std::fill(ctx->map_src, ctx->map_src + 6, nullptr);
+	}
+	if (!ctx->dense_active) {  // the M-step alone needs only the pixel columns
+		ctx->Ahi.release();
+		ctx->Alo.release();
+		return DFG_OK;
 	}
 	const long long R_pad = (long long)(ctx->M * ctx->num_rot + TILE - 1) / TILE * TILE;
 	const size_t n = (size_t)R_pad * ctx->K_pad;
@@ -945,15 +969,37 @@ static int dense_prepare_slices(dfg_ctx *ctx) {
 	return DFG_OK;
 }
 
-// One chunk's count rows (after the chunk layout is known).
+// One chunk's count rows and, for the dense M-step, probability rows (after
+// the chunk layout is known). The E-step reads the count tiles as 256 frame
+// rows x 64 pixels; the M-step as 64 frames x 64 pixels.
 static int dense_prepare_counts(dfg_ctx *ctx) {
 	const int rows = (ctx->chunk_frames + DN - 1) / DN * DN;
 	CK(ctx->cnt.ensure((size_t)rows * ctx->K_pad));
 	if (ctx->map_src[2] != ctx->cnt.p || ctx->cnt_rows != rows) {
 		if (int rc = encode_bf16_map(ctx, &ctx->map_cnt, ctx->cnt.p, rows, DN))
 			return rc;
-		ctx->map_src[2] = ctx->cnt.p;
+		if (int rc = encode_bf16_map(ctx, &ctx->map_cnt_m, ctx->cnt.p, rows, DK))
+			return rc;
+		ctx->map_src[2] = ctx->map_src[5] = ctx->cnt.p;
 		ctx->cnt_rows = rows;
+		ctx->map_src[3] = ctx->map_src[4] = nullptr;
+	}
+	if (ctx->m_dense_active) {
+		const size_t n = (size_t)ctx->RT * rows * 128;
+		CK(ctx->Phi.ensure(n));
+		CK(ctx->Plo.ensure(n));
+		if (ctx->map_src[3] != ctx->Phi.p || ctx->map_src[4] != ctx->Plo.p) {
+			if (int rc = encode_rows_map(ctx, &ctx->map_phi, ctx->Phi.p, (long long)ctx->RT * rows))
+				return rc;
+			if (int rc = encode_rows_map(ctx, &ctx->map_plo, ctx->Plo.p, (long long)ctx->RT * rows))
+				return rc;
+			ctx->map_src[3] = ctx->Phi.p;
+			ctx->map_src[4] = ctx->Plo.p;
+		}
+		CK(cudaFuncSetAttribute(mstep_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DSMEM_BYTES));
+	} else {
+		ctx->Phi.release();
+		ctx->Plo.release();
 	}
 	CK(ctx->derr.ensure(1));
 	CK(cudaMemsetAsync(ctx->derr.p, 0, sizeof(int), ctx->stream));
@@ -961,12 +1007,14 @@ static int dense_prepare_counts(dfg_ctx *ctx) {
 	return DFG_OK;
 }
 
-// The dense buffers are freed when the sparse form is in use.
+// The dense buffers are freed when the sparse forms are in use.
 static void dense_release(dfg_ctx *ctx) {
 	ctx->Ahi.release();
 	ctx->Alo.release();
 	ctx->cnt.release();
-	ctx->map_src[0] = ctx->map_src[1] = ctx->map_src[2] = nullptr;
+	ctx->Phi.release();
+	ctx->Plo.release();
+	std::fill(ctx->map_src, ctx->map_src + 6, nullptr);
 }
 
 static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par);
@@ -985,20 +1033,22 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 		if (int rc = run_autotune(ctx, par))
 			return rc;
 	const int form = ctx->tuning ? ctx->tune_form : (ctx->autotune ? ctx->tuned_form : ctx->estep_form);
-	ctx->dense_active = false;
-	if (form == 1) {
+	const int mform = ctx->tuning ? ctx->tune_mform : (ctx->autotune ? ctx->tuned_mform : ctx->mstep_form);
+	ctx->dense_active = ctx->m_dense_active = false;
+	if (form == 1 || mform == 1) {
 		NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0, DFG_ERR_STATE, "set detector, frames and quaternions");
 		const char *why = dense_refusal(ctx, par);
 		NEED(why == nullptr, DFG_ERR_ARG, "%s", why);
-		ctx->dense_active = true;
+		ctx->dense_active = form == 1;
+		ctx->m_dense_active = mform == 1;
 		if (int rc = dense_prepare_slices(ctx))
 			return rc;
-	} else if (ctx->Ahi.p != nullptr) {
+	} else if (ctx->cnt.p != nullptr || ctx->Ahi.p != nullptr) {
 		dense_release(ctx);
 	}
 	if (int rc = ensure_buffers(ctx))
 		return rc;
-	if (ctx->dense_active)
+	if (ctx->dense_active || ctx->m_dense_active)
 		if (int rc = dense_prepare_counts(ctx))
 			return rc;
 	cudaStream_t st = ctx->stream;
@@ -1095,15 +1145,50 @@ static int launch_slices(dfg_ctx *ctx, int ob, double *Wd) {
 
 // The E-step of one frame chunk: the tensor-core products (dense: counts
 // densified first) or the sparse gathers (background-aware with bg).
+// One chunk's photon counts as BF16 rows over the mask < 2 pixel columns
+// (for the dense E-step and M-step).
+static int launch_densify(dfg_ctx *ctx, const Chunk &ch) {
+	cudaStream_t st = ctx->stream;
+	CK(cudaMemsetAsync(ctx->cnt.p, 0, (size_t)ctx->cnt_rows * ctx->K_pad * 2, st));
+	if (ch.npix > 0) {
+		densify_counts_kernel<<<blocks_for((long long)ch.npix * 32, 256), 256, 0, st>>>(
+		    ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, ctx->pcol.p, ch.nc, ctx->K_pad,
+		    (__nv_bfloat16 *)ctx->cnt.p);
+		CKL("densify_counts_kernel");
+	}
+	return DFG_OK;
+}
+
+// The M-step of one chunk: tomogram products on the tensor cores (the
+// probabilities split into BF16 hi / lo rows first), or the sparse gathers.
+static int launch_mstep(dfg_ctx *ctx, const Chunk &ch, bool dense) {
+	cudaStream_t st = ctx->stream;
+	const int Nc = ch.nc, P = ctx->P, RT = ctx->RT;
+	if (dense) {
+		const int rows = ctx->cnt_rows;
+		split_prob_kernel<<<blocks_for((long long)RT * rows * 16, 256), 256, 0, st>>>(
+		    ctx->Pst.p, Nc, rows, RT, (__nv_bfloat16 *)ctx->Phi.p, (__nv_bfloat16 *)ctx->Plo.p);
+		CKL("split_prob_kernel");
+		const int n_tiles = ctx->K_pad / DN + (ctx->K_pad % DN ? 1 : 0);
+		mstep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
+		    ctx->map_phi, ctx->map_plo, ctx->map_cnt_m, (Nc + DK - 1) / DK, rows, RT, n_tiles, ctx->kpix.p, ctx->K,
+		    P, ctx->T.p, ctx->derr.p);
+		CKL("mstep_dense_kernel");
+		return DFG_OK;
+	}
+	if (ch.npix > 0) {
+		const long long warps = (long long)RT * ch.npix;
+		mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p,
+		                                                    ch.pix.p, ch.npix, P, RT, ctx->T.p);
+		CKL("mstep_kernel");
+	}
+	return DFG_OK;
+}
+
 static int launch_estep(dfg_ctx *ctx, const Chunk &ch, int use_scale, bool bg, const RefineMask &rm, bool dense) {
 	cudaStream_t st = ctx->stream;
 	const int Nc = ch.nc, P = ctx->P, R = ctx->R, RT = ctx->RT;
-	if (dense) {
-		CK(cudaMemsetAsync(ctx->cnt.p, 0, (size_t)ctx->cnt_rows * ctx->K_pad * 2, st));
-		densify_counts_kernel<<<blocks_for((long long)Nc * 32, 256), 256, 0, st>>>(
-		    ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->pcol.p, ch.d0, Nc, P, ctx->K_pad,
-		    (__nv_bfloat16 *)ctx->cnt.p);
-		CKL("densify_counts_kernel");
+	if (dense) {  // counts densified by launch_densify for this chunk
 		const int n_tiles = (Nc + DN - 1) / DN;
 		estep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
 		    ctx->map_hi, ctx->map_lo, ctx->map_cnt, ctx->K_pad / DK, RT, n_tiles, ctx->u.p, ctx->logw.p, R,
@@ -1131,6 +1216,27 @@ static int launch_estep(dfg_ctx *ctx, const Chunk &ch, int use_scale, bool bg, c
 		DFG_ESTEP(false);
 #undef DFG_ESTEP
 	CKL("estep_kernel");
+	return DFG_OK;
+}
+
+// Normalisation of one chunk (normalize_prob + the per-frame sums of
+// calc_psum_r); with bg the probabilities are also kept in FP64.
+static int launch_norm(dfg_ctx *ctx, const Chunk &ch, int psum_d_on, bool bg) {
+	cudaStream_t st = ctx->stream;
+	const int Nc = ch.nc, RT = ctx->RT, R = ctx->R, M = ctx->M;
+	if (M > 1)
+		norm_kernel<true><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
+		    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
+		    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
+		    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
+		    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
+	else
+		norm_kernel<false><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
+		    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
+		    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
+		    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
+		    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
+	CKL("norm_kernel");
 	return DFG_OK;
 }
 
@@ -1166,7 +1272,7 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CKL("logw_kernel");
 	if (ctx->dense_active) {
 		split_logw_kernel<<<dim3(ctx->K_pad / DK, RT), 256, 0, st>>>(
-		    ctx->logW.p, P, ctx->kpix.p, ctx->K, ctx->K_pad, (__nv_bfloat16 *)ctx->Ahi.p,
+		    ctx->logW.p, P, ctx->kpix.p, ctx->mask.p, ctx->K, ctx->K_pad, (__nv_bfloat16 *)ctx->Ahi.p,
 		    (__nv_bfloat16 *)ctx->Alo.p);
 		CKL("split_logw_kernel");
 	}
@@ -1188,24 +1294,16 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 		const int Nc = ch.nc;
 		// E-step (calculate_prob, max_prob.c:66-213)
 		phase_begin(ctx, PH_ESTEP);
+		if (ctx->dense_active || ctx->m_dense_active)
+			if (int rc = launch_densify(ctx, ch))
+				return rc;
 		if (int rc = launch_estep(ctx, ch, use_scale, bg, rm, ctx->dense_active))
 			return rc;
-		phase_end(ctx, PH_ESTEP, ctx->dense_active ? 2 : 1);
+		phase_end(ctx, PH_ESTEP, (ctx->dense_active || ctx->m_dense_active ? 1 : 0) + 1);
 		// normalisation and per-frame sums (normalize_prob + calc_psum_r)
 		phase_begin(ctx, PH_NORM);
-		if (M > 1)
-			norm_kernel<true><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
-			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
-			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
-			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
-			    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
-		else
-			norm_kernel<false><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
-			    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
-			    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
-			    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
-			    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
-		CKL("norm_kernel");
+		if (int rc = launch_norm(ctx, ch, psum_d_on, bg))
+			return rc;
 		phase_end(ctx, PH_NORM, 1);
 		if (ctx->keep_prob)
 			if (int rc = collect_prob(ctx, ch))
@@ -1233,9 +1331,12 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 		phase_end(ctx, PH_PSUM, bg ? 4 : 2);
 		// tomograms (update_tomogram_nobg, max_update.c:142-230)
 		phase_begin(ctx, PH_MSTEP);
-		if (ch.npix > 0) {
+		if (!bg) {
+			if (int rc = launch_mstep(ctx, ch, ctx->m_dense_active))
+				return rc;
+		} else if (ch.npix > 0) {
 			long long warps = (long long)RT * ch.npix;
-			if (bg) {
+			{
 				// update_tomogram_bg (max_update.c:343-543); the mean photons per
 				// pixel bound the first search window (:397-400)
 				mstep_bg_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(
@@ -1243,13 +1344,9 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 				    ctx->psum_r.p, ctx->scalemax.p, ctx->scale.p, ctx->bgscale.p, ctx->background.p, ctx->powder.p,
 				    ctx->mean_count / P, ctx->T.p);
 				CKL("mstep_bg_kernel");
-			} else {
-				mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p,
-				                                                    ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p);
-				CKL("mstep_kernel");
 			}
 		}
-		phase_end(ctx, PH_MSTEP, ch.npix > 0 ? 1 : 0);
+		phase_end(ctx, PH_MSTEP, ctx->m_dense_active ? 2 : (ch.npix > 0 ? 1 : 0));
 	}
 
 	// merge (merge_tomogram -> slice_merge3d); the weight grid is rebuilt only
@@ -1294,20 +1391,21 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 
 // Project autotuner. On the context's own inputs it times (CUDA events, best
 // of two after a warm-up launch) the slice kernel with 128, 64, 32 and 16 orientations per block and
-// both forms of the E-step photon term (sparse gathers, dense tensor-core
-// products where the inputs allow them) on the first frame chunk, and keeps
-// the fastest of each. tune_report: slice ms per block size (-1 if not
-// tried), sparse and dense E-step ms (-1 if refused), the chosen block and
-// form.
+// both forms of the E-step photon term and of the M-step (sparse gathers,
+// dense tensor-core products where the inputs allow them) on the first frame
+// chunk, and keeps the fastest of each. tune_report: slice ms per block size
+// (-1 if not tried), sparse and dense E-step ms (-1 if refused; the dense one
+// includes the count densification), the chosen block, the chosen forms
+// (E-step + 2 x M-step, 1 = dense), sparse and dense M-step ms.
 static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 	NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0 && ctx->S > 0, DFG_ERR_STATE,
 	     "autotune: set detector, frames, quaternions and model first");
-	double rep[8] = {-1., -1., -1., -1., -1., -1., -1., -1.};
+	double rep[10] = {-1., -1., -1., -1., -1., -1., -1., -1., -1., -1.};
 	const bool dense_ok = dense_refusal(ctx, par) == nullptr;
 	const bool save_timing = ctx->timing;
 	ctx->timing = false;
 	ctx->tuning = true;
-	ctx->tune_form = dense_ok ? 1 : 0;
+	ctx->tune_form = ctx->tune_mform = dense_ok ? 1 : 0;
 	int rc = max_prepare(ctx, par);
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	if (rc == DFG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
@@ -1356,18 +1454,35 @@ static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 		CKL("logw_kernel");
 		rc = timed([&] { return launch_estep(ctx, ctx->chunks[0], use_scale, bg, rm, false); }, rep[4]);
 	}
+	const Chunk &c0 = ctx->chunks[0];
 	if (rc == DFG_OK && dense_ok) {
 		split_logw_kernel<<<dim3(ctx->K_pad / DK, ctx->RT), 256, 0, st>>>(
-		    ctx->logW.p, ctx->P, ctx->kpix.p, ctx->K, ctx->K_pad, (__nv_bfloat16 *)ctx->Ahi.p,
+		    ctx->logW.p, ctx->P, ctx->kpix.p, ctx->mask.p, ctx->K, ctx->K_pad, (__nv_bfloat16 *)ctx->Ahi.p,
 		    (__nv_bfloat16 *)ctx->Alo.p);
 		CKL("split_logw_kernel");
-		rc = timed([&] { return launch_estep(ctx, ctx->chunks[0], use_scale, bg, rm, true); }, rep[5]);
+		// the densification counts to the dense E-step (when the M-step stays
+		// sparse it is needed for the E-step alone)
+		rc = timed(
+		    [&] {
+			    if (int r = launch_densify(ctx, c0))
+				    return r;
+			    return launch_estep(ctx, c0, use_scale, bg, rm, true);
+		    },
+		    rep[5]);
+	}
+	// the M-step forms on the first chunk's probabilities
+	const int psum_d_on = par->need_scaling && par->update_scale;
+	if (rc == DFG_OK)
+		rc = launch_norm(ctx, c0, psum_d_on, bg);
+	if (rc == DFG_OK && !bg)
+		rc = timed([&] { return launch_mstep(ctx, c0, false); }, rep[8]);
+	if (rc == DFG_OK && dense_ok)
+		rc = timed([&] { return launch_mstep(ctx, c0, true); }, rep[9]);
+	if (rc == DFG_OK && dense_ok) {
 		int derr = 0;
-		if (rc == DFG_OK) {
-			CK(cudaMemcpy(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost));
-			if (derr)
-				rc = ctx->fail(DFG_ERR_CUDA, "autotune: the dense E-step gave up");
-		}
+		CK(cudaMemcpy(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+		if (derr)
+			rc = ctx->fail(DFG_ERR_CUDA, "autotune: a dense kernel gave up");
 	}
 	if (e0)
 		cudaEventDestroy(e0);
@@ -1379,10 +1494,11 @@ static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 		return rc;
 	ctx->tuned_ob = best_ob;
 	ctx->tuned_form = (dense_ok && rep[5] >= 0. && rep[5] < rep[4]) ? 1 : 0;
+	ctx->tuned_mform = (dense_ok && rep[9] >= 0. && (rep[8] < 0. || rep[9] < rep[8])) ? 1 : 0;
 	ctx->tuned = true;
 	rep[6] = best_ob;
-	rep[7] = ctx->tuned_form;
-	std::copy(rep, rep + 8, ctx->tune_report);
+	rep[7] = ctx->tuned_form + 2 * ctx->tuned_mform;
+	std::copy(rep, rep + 10, ctx->tune_report);
 	return DFG_OK;
 }
 
@@ -1390,7 +1506,7 @@ extern "C" int dfg_get_autotune_report(dfg_ctx *ctx, double *report) {
 	if (!ctx || !report)
 		return DFG_ERR_ARG;
 	NEED(ctx->tuned, DFG_ERR_STATE, "not tuned for the current inputs");
-	std::copy(ctx->tune_report, ctx->tune_report + 8, report);
+	std::copy(ctx->tune_report, ctx->tune_report + 10, report);
 	return DFG_OK;
 }
 
@@ -1401,7 +1517,7 @@ extern "C" int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *re
 	if (int rc = run_autotune(ctx, par))
 		return rc;
 	if (report)
-		std::copy(ctx->tune_report, ctx->tune_report + 8, report);
+		std::copy(ctx->tune_report, ctx->tune_report + 10, report);
 	return DFG_OK;
 }
 
@@ -1423,11 +1539,11 @@ extern "C" int dfg_maximize(dfg_ctx *ctx, const dfg_iter_params *par, double *av
 	double h[3];
 	int derr = 0;
 	CK(cudaMemcpyAsync(h, ctx->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-	if (ctx->dense_active)
+	if (ctx->dense_active || ctx->m_dense_active)
 		CK(cudaMemcpyAsync(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
 	phase_collect(ctx);
-	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step: a pipeline wait gave up (results invalid)");
+	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step / M-step: a pipeline wait gave up (results invalid)");
 	max_finish(ctx, h);
 	if (avg_likelihood)
 		*avg_likelihood = ctx->avg_ll;
@@ -1706,11 +1822,11 @@ static int iteration_finish(dfg_ctx *ctx, const dfg_iter_params *par, double *ou
 	double h[6];
 	int derr = 0;
 	CK(cudaMemcpyAsync(h, ctx->scalars.p, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
-	if (ctx->dense_active)
+	if (ctx->dense_active || ctx->m_dense_active)
 		CK(cudaMemcpyAsync(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
 	phase_collect(ctx);
-	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step: a pipeline wait gave up (results invalid)");
+	NEED(derr == 0, DFG_ERR_CUDA, "dense E-step / M-step: a pipeline wait gave up (results invalid)");
 	max_finish(ctx, h);
 	ctx->rms = std::sqrt(h[3] / ctx->M / (double)ctx->V);
 	double mean = 1.;
@@ -2230,6 +2346,12 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 		ctx->estep_form = v;
 		return DFG_OK;
 	}
+	if (!strcmp(key, "mstep_form")) {
+		const int v = (int)value;
+		NEED(v == 0 || v == 1, DFG_ERR_ARG, "mstep_form must be 0 (sparse) or 1 (dense)");
+		ctx->mstep_form = v;
+		return DFG_OK;
+	}
 	if (!strcmp(key, "slice_block")) {
 		const int v = (int)value;
 		NEED(v == 0 || ((v == 16 || v == 32 || v == 64 || v == TILE) && v <= TILE), DFG_ERR_ARG,
@@ -2306,6 +2428,6 @@ extern "C" int dfg_get_workload(dfg_ctx *ctx, long long *out) {
 	out[5] = ctx->chunk_frames;
 	out[6] = ctx->launches;
 	out[7] = ctx->K_pad;
-	out[8] = ctx->dense_active ? 1 : 0;
+	out[8] = (ctx->dense_active ? 1 : 0) | (ctx->m_dense_active ? 2 : 0);
 	return DFG_OK;
 }

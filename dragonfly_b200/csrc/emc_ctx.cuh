@@ -170,19 +170,25 @@ struct dfg_ctx {
 	// log-slices [R_pad][K_pad] and one chunk's counts [cnt_rows][K_pad] in
 	// BF16 (stored as 16-bit words); their TMA tensor maps; derr = the dense
 	// kernel's give-up flag
-	int estep_form = 0;
-	bool dense_active = false, chunks_dense = false;
-	// autotuner (option autotune): the slice block and E-step form it chose
-	// for the current inputs; tuning / tune_form while it measures
+	// mstep_form likewise for the tomogram products (m_dense_active);
+	// chunks_dense = the forms the chunk layout was sized for. K = mask < 2
+	// pixel columns (the E-step's hi / lo rows are zero on mask-1 columns);
+	// Phi / Plo = one chunk's probabilities [RT][cnt_rows][128] in BF16
+	int estep_form = 0, mstep_form = 0;
+	bool dense_active = false, m_dense_active = false;
+	int chunks_dense = 0;
+	// autotuner (option autotune): the slice block and E-step / M-step forms
+	// it chose for the current inputs; tuning / tune_* while it measures
 	bool autotune = false, tuned = false, tuning = false;
-	int tuned_ob = 0, tuned_form = 0, tune_form = 0;
-	double tune_report[8] = {};
+	int tuned_ob = 0, tuned_form = 0, tuned_mform = 0, tune_form = 0, tune_mform = 0;
+	double tune_report[10] = {};
 	int K = 0, K_pad = 0, dense_P = -1, cnt_rows = 0;
-	int max_count0 = -1;  // largest count on a mask-0 pixel; -1 = not known
+	int max_count0 = -1;  // largest count on a mask < 2 pixel; -1 = not known
 	DevBuf<int> kpix, pcol, derr;
-	DevBuf<uint16_t> Ahi, Alo, cnt;
-	CUtensorMap map_hi, map_lo, map_cnt;
-	const void *map_src[3] = {nullptr, nullptr, nullptr};
+	DevBuf<uint16_t> Ahi, Alo, cnt, Phi, Plo;
+	// counts read by the E-step (256-frame boxes) and the M-step (64-frame boxes)
+	CUtensorMap map_hi, map_lo, map_cnt, map_phi, map_plo, map_cnt_m;
+	const void *map_src[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 	// coarse-to-fine refinement: coarse cell of every orientation (qmap,
 	// [R_pad], -1 past R) and per frame one bit per relevant coarse
 	// orientation (rel_bits, [N][rwords])

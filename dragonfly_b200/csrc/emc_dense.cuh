@@ -296,13 +296,188 @@ __global__ void __launch_bounds__(192, 1) estep_dense_kernel(
 	}
 }
 
-// hi / lo BF16 log-slices [R_pad][K_pad] (orientation rows, mask-0 pixels in
-// pixel order, zero past K) from the FP32 log-slice tiles [RT][P+1][TILE]:
+// ---------------------------------------------------------------------------
+// dense M-step: T[r][p] += sum_d P[r][d] count[d][p] over one frame chunk
+// ---------------------------------------------------------------------------
+// Both operands are MN-major (orientations and pixels contiguous, frames the
+// reduction): tiles of 64 elements (128 bytes) x 64 frames per TMA box,
+// 8-frame groups 1024 bytes apart (SBO), 64-element blocks one box (8192
+// bytes) apart (LBO); one K = 16 step is two 8-frame groups (2048 bytes).
+__device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t addr) {
+	return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)(8192 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+	       ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+constexpr uint32_t DIDESC_MN = DIDESC | (1u << 15) | (1u << 16);  // A and B MN-major
+
+__device__ __forceinline__ void umma_bf16_mn(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "setp.ne.b32 p, %4, 0;\n\t"
+	    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+	    "l"(adesc), "l"(bdesc), "r"(DIDESC_MN), "r"(accumulate)
+	    : "memory");
+}
+
+// One CTA per 128-orientation x 256-pixel-column tile over all frames of the
+// chunk: TMA loads of the hi / lo probability tiles ([RT * Nc_pad][128] BF16,
+// two 64-orientation boxes each) and of the count tile ([Nc_pad][K_pad],
+// four 64-pixel boxes), tcgen05.mma into a 256-column FP32 accumulator, and
+// an epilogue adding it to the tomograms T[rt][kpix[col]][j] (FP32, read and
+// written as the sparse M-step does). Roles and give-up rules as
+// estep_dense_kernel.
+__global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
+    const __grid_constant__ CUtensorMap map_phi, const __grid_constant__ CUtensorMap map_plo,
+    const __grid_constant__ CUtensorMap map_cnt, int num_kb, int Nc_pad, int RT, int n_tiles,
+    const int *__restrict__ kpix, int K, int P, float *__restrict__ T, int *__restrict__ err) {
+	extern __shared__ uint8_t dsm_raw[];
+	uint8_t *sm = (uint8_t *)(((uintptr_t)dsm_raw + 1023) & ~(uintptr_t)1023);
+	uint64_t *bars = (uint64_t *)(sm + DSTAGES * DSTAGE_BYTES + DEPI_BYTES);
+	uint64_t *full = bars, *empty = bars + DSTAGES, *accum = bars + 2 * DSTAGES;
+	uint32_t *tmem_slot = (uint32_t *)(bars + 2 * DSTAGES + 1);
+	volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int per_group = DGROUP * n_tiles;
+	const int grp = blockIdx.x / per_group, rem = blockIdx.x - grp * per_group;
+	const int rows = min(DGROUP, RT - grp * DGROUP);
+	const int rt = grp * DGROUP + rem % rows, nt = rem / rows;
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < DSTAGES; ++s) {
+			mbar_init(&full[s], 1);
+			mbar_init(&empty[s], 1);
+		}
+		mbar_init(accum, 1);
+		*abort_flag = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (warp == 1) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+		                 smem_addr(tmem_slot)),
+		             "r"(DN)
+		             : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = *tmem_slot;
+
+	if (warp == 0) {
+		if (lane == 0) {
+			int issued = 0;
+			for (int kb = 0; kb < num_kb; ++kb) {
+				const int s = kb % DSTAGES;
+				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
+				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u)) {
+					*abort_flag = 1;
+					atomicExch(err, 1);
+					break;
+				}
+				uint8_t *st = sm + s * DSTAGE_BYTES;
+				const int fy = rt * Nc_pad + kb * DK;  // probability rows of this frame block
+				mbar_expect_tx(&full[s], DSTAGE_BYTES);
+				for (int h = 0; h < 2; ++h) {
+					tma_load_2d(st + h * (DA_BYTES / 2), &map_phi, &full[s], h * 64, fy);
+					tma_load_2d(st + DA_BYTES + h * (DA_BYTES / 2), &map_plo, &full[s], h * 64, fy);
+				}
+				for (int h = 0; h < 4; ++h)
+					tma_load_2d(st + 2 * DA_BYTES + h * (DB_BYTES / 4), &map_cnt, &full[s], nt * DN + h * 64,
+					            kb * DK);
+				issued = kb + 1;
+			}
+			if (*abort_flag)
+				for (int kb = max(0, issued - DSTAGES); kb < issued; ++kb)
+					mbar_wait(&full[kb % DSTAGES], (uint32_t)(kb / DSTAGES) & 1u);
+		}
+		__syncwarp();
+	} else if (warp == 1) {
+		if (lane == 0) {
+			for (int kb = 0; kb < num_kb; ++kb) {
+				const int s = kb % DSTAGES;
+				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
+				if (*abort_flag || !mbar_wait(&full[s], ph)) {
+					*abort_flag = 1;
+					atomicExch(err, 1);
+					break;
+				}
+				tc_fence_after();
+				const uint32_t a_hi = smem_addr(sm + s * DSTAGE_BYTES);
+				const uint32_t a_lo = a_hi + DA_BYTES, b = a_hi + 2 * DA_BYTES;
+#pragma unroll
+				for (int k = 0; k < DK / 16; ++k) {
+					const uint64_t db = sw128_mn_desc(b + 2048 * k);
+					umma_bf16_mn(tmem, sw128_mn_desc(a_hi + 2048 * k), db, (kb | k) != 0);
+					umma_bf16_mn(tmem, sw128_mn_desc(a_lo + 2048 * k), db, 1u);
+				}
+				umma_commit(&empty[s]);
+			}
+			umma_commit(accum);
+		}
+		__syncwarp();
+	} else {
+		const int q = warp & 3, i = q * 32 + lane;
+		const bool ok = mbar_wait(accum, 0);
+		if (!ok) {
+			*abort_flag = 1;
+			atomicExch(err, 1);
+		}
+		tc_fence_after();
+		if (ok && !*abort_flag) {
+			for (int c = 0; c < DN / 16; ++c) {
+				float acc[16];
+				tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 16), acc);
+#pragma unroll
+				for (int j = 0; j < 16; ++j) {
+					const int col = nt * DN + c * 16 + j;
+					if (col < K) {
+						float *t = T + ((size_t)rt * P + kpix[col]) * 128 + i;
+						*t = (float)((double)*t + (double)acc[j]);
+					}
+				}
+			}
+		}
+	}
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 1) {
+		tc_fence_after();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(DN) : "memory");
+	}
+}
+
+// Probabilities of one chunk as BF16 hi / lo rows [RT][Nc_pad][128]
+// (p = max(Pst, 0): pairs at or below the PROB_MIN gate do not enter the
+// tomograms; rows past the chunk are zero).
+__global__ void split_prob_kernel(const float *__restrict__ Pst, int Nc, int Nc_pad, int RT,
+                                  __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // 8 values each
+	if (t >= (long long)RT * Nc_pad * 16)
+		return;
+	const long long row = t >> 4;
+	const int rt = (int)(row / Nc_pad), dl = (int)(row - (long long)rt * Nc_pad), j0 = (int)(t & 15) * 8;
+	__align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+	for (int e = 0; e < 8; ++e) {
+		const float p = dl < Nc ? fmaxf(Pst[((size_t)rt * (Nc + 1) + dl) * TILE + j0 + e], 0.f) : 0.f;
+		const __nv_bfloat16 ph = __float2bfloat16_rn(p);
+		h[e] = ph;
+		l[e] = __float2bfloat16_rn(p - __bfloat162float(ph));
+	}
+	const size_t o = (size_t)row * 128 + j0;
+	*reinterpret_cast<uint4 *>(hi + o) = *reinterpret_cast<const uint4 *>(h);
+	*reinterpret_cast<uint4 *>(lo + o) = *reinterpret_cast<const uint4 *>(l);
+}
+
+// hi / lo BF16 log-slices [R_pad][K_pad] (orientation rows, the mask < 2
+// pixels in pixel order; zero on mask-1 pixels, which the likelihood leaves
+// out, and past K) from the FP32 log-slice tiles [RT][P+1][TILE]:
 // x = hi + lo + O(2^-17 |x|), hi = bf16(x), lo = bf16(x - hi). A log of zero
 // (-inf) becomes -1e30 so that a zero count times it stays zero. Block = one
 // orientation tile x 64 pixels, transposed through shared memory.
 __global__ void __launch_bounds__(256) split_logw_kernel(const float *__restrict__ logW, int P,
-                                                         const int *__restrict__ kpix, int K, int K_pad,
+                                                         const int *__restrict__ kpix,
+                                                         const uint8_t *__restrict__ mask, int K, int K_pad,
                                                          __nv_bfloat16 *__restrict__ hi,
                                                          __nv_bfloat16 *__restrict__ lo) {
 	__shared__ float s[DK][128 + 1];
@@ -310,7 +485,7 @@ __global__ void __launch_bounds__(256) split_logw_kernel(const float *__restrict
 	for (int idx = t; idx < DK * 128; idx += 256) {
 		const int row = idx >> 7, col = idx & 127, k = kb * DK + row;
 		float v = 0.f;
-		if (k < K)
+		if (k < K && mask[kpix[k]] == 0)  // mask-1 columns hold the M-step's photons only
 			v = logW[((size_t)rt * (P + 1) + kpix[k]) * TILE + col];
 		s[row][col] = v;
 	}
@@ -332,27 +507,28 @@ __global__ void __launch_bounds__(256) split_logw_kernel(const float *__restrict
 	}
 }
 
-// Counts of one frame chunk as BF16 rows [Nc_pad][K_pad] over the mask-0
-// pixels (the buffer is zeroed before): one warp per frame scatters its
-// E-step photon words (counts <= 256, one word per pixel).
-__global__ void densify_counts_kernel(const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
-                                      const long long *__restrict__ ph_mid, const int *__restrict__ pcol, int d0,
-                                      int Nc, int P, int K_pad, __nv_bfloat16 *__restrict__ cnt) {
-	const int dl = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-	if (dl >= Nc)
+// Counts of one frame chunk as BF16 rows [Nc_pad][K_pad] over the mask < 2
+// pixels (the buffer is zeroed before): one warp per pixel with photons
+// scatters the M-step index words of the chunk (counts <= 256, so one word
+// per frame and pixel; padding words name frame Nc).
+__global__ void densify_counts_kernel(const uint32_t *__restrict__ cs, const long long *__restrict__ cs_off,
+                                      const long long *__restrict__ cs_mid, const int *__restrict__ pix,
+                                      int npix, const int *__restrict__ pcol, int Nc, int K_pad,
+                                      __nv_bfloat16 *__restrict__ cnt) {
+	const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+	if (w >= npix)
 		return;
-	const int d = d0 + dl;
-	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
+	const int p = pix[w], col = pcol[p];
+	if (col < 0)
+		return;
+	const long long beg = cs_off[p], mid = cs_mid[p], end = cs_off[p + 1];
 	for (long long j = beg + lane; j < end; j += 32) {
-		const uint32_t w = ph[j];
-		const uint32_t idx = j < mid ? w : (w & IDX_MASK);
-		if (idx >= (uint32_t)P)
+		const uint32_t word = cs[j];
+		const uint32_t idx = j < mid ? word : (word & IDX_MASK);
+		if (idx >= (uint32_t)Nc)
 			continue;
-		const int k = pcol[idx];
-		if (k < 0)
-			continue;
-		const uint32_t c = j < mid ? 1u : (w >> IDX_BITS);
-		cnt[(size_t)dl * K_pad + k] = __float2bfloat16_rn((float)c);
+		const uint32_t c = j < mid ? 1u : (word >> IDX_BITS);
+		cnt[(size_t)idx * K_pad + col] = __float2bfloat16_rn((float)c);
 	}
 }
 

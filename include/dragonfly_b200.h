@@ -236,15 +236,17 @@ DFG_API int dfg_slice_gen_noalloc(dfg_ctx *ctx, const double *quat, int mode, do
 DFG_API int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double alpha, double *out);
 
 /* Autotuner: on the context's current inputs, times the slice kernel with
- * 128, 64, 32 and 16 orientations per block and the E-step photon term in its
- * sparse (gathers) and dense (tensor-core) forms on the first frame chunk, and
- * keeps the fastest of each for later iterations when option autotune is 1
- * (with option autotune, dfg_maximize / dfg_run_iteration tune by themselves
- * whenever the inputs changed). report[8] (may be NULL): slice ms per block
- * size (-1: not tried), sparse and dense E-step ms (-1: form refused), the
- * chosen block and form (0 sparse, 1 dense). */
+ * 128, 64, 32 and 16 orientations per block, and the E-step photon term and
+ * the M-step each in their sparse (gathers) and dense (tensor-core) forms on
+ * the first frame chunk, and keeps the fastest of each for later iterations
+ * when option autotune is 1 (with option autotune, dfg_maximize /
+ * dfg_run_iteration tune by themselves whenever the inputs changed).
+ * report[10] (may be NULL): slice ms per block size (-1: not tried), sparse
+ * and dense E-step ms (-1: form refused), the chosen block, the chosen forms
+ * (E-step + 2 x M-step, 1 = dense), sparse and dense M-step ms. */
 DFG_API int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *report);
-/* The last autotuner report for the current inputs (DFG_ERR_STATE if none). */
+/* The last autotuner report (10 values) for the current inputs
+ * (DFG_ERR_STATE if none). */
 DFG_API int dfg_get_autotune_report(dfg_ctx *ctx, double *report);
 
 /* ---- batches of independent reconstructions -------------------------------
@@ -324,9 +326,10 @@ DFG_API int dfg_reset_phase_times(dfg_ctx *ctx);
 /* Sizes of the last iteration: out[0] = R (modes * num_rot), out[1] = frames,
  * out[2] = photon entries in the E-step lists, out[3] = M-step entries,
  * out[4] = frame chunks, out[5] = frames per chunk, out[6] = kernels launched
- * by this context so far, out[7] = mask-0 pixel columns of the dense form
- * (padded to 64; 0 before it is used), out[8] = 1 when the last iteration's
- * E-step took the dense form. out must hold 9 values. */
+ * by this context so far, out[7] = mask < 2 pixel columns of the dense forms
+ * (padded to 64; 0 before it is used), out[8] = forms of the last
+ * iteration: 1 = dense E-step, 2 = dense M-step (bits). out must hold 9
+ * values. */
 DFG_API int dfg_get_workload(dfg_ctx *ctx, long long *out);
 
 #ifdef __cplusplus

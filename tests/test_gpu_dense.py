@@ -29,11 +29,12 @@ def _synth():
                       d["count_multi"], d["quats"], d["model_start"], beta=1.)
 
 
+@pytest.mark.parametrize("forms", [(1, 0), (0, 1), (1, 1)], ids=["estep", "mstep", "both"])
 @pytest.mark.parametrize("case", ["beta1", "scaling", "modes2", "synth300"])
-def test_dense_estep_matches_sparse_and_oracle(oracle_built, case):
+def test_dense_estep_matches_sparse_and_oracle(oracle_built, case, forms):
     prob = _synth() if case == "synth300" else load_case(case)[0]
     sparse = GPUEngine(prob)
-    dense = GPUEngine(prob, estep_form=1)
+    dense = GPUEngine(prob, estep_form=forms[0], mstep_form=forms[1])
     orc = OracleEngine(prob)
     mo = np.concatenate([[0], np.cumsum(prob.multi)])
     cm = np.concatenate([[0], np.cumsum(prob.count_multi)])
@@ -49,8 +50,8 @@ def test_dense_estep_matches_sparse_and_oracle(oracle_built, case):
         dev = rel_l2(a["model1"], o["model1"])
         dev_sparse = rel_l2(b["model1"], o["model1"])
         agree = float(np.mean(np.asarray(a["rmax"]) == np.asarray(o["rmax"])))
-        print("dense %s iteration %d: max_exp %.2e / photon, ll %.2e, model %.2e (sparse %.2e), rmax %.4f"
-              % (case, it, per_photon, ll, dev, dev_sparse, agree))
+        print("dense %s %s iteration %d: max_exp %.2e / photon, ll %.2e, model %.2e (sparse %.2e), rmax %.4f"
+              % (forms, case, it, per_photon, ll, dev, dev_sparse, agree))
         assert per_photon <= MAXEXP_ABS_PER_PHOTON, per_photon
         assert ll <= LL_REL and dev <= MODEL_REL_L2 and agree >= RMAX_AGREE, (ll, dev, agree)
         # both engines continue from the oracle's model, so the errors do not compound
@@ -75,6 +76,8 @@ def test_autotuner_times_both_forms_and_keeps_the_fastest(oracle_built, case):
     assert rep["slice_block"] == min(rep["slice_ms"], key=rep["slice_ms"].get)
     assert rep["estep_sparse_ms"] > 0 and rep["estep_dense_ms"] is not None and rep["estep_dense_ms"] > 0
     assert rep["estep_form"] == int(rep["estep_dense_ms"] < rep["estep_sparse_ms"])
+    assert rep["mstep_sparse_ms"] > 0 and rep["mstep_dense_ms"] > 0
+    assert rep["mstep_form"] == int(rep["mstep_dense_ms"] < rep["mstep_sparse_ms"])
     # iterations with the tuned choice agree with the plain sparse form
     plain = GPUEngine(prob)
     orc = OracleEngine(prob)
