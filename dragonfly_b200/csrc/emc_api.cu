@@ -676,6 +676,7 @@ static int ensure_buffers(dfg_ctx *ctx) {
 	CK(ctx->Pst.ensure((size_t)ctx->R_pad * (ctx->chunk_frames + 1)));
 	CK(ctx->tmax.ensure((size_t)ctx->RT * ctx->chunk_frames));
 	CK(ctx->targ.ensure((size_t)ctx->RT * ctx->chunk_frames));
+	CK(ctx->tlive.ensure((size_t)ctx->RT * (ctx->chunk_frames + 1)));
 	const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
 	CK(ctx->psum_part.ensure((size_t)nsplit * ctx->R_pad));
 	return DFG_OK;
@@ -1145,6 +1146,13 @@ static int launch_slices(dfg_ctx *ctx, int ob, double *Wd) {
 
 // The E-step of one frame chunk: the tensor-core products (dense: counts
 // densified first) or the sparse gathers (background-aware with bg).
+// Tile skipping: the normalisation treats (tile, frame) pairs whose tile
+// maximum can keep no pair as dead (not read, no probability written, flagged
+// in tlive) and psum, the M-step and the probability split skip them. It pays
+// where most tiles are dead (refinement, option tile_skip); elsewhere the
+// plain kernels run and every probability row is written.
+static bool tile_skipping(const dfg_ctx *ctx) { return ctx->refine || ctx->mstep_skip; }
+
 // One chunk's photon counts as BF16 rows over the mask < 2 pixel columns
 // (for the dense E-step and M-step).
 static int launch_densify(dfg_ctx *ctx, const Chunk &ch) {
@@ -1167,7 +1175,8 @@ static int launch_mstep(dfg_ctx *ctx, const Chunk &ch, bool dense) {
 	if (dense) {
 		const int rows = ctx->cnt_rows;
 		split_prob_kernel<<<blocks_for((long long)RT * rows * 16, 256), 256, 0, st>>>(
-		    ctx->Pst.p, Nc, rows, RT, (__nv_bfloat16 *)ctx->Phi.p, (__nv_bfloat16 *)ctx->Plo.p);
+		    ctx->Pst.p, Nc, rows, RT, tile_skipping(ctx) ? ctx->tlive.p : nullptr, (__nv_bfloat16 *)ctx->Phi.p,
+		    (__nv_bfloat16 *)ctx->Plo.p);
 		CKL("split_prob_kernel");
 		const int n_tiles = ctx->K_pad / DN + (ctx->K_pad % DN ? 1 : 0);
 		mstep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
@@ -1178,8 +1187,12 @@ static int launch_mstep(dfg_ctx *ctx, const Chunk &ch, bool dense) {
 	}
 	if (ch.npix > 0) {
 		const long long warps = (long long)RT * ch.npix;
-		mstep_kernel<<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p,
-		                                                    ch.pix.p, ch.npix, P, RT, ctx->T.p);
+		if (tile_skipping(ctx))
+			mstep_kernel<true><<<blocks_for(warps, 8), 256, 0, st>>>(
+			    ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p, ctx->tlive.p);
+		else
+			mstep_kernel<false><<<blocks_for(warps, 8), 256, 0, st>>>(
+			    ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p, ctx->tlive.p);
 		CKL("mstep_kernel");
 	}
 	return DFG_OK;
@@ -1224,18 +1237,25 @@ static int launch_estep(dfg_ctx *ctx, const Chunk &ch, int use_scale, bool bg, c
 static int launch_norm(dfg_ctx *ctx, const Chunk &ch, int psum_d_on, bool bg) {
 	cudaStream_t st = ctx->stream;
 	const int Nc = ch.nc, RT = ctx->RT, R = ctx->R, M = ctx->M;
-	if (M > 1)
-		norm_kernel<true><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
-		    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
-		    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
-		    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
-		    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
-	else
-		norm_kernel<false><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(
-		    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,
-		    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p,
-		    ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p,
-		    ctx->num_prob.p, bg ? ctx->Pd.p : nullptr);
+	const int zero_dead = (ctx->keep_prob || bg) ? 1 : 0;
+#define DFG_NORM(MUL, SK)                                                                                     \
+	norm_kernel<MUL, SK><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(                                               \
+	    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,        \
+	    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p, ctx->max_exp.p, \
+	    ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p, ctx->num_prob.p,       \
+	    bg ? ctx->Pd.p : nullptr, ctx->tlive.p, zero_dead)
+	if (tile_skipping(ctx)) {
+		if (M > 1)
+			DFG_NORM(true, true);
+		else
+			DFG_NORM(false, true);
+	} else {
+		if (M > 1)
+			DFG_NORM(true, false);
+		else
+			DFG_NORM(false, false);
+	}
+#undef DFG_NORM
 	CKL("norm_kernel");
 	return DFG_OK;
 }
@@ -1314,7 +1334,8 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 			const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
 			const int fps = (Nc + nsplit - 1) / nsplit;
 			psum_r_kernel<<<dim3(RT, nsplit), 256, 0, st>>>(ctx->Pst.p, Nc, ch.d0, fps, ctx->scale.p,
-			                                                par->need_scaling, ctx->psum_part.p, R_pad);
+			                                                par->need_scaling, ctx->psum_part.p, R_pad,
+			                                                tile_skipping(ctx) ? ctx->tlive.p : nullptr);
 			CKL("psum_r_kernel");
 			psum_r_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->psum_part.p, nsplit, R, R_pad,
 			                                                          ctx->psum_r.p);
@@ -2344,6 +2365,10 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 		const int v = (int)value;
 		NEED(v == 0 || v == 1, DFG_ERR_ARG, "estep_form must be 0 (sparse) or 1 (dense)");
 		ctx->estep_form = v;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "tile_skip")) {
+		ctx->mstep_skip = value != 0.;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "mstep_form")) {

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(256, 3) estep_bg_kernel(
 	const int r0 = rt * TILE + lane * LW;
 	const unsigned live = refine_live(rm, d, r0);
 	if (rm.qmap != nullptr && !__any_sync(FULL, live)) {
-		refine_skip_tile(pval, tmax, targ, rt, Nc, dl, lane);
+		refine_skip_tile(tmax, targ, rt, Nc, dl, lane);
 		return;
 	}
 	const double *L = Wsl + (size_t)rt * (P + 1) * TILE + lane * LW;

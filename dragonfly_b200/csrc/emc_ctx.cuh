@@ -132,6 +132,8 @@ struct dfg_ctx {
 	DevBuf<double> logw;  // log w_r per orientation
 	DevBuf<int> rmax, num_prob, targ;
 	DevBuf<double> tmax;  // per (tile, frame) maximum of pval and its first orientation
+	DevBuf<uint8_t> tlive;  // [RT][Nc + 1]: the (tile, frame) has a kept pair (norm_kernel)
+	bool mstep_skip = false;  // option tile_skip: skip dead (tile, frame) pairs without refinement
 	DevBuf<double> info, likelihood, max_exp, p_norm, psum_d, quat_norm;
 	std::vector<Chunk> chunks;
 	int chunk_frames = 0;

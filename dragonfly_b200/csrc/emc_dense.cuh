@@ -448,18 +448,21 @@ __global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
 
 // Probabilities of one chunk as BF16 hi / lo rows [RT][Nc_pad][128]
 // (p = max(Pst, 0): pairs at or below the PROB_MIN gate do not enter the
-// tomograms; rows past the chunk are zero).
+// tomograms; rows past the chunk and of dead tiles are zero).
 __global__ void split_prob_kernel(const float *__restrict__ Pst, int Nc, int Nc_pad, int RT,
-                                  __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+                                  const uint8_t *__restrict__ tlive, __nv_bfloat16 *__restrict__ hi,
+                                  __nv_bfloat16 *__restrict__ lo) {
 	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // 8 values each
 	if (t >= (long long)RT * Nc_pad * 16)
 		return;
 	const long long row = t >> 4;
 	const int rt = (int)(row / Nc_pad), dl = (int)(row - (long long)rt * Nc_pad), j0 = (int)(t & 15) * 8;
+	// with tile skipping, dead tiles hold no probability (tlive)
+	const bool live = dl < Nc && (tlive == nullptr || tlive[(size_t)rt * (Nc + 1) + dl]);
 	__align__(16) __nv_bfloat16 h[8], l[8];
 #pragma unroll
 	for (int e = 0; e < 8; ++e) {
-		const float p = dl < Nc ? fmaxf(Pst[((size_t)rt * (Nc + 1) + dl) * TILE + j0 + e], 0.f) : 0.f;
+		const float p = live ? fmaxf(Pst[((size_t)rt * (Nc + 1) + dl) * TILE + j0 + e], 0.f) : 0.f;
 		const __nv_bfloat16 ph = __float2bfloat16_rn(p);
 		h[e] = ph;
 		l[e] = __float2bfloat16_rn(p - __bfloat162float(ph));

@@ -265,15 +265,11 @@ __device__ __forceinline__ unsigned refine_live(const RefineMask &rm, int d, int
 	return live;
 }
 
-// A (tile, frame) task with no evaluated pair: -inf log-likelihoods and an
-// empty tile maximum.
-__device__ __forceinline__ void refine_skip_tile(double *__restrict__ pval, double *__restrict__ tmax,
-                                                 int *__restrict__ targ, int rt, int Nc, int dl, int lane) {
-	double ninf[LW];
-#pragma unroll
-	for (int k = 0; k < LW; ++k)
-		ninf[k] = -INFINITY;
-	st_row(pval + ((size_t)rt * Nc + dl) * TILE + lane * LW, ninf);
+// A (tile, frame) task with no evaluated pair: an empty tile maximum, which
+// makes the normalisation treat the tile as dead without reading its
+// log-likelihoods (so none are written).
+__device__ __forceinline__ void refine_skip_tile(double *__restrict__ tmax, int *__restrict__ targ, int rt,
+                                                 int Nc, int dl, int lane) {
 	if (lane == 0) {
 		tmax[(size_t)rt * Nc + dl] = MAX_EXP_START;
 		targ[(size_t)rt * Nc + dl] = -1;
@@ -299,7 +295,7 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 	if constexpr (REFINE) {
 		live = refine_live(rm, d, r0);
 		if (!__any_sync(FULL, live)) {
-			refine_skip_tile(pval, tmax, targ, rt, Nc, dl, lane);
+			refine_skip_tile(tmax, targ, rt, Nc, dl, lane);
 			return;
 		}
 	}
@@ -412,7 +408,7 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 #ifndef DFG_NORM_MINB
 #define DFG_NORM_MINB 4
 #endif
-template <bool MULTI>
+template <bool MULTI, bool SKIP>
 __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
     const double *__restrict__ pval, const double *__restrict__ tmax, const int *__restrict__ targ, int RT,
     int Nc, int d0, int R, int M, const double *__restrict__ logw, const double *__restrict__ u,
@@ -420,7 +416,7 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
     int psum_d_on, const double *__restrict__ scalars, float *__restrict__ Pst, int *__restrict__ rmax,
     double *__restrict__ max_exp, double *__restrict__ p_norm, double *__restrict__ info,
     double *__restrict__ likelihood, double *__restrict__ psum_d, double *__restrict__ quat_norm,
-    int *__restrict__ num_prob, double *__restrict__ Pd) {
+    int *__restrict__ num_prob, double *__restrict__ Pd, uint8_t *__restrict__ tlive, int zero_dead) {
 	constexpr int UNR = LW == 1 ? 4 : 2;
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
@@ -433,11 +429,14 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 #pragma unroll
 	for (int k = 0; k < LW; ++k)
 		zerod[k] = 0.;
+	const size_t lstride = (size_t)Nc + 1;  // tlive [RT][Nc + 1]
 	if (warp == Nc) {  // the zero row that padding words of the M-step point at
 		for (int rt = 0; rt < RT; ++rt) {
 			st_row(Pst + rt * pstride + (size_t)Nc * TILE + lane * LW, zero);
 			if (Pd != nullptr)
 				st_row(Pd + rt * pstride + (size_t)Nc * TILE + lane * LW, zerod);
+			if (SKIP && lane == 0)
+				tlive[rt * lstride + Nc] = 0;
 		}
 		return;
 	}
@@ -470,9 +469,13 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 	}
 	if (bl || m == MAX_EXP_START) {
 		for (int rt = 0; rt < RT; ++rt) {
-			st_row(ps + rt * pstride, zero);
-			if (Pd != nullptr)
-				st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, zerod);
+			if (!SKIP || zero_dead) {
+				st_row(ps + rt * pstride, zero);
+				if (Pd != nullptr)
+					st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, zerod);
+			}
+			if (SKIP && lane == 0)
+				tlive[rt * lstride + dl] = 0;
 		}
 		if (lane == 0) {
 			rmax[d] = -1;
@@ -492,18 +495,38 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 	const double lo = dsub(m, thr);
 	const int rstar = am;
 
+	// a tile whose maximum can keep no pair is dead: its log-likelihoods are
+	// not read, its probabilities are zero (written only with zero_dead), and
+	// tlive tells the later phases to skip it
+	auto dead = [&](int rt) {
+		if constexpr (!SKIP)
+			return false;
+		const double t = tmax[(size_t)rt * Nc + dl];
+		return !(t > lo) && !(dadd(t, thr) > m);
+	};
 	double s = 0.;
 	int cnt = 0;
 	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
 		double v[UNR][LW];
+		bool dd[UNR];
 #pragma unroll
-		for (int k = 0; k < UNR; ++k)
-			if (rt0 + k < RT)
-				ld_row(pv + (rt0 + k) * tstride, v[k]);
+		for (int k = 0; k < UNR; ++k) {
+			if constexpr (SKIP) {
+				dd[k] = rt0 + k >= RT || dead(rt0 + k);
+				if (!dd[k])
+					ld_row(pv + (rt0 + k) * tstride, v[k]);
+			} else {
+				dd[k] = false;
+				if (rt0 + k < RT)
+					ld_row(pv + (rt0 + k) * tstride, v[k]);
+			}
+		}
 #pragma unroll
 		for (int k = 0; k < UNR; ++k) {
 			if (rt0 + k >= RT)
 				break;
+			if (SKIP && dd[k])
+				continue;
 #pragma unroll
 			for (int e = 0; e < LW; ++e) {
 				const int r = (rt0 + k) * TILE + lane * LW + e;
@@ -530,15 +553,34 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 		qn[k] = 0.;
 	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
 		double v[UNR][LW];
+		bool dd[UNR];
 #pragma unroll
-		for (int k = 0; k < UNR; ++k)
-			if (rt0 + k < RT)
-				ld_row(pv + (rt0 + k) * tstride, v[k]);
+		for (int k = 0; k < UNR; ++k) {
+			if constexpr (SKIP) {
+				dd[k] = rt0 + k >= RT || dead(rt0 + k);
+				if (!dd[k])
+					ld_row(pv + (rt0 + k) * tstride, v[k]);
+			} else {
+				dd[k] = false;
+				if (rt0 + k < RT)
+					ld_row(pv + (rt0 + k) * tstride, v[k]);
+			}
+		}
 #pragma unroll
 		for (int k = 0; k < UNR; ++k) {
 			const int rt = rt0 + k;
 			if (rt >= RT)
 				break;
+			if (SKIP && lane == 0)
+				tlive[rt * lstride + dl] = dd[k] ? 0 : 1;
+			if (SKIP && dd[k]) {
+				if (zero_dead) {
+					st_row(ps + rt * pstride, zero);
+					if (Pd != nullptr)
+						st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, zerod);
+				}
+				continue;
+			}
 			float out[LW];
 			double outd[LW];
 #pragma unroll
@@ -600,7 +642,8 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 // (max_update.c:108-116). Grid (RT, splits), 8 warps per block; fixed order.
 __global__ void __launch_bounds__(256) psum_r_kernel(const float *__restrict__ Pst, int Nc, int d0,
                                                       int frames_per_split, const double *__restrict__ scale,
-                                                      int need_scaling, double *__restrict__ part, int R_pad) {
+                                                      int need_scaling, double *__restrict__ part, int R_pad,
+                                                      const uint8_t *__restrict__ tlive) {
 	__shared__ double s[8][TILE];
 	const int rt = blockIdx.x, split = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int beg = split * frames_per_split, end = min(Nc, beg + frames_per_split);
@@ -609,7 +652,10 @@ __global__ void __launch_bounds__(256) psum_r_kernel(const float *__restrict__ P
 	for (int k = 0; k < LW; ++k)
 		acc[k] = 0.;
 	const float *p = Pst + (size_t)rt * (Nc + 1) * TILE + lane * LW;
+	const uint8_t *live = tlive ? tlive + (size_t)rt * (Nc + 1) : nullptr;
 	for (int dl = beg + w; dl < end; dl += 8) {
+		if (live && !live[dl])  // dead tile: no probability (norm_kernel with tile skipping)
+			continue;
 		float v[LW];
 		ld_row(p + (size_t)dl * TILE, v);
 		const double f = need_scaling ? scale[d0 + dl] : 1.;
@@ -653,12 +699,13 @@ __global__ void psum_r_reduce_kernel(const double *__restrict__ part, int nsplit
 // pairing). No atomics; pixels are visited heaviest first for balance.
 constexpr int MSTEP_MINB = LW == 4 ? 4 : 6;
 
+template <bool SKIP>
 __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__restrict__ Pst, int Nc,
                                                      const uint32_t *__restrict__ cs,
                                                      const long long *__restrict__ cs_off,
                                                      const long long *__restrict__ cs_mid,
                                                      const int *__restrict__ pix, int npix, int P, int RT,
-                                                     float *__restrict__ T) {
+                                                     float *__restrict__ T, const uint8_t *__restrict__ tlive) {
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * npix)
@@ -666,6 +713,16 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 	const int rt = (int)(warp / npix), kp = (int)(warp - (long long)rt * npix);
 	const int p = pix[kp];
 	const float *Pr = Pst + (size_t)rt * (Nc + 1) * TILE + lane * LW;
+	// SKIP: frames whose tile is dead (norm_kernel) read the chunk's zero row
+	// instead (cached), so their probability rows are never fetched
+	const uint8_t *live = tlive + (size_t)rt * (Nc + 1);
+	const uint32_t zrow = (uint32_t)Nc;
+	auto lv = [&](uint32_t f) {
+		if constexpr (SKIP)
+			return live[f] ? f : zrow;
+		else
+			return f;
+	};
 	const long long beg = cs_off[p], mid = cs_mid[p], end = cs_off[p + 1];
 	const uint4 *w4 = reinterpret_cast<const uint4 *>(cs);
 	float s[ECH][LW], c[ECH][LW];
@@ -688,15 +745,26 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 			b = __ldg(w4 + (beg >> 2) + 1);
 		}
 		for (long long j = beg; j < mid; j += 8) {
+			if constexpr (SKIP) {
+				// a group of 8 frames without a live tile adds nothing
+				if (!(live[a.x] | live[a.y] | live[a.z] | live[a.w] | live[b.x] | live[b.y] | live[b.z] |
+				      live[b.w])) {
+					if (j + 8 < mid) {
+						a = __ldg(w4 + ((j + 8) >> 2));
+						b = __ldg(w4 + ((j + 8) >> 2) + 1);
+					}
+					continue;
+				}
+			}
 			f32x2 v[8][NP];
-			ld_pairs(Pr + a.x * TILE, v[0]);
-			ld_pairs(Pr + a.y * TILE, v[1]);
-			ld_pairs(Pr + a.z * TILE, v[2]);
-			ld_pairs(Pr + a.w * TILE, v[3]);
-			ld_pairs(Pr + b.x * TILE, v[4]);
-			ld_pairs(Pr + b.y * TILE, v[5]);
-			ld_pairs(Pr + b.z * TILE, v[6]);
-			ld_pairs(Pr + b.w * TILE, v[7]);
+			ld_pairs(Pr + lv(a.x) * TILE, v[0]);
+			ld_pairs(Pr + lv(a.y) * TILE, v[1]);
+			ld_pairs(Pr + lv(a.z) * TILE, v[2]);
+			ld_pairs(Pr + lv(a.w) * TILE, v[3]);
+			ld_pairs(Pr + lv(b.x) * TILE, v[4]);
+			ld_pairs(Pr + lv(b.y) * TILE, v[5]);
+			ld_pairs(Pr + lv(b.z) * TILE, v[6]);
+			ld_pairs(Pr + lv(b.w) * TILE, v[7]);
 			if (j + 8 < mid) {
 				a = __ldg(w4 + ((j + 8) >> 2));
 				b = __ldg(w4 + ((j + 8) >> 2) + 1);
@@ -713,10 +781,18 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 		for (long long j = mid; j < end; j += 8) {
 			const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
 			const uint32_t e[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+			if constexpr (SKIP) {
+				uint32_t any = 0;
+#pragma unroll
+				for (int q = 0; q < 8; ++q)
+					any |= live[e[q] & IDX_MASK];
+				if (!any)
+					continue;
+			}
 			f32x2 v[8][NP];
 #pragma unroll
 			for (int q = 0; q < 8; ++q)
-				ld_pairs(Pr + (e[q] & IDX_MASK) * TILE, v[q]);
+				ld_pairs(Pr + lv(e[q] & IDX_MASK) * TILE, v[q]);
 #pragma unroll
 			for (int q = 0; q < 8; ++q)
 #pragma unroll
@@ -736,14 +812,14 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 	for (long long j = beg; j < mid; j += 8) {
 		const uint4 a = __ldg(w4 + (j >> 2)), b = __ldg(w4 + (j >> 2) + 1);
 		float v[8][LW];
-		ld_row(Pr + a.x * TILE, v[0]);
-		ld_row(Pr + a.y * TILE, v[1]);
-		ld_row(Pr + a.z * TILE, v[2]);
-		ld_row(Pr + a.w * TILE, v[3]);
-		ld_row(Pr + b.x * TILE, v[4]);
-		ld_row(Pr + b.y * TILE, v[5]);
-		ld_row(Pr + b.z * TILE, v[6]);
-		ld_row(Pr + b.w * TILE, v[7]);
+		ld_row(Pr + lv(a.x) * TILE, v[0]);
+		ld_row(Pr + lv(a.y) * TILE, v[1]);
+		ld_row(Pr + lv(a.z) * TILE, v[2]);
+		ld_row(Pr + lv(a.w) * TILE, v[3]);
+		ld_row(Pr + lv(b.x) * TILE, v[4]);
+		ld_row(Pr + lv(b.y) * TILE, v[5]);
+		ld_row(Pr + lv(b.z) * TILE, v[6]);
+		ld_row(Pr + lv(b.w) * TILE, v[7]);
 #pragma unroll
 		for (int q = 0; q < 8; ++q)
 #pragma unroll
@@ -756,7 +832,7 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 		float v[8][LW];
 #pragma unroll
 		for (int q = 0; q < 8; ++q)
-			ld_row(Pr + (e[q] & IDX_MASK) * TILE, v[q]);
+			ld_row(Pr + lv(e[q] & IDX_MASK) * TILE, v[q]);
 #pragma unroll
 		for (int q = 0; q < 8; ++q)
 #pragma unroll
