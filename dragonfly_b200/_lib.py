@@ -75,8 +75,24 @@ _SIGS = {
     "dfg_batch_set_lanes": (C.c_int, [_V, C.c_int]),
     "dfg_batch_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
     "dfg_batch_destroy": (None, [_V]),
+    "dfg_pnet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_V)]),
+    "dfg_pnet_destroy": (None, [_V]),
+    "dfg_pnet_last_error": (C.c_char_p, [_V]),
+    "dfg_pnet_num_params": (C.c_longlong, [_V]),
+    "dfg_pnet_get_params": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "dfg_pnet_set_params": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "dfg_pnet_set_bins": (C.c_int, [_V, C.c_int, _I]),
+    "dfg_pnet_load_frames": (C.c_int, [_V, _V]),
+    "dfg_pnet_set_images": (C.c_int, [_V, C.c_longlong, C.POINTER(C.c_float)]),
+    "dfg_pnet_get_images": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "dfg_pnet_train": (C.c_int, [_V, _I, C.c_int, C.c_double, C.c_ulonglong, _D]),
+    "dfg_pnet_topk": (C.c_int, [_V, C.c_int, _I]),
+    "dfg_pnet_logits": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "dfg_pnet_gradients": (C.c_int, [_V, _I, C.POINTER(C.c_float), _D]),
     "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
     "dfg_voronoi_subset": (C.c_int, [_V, C.c_int, _D, C.c_int, _D, _I]),
+    "dfg_set_watch": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_longlong), _I]),
+    "dfg_get_watch_mass": (C.c_int, [_V, _D]),
     "dfg_set_bgscale": (C.c_int, [_V, _D]),
     "dfg_get_sparse_prob_offsets": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
     "dfg_get_sparse_prob": (C.c_int, [_V, _I, _D]),
@@ -169,6 +185,7 @@ class Context:
             raise ValueError("qvals must be [P,3], corr and mask [P]")
         self.call("dfg_set_detector", c.size, ptr(q, C.c_double), ptr(c, C.c_double), ptr(m, C.c_uint8))
         self.num_pix = c.size
+        self._qvals, self._corr, self._mask = q.reshape(-1, 3), c, m
 
     def set_frames(self, ones, multi, place_ones, place_multi, count_multi):
         a = [np.ascontiguousarray(x, np.int32) for x in (ones, multi, place_ones, place_multi, count_multi)]
@@ -236,6 +253,25 @@ class Context:
                                     if len(lens) else np.zeros(0, np.int32), np.int32)
         self.call("dfg_set_refinement", int(num_coarse), ptr(qm, C.c_int), ptr(off, C.c_longlong),
                   ptr(flat, C.c_int))
+
+    def set_watch(self, frames, cells):
+        """Watched frames (ascending) with a coarse-cell list each; None clears."""
+        if frames is None or len(frames) == 0:
+            self.call("dfg_set_watch", 0, None, None, None)
+            self._n_watch = 0
+            return
+        fr = np.ascontiguousarray(frames, np.int32)
+        lens = np.array([len(x) for x in cells], np.int64)
+        off = np.zeros(len(lens) + 1, np.int64)
+        np.cumsum(lens, out=off[1:])
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in cells]), np.int32)
+        self.call("dfg_set_watch", fr.size, ptr(fr, C.c_int), ptr(off, C.c_longlong), ptr(flat, C.c_int))
+        self._n_watch = fr.size
+
+    def watch_mass(self):
+        out = np.zeros(self._n_watch)
+        self.call("dfg_get_watch_mass", ptr(out, C.c_double))
+        return out
 
     def voronoi_subset(self, coarse, fine):
         """Nearest coarse orientation of every fine one (rows of five)."""
@@ -523,6 +559,105 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             self.lib.dfg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ProposalNet:
+    """Orientation-proposal network on the GPU (dfg_pnet_*): 32 x 32 binned
+    log(1 + photons) frame images -> logits over num_classes coarse
+    orientations; trained and evaluated by the library's own kernels."""
+
+    IMG = 32
+
+    def __init__(self, num_classes, batch=256, seed=1, device=0):
+        self.lib = load()
+        h = _V()
+        rc = self.lib.dfg_pnet_create(int(device), int(num_classes), int(batch), int(seed), C.byref(h))
+        if rc != DFG_OK:
+            raise DFGError(rc, "dfg_pnet_create failed")
+        self.h = h
+        self.num_classes = int(num_classes)
+        self.n_images = 0
+
+    def _call(self, name, *args):
+        rc = getattr(self.lib, name)(self.h, *args)
+        if rc != DFG_OK:
+            raise DFGError(rc, self.lib.dfg_pnet_last_error(self.h).decode())
+
+    @property
+    def num_params(self):
+        return int(self.lib.dfg_pnet_num_params(self.h))
+
+    def params(self):
+        out = np.zeros(self.num_params, np.float32)
+        self._call("dfg_pnet_get_params", ptr(out, C.c_float))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._call("dfg_pnet_set_params", ptr(p, C.c_float))
+
+    @staticmethod
+    def pixel_bins(qvals, qmax=None):
+        """Bin of every pixel on a 32 x 32 grid over the detector plane
+        (qx, qy within +-qmax), -1 outside."""
+        q = np.asarray(qvals, np.float64).reshape(-1, 3)
+        qmax = float(np.abs(q[:, :2]).max()) * 1.0001 if qmax is None else float(qmax)
+        ix = np.floor((q[:, 0] + qmax) / (2 * qmax) * ProposalNet.IMG).astype(np.int64)
+        iy = np.floor((q[:, 1] + qmax) / (2 * qmax) * ProposalNet.IMG).astype(np.int64)
+        ok = (ix >= 0) & (ix < ProposalNet.IMG) & (iy >= 0) & (iy < ProposalNet.IMG)
+        return np.where(ok, ix * ProposalNet.IMG + iy, -1).astype(np.int32)
+
+    def set_bins(self, pixel_bin):
+        b = np.ascontiguousarray(pixel_bin, np.int32)
+        self._call("dfg_pnet_set_bins", b.size, ptr(b, C.c_int))
+
+    def load_frames(self, ctx):
+        self._call("dfg_pnet_load_frames", ctx.h)
+        self.n_images = int(ctx.num_data)
+
+    def set_images(self, images):
+        x = np.ascontiguousarray(images, np.float32).reshape(-1, self.IMG * self.IMG)
+        self._call("dfg_pnet_set_images", x.shape[0], ptr(x, C.c_float))
+        self.n_images = x.shape[0]
+
+    def images(self):
+        out = np.zeros((self.n_images, self.IMG * self.IMG), np.float32)
+        self._call("dfg_pnet_get_images", ptr(out, C.c_float))
+        return out
+
+    def train(self, labels, epochs=1, lr=1e-3, seed=0):
+        lab = np.ascontiguousarray(labels, np.int32)
+        loss = C.c_double(0.)
+        self._call("dfg_pnet_train", ptr(lab, C.c_int), int(epochs), float(lr), int(seed), C.byref(loss))
+        return loss.value
+
+    def topk(self, K):
+        out = np.zeros((self.n_images, int(K)), np.int32)
+        self._call("dfg_pnet_topk", int(K), ptr(out, C.c_int))
+        return out
+
+    def logits(self):
+        out = np.zeros((self.n_images, self.num_classes), np.float32)
+        self._call("dfg_pnet_logits", ptr(out, C.c_float))
+        return out
+
+    def gradients(self, labels):
+        lab = np.ascontiguousarray(labels, np.int32)
+        g = np.zeros(self.num_params, np.float32)
+        loss = C.c_double(0.)
+        self._call("dfg_pnet_gradients", ptr(lab, C.c_int), ptr(g, C.c_float), C.byref(loss))
+        return g, loss.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dfg_pnet_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdfgpu.so")
-SOURCES = ["emc_api.cu", "simulate.cu", "noalloc.cu"]
+SOURCES = ["emc_api.cu", "simulate.cu", "noalloc.cu", "proposal.cu"]
 HEADERS = ["emc_common.cuh", "emc_device.cuh", "emc_ctx.cuh", os.path.join("..", "..", "include", "dragonfly_b200.h")]
 
 NVCC_FLAGS = [

@@ -368,10 +368,49 @@ extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_
 	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->h_qmap.assign(quat_mapping, quat_mapping + ctx->num_rot);
+	if (num_coarse != ctx->num_coarse)
+		ctx->h_watch.clear();  // the cell bits were for another coarse set
 	ctx->num_coarse = num_coarse;
 	ctx->rwords = rw;
 	ctx->refine = true;
 	ctx->qmap_valid = false;
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_watch(dfg_ctx *ctx, int n, const int *frames, const long long *cell_off, const int *cells) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	if (n == 0 || frames == nullptr) {
+		ctx->h_watch.clear();
+		return DFG_OK;
+	}
+	NEED(ctx->refine, DFG_ERR_STATE, "watched frames need refinement (dfg_set_refinement) first");
+	NEED(n > 0 && cell_off && cells && cell_off[0] == 0, DFG_ERR_ARG, "watch: need frames and cell lists");
+	const int rw = ctx->rwords;
+	std::vector<uint32_t> bits((size_t)n * rw, 0u);
+	for (int i = 0; i < n; ++i) {
+		NEED(frames[i] >= 0 && frames[i] < ctx->N && (i == 0 || frames[i] > frames[i - 1]), DFG_ERR_ARG,
+		     "watch: frames must be ascending and in range");
+		for (long long t = cell_off[i]; t < cell_off[i + 1]; ++t) {
+			NEED(cells[t] >= 0 && cells[t] < ctx->num_coarse, DFG_ERR_ARG, "watch: cell %d out of range", cells[t]);
+			bits[(size_t)i * rw + (cells[t] >> 5)] |= 1u << (cells[t] & 31);
+		}
+	}
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->watch_bits, bits.data(), bits.size(), ctx->stream));
+	CK(ctx->watch_local.ensure((size_t)n));
+	CK(ctx->watch_mass.ensure((size_t)n));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->h_watch.assign(frames, frames + n);
+	return DFG_OK;
+}
+
+extern "C" int dfg_get_watch_mass(dfg_ctx *ctx, double *mass) {
+	if (!ctx || !mass)
+		return DFG_ERR_ARG;
+	NEED(!ctx->h_watch.empty(), DFG_ERR_STATE, "no watched frames");
+	CK(cudaSetDevice(ctx->device));
+	CK(cudaMemcpy(mass, ctx->watch_mass.p, ctx->h_watch.size() * sizeof(double), cudaMemcpyDeviceToHost));
 	return DFG_OK;
 }
 
@@ -1053,6 +1092,13 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 		if (int rc = dense_prepare_counts(ctx))
 			return rc;
 	cudaStream_t st = ctx->stream;
+	if (ctx->refine && !ctx->h_watch.empty()) {  // chunk-local indices of the watched frames
+		std::vector<int> local(ctx->h_watch.size());
+		for (size_t i = 0; i < local.size(); ++i)
+			local[i] = ctx->h_watch[i] % ctx->chunk_frames;
+		CK(upload(ctx->watch_local, local.data(), local.size(), st));
+		CK(cudaStreamSynchronize(st));
+	}
 	// recon.pyx:86-91 selects the 3-D or the 2-D slice functions; an RZ
 	// iteration has none there
 	NEED(ctx->model_type != MT_RZ, DFG_ERR_ARG, "RZ models: slice_gen / slice_merge only, no iteration");
@@ -1260,6 +1306,22 @@ static int launch_norm(dfg_ctx *ctx, const Chunk &ch, int psum_d_on, bool bg) {
 	return DFG_OK;
 }
 
+// Captured probability mass of the watched frames that lie in this chunk
+// (their chunk-local indices were uploaded by max_prepare).
+static int launch_watch(dfg_ctx *ctx, const Chunk &ch) {
+	const auto &W = ctx->h_watch;
+	const int lo = (int)(std::lower_bound(W.begin(), W.end(), ch.d0) - W.begin());
+	const int hi = (int)(std::lower_bound(W.begin(), W.end(), ch.d0 + ch.nc) - W.begin());
+	if (hi <= lo)
+		return DFG_OK;
+	captured_mass_kernel<<<blocks_for((long long)(hi - lo) * 32, 256), 256, 0, ctx->stream>>>(
+	    ctx->Pst.p, ctx->RT, ch.nc, tile_skipping(ctx) ? ctx->tlive.p : nullptr, ctx->qmap.p,
+	    ctx->watch_local.p + lo, hi - lo, ctx->watch_bits.p + (size_t)lo * ctx->rwords, ctx->rwords,
+	    ctx->watch_mass.p + lo);
+	CKL("captured_mass_kernel");
+	return DFG_OK;
+}
+
 // Queues maximize's kernels (after max_prepare). Synchronises only where
 // graphable() is false.
 static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
@@ -1324,6 +1386,9 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 		phase_begin(ctx, PH_NORM);
 		if (int rc = launch_norm(ctx, ch, psum_d_on, bg))
 			return rc;
+		if (ctx->refine && !ctx->h_watch.empty())
+			if (int rc = launch_watch(ctx, ch))
+				return rc;
 		phase_end(ctx, PH_NORM, 1);
 		if (ctx->keep_prob)
 			if (int rc = collect_prob(ctx, ch))

@@ -195,6 +195,12 @@ struct dfg_ctx {
 	// [R_pad], -1 past R) and per frame one bit per relevant coarse
 	// orientation (rel_bits, [N][rwords])
 	bool refine = false, qmap_valid = false;
+	// watched frames (refinement): their proposed coarse cells as bits, and
+	// the captured probability mass of each after maximize
+	std::vector<int> h_watch;  // frame indices, ascending
+	DevBuf<int> watch_local;
+	DevBuf<uint32_t> watch_bits;
+	DevBuf<double> watch_mass;
 	int num_coarse = 0, rwords = 0;
 	std::vector<int> h_qmap;
 	DevBuf<int> qmap;

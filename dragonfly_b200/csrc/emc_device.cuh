@@ -1298,6 +1298,43 @@ __global__ void apply_scale_norm_kernel(double *__restrict__ scale, const uint8_
 		scale[i] /= m;
 }
 
+// Captured probability mass of watched frames (learned proposals): for watched
+// frame w (chunk-local frame wl[w]) the sum of |P| over the orientations whose
+// coarse cell qmap[r] is among the frame's proposed cells (bits[w * rwords ..]),
+// divided by the sum over all orientations. Dead tiles (tlive 0) hold no
+// probability. One warp per watched frame of the chunk.
+__global__ void __launch_bounds__(256) captured_mass_kernel(const float *__restrict__ Pst, int RT, int Nc,
+                                                            const uint8_t *__restrict__ tlive,
+                                                            const int *__restrict__ qmap, const int *__restrict__ wl,
+                                                            int nw, const uint32_t *__restrict__ bits, int rwords,
+                                                            double *__restrict__ mass) {
+	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (w >= nw)
+		return;
+	const int dl = wl[w];
+	const size_t pstride = (size_t)(Nc + 1) * TILE;
+	const uint32_t *b = bits + (size_t)w * rwords;
+	double in = 0., all = 0.;
+	for (int rt = 0; rt < RT; ++rt) {
+		if (tlive && !tlive[(size_t)rt * (Nc + 1) + dl])
+			continue;
+		float v[LW];
+		ld_row(Pst + rt * pstride + (size_t)dl * TILE + lane * LW, v);
+#pragma unroll
+		for (int k = 0; k < LW; ++k) {
+			const double p = fabs((double)v[k]);
+			const int c = qmap[rt * TILE + lane * LW + k];
+			all += p;
+			if (c >= 0 && (b[c >> 5] >> (c & 31) & 1u))
+				in += p;
+		}
+	}
+	in = warp_sum(in);
+	all = warp_sum(all);
+	if (lane == 0)
+		mass[w] = all > 0. ? in / all : 0.;
+}
+
 // Nearest coarse orientation of every fine one (voronoi_subset,
 // quaternion.c:844-862): distance 1 - (q . q')^2 with the dot product summed
 // in component order, first coarse index on ties (strict <). One thread per

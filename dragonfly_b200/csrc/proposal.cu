@@ -1,0 +1,843 @@
+// Learned orientation proposals: a small convolutional network that maps a
+// frame's binned photon image to logits over the coarse orientations, trained
+// and evaluated on the GPU by the kernels below (BF16 weights for the
+// products, FP32 activations, accumulation and optimiser state).
+//
+// Network (NHWC activations, batch B):
+//   image [B][32][32][1] = log(1 + photons binned on a 32 x 32 grid of q)
+//   conv1 3x3 stride 1 -> [B][32][32][32], ReLU
+//   conv2 3x3 stride 2 -> [B][16][16][32], ReLU
+//   conv3 3x3 stride 1 -> [B][16][16][64], ReLU
+//   conv4 3x3 stride 2 -> [B][8][8][64],  ReLU   (= [B][4096])
+//   fc1 4096 -> 256, ReLU
+//   fc2 256 -> num_classes (logits)
+// Convolutions are products of im2col matrices [B*Ho*Wo][9*C] with the
+// weights [Cout][9*C] (rows ordered ky, kx, c); the backward pass forms the
+// weight gradients as dY^T . cols, the input gradients as dY . W followed by a
+// gather (col2im, deterministic). Loss: softmax cross-entropy against a class
+// label per frame. Optimiser: Adam on FP32 master weights, BF16 copies for the
+// products. No counterpart in the reference (its E-step searches every
+// orientation).
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <random>
+
+#include "emc_ctx.cuh"
+
+namespace {
+
+constexpr int IMG = 32;  // image side
+constexpr int NL = 6;    // layers
+
+struct LayerShape {
+	int kind;  // 0 conv 3x3, 1 fully connected
+	int cin, cout, hin, stride, hout;
+	int fan_in() const { return kind == 0 ? 9 * cin : cin; }
+	long long nw() const { return (long long)cout * fan_in(); }
+};
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ float to_f(T x);
+template <>
+__device__ __forceinline__ float to_f<float>(float x) {
+	return x;
+}
+template <>
+__device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 x) {
+	return __bfloat162float(x);
+}
+
+// C[M][N] = alpha * op(A) op(B) + beta * C, op(A) [M][K], op(B) [K][N]; A is
+// stored [M][K] (or [K][M] with TA), B [K][N] (or [N][K] with TB). 64 x 64
+// tiles, 16-deep k steps through shared memory, 4 x 4 outputs per thread,
+// FP32 accumulation. Split k: block z covers k in [z kchunk, (z + 1) kchunk)
+// and writes its partial product to C + z cstride.
+template <typename TAe, typename TBe, bool TA, bool TB>
+__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, float alpha, const TAe *__restrict__ A,
+                                                   int lda, const TBe *__restrict__ B, int ldb, float beta,
+                                                   float *__restrict__ C, int ldc, int kchunk, long long cstride) {
+	__shared__ float As[16][64 + 4], Bs[16][64 + 4];
+	const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+	const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+	const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+	C += blockIdx.z * cstride;
+	float acc[4][4] = {};
+	for (int k0 = kb; k0 < ke; k0 += 16) {
+		// consecutive threads read consecutive addresses: along k for A
+		// [M][K] and B^T [N][K], along the 64-wide tile for A^T and B
+		for (int e = t; e < 64 * 16; e += 256) {
+			const int r = TA ? (e & 63) : (e >> 4), kk = TA ? (e >> 6) : (e & 15);
+			const int i = i0 + r, k = k0 + kk;
+			float a = 0.f;
+			if (i < M && k < ke)
+				a = to_f(TA ? A[(size_t)k * lda + i] : A[(size_t)i * lda + k]);
+			As[kk][r] = a;
+		}
+		for (int e = t; e < 64 * 16; e += 256) {
+			const int r = TB ? (e >> 4) : (e & 63), kk = TB ? (e & 15) : (e >> 6);
+			const int j = j0 + r, k = k0 + kk;
+			float b = 0.f;
+			if (j < N && k < ke)
+				b = to_f(TB ? B[(size_t)j * ldb + k] : B[(size_t)k * ldb + j]);
+			Bs[kk][r] = b;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int kk = 0; kk < 16; ++kk) {
+			float a[4], b[4];
+#pragma unroll
+			for (int q = 0; q < 4; ++q) {
+				a[q] = As[kk][ty * 4 + q];
+				b[q] = Bs[kk][tx * 4 + q];
+			}
+#pragma unroll
+			for (int p = 0; p < 4; ++p)
+#pragma unroll
+				for (int q = 0; q < 4; ++q)
+					acc[p][q] = fmaf(a[p], b[q], acc[p][q]);
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int p = 0; p < 4; ++p) {
+		const int i = i0 + ty * 4 + p;
+		if (i >= M)
+			continue;
+#pragma unroll
+		for (int q = 0; q < 4; ++q) {
+			const int j = j0 + tx * 4 + q;
+			if (j >= N)
+				continue;
+			float *c = C + (size_t)i * ldc + j;
+			*c = alpha * acc[p][q] + (beta != 0.f ? beta * *c : 0.f);
+		}
+	}
+}
+
+// cols[(b, ho, wo)][(ky, kx, c)] = X[b][ho s + ky - 1][wo s + kx - 1][c]
+// (zero outside the image).
+__global__ void im2col_kernel(const float *__restrict__ X, int B, int H, int C, int s, int Ho,
+                              float *__restrict__ cols) {
+	const long long n = (long long)B * Ho * Ho * 9 * C;
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int c = (int)(e % C);
+		long long r = e / C;
+		const int kx = (int)(r % 3);
+		r /= 3;
+		const int ky = (int)(r % 3);
+		r /= 3;
+		const int wo = (int)(r % Ho);
+		r /= Ho;
+		const int ho = (int)(r % Ho);
+		const int b = (int)(r / Ho);
+		const int y = ho * s + ky - 1, x = wo * s + kx - 1;
+		cols[e] = (y >= 0 && y < H && x >= 0 && x < H) ? X[(((size_t)b * H + y) * H + x) * C + c] : 0.f;
+	}
+}
+
+// dX[b][y][x][c] = sum of dcols over the (ho, wo, ky, kx) that read it.
+__global__ void col2im_kernel(const float *__restrict__ dcols, int B, int H, int C, int s, int Ho,
+                              float *__restrict__ dX) {
+	const long long n = (long long)B * H * H * C;
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int c = (int)(e % C);
+		long long r = e / C;
+		const int x = (int)(r % H);
+		r /= H;
+		const int y = (int)(r % H);
+		const int b = (int)(r / H);
+		float acc = 0.f;
+		for (int ky = 0; ky < 3; ++ky) {
+			const int yy = y + 1 - ky;
+			if (yy < 0 || yy % s)
+				continue;
+			const int ho = yy / s;
+			if (ho >= Ho)
+				continue;
+			for (int kx = 0; kx < 3; ++kx) {
+				const int xx = x + 1 - kx;
+				if (xx < 0 || xx % s)
+					continue;
+				const int wo = xx / s;
+				if (wo >= Ho)
+					continue;
+				acc += dcols[((((size_t)b * Ho + ho) * Ho + wo) * 9 + ky * 3 + kx) * C + c];
+			}
+		}
+		dX[e] = acc;
+	}
+}
+
+// Y[r][c] += bias[c], then ReLU when relu.
+__global__ void bias_act_kernel(float *__restrict__ Y, long long rows, int cols, const float *__restrict__ bias,
+                                int relu) {
+	const long long n = rows * cols;
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		float v = Y[e] + bias[e % cols];
+		Y[e] = relu ? fmaxf(v, 0.f) : v;
+	}
+}
+
+// out[e] = sum over z of part[z n + e], z in order.
+__global__ void sum_splits_kernel(const float *__restrict__ part, int S, long long n, float *__restrict__ out) {
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		float acc = 0.f;
+		for (int z = 0; z < S; ++z)
+			acc += part[z * n + e];
+		out[e] = acc;
+	}
+}
+
+// *acc += sum of loss[0, n) (one block, fixed-order tree).
+__global__ void __launch_bounds__(256) loss_sum_kernel(const float *__restrict__ loss, int n, double *__restrict__ acc) {
+	__shared__ double s[256];
+	double v = 0.;
+	for (int k = threadIdx.x; k < n; k += 256)
+		v += loss[k];
+	s[threadIdx.x] = v;
+	__syncthreads();
+	for (int h = 128; h > 0; h >>= 1) {
+		if (threadIdx.x < h)
+			s[threadIdx.x] += s[threadIdx.x + h];
+		__syncthreads();
+	}
+	if (threadIdx.x == 0)
+		*acc += s[0];
+}
+
+// dY *= (Y > 0) (ReLU backward, Y the forward output).
+__global__ void relu_back_kernel(float *__restrict__ dY, const float *__restrict__ Y, long long n) {
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+		if (!(Y[e] > 0.f))
+			dY[e] = 0.f;
+}
+
+// db[c] = sum_r dY[r][c]: one block per column, a fixed-order tree over
+// per-thread strided partial sums.
+__global__ void __launch_bounds__(256) bias_grad_kernel(const float *__restrict__ dY, long long rows, int cols,
+                                                        float *__restrict__ db) {
+	__shared__ float s[256];
+	const int c = blockIdx.x;
+	float acc = 0.f;
+	for (long long r = threadIdx.x; r < rows; r += 256)
+		acc += dY[r * cols + c];
+	s[threadIdx.x] = acc;
+	__syncthreads();
+	for (int h = 128; h > 0; h >>= 1) {
+		if (threadIdx.x < h)
+			s[threadIdx.x] += s[threadIdx.x + h];
+		__syncthreads();
+	}
+	if (threadIdx.x == 0)
+		db[c] = s[0];
+}
+
+// Softmax cross-entropy per row (one warp per row): loss[b] =
+// logsumexp(z) - z[label]; dz = (softmax(z) - onehot) / B.
+__global__ void softmax_xent_kernel(const float *__restrict__ z, const int *__restrict__ label, int B, int n,
+                                    float *__restrict__ dz, float *__restrict__ loss) {
+	const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (b >= B)
+		return;
+	const float *r = z + (size_t)b * n;
+	float m = -INFINITY;
+	for (int j = lane; j < n; j += 32)
+		m = fmaxf(m, r[j]);
+	for (int o = 16; o > 0; o >>= 1)
+		m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+	float s = 0.f;
+	for (int j = lane; j < n; j += 32)
+		s += expf(r[j] - m);
+	for (int o = 16; o > 0; o >>= 1)
+		s += __shfl_xor_sync(FULL, s, o);
+	const int y = label[b];
+	for (int j = lane; j < n; j += 32)
+		dz[(size_t)b * n + j] = (expf(r[j] - m) / s - (j == y ? 1.f : 0.f)) / (float)B;
+	if (lane == 0)
+		loss[b] = logf(s) + m - r[y];
+}
+
+// Adam on FP32 master weights; the BF16 copy is refreshed.
+__global__ void adam_kernel(float *__restrict__ w, float *__restrict__ m, float *__restrict__ v,
+                            const float *__restrict__ g, __nv_bfloat16 *__restrict__ wb, long long n, float lr,
+                            float b1, float b2, float c1, float c2, float eps) {
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const float gg = g[e];
+		const float mm = b1 * m[e] + (1.f - b1) * gg, vv = b2 * v[e] + (1.f - b2) * gg * gg;
+		m[e] = mm;
+		v[e] = vv;
+		const float ww = w[e] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+		w[e] = ww;
+		if (wb)
+			wb[e] = __float2bfloat16_rn(ww);
+	}
+}
+
+__global__ void to_bf16_kernel(const float *__restrict__ x, __nv_bfloat16 *__restrict__ y, long long n) {
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+		y[e] = __float2bfloat16_rn(x[e]);
+}
+
+// Image of each frame: photons of its mask-0 pixels (the E-step lists) summed
+// per bin (pixel_bin[p] in [0, 1024), -1 outside the grid), then log(1 + n).
+// One block per frame; the image is built in shared memory.
+__global__ void frame_image_kernel(const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off,
+                                   const long long *__restrict__ ph_mid, const int *__restrict__ pixel_bin, int P,
+                                   int d0, int n, float *__restrict__ img) {
+	__shared__ float s[IMG * IMG];
+	const int dl = blockIdx.x, d = d0 + dl;
+	if (dl >= n)
+		return;
+	for (int k = threadIdx.x; k < IMG * IMG; k += blockDim.x)
+		s[k] = 0.f;
+	__syncthreads();
+	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
+	for (long long j = beg + threadIdx.x; j < end; j += blockDim.x) {
+		const uint32_t w = ph[j];
+		const uint32_t idx = j < mid ? w : (w & IDX_MASK);
+		if (idx >= (uint32_t)P)
+			continue;
+		const int b = pixel_bin[idx];
+		if (b >= 0)
+			atomicAdd(&s[b], (float)(j < mid ? 1u : (w >> IDX_BITS)));
+	}
+	__syncthreads();
+	for (int k = threadIdx.x; k < IMG * IMG; k += blockDim.x)
+		img[(size_t)dl * IMG * IMG + k] = log1pf(s[k]);
+}
+
+// The K largest logits of each row, in decreasing order (first index on
+// ties); one warp per row, K rounds of a warp-wide arg-max.
+__global__ void topk_kernel(const float *__restrict__ z, int B, int n, int K, int *__restrict__ out) {
+	const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (b >= B)
+		return;
+	const float *r = z + (size_t)b * n;
+	float last = INFINITY;
+	int last_i = -1;
+	for (int k = 0; k < K; ++k) {
+		float m = -INFINITY;
+		int mi = n;
+		for (int j = lane; j < n; j += 32) {
+			const float v = r[j];
+			// strictly after the previous pick in (value desc, index asc) order
+			const bool after = v < last || (v == last && j > last_i);
+			if (after && (v > m || (v == m && j < mi))) {
+				m = v;
+				mi = j;
+			}
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			const float om = __shfl_xor_sync(FULL, m, o);
+			const int oi = __shfl_xor_sync(FULL, mi, o);
+			if (om > m || (om == m && oi < mi)) {
+				m = om;
+				mi = oi;
+			}
+		}
+		if (lane == 0)
+			out[(size_t)b * K + k] = mi < n ? mi : -1;
+		last = m;
+		last_i = mi;
+	}
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// the network object
+// ---------------------------------------------------------------------------
+// A training batch: dst row k = src row idx[k], lab_out[k] = lab[idx[k]].
+__global__ void gather_rows_kernel(const float *__restrict__ src, const int *__restrict__ idx, int n, int row,
+                                   float *__restrict__ dst, const int *__restrict__ lab, int *__restrict__ lab_out) {
+	const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e < (long long)n * row)
+		dst[e] = src[(size_t)idx[e / row] * row + e % row];
+	if (e < n)
+		lab_out[e] = lab[idx[e]];
+}
+
+struct dfg_pnet {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	std::string err;
+	int num_classes = 0, batch = 0;
+	LayerShape L[NL];
+	DevBuf<float> w[NL], b[NL], mw[NL], vw[NL], mb[NL], vb[NL], gw[NL], gb[NL];
+	DevBuf<__nv_bfloat16> wb[NL];
+	DevBuf<float> act[NL + 1], dact[NL + 1], cols[4], dcols[4], loss, xbatch;
+	DevBuf<int> labels, idx, perm, lab_all;
+	DevBuf<float> wsplit;  // split-k partial weight gradients
+	DevBuf<double> loss_acc;
+	DevBuf<float> images;
+	long long n_images = 0;
+	DevBuf<int> pixel_bin;
+	int P = 0;
+	long long step = 0;
+	int fail(int code, const char *fmt, ...) {
+		char buf[1024];
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(buf, sizeof(buf), fmt, ap);
+		va_end(ap);
+		err = buf;
+		return code;
+	}
+	long long rows(int l, int n) const {  // output rows of layer l for n images
+		return L[l].kind == 0 ? (long long)n * L[l].hout * L[l].hout : n;
+	}
+};
+
+#define PK(call)                                                                                  \
+	do {                                                                                          \
+		cudaError_t e_ = (call);                                                                  \
+		if (e_ != cudaSuccess)                                                                    \
+			return net->fail(e_ == cudaErrorMemoryAllocation ? DFG_ERR_NOMEM : DFG_ERR_CUDA,      \
+			                 "%s failed: %s", #call, cudaGetErrorString(e_));                    \
+	} while (0)
+#define PKL(name)                                                                                 \
+	do {                                                                                          \
+		cudaError_t e_ = cudaGetLastError();                                                      \
+		if (e_ != cudaSuccess)                                                                    \
+			return net->fail(DFG_ERR_CUDA, "launch of %s failed: %s", name, cudaGetErrorString(e_)); \
+	} while (0)
+
+static unsigned grid_for(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 1 << 20); }
+
+// Split of the k range of an M x N product so that the grid fills about two
+// blocks per SM (chunks of at least 512, multiples of 16): (splits, chunk).
+static void k_split(int M, int N, long long K, int *S, int *chunk) {
+	const long long blocks = (long long)((N + 63) / 64) * ((M + 63) / 64);
+	long long s = std::min<long long>(K / 512, (296 + blocks - 1) / blocks);
+	s = std::max<long long>(1, std::min<long long>(s, 1024));
+	long long c = (K + s - 1) / s;
+	c = (c + 15) / 16 * 16;
+	*chunk = (int)c;
+	*S = (int)((K + c - 1) / c);
+}
+
+template <typename TAe, typename TBe, bool TA, bool TB>
+static int gemm(dfg_pnet *net, int M, int N, int K, float alpha, const TAe *A, int lda, const TBe *B, int ldb,
+                float beta, float *C, int ldc) {
+	dim3 grid((N + 63) / 64, (M + 63) / 64);
+	gemm_kernel<TAe, TBe, TA, TB><<<grid, 256, 0, net->stream>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, K, 0);
+	PKL("gemm_kernel");
+	return DFG_OK;
+}
+
+// Weight gradient C [M][N] = A^T B with A [K][M], B [K][N] and a long k range
+// (the batch's output positions): split-k partials, summed in split order.
+static int gemm_wgrad(dfg_pnet *net, int M, int N, int K, const float *A, const float *B, float *C) {
+	int S, chunk;
+	k_split(M, N, K, &S, &chunk);
+	if (S == 1)
+		return gemm<float, float, true, false>(net, M, N, K, 1.f, A, M, B, N, 0.f, C, N);
+	dim3 grid((N + 63) / 64, (M + 63) / 64, S);
+	gemm_kernel<float, float, true, false><<<grid, 256, 0, net->stream>>>(M, N, K, 1.f, A, M, B, N, 0.f,
+	                                                                      net->wsplit.p, N, chunk,
+	                                                                      (long long)M * N);
+	PKL("gemm_kernel");
+	sum_splits_kernel<<<grid_for((long long)M * N), 256, 0, net->stream>>>(net->wsplit.p, S, (long long)M * N, C);
+	PKL("sum_splits_kernel");
+	return DFG_OK;
+}
+
+// Forward pass of n images at X (device, [n][1024]); logits in act[NL].
+static int forward(dfg_pnet *net, const float *X, int n) {
+	cudaStream_t st = net->stream;
+	const float *in = X;
+	for (int l = 0; l < NL; ++l) {
+		const LayerShape &s = net->L[l];
+		const long long rows = net->rows(l, n);
+		float *out = net->act[l + 1].p;
+		if (s.kind == 0) {
+			const long long nc = rows * 9 * s.cin;
+			im2col_kernel<<<grid_for(nc), 256, 0, st>>>(in, n, s.hin, s.cin, s.stride, s.hout, net->cols[l].p);
+			PKL("im2col_kernel");
+			if (int rc = gemm<float, __nv_bfloat16, false, true>(net, (int)rows, s.cout, 9 * s.cin, 1.f,
+			                                                       net->cols[l].p, 9 * s.cin, net->wb[l].p,
+			                                                       9 * s.cin, 0.f, out, s.cout))
+				return rc;
+		} else {
+			if (int rc = gemm<float, __nv_bfloat16, false, true>(net, n, s.cout, s.cin, 1.f, in, s.cin,
+			                                                       net->wb[l].p, s.cin, 0.f, out, s.cout))
+				return rc;
+		}
+		bias_act_kernel<<<grid_for(rows * s.cout), 256, 0, st>>>(out, rows, s.cout, net->b[l].p, l < NL - 1);
+		PKL("bias_act_kernel");
+		in = out;
+	}
+	return DFG_OK;
+}
+
+// Loss and gradients of n images at X with labels (device); per-image losses in loss.
+static int backward(dfg_pnet *net, const float *X, const int *lab, int n) {
+	cudaStream_t st = net->stream;
+	softmax_xent_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(net->act[NL].p, lab, n, net->num_classes,
+	                                                          net->dact[NL].p, net->loss.p);
+	PKL("softmax_xent_kernel");
+	for (int l = NL - 1; l >= 0; --l) {
+		const LayerShape &s = net->L[l];
+		const long long rows = net->rows(l, n);
+		float *dY = net->dact[l + 1].p;
+		if (l < NL - 1) {
+			relu_back_kernel<<<grid_for(rows * s.cout), 256, 0, st>>>(dY, net->act[l + 1].p, rows * s.cout);
+			PKL("relu_back_kernel");
+		}
+		bias_grad_kernel<<<s.cout, 256, 0, st>>>(dY, rows, s.cout, net->gb[l].p);
+		PKL("bias_grad_kernel");
+		const float *in = l == 0 ? X : net->act[l].p;
+		if (s.kind == 0) {
+			if (int rc = gemm_wgrad(net, s.cout, 9 * s.cin, (int)rows, dY, net->cols[l].p, net->gw[l].p))
+				return rc;
+			if (l > 0) {
+				if (int rc = gemm<float, __nv_bfloat16, false, false>(net, (int)rows, 9 * s.cin, s.cout, 1.f, dY,
+				                                                        s.cout, net->wb[l].p, 9 * s.cin, 0.f,
+				                                                        net->dcols[l].p, 9 * s.cin))
+					return rc;
+				const long long nx = (long long)n * s.hin * s.hin * s.cin;
+				col2im_kernel<<<grid_for(nx), 256, 0, st>>>(net->dcols[l].p, n, s.hin, s.cin, s.stride, s.hout,
+				                                             net->dact[l].p);
+				PKL("col2im_kernel");
+			}
+		} else {
+			if (int rc = gemm_wgrad(net, s.cout, s.cin, n, dY, in, net->gw[l].p))
+				return rc;
+			if (int rc = gemm<float, __nv_bfloat16, false, false>(net, n, s.cin, s.cout, 1.f, dY, s.cout,
+			                                                        net->wb[l].p, s.cin, 0.f, net->dact[l].p,
+			                                                        s.cin))
+				return rc;
+		}
+	}
+	return DFG_OK;
+}
+
+static int adam_step(dfg_pnet *net, float lr) {
+	const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+	net->step++;
+	const float c1 = 1.f - powf(b1, (float)net->step), c2 = 1.f - powf(b2, (float)net->step);
+	for (int l = 0; l < NL; ++l) {
+		const long long nw = net->L[l].nw();
+		adam_kernel<<<grid_for(nw), 256, 0, net->stream>>>(net->w[l].p, net->mw[l].p, net->vw[l].p, net->gw[l].p,
+		                                                    net->wb[l].p, nw, lr, b1, b2, c1, c2, eps);
+		PKL("adam_kernel");
+		adam_kernel<<<grid_for(net->L[l].cout), 256, 0, net->stream>>>(net->b[l].p, net->mb[l].p, net->vb[l].p,
+		                                                                net->gb[l].p, nullptr, net->L[l].cout, lr,
+		                                                                b1, b2, c1, c2, eps);
+		PKL("adam_kernel");
+	}
+	return DFG_OK;
+}
+
+static int upload_params(dfg_pnet *net, const float *h) {
+	size_t o = 0;
+	for (int l = 0; l < NL; ++l) {
+		const long long nw = net->L[l].nw();
+		PK(cudaMemcpyAsync(net->w[l].p, h + o, nw * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+		o += nw;
+		PK(cudaMemcpyAsync(net->b[l].p, h + o, net->L[l].cout * sizeof(float), cudaMemcpyHostToDevice, net->stream));
+		o += net->L[l].cout;
+		to_bf16_kernel<<<grid_for(nw), 256, 0, net->stream>>>(net->w[l].p, net->wb[l].p, nw);
+		PKL("to_bf16_kernel");
+	}
+	PK(cudaStreamSynchronize(net->stream));
+	return DFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" void dfg_pnet_destroy(dfg_pnet *net) {
+	if (!net)
+		return;
+	cudaSetDevice(net->device);
+	if (net->stream) {
+		cudaStreamSynchronize(net->stream);
+		cudaStreamDestroy(net->stream);
+	}
+	delete net;
+}
+
+extern "C" int dfg_pnet_create(int device, int num_classes, int batch, unsigned long long seed, dfg_pnet **out) {
+	if (!out || num_classes < 2 || batch < 1)
+		return DFG_ERR_ARG;
+	*out = nullptr;
+	if (cudaSetDevice(device) != cudaSuccess)
+		return DFG_ERR_CUDA;
+	dfg_pnet *net = new dfg_pnet();
+	net->device = device;
+	net->num_classes = num_classes;
+	net->batch = batch;
+	if (cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess) {
+		delete net;
+		return DFG_ERR_CUDA;
+	}
+	const LayerShape shapes[NL] = {{0, 1, 32, 32, 1, 32},   {0, 32, 32, 32, 2, 16}, {0, 32, 64, 16, 1, 16},
+	                               {0, 64, 64, 16, 2, 8},   {1, 4096, 256, 0, 0, 0}, {1, 256, num_classes, 0, 0, 0}};
+	std::mt19937_64 rng(seed);
+	std::vector<float> params;
+	for (int l = 0; l < NL; ++l) {
+		net->L[l] = shapes[l];
+		// He initialisation (unit variance for the logits' layer)
+		std::normal_distribution<float> nd(0.f, std::sqrt((l < NL - 1 ? 2.f : 1.f) / shapes[l].fan_in()));
+		for (long long k = 0; k < shapes[l].nw(); ++k)
+			params.push_back(nd(rng));
+		for (int k = 0; k < shapes[l].cout; ++k)
+			params.push_back(0.f);
+	}
+	auto bad = [&](int rc) {
+		dfg_pnet_destroy(net);
+		return rc;
+	};
+	for (int l = 0; l < NL; ++l) {
+		const LayerShape &s = net->L[l];
+		const long long nw = s.nw(), rows = net->rows(l, batch);
+		bool ok = net->w[l].ensure(nw) == cudaSuccess && net->mw[l].ensure(nw) == cudaSuccess &&
+		          net->vw[l].ensure(nw) == cudaSuccess && net->gw[l].ensure(nw) == cudaSuccess &&
+		          net->wb[l].ensure(nw) == cudaSuccess && net->b[l].ensure(s.cout) == cudaSuccess &&
+		          net->mb[l].ensure(s.cout) == cudaSuccess && net->vb[l].ensure(s.cout) == cudaSuccess &&
+		          net->gb[l].ensure(s.cout) == cudaSuccess && net->act[l + 1].ensure(rows * s.cout) == cudaSuccess &&
+		          net->dact[l + 1].ensure(rows * s.cout) == cudaSuccess;
+		if (ok && s.kind == 0)
+			ok = net->cols[l].ensure(rows * 9 * s.cin) == cudaSuccess &&
+			     net->dcols[l].ensure(rows * 9 * s.cin) == cudaSuccess;
+		if (!ok)
+			return bad(DFG_ERR_NOMEM);
+		cudaMemsetAsync(net->mw[l].p, 0, nw * sizeof(float), net->stream);
+		cudaMemsetAsync(net->vw[l].p, 0, nw * sizeof(float), net->stream);
+		cudaMemsetAsync(net->mb[l].p, 0, s.cout * sizeof(float), net->stream);
+		cudaMemsetAsync(net->vb[l].p, 0, s.cout * sizeof(float), net->stream);
+	}
+	long long ws = 0;
+	for (int l = 0; l < NL; ++l) {
+		int S, chunk;
+		k_split(net->L[l].cout, net->L[l].fan_in(), net->rows(l, batch), &S, &chunk);
+		if (S > 1)
+			ws = std::max(ws, (long long)S * net->L[l].nw());
+	}
+	if (ws > 0 && net->wsplit.ensure(ws) != cudaSuccess)
+		return bad(DFG_ERR_NOMEM);
+	if (net->loss_acc.ensure(1) != cudaSuccess)
+		return bad(DFG_ERR_NOMEM);
+	if (net->dact[0].ensure((long long)batch * IMG * IMG) != cudaSuccess ||
+	    net->loss.ensure(batch) != cudaSuccess || net->labels.ensure(batch) != cudaSuccess ||
+	    net->idx.ensure(batch) != cudaSuccess || net->xbatch.ensure((long long)batch * IMG * IMG) != cudaSuccess)
+		return bad(DFG_ERR_NOMEM);
+	if (upload_params(net, params.data()) != DFG_OK)
+		return bad(DFG_ERR_CUDA);
+	*out = net;
+	return DFG_OK;
+}
+
+extern "C" const char *dfg_pnet_last_error(const dfg_pnet *net) { return net ? net->err.c_str() : "null network"; }
+
+extern "C" long long dfg_pnet_num_params(const dfg_pnet *net) {
+	if (!net)
+		return 0;
+	long long n = 0;
+	for (int l = 0; l < NL; ++l)
+		n += net->L[l].nw() + net->L[l].cout;
+	return n;
+}
+
+extern "C" int dfg_pnet_get_params(dfg_pnet *net, float *out) {
+	if (!net || !out)
+		return DFG_ERR_ARG;
+	PK(cudaSetDevice(net->device));
+	size_t o = 0;
+	for (int l = 0; l < NL; ++l) {
+		const long long nw = net->L[l].nw();
+		PK(cudaMemcpyAsync(out + o, net->w[l].p, nw * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+		o += nw;
+		PK(cudaMemcpyAsync(out + o, net->b[l].p, net->L[l].cout * sizeof(float), cudaMemcpyDeviceToHost,
+		                   net->stream));
+		o += net->L[l].cout;
+	}
+	PK(cudaStreamSynchronize(net->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_set_params(dfg_pnet *net, const float *in) {
+	if (!net || !in)
+		return DFG_ERR_ARG;
+	PK(cudaSetDevice(net->device));
+	return upload_params(net, in);
+}
+
+extern "C" int dfg_pnet_set_bins(dfg_pnet *net, int num_pix, const int *pixel_bin) {
+	if (!net || num_pix < 1 || !pixel_bin)
+		return DFG_ERR_ARG;
+	for (int p = 0; p < num_pix; ++p)
+		if (pixel_bin[p] < -1 || pixel_bin[p] >= IMG * IMG)
+			return net->fail(DFG_ERR_ARG, "pixel_bin[%d] = %d outside [-1, %d)", p, pixel_bin[p], IMG * IMG);
+	PK(cudaSetDevice(net->device));
+	PK(upload(net->pixel_bin, pixel_bin, (size_t)num_pix, net->stream));
+	PK(cudaStreamSynchronize(net->stream));
+	net->P = num_pix;
+	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_load_frames(dfg_pnet *net, dfg_ctx *ctx) {
+	if (!net || !ctx)
+		return DFG_ERR_ARG;
+	if (ctx->N <= 0 || ctx->P != net->P)
+		return net->fail(DFG_ERR_STATE, "the context's frames and detector (%d pixels) must match the bins (%d)",
+		                 ctx->P, net->P);
+	if (ctx->device != net->device)
+		return net->fail(DFG_ERR_ARG, "context and network on different devices");
+	PK(cudaSetDevice(net->device));
+	PK(net->images.ensure((size_t)ctx->N * IMG * IMG));
+	PK(cudaStreamSynchronize(ctx->stream));
+	frame_image_kernel<<<ctx->N, 256, 0, net->stream>>>(ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, net->pixel_bin.p,
+	                                                    ctx->P, 0, ctx->N, net->images.p);
+	PKL("frame_image_kernel");
+	PK(cudaStreamSynchronize(net->stream));
+	net->n_images = ctx->N;
+	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_set_images(dfg_pnet *net, long long n, const float *images) {
+	if (!net || n < 1 || !images)
+		return DFG_ERR_ARG;
+	PK(cudaSetDevice(net->device));
+	PK(upload(net->images, images, (size_t)n * IMG * IMG, net->stream));
+	PK(cudaStreamSynchronize(net->stream));
+	net->n_images = n;
+	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_get_images(dfg_pnet *net, float *out) {
+	if (!net || !out)
+		return DFG_ERR_ARG;
+	PK(cudaSetDevice(net->device));
+	PK(cudaMemcpy(out, net->images.p, (size_t)net->n_images * IMG * IMG * sizeof(float), cudaMemcpyDeviceToHost));
+	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, double lr, unsigned long long seed,
+                              double *mean_loss) {
+	if (!net || !labels || epochs < 1 || !(lr > 0.))
+		return DFG_ERR_ARG;
+	if (net->n_images < 1)
+		return net->fail(DFG_ERR_STATE, "no images loaded");
+	for (long long i = 0; i < net->n_images; ++i)
+		if (labels[i] < 0 || labels[i] >= net->num_classes)
+			return net->fail(DFG_ERR_ARG, "label %d of image %lld outside [0, %d)", labels[i], i, net->num_classes);
+	PK(cudaSetDevice(net->device));
+	cudaStream_t st = net->stream;
+	const long long n = net->n_images;
+	// each epoch's shuffled order goes up once; batches are gathered on the
+	// device and the losses summed there (one synchronisation per epoch)
+	std::vector<int> perm((size_t)n);
+	for (long long i = 0; i < n; ++i)
+		perm[(size_t)i] = (int)i;
+	PK(upload(net->lab_all, labels, (size_t)n, st));
+	PK(net->perm.ensure((size_t)n));
+	std::mt19937_64 rng(seed);
+	double last = 0.;
+	for (int ep = 0; ep < epochs; ++ep) {
+		std::shuffle(perm.begin(), perm.end(), rng);
+		PK(cudaMemcpyAsync(net->perm.p, perm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
+		PK(cudaMemsetAsync(net->loss_acc.p, 0, sizeof(double), st));
+		for (long long b0 = 0; b0 < n; b0 += net->batch) {
+			const int m = (int)std::min<long long>(net->batch, n - b0);
+			gather_rows_kernel<<<grid_for((long long)m * IMG * IMG), 256, 0, st>>>(
+			    net->images.p, net->perm.p + b0, m, IMG * IMG, net->xbatch.p, net->lab_all.p, net->labels.p);
+			PKL("gather_rows_kernel");
+			if (int rc = forward(net, net->xbatch.p, m))
+				return rc;
+			if (int rc = backward(net, net->xbatch.p, net->labels.p, m))
+				return rc;
+			if (int rc = adam_step(net, (float)lr))
+				return rc;
+			loss_sum_kernel<<<1, 256, 0, st>>>(net->loss.p, m, net->loss_acc.p);
+			PKL("loss_sum_kernel");
+		}
+		double sum = 0.;
+		PK(cudaMemcpyAsync(&sum, net->loss_acc.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+		PK(cudaStreamSynchronize(st));
+		last = sum / (double)n;
+	}
+	if (mean_loss)
+		*mean_loss = last;
+	return DFG_OK;
+}
+
+// Runs fn(b0, m) over the loaded images in batches after a forward pass.
+template <typename F>
+static int for_batches(dfg_pnet *net, F fn) {
+	for (long long b0 = 0; b0 < net->n_images; b0 += net->batch) {
+		const int m = (int)std::min<long long>(net->batch, net->n_images - b0);
+		if (int rc = forward(net, net->images.p + (size_t)b0 * IMG * IMG, m))
+			return rc;
+		if (int rc = fn(b0, m))
+			return rc;
+	}
+	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_topk(dfg_pnet *net, int K, int *out) {
+	if (!net || K < 1 || K > net->num_classes || !out)
+		return DFG_ERR_ARG;
+	PK(cudaSetDevice(net->device));
+	DevBuf<int> d;
+	PK(d.ensure((size_t)net->batch * K));
+	return for_batches(net, [&](long long b0, int m) -> int {
+		topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(net->act[NL].p, m, net->num_classes, K, d.p);
+		PKL("topk_kernel");
+		PK(cudaMemcpyAsync(out + (size_t)b0 * K, d.p, (size_t)m * K * sizeof(int), cudaMemcpyDeviceToHost,
+		                   net->stream));
+		PK(cudaStreamSynchronize(net->stream));
+		return DFG_OK;
+	});
+}
+
+extern "C" int dfg_pnet_logits(dfg_pnet *net, float *out) {
+	if (!net || !out)
+		return DFG_ERR_ARG;
+	PK(cudaSetDevice(net->device));
+	return for_batches(net, [&](long long b0, int m) -> int {
+		PK(cudaMemcpyAsync(out + (size_t)b0 * net->num_classes, net->act[NL].p,
+		                   (size_t)m * net->num_classes * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+		PK(cudaStreamSynchronize(net->stream));
+		return DFG_OK;
+	});
+}
+
+// Mean loss and gradients (flat, as dfg_pnet_get_params) of the first
+// min(n_images, batch) loaded images with the given labels; no update.
+extern "C" int dfg_pnet_gradients(dfg_pnet *net, const int *labels, float *grads, double *mean_loss) {
+	if (!net || !labels || !grads)
+		return DFG_ERR_ARG;
+	if (net->n_images < 1)
+		return net->fail(DFG_ERR_STATE, "no images loaded");
+	PK(cudaSetDevice(net->device));
+	const int m = (int)std::min<long long>(net->batch, net->n_images);
+	PK(cudaMemcpyAsync(net->labels.p, labels, m * sizeof(int), cudaMemcpyHostToDevice, net->stream));
+	if (int rc = forward(net, net->images.p, m))
+		return rc;
+	if (int rc = backward(net, net->images.p, net->labels.p, m))
+		return rc;
+	size_t o = 0;
+	for (int l = 0; l < NL; ++l) {
+		const long long nw = net->L[l].nw();
+		PK(cudaMemcpyAsync(grads + o, net->gw[l].p, nw * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+		o += nw;
+		PK(cudaMemcpyAsync(grads + o, net->gb[l].p, net->L[l].cout * sizeof(float), cudaMemcpyDeviceToHost,
+		                   net->stream));
+		o += net->L[l].cout;
+	}
+	std::vector<float> loss((size_t)m);
+	PK(cudaMemcpyAsync(loss.data(), net->loss.p, m * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+	PK(cudaStreamSynchronize(net->stream));
+	double s = 0.;
+	for (float v : loss)
+		s += v;
+	if (mean_loss)
+		*mean_loss = s / m;
+	return DFG_OK;
+}

@@ -1,0 +1,131 @@
+"""Learned orientation proposals for the E-step (no counterpart in the
+reference, whose E-step searches every orientation of every frame).
+
+A small network (``_lib.ProposalNet``, trained and run on the GPU by the
+library's own kernels) maps each frame's photon image to logits over a coarse
+orientation set (``quat_gen(coarse_div)``); a frame's E-step then evaluates
+only the fine orientations whose nearest coarse orientation is among its top
+K (``Context.set_refinement`` with the coarse map of ``voronoi_subset``; with
+the fine orientations sorted by coarse cell, the skipped orientations form
+whole tiles that every phase of the iteration skips). Each iteration a
+held-out share of the frames is searched in full and watched: the probability
+mass its proposals would have captured (``Context.watch_mass``) judges the
+network, and when it falls below ``threshold`` the next iteration is a full
+search and the network is trained again, on frames simulated from the
+current model at known orientations and on the last full search's most likely
+orientations.
+"""
+import numpy as np
+
+from .quatgen import quat_gen
+
+
+def sort_by_coarse(fine, coarse_div, ctx):
+    """Fine orientations [R, 5] ordered by their nearest coarse orientation
+    (stable), so that a coarse cell's orientations are contiguous. Returns
+    (sorted quaternions, order, coarse map of the sorted list)."""
+    coarse = quat_gen(coarse_div)
+    qmap = ctx.voronoi_subset(coarse, fine)
+    order = np.lexsort((np.arange(fine.shape[0]), qmap))
+    return np.ascontiguousarray(fine[order]), order, np.ascontiguousarray(qmap[order])
+
+
+class LearnedProposals:
+    """Drives proposal-restricted iterations of one reconstruction context.
+
+    Args:
+        ctx: the reconstruction's ``_lib.Context`` (detector, frames and the
+            fine orientations already set; one model mode).
+        qvals: the detector's q vectors (image binning).
+        fine: the context's orientation list [R, 5] (ideally from
+            ``sort_by_coarse``).
+        coarse_div: num_div of the coarse orientation set (the classes).
+        K: coarse cells kept per frame.
+        held_out: share of frames searched in full and watched each iteration.
+        threshold: mean captured probability mass below which the next
+            iteration searches in full and the network is retrained.
+    """
+
+    def __init__(self, ctx, qvals, fine, coarse_div=4, K=16, held_out=0.01, threshold=0.99, batch=256, seed=0):
+        from ._lib import Context, ProposalNet
+        self.ctx = ctx
+        self.coarse = quat_gen(coarse_div)
+        self.nc = self.coarse.shape[0]
+        self.K = int(K)
+        self.held_out = float(held_out)
+        self.threshold = float(threshold)
+        self.qmap = np.ascontiguousarray(ctx.voronoi_subset(self.coarse, fine), np.int32)
+        self.net = ProposalNet(self.nc, batch=batch, seed=seed, device=ctx.device)
+        self.net.set_bins(ProposalNet.pixel_bins(qvals))
+        self.sim = Context(ctx.device)          # frames simulated for training
+        self.sim.set_detector(qvals, ctx._corr, ctx._mask)
+        self.rng = np.random.default_rng(seed)
+        self.full_next = False
+        self.history = []
+
+    def train_simulated(self, model, n_frames=20000, epochs=3, lr=2e-3, phi=None):
+        """Trains on frames simulated from model at uniformly random
+        orientations (label: their nearest coarse orientation). phi: per-frame
+        fluence factors (default ones)."""
+        from . import synth
+        q = synth.random_quaternions(int(n_frames), self.rng)
+        f = np.ones(len(q)) if phi is None else np.asarray(phi, np.float64)
+        self.sim.simulate_frames(model, q, f, int(self.rng.integers(1 << 30)))
+        labels = self.sim.voronoi_subset(self.coarse, np.pad(q[:, :4], ((0, 0), (0, 1))))
+        self.net.load_frames(self.sim)
+        return self.net.train(labels, epochs=epochs, lr=lr, seed=int(self.rng.integers(1 << 30)))
+
+    def train_full_search(self, rmax, epochs=1, lr=1e-3):
+        """Trains on the context's own frames labelled by the coarse cell of a
+        full search's most likely orientation (frames with none are left out)."""
+        ok = np.asarray(rmax) >= 0
+        if not ok.any():
+            return None
+        self.net.load_frames(self.ctx)
+        labels = np.where(ok, self.qmap[np.maximum(rmax, 0)], 0).astype(np.int32)
+        return self.net.train(labels, epochs=epochs, lr=lr, seed=int(self.rng.integers(1 << 30)))
+
+    def propose(self):
+        """Top-K coarse cells of every frame of the context."""
+        self.net.load_frames(self.ctx)
+        return self.net.topk(self.K)
+
+    def iteration(self, par, alpha=0.):
+        """One iteration: proposal-restricted (held-out frames in full and
+        watched), or a full search when the last judgement failed. Returns
+        the iteration's results with 'mode', 'captured_mass' and
+        'evaluated_fraction'."""
+        ctx = self.ctx
+        N = ctx.num_data
+        info = {}
+        if self.full_next:
+            ctx.set_refinement(None)
+            out = ctx.run_iteration(par, alpha)
+            info.update(mode="full", captured_mass=None, evaluated_fraction=1.)
+            self.train_full_search(ctx.frame_results()["rmax"])
+            self.full_next = False
+        else:
+            top = self.propose()
+            n_watch = max(1, int(round(self.held_out * N)))
+            watch = np.sort(self.rng.choice(N, n_watch, replace=False)).astype(np.int32)
+            allc = np.arange(self.nc, dtype=np.int32)
+            rel = [top[d] for d in range(N)]
+            for d in watch:
+                rel[d] = allc
+            ctx.set_refinement(self.nc, self.qmap, rel)
+            ctx.set_watch(watch, [top[d] for d in watch])
+            out = ctx.run_iteration(par, alpha)
+            mass = ctx.watch_mass()
+            frac = (self.K * (N - n_watch) + self.nc * n_watch) / float(self.nc * N)
+            info.update(mode="proposal", captured_mass=float(mass.mean()), min_mass=float(mass.min()),
+                        evaluated_fraction=frac)
+            if mass.mean() < self.threshold:
+                self.full_next = True
+        out = dict(out)
+        out.update(info)
+        self.history.append(info)
+        return out
+
+    def close(self):
+        self.net.close()
+        self.sim.close()

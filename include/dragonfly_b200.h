@@ -157,6 +157,16 @@ DFG_API int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order);
 DFG_API int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
                                const long long *rel_off, const int *rel_quat);
 
+/* Watched frames of a refined (proposal-restricted) search: frames[n]
+ * (ascending) and, per frame, a list of coarse cells cells[cell_off[i] ..
+ * cell_off[i+1]). After each dfg_maximize / dfg_run_iteration,
+ * dfg_get_watch_mass gives for every watched frame the share of its
+ * probability (sum of P) on orientations whose coarse cell is in its list:
+ * with the frame searched in full and the list its proposal, the probability
+ * mass the proposal would have captured. n = 0 clears. */
+DFG_API int dfg_set_watch(dfg_ctx *ctx, int n, const int *frames, const long long *cell_off, const int *cells);
+DFG_API int dfg_get_watch_mass(dfg_ctx *ctx, double *mass);
+
 /* voronoi_subset (quaternion.c:844-862, Quaternion.voronoi_subset
  * quaternion.pyx:257-281): nearest[i] = the coarse orientation with the
  * smallest 1 - (q_i . c_j)^2, first on ties. Quaternions are rows of five
@@ -273,6 +283,42 @@ DFG_API int dfg_batch_set_lanes(dfg_batch *batch, int lanes);
 /* out[0] = graph launches, out[1] = instantiations, out[2] = in-place updates. */
 DFG_API int dfg_batch_stats(dfg_batch *batch, long *out);
 DFG_API void dfg_batch_destroy(dfg_batch *batch);
+
+/* ---- learned orientation proposals ----------------------------------------
+ * A small convolutional network (csrc/proposal.cu) mapping a frame's photon
+ * image (log(1 + photons) binned on a 32 x 32 grid: pixel_bin[p] in
+ * [0, 1024) or -1) to logits over num_classes coarse orientations: conv 3x3
+ * 1->32, 32->32 (stride 2), 32->64, 64->64 (stride 2), fully connected
+ * 4096->256->num_classes, ReLU between; BF16 weights in the products, FP32
+ * accumulation and Adam state. Training and inference run on the GPU by this
+ * library's own kernels. The top-K classes of a frame restrict its E-step
+ * (dfg_set_refinement with the coarse map of dfg_voronoi_subset). No
+ * counterpart in the reference. Parameters are flat FP32: per layer the
+ * weights [cout][fan_in] (convolution rows ordered ky, kx, c), then the
+ * biases. */
+typedef struct dfg_pnet dfg_pnet;
+DFG_API int dfg_pnet_create(int device, int num_classes, int batch, unsigned long long seed, dfg_pnet **out);
+DFG_API void dfg_pnet_destroy(dfg_pnet *net);
+DFG_API const char *dfg_pnet_last_error(const dfg_pnet *net);
+DFG_API long long dfg_pnet_num_params(const dfg_pnet *net);
+DFG_API int dfg_pnet_get_params(dfg_pnet *net, float *out);
+DFG_API int dfg_pnet_set_params(dfg_pnet *net, const float *in);
+DFG_API int dfg_pnet_set_bins(dfg_pnet *net, int num_pix, const int *pixel_bin);
+/* Images of the context's frames (its mask-0 photons), kept on the device. */
+DFG_API int dfg_pnet_load_frames(dfg_pnet *net, dfg_ctx *ctx);
+/* Images [n][1024] from the host (tests), and the loaded images back. */
+DFG_API int dfg_pnet_set_images(dfg_pnet *net, long long n, const float *images);
+DFG_API int dfg_pnet_get_images(dfg_pnet *net, float *out);
+/* epochs of Adam over the loaded images (shuffled by seed) against labels
+ * [n] in [0, num_classes); *mean_loss = the last epoch's mean loss. */
+DFG_API int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, double lr, unsigned long long seed,
+                           double *mean_loss);
+/* out[n][K]: the K largest logits' classes of every loaded image, largest first. */
+DFG_API int dfg_pnet_topk(dfg_pnet *net, int K, int *out);
+DFG_API int dfg_pnet_logits(dfg_pnet *net, float *out);
+/* Mean loss and gradients (flat, as the parameters) on the first
+ * min(n, batch) loaded images with labels; the parameters are not changed. */
+DFG_API int dfg_pnet_gradients(dfg_pnet *net, const int *labels, float *grads, double *mean_loss);
 
 /* Graph use of dfg_run_iteration: out[0] = graph launches, out[1] =
  * instantiations, out[2] = in-place updates. */

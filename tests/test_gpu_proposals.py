@@ -1,0 +1,65 @@
+"""Learned orientation proposals end to end: the network trained on frames
+simulated from the model at known orientations, frames restricted to their
+top-K coarse cells, a held-out share searched in full and watched. Against a
+full search over the same frames from the same model: the captured
+probability mass, the most likely orientations and the model, and what the
+network gains over proposals without it (random cells)."""
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_learned_proposals_against_full_search():
+    from dragonfly_b200 import synth
+    from dragonfly_b200._lib import Context
+    from dragonfly_b200.proposals import LearnedProposals, sort_by_coarse
+    from dragonfly_b200.quatgen import quat_gen
+    d = synth.small_problem(seed=9, det_side=64, size=61, qmax=29., n_atoms=200, atom_radius=10., num_div=6,
+                            n_frames=4000, mean_count=300., hole_radius=3.)
+    ctxs = []
+    for k in range(2):
+        c = Context(0)
+        c.set_detector(d["qvals"], d["corr"], d["mask"])
+        c.set_frames(d["ones"], d["multi"], d["place_ones"], d["place_multi"], d["count_multi"])
+        ctxs.append(c)
+    full, restr = ctxs
+    fine, _, qmap = sort_by_coarse(quat_gen(6), 2, full)
+    for c in ctxs:
+        c.set_quaternions(fine)
+        c.set_model(d["model_true"][None])
+        c.calc_beta(1., 0)
+    lp = LearnedProposals(restr, d["qvals"], fine, coarse_div=2, K=24, held_out=0.02, threshold=0.99, seed=1)
+    loss = lp.train_simulated(d["model_true"], n_frames=30000, epochs=4)
+    # the network's gain: top-K hit rate of the true orientations' cells
+    cells = full.voronoi_subset(quat_gen(2), np.pad(d["frame_quats"][:, :4], ((0, 0), (0, 1))))
+    top = lp.propose()
+    hit = float(np.mean([cells[i] in top[i] for i in range(len(cells))]))
+    chance = lp.K / lp.nc
+    print("training loss %.3f; top-%d hit rate %.3f (random cells %.3f)" % (loss, lp.K, hit, chance))
+    assert hit >= 0.9 and hit > 10 * chance
+    for it in (1, 2):
+        par = full.params(it)
+        t0 = time.time()
+        a = full.run_iteration(par, 0.)
+        t1 = time.time()
+        b = lp.iteration(restr.params(it), 0.)
+        t2 = time.time()
+        ma, _, _ = full.model()
+        mb, _, _ = restr.model()
+        dev = float(np.linalg.norm(ma - mb) / np.linalg.norm(ma))
+        agree = float(np.mean(full.frame_results()["rmax"] == restr.frame_results()["rmax"]))
+        print("iteration %d (%s): captured mass %s, evaluated %.3f of the pairs, model %.2e, rmax %.4f, "
+              "full %.0f ms, proposal %.0f ms" % (it, b["mode"], b["captured_mass"], b["evaluated_fraction"], dev,
+                                                 agree, 1e3 * (t1 - t0), 1e3 * (t2 - t1)))
+        if b["mode"] == "proposal":
+            assert b["evaluated_fraction"] < 0.2
+            if b["captured_mass"] >= lp.threshold:
+                assert dev <= 1e-3 and agree >= 0.99, (dev, agree)
+            else:
+                assert lp.full_next          # the next iteration falls back to full search
+    lp.close()
+    for c in ctxs:
+        c.close()

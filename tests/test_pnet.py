@@ -1,0 +1,65 @@
+"""The orientation-proposal network: its CPU oracle pinned by finite
+differences, and the GPU kernels' loss and gradients against the oracle."""
+import numpy as np
+import pytest
+
+from oracle.pnet_oracle import bf16, layers, loss_and_grads
+
+
+def _params(rng, nc):
+    out = []
+    for kind, cin, cout, *_ in layers(nc):
+        fan = 9 * cin if kind == 0 else cin
+        out += [rng.normal(0., np.sqrt(2. / fan), cout * fan), rng.normal(0., 0.05, cout)]
+    return np.concatenate(out)
+
+
+def test_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(0)
+    nc = 12
+    p = _params(rng, nc)
+    x = np.log1p(rng.poisson(0.7, (3, 1024)).astype(np.float64))
+    y = np.array([1, 5, 11])
+    loss, g = loss_and_grads(p, x, y, nc, round_weights=False)
+    idx = rng.choice(p.size, 40, replace=False)
+    h = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += h
+        lp, _ = loss_and_grads(q, x, y, nc, round_weights=False)
+        q[i] -= 2 * h
+        lm, _ = loss_and_grads(q, x, y, nc, round_weights=False)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding():
+    x = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 1e-30], np.float32)
+    r = bf16(x)
+    # BF16 keeps 8 mantissa bits: 1 + 2^-8 rounds to even (1.0), 1 + 3 * 2^-9 up
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0078125
+    assert abs(r[3] - x[3]) <= 2 ** -8 * abs(x[3])
+
+
+@pytest.mark.gpu
+def test_gpu_gradients_match_oracle():
+    from dragonfly_b200._lib import ProposalNet
+    rng = np.random.default_rng(1)
+    nc = 40
+    net = ProposalNet(nc, batch=8, seed=3)
+    p = net.params().astype(np.float64)
+    x = np.log1p(rng.poisson(0.5, (8, 1024)).astype(np.float64))
+    y = rng.integers(0, nc, 8)
+    net.set_images(x)
+    g, loss = net.gradients(y)
+    loss_ref, g_ref = loss_and_grads(p, x.astype(np.float32).astype(np.float64), y, nc)
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref), (loss, loss_ref)
+    # per layer: relative L2 of the gradient (FP32 accumulation on the GPU)
+    o = 0
+    for kind, cin, cout, *_ in layers(nc):
+        fan = 9 * cin if kind == 0 else cin
+        for n in (cout * fan, cout):
+            a, b = g[o:o + n].astype(np.float64), g_ref[o:o + n]
+            o += n
+            assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b) + 1e-9, (kind, cin, cout, n)
+    net.close()
