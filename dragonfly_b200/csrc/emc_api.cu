@@ -15,6 +15,7 @@
 #include "emc_device.cuh"
 #include "emc_bg.cuh"
 #include "emc_dense.cuh"
+#include "emc_pairs.cuh"
 
 using namespace dfg;
 
@@ -257,6 +258,7 @@ extern "C" int dfg_set_frames(dfg_ctx *ctx, int num_data, const int *ones, const
 	ctx->chunks_R = -1;
 	ctx->have_results = false;
 	ctx->refine = false;  // relevant orientations are per frame
+	ctx->pairs_valid = ctx->mw_valid = false;
 	ctx->max_count0 = -1;
 	ctx->tuned = false;
 	return DFG_OK;
@@ -368,6 +370,9 @@ extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_
 	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->h_qmap.assign(quat_mapping, quat_mapping + ctx->num_rot);
+	ctx->h_rel_off.assign(rel_off, rel_off + N + 1);
+	ctx->h_rel.assign(rel_quat, rel_quat + rel_off[N]);
+	ctx->pairs_valid = false;
 	if (num_coarse != ctx->num_coarse)
 		ctx->h_watch.clear();  // the cell bits were for another coarse set
 	ctx->num_coarse = num_coarse;
@@ -1058,6 +1063,50 @@ static void dense_release(dfg_ctx *ctx) {
 }
 
 static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par);
+static bool pair_mode(const dfg_ctx *ctx);
+static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par);
+
+// The coarse cell of every orientation on the device ([R_pad], -1 past R).
+static int prepare_qmap(dfg_ctx *ctx) {
+	NEED(ctx->M == 1, DFG_ERR_ARG, "refinement needs num_modes == 1");
+	if (!ctx->qmap_valid || ctx->qmap.n < (size_t)ctx->R_pad) {
+		std::vector<int> q((size_t)ctx->R_pad, -1);
+		std::copy(ctx->h_qmap.begin(), ctx->h_qmap.end(), q.begin());
+		CK(upload(ctx->qmap, q.data(), q.size(), ctx->stream));
+		CK(cudaStreamSynchronize(ctx->stream));
+		ctx->qmap_valid = true;
+	}
+	return DFG_OK;
+}
+
+// Merge weight cache: grid, psum_r > 0 pattern and flags (on the device).
+static int prepare_weight_cache(dfg_ctx *ctx) {
+	cudaStream_t st = ctx->stream;
+	CK(ctx->weight_cache.ensure((size_t)ctx->M * ctx->V));
+	CK(ctx->wpattern.ensure((size_t)ctx->R_pad));
+	CK(ctx->wflags.ensure(2));
+	if (!ctx->weight_cache_valid) {
+		CK(cudaMemsetAsync(ctx->wflags.p, 0, 2 * sizeof(int), st));
+		CK(cudaMemsetAsync(ctx->wpattern.p, 0, (size_t)ctx->R_pad, st));
+		ctx->weight_cache_valid = true;  // from here on the device tracks it
+	}
+	return DFG_OK;
+}
+
+// max_prepare of the pair layout (no autotuner, no dense forms); watched
+// frames by their global index.
+static int pair_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
+	ctx->dense_active = ctx->m_dense_active = false;
+	if (int rc = ensure_pair_buffers(ctx, par))
+		return rc;
+	if (!ctx->h_watch.empty()) {
+		CK(upload(ctx->watch_local, ctx->h_watch.data(), ctx->h_watch.size(), ctx->stream));
+		CK(cudaStreamSynchronize(ctx->stream));
+	}
+	if (int rc = prepare_qmap(ctx))
+		return rc;
+	return prepare_weight_cache(ctx);
+}
 
 // The part of maximize that allocates, uploads or checks on the host, done
 // before any of its kernels is queued (so that the queued part can be
@@ -1067,6 +1116,8 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 		return DFG_ERR_ARG;
 	NEED(par->beta_period > 0, DFG_ERR_ARG, "beta_period must be > 0");
 	CK(cudaSetDevice(ctx->device));
+	if (pair_mode(ctx))
+		return pair_prepare(ctx, par);
 	// E-step form: dense tensor-core products (option estep_form 1, or the
 	// autotuner's choice) where the inputs allow it
 	if (ctx->autotune && !ctx->tuned && !ctx->tuning)
@@ -1113,26 +1164,10 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 	}
 	// refinement: the reference indexes quat_mapping by the flat orientation
 	// index over all modes (max_prob.c:114), which only covers one mode
-	if (ctx->refine) {
-		NEED(ctx->M == 1, DFG_ERR_ARG, "refinement needs num_modes == 1");
-		if (!ctx->qmap_valid || ctx->qmap.n < (size_t)ctx->R_pad) {
-			std::vector<int> q((size_t)ctx->R_pad, -1);
-			std::copy(ctx->h_qmap.begin(), ctx->h_qmap.end(), q.begin());
-			CK(upload(ctx->qmap, q.data(), q.size(), st));
-			CK(cudaStreamSynchronize(st));
-			ctx->qmap_valid = true;
-		}
-	}
-	// merge weight cache: grid, psum_r > 0 pattern and flags (on the device)
-	CK(ctx->weight_cache.ensure((size_t)ctx->M * ctx->V));
-	CK(ctx->wpattern.ensure((size_t)ctx->R_pad));
-	CK(ctx->wflags.ensure(2));
-	if (!ctx->weight_cache_valid) {
-		CK(cudaMemsetAsync(ctx->wflags.p, 0, 2 * sizeof(int), st));
-		CK(cudaMemsetAsync(ctx->wpattern.p, 0, (size_t)ctx->R_pad, st));
-		ctx->weight_cache_valid = true;  // from here on the device tracks it
-	}
-	return DFG_OK;
+	if (ctx->refine)
+		if (int rc = prepare_qmap(ctx))
+			return rc;
+	return prepare_weight_cache(ctx);
 }
 
 // Whether one iteration queues its kernels without waiting on the host: the
@@ -1322,9 +1357,299 @@ static int launch_watch(dfg_ctx *ctx, const Chunk &ch) {
 	return DFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// pair lists (restricted searches; kernels in emc_pairs.cuh)
+// ---------------------------------------------------------------------------
+static bool pair_mode(const dfg_ctx *ctx) { return ctx->refine && ctx->pair_lists; }
+
+// The live (tile, frame) pairs of the refinement: a frame's tiles are those
+// holding an orientation of one of its relevant coarse cells; pair ids are
+// tile-major, frames ascending within a tile.
+static int build_pairs(dfg_ctx *ctx) {
+	const int N = ctx->N, R = ctx->num_rot, RT = (R + TILE - 1) / TILE, nc = ctx->num_coarse;
+	cudaStream_t st = ctx->stream;
+	// tiles of each coarse cell, ascending
+	std::vector<long long> coff((size_t)nc + 1, 0);
+	std::vector<int> last((size_t)nc, -1);
+	for (int r = 0; r < R; ++r) {
+		const int c = ctx->h_qmap[r], t = r / TILE;
+		if (last[c] != t) {
+			last[c] = t;
+			coff[c + 1]++;
+		}
+	}
+	for (int c = 0; c < nc; ++c)
+		coff[c + 1] += coff[c];
+	std::vector<int> ctiles((size_t)coff[nc]);
+	{
+		std::vector<long long> cur(coff.begin(), coff.end() - 1);
+		std::fill(last.begin(), last.end(), -1);
+		for (int r = 0; r < R; ++r) {
+			const int c = ctx->h_qmap[r], t = r / TILE;
+			if (last[c] != t) {
+				last[c] = t;
+				ctiles[cur[c]++] = t;
+			}
+		}
+	}
+	// each frame's tiles, ascending
+	std::vector<long long> foff((size_t)N + 1, 0);
+	std::vector<int> ftile, stamp((size_t)RT, -1), tmp;
+	for (int d = 0; d < N; ++d) {
+		tmp.clear();
+		for (long long k = ctx->h_rel_off[d]; k < ctx->h_rel_off[d + 1]; ++k) {
+			const int c = ctx->h_rel[k];
+			for (long long j = coff[c]; j < coff[c + 1]; ++j)
+				if (stamp[ctiles[j]] != d) {
+					stamp[ctiles[j]] = d;
+					tmp.push_back(ctiles[j]);
+				}
+		}
+		std::sort(tmp.begin(), tmp.end());
+		ftile.insert(ftile.end(), tmp.begin(), tmp.end());
+		foff[d + 1] = (long long)ftile.size();
+	}
+	const long long np = foff[N];
+	NEED(np < (long long)INT32_MAX, DFG_ERR_ARG, "pair lists: %lld pairs exceed the int32 pair index", np);
+	std::vector<long long> toff((size_t)RT + 1, 0);
+	for (int t : ftile)
+		toff[t + 1]++;
+	for (int t = 0; t < RT; ++t)
+		toff[t + 1] += toff[t];
+	std::vector<long long> cur(toff.begin(), toff.end() - 1);
+	std::vector<int> ptile((size_t)np), pframe((size_t)np), fpair((size_t)np);
+	for (int d = 0; d < N; ++d)
+		for (long long k = foff[d]; k < foff[d + 1]; ++k) {
+			const int t = ftile[k];
+			const long long q = cur[t]++;
+			ptile[q] = t;
+			pframe[q] = d;
+			fpair[k] = (int)q;
+		}
+	CK(upload(ctx->frame_off, foff.data(), foff.size(), st));
+	CK(upload(ctx->tile_off, toff.data(), toff.size(), st));
+	CK(upload(ctx->pair_tile, ptile.data(), ptile.size(), st));
+	CK(upload(ctx->pair_frame, pframe.data(), pframe.size(), st));
+	CK(upload(ctx->frame_pair, fpair.data(), fpair.size(), st));
+	CK(cudaStreamSynchronize(st));
+	ctx->npairs = np;
+	ctx->h_tile_off = std::move(toff);
+	ctx->pairs_valid = true;
+	return DFG_OK;
+}
+
+// Per frame, its photons on mask < 2 pixels as pixel | count << IDX_BITS
+// words (the frame-major tomogram scatter).
+static int build_mstep_words(dfg_ctx *ctx) {
+	const int N = ctx->N;
+	const uint8_t *mk = ctx->h_mask.data();
+	std::vector<uint32_t> words;
+	std::vector<long long> off((size_t)N + 1, 0);
+	for (int d = 0; d < N; ++d) {
+		for (long long i = ctx->h_ones_off[d]; i < ctx->h_ones_off[d + 1]; ++i)
+			if (mk[ctx->h_place_ones[i]] < 2)
+				push_word(words, (uint32_t)ctx->h_place_ones[i], 1);
+		for (long long i = ctx->h_multi_off[d]; i < ctx->h_multi_off[d + 1]; ++i)
+			if (mk[ctx->h_place_multi[i]] < 2)
+				push_word(words, (uint32_t)ctx->h_place_multi[i], ctx->h_count_multi[i]);
+		off[d + 1] = (long long)words.size();
+	}
+	CK(upload(ctx->mw, words.data(), words.size(), ctx->stream));
+	CK(upload(ctx->mw_off, off.data(), off.size(), ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->mw_valid = true;
+	return DFG_OK;
+}
+
+// Buffers of the pair layout. The dense layout's log-slices, tomograms and
+// per-pair arrays are released (the next full search allocates them again).
+static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par) {
+	NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0 && ctx->S > 0, DFG_ERR_STATE,
+	     "pair lists: set detector, frames, quaternions and model first");
+	NEED(ctx->beta_set, DFG_ERR_STATE, "beta not set (dfg_calc_beta or dfg_set_beta_start)");
+	NEED(ctx->M == 1, DFG_ERR_ARG, "refinement needs num_modes == 1");
+	NEED(ctx->model_type == MT_3D, DFG_ERR_ARG, "pair lists: 3-D models only");
+	NEED(!ctx->keep_prob, DFG_ERR_ARG, "pair lists: keep_prob (sparse probability lists) is not supported");
+	NEED(!(ctx->with_bg && par->need_scaling), DFG_ERR_ARG, "pair lists: no background-aware updates");
+	ctx->R = ctx->num_rot;
+	ctx->RT = (ctx->R + TILE - 1) / TILE;
+	ctx->R_pad = ctx->RT * TILE;
+	if (!ctx->pairs_valid)
+		if (int rc = build_pairs(ctx))
+			return rc;
+	if (!ctx->mw_valid)
+		if (int rc = build_mstep_words(ctx))
+			return rc;
+	ctx->logW.release();
+	ctx->T.release();
+	ctx->pval.release();
+	ctx->Pst.release();
+	ctx->tmax.release();
+	ctx->targ.release();
+	ctx->tlive.release();
+	ctx->chunks_R = -1;
+	dense_release(ctx);
+	const size_t N = (size_t)ctx->N, P = (size_t)ctx->P;
+	CK(ctx->u.ensure((size_t)ctx->R_pad));
+	CK(ctx->logw.ensure((size_t)ctx->R_pad));
+	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
+	CK(ctx->scalars.ensure(8));
+	CK(ctx->red_part.ensure(std::max<size_t>(blocks_for((long long)ctx->M * ctx->V, 256), 1024)));
+	CK(ctx->rmax.ensure(N));
+	CK(ctx->num_prob.ensure(N));
+	CK(ctx->info.ensure(N));
+	CK(ctx->likelihood.ensure(N));
+	CK(ctx->max_exp.ensure(N));
+	CK(ctx->p_norm.ensure(N));
+	CK(ctx->psum_d.ensure(N));
+	CK(ctx->quat_norm.ensure(N * ctx->M));
+	CK(ctx->raw.ensure((size_t)std::max<long long>(ctx->npairs, 1) * TILE));
+	CK(ctx->Pq.ensure((size_t)std::max<long long>(ctx->npairs, 1) * TILE));
+	// one orientation block: (P + 1) x 128 floats per tile (log-slices with
+	// their zero row; the tomograms use P rows of the same space)
+	const size_t tile_bytes = (P + 1) * TILE * sizeof(float);
+	if (ctx->blk_tiles <= 0 || ctx->blk.n < (size_t)ctx->blk_tiles * (P + 1) * TILE) {
+		size_t budget;
+		if (ctx->block_budget_mb > 0.) {
+			budget = (size_t)(ctx->block_budget_mb * 1048576.);
+		} else {
+			ctx->blk.release();
+			size_t fr = 0, tot = 0;
+			CK(cudaMemGetInfo(&fr, &tot));
+			budget = (size_t)(0.8 * (double)fr);
+		}
+		ctx->blk_tiles = (int)std::max<size_t>(1, std::min<size_t>((size_t)ctx->RT, budget / tile_bytes));
+		CK(ctx->blk.ensure((size_t)ctx->blk_tiles * (P + 1) * TILE));
+	}
+	return DFG_OK;
+}
+
+// maximize over pair lists: per orientation block its slices and the E-step
+// of its pairs; u_r and the rescale factor once every block is sliced; the
+// normalisation, watched frames and psum_r over all pairs; per block the
+// tomogram scatter and its merge.
+static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
+	cudaStream_t st = ctx->stream;
+	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT;
+	const long long S = ctx->S, V = ctx->V;
+	const int nblk = (P + PB - 1) / PB, BT = ctx->blk_tiles;
+	const RefineMask rm{ctx->qmap.p, ctx->rel_bits.p, ctx->rwords};
+	const int ob = slice_block_for(ctx);
+	{
+		double factor = std::pow(par->beta_jump, (double)((par->iteration - 1) / par->beta_period));
+		factor *= par->beta_factor;
+		beta_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->beta_start.p, ctx->blacklist.p, N, factor,
+		                                                 ctx->beta.p);
+		CKL("beta_kernel");
+	}
+	for (int t0 = 0; t0 < RT; t0 += BT) {
+		const int nt = std::min(BT, RT - t0), r0 = t0 * TILE, Rb = std::min(R - r0, nt * TILE);
+		phase_begin(ctx, PH_SLICE);
+		// zero row (pixel P) of every tile: the M-step of the last block wrote over it
+		CK(cudaMemset2DAsync(ctx->blk.p + (size_t)P * TILE, (size_t)(P + 1) * TILE * sizeof(float), 0,
+		                     TILE * sizeof(float), nt, st));
+		const int nb = nt * TILE / ob;
+#define DFG_SLICE_B(OBV)                                                                                      	slice_u_kernel<double, OBV, MT_3D><<<nb, 256, 0, st>>>(ctx->quats.p + 5 * (size_t)r0, 1, Rb, ctx->qvals.p,    	                                                       ctx->corr.p, ctx->mask.p, P, ctx->model1.p, S, V,    	                                                       ctx->blk.p, ctx->u.p + r0, nullptr)
+		if (ob == TILE)
+			slice_u_tile_kernel<double, MT_3D><<<nt, 256, 0, st>>>(ctx->quats.p + 5 * (size_t)r0, 1, Rb,
+			                                                       ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
+			                                                       ctx->model1.p, S, V, ctx->blk.p,
+			                                                       ctx->u.p + r0, nullptr);
+		else if (ob == 64)
+			DFG_SLICE_B(TILE >= 64 ? 64 : 16);
+		else if (ob == 32)
+			DFG_SLICE_B(32);
+		else
+			DFG_SLICE_B(16);
+#undef DFG_SLICE_B
+		CKL("slice_u_kernel");
+		phase_end(ctx, PH_SLICE, 1);
+		phase_begin(ctx, PH_ESTEP);
+		const long long q0 = ctx->h_tile_off[t0], nq = ctx->h_tile_off[t0 + nt] - q0;
+		if (nq > 0) {
+			estep_pairs_kernel<<<blocks_for(nq, 8), 256, 0, st>>>(
+			    ctx->blk.p, t0, q0, nq, ctx->pair_tile.p, ctx->pair_frame.p, ctx->ph.p, ctx->ph_off.p,
+			    ctx->ph_mid.p, ctx->blacklist.p, R, P, rm, ctx->raw.p);
+			CKL("estep_pairs_kernel");
+		}
+		phase_end(ctx, PH_ESTEP, nq > 0 ? 1 : 0);
+	}
+	phase_begin(ctx, PH_SLICE);
+	rescale_kernel<<<1, 256, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
+	CKL("rescale_kernel");
+	logw_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->quats.p, M, R, ctx->logw.p);
+	CKL("logw_kernel");
+	phase_end(ctx, PH_SLICE, 2);
+
+	const int use_scale = par->need_scaling && (par->iteration > 1 || par->known_scale);
+	const int psum_d_on = par->need_scaling && par->update_scale;
+	phase_begin(ctx, PH_NORM);
+	norm_pairs_kernel<<<blocks_for((long long)N * 32, 256), 256, 0, st>>>(
+	    ctx->raw.p, ctx->frame_off.p, ctx->frame_pair.p, ctx->pair_tile.p, N, R, ctx->logw.p, ctx->u.p,
+	    ctx->scale.p, use_scale, ctx->beta.p, ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p,
+	    ctx->Pq.p, ctx->rmax.p, ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p,
+	    ctx->num_prob.p);
+	CKL("norm_pairs_kernel");
+	const int nw = (int)ctx->h_watch.size();
+	if (nw > 0) {
+		captured_mass_pairs_kernel<<<blocks_for((long long)nw * 32, 256), 256, 0, st>>>(
+		    ctx->Pq.p, ctx->frame_off.p, ctx->frame_pair.p, ctx->pair_tile.p, ctx->qmap.p, ctx->watch_local.p, nw,
+		    ctx->watch_bits.p, ctx->rwords, ctx->watch_mass.p);
+		CKL("captured_mass_pairs_kernel");
+	}
+	phase_end(ctx, PH_NORM, nw > 0 ? 2 : 1);
+	phase_begin(ctx, PH_PSUM);
+	psum_pairs_kernel<<<RT, 256, 0, st>>>(ctx->Pq.p, ctx->tile_off.p, ctx->pair_frame.p, ctx->scale.p,
+	                                      par->need_scaling, R, ctx->psum_r.p);
+	CKL("psum_pairs_kernel");
+	phase_end(ctx, PH_PSUM, 1);
+
+	weight_pattern_kernel<<<1, 1024, 0, st>>>(ctx->psum_r.p, R, ctx->wpattern.p, ctx->wflags.p);
+	CKL("weight_pattern_kernel");
+	CK(cudaMemsetAsync(ctx->accum.p, 0, (size_t)M * V * sizeof(double2), st));
+	for (int t0 = 0; t0 < RT; t0 += BT) {
+		const int nt = std::min(BT, RT - t0), r0 = t0 * TILE, Rb = std::min(R - r0, nt * TILE);
+		phase_begin(ctx, PH_MSTEP);
+		CK(cudaMemsetAsync(ctx->blk.p, 0, (size_t)nt * P * TILE * sizeof(float), st));
+		const long long q0 = ctx->h_tile_off[t0], nq = ctx->h_tile_off[t0 + nt] - q0;
+		if (nq > 0) {
+			mstep_pairs_kernel<<<blocks_for(nq, 8), 256, 0, st>>>(ctx->Pq.p, t0, q0, nq, ctx->pair_tile.p,
+			                                                       ctx->pair_frame.p, ctx->mw.p, ctx->mw_off.p, P,
+			                                                       ctx->blk.p);
+			CKL("mstep_pairs_kernel");
+		}
+		phase_end(ctx, PH_MSTEP, nq > 0 ? 1 : 0);
+		phase_begin(ctx, PH_MERGE);
+		merge_kernel<MT_3D><<<dim3(nblk, nt), 256, 0, st>>>(ctx->blk.p, ctx->psum_r.p + r0,
+		                                                     ctx->quats.p + 5 * (size_t)r0, 1, Rb, ctx->qvals.p,
+		                                                     ctx->corr.p, ctx->mask.p, P, S, V,
+		                                                     (double *)ctx->accum.p, ctx->wflags.p, 0);
+		CKL("merge_kernel");
+		phase_end(ctx, PH_MERGE, 1);
+	}
+	phase_begin(ctx, PH_UPDATE);
+	unpack_accum_kernel<<<blocks_for((long long)M * V, 256), 256, 0, st>>>(
+	    ctx->accum.p, (long long)M * V, ctx->model2.p, ctx->weight.p, ctx->weight_cache.p, ctx->wflags.p);
+	CKL("unpack_accum_kernel");
+	frame_totals_kernel<<<1, 1024, 0, st>>>(ctx->info.p, ctx->likelihood.p, ctx->blacklist.p, N,
+	                                        ctx->scalars.p + 1);
+	CKL("frame_totals_kernel");
+	if (par->need_scaling && par->update_scale) {
+		scale_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->fcounts.p, ctx->psum_d.p, ctx->blacklist.p, N,
+		                                                  ctx->scale.p);
+		CKL("scale_kernel");
+	}
+	phase_end(ctx, PH_UPDATE, par->need_scaling && par->update_scale ? 3 : 2);
+	ctx->views_final = false;
+	return DFG_OK;
+}
+
 // Queues maximize's kernels (after max_prepare). Synchronises only where
 // graphable() is false.
 static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
+	ctx->last_pairs = pair_mode(ctx);
+	if (ctx->last_pairs)
+		return max_enqueue_pairs(ctx, par);
 	cudaStream_t st = ctx->stream;
 	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
 	const long long S = ctx->S, V = ctx->V;
@@ -1600,6 +1925,7 @@ extern "C" int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *re
 	if (!ctx || !par)
 		return DFG_ERR_ARG;
 	CK(cudaSetDevice(ctx->device));
+	NEED(!pair_mode(ctx), DFG_ERR_STATE, "autotune: not with pair lists (their kernels have one form)");
 	if (int rc = run_autotune(ctx, par))
 		return rc;
 	if (report)
@@ -2228,6 +2554,7 @@ extern "C" int dfg_get_tomograms(dfg_ctx *ctx, int r0, int n, double *out) {
 	if (!ctx || !out)
 		return DFG_ERR_ARG;
 	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
+	NEED(!ctx->last_pairs, DFG_ERR_STATE, "tomograms are not kept with pair lists (one orientation block at a time)");
 	NEED(r0 >= 0 && n >= 1 && (long long)r0 + n <= ctx->R, DFG_ERR_ARG,
 	     "orientations %d..%lld outside 0..%d", r0, (long long)r0 + n - 1, ctx->R - 1);
 	CK(cudaSetDevice(ctx->device));
@@ -2430,6 +2757,16 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 		const int v = (int)value;
 		NEED(v == 0 || v == 1, DFG_ERR_ARG, "estep_form must be 0 (sparse) or 1 (dense)");
 		ctx->estep_form = v;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "pair_lists")) {
+		ctx->pair_lists = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "block_budget_mb")) {
+		NEED(value >= 0., DFG_ERR_ARG, "block_budget_mb must be >= 0");
+		ctx->block_budget_mb = value;
+		ctx->blk_tiles = 0;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "tile_skip")) {

@@ -205,6 +205,22 @@ struct dfg_ctx {
 	std::vector<int> h_qmap;
 	DevBuf<int> qmap;
 	DevBuf<uint32_t> rel_bits;
+	// pair lists (option pair_lists with refinement): the live (tile, frame)
+	// pairs tile-major, per-pair photon sums and probabilities, one
+	// orientation block's log-slices or tomograms at a time (emc_pairs.cuh)
+	bool pair_lists = false, pairs_valid = false, mw_valid = false, last_pairs = false;
+	double block_budget_mb = 0.;
+	std::vector<long long> h_rel_off;
+	std::vector<int> h_rel;
+	long long npairs = 0;
+	std::vector<long long> h_tile_off;  // [RT + 1]
+	DevBuf<long long> tile_off, frame_off;
+	DevBuf<int> pair_tile, pair_frame, frame_pair;
+	DevBuf<double> raw;
+	DevBuf<float> Pq, blk;
+	int blk_tiles = 0;
+	DevBuf<uint32_t> mw;  // per frame: pixel | count << IDX_BITS on mask < 2 pixels
+	DevBuf<long long> mw_off;
 	bool timing = false;
 	struct PhaseRec {
 		int phase, ev;  // phase, begin event (end = ev + 1) in ev_pool

@@ -44,11 +44,17 @@ class LearnedProposals:
         held_out: share of frames searched in full and watched each iteration.
         threshold: mean captured probability mass below which the next
             iteration searches in full and the network is retrained.
+        pair_lists: run proposal iterations over pair lists (option
+            pair_lists: only the live (tile, frame) pairs are stored and the
+            orientations are processed in blocks, so that neither all
+            log-slices nor all tomograms need to be resident).
     """
 
-    def __init__(self, ctx, qvals, fine, coarse_div=4, K=16, held_out=0.01, threshold=0.99, batch=256, seed=0):
+    def __init__(self, ctx, qvals, fine, coarse_div=4, K=16, held_out=0.01, threshold=0.99, batch=256, seed=0,
+                 pair_lists=False):
         from ._lib import Context, ProposalNet
         self.ctx = ctx
+        ctx.set_option("pair_lists", 1 if pair_lists else 0)
         self.coarse = quat_gen(coarse_div)
         self.nc = self.coarse.shape[0]
         self.K = int(K)

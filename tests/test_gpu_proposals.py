@@ -12,7 +12,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_learned_proposals_against_full_search():
+@pytest.mark.parametrize("pair_lists", [False, True])
+def test_learned_proposals_against_full_search(pair_lists):
     from dragonfly_b200 import synth
     from dragonfly_b200._lib import Context
     from dragonfly_b200.proposals import LearnedProposals, sort_by_coarse
@@ -31,7 +32,8 @@ def test_learned_proposals_against_full_search():
         c.set_quaternions(fine)
         c.set_model(d["model_true"][None])
         c.calc_beta(1., 0)
-    lp = LearnedProposals(restr, d["qvals"], fine, coarse_div=2, K=24, held_out=0.02, threshold=0.99, seed=1)
+    lp = LearnedProposals(restr, d["qvals"], fine, coarse_div=2, K=24, held_out=0.02, threshold=0.99, seed=1,
+                          pair_lists=pair_lists)
     loss = lp.train_simulated(d["model_true"], n_frames=30000, epochs=4)
     # the network's gain: top-K hit rate of the true orientations' cells
     cells = full.voronoi_subset(quat_gen(2), np.pad(d["frame_quats"][:, :4], ((0, 0), (0, 1))))

@@ -150,3 +150,68 @@ def test_gpu_refinement_matches_reference(oracle_built, mode, need_scaling):
         assert all(ok)
     gpu.close()
     ref.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("need_scaling,block_mb", [(0, 0.), (1, 6.)])
+def test_gpu_pair_lists_match_reference(oracle_built, need_scaling, block_mb):
+    """Pair lists (option pair_lists): only the live (tile, frame) pairs are
+    stored, orientations in blocks of whole tiles (block_budget_mb 6: five
+    tiles per block at this detector, six blocks). Against the reference
+    engine with the same lists, and against the dense restricted path: the
+    same log-likelihood sums and kept sets (identical rmax, p_norm and
+    likelihood to FP64 rounding), tomograms scattered with FP32 atomics."""
+    if not reference_available():
+        pytest.skip("reference engine library not built")
+    from dragonfly_b200 import synth
+    d = synth.small_problem(seed=9, det_side=48, size=41, qmax=19., n_atoms=120, atom_radius=7., num_div=4,
+                            n_frames=500, mean_count=80., hole_radius=3.)
+    fine = quat_gen(4)
+    qmap = voronoi_subset_reference(2, fine)
+    order = np.lexsort((np.arange(fine.shape[0]), qmap))   # cells contiguous, as proposals use them
+    fine, qmap = np.ascontiguousarray(fine[order]), np.ascontiguousarray(qmap[order])
+    nc = quat_gen(2).shape[0]
+    rng = np.random.default_rng(17)
+    true_cell = qmap[rng.integers(0, fine.shape[0], d["ones"].size)]
+    rel = _rel_lists(rng, d["ones"].size, nc, true_cell, "lists", allow_empty=not need_scaling)
+    prob = EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"], d["place_multi"],
+                      d["count_multi"], fine, d["model_start"], beta=1., need_scaling=need_scaling,
+                      update_scale=need_scaling)
+    ref = ReferenceEngine(prob)
+    ref.set_refinement(qmap, rel)
+    opts = dict(pair_lists=1)
+    if block_mb:
+        opts["block_budget_mb"] = block_mb
+    gpu = GPUEngine(prob, **opts)
+    gpu.ctx.set_refinement(nc, qmap, rel)
+    dense = GPUEngine(prob)
+    dense.ctx.set_refinement(nc, qmap, rel)
+    for it in (1, 2):
+        a = gpu.run_iteration(it)
+        b = ref.run_iteration(it)
+        c = dense.run_iteration(it)
+        dev = rel_l2(a["model1"], b["model1"])
+        ll = abs(a["avg_likelihood"] - b["avg_likelihood"]) / abs(b["avg_likelihood"])
+        mi = abs(a["mutual_info"] - b["mutual_info"]) / max(abs(b["mutual_info"]), 1e-300)
+        agree = float(np.mean(np.asarray(a["rmax"]) == np.asarray(b["rmax"])))
+        dd = rel_l2(a["model1"], c["model1"])
+        print("pair lists (scaling %d, block %g MB) iteration %d: vs reference model %.2e, ll %.2e, mi %.2e, "
+              "rmax %.4f; vs dense restricted path model %.2e" % (need_scaling, block_mb, it, dev, ll, mi, agree, dd))
+        assert dev <= MODEL_REL_L2 and ll <= SCALAR_REL and mi <= SCALAR_REL, (dev, ll, mi)
+        assert agree >= RMAX_AGREE, agree
+        np.testing.assert_array_equal(a["rmax"], c["rmax"])
+        # iteration 1 starts from the same model: equal sums; later the
+        # models differ by the tomograms' atomic rounding (about 1e-9), which
+        # moves log-likelihoods of about 200 by about 2e-7 and probabilities
+        # by as much relative
+        tol = 1e-12 if it == 1 else 1e-7
+        np.testing.assert_allclose(a["likelihood"], c["likelihood"], rtol=tol, atol=tol)
+        np.testing.assert_allclose(a["psum_r"], c["psum_r"], rtol=1e-12 if it == 1 else 1e-5, atol=1e-300)
+        assert dd <= 1e-6, dd
+        empty = np.array([len(x) == 0 for x in rel])
+        assert (np.asarray(a["rmax"])[empty] == -1).all()
+    with pytest.raises(RuntimeError):
+        gpu.ctx.tomograms(0, 1)        # not kept with pair lists
+    for e in (gpu, dense):
+        e.close()
+    ref.close()
