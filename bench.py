@@ -514,6 +514,138 @@ def run_batched(args):
         c.close()
 
 
+# learned-proposal workload: the production detector and 201^3 model,
+# num_div 20 (400200 orientations), 500000 frames at median 300 photons; a
+# network over 3240 coarse cells (num_div 4), top 16 refined at full
+# resolution, 1 % of the frames searched in full and watched
+PROPOSALS = dict(num_div=20, n_frames=500000, coarse_div=4, K=16, held_out=0.01, threshold=0.99,
+                 train_frames=100000, epochs=2, rounds=10, lr=5e-4, lr_end=1e-4, full_fracs=(8, 4))
+
+
+def _full_search_ms(w, inp, stride, steps, warmup):
+    """Device ms of one full-search iteration (graph, autotuned) over every
+    stride-th orientation of the workload (the full set's log-slices and
+    tomograms, 4 B x R x P each, do not fit one GPU at num_div 20)."""
+    from dragonfly_b200._lib import Context
+    c = Context(0)
+    c.set_detector(inp["qvals"], inp["corr"], inp["mask"])
+    c.simulate_frames(inp["intens"], inp["frame_q"], inp["phi"], seed=777)
+    q = np.ascontiguousarray(inp["quats"][::stride])
+    q[:, 4] = 1. / q.shape[0]
+    c.set_quaternions(q)
+    c.set_model(inp["intens"][None])
+    c.set_scale(inp["phi"])
+    c.calc_beta(1., 1)
+    c.set_option("autotune", 1)
+    par = lambda it: c.params(it, 1, 1, 1, w["beta_jump"], w["beta_period"], 1.)
+    for it in range(1, warmup + 1):
+        c.run_iteration(par(it), 0.)
+    ms = []
+    for it in range(warmup + 1, warmup + 1 + steps):
+        c.event_record(0)
+        c.run_iteration(par(it), 0.)
+        c.event_record(1)
+        ms.append(c.event_elapsed_ms(0, 1))
+    R = q.shape[0]
+    c.close()
+    return R, float(np.mean(ms))
+
+
+def run_proposals(args):
+    """The learned-proposal workload: proposal-restricted iterations over pair
+    lists (network images and top-K, restriction lists, iteration; wall clock)
+    against the plain full search, whose time is measured on every 8th and
+    every 4th orientation and extrapolated linearly to all of them. Prints one
+    JSON line."""
+    import torch
+    from dragonfly_b200._lib import Context
+    from dragonfly_b200.proposals import LearnedProposals, sort_by_coarse
+    P_ = dict(PROPOSALS)
+    w = dict(WORKLOAD)
+    w.update(num_div=P_["num_div"], n_frames=args.frames or P_["n_frames"])
+    if args.num_div:
+        w["num_div"] = args.num_div
+    t0 = time.perf_counter()
+    inp = build_inputs(w)
+    R = inp["quats"].shape[0]
+    N = w["n_frames"]
+    # the full search at two orientation subsets
+    full = {}
+    for stride in P_["full_fracs"]:
+        full[stride] = _full_search_ms(w, inp, stride, 1, 1)
+    (Ra, ta), (Rb, tb) = full[P_["full_fracs"][0]], full[P_["full_fracs"][1]]
+    slope = (tb - ta) / (Rb - Ra)
+    full_ms = tb + slope * (R - Rb)
+    torch.cuda.synchronize()
+    # the proposal form at the full orientation set
+    c = Context(0)
+    c.set_detector(inp["qvals"], inp["corr"], inp["mask"])
+    c.simulate_frames(inp["intens"], inp["frame_q"], inp["phi"], seed=777)
+    fine, _, _ = sort_by_coarse(inp["quats"], P_["coarse_div"], c)
+    c.set_quaternions(fine)
+    c.set_model(inp["intens"][None])
+    c.set_scale(inp["phi"])
+    c.calc_beta(1., 1)
+    setup_s = time.perf_counter() - t0
+    lp = LearnedProposals(c, inp["qvals"], fine, coarse_div=P_["coarse_div"], K=P_["K"], held_out=P_["held_out"],
+                          threshold=P_["threshold"], seed=5, pair_lists=True)
+    t1 = time.perf_counter()
+    loss = lp.train_simulated(inp["intens"], n_frames=P_["train_frames"], epochs=P_["epochs"], lr=P_["lr"],
+                              lr_end=P_["lr_end"], rounds=P_["rounds"],
+                              phi=np.exp(np.random.default_rng(9).normal(0., w["fluence_sigma"],
+                                                                          P_["train_frames"])))
+    train_s = time.perf_counter() - t1
+    # hit rate of the true orientation's cell
+    cells = c.voronoi_subset(lp.coarse, np.pad(inp["frame_q"][:, :4], ((0, 0), (0, 1))))
+    par = lambda it: c.params(it, 1, 1, 1, w["beta_jump"], w["beta_period"], 1.)
+    runs = []
+    c.set_option("timing", 1)
+    for it in range(1, args.warmup + args.steps + 1):
+        if it == args.warmup + 1:
+            c.reset_phase_times()
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        out = lp.proposal_iteration(par(it), 0.)
+        torch.cuda.synchronize()
+        runs.append(dict(wall_ms=1e3 * (time.perf_counter() - ts), mass=out["captured_mass"],
+                         min_mass=out["min_mass"], propose_ms=1e3 * out["propose_s"], lists_ms=1e3 * out["lists_s"],
+                         iterate_ms=1e3 * out["iterate_s"], fallback_next=lp.full_next))
+    phases = {k: round(v[0] / args.steps, 1) for k, v in c.phase_times().items()}
+    top = lp.propose()
+    hit = float(np.mean(np.any(top == cells[:, None], axis=1)))
+    wl = c.workload()
+    timed = runs[args.warmup:]
+    ms = float(np.mean([r["wall_ms"] for r in timed]))
+    it_ms = float(np.mean([r["iterate_ms"] for r in timed]))
+    tiles = -(-R // 128)
+    out = {"metric": "s per EMC iteration, learned-proposal form vs plain full search",
+           "value": ms / 1e3, "unit": "s/iteration", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "bf16 network / f64 accumulate / f32 log-slices",
+           "data": "synthetic (seeded; frames simulated on the GPU; model at the truth, true scales, beta 1)",
+           "config": {"workload": "learned proposals: 260x257 pnCCD-like detector, 201^3 model, num_div %d (%d "
+                                  "orientations), %d frames, median %g photons (lognormal sigma %g); %d coarse "
+                                  "cells (num_div %d), top %d, %g %% held out" % (
+                                      w["num_div"], R, N, w["median_photons"], w["fluence_sigma"], lp.nc,
+                                      P_["coarse_div"], P_["K"], 100 * P_["held_out"]),
+                      "setup_s": setup_s, "train_s": train_s,
+                      "training": "%d rounds x %d epochs of %d newly simulated frames, lr %g -> %g" % (
+                          P_["rounds"], P_["epochs"], P_["train_frames"], P_["lr"], P_["lr_end"]),
+                      "train_loss": loss},
+           "proposal": {"wall_ms": ms, "iteration_ms": it_ms, "phases_ms": phases, "runs": timed,
+                        "live_pairs": wl["live_pairs"], "block_tiles": wl["block_tiles"],
+                        "live_fraction_of_tiles": wl["live_pairs"] / float(tiles * N),
+                        "top_k_hit_rate": hit, "evaluated_fraction_of_cells": out["evaluated_fraction"]},
+           "full_search": {"ms_extrapolated": full_ms,
+                           "measured": {str(Rx): tx for Rx, tx in full.values()},
+                           "rule": "t(R) linear in R through the two measured subsets"},
+           "speedup_vs_full_search": full_ms / ms,
+           "effective_pairs_per_s": R * N / (ms / 1e3)}
+    print(json.dumps(out))
+    lp.close()
+    c.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -527,9 +659,10 @@ def main():
     ap.add_argument("--fluence-sigma", type=float, default=-1., help="override the lognormal fluence sigma")
     ap.add_argument("--estep-form", default="auto", choices=["auto", "sparse", "dense"],
                     help="E-step photon term: autotuned (default), sparse gathers or tensor-core products")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "proposals"],
                     help="plain: the production-size iteration (default); batched: nine reconstructions "
-                         "iterated together against one after another")
+                         "iterated together against one after another; proposals: the learned-proposal "
+                         "form at num_div 20 against the full search")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
@@ -537,6 +670,16 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "proposals":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned-proposal "
+                                  "form, and its full search at 400200 orientations x 500000 frames would run "
+                                  "for days on the host cores"}))
+            return
+        if rank == 0:
+            run_proposals(args)
+        return
     if args.workload == "batched":
         if args.impl == "reference":
             if rank == 0:

@@ -87,6 +87,7 @@ _SIGS = {
     "dfg_pnet_get_images": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "dfg_pnet_train": (C.c_int, [_V, _I, C.c_int, C.c_double, C.c_ulonglong, _D]),
     "dfg_pnet_topk": (C.c_int, [_V, C.c_int, _I]),
+    "dfg_pnet_set_tensor_cores": (C.c_int, [_V, C.c_int]),
     "dfg_pnet_logits": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "dfg_pnet_gradients": (C.c_int, [_V, _I, C.POINTER(C.c_float), _D]),
     "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
@@ -143,6 +144,24 @@ def ptr(a, ctype):
         return None
     assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
     return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _csr(lists):
+    """(offsets int64 [n + 1], flat int32) of per-item lists given as a
+    sequence of arrays, a 2-D array (equal lengths) or an (offsets, flat)
+    tuple."""
+    if isinstance(lists, tuple):
+        off, flat = lists
+        return np.ascontiguousarray(off, np.int64), np.ascontiguousarray(flat, np.int32)
+    if isinstance(lists, np.ndarray) and lists.ndim == 2:
+        n, k = lists.shape
+        return np.arange(n + 1, dtype=np.int64) * k, np.ascontiguousarray(lists, np.int32).ravel()
+    lens = np.array([len(x) for x in lists], np.int64)
+    off = np.zeros(len(lens) + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in lists])
+                                if len(lens) else np.zeros(0, np.int32), np.int32)
+    return off, flat
 
 
 class Context:
@@ -241,30 +260,26 @@ class Context:
     def set_refinement(self, num_coarse=0, quat_mapping=None, rel_quat=None):
         """Coarse-to-fine refinement: frame d evaluates orientation r only
         when quat_mapping[r] is in rel_quat[d] (a sequence of per-frame
-        coarse-orientation lists). quat_mapping None switches it off."""
+        coarse-orientation lists, a 2-D array with one row per frame, or a
+        tuple (offsets [N + 1], flat lists)). quat_mapping None switches it
+        off."""
         if quat_mapping is None:
             self.call("dfg_set_refinement", 0, None, None, None)
             return
         qm = np.ascontiguousarray(quat_mapping, np.int32).ravel()
-        lens = np.array([len(x) for x in rel_quat], np.int64)
-        off = np.zeros(len(lens) + 1, np.int64)
-        np.cumsum(lens, out=off[1:])
-        flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in rel_quat])
-                                    if len(lens) else np.zeros(0, np.int32), np.int32)
+        off, flat = _csr(rel_quat)
         self.call("dfg_set_refinement", int(num_coarse), ptr(qm, C.c_int), ptr(off, C.c_longlong),
                   ptr(flat, C.c_int))
 
     def set_watch(self, frames, cells):
-        """Watched frames (ascending) with a coarse-cell list each; None clears."""
+        """Watched frames (ascending) with a coarse-cell list each (lists, a
+        2-D array or (offsets, flat) as set_refinement); None clears."""
         if frames is None or len(frames) == 0:
             self.call("dfg_set_watch", 0, None, None, None)
             self._n_watch = 0
             return
         fr = np.ascontiguousarray(frames, np.int32)
-        lens = np.array([len(x) for x in cells], np.int64)
-        off = np.zeros(len(lens) + 1, np.int64)
-        np.cumsum(lens, out=off[1:])
-        flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in cells]), np.int32)
+        off, flat = _csr(cells)
         self.call("dfg_set_watch", fr.size, ptr(fr, C.c_int), ptr(off, C.c_longlong), ptr(flat, C.c_int))
         self._n_watch = fr.size
 
@@ -511,10 +526,10 @@ class Context:
         return ms.value
 
     def workload(self):
-        out = (C.c_longlong * 9)()
+        out = (C.c_longlong * 11)()
         self.call("dfg_get_workload", out)
         keys = ("num_orient", "num_data", "estep_entries", "mstep_entries", "chunks", "chunk_frames",
-                "launches", "k_pad", "dense_estep")
+                "launches", "k_pad", "dense_estep", "live_pairs", "block_tiles")
         return dict(zip(keys, list(out)))
 
 
@@ -637,6 +652,11 @@ class ProposalNet:
         loss = C.c_double(0.)
         self._call("dfg_pnet_train", ptr(lab, C.c_int), int(epochs), float(lr), int(seed), C.byref(loss))
         return loss.value
+
+    def set_tensor_cores(self, on):
+        """Inference products on the tcgen05 tensor cores (default) or the
+        FP32 path training uses."""
+        self._call("dfg_pnet_set_tensor_cores", 1 if on else 0)
 
     def topk(self, K):
         out = np.zeros((self.n_images, int(K)), np.int32)

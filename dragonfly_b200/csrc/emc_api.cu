@@ -11,6 +11,8 @@
 
 #include <cudaTypedefs.h>
 
+#include <thread>
+
 #include "emc_ctx.cuh"
 #include "emc_device.cuh"
 #include "emc_bg.cuh"
@@ -143,6 +145,19 @@ extern "C" int dfg_set_detector(dfg_ctx *ctx, int num_pix, const double *qvals, 
 			return rc;
 	}
 	return DFG_OK;
+}
+
+// Runs fn(thread, begin, end) over [0, n) split into contiguous ranges, one
+// per host thread (ascending ranges for ascending thread numbers).
+template <typename F>
+static void parallel_ranges(long long n, int threads, F fn) {
+	std::vector<std::thread> pool;
+	for (int k = 0; k < threads; ++k) {
+		const long long b = n * k / threads, e = n * (k + 1) / threads;
+		pool.emplace_back([=, &fn] { fn(k, b, e); });
+	}
+	for (auto &t : pool)
+		t.join();
 }
 
 // Packs (index, count) words, splitting counts above MAX_COUNT.
@@ -357,15 +372,28 @@ extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_
 		NEED(quat_mapping[r] >= 0 && quat_mapping[r] < num_coarse, DFG_ERR_ARG,
 		     "refinement: quat_mapping[%d] = %d outside [0, %d)", r, quat_mapping[r], num_coarse);
 	NEED(rel_off[0] == 0, DFG_ERR_ARG, "refinement: rel_off[0] must be 0");
-	std::vector<uint32_t> bits((size_t)N * rw, 0u);
-	for (int d = 0; d < N; ++d) {
+	for (int d = 0; d < N; ++d)
 		NEED(rel_off[d + 1] >= rel_off[d], DFG_ERR_ARG, "refinement: rel_off decreases at frame %d", d);
-		for (long long t = rel_off[d]; t < rel_off[d + 1]; ++t) {
-			const int c = rel_quat[t];
-			NEED(c >= 0 && c < num_coarse, DFG_ERR_ARG, "refinement: frame %d lists coarse orientation %d", d, c);
-			bits[(size_t)d * rw + (c >> 5)] |= 1u << (c & 31);
-		}
-	}
+	// one bit per relevant coarse orientation, frames split over the host
+	// threads; the first bad entry of each range is reported
+	std::vector<uint32_t> bits((size_t)N * rw, 0u);
+	const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+	std::vector<long long> bad((size_t)nth, -1);
+	parallel_ranges(N, std::min<int>(nth, std::max(1, N / 4096)), [&](int k, long long b, long long e) {
+		for (long long d = b; d < e; ++d)
+			for (long long t = rel_off[d]; t < rel_off[d + 1]; ++t) {
+				const int c = rel_quat[t];
+				if (c < 0 || c >= num_coarse) {
+					if (bad[k] < 0)
+						bad[k] = t;
+					continue;
+				}
+				bits[(size_t)d * rw + (c >> 5)] |= 1u << (c & 31);
+			}
+	});
+	for (long long t : bad)
+		NEED(t < 0, DFG_ERR_ARG, "refinement: entry %lld lists coarse orientation %d outside [0, %d)", t, rel_quat[t],
+		     num_coarse);
 	CK(cudaSetDevice(ctx->device));
 	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
@@ -1364,7 +1392,10 @@ static bool pair_mode(const dfg_ctx *ctx) { return ctx->refine && ctx->pair_list
 
 // The live (tile, frame) pairs of the refinement: a frame's tiles are those
 // holding an orientation of one of its relevant coarse cells; pair ids are
-// tile-major, frames ascending within a tile.
+// tile-major, frames ascending within a tile. Built on the host threads over
+// contiguous frame ranges: each range's tile lists and per-tile counts, then
+// per-range cursors into each tile's pair range (ranges in frame order, so
+// frames stay ascending within a tile).
 static int build_pairs(dfg_ctx *ctx) {
 	const int N = ctx->N, R = ctx->num_rot, RT = (R + TILE - 1) / TILE, nc = ctx->num_coarse;
 	cudaStream_t st = ctx->stream;
@@ -1392,40 +1423,66 @@ static int build_pairs(dfg_ctx *ctx) {
 			}
 		}
 	}
-	// each frame's tiles, ascending
-	std::vector<long long> foff((size_t)N + 1, 0);
-	std::vector<int> ftile, stamp((size_t)RT, -1), tmp;
-	for (int d = 0; d < N; ++d) {
-		tmp.clear();
-		for (long long k = ctx->h_rel_off[d]; k < ctx->h_rel_off[d + 1]; ++k) {
-			const int c = ctx->h_rel[k];
-			for (long long j = coff[c]; j < coff[c + 1]; ++j)
-				if (stamp[ctiles[j]] != d) {
-					stamp[ctiles[j]] = d;
-					tmp.push_back(ctiles[j]);
-				}
+	const int TH = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+	const int nth = (int)std::min<long long>(TH, std::max(1, N / 4096));
+	// pass 1: each frame's tiles (ascending) and per-range tile counts
+	std::vector<std::vector<int>> ftile_th((size_t)nth);
+	std::vector<std::vector<long long>> tcount_th((size_t)nth, std::vector<long long>((size_t)RT, 0));
+	std::vector<long long> fcount((size_t)N);
+	parallel_ranges(N, nth, [&](int k, long long b, long long e) {
+		std::vector<int> stamp((size_t)RT, -1), tmp;
+		auto &out = ftile_th[k];
+		auto &tc = tcount_th[k];
+		for (long long d = b; d < e; ++d) {
+			tmp.clear();
+			for (long long j = ctx->h_rel_off[d]; j < ctx->h_rel_off[d + 1]; ++j) {
+				const int c = ctx->h_rel[j];
+				for (long long q = coff[c]; q < coff[c + 1]; ++q)
+					if (stamp[ctiles[q]] != (int)d) {
+						stamp[ctiles[q]] = (int)d;
+						tmp.push_back(ctiles[q]);
+					}
+			}
+			std::sort(tmp.begin(), tmp.end());
+			out.insert(out.end(), tmp.begin(), tmp.end());
+			fcount[d] = (long long)tmp.size();
+			for (int t : tmp)
+				tc[t]++;
 		}
-		std::sort(tmp.begin(), tmp.end());
-		ftile.insert(ftile.end(), tmp.begin(), tmp.end());
-		foff[d + 1] = (long long)ftile.size();
-	}
+	});
+	std::vector<long long> foff((size_t)N + 1, 0);
+	for (int d = 0; d < N; ++d)
+		foff[d + 1] = foff[d] + fcount[d];
 	const long long np = foff[N];
 	NEED(np < (long long)INT32_MAX, DFG_ERR_ARG, "pair lists: %lld pairs exceed the int32 pair index", np);
 	std::vector<long long> toff((size_t)RT + 1, 0);
-	for (int t : ftile)
-		toff[t + 1]++;
-	for (int t = 0; t < RT; ++t)
-		toff[t + 1] += toff[t];
-	std::vector<long long> cur(toff.begin(), toff.end() - 1);
+	for (int t = 0; t < RT; ++t) {
+		long long s = 0;
+		for (int k = 0; k < nth; ++k)
+			s += tcount_th[k][t];
+		toff[t + 1] = toff[t] + s;
+	}
+	// pass 2: per-range cursors, then the pair arrays
 	std::vector<int> ptile((size_t)np), pframe((size_t)np), fpair((size_t)np);
-	for (int d = 0; d < N; ++d)
-		for (long long k = foff[d]; k < foff[d + 1]; ++k) {
-			const int t = ftile[k];
-			const long long q = cur[t]++;
-			ptile[q] = t;
-			pframe[q] = d;
-			fpair[k] = (int)q;
+	parallel_ranges(N, nth, [&](int k, long long b, long long e) {
+		std::vector<long long> cur((size_t)RT);
+		for (int t = 0; t < RT; ++t) {
+			long long s = toff[t];
+			for (int j = 0; j < k; ++j)
+				s += tcount_th[j][t];
+			cur[t] = s;
 		}
+		const auto &ft = ftile_th[k];
+		long long i = 0;
+		for (long long d = b; d < e; ++d)
+			for (long long j = foff[d]; j < foff[d + 1]; ++j, ++i) {
+				const int t = ft[i];
+				const long long q = cur[t]++;
+				ptile[q] = t;
+				pframe[q] = (int)d;
+				fpair[j] = (int)q;
+			}
+	});
 	CK(upload(ctx->frame_off, foff.data(), foff.size(), st));
 	CK(upload(ctx->tile_off, toff.data(), toff.size(), st));
 	CK(upload(ctx->pair_tile, ptile.data(), ptile.size(), st));
@@ -1493,6 +1550,7 @@ static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CK(ctx->u.ensure((size_t)ctx->R_pad));
 	CK(ctx->logw.ensure((size_t)ctx->R_pad));
 	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
+	CK(ctx->wsign.ensure((size_t)ctx->R_pad));
 	CK(ctx->scalars.ensure(8));
 	CK(ctx->red_part.ensure(std::max<size_t>(blocks_for((long long)ctx->M * ctx->V, 256), 1024)));
 	CK(ctx->rmax.ensure(N));
@@ -1503,8 +1561,18 @@ static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CK(ctx->p_norm.ensure(N));
 	CK(ctx->psum_d.ensure(N));
 	CK(ctx->quat_norm.ensure(N * ctx->M));
-	CK(ctx->raw.ensure((size_t)std::max<long long>(ctx->npairs, 1) * TILE));
-	CK(ctx->Pq.ensure((size_t)std::max<long long>(ctx->npairs, 1) * TILE));
+	// per-pair buffers with 10 % headroom (the live pairs change with every
+	// new restriction); the block buffer, sized from the memory left, gives
+	// way when they grow
+	const size_t need = (size_t)std::max<long long>(ctx->npairs, 1) * TILE;
+	if (ctx->raw.n < need || ctx->Pq.n < need) {
+		ctx->blk.release();
+		ctx->blk_tiles = 0;
+		ctx->raw.release();
+		ctx->Pq.release();
+		CK(ctx->raw.ensure(need + need / 10));
+		CK(ctx->Pq.ensure(need + need / 10));
+	}
 	// one orientation block: (P + 1) x 128 floats per tile (log-slices with
 	// their zero row; the tomograms use P rows of the same space)
 	const size_t tile_bytes = (P + 1) * TILE * sizeof(float);
@@ -1604,8 +1672,8 @@ static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CKL("psum_pairs_kernel");
 	phase_end(ctx, PH_PSUM, 1);
 
-	weight_pattern_kernel<<<1, 1024, 0, st>>>(ctx->psum_r.p, R, ctx->wpattern.p, ctx->wflags.p);
-	CKL("weight_pattern_kernel");
+	weight_sign_kernel<<<1, 1024, 0, st>>>(ctx->psum_r.p, R, ctx->wpattern.p, ctx->wsign.p, ctx->wflags.p);
+	CKL("weight_sign_kernel");
 	CK(cudaMemsetAsync(ctx->accum.p, 0, (size_t)M * V * sizeof(double2), st));
 	for (int t0 = 0; t0 < RT; t0 += BT) {
 		const int nt = std::min(BT, RT - t0), r0 = t0 * TILE, Rb = std::min(R - r0, nt * TILE);
@@ -1620,10 +1688,9 @@ static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
 		}
 		phase_end(ctx, PH_MSTEP, nq > 0 ? 1 : 0);
 		phase_begin(ctx, PH_MERGE);
-		merge_kernel<MT_3D><<<dim3(nblk, nt), 256, 0, st>>>(ctx->blk.p, ctx->psum_r.p + r0,
-		                                                     ctx->quats.p + 5 * (size_t)r0, 1, Rb, ctx->qvals.p,
-		                                                     ctx->corr.p, ctx->mask.p, P, S, V,
-		                                                     (double *)ctx->accum.p, ctx->wflags.p, 0);
+		merge_kernel<MT_3D, true><<<dim3(nblk, nt), 256, 0, st>>>(
+		    ctx->blk.p, ctx->psum_r.p + r0, ctx->quats.p + 5 * (size_t)r0, 1, Rb, ctx->qvals.p, ctx->corr.p,
+		    ctx->mask.p, P, S, V, (double *)ctx->accum.p, ctx->wflags.p, 0, ctx->wsign.p + r0);
 		CKL("merge_kernel");
 		phase_end(ctx, PH_MERGE, 1);
 	}
@@ -2856,5 +2923,7 @@ extern "C" int dfg_get_workload(dfg_ctx *ctx, long long *out) {
 	out[6] = ctx->launches;
 	out[7] = ctx->K_pad;
 	out[8] = (ctx->dense_active ? 1 : 0) | (ctx->m_dense_active ? 2 : 0);
+	out[9] = ctx->last_pairs ? ctx->npairs : 0;
+	out[10] = ctx->last_pairs ? ctx->blk_tiles : 0;
 	return DFG_OK;
 }

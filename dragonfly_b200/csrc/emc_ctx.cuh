@@ -218,6 +218,7 @@ struct dfg_ctx {
 	DevBuf<int> pair_tile, pair_frame, frame_pair;
 	DevBuf<double> raw;
 	DevBuf<float> Pq, blk;
+	DevBuf<signed char> wsign;  // per orientation: weight change of the merge
 	int blk_tiles = 0;
 	DevBuf<uint32_t> mw;  // per frame: pixel | count << IDX_BITS on mask < 2 pixels
 	DevBuf<long long> mw_off;

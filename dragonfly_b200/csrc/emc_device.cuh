@@ -867,7 +867,11 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 // that set is the one of a cached weight grid, with_weight is 0 and only the
 // model sums are accumulated. With views_final the tomograms already are the
 // views (background-aware update) and are not divided by psum_r.
-template <int GEO>
+// INCR (pair lists): zero tomogram values add nothing and are skipped, and
+// the weights are a change to the cached grid: wsign[r] = +1 / -1 adds /
+// subtracts orientation r's weights (its psum_r > 0 state changed, or +1 for
+// every orientation with psum_r > 0 when no grid is cached), 0 adds none.
+template <int GEO, bool INCR = false>
 __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ psum_r,
                                                      const double *__restrict__ quats, int M, int R,
@@ -876,10 +880,11 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
                                                      const uint8_t *__restrict__ mask, int P, long long S,
                                                      long long V, double *__restrict__ accum,
                                                      const int *__restrict__ weight_flag,
-                                                     int views_final) {
+                                                     int views_final, const signed char *__restrict__ wsign = nullptr) {
 	__shared__ double s_rot[TILE][9];
 	__shared__ int s_mode[TILE];
 	__shared__ double s_ps[TILE];
+	__shared__ signed char s_sg[INCR ? TILE : 1];
 	__shared__ float s_tile[PB][TILE + 1];
 	const int t = threadIdx.x, rt = blockIdx.y, p0 = blockIdx.x * PB;
 	const int with_weight = *weight_flag;
@@ -889,6 +894,8 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 		geo_setup<GEO>(quats, rr / M, s_rot[j]);
 		s_mode[j] = rr % M;
 		s_ps[j] = r < R ? psum_r[r] : 0.;
+		if constexpr (INCR)
+			s_sg[j] = r < R ? wsign[r] : 0;
 	}
 	{
 		const int w = t >> 5, lane = t & 31;
@@ -924,8 +931,16 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 	for (int k = 0; k < TILE / 4; ++k) {
 		const int j = g + 4 * k;
 		const double ps = s_ps[j];
-		if (!(ps > 0.))
+		bool model = ps > 0.;
+		int sg = 0;
+		if constexpr (INCR) {
+			sg = s_sg[j];
+			model = model && s_tile[i][j] != 0.f;
+			if (!model && sg == 0)
+				continue;
+		} else if (!model) {
 			continue;
+		}
 		double fw[8];
 		long long base;
 		if constexpr (GEO == MT_3D) {
@@ -941,8 +956,22 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 			corner_weights2(c, fw);
 			base = c.i00;
 		}
-		const double wv = views_final ? (double)s_tile[i][j] / cr : ((double)s_tile[i][j] / ps) / cr;
 		double *a = accum + 2 * ((size_t)s_mode[j] * V + base);
+		if constexpr (INCR) {
+			if (model) {
+				const double wv = ((double)s_tile[i][j] / ps) / cr;
+#pragma unroll
+				for (int q = 0; q < NC; ++q)
+					atomicAdd(a + 2 * o[q], fw[q] * wv);
+			}
+			if (sg != 0) {
+#pragma unroll
+				for (int q = 0; q < NC; ++q)
+					atomicAdd(a + 2 * o[q] + 1, sg > 0 ? fw[q] : -fw[q]);
+			}
+			continue;
+		}
+		const double wv = views_final ? (double)s_tile[i][j] / cr : ((double)s_tile[i][j] / ps) / cr;
 		if (with_weight) {
 #pragma unroll
 			for (int q = 0; q < NC; ++q) {
@@ -982,8 +1011,29 @@ __global__ void __launch_bounds__(1024) weight_pattern_kernel(const double *__re
 	}
 }
 
-// model2 / inter_weight from the accumulators; the weights either come from
-// this merge (and are kept in weight_cache) or from weight_cache.
+// Pair lists: the weight change of this merge. sign[r] = +1 for every
+// orientation with psum_r > 0 when no grid is cached (flags[0] = 1), else
+// the change of its psum_r > 0 state against the cached grid's (flags[0] =
+// 2: the merge's weight sums are added to the cached grid). One block.
+__global__ void __launch_bounds__(1024) weight_sign_kernel(const double *__restrict__ psum_r, int R,
+                                                           uint8_t *__restrict__ pattern,
+                                                           signed char *__restrict__ sign, int *__restrict__ flags) {
+	const bool full = flags[1] == 0;
+	for (int r = threadIdx.x; r < R; r += blockDim.x) {
+		const uint8_t p = psum_r[r] > 0. ? 1 : 0;
+		sign[r] = full ? (signed char)p : (signed char)((int)p - (int)pattern[r]);
+		pattern[r] = p;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		flags[0] = full ? 1 : 2;
+		flags[1] = 1;
+	}
+}
+
+// model2 / inter_weight from the accumulators; the weights come from this
+// merge (flag 1), from weight_cache (flag 0) or from weight_cache plus this
+// merge's change (flag 2); weight_cache keeps the result.
 __global__ void unpack_accum_kernel(const double2 *__restrict__ accum, long long n, double *__restrict__ model2,
                                     double *__restrict__ weight, double *__restrict__ weight_cache,
                                     const int *__restrict__ weight_flag) {
@@ -993,9 +1043,13 @@ __global__ void unpack_accum_kernel(const double2 *__restrict__ accum, long long
 	const int with_weight = *weight_flag;
 	double2 a = accum[i];
 	model2[i] = a.x;
-	if (with_weight) {
+	if (with_weight == 1) {
 		weight[i] = a.y;
 		weight_cache[i] = a.y;
+	} else if (with_weight == 2) {
+		const double w = weight_cache[i] + a.y;
+		weight[i] = w;
+		weight_cache[i] = w;
 	} else {
 		weight[i] = weight_cache[i];
 	}

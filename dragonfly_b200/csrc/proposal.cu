@@ -23,7 +23,10 @@
 #include <cmath>
 #include <random>
 
+#include <cudaTypedefs.h>
+
 #include "emc_ctx.cuh"
+#include "tcgen05.cuh"
 
 namespace {
 
@@ -346,6 +349,236 @@ __global__ void topk_kernel(const float *__restrict__ z, int B, int n, int K, in
 	}
 }
 
+// ---------------------------------------------------------------------------
+// inference products on the tensor cores
+// ---------------------------------------------------------------------------
+constexpr int GK = 64;  // K per stage: one 128-byte swizzle row of BF16
+constexpr int GSTAGES = 4;
+
+template <int BN>
+struct GemmCfg {
+	static constexpr int A_BYTES = 128 * GK * 2;
+	static constexpr int B_BYTES = BN * GK * 2;
+	static constexpr int STAGE = A_BYTES + B_BYTES;
+	static constexpr int SMEM = 1024 + GSTAGES * STAGE + 128;
+	// kind::f16: FP32 accumulator, BF16 A and B, both K-major, N = BN, M = 128
+	static constexpr uint32_t IDESC =
+	    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
+};
+
+// C[M][N] = act(A B^T + bias) for A [M][K] and B [N][K] in BF16 (K a multiple
+// of 64; both read by TMA with the 128-byte swizzle, rows past M or N read as
+// zero), accumulated in FP32 in TMEM. One CTA per 128 x BN tile: warp 0
+// issues the TMA loads (GSTAGES-deep ring), warp 1 the MMAs (and owns the
+// TMEM allocation), warps 2-5 read their 32 TMEM lanes, add the bias, apply
+// the ReLU and store FP32 rows. Every wait gives up after about a second,
+// sets *err and lets the CTA free its TMEM and exit.
+template <int BN>
+__global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a,
+                                                              const __grid_constant__ CUtensorMap map_b, int num_kb,
+                                                              int M, int N, const float *__restrict__ bias, int relu,
+                                                              float *__restrict__ C, int ldc, int *__restrict__ err) {
+	using G = GemmCfg<BN>;
+	extern __shared__ uint8_t gsm_raw[];
+	uint8_t *sm = (uint8_t *)(((uintptr_t)gsm_raw + 1023) & ~(uintptr_t)1023);
+	uint64_t *bars = (uint64_t *)(sm + GSTAGES * G::STAGE);
+	uint64_t *full = bars, *empty = bars + GSTAGES, *accum = bars + 2 * GSTAGES;
+	uint32_t *tmem_slot = (uint32_t *)(bars + 2 * GSTAGES + 1);
+	volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int mt = blockIdx.x, nt = blockIdx.y;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < GSTAGES; ++s) {
+			mbar_init(&full[s], 1);
+			mbar_init(&empty[s], 1);
+		}
+		mbar_init(accum, 1);
+		*abort_flag = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (warp == 1) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+		             "r"(BN)
+		             : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = *tmem_slot;
+	if (warp == 0) {
+		if (lane == 0) {
+			int issued = 0;
+			for (int kb = 0; kb < num_kb; ++kb) {
+				const int s = kb % GSTAGES;
+				const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
+				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u)) {
+					*abort_flag = 1;
+					atomicExch(err, 1);
+					break;
+				}
+				uint8_t *st = sm + s * G::STAGE;
+				mbar_expect_tx(&full[s], G::STAGE);
+				tma_load_2d(st, &map_a, &full[s], kb * GK, mt * 128);
+				tma_load_2d(st + G::A_BYTES, &map_b, &full[s], kb * GK, nt * BN);
+				issued = kb + 1;
+			}
+			// on a give-up, let the copies still in flight land before exiting
+			if (*abort_flag)
+				for (int kb = max(0, issued - GSTAGES); kb < issued; ++kb)
+					mbar_wait(&full[kb % GSTAGES], (uint32_t)(kb / GSTAGES) & 1u);
+		}
+		__syncwarp();
+	} else if (warp == 1) {
+		if (lane == 0) {
+			for (int kb = 0; kb < num_kb; ++kb) {
+				const int s = kb % GSTAGES;
+				const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
+				if (*abort_flag || !mbar_wait(&full[s], ph)) {
+					*abort_flag = 1;
+					atomicExch(err, 1);
+					break;
+				}
+				tc_fence_after();
+				const uint32_t a = smem_addr(sm + s * G::STAGE), b = a + G::A_BYTES;
+#pragma unroll
+				for (int k = 0; k < GK / 16; ++k)
+					umma_f16(tmem, sw128_desc(a + 32 * k), sw128_desc(b + 32 * k), G::IDESC, (kb | k) != 0);
+				umma_commit(&empty[s]);
+			}
+			umma_commit(accum);
+		}
+		__syncwarp();
+	} else {
+		// warp w reads TMEM lanes 32 (w % 4) .. + 31
+		const int q = warp & 3, row = mt * 128 + q * 32 + lane;
+		const bool ok = mbar_wait(accum, 0);
+		if (!ok) {
+			*abort_flag = 1;
+			atomicExch(err, 1);
+		}
+		tc_fence_after();
+		if (ok && !*abort_flag) {
+			for (int c = 0; c < BN / 16; ++c) {
+				float v[16];
+				tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 16), v);
+				if (row < M) {
+#pragma unroll
+					for (int j = 0; j < 16; ++j) {
+						const int col = nt * BN + c * 16 + j;
+						if (col < N) {
+							const float x = v[j] + bias[col];
+							C[(size_t)row * ldc + col] = relu ? fmaxf(x, 0.f) : x;
+						}
+					}
+				}
+			}
+		}
+	}
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 1) {
+		tc_fence_after();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+	}
+}
+
+// cols[(b, ho, wo)][k] in BF16, k = (ky, kx, c) < 9 C as im2col_kernel, zero
+// for 9 C <= k < Kp (the products' K padding). C and Kp are multiples of 8:
+// each thread writes 8 consecutive k (8 channels of one input pixel: two
+// 16-byte loads, one 16-byte store).
+__global__ void im2col_bf16_kernel(const float *__restrict__ X, int B, int H, int C, int s, int Ho, int Kp,
+                                   __nv_bfloat16 *__restrict__ cols) {
+	const int groups = Kp >> 3, K = 9 * C;
+	const long long n = (long long)B * Ho * Ho * groups;
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const unsigned r = (unsigned)(e / groups), k0 = (unsigned)(e - (long long)r * groups) * 8u;
+		float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+		if ((int)k0 < K) {
+			const unsigned tap = k0 / (unsigned)C, c0 = k0 - tap * (unsigned)C;
+			const unsigned ky = tap / 3u, kx = tap - ky * 3u;
+			const unsigned wo = r % (unsigned)Ho, t = r / (unsigned)Ho;
+			const unsigned ho = t % (unsigned)Ho, b = t / (unsigned)Ho;
+			const int y = (int)(ho * s + ky) - 1, x = (int)(wo * s + kx) - 1;
+			if (y >= 0 && y < H && x >= 0 && x < H) {
+				const float4 *src = reinterpret_cast<const float4 *>(X + (((size_t)b * H + y) * H + x) * C + c0);
+				const float4 p = src[0], q = src[1];
+				v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
+				v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+			}
+		}
+		__align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+			o[j] = __float2bfloat16_rn(v[j]);
+		*reinterpret_cast<uint4 *>(cols + (size_t)r * Kp + k0) = *reinterpret_cast<const uint4 *>(o);
+	}
+}
+
+// Layer 0 of the inference pass (conv 3x3, 1 -> 32 channels, stride 1 on the
+// 32 x 32 image) directly: one thread per output pixel, its 9 inputs times
+// the BF16 weights in tap order with fmaf from zero (the operation order of
+// the FP32 product path), + bias, ReLU; 32 channels stored as 8 16-byte
+// vectors.
+__global__ void __launch_bounds__(256) conv0_kernel(const float *__restrict__ X, int B,
+                                                    const __nv_bfloat16 *__restrict__ w,
+                                                    const float *__restrict__ bias, float *__restrict__ Y) {
+	__shared__ float ws[32 * 9], bs[32];
+	for (int i = threadIdx.x; i < 32 * 9; i += blockDim.x)
+		ws[i] = __bfloat162float(w[i]);
+	for (int i = threadIdx.x; i < 32; i += blockDim.x)
+		bs[i] = bias[i];
+	__syncthreads();
+	const long long n = (long long)B * IMG * IMG;
+	for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+		const int x = (int)(p & (IMG - 1)), y = (int)((p >> 5) & (IMG - 1));
+		const float *img = X + (p - (long long)y * IMG - x);
+		float in[9];
+#pragma unroll
+		for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+			for (int kx = 0; kx < 3; ++kx) {
+				const int yy = y + ky - 1, xx = x + kx - 1;
+				in[ky * 3 + kx] = (yy >= 0 && yy < IMG && xx >= 0 && xx < IMG) ? img[yy * IMG + xx] : 0.f;
+			}
+		float4 *out = reinterpret_cast<float4 *>(Y + p * 32);
+#pragma unroll
+		for (int o4 = 0; o4 < 8; ++o4) {
+			float r[4];
+#pragma unroll
+			for (int j = 0; j < 4; ++j) {
+				const int o = o4 * 4 + j;
+				float acc = 0.f;
+#pragma unroll
+				for (int k = 0; k < 9; ++k)
+					acc = fmaf(in[k], ws[o * 9 + k], acc);
+				r[j] = fmaxf(acc + bs[o], 0.f);
+			}
+			out[o4] = make_float4(r[0], r[1], r[2], r[3]);
+		}
+	}
+}
+
+// W [rows][K] BF16 -> [rows][Kp] with zero columns K .. Kp - 1.
+__global__ void pad_rows_bf16_kernel(const __nv_bfloat16 *__restrict__ W, long long rows, int K, int Kp,
+                                     __nv_bfloat16 *__restrict__ out) {
+	const long long n = rows * Kp;
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int k = (int)(e % Kp);
+		out[e] = k < K ? W[(e / Kp) * K + k] : __float2bfloat16_rn(0.f);
+	}
+}
+
+// X [rows][K] FP32 -> [rows][Kp] BF16 with zero columns K .. Kp - 1.
+__global__ void rows_bf16_kernel(const float *__restrict__ X, long long rows, int K, int Kp,
+                                 __nv_bfloat16 *__restrict__ out) {
+	const long long n = rows * Kp;
+	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int k = (int)(e % Kp);
+		out[e] = __float2bfloat16_rn(k < K ? X[(e / Kp) * K + k] : 0.f);
+	}
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -366,6 +599,7 @@ struct dfg_pnet {
 	cudaStream_t stream = nullptr;
 	std::string err;
 	int num_classes = 0, batch = 0;
+	int infer_batch = 0;  // images per forward pass outside training (>= batch)
 	LayerShape L[NL];
 	DevBuf<float> w[NL], b[NL], mw[NL], vw[NL], mb[NL], vb[NL], gw[NL], gb[NL];
 	DevBuf<__nv_bfloat16> wb[NL];
@@ -377,6 +611,10 @@ struct dfg_pnet {
 	long long n_images = 0;
 	DevBuf<int> pixel_bin;
 	int P = 0;
+	// tensor-core inference: BF16 operands with K padded to 64, error flag
+	bool use_tc = true;
+	DevBuf<__nv_bfloat16> colsb, wbp[NL];
+	DevBuf<int> terr;
 	long long step = 0;
 	int fail(int code, const char *fmt, ...) {
 		char buf[1024];
@@ -470,6 +708,112 @@ static int forward(dfg_pnet *net, const float *X, int n) {
 		bias_act_kernel<<<grid_for(rows * s.cout), 256, 0, st>>>(out, rows, s.cout, net->b[l].p, l < NL - 1);
 		PKL("bias_act_kernel");
 		in = out;
+	}
+	return DFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tensor-core forward pass (inference)
+// ---------------------------------------------------------------------------
+static int kpad64(int k) { return (k + GK - 1) / GK * GK; }
+
+static PFN_cuTensorMapEncodeTiled_v12000 pnet_map_encoder() {
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	if (fn == nullptr) {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+		        cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+	}
+	return fn;
+}
+
+// Tensor map of a row-major BF16 matrix [rows][K] (K a multiple of 64) read in
+// boxes of 64 columns x box_rows rows with the 128-byte swizzle.
+static int pnet_map(dfg_pnet *net, CUtensorMap *map, const void *base, long long rows, int K, int box_rows) {
+	auto fn = pnet_map_encoder();
+	if (fn == nullptr)
+		return net->fail(DFG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+	cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+	cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+	cuuint32_t box[2] = {(cuuint32_t)GK, (cuuint32_t)box_rows};
+	cuuint32_t estr[2] = {1, 1};
+	const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+	                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+	                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS)
+		return net->fail(DFG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+	return DFG_OK;
+}
+
+template <int BN>
+static int launch_tc_gemm(dfg_pnet *net, const CUtensorMap &ma, const CUtensorMap &mb, int num_kb, int M, int N,
+                          const float *bias, int relu, float *C) {
+	static bool attr = false;
+	if (!attr) {
+		PK(cudaFuncSetAttribute(pnet_gemm_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                        GemmCfg<BN>::SMEM));
+		attr = true;
+	}
+	dim3 grid((M + 127) / 128, (N + BN - 1) / BN);
+	pnet_gemm_tc_kernel<BN><<<grid, 192, GemmCfg<BN>::SMEM, net->stream>>>(ma, mb, num_kb, M, N, bias, relu, C, N,
+	                                                                     net->terr.p);
+	PKL("pnet_gemm_tc_kernel");
+	return DFG_OK;
+}
+
+// BF16 weight copies with K padded to 64 for the tensor-core products (after
+// any change of the weights).
+static int pad_weights(dfg_pnet *net) {
+	for (int l = 1; l < NL; ++l) {
+		const LayerShape &sh = net->L[l];
+		const int K = sh.fan_in(), Kp = kpad64(K);
+		pad_rows_bf16_kernel<<<grid_for((long long)sh.cout * Kp), 256, 0, net->stream>>>(net->wb[l].p, sh.cout, K,
+		                                                                                Kp, net->wbp[l].p);
+		PKL("pad_rows_bf16_kernel");
+	}
+	return DFG_OK;
+}
+
+// Forward pass of n <= infer_batch images with the products of layers 1-5 on
+// the tensor cores (BF16 activations and weights, FP32 accumulation); layer 0
+// (K = 9) stays in FP32 (conv0_kernel, the FP32 path's arithmetic). Logits
+// in act[NL].
+static int forward_tc(dfg_pnet *net, const float *X, int n) {
+	cudaStream_t st = net->stream;
+	conv0_kernel<<<grid_for((long long)n * IMG * IMG), 256, 0, st>>>(X, n, net->wb[0].p, net->b[0].p, net->act[1].p);
+	PKL("conv0_kernel");
+	for (int l = 1; l < NL; ++l) {
+		const LayerShape &s = net->L[l];
+		const long long rows = net->rows(l, n);
+		const int K = s.fan_in(), Kp = kpad64(K);
+		const float *in = net->act[l].p;
+		if (s.kind == 0) {
+			im2col_bf16_kernel<<<grid_for(rows * Kp / 8), 256, 0, st>>>(in, n, s.hin, s.cin, s.stride, s.hout, Kp,
+			                                                            net->colsb.p);
+			PKL("im2col_bf16_kernel");
+		} else {
+			rows_bf16_kernel<<<grid_for(rows * Kp), 256, 0, st>>>(in, rows, K, Kp, net->colsb.p);
+			PKL("rows_bf16_kernel");
+		}
+		CUtensorMap ma, mb;
+		if (int rc = pnet_map(net, &ma, net->colsb.p, rows, Kp, 128))
+			return rc;
+		const int BN = s.cout <= 32 ? 32 : (s.cout <= 64 ? 64 : 256);
+		if (int rc = pnet_map(net, &mb, net->wbp[l].p, s.cout, Kp, BN))
+			return rc;
+		const int relu = l < NL - 1;
+		int rc;
+		if (BN == 32)
+			rc = launch_tc_gemm<32>(net, ma, mb, Kp / GK, (int)rows, s.cout, net->b[l].p, relu, net->act[l + 1].p);
+		else if (BN == 64)
+			rc = launch_tc_gemm<64>(net, ma, mb, Kp / GK, (int)rows, s.cout, net->b[l].p, relu, net->act[l + 1].p);
+		else
+			rc = launch_tc_gemm<256>(net, ma, mb, Kp / GK, (int)rows, s.cout, net->b[l].p, relu, net->act[l + 1].p);
+		if (rc)
+			return rc;
 	}
 	return DFG_OK;
 }
@@ -593,17 +937,20 @@ extern "C" int dfg_pnet_create(int device, int num_classes, int batch, unsigned 
 		dfg_pnet_destroy(net);
 		return rc;
 	};
+	// forward buffers for the inference batch, backward ones for the
+	// training batch
+	net->infer_batch = std::max(batch, 2048);
 	for (int l = 0; l < NL; ++l) {
 		const LayerShape &s = net->L[l];
-		const long long nw = s.nw(), rows = net->rows(l, batch);
+		const long long nw = s.nw(), rows = net->rows(l, batch), irows = net->rows(l, net->infer_batch);
 		bool ok = net->w[l].ensure(nw) == cudaSuccess && net->mw[l].ensure(nw) == cudaSuccess &&
 		          net->vw[l].ensure(nw) == cudaSuccess && net->gw[l].ensure(nw) == cudaSuccess &&
 		          net->wb[l].ensure(nw) == cudaSuccess && net->b[l].ensure(s.cout) == cudaSuccess &&
 		          net->mb[l].ensure(s.cout) == cudaSuccess && net->vb[l].ensure(s.cout) == cudaSuccess &&
-		          net->gb[l].ensure(s.cout) == cudaSuccess && net->act[l + 1].ensure(rows * s.cout) == cudaSuccess &&
+		          net->gb[l].ensure(s.cout) == cudaSuccess && net->act[l + 1].ensure(irows * s.cout) == cudaSuccess &&
 		          net->dact[l + 1].ensure(rows * s.cout) == cudaSuccess;
 		if (ok && s.kind == 0)
-			ok = net->cols[l].ensure(rows * 9 * s.cin) == cudaSuccess &&
+			ok = net->cols[l].ensure(irows * 9 * s.cin) == cudaSuccess &&
 			     net->dcols[l].ensure(rows * 9 * s.cin) == cudaSuccess;
 		if (!ok)
 			return bad(DFG_ERR_NOMEM);
@@ -621,6 +968,17 @@ extern "C" int dfg_pnet_create(int device, int num_classes, int batch, unsigned 
 	}
 	if (ws > 0 && net->wsplit.ensure(ws) != cudaSuccess)
 		return bad(DFG_ERR_NOMEM);
+	// tensor-core inference: BF16 operand rows (the largest layer) and padded weights
+	long long cb = 0;
+	for (int l = 1; l < NL; ++l) {
+		const int Kp = (net->L[l].fan_in() + 63) / 64 * 64;
+		cb = std::max(cb, net->rows(l, net->infer_batch) * Kp);
+		if (net->wbp[l].ensure((size_t)net->L[l].cout * Kp) != cudaSuccess)
+			return bad(DFG_ERR_NOMEM);
+	}
+	if (net->colsb.ensure((size_t)cb) != cudaSuccess || net->terr.ensure(1) != cudaSuccess)
+		return bad(DFG_ERR_NOMEM);
+	cudaMemsetAsync(net->terr.p, 0, sizeof(int), net->stream);
 	if (net->loss_acc.ensure(1) != cudaSuccess)
 		return bad(DFG_ERR_NOMEM);
 	if (net->dact[0].ensure((long long)batch * IMG * IMG) != cudaSuccess ||
@@ -634,6 +992,13 @@ extern "C" int dfg_pnet_create(int device, int num_classes, int batch, unsigned 
 }
 
 extern "C" const char *dfg_pnet_last_error(const dfg_pnet *net) { return net ? net->err.c_str() : "null network"; }
+
+extern "C" int dfg_pnet_set_tensor_cores(dfg_pnet *net, int on) {
+	if (!net)
+		return DFG_ERR_ARG;
+	net->use_tc = on != 0;
+	return DFG_OK;
+}
 
 extern "C" long long dfg_pnet_num_params(const dfg_pnet *net) {
 	if (!net)
@@ -767,15 +1132,35 @@ extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, doub
 	return DFG_OK;
 }
 
-// Runs fn(b0, m) over the loaded images in batches after a forward pass.
+// Runs fn(b0, m) over the loaded images in inference batches after a
+// forward pass.
 template <typename F>
 static int for_batches(dfg_pnet *net, F fn) {
-	for (long long b0 = 0; b0 < net->n_images; b0 += net->batch) {
-		const int m = (int)std::min<long long>(net->batch, net->n_images - b0);
-		if (int rc = forward(net, net->images.p + (size_t)b0 * IMG * IMG, m))
+	if (net->use_tc)
+		if (int rc = pad_weights(net))
+			return rc;
+	for (long long b0 = 0; b0 < net->n_images; b0 += net->infer_batch) {
+		const int m = (int)std::min<long long>(net->infer_batch, net->n_images - b0);
+		const float *X = net->images.p + (size_t)b0 * IMG * IMG;
+		if (int rc = net->use_tc ? forward_tc(net, X, m) : forward(net, X, m))
 			return rc;
 		if (int rc = fn(b0, m))
 			return rc;
+	}
+	return DFG_OK;
+}
+
+// After tensor-core products: a pipeline wait that gave up makes the results
+// invalid (the flag is cleared for the next call).
+static int check_tc(dfg_pnet *net) {
+	if (!net->use_tc)
+		return DFG_OK;
+	int e = 0;
+	PK(cudaMemcpyAsync(&e, net->terr.p, sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+	PK(cudaStreamSynchronize(net->stream));
+	if (e) {
+		PK(cudaMemsetAsync(net->terr.p, 0, sizeof(int), net->stream));
+		return net->fail(DFG_ERR_CUDA, "tensor-core product: a pipeline wait gave up (results invalid)");
 	}
 	return DFG_OK;
 }
@@ -784,28 +1169,32 @@ extern "C" int dfg_pnet_topk(dfg_pnet *net, int K, int *out) {
 	if (!net || K < 1 || K > net->num_classes || !out)
 		return DFG_ERR_ARG;
 	PK(cudaSetDevice(net->device));
-	DevBuf<int> d;
-	PK(d.ensure((size_t)net->batch * K));
-	return for_batches(net, [&](long long b0, int m) -> int {
-		topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(net->act[NL].p, m, net->num_classes, K, d.p);
-		PKL("topk_kernel");
-		PK(cudaMemcpyAsync(out + (size_t)b0 * K, d.p, (size_t)m * K * sizeof(int), cudaMemcpyDeviceToHost,
-		                   net->stream));
-		PK(cudaStreamSynchronize(net->stream));
-		return DFG_OK;
-	});
+	DevBuf<int> d;  // every image's picks, read back once
+	PK(d.ensure((size_t)net->n_images * K));
+	if (int rc = for_batches(net, [&](long long b0, int m) -> int {
+		    topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(net->act[NL].p, m, net->num_classes, K,
+		                                                                 d.p + (size_t)b0 * K);
+		    PKL("topk_kernel");
+		    return DFG_OK;
+	    }))
+		return rc;
+	PK(cudaMemcpyAsync(out, d.p, (size_t)net->n_images * K * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+	PK(cudaStreamSynchronize(net->stream));
+	return check_tc(net);
 }
 
 extern "C" int dfg_pnet_logits(dfg_pnet *net, float *out) {
 	if (!net || !out)
 		return DFG_ERR_ARG;
 	PK(cudaSetDevice(net->device));
-	return for_batches(net, [&](long long b0, int m) -> int {
-		PK(cudaMemcpyAsync(out + (size_t)b0 * net->num_classes, net->act[NL].p,
-		                   (size_t)m * net->num_classes * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
-		PK(cudaStreamSynchronize(net->stream));
-		return DFG_OK;
-	});
+	if (int rc = for_batches(net, [&](long long b0, int m) -> int {
+		    PK(cudaMemcpyAsync(out + (size_t)b0 * net->num_classes, net->act[NL].p,
+		                       (size_t)m * net->num_classes * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+		    PK(cudaStreamSynchronize(net->stream));
+		    return DFG_OK;
+	    }))
+		return rc;
+	return check_tc(net);
 }
 
 // Mean loss and gradients (flat, as dfg_pnet_get_params) of the first

@@ -313,6 +313,11 @@ DFG_API int dfg_pnet_get_images(dfg_pnet *net, float *out);
  * [n] in [0, num_classes); *mean_loss = the last epoch's mean loss. */
 DFG_API int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, double lr, unsigned long long seed,
                            double *mean_loss);
+/* Inference products (dfg_pnet_topk, dfg_pnet_logits) of layers 1-5 on the
+ * tcgen05 tensor cores with BF16 activations (on = 1, the default) or on the
+ * FP32 path that training uses (on = 0). */
+DFG_API int dfg_pnet_set_tensor_cores(dfg_pnet *net, int on);
+
 /* out[n][K]: the K largest logits' classes of every loaded image, largest first. */
 DFG_API int dfg_pnet_topk(dfg_pnet *net, int K, int *out);
 DFG_API int dfg_pnet_logits(dfg_pnet *net, float *out);
@@ -374,8 +379,9 @@ DFG_API int dfg_reset_phase_times(dfg_ctx *ctx);
  * out[4] = frame chunks, out[5] = frames per chunk, out[6] = kernels launched
  * by this context so far, out[7] = mask < 2 pixel columns of the dense forms
  * (padded to 64; 0 before it is used), out[8] = forms of the last
- * iteration: 1 = dense E-step, 2 = dense M-step (bits). out must hold 9
- * values. */
+ * iteration: 1 = dense E-step, 2 = dense M-step (bits), out[9] = live
+ * (tile, frame) pairs of the pair lists (0 without them), out[10] =
+ * orientation tiles per block of the pair lists. out must hold 11 values. */
 DFG_API int dfg_get_workload(dfg_ctx *ctx, long long *out);
 
 #ifdef __cplusplus

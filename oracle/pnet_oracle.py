@@ -60,6 +60,23 @@ def col2im(dcols, B, H, C, s, ho):
     return dxp[:, 1:H + 1, 1:H + 1]
 
 
+def logits(params, images, num_classes, round_activations=False):
+    """Forward pass of the images [B][1024] to logits [B][classes] with BF16
+    weights; with round_activations the inputs of layers 1-5 are rounded to
+    BF16 too (the tensor-core inference path: BF16 operands, FP32 sums)."""
+    L = layers(num_classes)
+    P = unflatten(params, num_classes)
+    B = images.shape[0]
+    a = np.asarray(images, np.float64).reshape(B, IMG, IMG, 1)
+    for l, ((kind, cin, cout, hin, s, ho), (w, b)) in enumerate(zip(L, P)):
+        x = bf16(a) if (round_activations and l > 0) else a
+        cols = im2col(x, s, ho) if kind == 0 else x.reshape(B, -1)
+        y = cols @ bf16(w).T + b
+        y = y.reshape(B, ho, ho, cout) if kind == 0 else y
+        a = np.maximum(y, 0.) if l < len(L) - 1 else y
+    return a
+
+
 def loss_and_grads(params, images, labels, num_classes, round_weights=True):
     """Mean softmax cross-entropy of the images [B][1024] and its gradient
     with respect to the flat parameters."""

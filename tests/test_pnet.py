@@ -63,3 +63,39 @@ def test_gpu_gradients_match_oracle():
             o += n
             assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b) + 1e-9, (kind, cin, cout, n)
     net.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nc", [40, 420])
+def test_gpu_tensor_core_inference_matches_oracle(nc):
+    """Inference on the tcgen05 tensor cores (layers 1-5: BF16 activations and
+    weights, FP32 accumulation in TMEM) against the oracle's forward pass with
+    the same roundings, and against the FP32 path training uses; 3000 images
+    (two inference batches, the second partial; 420 classes: two N tiles of
+    256, the second partial)."""
+    from dragonfly_b200._lib import ProposalNet
+    from oracle.pnet_oracle import logits
+    rng = np.random.default_rng(4)
+    net = ProposalNet(nc, batch=64, seed=5)
+    p = net.params().astype(np.float64)
+    x = np.log1p(rng.poisson(0.8, (3000, 1024)).astype(np.float64)).astype(np.float32)
+    net.set_images(x)
+    z_tc = net.logits().astype(np.float64)
+    net.set_tensor_cores(False)
+    z_fp = net.logits().astype(np.float64)
+    sel = rng.choice(3000, 64, replace=False)
+    ref_tc = logits(p, x[sel].astype(np.float64), nc, round_activations=True)
+    ref_fp = logits(p, x[sel].astype(np.float64), nc, round_activations=False)
+    e_tc = np.linalg.norm(z_tc[sel] - ref_tc) / np.linalg.norm(ref_tc)
+    e_fp = np.linalg.norm(z_fp[sel] - ref_fp) / np.linalg.norm(ref_fp)
+    e_mix = np.linalg.norm(z_tc - z_fp) / np.linalg.norm(z_fp)
+    print("logits: tensor cores vs oracle %.2e, FP32 path vs oracle %.2e, tensor cores vs FP32 path %.2e"
+          % (e_tc, e_fp, e_mix))
+    # activations computed in FP32 on the GPU and in FP64 by the oracle round
+    # to different BF16 neighbours now and then (one BF16 step is 2^-8), so the
+    # rounded paths agree to a few 1e-4, several times closer than the two
+    # forms of the product are to each other
+    assert e_fp <= 1e-4, e_fp
+    assert e_tc <= 2e-3 and e_tc * 3 < e_mix, (e_tc, e_mix)
+    assert e_mix <= 3e-2, e_mix
+    net.close()
