@@ -571,11 +571,13 @@ def run_proposals(args):
     N = w["n_frames"]
     # the full search at two orientation subsets
     full = {}
-    for stride in P_["full_fracs"]:
-        full[stride] = _full_search_ms(w, inp, stride, 1, 1)
-    (Ra, ta), (Rb, tb) = full[P_["full_fracs"][0]], full[P_["full_fracs"][1]]
-    slope = (tb - ta) / (Rb - Ra)
-    full_ms = tb + slope * (R - Rb)
+    full_ms = None
+    if not args.no_full_search:
+        for stride in P_["full_fracs"]:
+            full[stride] = _full_search_ms(w, inp, stride, 1, 1)
+        (Ra, ta), (Rb, tb) = full[P_["full_fracs"][0]], full[P_["full_fracs"][1]]
+        slope = (tb - ta) / (Rb - Ra)
+        full_ms = tb + slope * (R - Rb)
     torch.cuda.synchronize()
     # the proposal form at the full orientation set
     c = Context(0)
@@ -590,6 +592,8 @@ def run_proposals(args):
     lp = LearnedProposals(c, inp["qvals"], fine, coarse_div=P_["coarse_div"], K=P_["K"], held_out=P_["held_out"],
                           threshold=P_["threshold"], seed=5, pair_lists=True)
     t1 = time.perf_counter()
+    if args.train_rounds:
+        P_["rounds"] = args.train_rounds
     loss = lp.train_simulated(inp["intens"], n_frames=P_["train_frames"], epochs=P_["epochs"], lr=P_["lr"],
                               lr_end=P_["lr_end"], rounds=P_["rounds"],
                               phi=np.exp(np.random.default_rng(9).normal(0., w["fluence_sigma"],
@@ -639,7 +643,7 @@ def run_proposals(args):
            "full_search": {"ms_extrapolated": full_ms,
                            "measured": {str(Rx): tx for Rx, tx in full.values()},
                            "rule": "t(R) linear in R through the two measured subsets"},
-           "speedup_vs_full_search": full_ms / ms,
+           "speedup_vs_full_search": full_ms / ms if full_ms else None,
            "effective_pairs_per_s": R * N / (ms / 1e3)}
     print(json.dumps(out))
     lp.close()
@@ -659,6 +663,10 @@ def main():
     ap.add_argument("--fluence-sigma", type=float, default=-1., help="override the lognormal fluence sigma")
     ap.add_argument("--estep-form", default="auto", choices=["auto", "sparse", "dense"],
                     help="E-step photon term: autotuned (default), sparse gathers or tensor-core products")
+    ap.add_argument("--train-rounds", type=int, default=0,
+                    help="proposals: rounds of network training (default 10; fewer for profiling runs)")
+    ap.add_argument("--no-full-search", action="store_true",
+                    help="proposals: skip timing the full search (profiling runs)")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "proposals"],
                     help="plain: the production-size iteration (default); batched: nine reconstructions "
                          "iterated together against one after another; proposals: the learned-proposal "

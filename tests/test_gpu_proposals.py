@@ -32,9 +32,11 @@ def test_learned_proposals_against_full_search(pair_lists):
         c.set_quaternions(fine)
         c.set_model(d["model_true"][None])
         c.calc_beta(1., 0)
+    # a 64 x 64 detector and 420 classes: the whole detector as the image and
+    # a larger rate than the production detector's 3240 classes want
     lp = LearnedProposals(restr, d["qvals"], fine, coarse_div=2, K=24, held_out=0.02, threshold=0.99, seed=1,
-                          pair_lists=pair_lists)
-    loss = lp.train_simulated(d["model_true"], n_frames=30000, epochs=4)
+                          pair_lists=pair_lists, zoom=1.0)
+    loss = lp.train_simulated(d["model_true"], n_frames=30000, epochs=4, lr=2e-3)
     # the network's gain: top-K hit rate of the true orientations' cells
     cells = full.voronoi_subset(quat_gen(2), np.pad(d["frame_quats"][:, :4], ((0, 0), (0, 1))))
     top = lp.propose()
