@@ -88,6 +88,7 @@ _SIGS = {
     "dfg_pnet_train": (C.c_int, [_V, _I, C.c_int, C.c_double, C.c_ulonglong, _D]),
     "dfg_pnet_topk": (C.c_int, [_V, C.c_int, _I]),
     "dfg_pnet_set_tensor_cores": (C.c_int, [_V, C.c_int]),
+    "dfg_pnet_set_targets": (C.c_int, [_V, C.POINTER(C.c_longlong), _I, C.POINTER(C.c_float)]),
     "dfg_pnet_logits": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "dfg_pnet_gradients": (C.c_int, [_V, _I, C.POINTER(C.c_float), _D]),
     "dfg_set_detector_distance": (C.c_int, [_V, C.c_double]),
@@ -647,8 +648,19 @@ class ProposalNet:
         self._call("dfg_pnet_get_images", ptr(out, C.c_float))
         return out
 
-    def train(self, labels, epochs=1, lr=1e-3, seed=0):
-        lab = np.ascontiguousarray(labels, np.int32)
+    def set_targets(self, offsets, classes, weights):
+        """Soft targets of the loaded images (CSR: image i's classes
+        classes[offsets[i]:offsets[i + 1]] with weights summing to 1); train()
+        and gradients() without labels use them."""
+        off = np.ascontiguousarray(offsets, np.int64)
+        cls = np.ascontiguousarray(classes, np.int32)
+        w = np.ascontiguousarray(weights, np.float32)
+        self._call("dfg_pnet_set_targets", ptr(off, C.c_longlong), ptr(cls, C.c_int), ptr(w, C.c_float))
+
+    def train(self, labels=None, epochs=1, lr=1e-3, seed=0):
+        """Epochs of Adam against labels, or (labels None) against the soft
+        targets of set_targets. Returns the last epoch's mean loss."""
+        lab = None if labels is None else np.ascontiguousarray(labels, np.int32)
         loss = C.c_double(0.)
         self._call("dfg_pnet_train", ptr(lab, C.c_int), int(epochs), float(lr), int(seed), C.byref(loss))
         return loss.value
@@ -668,8 +680,8 @@ class ProposalNet:
         self._call("dfg_pnet_logits", ptr(out, C.c_float))
         return out
 
-    def gradients(self, labels):
-        lab = np.ascontiguousarray(labels, np.int32)
+    def gradients(self, labels=None):
+        lab = None if labels is None else np.ascontiguousarray(labels, np.int32)
         g = np.zeros(self.num_params, np.float32)
         loss = C.c_double(0.)
         self._call("dfg_pnet_gradients", ptr(lab, C.c_int), ptr(g, C.c_float), C.byref(loss))

@@ -264,6 +264,44 @@ __global__ void softmax_xent_kernel(const float *__restrict__ z, const int *__re
 		loss[b] = logf(s) + m - r[y];
 }
 
+// Softmax cross-entropy against a target distribution per row (one warp per
+// row): row b is image img[b], whose targets are classes t_cls[t_off[img] ..
+// t_off[img + 1]) with weights t_w (distinct classes, weights summing to 1):
+// loss[b] = logsumexp(z) - sum_t w_t z[c_t]; dz = (softmax(z) - q) / B.
+__global__ void softmax_xent_soft_kernel(const float *__restrict__ z, const int *__restrict__ img,
+                                         const long long *__restrict__ t_off, const int *__restrict__ t_cls,
+                                         const float *__restrict__ t_w, int B, int n, float *__restrict__ dz,
+                                         float *__restrict__ loss) {
+	const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (b >= B)
+		return;
+	const float *r = z + (size_t)b * n;
+	float m = -INFINITY;
+	for (int j = lane; j < n; j += 32)
+		m = fmaxf(m, r[j]);
+	for (int o = 16; o > 0; o >>= 1)
+		m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+	float s = 0.f;
+	for (int j = lane; j < n; j += 32)
+		s += expf(r[j] - m);
+	for (int o = 16; o > 0; o >>= 1)
+		s += __shfl_xor_sync(FULL, s, o);
+	for (int j = lane; j < n; j += 32)
+		dz[(size_t)b * n + j] = expf(r[j] - m) / s / (float)B;
+	__syncwarp();
+	const long long t0 = t_off[img[b]], t1 = t_off[img[b] + 1];
+	float zt = 0.f;
+	for (long long t = t0 + lane; t < t1; t += 32) {
+		const int c = t_cls[t];
+		dz[(size_t)b * n + c] -= t_w[t] / (float)B;
+		zt += t_w[t] * r[c];
+	}
+	for (int o = 16; o > 0; o >>= 1)
+		zt += __shfl_xor_sync(FULL, zt, o);
+	if (lane == 0)
+		loss[b] = logf(s) + m - zt;
+}
+
 // Adam on FP32 master weights; the BF16 copy is refreshed.
 __global__ void adam_kernel(float *__restrict__ w, float *__restrict__ m, float *__restrict__ v,
                             const float *__restrict__ g, __nv_bfloat16 *__restrict__ wb, long long n, float lr,
@@ -590,7 +628,7 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int *__r
 	const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	if (e < (long long)n * row)
 		dst[e] = src[(size_t)idx[e / row] * row + e % row];
-	if (e < n)
+	if (lab != nullptr && e < n)
 		lab_out[e] = lab[idx[e]];
 }
 
@@ -615,6 +653,11 @@ struct dfg_pnet {
 	bool use_tc = true;
 	DevBuf<__nv_bfloat16> colsb, wbp[NL];
 	DevBuf<int> terr;
+	// soft targets of the loaded images (dfg_pnet_set_targets)
+	DevBuf<long long> t_off;
+	DevBuf<int> t_cls, iota;
+	DevBuf<float> t_w;
+	long long n_targets_images = -1;
 	long long step = 0;
 	int fail(int code, const char *fmt, ...) {
 		char buf[1024];
@@ -818,12 +861,21 @@ static int forward_tc(dfg_pnet *net, const float *X, int n) {
 	return DFG_OK;
 }
 
-// Loss and gradients of n images at X with labels (device); per-image losses in loss.
-static int backward(dfg_pnet *net, const float *X, const int *lab, int n) {
+// Loss and gradients of n images at X with labels (device), or with the soft
+// targets of the loaded images img (device, lab == nullptr); per-image losses
+// in loss.
+static int backward(dfg_pnet *net, const float *X, const int *lab, int n, const int *img = nullptr) {
 	cudaStream_t st = net->stream;
-	softmax_xent_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(net->act[NL].p, lab, n, net->num_classes,
-	                                                          net->dact[NL].p, net->loss.p);
-	PKL("softmax_xent_kernel");
+	if (lab != nullptr) {
+		softmax_xent_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(net->act[NL].p, lab, n, net->num_classes,
+		                                                          net->dact[NL].p, net->loss.p);
+		PKL("softmax_xent_kernel");
+	} else {
+		softmax_xent_soft_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(
+		    net->act[NL].p, img, net->t_off.p, net->t_cls.p, net->t_w.p, n, net->num_classes, net->dact[NL].p,
+		    net->loss.p);
+		PKL("softmax_xent_soft_kernel");
+	}
 	for (int l = NL - 1; l >= 0; --l) {
 		const LayerShape &s = net->L[l];
 		const long long rows = net->rows(l, n);
@@ -1062,6 +1114,7 @@ extern "C" int dfg_pnet_load_frames(dfg_pnet *net, dfg_ctx *ctx) {
 	PKL("frame_image_kernel");
 	PK(cudaStreamSynchronize(net->stream));
 	net->n_images = ctx->N;
+	net->n_targets_images = -1;
 	return DFG_OK;
 }
 
@@ -1072,6 +1125,7 @@ extern "C" int dfg_pnet_set_images(dfg_pnet *net, long long n, const float *imag
 	PK(upload(net->images, images, (size_t)n * IMG * IMG, net->stream));
 	PK(cudaStreamSynchronize(net->stream));
 	net->n_images = n;
+	net->n_targets_images = -1;
 	return DFG_OK;
 }
 
@@ -1083,13 +1137,51 @@ extern "C" int dfg_pnet_get_images(dfg_pnet *net, float *out) {
 	return DFG_OK;
 }
 
+// Soft targets of the loaded images: image i's classes t_cls[t_off[i] ..
+// t_off[i + 1]) with weights t_w (distinct classes, weights >= 0 summing to
+// 1); used by dfg_pnet_train / dfg_pnet_gradients called without labels.
+extern "C" int dfg_pnet_set_targets(dfg_pnet *net, const long long *t_off, const int *t_cls, const float *t_w) {
+	if (!net || !t_off)
+		return DFG_ERR_ARG;
+	const long long n = net->n_images;
+	if (n < 1)
+		return net->fail(DFG_ERR_STATE, "no images loaded");
+	if (t_off[0] != 0 || (t_off[n] > 0 && (!t_cls || !t_w)))
+		return net->fail(DFG_ERR_ARG, "targets: t_off[0] must be 0 and classes / weights given");
+	std::vector<long long> stamp((size_t)net->num_classes, -1);
+	for (long long i = 0; i < n; ++i) {
+		if (t_off[i + 1] < t_off[i])
+			return net->fail(DFG_ERR_ARG, "targets: t_off decreases at image %lld", i);
+		for (long long t = t_off[i]; t < t_off[i + 1]; ++t) {
+			const int c = t_cls[t];
+			if (c < 0 || c >= net->num_classes || stamp[c] == i || !(t_w[t] >= 0.f) || !std::isfinite(t_w[t]))
+				return net->fail(DFG_ERR_ARG, "targets: image %lld: class %d repeated, out of range or bad weight", i,
+				                 c);
+			stamp[c] = i;
+		}
+	}
+	PK(cudaSetDevice(net->device));
+	PK(upload(net->t_off, t_off, (size_t)n + 1, net->stream));
+	PK(upload(net->t_cls, t_cls ? t_cls : nullptr, (size_t)std::max<long long>(t_off[n], 0), net->stream));
+	PK(upload(net->t_w, t_w ? t_w : nullptr, (size_t)std::max<long long>(t_off[n], 0), net->stream));
+	std::vector<int> io((size_t)net->batch);
+	for (int k = 0; k < net->batch; ++k)
+		io[k] = k;
+	PK(upload(net->iota, io.data(), io.size(), net->stream));
+	PK(cudaStreamSynchronize(net->stream));
+	net->n_targets_images = n;
+	return DFG_OK;
+}
+
 extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, double lr, unsigned long long seed,
                               double *mean_loss) {
-	if (!net || !labels || epochs < 1 || !(lr > 0.))
+	if (!net || epochs < 1 || !(lr > 0.))
 		return DFG_ERR_ARG;
 	if (net->n_images < 1)
 		return net->fail(DFG_ERR_STATE, "no images loaded");
-	for (long long i = 0; i < net->n_images; ++i)
+	if (labels == nullptr && net->n_targets_images != net->n_images)
+		return net->fail(DFG_ERR_STATE, "no labels and no soft targets for the loaded images");
+	for (long long i = 0; labels && i < net->n_images; ++i)
 		if (labels[i] < 0 || labels[i] >= net->num_classes)
 			return net->fail(DFG_ERR_ARG, "label %d of image %lld outside [0, %d)", labels[i], i, net->num_classes);
 	PK(cudaSetDevice(net->device));
@@ -1100,7 +1192,8 @@ extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, doub
 	std::vector<int> perm((size_t)n);
 	for (long long i = 0; i < n; ++i)
 		perm[(size_t)i] = (int)i;
-	PK(upload(net->lab_all, labels, (size_t)n, st));
+	if (labels)
+		PK(upload(net->lab_all, labels, (size_t)n, st));
 	PK(net->perm.ensure((size_t)n));
 	std::mt19937_64 rng(seed);
 	double last = 0.;
@@ -1111,11 +1204,12 @@ extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, doub
 		for (long long b0 = 0; b0 < n; b0 += net->batch) {
 			const int m = (int)std::min<long long>(net->batch, n - b0);
 			gather_rows_kernel<<<grid_for((long long)m * IMG * IMG), 256, 0, st>>>(
-			    net->images.p, net->perm.p + b0, m, IMG * IMG, net->xbatch.p, net->lab_all.p, net->labels.p);
+			    net->images.p, net->perm.p + b0, m, IMG * IMG, net->xbatch.p, labels ? net->lab_all.p : nullptr,
+			    net->labels.p);
 			PKL("gather_rows_kernel");
 			if (int rc = forward(net, net->xbatch.p, m))
 				return rc;
-			if (int rc = backward(net, net->xbatch.p, net->labels.p, m))
+			if (int rc = backward(net, net->xbatch.p, labels ? net->labels.p : nullptr, m, net->perm.p + b0))
 				return rc;
 			if (int rc = adam_step(net, (float)lr))
 				return rc;
@@ -1200,16 +1294,19 @@ extern "C" int dfg_pnet_logits(dfg_pnet *net, float *out) {
 // Mean loss and gradients (flat, as dfg_pnet_get_params) of the first
 // min(n_images, batch) loaded images with the given labels; no update.
 extern "C" int dfg_pnet_gradients(dfg_pnet *net, const int *labels, float *grads, double *mean_loss) {
-	if (!net || !labels || !grads)
+	if (!net || !grads)
 		return DFG_ERR_ARG;
 	if (net->n_images < 1)
 		return net->fail(DFG_ERR_STATE, "no images loaded");
+	if (labels == nullptr && net->n_targets_images != net->n_images)
+		return net->fail(DFG_ERR_STATE, "no labels and no soft targets for the loaded images");
 	PK(cudaSetDevice(net->device));
 	const int m = (int)std::min<long long>(net->batch, net->n_images);
-	PK(cudaMemcpyAsync(net->labels.p, labels, m * sizeof(int), cudaMemcpyHostToDevice, net->stream));
+	if (labels)
+		PK(cudaMemcpyAsync(net->labels.p, labels, m * sizeof(int), cudaMemcpyHostToDevice, net->stream));
 	if (int rc = forward(net, net->images.p, m))
 		return rc;
-	if (int rc = backward(net, net->images.p, net->labels.p, m))
+	if (int rc = backward(net, net->images.p, labels ? net->labels.p : nullptr, m, net->iota.p))
 		return rc;
 	size_t o = 0;
 	for (int l = 0; l < NL; ++l) {

@@ -55,7 +55,7 @@ class LearnedProposals:
     """
 
     def __init__(self, ctx, qvals, fine, coarse_div=4, K=16, held_out=0.01, threshold=0.99, batch=256, seed=0,
-                 pair_lists=False, zoom=0.3):
+                 pair_lists=False, zoom=0.3, retrain_epochs=3, retrain_lr=1e-3):
         from ._lib import Context, ProposalNet
         self.ctx = ctx
         ctx.set_option("pair_lists", 1 if pair_lists else 0)
@@ -72,6 +72,8 @@ class LearnedProposals:
         self.sim.set_detector(qvals, ctx._corr, ctx._mask)
         self.rng = np.random.default_rng(seed)
         self.full_next = False
+        self.retrain_epochs = int(retrain_epochs)
+        self.retrain_lr = float(retrain_lr)
         self.history = []
 
     def train_simulated(self, model, n_frames=20000, epochs=3, lr=5e-4, phi=None, rounds=1, lr_end=None):
@@ -111,6 +113,30 @@ class LearnedProposals:
         labels = np.where(ok, self.qmap[np.maximum(rmax, 0)], 0).astype(np.int32)
         return self.net.train(labels, epochs=epochs, lr=lr, seed=int(self.rng.integers(1 << 30)))
 
+    def train_full_search_probs(self, offsets, place, prob, epochs=3, lr=1e-3, min_share=1e-3):
+        """Trains on the context's own frames against a full search's
+        probabilities summed per coarse cell (the per-frame lists of pairs
+        with P > 1e-6: offsets [N + 1], orientation indices, P), keeping the
+        cells with at least min_share of their frame's mass, renormalised."""
+        N, nc = self.ctx.num_data, self.nc
+        off = np.asarray(offsets, np.int64)
+        if off[-1] == 0:
+            return None
+        frame = np.repeat(np.arange(N, dtype=np.int64), np.diff(off))
+        key = frame * nc + self.qmap[np.asarray(place)]
+        uk, inv = np.unique(key, return_inverse=True)
+        mass = np.bincount(inv, weights=np.asarray(prob, np.float64))
+        f, c = uk // nc, uk % nc
+        tot = np.bincount(f, weights=mass, minlength=N)
+        keep = mass >= min_share * tot[f]
+        f, c, mass = f[keep], c[keep], mass[keep]
+        tot = np.bincount(f, weights=mass, minlength=N)
+        t_off = np.zeros(N + 1, np.int64)
+        np.cumsum(np.bincount(f, minlength=N), out=t_off[1:])
+        self.net.load_frames(self.ctx)
+        self.net.set_targets(t_off, c.astype(np.int32), (mass / tot[f]).astype(np.float32))
+        return self.net.train(None, epochs=epochs, lr=lr, seed=int(self.rng.integers(1 << 30)))
+
     def propose(self):
         """Top-K coarse cells of every frame of the context."""
         self.net.load_frames(self.ctx)
@@ -123,10 +149,15 @@ class LearnedProposals:
         'evaluated_fraction'."""
         ctx = self.ctx
         if self.full_next:
+            # the full search keeps its probabilities, and the network learns
+            # their distribution over the coarse cells
             ctx.set_refinement(None)
+            ctx.set_option("keep_prob", 1)
             out = dict(ctx.run_iteration(par, alpha))
+            off, place, prob = ctx.sparse_prob()
+            ctx.set_option("keep_prob", 0)
             info = dict(mode="full", captured_mass=None, evaluated_fraction=1.)
-            self.train_full_search(ctx.frame_results()["rmax"])
+            self.train_full_search_probs(off, place, prob, epochs=self.retrain_epochs, lr=self.retrain_lr)
             self.full_next = False
             out.update(info)
             self.history.append(info)

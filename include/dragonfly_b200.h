@@ -313,6 +313,11 @@ DFG_API int dfg_pnet_get_images(dfg_pnet *net, float *out);
  * [n] in [0, num_classes); *mean_loss = the last epoch's mean loss. */
 DFG_API int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, double lr, unsigned long long seed,
                            double *mean_loss);
+/* Soft targets of the loaded images (until images are loaded again): image
+ * i's classes t_cls[t_off[i] .. t_off[i + 1]) with weights t_w (distinct
+ * classes, weights >= 0 summing to 1). dfg_pnet_train and dfg_pnet_gradients
+ * called with labels == NULL minimise the cross-entropy against them. */
+DFG_API int dfg_pnet_set_targets(dfg_pnet *net, const long long *t_off, const int *t_cls, const float *t_w);
 /* Inference products (dfg_pnet_topk, dfg_pnet_logits) of layers 1-5 on the
  * tcgen05 tensor cores with BF16 activations (on = 1, the default) or on the
  * FP32 path that training uses (on = 0). */

@@ -77,9 +77,10 @@ def logits(params, images, num_classes, round_activations=False):
     return a
 
 
-def loss_and_grads(params, images, labels, num_classes, round_weights=True):
+def loss_and_grads(params, images, labels, num_classes, round_weights=True, targets=None):
     """Mean softmax cross-entropy of the images [B][1024] and its gradient
-    with respect to the flat parameters."""
+    with respect to the flat parameters; against the labels, or (targets
+    [B][classes], rows summing to 1) against soft targets."""
     L = layers(num_classes)
     P = unflatten(params, num_classes)
     B = images.shape[0]
@@ -99,10 +100,11 @@ def loss_and_grads(params, images, labels, num_classes, round_weights=True):
     m = z.max(1, keepdims=True)
     e = np.exp(z - m)
     sm = e / e.sum(1, keepdims=True)
-    loss = float(np.mean(np.log(e.sum(1)) + m[:, 0] - z[np.arange(B), labels]))
-    dy = sm.copy()
-    dy[np.arange(B), labels] -= 1.
-    dy /= B
+    if targets is None:
+        targets = np.zeros_like(z)
+        targets[np.arange(B), labels] = 1.
+    loss = float(np.mean(np.log(e.sum(1)) + m[:, 0] - (targets * z).sum(1)))
+    dy = (sm - targets) / B
     grads = [None] * len(L)
     for l in range(len(L) - 1, -1, -1):
         kind, cin, cout, hin, s, ho = L[l]

@@ -99,3 +99,38 @@ def test_gpu_tensor_core_inference_matches_oracle(nc):
     assert e_tc <= 2e-3 and e_tc * 3 < e_mix, (e_tc, e_mix)
     assert e_mix <= 3e-2, e_mix
     net.close()
+
+
+@pytest.mark.gpu
+def test_gpu_soft_target_gradients_match_oracle():
+    """Soft targets (a distribution over a few classes per image, as the
+    full search's probabilities aggregated per coarse cell give them): loss
+    and gradients against the oracle's soft cross-entropy."""
+    from dragonfly_b200._lib import ProposalNet
+    rng = np.random.default_rng(2)
+    nc = 40
+    net = ProposalNet(nc, batch=8, seed=4)
+    p = net.params().astype(np.float64)
+    x = np.log1p(rng.poisson(0.5, (8, 1024)).astype(np.float64))
+    net.set_images(x)
+    T = np.zeros((8, nc))
+    off, cls, w = [0], [], []
+    for i in range(8):
+        c = rng.choice(nc, rng.integers(1, 5), replace=False)
+        q = rng.random(c.size).astype(np.float32)
+        q /= q.sum()
+        T[i, c] = q
+        cls.extend(c.tolist())
+        w.extend(q.tolist())
+        off.append(len(cls))
+    net.set_targets(np.array(off), np.array(cls), np.array(w, np.float32))
+    g, loss = net.gradients()
+    loss_ref, g_ref = loss_and_grads(p, x.astype(np.float32).astype(np.float64), None, nc, targets=T)
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref), (loss, loss_ref)
+    assert np.linalg.norm(g - g_ref) <= 1e-4 * np.linalg.norm(g_ref), np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    # training against the targets lowers their cross-entropy
+    l1 = net.train(epochs=20, lr=1e-3)
+    assert l1 < loss, (l1, loss)
+    with pytest.raises(RuntimeError):
+        net.set_targets(np.array([0, 2] + [2] * 7), np.array([3, 3]), np.array([0.5, 0.5], np.float32))
+    net.close()
