@@ -199,25 +199,39 @@ def reference_step(w, inp, n_frames, seed, threads):
 
 def reference_throughput(w, inp, threads, budget_s=40., steps=2):
     """Reference pairs/s at the full frame count, extrapolated from frame
-    samples: t(n) = a + b n fitted on samples of n and 4 n frames."""
+    samples: t(n) = a + b n through a small sample (64 frames: mostly the
+    per-iteration slice work a) and a sample grown by 4x until its time is at
+    least three times the small one's (so that the frame-dependent part b n
+    dominates the difference) or the budget is spent; that sample is timed
+    steps - 1 times."""
     R = inp["quats"].shape[0]
     n1 = 64
     t1 = reference_step(w, inp, n1, 11, threads)
-    # grow the sample while a step stays well inside the budget
-    while t1 < budget_s / 10 and n1 < 4096:
-        n1 *= 2
-        t1 = reference_step(w, inp, n1, 11, threads)
-    n2 = 4 * n1
-    times = {n1: [t1]}
-    for k in range(max(1, steps - 1)):
-        times.setdefault(n2, []).append(reference_step(w, inp, n2, 12 + k, threads))
-    t2 = float(np.mean(times[n2]))
+    spent, n2, t2 = t1, n1, t1
+    while n2 < 16384:
+        nxt = 4 * n2
+        if n2 > n1:  # predicted time of the next sample from the line so far
+            pred = t1 + (t2 - t1) * (nxt - n1) / (n2 - n1)
+            if spent + pred > budget_s:
+                break
+        t2 = reference_step(w, inp, nxt, 12, threads)
+        n2 = nxt
+        spent += t2
+        if t2 >= 3. * t1:
+            break
+    reps = [t2]
+    for k in range(max(0, steps - 2)):
+        if spent + t2 > budget_s:
+            break
+        reps.append(reference_step(w, inp, n2, 13 + k, threads))
+        spent += reps[-1]
+    t2 = float(np.mean(reps))
     b = max((t2 - t1) / (n2 - n1), 1e-12)
     a = max(t1 - b * n1, 0.)
     N = w["n_frames"]
     t_full = a + b * N
     return dict(value=R * N / t_full, t_full=t_full, fixed_s=a, per_frame_s=b, samples={n1: t1, n2: t2},
-                raw_sample_pairs_s=R * n2 / t2, cores=threads)
+                raw_sample_pairs_s=R * n2 / t2, cores=threads, frame_share=(t2 - t1) / t2)
 
 
 # ---------------------------------------------------------------------------
@@ -720,7 +734,7 @@ def main():
         threads = reference_threads(w)
         for _ in range(args.warmup):
             pass  # every reference step builds its own engine; nothing to warm
-        res = reference_throughput(w, inp, threads, steps=max(2, args.steps))
+        res = reference_throughput(w, inp, threads, budget_s=150., steps=max(2, args.steps))
         sample = ("reference engine (dragonfly/src, -O3 -march=native, OpenMP %d threads) on %s frames at "
                   "all %d orientations; t(n) = a + b n fitted, extrapolated to %d frames"
                   % (threads, "/".join(str(k) for k in res["samples"]), inp["quats"].shape[0], w["n_frames"]))
@@ -731,7 +745,8 @@ def main():
                "config": {"workload": w["name"], "num_orientations": int(inp["quats"].shape[0]),
                           "num_frames": w["n_frames"], "parallelism": "host cores"},
                "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": threads, "kind": "reference",
-                                "sample": sample, "fixed_s": res["fixed_s"], "per_frame_s": res["per_frame_s"]},
+                                "sample": sample, "fixed_s": res["fixed_s"], "per_frame_s": res["per_frame_s"],
+                                "frame_share": res["frame_share"]},
                "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
         return
@@ -746,13 +761,13 @@ def main():
         from oracle.oracle import reference_available
         if reference_available(fast=True):
             threads = reference_threads(w)
-            res = reference_throughput(w, inp, threads, budget_s=30., steps=2)
+            res = reference_throughput(w, inp, threads, budget_s=120., steps=2)
             out["cpu_baseline"] = {
                 "value": res["value"], "unit": UNIT, "cores": threads, "kind": "reference",
                 "sample": "reference engine (dragonfly/src) on %s frames at all orientations, OpenMP %d threads; "
                           "extrapolated to %d frames by t(n) = a + b n" % (
                               "/".join(str(k) for k in res["samples"]), threads, w["n_frames"]),
-                "raw_sample_pairs_s": res["raw_sample_pairs_s"]}
+                "raw_sample_pairs_s": res["raw_sample_pairs_s"], "frame_share": res["frame_share"]}
         else:
             out["cpu_baseline"] = None
     if world > 1:
