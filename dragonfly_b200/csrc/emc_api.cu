@@ -1093,6 +1093,8 @@ static void dense_release(dfg_ctx *ctx) {
 static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par);
 static bool pair_mode(const dfg_ctx *ctx);
 static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par);
+static bool blocked_wanted(dfg_ctx *ctx);
+static int blocked_prepare(dfg_ctx *ctx, const dfg_iter_params *par);
 
 // The coarse cell of every orientation on the device ([R_pad], -1 past R).
 static int prepare_qmap(dfg_ctx *ctx) {
@@ -1125,6 +1127,12 @@ static int prepare_weight_cache(dfg_ctx *ctx) {
 // frames by their global index.
 static int pair_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 	ctx->dense_active = ctx->m_dense_active = false;
+	ctx->blocked = false;
+	if (ctx->blkT.p != nullptr) {  // block buffers sized for the blocked full search
+		ctx->blkT.release();
+		ctx->blk.release();
+		ctx->blk_tiles = 0;
+	}
 	if (int rc = ensure_pair_buffers(ctx, par))
 		return rc;
 	if (!ctx->h_watch.empty()) {
@@ -1146,6 +1154,9 @@ static int max_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CK(cudaSetDevice(ctx->device));
 	if (pair_mode(ctx))
 		return pair_prepare(ctx, par);
+	if (blocked_wanted(ctx))
+		return blocked_prepare(ctx, par);
+	ctx->blocked = false;
 	// E-step form: dense tensor-core products (option estep_form 1, or the
 	// autotuner's choice) where the inputs allow it
 	if (ctx->autotune && !ctx->tuned && !ctx->tuning)
@@ -1592,6 +1603,36 @@ static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par) {
 	return DFG_OK;
 }
 
+// Log-slices of the tiles [t0, t0 + nt) into the block buffer (one mode, 3-D)
+// and their u_r; the zero row (pixel P) of every tile is cleared first (a
+// tomogram may have been written over it).
+static int launch_slices_block(dfg_ctx *ctx, int ob, int t0, int nt) {
+	cudaStream_t st = ctx->stream;
+	const int P = ctx->P, r0 = t0 * TILE, Rb = std::min(ctx->R - r0, nt * TILE);
+	const long long S = ctx->S, V = ctx->V;
+	CK(cudaMemset2DAsync(ctx->blk.p + (size_t)P * TILE, (size_t)(P + 1) * TILE * sizeof(float), 0,
+	                     TILE * sizeof(float), nt, st));
+	const int nb = nt * TILE / ob;
+	const double *q = ctx->quats.p + 5 * (size_t)r0;
+	if (ob == TILE)
+		slice_u_tile_kernel<double, MT_3D><<<nt, 256, 0, st>>>(q, 1, Rb, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
+		                                                       ctx->model1.p, S, V, ctx->blk.p, ctx->u.p + r0, nullptr);
+	else if (ob == 64)
+		slice_u_kernel<double, TILE >= 64 ? 64 : 16, MT_3D><<<nb, 256, 0, st>>>(
+		    q, 1, Rb, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P, ctx->model1.p, S, V, ctx->blk.p, ctx->u.p + r0,
+		    nullptr);
+	else if (ob == 32)
+		slice_u_kernel<double, 32, MT_3D><<<nb, 256, 0, st>>>(q, 1, Rb, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
+		                                                      ctx->model1.p, S, V, ctx->blk.p, ctx->u.p + r0,
+		                                                      nullptr);
+	else
+		slice_u_kernel<double, 16, MT_3D><<<nb, 256, 0, st>>>(q, 1, Rb, ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
+		                                                      ctx->model1.p, S, V, ctx->blk.p, ctx->u.p + r0,
+		                                                      nullptr);
+	CKL("slice_u_kernel");
+	return DFG_OK;
+}
+
 // maximize over pair lists: per orientation block its slices and the E-step
 // of its pairs; u_r and the rescale factor once every block is sliced; the
 // normalisation, watched frames and psum_r over all pairs; per block the
@@ -1611,26 +1652,10 @@ static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
 		CKL("beta_kernel");
 	}
 	for (int t0 = 0; t0 < RT; t0 += BT) {
-		const int nt = std::min(BT, RT - t0), r0 = t0 * TILE, Rb = std::min(R - r0, nt * TILE);
+		const int nt = std::min(BT, RT - t0);
 		phase_begin(ctx, PH_SLICE);
-		// zero row (pixel P) of every tile: the M-step of the last block wrote over it
-		CK(cudaMemset2DAsync(ctx->blk.p + (size_t)P * TILE, (size_t)(P + 1) * TILE * sizeof(float), 0,
-		                     TILE * sizeof(float), nt, st));
-		const int nb = nt * TILE / ob;
-#define DFG_SLICE_B(OBV)                                                                                      	slice_u_kernel<double, OBV, MT_3D><<<nb, 256, 0, st>>>(ctx->quats.p + 5 * (size_t)r0, 1, Rb, ctx->qvals.p,    	                                                       ctx->corr.p, ctx->mask.p, P, ctx->model1.p, S, V,    	                                                       ctx->blk.p, ctx->u.p + r0, nullptr)
-		if (ob == TILE)
-			slice_u_tile_kernel<double, MT_3D><<<nt, 256, 0, st>>>(ctx->quats.p + 5 * (size_t)r0, 1, Rb,
-			                                                       ctx->qvals.p, ctx->corr.p, ctx->mask.p, P,
-			                                                       ctx->model1.p, S, V, ctx->blk.p,
-			                                                       ctx->u.p + r0, nullptr);
-		else if (ob == 64)
-			DFG_SLICE_B(TILE >= 64 ? 64 : 16);
-		else if (ob == 32)
-			DFG_SLICE_B(32);
-		else
-			DFG_SLICE_B(16);
-#undef DFG_SLICE_B
-		CKL("slice_u_kernel");
+		if (int rc = launch_slices_block(ctx, ob, t0, nt))
+			return rc;
 		phase_end(ctx, PH_SLICE, 1);
 		phase_begin(ctx, PH_ESTEP);
 		const long long q0 = ctx->h_tile_off[t0], nq = ctx->h_tile_off[t0 + nt] - q0;
@@ -1711,12 +1736,245 @@ static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
 	return DFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// orientation-blocked full search (log-slices and tomograms too large to keep
+// for every orientation)
+// ---------------------------------------------------------------------------
+// Whether a full search runs in orientation blocks: option block_budget_mb
+// (without refinement), or the log-slices and tomograms of every orientation
+// would take more than half of the device memory.
+static bool blocked_wanted(dfg_ctx *ctx) {
+	if (ctx->refine || ctx->P <= 0 || ctx->num_rot <= 0 || ctx->M <= 0)
+		return false;
+	if (ctx->block_budget_mb > 0.)
+		return true;
+	const size_t RT = ((size_t)ctx->M * ctx->num_rot + TILE - 1) / TILE;
+	const size_t need = RT * ((size_t)2 * ctx->P + 1) * TILE * sizeof(float);
+	size_t fr = 0, tot = 0;
+	if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+		cudaGetLastError();
+		return false;
+	}
+	const size_t held = (ctx->logW.n + ctx->T.n + ctx->blk.n + ctx->blkT.n) * sizeof(float);
+	return need > (fr + held) / 2;
+}
+
+// Buffers of the blocked full search: one block of log-slices (blk) and one
+// of tomograms (blkT), then the frame chunks from the memory left.
+static int blocked_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
+	NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0 && ctx->S > 0, DFG_ERR_STATE,
+	     "set detector, frames, quaternions and model first");
+	NEED(ctx->beta_set, DFG_ERR_STATE, "beta not set (dfg_calc_beta or dfg_set_beta_start)");
+	NEED(ctx->M == 1 && ctx->model_type == MT_3D, DFG_ERR_ARG,
+	     "orientation blocks (the full search's log-slices and tomograms exceed the memory, or block_budget_mb): "
+	     "one mode, 3-D models only");
+	NEED(!(ctx->with_bg && par->need_scaling), DFG_ERR_ARG, "orientation blocks: no background-aware updates");
+	ctx->dense_active = ctx->m_dense_active = false;
+	ctx->blocked = true;
+	ctx->R = ctx->num_rot;
+	ctx->RT = (ctx->R + TILE - 1) / TILE;
+	ctx->R_pad = ctx->RT * TILE;
+	ctx->logW.release();
+	ctx->T.release();
+	dense_release(ctx);
+	const size_t N = (size_t)ctx->N, P = (size_t)ctx->P;
+	CK(ctx->u.ensure((size_t)ctx->R_pad));
+	CK(ctx->logw.ensure((size_t)ctx->R_pad));
+	CK(ctx->psum_r.ensure((size_t)ctx->R_pad));
+	CK(ctx->scalars.ensure(8));
+	CK(ctx->red_part.ensure(std::max<size_t>(blocks_for((long long)ctx->M * ctx->V, 256), 1024)));
+	CK(ctx->rmax.ensure(N));
+	CK(ctx->num_prob.ensure(N));
+	CK(ctx->info.ensure(N));
+	CK(ctx->likelihood.ensure(N));
+	CK(ctx->max_exp.ensure(N));
+	CK(ctx->p_norm.ensure(N));
+	CK(ctx->psum_d.ensure(N));
+	CK(ctx->quat_norm.ensure(N * ctx->M));
+	const size_t tile_bytes = ((size_t)2 * P + 1) * TILE * sizeof(float);
+	if (ctx->blk_tiles <= 0 || ctx->blkT.n < (size_t)ctx->blk_tiles * P * TILE ||
+	    ctx->blk.n < (size_t)ctx->blk_tiles * (P + 1) * TILE) {
+		ctx->blk.release();
+		ctx->blkT.release();
+		size_t budget;
+		if (ctx->block_budget_mb > 0.) {
+			budget = (size_t)(ctx->block_budget_mb * 1048576.);
+		} else {
+			size_t fr = 0, tot = 0;
+			CK(cudaMemGetInfo(&fr, &tot));
+			budget = (size_t)(0.35 * (double)fr);
+		}
+		ctx->blk_tiles = (int)std::max<size_t>(1, std::min<size_t>((size_t)ctx->RT, budget / tile_bytes));
+		CK(ctx->blk.ensure((size_t)ctx->blk_tiles * (P + 1) * TILE));
+		CK(ctx->blkT.ensure((size_t)ctx->blk_tiles * P * TILE));
+	}
+	if (ctx->chunks_R != ctx->R || ctx->chunks_dense != 0) {
+		ctx->pval.release();
+		ctx->Pst.release();
+		ctx->tmax.release();
+		ctx->targ.release();
+		if (int rc = build_chunks(ctx))
+			return rc;
+	}
+	const size_t pairs = (size_t)ctx->R_pad * ctx->chunk_frames;
+	CK(ctx->pval.ensure(pairs));
+	CK(ctx->Pst.ensure((size_t)ctx->R_pad * (ctx->chunk_frames + 1)));
+	CK(ctx->tmax.ensure((size_t)ctx->RT * ctx->chunk_frames));
+	CK(ctx->targ.ensure((size_t)ctx->RT * ctx->chunk_frames));
+	CK(ctx->tlive.ensure((size_t)ctx->RT * (ctx->chunk_frames + 1)));
+	const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
+	CK(ctx->psum_part.ensure((size_t)nsplit * ctx->R_pad));
+	return prepare_weight_cache(ctx);
+}
+
+// E-step of the tiles [t0, t0 + nt) for one chunk from the block buffer.
+static int launch_estep_block(dfg_ctx *ctx, const Chunk &ch, int t0, int nt, int use_scale) {
+	const RefineMask none{nullptr, nullptr, 0};
+	estep_kernel<false><<<blocks_for((long long)nt * ch.nc, 8), 256, 0, ctx->stream>>>(
+	    ctx->blk.p, ctx->u.p, ctx->logw.p, ctx->R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,
+	    ctx->blacklist.p, ch.d0, ch.nc, use_scale, ctx->scalars.p, ctx->P, nt, ctx->pval.p, ctx->tmax.p, ctx->targ.p,
+	    none, t0);
+	CKL("estep_kernel");
+	return DFG_OK;
+}
+
+// maximize with the orientations in blocks of whole tiles, in two passes.
+// Pass 1, per frame chunk: every block's slices and E-step into the chunk's
+// log-likelihoods, then the normalisation over all orientations (exact: the
+// per-frame maximum, first argmax, kept sum and frame sums as the one-chunk
+// path) and psum_r. Pass 2, per block: its slices once, then per chunk its
+// E-step again, its probabilities from the pass-1 per-frame results
+// (prob_block_kernel) and its tomograms; the block is merged once all chunks
+// are in. u_r (and the rescale factor the E-step needs) come from a slice
+// pass over every block first.
+static int max_enqueue_blocked(dfg_ctx *ctx, const dfg_iter_params *par) {
+	cudaStream_t st = ctx->stream;
+	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
+	const long long S = ctx->S, V = ctx->V;
+	const int nblk = (P + PB - 1) / PB, BT = ctx->blk_tiles;
+	const int ob = slice_block_for(ctx);
+	{
+		double factor = std::pow(par->beta_jump, (double)((par->iteration - 1) / par->beta_period));
+		factor *= par->beta_factor;
+		beta_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->beta_start.p, ctx->blacklist.p, N, factor,
+		                                                 ctx->beta.p);
+		CKL("beta_kernel");
+	}
+	phase_begin(ctx, PH_SLICE);
+	for (int t0 = 0; t0 < RT; t0 += BT)
+		if (int rc = launch_slices_block(ctx, ob, t0, std::min(BT, RT - t0)))
+			return rc;
+	rescale_kernel<<<1, 256, 0, st>>>(ctx->u.p, ctx->quats.p, M, R, ctx->mean_count, ctx->scalars.p);
+	CKL("rescale_kernel");
+	logw_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->quats.p, M, R, ctx->logw.p);
+	CKL("logw_kernel");
+	phase_end(ctx, PH_SLICE, (RT + BT - 1) / BT + 2);
+	CK(cudaMemsetAsync(ctx->psum_r.p, 0, (size_t)R_pad * sizeof(double), st));
+	CK(cudaMemsetAsync(ctx->accum.p, 0, (size_t)M * V * sizeof(double2), st));
+	const int use_scale = par->need_scaling && (par->iteration > 1 || par->known_scale);
+	const int psum_d_on = par->need_scaling && par->update_scale;
+	if (ctx->keep_prob) {
+		ctx->h_prob_off.assign((size_t)N + 1, 0);
+		ctx->h_place_prob.clear();
+		ctx->h_prob.clear();
+	}
+	ctx->have_prob = false;
+	// pass 1
+	for (Chunk &ch : ctx->chunks) {
+		const int Nc = ch.nc;
+		for (int t0 = 0; t0 < RT; t0 += BT) {
+			const int nt = std::min(BT, RT - t0);
+			phase_begin(ctx, PH_SLICE);
+			if (int rc = launch_slices_block(ctx, ob, t0, nt))
+				return rc;
+			phase_end(ctx, PH_SLICE, 1);
+			phase_begin(ctx, PH_ESTEP);
+			if (int rc = launch_estep_block(ctx, ch, t0, nt, use_scale))
+				return rc;
+			phase_end(ctx, PH_ESTEP, 1);
+		}
+		phase_begin(ctx, PH_NORM);
+		if (int rc = launch_norm(ctx, ch, psum_d_on, false))
+			return rc;
+		phase_end(ctx, PH_NORM, 1);
+		if (ctx->keep_prob)
+			if (int rc = collect_prob(ctx, ch))
+				return rc;
+		phase_begin(ctx, PH_PSUM);
+		const int nsplit = std::max(1, std::min(64, ctx->chunk_frames / 2048));
+		const int fps = (Nc + nsplit - 1) / nsplit;
+		psum_r_kernel<<<dim3(RT, nsplit), 256, 0, st>>>(ctx->Pst.p, Nc, ch.d0, fps, ctx->scale.p, par->need_scaling,
+		                                                ctx->psum_part.p, R_pad,
+		                                                tile_skipping(ctx) ? ctx->tlive.p : nullptr);
+		CKL("psum_r_kernel");
+		psum_r_reduce_kernel<<<blocks_for(R, 256), 256, 0, st>>>(ctx->psum_part.p, nsplit, R, R_pad, ctx->psum_r.p);
+		CKL("psum_r_reduce_kernel");
+		phase_end(ctx, PH_PSUM, 2);
+	}
+	weight_pattern_kernel<<<1, 1024, 0, st>>>(ctx->psum_r.p, R, ctx->wpattern.p, ctx->wflags.p);
+	CKL("weight_pattern_kernel");
+	// pass 2
+	for (int t0 = 0; t0 < RT; t0 += BT) {
+		const int nt = std::min(BT, RT - t0), r0 = t0 * TILE, Rb = std::min(R - r0, nt * TILE);
+		phase_begin(ctx, PH_SLICE);
+		if (int rc = launch_slices_block(ctx, ob, t0, nt))
+			return rc;
+		phase_end(ctx, PH_SLICE, 1);
+		CK(cudaMemsetAsync(ctx->blkT.p, 0, (size_t)nt * P * TILE * sizeof(float), st));
+		for (Chunk &ch : ctx->chunks) {
+			const int Nc = ch.nc;
+			phase_begin(ctx, PH_ESTEP);
+			if (int rc = launch_estep_block(ctx, ch, t0, nt, use_scale))
+				return rc;
+			phase_end(ctx, PH_ESTEP, 1);
+			phase_begin(ctx, PH_NORM);
+			prob_block_kernel<<<blocks_for((long long)nt * (Nc + 1), 8), 256, 0, st>>>(
+			    ctx->pval.p, t0, nt, Nc, ch.d0, R, ctx->beta.p, ctx->max_exp.p, ctx->rmax.p, ctx->p_norm.p,
+			    ctx->blacklist.p, ctx->Pst.p);
+			CKL("prob_block_kernel");
+			phase_end(ctx, PH_NORM, 1);
+			phase_begin(ctx, PH_MSTEP);
+			if (ch.npix > 0) {
+				mstep_kernel<false><<<blocks_for((long long)nt * ch.npix, 8), 256, 0, st>>>(
+				    ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, P, nt, ctx->blkT.p,
+				    ctx->tlive.p, t0);
+				CKL("mstep_kernel");
+			}
+			phase_end(ctx, PH_MSTEP, ch.npix > 0 ? 1 : 0);
+		}
+		phase_begin(ctx, PH_MERGE);
+		merge_kernel<MT_3D><<<dim3(nblk, nt), 256, 0, st>>>(ctx->blkT.p, ctx->psum_r.p + r0,
+		                                                     ctx->quats.p + 5 * (size_t)r0, 1, Rb, ctx->qvals.p,
+		                                                     ctx->corr.p, ctx->mask.p, P, S, V,
+		                                                     (double *)ctx->accum.p, ctx->wflags.p, 0);
+		CKL("merge_kernel");
+		phase_end(ctx, PH_MERGE, 1);
+	}
+	phase_begin(ctx, PH_UPDATE);
+	unpack_accum_kernel<<<blocks_for((long long)M * V, 256), 256, 0, st>>>(
+	    ctx->accum.p, (long long)M * V, ctx->model2.p, ctx->weight.p, ctx->weight_cache.p, ctx->wflags.p);
+	CKL("unpack_accum_kernel");
+	frame_totals_kernel<<<1, 1024, 0, st>>>(ctx->info.p, ctx->likelihood.p, ctx->blacklist.p, N,
+	                                        ctx->scalars.p + 1);
+	CKL("frame_totals_kernel");
+	if (par->need_scaling && par->update_scale) {
+		scale_kernel<<<blocks_for(N, 256), 256, 0, st>>>(ctx->fcounts.p, ctx->psum_d.p, ctx->blacklist.p, N,
+		                                                  ctx->scale.p);
+		CKL("scale_kernel");
+	}
+	phase_end(ctx, PH_UPDATE, par->need_scaling && par->update_scale ? 3 : 2);
+	ctx->views_final = false;
+	return DFG_OK;
+}
+
 // Queues maximize's kernels (after max_prepare). Synchronises only where
 // graphable() is false.
 static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 	ctx->last_pairs = pair_mode(ctx);
 	if (ctx->last_pairs)
 		return max_enqueue_pairs(ctx, par);
+	if (ctx->blocked)
+		return max_enqueue_blocked(ctx, par);
 	cudaStream_t st = ctx->stream;
 	const int N = ctx->N, P = ctx->P, M = ctx->M, R = ctx->R, RT = ctx->RT, R_pad = ctx->R_pad;
 	const long long S = ctx->S, V = ctx->V;
@@ -2621,7 +2879,8 @@ extern "C" int dfg_get_tomograms(dfg_ctx *ctx, int r0, int n, double *out) {
 	if (!ctx || !out)
 		return DFG_ERR_ARG;
 	NEED(ctx->have_results, DFG_ERR_STATE, "no results yet");
-	NEED(!ctx->last_pairs, DFG_ERR_STATE, "tomograms are not kept with pair lists (one orientation block at a time)");
+	NEED(!ctx->last_pairs && !ctx->blocked, DFG_ERR_STATE,
+	     "tomograms are not kept with pair lists or orientation blocks (one block at a time)");
 	NEED(r0 >= 0 && n >= 1 && (long long)r0 + n <= ctx->R, DFG_ERR_ARG,
 	     "orientations %d..%lld outside 0..%d", r0, (long long)r0 + n - 1, ctx->R - 1);
 	CK(cudaSetDevice(ctx->device));

@@ -282,12 +282,13 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
     const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off, const long long *__restrict__ ph_mid,
     const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
     const double *__restrict__ scalars, int P, int RT, double *__restrict__ pval, double *__restrict__ tmax,
-    int *__restrict__ targ, RefineMask rm) {
+    int *__restrict__ targ, RefineMask rm, int t0 = 0) {
+	// RT tiles from tile t0 (orientation blocks: logW holds tiles t0 ..)
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * Nc)
 		return;
-	const int rt = (int)(warp / Nc), dl = (int)(warp - (long long)rt * Nc), d = d0 + dl;
+	const int rl = (int)(warp / Nc), dl = (int)(warp - (long long)rl * Nc), d = d0 + dl, rt = t0 + rl;
 	if (blacklist[d])
 		return;
 	const int r0 = rt * TILE + lane * LW;
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 			return;
 		}
 	}
-	const float *L = logW + (size_t)rt * (P + 1) * TILE + lane * LW;
+	const float *L = logW + (size_t)rl * (P + 1) * TILE + lane * LW;
 	const long long beg = ph_off[d], mid = ph_mid[d], end = ph_off[d + 1];
 	// segments start at multiples of 8 words: two 16-byte loads, identical for
 	// every lane (broadcast), bring 8 photon words
@@ -705,12 +706,14 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
                                                      const long long *__restrict__ cs_off,
                                                      const long long *__restrict__ cs_mid,
                                                      const int *__restrict__ pix, int npix, int P, int RT,
-                                                     float *__restrict__ T, const uint8_t *__restrict__ tlive) {
+                                                     float *__restrict__ T, const uint8_t *__restrict__ tlive,
+                                                     int t0 = 0) {
+	// RT tiles from tile t0 (orientation blocks: T holds tiles t0 ..)
 	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= (long long)RT * npix)
 		return;
-	const int rt = (int)(warp / npix), kp = (int)(warp - (long long)rt * npix);
+	const int rl = (int)(warp / npix), kp = (int)(warp - (long long)rl * npix), rt = t0 + rl;
 	const int p = pix[kp];
 	const float *Pr = Pst + (size_t)rt * (Nc + 1) * TILE + lane * LW;
 	// SKIP: frames whose tile is dead (norm_kernel) read the chunk's zero row
@@ -840,7 +843,7 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 				kahan_add_count(s[q % ECH][k], c[q % ECH][k], e[q] >> IDX_BITS, fmaxf(v[q][k], 0.f));
 	}
 	}
-	float *out = T + ((size_t)rt * P + p) * TILE + lane * LW;
+	float *out = T + ((size_t)rl * P + p) * TILE + lane * LW;
 	float o[LW];
 	ld_row_rw(out, o);
 #pragma unroll

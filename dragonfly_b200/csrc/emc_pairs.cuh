@@ -337,6 +337,59 @@ __global__ void __launch_bounds__(256) mstep_pairs_kernel(const float *__restric
 	}
 }
 
+// Orientation-blocked full search, second pass: the probabilities of the
+// tiles [t0, t0 + nt) for one frame chunk from their log-likelihoods (pval,
+// the chunk's dense layout) and the per-frame results of the first pass
+// (max_exp = maximum, rmax = its first orientation, p_norm = kept sum): the
+// kept rule and P = exp(beta (x - max)) x (1 / p_norm) exactly as
+// norm_kernel forms them, sign = PROB_MIN gate. One warp per (tile, frame);
+// warp index Nc of a tile writes the chunk's zero row.
+__global__ void __launch_bounds__(256) prob_block_kernel(const double *__restrict__ pval, int t0, int nt, int Nc,
+                                                         int d0, int R, const double *__restrict__ beta,
+                                                         const double *__restrict__ max_exp,
+                                                         const int *__restrict__ rmax,
+                                                         const double *__restrict__ p_norm,
+                                                         const uint8_t *__restrict__ blacklist,
+                                                         float *__restrict__ Pst) {
+	const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (w >= (long long)nt * (Nc + 1))
+		return;
+	const int rl = (int)(w / (Nc + 1)), dl = (int)(w - (long long)rl * (Nc + 1)), rt = t0 + rl;
+	float out[LW];
+#pragma unroll
+	for (int e = 0; e < LW; ++e)
+		out[e] = 0.f;
+	float *dst = Pst + ((size_t)rt * (Nc + 1) + dl) * TILE + lane * LW;
+	if (dl == Nc) {
+		st_row(dst, out);
+		return;
+	}
+	const int d = d0 + dl;
+	const double m = max_exp[d], s = p_norm[d];
+	if (!blacklist[d] && m != MAX_EXP_START && s > 0.) {
+		double x[LW];
+		ld_row(pval + ((size_t)rt * Nc + dl) * TILE + lane * LW, x);
+		const double b = beta[d];
+		const double thr = PDIFF_THRESH / b;
+		const double lo = dsub(m, thr);
+		const int rstar = rmax[d];
+		const double inv_s = 1. / s;
+#pragma unroll
+		for (int e = 0; e < LW; ++e) {
+			const int r = rt * TILE + lane * LW + e;
+			if (r < R) {
+				const bool kept = (r <= rstar) ? (x[e] > lo) : (dadd(x[e], thr) > m);
+				if (kept) {
+					const double P = exp(dmul(b, dsub(x[e], m))) * inv_s;
+					out[e] = (P > PROB_MIN) ? (float)P : -(float)P;
+				}
+			}
+		}
+	}
+	st_row(dst, out);
+}
+
 // Captured probability mass of watched frames over pair lists (as
 // captured_mass_kernel): for watched frame wf[w] the sum of |P| over the
 // orientations whose cell is among its proposed cells, over the sum of all.
