@@ -631,6 +631,41 @@ def run_proposals(args):
     phases = {k: round(v[0] / args.steps, 1) for k, v in c.phase_times().items()}
     top = lp.propose()
     hit = float(np.mean(np.any(top == cells[:, None], axis=1)))
+    loop = None
+    if args.loop:
+        # the fallback: a full search over all orientations (in orientation
+        # blocks) keeping its probabilities, the network retrained on them;
+        # then a proposal iteration, compared with a full search from the same
+        # state
+        it = args.warmup + args.steps + 1
+        lp.full_next = True
+        c.reset_phase_times()
+        f = lp.iteration(par(it), 0.)
+        full_phases = {k: round(v[0], 1) for k, v in c.phase_times().items()}
+        wl_full = c.workload()
+        m0, _, _ = c.model()
+        s0 = c.frame_params()["scale"]
+        p_ = lp.proposal_iteration(par(it + 1), 0.)
+        mp, _, _ = c.model()
+        rp = c.frame_results()["rmax"].copy()
+        c.set_model(m0)
+        c.set_scale(s0)
+        c.set_refinement(None)
+        t0 = time.perf_counter()
+        c.run_iteration(par(it + 1), 0.)
+        t_same = time.perf_counter() - t0
+        mf, _, _ = c.model()
+        rf = c.frame_results()["rmax"]
+        loop = {"full_search_s": f["iterate_s"], "full_search_phases_ms": full_phases,
+                "full_search_chunks": wl_full["chunks"], "retrain_s": f["retrain_s"],
+                "retrain": "%d epochs on the %d frames against the full search's probabilities per cell" % (
+                    lp.retrain_epochs, N),
+                "proposal_after_retrain": {"captured_mass": p_["captured_mass"], "min_mass": p_["min_mass"],
+                                           "wall_s": p_["propose_s"] + p_["lists_s"] + p_["iterate_s"],
+                                           "fallback_next": lp.full_next},
+                "vs_full_search_same_state": {"model_rel_l2": float(np.linalg.norm(mp - mf) / np.linalg.norm(mf)),
+                                              "rmax_agreement": float(np.mean(rp == rf)),
+                                              "full_search_s": t_same}}
     wl = c.workload()
     timed = runs[args.warmup:]
     ms = float(np.mean([r["wall_ms"] for r in timed]))
@@ -658,6 +693,7 @@ def run_proposals(args):
                            "measured": {str(Rx): tx for Rx, tx in full.values()},
                            "rule": "t(R) linear in R through the two measured subsets"},
            "speedup_vs_full_search": full_ms / ms if full_ms else None,
+           "loop": loop,
            "effective_pairs_per_s": R * N / (ms / 1e3)}
     print(json.dumps(out))
     lp.close()
@@ -679,6 +715,9 @@ def main():
                     help="E-step photon term: autotuned (default), sparse gathers or tensor-core products")
     ap.add_argument("--train-rounds", type=int, default=0,
                     help="proposals: rounds of network training (default 10; fewer for profiling runs)")
+    ap.add_argument("--loop", action="store_true",
+                    help="proposals: also run the fallback full search (orientation blocks), retrain on its "
+                         "probabilities and compare the next proposal iteration with a full search")
     ap.add_argument("--no-full-search", action="store_true",
                     help="proposals: skip timing the full search (profiling runs)")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "proposals"],

@@ -1776,6 +1776,8 @@ static int blocked_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 	ctx->R_pad = ctx->RT * TILE;
 	ctx->logW.release();
 	ctx->T.release();
+	ctx->raw.release();  // per-pair buffers of the pair lists
+	ctx->Pq.release();
 	dense_release(ctx);
 	const size_t N = (size_t)ctx->N, P = (size_t)ctx->P;
 	CK(ctx->u.ensure((size_t)ctx->R_pad));

@@ -147,17 +147,21 @@ class LearnedProposals:
         watched), or a full search when the last judgement failed. Returns
         the iteration's results with 'mode', 'captured_mass' and
         'evaluated_fraction'."""
+        import time
         ctx = self.ctx
         if self.full_next:
             # the full search keeps its probabilities, and the network learns
             # their distribution over the coarse cells
             ctx.set_refinement(None)
             ctx.set_option("keep_prob", 1)
+            t0 = time.perf_counter()
             out = dict(ctx.run_iteration(par, alpha))
+            t1 = time.perf_counter()
             off, place, prob = ctx.sparse_prob()
             ctx.set_option("keep_prob", 0)
-            info = dict(mode="full", captured_mass=None, evaluated_fraction=1.)
             self.train_full_search_probs(off, place, prob, epochs=self.retrain_epochs, lr=self.retrain_lr)
+            info = dict(mode="full", captured_mass=None, evaluated_fraction=1., iterate_s=t1 - t0,
+                        retrain_s=time.perf_counter() - t1)
             self.full_next = False
             out.update(info)
             self.history.append(info)
