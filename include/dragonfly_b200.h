@@ -366,7 +366,17 @@ DFG_API int dfg_save_emc(dfg_ctx *ctx, const char *path);
 
 /* ---- tuning and instrumentation ------------------------------------------
  * Options: "pair_budget_mb" (device memory for the per-pair buffers, which
- * sets the frame chunk), "timing" (1: record per-phase CUDA-event times). */
+ * sets the frame chunk), "timing" (1: record per-phase CUDA-event times),
+ * "keep_prob" (1: keep the sparse probability lists), "graph" (1: capture
+ * iterations as CUDA graphs), "autotune" (1: time the kernel forms on the
+ * inputs and keep the fastest), "estep_form" / "mstep_form" (0 sparse, 1
+ * tensor-core products), "slice_block" (orientations per slice block, 0
+ * automatic), "tile_skip" (skip dead (tile, frame) pairs without
+ * refinement), "pair_lists" (1: restricted searches store only their live
+ * (tile, frame) pairs, orientations in blocks), "block_budget_mb" (device
+ * memory for one block of log-slices (and tomograms); without refinement a
+ * value > 0 runs the full search in orientation blocks, which it also does
+ * when the resident log-slices and tomograms would exceed half the memory). */
 DFG_API int dfg_set_option(dfg_ctx *ctx, const char *key, double value);
 /* Phase times in ms summed since the last reset, and launch counts:
  * names[i] = "slice", "estep", "norm", "psum", "mstep", "merge", "update".
