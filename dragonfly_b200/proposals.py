@@ -20,6 +20,48 @@ import numpy as np
 from .quatgen import quat_gen
 
 
+def cell_targets(offsets, place, prob, qmap, num_cells, min_share=1e-3):
+    """Soft targets per frame from a full search's sparse probabilities
+    (frame d's pairs [offsets[d], offsets[d + 1]) with orientation indices
+    place and probabilities prob): the probability summed per coarse cell
+    (qmap[orientation]), cells below min_share of their frame's total dropped,
+    the rest renormalised. Returns (t_off [N + 1], cells, weights), cells
+    ascending within a frame."""
+    off = np.asarray(offsets, np.int64)
+    N = off.size - 1
+    frame = np.repeat(np.arange(N, dtype=np.int64), np.diff(off))
+    key = frame * num_cells + np.asarray(qmap)[np.asarray(place, np.int64)]
+    uk, inv = np.unique(key, return_inverse=True)
+    mass = np.bincount(inv, weights=np.asarray(prob, np.float64))
+    f, c = uk // num_cells, uk % num_cells
+    tot = np.bincount(f, weights=mass, minlength=N)
+    keep = mass >= min_share * tot[f]
+    f, c, mass = f[keep], c[keep], mass[keep]
+    tot = np.bincount(f, weights=mass, minlength=N)
+    t_off = np.zeros(N + 1, np.int64)
+    np.cumsum(np.bincount(f, minlength=N), out=t_off[1:])
+    return t_off, c.astype(np.int32), (mass / tot[f]).astype(np.float32)
+
+
+def restriction_lists(top, watch, num_cells):
+    """Per-frame coarse-cell lists of a proposal iteration as (offsets, flat):
+    frame d's top-K cells (top [N, K]), every cell for the watched frames."""
+    top = np.asarray(top, np.int32)
+    N, K = top.shape
+    watch = np.asarray(watch, np.int64)
+    lens = np.full(N, K, np.int64)
+    lens[watch] = num_cells
+    off = np.zeros(N + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    flat = np.empty(int(off[-1]), np.int32)
+    keep = np.ones(N, bool)
+    keep[watch] = False
+    flat[(off[:-1][keep][:, None] + np.arange(K)).ravel()] = top[keep].ravel()
+    flat[(off[:-1][watch][:, None] + np.arange(num_cells)).ravel()] = np.tile(np.arange(num_cells, dtype=np.int32),
+                                                                            watch.size)
+    return off, flat
+
+
 def sort_by_coarse(fine, coarse_div, ctx):
     """Fine orientations [R, 5] ordered by their nearest coarse orientation
     (stable), so that a coarse cell's orientations are contiguous. Returns
@@ -118,23 +160,11 @@ class LearnedProposals:
         probabilities summed per coarse cell (the per-frame lists of pairs
         with P > 1e-6: offsets [N + 1], orientation indices, P), keeping the
         cells with at least min_share of their frame's mass, renormalised."""
-        N, nc = self.ctx.num_data, self.nc
-        off = np.asarray(offsets, np.int64)
-        if off[-1] == 0:
+        if np.asarray(offsets)[-1] == 0:
             return None
-        frame = np.repeat(np.arange(N, dtype=np.int64), np.diff(off))
-        key = frame * nc + self.qmap[np.asarray(place)]
-        uk, inv = np.unique(key, return_inverse=True)
-        mass = np.bincount(inv, weights=np.asarray(prob, np.float64))
-        f, c = uk // nc, uk % nc
-        tot = np.bincount(f, weights=mass, minlength=N)
-        keep = mass >= min_share * tot[f]
-        f, c, mass = f[keep], c[keep], mass[keep]
-        tot = np.bincount(f, weights=mass, minlength=N)
-        t_off = np.zeros(N + 1, np.int64)
-        np.cumsum(np.bincount(f, minlength=N), out=t_off[1:])
+        t_off, cells, w = cell_targets(offsets, place, prob, self.qmap, self.nc, min_share)
         self.net.load_frames(self.ctx)
-        self.net.set_targets(t_off, c.astype(np.int32), (mass / tot[f]).astype(np.float32))
+        self.net.set_targets(t_off, cells, w)
         return self.net.train(None, epochs=epochs, lr=lr, seed=int(self.rng.integers(1 << 30)))
 
     def propose(self):
@@ -184,17 +214,7 @@ class LearnedProposals:
         t1 = time.perf_counter()
         n_watch = max(1, int(round(self.held_out * N)))
         watch = np.sort(self.rng.choice(N, n_watch, replace=False)).astype(np.int32)
-        lens = np.full(N, self.K, np.int64)
-        lens[watch] = self.nc
-        off = np.zeros(N + 1, np.int64)
-        np.cumsum(lens, out=off[1:])
-        flat = np.empty(int(off[-1]), np.int32)
-        keep = np.ones(N, bool)
-        keep[watch] = False
-        flat[(off[:-1][keep][:, None] + np.arange(self.K)).ravel()] = top[keep].ravel()
-        flat[(off[:-1][watch][:, None] + np.arange(self.nc)).ravel()] = np.tile(np.arange(self.nc, dtype=np.int32),
-                                                                                n_watch)
-        ctx.set_refinement(self.nc, self.qmap, (off, flat))
+        ctx.set_refinement(self.nc, self.qmap, restriction_lists(top, watch, self.nc))
         ctx.set_watch(watch, top[watch])
         t2 = time.perf_counter()
         out = dict(ctx.run_iteration(par, alpha))
