@@ -604,7 +604,8 @@ def run_proposals(args):
     c.calc_beta(1., 1)
     setup_s = time.perf_counter() - t0
     lp = LearnedProposals(c, inp["qvals"], fine, coarse_div=P_["coarse_div"], K=P_["K"], held_out=P_["held_out"],
-                          threshold=P_["threshold"], seed=5, pair_lists=True)
+                          threshold=P_["threshold"], seed=5, pair_lists=True, retrain_epochs=args.retrain_epochs,
+                          retrain_lr=args.retrain_lr)
     t1 = time.perf_counter()
     if args.train_rounds:
         P_["rounds"] = args.train_rounds
@@ -658,8 +659,8 @@ def run_proposals(args):
         rf = c.frame_results()["rmax"]
         loop = {"full_search_s": f["iterate_s"], "full_search_phases_ms": full_phases,
                 "full_search_chunks": wl_full["chunks"], "retrain_s": f["retrain_s"],
-                "retrain": "%d epochs on the %d frames against the full search's probabilities per cell" % (
-                    lp.retrain_epochs, N),
+                "retrain": "%d epochs (lr %g) on the %d frames against the full search's probabilities per cell" % (
+                    lp.retrain_epochs, lp.retrain_lr, N),
                 "proposal_after_retrain": {"captured_mass": p_["captured_mass"], "min_mass": p_["min_mass"],
                                            "wall_s": p_["propose_s"] + p_["lists_s"] + p_["iterate_s"],
                                            "fallback_next": lp.full_next},
@@ -715,6 +716,9 @@ def main():
                     help="E-step photon term: autotuned (default), sparse gathers or tensor-core products")
     ap.add_argument("--train-rounds", type=int, default=0,
                     help="proposals: rounds of network training (default 10; fewer for profiling runs)")
+    ap.add_argument("--retrain-epochs", type=int, default=3,
+                    help="proposals --loop: epochs of retraining on the fallback full search's probabilities")
+    ap.add_argument("--retrain-lr", type=float, default=1e-3, help="proposals --loop: retraining rate")
     ap.add_argument("--loop", action="store_true",
                     help="proposals: also run the fallback full search (orientation blocks), retrain on its "
                          "probabilities and compare the next proposal iteration with a full search")
