@@ -33,6 +33,35 @@ def test_oracle_gradients_match_finite_differences():
         assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
 
 
+def test_oracle_soft_target_gradients_match_finite_differences():
+    """The oracle's soft cross-entropy (the checker of the soft-target
+    training) against finite differences; one-hot targets give the
+    hard-label loss."""
+    rng = np.random.default_rng(1)
+    nc = 12
+    p = _params(rng, nc)
+    x = np.log1p(rng.poisson(0.7, (3, 1024)).astype(np.float64))
+    T = rng.random((3, nc)) * (rng.random((3, nc)) < 0.3)
+    T[:, 0] += 0.1
+    T /= T.sum(1, keepdims=True)
+    loss, g = loss_and_grads(p, x, None, nc, round_weights=False, targets=T)
+    idx = rng.choice(p.size, 40, replace=False)
+    h = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += h
+        lp, _ = loss_and_grads(q, x, None, nc, round_weights=False, targets=T)
+        q[i] -= 2 * h
+        lm, _ = loss_and_grads(q, x, None, nc, round_weights=False, targets=T)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+    y = np.array([1, 5, 11])
+    onehot = np.eye(nc)[y]
+    l1, g1 = loss_and_grads(p, x, y, nc)
+    l2, g2 = loss_and_grads(p, x, None, nc, targets=onehot)
+    assert abs(l1 - l2) <= 1e-12 * abs(l1) and np.allclose(g1, g2, rtol=1e-12, atol=1e-15)
+
+
 def test_bf16_rounding():
     x = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 1e-30], np.float32)
     r = bf16(x)
