@@ -9,7 +9,7 @@ K (``Context.set_refinement`` with the coarse map of ``voronoi_subset``; with
 the fine orientations sorted by coarse cell, the skipped orientations form
 whole tiles that every phase of the iteration skips). Each iteration a
 held-out share of the frames is searched in full and watched: the probability
-mass its proposals would have captured (``Context.watch_mass``) judges the
+mass its proposals would have captured (``Context.watch_mass``) measures the
 network, and when it falls below ``threshold`` the next iteration is a full
 search and the network is trained again, on frames simulated from the
 current model at known orientations and on the last full search's most likely
@@ -174,7 +174,7 @@ class LearnedProposals:
 
     def iteration(self, par, alpha=0.):
         """One iteration: proposal-restricted (held-out frames in full and
-        watched), or a full search when the last judgement failed. Returns
+        watched), or a full search when the last captured mass was too low. Returns
         the iteration's results with 'mode', 'captured_mass' and
         'evaluated_fraction'."""
         import time
