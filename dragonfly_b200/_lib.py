@@ -64,6 +64,7 @@ _SIGS = {
     "dfg_save_emc": (C.c_int, [_V, C.c_char_p]),
     "dfg_set_symmetry": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_set_refinement": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_longlong), _I]),
+    "dfg_set_refinement_topk": (C.c_int, [_V, C.c_int, _I, C.c_int, _I, C.c_int, _I]),
     "dfg_set_model_type": (C.c_int, [_V, C.c_int, C.c_int]),
     "dfg_run_iteration": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D]),
     "dfg_get_graph_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
@@ -271,6 +272,15 @@ class Context:
         off, flat = _csr(rel_quat)
         self.call("dfg_set_refinement", int(num_coarse), ptr(qm, C.c_int), ptr(off, C.c_longlong),
                   ptr(flat, C.c_int))
+
+    def set_refinement_topk(self, num_coarse, quat_mapping, top, all_frames=()):
+        """Refinement from a top-K array [N, K] of coarse cells per frame; the
+        frames in all_frames evaluate every orientation."""
+        qm = np.ascontiguousarray(quat_mapping, np.int32).ravel()
+        t = np.ascontiguousarray(top, np.int32)
+        af = np.ascontiguousarray(all_frames, np.int32).ravel()
+        self.call("dfg_set_refinement_topk", int(num_coarse), ptr(qm, C.c_int), int(t.shape[1]), ptr(t, C.c_int),
+                  int(af.size), ptr(af, C.c_int) if af.size else None)
 
     def set_watch(self, frames, cells):
         """Watched frames (ascending) with a coarse-cell list each (lists, a

@@ -354,6 +354,78 @@ extern "C" int dfg_set_detector_distance(dfg_ctx *ctx, double detd) {
 	return DFG_OK;
 }
 
+// The common end of dfg_set_refinement / dfg_set_refinement_topk: the cell
+// bits go up, the coarse map is kept, the pair lists are rebuilt at the next
+// iteration.
+static int finish_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
+                             const std::vector<uint32_t> &bits) {
+	CK(cudaSetDevice(ctx->device));
+	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->h_qmap.assign(quat_mapping, quat_mapping + ctx->num_rot);
+	ctx->pairs_valid = false;
+	if (num_coarse != ctx->num_coarse)
+		ctx->h_watch.clear();  // the cell bits were for another coarse set
+	ctx->num_coarse = num_coarse;
+	ctx->rwords = (num_coarse + 31) / 32;
+	ctx->refine = true;
+	ctx->qmap_valid = false;
+	return DFG_OK;
+}
+
+extern "C" int dfg_set_refinement_topk(dfg_ctx *ctx, int num_coarse, const int *quat_mapping, int K, const int *top,
+                                       int n_all, const int *all_frames) {
+	if (!ctx)
+		return DFG_ERR_ARG;
+	if (int rc = need_frames(ctx))
+		return rc;
+	NEED(ctx->num_rot > 0, DFG_ERR_STATE, "refinement: set the quaternions first");
+	NEED(num_coarse > 0 && quat_mapping && K >= 1 && top && n_all >= 0 && (n_all == 0 || all_frames), DFG_ERR_ARG,
+	     "refinement: need num_coarse > 0, the coarse map, K >= 1 cells per frame and the full-search frames");
+	const int N = ctx->N, rw = (num_coarse + 31) / 32;
+	for (int r = 0; r < ctx->num_rot; ++r)
+		NEED(quat_mapping[r] >= 0 && quat_mapping[r] < num_coarse, DFG_ERR_ARG,
+		     "refinement: quat_mapping[%d] = %d outside [0, %d)", r, quat_mapping[r], num_coarse);
+	std::vector<uint8_t> all((size_t)N, 0);
+	for (int i = 0; i < n_all; ++i) {
+		NEED(all_frames[i] >= 0 && all_frames[i] < N, DFG_ERR_ARG, "refinement: frame %d out of range",
+		     all_frames[i]);
+		all[all_frames[i]] = 1;
+	}
+	std::vector<uint32_t> bits((size_t)N * rw, 0u);
+	const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+	std::vector<long long> bad((size_t)nth, -1);
+	const uint32_t last = (num_coarse & 31) ? ((1u << (num_coarse & 31)) - 1u) : 0xffffffffu;
+	parallel_ranges(N, std::min<int>(nth, std::max(1, N / 4096)), [&](int k, long long b, long long e) {
+		for (long long d = b; d < e; ++d) {
+			uint32_t *w = bits.data() + (size_t)d * rw;
+			if (all[d]) {
+				for (int j = 0; j < rw; ++j)
+					w[j] = j + 1 < rw ? 0xffffffffu : last;
+				continue;
+			}
+			for (long long t = d * K; t < (d + 1) * K; ++t) {
+				const int c = top[t];
+				if (c < 0 || c >= num_coarse) {
+					if (bad[k] < 0)
+						bad[k] = t;
+					continue;
+				}
+				w[c >> 5] |= 1u << (c & 31);
+			}
+		}
+	});
+	for (long long t : bad)
+		NEED(t < 0, DFG_ERR_ARG, "refinement: entry %lld lists coarse orientation %d outside [0, %d)", t, top[t],
+		     num_coarse);
+	ctx->h_rel_off.resize((size_t)N + 1);
+	for (int d = 0; d <= N; ++d)
+		ctx->h_rel_off[d] = (long long)d * K;
+	ctx->h_rel.assign(top, top + (size_t)N * K);
+	ctx->h_rel_all = std::move(all);
+	return finish_refinement(ctx, num_coarse, quat_mapping, bits);
+}
+
 extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
                                   const long long *rel_off, const int *rel_quat) {
 	if (!ctx)
@@ -394,20 +466,10 @@ extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_
 	for (long long t : bad)
 		NEED(t < 0, DFG_ERR_ARG, "refinement: entry %lld lists coarse orientation %d outside [0, %d)", t, rel_quat[t],
 		     num_coarse);
-	CK(cudaSetDevice(ctx->device));
-	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
-	CK(cudaStreamSynchronize(ctx->stream));
-	ctx->h_qmap.assign(quat_mapping, quat_mapping + ctx->num_rot);
 	ctx->h_rel_off.assign(rel_off, rel_off + N + 1);
 	ctx->h_rel.assign(rel_quat, rel_quat + rel_off[N]);
-	ctx->pairs_valid = false;
-	if (num_coarse != ctx->num_coarse)
-		ctx->h_watch.clear();  // the cell bits were for another coarse set
-	ctx->num_coarse = num_coarse;
-	ctx->rwords = rw;
-	ctx->refine = true;
-	ctx->qmap_valid = false;
-	return DFG_OK;
+	ctx->h_rel_all.clear();
+	return finish_refinement(ctx, num_coarse, quat_mapping, bits);
 }
 
 extern "C" int dfg_set_watch(dfg_ctx *ctx, int n, const int *frames, const long long *cell_off, const int *cells) {
@@ -1444,8 +1506,18 @@ static int build_pairs(dfg_ctx *ctx) {
 		std::vector<int> stamp((size_t)RT, -1), tmp;
 		auto &out = ftile_th[k];
 		auto &tc = tcount_th[k];
+		const bool any_all = !ctx->h_rel_all.empty();
 		for (long long d = b; d < e; ++d) {
 			tmp.clear();
+			if (any_all && ctx->h_rel_all[d]) {  // every tile
+				for (int t = 0; t < RT; ++t)
+					tmp.push_back(t);
+				out.insert(out.end(), tmp.begin(), tmp.end());
+				fcount[d] = RT;
+				for (int t = 0; t < RT; ++t)
+					tc[t]++;
+				continue;
+			}
 			for (long long j = ctx->h_rel_off[d]; j < ctx->h_rel_off[d + 1]; ++j) {
 				const int c = ctx->h_rel[j];
 				for (long long q = coff[c]; q < coff[c + 1]; ++q)

@@ -212,6 +212,7 @@ struct dfg_ctx {
 	double block_budget_mb = 0.;
 	std::vector<long long> h_rel_off;
 	std::vector<int> h_rel;
+	std::vector<uint8_t> h_rel_all;  // per frame: every coarse cell relevant (empty: none)
 	long long npairs = 0;
 	std::vector<long long> h_tile_off;  // [RT + 1]
 	DevBuf<long long> tile_off, frame_off;

@@ -214,7 +214,7 @@ class LearnedProposals:
         t1 = time.perf_counter()
         n_watch = max(1, int(round(self.held_out * N)))
         watch = np.sort(self.rng.choice(N, n_watch, replace=False)).astype(np.int32)
-        ctx.set_refinement(self.nc, self.qmap, restriction_lists(top, watch, self.nc))
+        ctx.set_refinement_topk(self.nc, self.qmap, top, watch)
         ctx.set_watch(watch, top[watch])
         t2 = time.perf_counter()
         out = dict(ctx.run_iteration(par, alpha))

@@ -156,6 +156,11 @@ DFG_API int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order);
  * setting either again switches it off. One model mode only. */
 DFG_API int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
                                const long long *rel_off, const int *rel_quat);
+/* The same from a top-K array: frame d's relevant coarse orientations are
+ * top[d * K .. d * K + K), except for the n_all frames in all_frames, which
+ * evaluate every orientation (learned proposals with held-out frames). */
+DFG_API int dfg_set_refinement_topk(dfg_ctx *ctx, int num_coarse, const int *quat_mapping, int K, const int *top,
+                                    int n_all, const int *all_frames);
 
 /* Watched frames of a refined (proposal-restricted) search: frames[n]
  * (ascending) and, per frame, a list of coarse cells cells[cell_off[i] ..
