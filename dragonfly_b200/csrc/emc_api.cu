@@ -357,10 +357,10 @@ extern "C" int dfg_set_detector_distance(dfg_ctx *ctx, double detd) {
 // The common end of dfg_set_refinement / dfg_set_refinement_topk: the cell
 // bits go up, the coarse map is kept, the pair lists are rebuilt at the next
 // iteration.
-static int finish_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
-                             const std::vector<uint32_t> &bits) {
+static int finish_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping, const uint32_t *bits,
+                             size_t nbits) {
 	CK(cudaSetDevice(ctx->device));
-	CK(upload(ctx->rel_bits, bits.data(), bits.size(), ctx->stream));
+	CK(upload(ctx->rel_bits, bits, nbits, ctx->stream));
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->h_qmap.assign(quat_mapping, quat_mapping + ctx->num_rot);
 	ctx->pairs_valid = false;
@@ -392,18 +392,22 @@ extern "C" int dfg_set_refinement_topk(dfg_ctx *ctx, int num_coarse, const int *
 		     all_frames[i]);
 		all[all_frames[i]] = 1;
 	}
-	std::vector<uint32_t> bits((size_t)N * rw, 0u);
+	CK(cudaSetDevice(ctx->device));
+	CK(ctx->stage_bits.ensure((size_t)N * rw));
+	uint32_t *bits = ctx->stage_bits.p;
 	const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
 	std::vector<long long> bad((size_t)nth, -1);
 	const uint32_t last = (num_coarse & 31) ? ((1u << (num_coarse & 31)) - 1u) : 0xffffffffu;
 	parallel_ranges(N, std::min<int>(nth, std::max(1, N / 4096)), [&](int k, long long b, long long e) {
 		for (long long d = b; d < e; ++d) {
-			uint32_t *w = bits.data() + (size_t)d * rw;
+			uint32_t *w = bits + (size_t)d * rw;
 			if (all[d]) {
 				for (int j = 0; j < rw; ++j)
 					w[j] = j + 1 < rw ? 0xffffffffu : last;
 				continue;
 			}
+			for (int j = 0; j < rw; ++j)
+				w[j] = 0u;
 			for (long long t = d * K; t < (d + 1) * K; ++t) {
 				const int c = top[t];
 				if (c < 0 || c >= num_coarse) {
@@ -423,7 +427,7 @@ extern "C" int dfg_set_refinement_topk(dfg_ctx *ctx, int num_coarse, const int *
 		ctx->h_rel_off[d] = (long long)d * K;
 	ctx->h_rel.assign(top, top + (size_t)N * K);
 	ctx->h_rel_all = std::move(all);
-	return finish_refinement(ctx, num_coarse, quat_mapping, bits);
+	return finish_refinement(ctx, num_coarse, quat_mapping, bits, (size_t)N * rw);
 }
 
 extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
@@ -448,10 +452,13 @@ extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_
 		NEED(rel_off[d + 1] >= rel_off[d], DFG_ERR_ARG, "refinement: rel_off decreases at frame %d", d);
 	// one bit per relevant coarse orientation, frames split over the host
 	// threads; the first bad entry of each range is reported
-	std::vector<uint32_t> bits((size_t)N * rw, 0u);
+	CK(cudaSetDevice(ctx->device));
+	CK(ctx->stage_bits.ensure((size_t)N * rw));
+	uint32_t *bits = ctx->stage_bits.p;
 	const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
 	std::vector<long long> bad((size_t)nth, -1);
 	parallel_ranges(N, std::min<int>(nth, std::max(1, N / 4096)), [&](int k, long long b, long long e) {
+		std::fill(bits + (size_t)b * rw, bits + (size_t)e * rw, 0u);
 		for (long long d = b; d < e; ++d)
 			for (long long t = rel_off[d]; t < rel_off[d + 1]; ++t) {
 				const int c = rel_quat[t];
@@ -469,7 +476,7 @@ extern "C" int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_
 	ctx->h_rel_off.assign(rel_off, rel_off + N + 1);
 	ctx->h_rel.assign(rel_quat, rel_quat + rel_off[N]);
 	ctx->h_rel_all.clear();
-	return finish_refinement(ctx, num_coarse, quat_mapping, bits);
+	return finish_refinement(ctx, num_coarse, quat_mapping, bits, (size_t)N * rw);
 }
 
 extern "C" int dfg_set_watch(dfg_ctx *ctx, int n, const int *frames, const long long *cell_off, const int *cells) {
@@ -1545,8 +1552,10 @@ static int build_pairs(dfg_ctx *ctx) {
 			s += tcount_th[k][t];
 		toff[t + 1] = toff[t] + s;
 	}
-	// pass 2: per-range cursors, then the pair arrays
-	std::vector<int> ptile((size_t)np), pframe((size_t)np), fpair((size_t)np);
+	// pass 2: per-range cursors, then the pair arrays, written straight into
+	// page-locked staging
+	CK(ctx->stage_pairs.ensure((size_t)3 * std::max<long long>(np, 1)));
+	int *ptile = ctx->stage_pairs.p, *pframe = ptile + np, *fpair = pframe + np;
 	parallel_ranges(N, nth, [&](int k, long long b, long long e) {
 		std::vector<long long> cur((size_t)RT);
 		for (int t = 0; t < RT; ++t) {
@@ -1568,9 +1577,9 @@ static int build_pairs(dfg_ctx *ctx) {
 	});
 	CK(upload(ctx->frame_off, foff.data(), foff.size(), st));
 	CK(upload(ctx->tile_off, toff.data(), toff.size(), st));
-	CK(upload(ctx->pair_tile, ptile.data(), ptile.size(), st));
-	CK(upload(ctx->pair_frame, pframe.data(), pframe.size(), st));
-	CK(upload(ctx->frame_pair, fpair.data(), fpair.size(), st));
+	CK(upload(ctx->pair_tile, ptile, (size_t)np, st));
+	CK(upload(ctx->pair_frame, pframe, (size_t)np, st));
+	CK(upload(ctx->frame_pair, fpair, (size_t)np, st));
 	CK(cudaStreamSynchronize(st));
 	ctx->npairs = np;
 	ctx->h_tile_off = std::move(toff);

@@ -59,6 +59,35 @@ struct DevBuf {
 	}
 };
 
+// Page-locked host staging buffer (grow-only): large per-iteration uploads go
+// through it at full copy speed, written in place by the host threads.
+template <typename T>
+struct HostBuf {
+	T *p = nullptr;
+	size_t n = 0;
+	HostBuf() = default;
+	HostBuf(const HostBuf &) = delete;
+	HostBuf &operator=(const HostBuf &) = delete;
+	~HostBuf() { release(); }
+	void release() {
+		if (p)
+			cudaFreeHost(p);
+		p = nullptr;
+		n = 0;
+	}
+	cudaError_t ensure(size_t count) {
+		if (count <= n && p)
+			return cudaSuccess;
+		release();
+		cudaError_t e = cudaMallocHost(&p, std::max<size_t>(count, 1) * sizeof(T));
+		if (e == cudaSuccess)
+			n = std::max<size_t>(count, 1);
+		else
+			p = nullptr;
+		return e;
+	}
+};
+
 struct Chunk {
 	int d0 = 0, nc = 0;
 	DevBuf<uint32_t> cs;       // per pixel: count-1 frames, then (frame | count << 22), padded
@@ -213,6 +242,8 @@ struct dfg_ctx {
 	std::vector<long long> h_rel_off;
 	std::vector<int> h_rel;
 	std::vector<uint8_t> h_rel_all;  // per frame: every coarse cell relevant (empty: none)
+	HostBuf<int> stage_pairs;        // pair_tile, pair_frame, frame_pair staged for upload
+	HostBuf<uint32_t> stage_bits;    // rel_bits staged for upload
 	long long npairs = 0;
 	std::vector<long long> h_tile_off;  // [RT + 1]
 	DevBuf<long long> tile_off, frame_off;
