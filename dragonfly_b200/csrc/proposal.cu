@@ -794,12 +794,6 @@ static int pnet_map(dfg_pnet *net, CUtensorMap *map, const void *base, long long
 template <int BN>
 static int launch_tc_gemm(dfg_pnet *net, const CUtensorMap &ma, const CUtensorMap &mb, int num_kb, int M, int N,
                           const float *bias, int relu, float *C) {
-	static bool attr = false;
-	if (!attr) {
-		PK(cudaFuncSetAttribute(pnet_gemm_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                        GemmCfg<BN>::SMEM));
-		attr = true;
-	}
 	dim3 grid((M + 127) / 128, (N + BN - 1) / BN);
 	pnet_gemm_tc_kernel<BN><<<grid, 192, GemmCfg<BN>::SMEM, net->stream>>>(ma, mb, num_kb, M, N, bias, relu, C, N,
 	                                                                     net->terr.p);
@@ -808,8 +802,13 @@ static int launch_tc_gemm(dfg_pnet *net, const CUtensorMap &ma, const CUtensorMa
 }
 
 // BF16 weight copies with K padded to 64 for the tensor-core products (after
-// any change of the weights).
+// any change of the weights), and the products' shared-memory limits on this
+// network's device.
 static int pad_weights(dfg_pnet *net) {
+	PK(cudaFuncSetAttribute(pnet_gemm_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<32>::SMEM));
+	PK(cudaFuncSetAttribute(pnet_gemm_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmCfg<64>::SMEM));
+	PK(cudaFuncSetAttribute(pnet_gemm_tc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                        GemmCfg<256>::SMEM));
 	for (int l = 1; l < NL; ++l) {
 		const LayerShape &sh = net->L[l];
 		const int K = sh.fan_in(), Kp = kpad64(K);
