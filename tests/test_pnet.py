@@ -163,3 +163,22 @@ def test_gpu_soft_target_gradients_match_oracle():
     with pytest.raises(RuntimeError):
         net.set_targets(np.array([0, 2] + [2] * 7), np.array([3, 3]), np.array([0.5, 0.5], np.float32))
     net.close()
+
+
+def test_oracle_logits_agree_with_the_loss_forward():
+    """The oracle's inference forward (BF16 weights, FP64 activations) gives
+    the loss that loss_and_grads computes from its own forward pass; with
+    rounded activations it stays within a BF16 step's effect."""
+    from oracle.pnet_oracle import logits
+    rng = np.random.default_rng(5)
+    nc = 12
+    p = _params(rng, nc)
+    x = np.log1p(rng.poisson(0.7, (4, 1024)).astype(np.float64))
+    y = np.array([0, 3, 7, 11])
+    z = logits(p, x, nc)
+    m = z.max(1, keepdims=True)
+    loss = float(np.mean(np.log(np.exp(z - m).sum(1)) + m[:, 0] - z[np.arange(4), y]))
+    ref, _ = loss_and_grads(p, x, y, nc)
+    assert abs(loss - ref) <= 1e-12 * abs(ref)
+    zr = logits(p, x, nc, round_activations=True)
+    assert np.linalg.norm(zr - z) <= 2e-2 * np.linalg.norm(z)
