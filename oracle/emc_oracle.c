@@ -12,6 +12,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #define ORC_PROB_MIN 1.e-6         /* max_internal.h:6 */
 #define ORC_PDIFF_THRESH 14.       /* max_internal.h:7 */
@@ -220,16 +223,169 @@ static int list_find(const kept_list *l, int r) {
 	return -1;
 }
 
+/* Probability lists of the last orc_maximize call, kept when g_keep_prob is
+ * set (the save_prob path of max_prob.c:294-325 needs the same lists). */
+static int g_keep_prob = 0;
+static kept_list *g_kept = NULL;
+static int g_kept_n = 0;
+
+static void orc_free_kept(void) {
+	int d;
+	for (d = 0; d < g_kept_n; ++d) {
+		free(g_kept[d].pos);
+		free(g_kept[d].val);
+	}
+	free(g_kept);
+	g_kept = NULL;
+	g_kept_n = 0;
+}
+
+void orc_set_keep_prob(int on) {
+	g_keep_prob = on != 0;
+	if (!g_keep_prob)
+		orc_free_kept();
+}
+
+int orc_kept_prob(int d, int *pos, double *val) {
+	const kept_list *l;
+	if (g_kept == NULL || d < 0 || d >= g_kept_n)
+		return -1;
+	l = &g_kept[d];
+	if (pos != NULL)
+		memcpy(pos, l->pos, (size_t)l->n * sizeof(int));
+	if (val != NULL)
+		memcpy(val, l->val, (size_t)l->n * sizeof(double));
+	return l->n;
+}
+
 /* Orientations are processed in blocks whose slices fit in this many doubles. */
 #define ORC_BLOCK_DOUBLES (1L << 27)
+
+/* Geometry of one (orientation, pixel) term of the merge: base voxel index
+ * (mode * vol + x * size^2 + y * size + z; -1 when the pixel is skipped),
+ * fractional offsets and the merged value slice / corr. */
+typedef struct {
+	long base;
+	double fx, fy, fz, w;
+} merge_rec;
+
+/* Orientations per sub-block of the parallel merge. */
+#define ORC_MERGE_SUB 64
+
+/* Scratch of merge_block: per (orientation, pixel) geometry, and per
+ * (orientation, grid plane) the pixels with corners on that plane. */
+typedef struct {
+	merge_rec *rec;     /* [ORC_MERGE_SUB][num_pix] */
+	int *idx;           /* [ORC_MERGE_SUB][2 * num_pix] */
+	long *off;          /* [ORC_MERGE_SUB][planes + 1] */
+	double *acc;        /* [M * V][2]: weight, model2 */
+	long planes;        /* M * size */
+} merge_scratch;
+
+/* slice_merge3d (model.c:171-244) for orientations r0 .. r1-1 in ascending
+ * order, as the sequential loop of merge_tomogram (max_update.c:18-40) does.
+ * The additions to every voxel happen in the order of that loop (orientation,
+ * pixel, corner), so the sums are bit-identical to it at any thread count:
+ * the geometry of each (orientation, pixel) is computed in parallel over
+ * orientations and listed under the two grid planes (mode * size + x and
+ * x + 1) its corners lie on; then the planes are shared out among the threads
+ * and each walks its planes' lists in orientation and pixel order. The sums go
+ * to acc, (weight, model2) interleaved per voxel so that one cache line holds
+ * both. */
+static void merge_block(int r0, int r1, int M, const double *quats, const double *psum_r, const double *views,
+                        double *acc, long size, int num_pix, const double *qvals,
+                        const double *corr, const uint8_t *mask, merge_scratch *ms) {
+	const long vol = size * size * size, s2 = size * size;
+	const long planes = ms->planes;
+	int s0;
+	for (s0 = r0; s0 < r1; s0 += ORC_MERGE_SUB) {
+		const int s1 = s0 + ORC_MERGE_SUB < r1 ? s0 + ORC_MERGE_SUB : r1;
+		int r;
+		long j;
+		#pragma omp parallel for schedule(dynamic, 1)
+		for (r = s0; r < s1; ++r) {
+			merge_rec *out = &ms->rec[(long)(r - s0) * num_pix];
+			int *idx = &ms->idx[(long)(r - s0) * 2 * num_pix];
+			long *off = &ms->off[(long)(r - s0) * (planes + 1)];
+			const double *slice = &views[(long)(r - r0) * num_pix];
+			double rot[3][3], pos[3];
+			long t, x, y, z, p;
+			for (p = 0; p <= planes; ++p)
+				off[p] = 0;
+			if (!(psum_r[r] > 0.))
+				continue;
+			orc_make_rot_quat(&quats[(r / M) * 5], rot);
+			for (t = 0; t < num_pix; ++t) {
+				long pl;
+				out[t].base = -1;
+				if (mask[t] > 1)
+					continue;
+				rotate_pixel(rot, &qvals[t * 3], (double)(size / 2), pos);
+				x = (long)pos[0];
+				y = (long)pos[1];
+				z = (long)pos[2];
+				if (x < 0 || x > size - 2 || y < 0 || y > size - 2 || z < 0 || z > size - 2)
+					continue;
+				out[t].base = (long)(r % M) * vol + x * s2 + y * size + z;
+				out[t].fx = pos[0] - x;
+				out[t].fy = pos[1] - y;
+				out[t].fz = pos[2] - z;
+				out[t].w = slice[t] / corr[t];
+				/* corners 0-3 lie on plane pl, 4-7 on pl + 1 (x + 1 <= size - 1) */
+				pl = (long)(r % M) * size + x;
+				off[pl + 1]++;
+				off[pl + 2]++;
+			}
+			for (p = 0; p < planes; ++p)
+				off[p + 1] += off[p];
+			for (t = 0; t < num_pix; ++t) {
+				long pl;
+				if (out[t].base < 0)
+					continue;
+				pl = out[t].base / s2;
+				idx[off[pl]++] = (int)t;
+				idx[off[pl + 1]++] = (int)t;
+			}
+			/* the fill advanced each start to the next plane's: shift back */
+			for (p = planes; p > 0; --p)
+				off[p] = off[p - 1];
+			off[0] = 0;
+		}
+		#pragma omp parallel for schedule(dynamic, 1)
+		for (j = 0; j < planes; ++j) {
+			int rr;
+			for (rr = s0; rr < s1; ++rr) {
+				const merge_rec *rec = &ms->rec[(long)(rr - s0) * num_pix];
+				const int *idx = &ms->idx[(long)(rr - s0) * 2 * num_pix];
+				const long *off = &ms->off[(long)(rr - s0) * (planes + 1)];
+				long i, k;
+				for (i = off[j]; i < off[j + 1]; ++i) {
+					const merge_rec *e = &rec[idx[i]];
+					const long b = e->base;
+					const int upper = b / s2 != j;     /* j is the plane of corners 4-7 */
+					const double fx = e->fx, fy = e->fy, fz = e->fz, w = e->w;
+					const double cx = 1. - fx, cy = 1. - fy, cz = 1. - fz;
+					const long id[8] = {b, b + 1, b + size, b + size + 1,
+					                    b + s2, b + s2 + 1, b + s2 + size, b + s2 + size + 1};
+					const double fw[8] = {cx * cy * cz, cx * cy * fz, cx * fy * cz, cx * fy * fz,
+					                      fx * cy * cz, fx * cy * fz, fx * fy * cz, fx * fy * fz};
+					for (k = upper ? 4 : 0; k < (upper ? 8 : 4); ++k) {
+						acc[2 * id[k]] += fw[k];
+						acc[2 * id[k] + 1] += fw[k] * w;
+					}
+				}
+			}
+		}
+	}
+}
 
 /* The reference visits orientations in an outer loop and frames in an inner
  * loop. Every quantity it accumulates is either per frame (summed over
  * orientations in ascending order) or per orientation (summed over frames in
  * ascending order); this restatement keeps each of those orders and
  * parallelises only across independent frames or orientations, so its results
- * do not depend on the thread count. The merge into model2 is sequential in
- * orientation order, as with one reference thread. */
+ * do not depend on the thread count. The merge into model2 adds to every voxel
+ * in orientation order, as with one reference thread (merge_block). */
 double orc_maximize(int num_pix, const double *qvals, const double *corr, const uint8_t *mask,
                     int num_data, const int *ones, const int *multi, const int *place_ones,
                     const int *place_multi, const int *count_multi,
@@ -247,6 +403,7 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 	long *multi_off = malloc((size_t)(num_data + 1) * sizeof(long));
 	long blk = ORC_BLOCK_DOUBLES / (num_pix > 0 ? num_pix : 1);
 	double *views;
+	merge_scratch ms;
 	kept_list *lists = calloc((size_t)num_data, sizeof(kept_list));
 	double total = 0., rescale, avg_ll = 0., mutual_info = 0.;
 	const int use_scale = need_scaling && (iteration > 1 || known_scale);
@@ -257,6 +414,11 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 	if (blk > R)
 		blk = R;
 	views = malloc((size_t)blk * num_pix * sizeof(double));
+	ms.planes = (long)M * size;
+	ms.rec = malloc((size_t)ORC_MERGE_SUB * num_pix * sizeof(merge_rec));
+	ms.idx = malloc((size_t)ORC_MERGE_SUB * 2 * num_pix * sizeof(int));
+	ms.off = malloc((size_t)ORC_MERGE_SUB * (ms.planes + 1) * sizeof(long));
+	ms.acc = calloc((size_t)2 * M * vol, sizeof(double));
 	ones_off[0] = multi_off[0] = 0;
 	for (d = 0; d < num_data; ++d) {
 		ones_off[d + 1] = ones_off[d] + ones[d];
@@ -410,10 +572,15 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 				for (t = 0; t < num_pix; ++t)
 					view[t] /= pr;
 		}
-		for (r = r0; r < r1; ++r)
-			if (psum_r[r] > 0.)
-				orc_slice_merge3d(&quats[ROTIND(r) * 5], MODE(r), &views[(long)(r - r0) * num_pix], model2,
-				                  weight, size, num_pix, qvals, corr, mask);
+		merge_block(r0, r1, M, quats, psum_r, views, ms.acc, size, num_pix, qvals, corr, mask, &ms);
+	}
+
+	for (r0 = 0; r0 < M; ++r0) {
+		long x;
+		for (x = r0 * vol; x < (r0 + 1) * vol; ++x) {
+			weight[x] = ms.acc[2 * x];
+			model2[x] = ms.acc[2 * x + 1];
+		}
 	}
 
 	/* combine_information_mpi (max_prob.c:344-427). The packaged Iterate never
@@ -439,12 +606,23 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 	scalars_out[1] = mutual_info;
 	scalars_out[2] = avg_ll;
 
-	for (d = 0; d < num_data; ++d) {
-		free(lists[d].pos);
-		free(lists[d].val);
+	if (g_keep_prob) {      /* retained for orc_kept_prob until the next call */
+		orc_free_kept();
+		g_kept = lists;
+		g_kept_n = num_data;
 	}
-	free(lists);
+	else {
+		for (d = 0; d < num_data; ++d) {
+			free(lists[d].pos);
+			free(lists[d].val);
+		}
+		free(lists);
+	}
 	free(views);
+	free(ms.rec);
+	free(ms.idx);
+	free(ms.off);
+	free(ms.acc);
 	free(ones_off);
 	free(multi_off);
 #undef ROTIND

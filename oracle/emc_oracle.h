@@ -2,14 +2,14 @@
  * photon data. TEST INFRASTRUCTURE ONLY: the product never links it; tests/,
  * the smoke check and bench.py's CPU-baseline leg use it as the checker.
  *
- * A single-threaded FP64 restatement of duaneloh/Dragonfly's packaged engine
+ * An FP64 restatement of duaneloh/Dragonfly's packaged engine
  * (dragonfly/src/maximize.c, max_prob.c, max_update.c, max_scale.c, model.c,
  * iterate.c) and of the model update in dragonfly/recon.pyx:112-149. Floating
  * point operations are written in the reference's order so that, built without
  * FMA contraction, results are bit-identical to the reference engine run with
- * one OpenMP thread. Pinned against the compiled reference (oracle/_ref) by
- * tests/test_oracle_vs_reference.py and against committed golden vectors by
- * tests/test_golden.py.
+ * one OpenMP thread, at any thread count of the oracle itself (it parallelises
+ * only where every sum keeps its order). Pinned against the compiled reference
+ * (oracle/_ref) and against committed golden vectors by tests/test_oracle.py.
  */
 #ifndef DFG_EMC_ORACLE_H
 #define DFG_EMC_ORACLE_H
@@ -67,6 +67,13 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
                     double *model2, double *weight, double *u, double *psum_r,
                     int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
                     double *psum_d, double *quat_norm, int *num_prob, double *scalars_out);
+
+/* With on != 0, orc_maximize keeps its per-frame probability lists (kept
+ * orientations in ascending order and their normalised probabilities P) until
+ * the next call; orc_kept_prob(d, pos, val) copies frame d's list into pos /
+ * val (either may be NULL) and returns its length, -1 when none is kept. */
+void orc_set_keep_prob(int on);
+int orc_kept_prob(int d, int *pos, double *val);
 
 /* EMCRecon.update_model for RECON3D with Friedel symmetry only (recon.pyx:112-149).
  * model2 is normalised in place and model1 is replaced (alpha = 0) or mixed.

@@ -2,8 +2,9 @@
 
 Two engines with one interface:
 
-* ``OracleEngine`` -- our own single-threaded C restatement (``liboracle.so``,
-  source ``emc_oracle.c``) of duaneloh/Dragonfly's packaged EMC engine;
+* ``OracleEngine`` -- our own C restatement (``liboracle.so``,
+  source ``emc_oracle.c``; OpenMP, bit-identical to the reference with one
+  thread at any thread count) of duaneloh/Dragonfly's packaged EMC engine;
 * ``ReferenceEngine`` -- the reference's own C engine compiled from its sources
   (``_ref/libdragonfly_ref.so``, driver ``ref_driver.c``).
 
@@ -316,6 +317,10 @@ class OracleEngine:
         L.orc_calc_beta.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp]
         L.orc_slice_gen3d.argtypes = [_dp, C.c_int, _dp, C.c_int, _dp, _dp, C.c_long, C.c_long, _dp]
         L.orc_slice_merge3d.argtypes = [_dp, C.c_int, _dp, _dp, _dp, C.c_long, C.c_int, _dp, _dp, _up]
+        L.orc_set_keep_prob.argtypes = [C.c_int]
+        L.orc_kept_prob.restype = C.c_int
+        L.orc_kept_prob.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        self.save_prob = False
         self.prob = p = prob
         n = p.num_data
         self.fcounts = np.zeros(n, np.int32)
@@ -334,6 +339,25 @@ class OracleEngine:
 
     def model1(self):
         return self._model1.copy()
+
+    def set_save_prob(self, on):
+        """Makes run_iteration return the per-frame probability lists as
+        res["sparse_prob"] = (offsets, place, prob), the layout of
+        ReferenceEngine.set_save_prob."""
+        self.save_prob = bool(on)
+
+    def _sparse_prob(self):
+        L = self.lib
+        n = self.prob.num_data
+        counts = np.array([max(L.orc_kept_prob(d, None, None), 0) for d in range(n)], np.int64)
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum(counts)
+        place = np.zeros(int(off[-1]), np.int32)
+        prob = np.zeros(int(off[-1]))
+        for d in range(n):
+            if counts[d]:
+                L.orc_kept_prob(d, place[off[d]:].ctypes.data, prob[off[d]:].ctypes.data)
+        return off, place, prob
 
     def slice_gen(self, quat, mode=0):
         p = self.prob
@@ -366,6 +390,7 @@ class OracleEngine:
         qn = np.zeros((n, M))
         nprob = np.zeros(n, np.int32)
         sc = np.zeros(3)
+        L.orc_set_keep_prob(int(self.save_prob))
         avg_ll = L.orc_maximize(
             p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, n, p.ones, p.multi, p.place_ones,
             p.place_multi, p.count_multi, p.num_rot, M, p.quats.reshape(-1), p.size,
@@ -377,6 +402,9 @@ class OracleEngine:
                               psum_d=pd, u=u, psum_r=psum_r, quat_norm=qn, num_prob=nprob,
                               rescale=sc[0], mutual_info=sc[1], avg_likelihood=avg_ll,
                               mean_count=self.mean_count, beta=self.beta.copy())
+        if self.save_prob:
+            res["sparse_prob"] = self._sparse_prob()
+            L.orc_set_keep_prob(0)
         res["model2_sum"] = model2.copy()
         res["inter_weight"] = weight
         rms = L.orc_update_model(p.size, M, self._model1.reshape(-1), model2.reshape(-1),

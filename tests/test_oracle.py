@@ -98,3 +98,55 @@ def test_oracle_slice_ops_match_reference(oracle_built):
     for r in (0, 17, 200, 419):
         np.testing.assert_array_equal(ref.slice_gen(prob.quats[r]), orc.slice_gen(prob.quats[r]))
     ref.close()
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference sources not compiled here")
+def test_oracle_probability_lists_match_reference(oracle_built):
+    """The kept (orientation, probability) lists of one iteration equal the
+    reference's save_prob lists (max_prob.c:294-325) bit for bit."""
+    prob, _ = load_case("scaling")
+    ref = ReferenceEngine(prob, num_threads=1)
+    orc = OracleEngine(prob)
+    ref.set_save_prob(True)
+    orc.set_save_prob(True)
+    for it in (1, 2):
+        a = ref.run_iteration(it)["sparse_prob"]
+        b = orc.run_iteration(it)["sparse_prob"]
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    ref.close()
+
+
+_THREADS_SCRIPT = """
+import sys, hashlib
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, sys.argv[1] + "/tests")
+from common import load_case
+from oracle.oracle import OracleEngine
+prob, _ = load_case("modes2")
+eng = OracleEngine(prob)
+h = hashlib.sha256()
+for it in (1, 2):
+    r = eng.run_iteration(it)
+    for k in ("rmax", "likelihood", "p_norm", "psum_r", "model2_sum", "inter_weight", "model1"):
+        h.update(np.ascontiguousarray(r[k]).tobytes())
+print(h.hexdigest())
+"""
+
+
+def test_oracle_results_do_not_depend_on_its_thread_count(oracle_built):
+    """The oracle parallelises only where every sum keeps its order (frames,
+    orientations, and the merge's grid planes), so 1 and 5 OpenMP threads
+    give the same bytes."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = []
+    for n in ("1", "5"):
+        env = dict(os.environ, OMP_NUM_THREADS=n)
+        r = subprocess.run([sys.executable, "-c", _THREADS_SCRIPT, root], env=env, capture_output=True,
+                           text=True, check=True)
+        out.append(r.stdout.strip().splitlines()[-1])
+    assert out[0] == out[1]
