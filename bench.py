@@ -167,7 +167,11 @@ def max_over_ranks(x, world, device):
 # reference engine on the host cores
 # ---------------------------------------------------------------------------
 def reference_threads(w):
-    n = os.cpu_count() or 1
+    """Host threads for the reference engines: every core, unless the private
+    model copies of the packaged engine (maximize.c:103-104) would not fit in
+    half of the available memory. Returns (threads, nproc)."""
+    nproc = os.cpu_count() or 1
+    n = nproc
     try:
         import psutil
         avail = psutil.virtual_memory().available
@@ -175,38 +179,88 @@ def reference_threads(w):
         n = max(1, min(n, int(avail * 0.5 // per_thread)))
     except Exception:
         pass
-    return n
+    return n, nproc
 
 
-def reference_step(w, inp, n_frames, seed, threads):
-    """One reference iteration (maximize + update_model + normalize_scale) on
-    n_frames frames at the full orientation set. Returns seconds."""
-    from dragonfly_b200 import synth
-    from oracle.oracle import EMCProblem, ReferenceEngine
-    rng = np.random.default_rng(seed)
-    phi = np.exp(rng.normal(0., w["fluence_sigma"], n_frames))
-    fr = synth.sample_frames(inp["intens"], inp["qvals"], inp["corr"], inp["mask"], n_frames, rng, phi=phi)
-    prob = EMCProblem(inp["qvals"], inp["corr"], inp["mask"], fr["ones"], fr["multi"], fr["place_ones"],
-                      fr["place_multi"], fr["count_multi"], inp["quats"], inp["start"], need_scaling=1,
-                      update_scale=1, beta=w["beta"], beta_jump=w["beta_jump"], beta_period=w["beta_period"])
-    eng = ReferenceEngine(prob, num_threads=threads, fast=True)
+class FrameStock:
+    """Frames of the workload sampled on the host for the CPU engines, grown
+    on demand (a sample of n frames is the first n): each frame at a random
+    orientation with the workload's lognormal fluence, Poisson counts of the
+    FP64 slice (the oracle's slice_gen, the reference's geometry) on the
+    pixels with mask <= 1."""
+
+    def __init__(self, w, inp, seed):
+        from oracle.oracle import EMCProblem, OracleEngine
+        from dragonfly_b200 import synth
+        self.w, self.inp = w, inp
+        self.rng = np.random.default_rng(seed)
+        self.synth = synth
+        z = np.zeros(1, np.int32)
+        e = np.zeros(0, np.int32)
+        self.slicer = OracleEngine(EMCProblem(inp["qvals"], inp["corr"], inp["mask"], z, z, e, e, e,
+                                              np.array([[1., 0., 0., 0., 1.]]), inp["intens"][None]))
+        self.good = inp["mask"] <= 1
+        self.ones, self.multi, self.po, self.pm, self.cm = [], [], [], [], []
+
+    def _grow(self, n):
+        while len(self.ones) < n:
+            q = self.synth.random_quaternions(1, self.rng)[0]
+            phi = np.exp(self.rng.normal(0., self.w["fluence_sigma"]))
+            lam = self.slicer.slice_gen(np.append(q, 1.)) * phi
+            lam[~self.good] = 0.
+            c = self.rng.poisson(np.maximum(lam, 0.))
+            p1, pmu = np.nonzero(c == 1)[0], np.nonzero(c > 1)[0]
+            self.ones.append(p1.size)
+            self.multi.append(pmu.size)
+            self.po.append(p1.astype(np.int32))
+            self.pm.append(pmu.astype(np.int32))
+            self.cm.append(c[pmu].astype(np.int32))
+
+    def problem(self, n):
+        """An EMCProblem of the first n frames at the workload's orientations,
+        start model and schedule (need_scaling, update_scale)."""
+        from oracle.oracle import EMCProblem
+        self._grow(n)
+        cat = lambda xs: np.concatenate(xs[:n]).astype(np.int32)
+        inp, w = self.inp, self.w
+        return EMCProblem(inp["qvals"], inp["corr"], inp["mask"], np.array(self.ones[:n], np.int32),
+                          np.array(self.multi[:n], np.int32), cat(self.po), cat(self.pm), cat(self.cm),
+                          inp["quats"], inp["start"], need_scaling=1, update_scale=1, beta=w["beta"],
+                          beta_jump=w["beta_jump"], beta_period=w["beta_period"])
+
+
+def reference_step(w, inp, n_frames, seed, threads, engine="packaged", iteration=1, stock=None):
+    """One iteration of a reference engine (maximize + update_model +
+    normalize_scale) on n_frames frames at the full orientation set, from the
+    workload's start model, at the given iteration index (its beta and
+    whether the scale factors enter the likelihood). engine "packaged" is
+    dragonfly/src (the engine behind the Python API), "legacy" is src/ (the
+    `emc` binary). Returns seconds."""
+    from oracle.oracle import LegacyEngine, ReferenceEngine
+    stock = stock or FrameStock(w, inp, seed)
+    prob = stock.problem(n_frames)
+    eng = ReferenceEngine(prob, num_threads=threads, fast=True) if engine == "packaged" else \
+        LegacyEngine(prob, num_threads=threads)
     t0 = time.perf_counter()
-    eng.run_iteration(1)
+    eng.run_iteration(iteration)
     t = time.perf_counter() - t0
     eng.close()
     return t
 
 
-def reference_throughput(w, inp, threads, budget_s=40., steps=2):
+def reference_throughput(w, inp, threads, budget_s=40., steps=2, engine="packaged", iteration=1, seed=11,
+                         stock=None):
     """Reference pairs/s at the full frame count, extrapolated from frame
     samples: t(n) = a + b n through a small sample (64 frames: mostly the
     per-iteration slice work a) and a sample grown by 4x until its time is at
     least three times the small one's (so that the frame-dependent part b n
     dominates the difference) or the budget is spent; that sample is timed
-    steps - 1 times."""
+    steps - 1 times. The samples are prefixes of one host-sampled frame
+    stream (stock, a FrameStock; one is made when None)."""
     R = inp["quats"].shape[0]
+    kw = dict(engine=engine, iteration=iteration, stock=stock)
     n1 = 64
-    t1 = reference_step(w, inp, n1, 11, threads)
+    t1 = reference_step(w, inp, n1, seed, threads, **kw)
     spent, n2, t2 = t1, n1, t1
     while n2 < 16384:
         nxt = 4 * n2
@@ -214,7 +268,7 @@ def reference_throughput(w, inp, threads, budget_s=40., steps=2):
             pred = t1 + (t2 - t1) * (nxt - n1) / (n2 - n1)
             if spent + pred > budget_s:
                 break
-        t2 = reference_step(w, inp, nxt, 12, threads)
+        t2 = reference_step(w, inp, nxt, seed, threads, **kw)
         n2 = nxt
         spent += t2
         if t2 >= 3. * t1:
@@ -223,7 +277,7 @@ def reference_throughput(w, inp, threads, budget_s=40., steps=2):
     for k in range(max(0, steps - 2)):
         if spent + t2 > budget_s:
             break
-        reps.append(reference_step(w, inp, n2, 13 + k, threads))
+        reps.append(reference_step(w, inp, n2, seed, threads, **kw))
         spent += reps[-1]
     t2 = float(np.mean(reps))
     b = max((t2 - t1) / (n2 - n1), 1e-12)
@@ -231,7 +285,56 @@ def reference_throughput(w, inp, threads, budget_s=40., steps=2):
     N = w["n_frames"]
     t_full = a + b * N
     return dict(value=R * N / t_full, t_full=t_full, fixed_s=a, per_frame_s=b, samples={n1: t1, n2: t2},
-                raw_sample_pairs_s=R * n2 / t2, cores=threads, frame_share=(t2 - t1) / t2)
+                raw_sample_pairs_s=R * n2 / t2, cores=threads, frame_share=(t2 - t1) / t2, engine=engine,
+                iteration=iteration)
+
+
+def reference_engines(w, inp, threads, nproc, budget_s, steps, iteration):
+    """Both reference engines timed as above at one iteration index; the
+    faster is the baseline. Returns the cpu_baseline object."""
+    from oracle.oracle import legacy_available
+    stock = FrameStock(w, inp, 11)
+    res = {"packaged": reference_throughput(w, inp, threads, budget_s, steps, "packaged", iteration, stock=stock)}
+    if legacy_available():
+        res["legacy"] = reference_throughput(w, inp, threads, budget_s, steps, "legacy", iteration, stock=stock)
+    best = max(res, key=lambda k: res[k]["value"])
+    beta = min(1., w["beta"] * w["beta_jump"] ** ((iteration - 1) // w["beta_period"]))
+    names = {"packaged": "dragonfly/src (the engine behind the Python API)", "legacy": "src/ (the emc binary)"}
+    r = res[best]
+    return {"value": r["value"], "unit": UNIT, "cores": threads, "nproc": nproc, "kind": "reference",
+            "engine": best,
+            "sample": "reference engine %s, -O3 -march=native, OpenMP %d threads of %d cores, iteration %d "
+                      "(beta %.4g) from the workload's start model, on %s host-sampled frames at all %d "
+                      "orientations; t(n) = a + b n fitted and extrapolated to %d frames; the faster of the "
+                      "two reference engines" % (names[best], threads, nproc, iteration, beta,
+                                                 "/".join(str(k) for k in r["samples"]), inp["quats"].shape[0],
+                                                 w["n_frames"]),
+            "engines": {k: {"value": v["value"], "fixed_s": v["fixed_s"], "per_frame_s": v["per_frame_s"],
+                            "samples_s": {str(n): t for n, t in v["samples"].items()},
+                            "frame_share": v["frame_share"]} for k, v in res.items()}}
+
+
+# iterations of the parity block: beta 0.01 from the start model (rescale in
+# the likelihood), then beta 0.01 x sqrt(2) with the scale factors
+PARITY_ITERATIONS = (1, 6)
+
+
+def parity_block(w, inp, n_frames, iterations):
+    """The product's graph-launched iteration against the FP64 oracle
+    (bit-identical to the reference engine with one thread) on n_frames
+    frames simulated at the workload's geometry and fluence, at all of its
+    orientations; run after the timed region, on the host cores and the GPU.
+    Returns the per-iteration deviations and whether each meets the bar."""
+    from oracle.parity import BAR, compare_runs, simulated_subset
+    t0 = time.perf_counter()
+    prob = simulated_subset(inp, w, n_frames, seed=4242)
+    devs = compare_runs(prob, iterations, graph=True)
+    keep = ("iteration", "beta", "model_rel_l2", "ll_rel", "mi_rel", "rmax_agree", "scale_rel",
+            "frame_ll_max_rel", "within_bar")
+    return {"frames": n_frames, "orientations": int(inp["quats"].shape[0]),
+            "oracle": "FP64 restatement of dragonfly/src, bit-identical to the reference engine with one thread",
+            "bar": BAR, "iterations": [{k: d[k] for k in keep} for d in devs],
+            "all_within_bar": all(d["within_bar"] for d in devs), "seconds": time.perf_counter() - t0}
 
 
 # ---------------------------------------------------------------------------
@@ -289,6 +392,11 @@ def run_ours(args, rank, world, local_rank):
         step(it)
         it += 1
     wl = ctx.workload()
+    # the ceiling of the gather kernels' access pattern on this device: random
+    # 512-byte rows of a table the size of one log-slice tile (E-step) and of
+    # one probability tile (M-step), measured before the timed region
+    gather_peak = {"estep": ctx.measure_gather_rate(inp["qvals"].shape[0] + 1),
+                   "mstep": ctx.measure_gather_rate(wl["chunk_frames"] + 1)}
 
     def barrier():
         if world > 1:
@@ -361,12 +469,28 @@ def run_ours(args, rank, world, local_rank):
         roof = {"kernel": dom + " (dense, tensor cores)", "bound": "tensor", "achieved": achieved, "peak": tpeak,
                 "unit": "TFLOP/s", "frac": achieved / tpeak, "peak_source": tsrc, "traffic": None,
                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
+    elif dom in gather_peak:
+        # the row gathers are served by L2 / L1 (the tile stays resident while
+        # its warps run): the roofline is the measured gather ceiling of the
+        # same access pattern; the DRAM side is reported beside it
+        achieved = algo[dom] / per_launch_s / 1e9
+        traffic = roofline_traffic(dom, -(-R // 128) * 128, inp["qvals"].shape[0], wl["chunk_frames"])
+        dram = traffic / per_launch_s / 1e9
+        roof = {"kernel": dom, "bound": "l2", "achieved": achieved, "peak": gather_peak[dom], "unit": "GB/s",
+                "frac": achieved / gather_peak[dom],
+                "peak_source": "measured in this run on this GPU: uniformly random 512-byte rows of a table the "
+                               "size of the kernel's tile (dfg_measure_gather_rate)",
+                "algorithmic_bytes_per_launch": algo[dom], "launch_ms": per_launch_s * 1e3,
+                "traffic": traffic,
+                "traffic_note": "modelled from ncu DRAM bytes of a small capture (compulsory streams)",
+                "dram": {"achieved": dram, "peak": peak, "frac": dram / peak, "peak_source": peak_src},
+                "gather_peaks": gather_peak,
+                "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
     else:
         achieved = algo[dom] / per_launch_s / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src,
                 "traffic": roofline_traffic(dom, -(-R // 128) * 128, inp["qvals"].shape[0], wl["chunk_frames"]),
-                "traffic_note": "modelled from ncu DRAM bytes of a small capture (compulsory streams)",
                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()}}
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -710,6 +834,9 @@ def main():
     ap.add_argument("--frames", type=int, default=0, help="override the frame count (testing)")
     ap.add_argument("--num-div", type=int, default=0, help="override num_div (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity block (GPU iteration against the oracle on a frame subset)")
+    ap.add_argument("--parity-frames", type=int, default=512, help="frames of the parity block")
     ap.add_argument("--median-photons", type=float, default=0., help="override the median photons per frame")
     ap.add_argument("--fluence-sigma", type=float, default=-1., help="override the lognormal fluence sigma")
     ap.add_argument("--estep-form", default="auto", choices=["auto", "sparse", "dense"],
@@ -774,23 +901,20 @@ def main():
                               "reference engine library oracle/_ref/libdragonfly_ref_fast.so not built"}))
             return
         inp = build_inputs(w)
-        threads = reference_threads(w)
-        for _ in range(args.warmup):
-            pass  # every reference step builds its own engine; nothing to warm
-        res = reference_throughput(w, inp, threads, budget_s=150., steps=max(2, args.steps))
-        sample = ("reference engine (dragonfly/src, -O3 -march=native, OpenMP %d threads) on %s frames at "
-                  "all %d orientations; t(n) = a + b n fitted, extrapolated to %d frames"
-                  % (threads, "/".join(str(k) for k in res["samples"]), inp["quats"].shape[0], w["n_frames"]))
-        out = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
-               "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["t_full"] * 1e3,
+        threads, nproc = reference_threads(w)
+        # the middle of the timed iterations of the GPU arm (warm-up steps
+        # first), i.e. the same iteration index and beta
+        iteration = args.warmup + 1 + args.steps // 2
+        cb = reference_engines(w, inp, threads, nproc, budget_s=110., steps=max(2, args.steps), iteration=iteration)
+        t_full = inp["quats"].shape[0] * w["n_frames"] / cb["value"]
+        out = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_full * 1e3,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                "data": "synthetic (seeded)", "impl": "reference",
                "config": {"workload": w["name"], "num_orientations": int(inp["quats"].shape[0]),
                           "num_frames": w["n_frames"], "parallelism": "host cores"},
-               "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": threads, "kind": "reference",
-                                "sample": sample, "fixed_s": res["fixed_s"], "per_frame_s": res["per_frame_s"],
-                                "frame_share": res["frame_share"]},
-               "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+               "cpu_baseline": cb,
+               "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
         return
 
@@ -803,16 +927,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.oracle import reference_available
         if reference_available(fast=True):
-            threads = reference_threads(w)
-            res = reference_throughput(w, inp, threads, budget_s=120., steps=2)
-            out["cpu_baseline"] = {
-                "value": res["value"], "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": "reference engine (dragonfly/src) on %s frames at all orientations, OpenMP %d threads; "
-                          "extrapolated to %d frames by t(n) = a + b n" % (
-                              "/".join(str(k) for k in res["samples"]), threads, w["n_frames"]),
-                "raw_sample_pairs_s": res["raw_sample_pairs_s"], "frame_share": res["frame_share"]}
+            threads, nproc = reference_threads(w)
+            out["cpu_baseline"] = reference_engines(w, inp, threads, nproc, budget_s=60., steps=2,
+                                                    iteration=args.warmup + 1 + args.steps // 2)
         else:
             out["cpu_baseline"] = None
+        if not args.no_parity:
+            out["parity"] = parity_block(w, inp, args.parity_frames, PARITY_ITERATIONS)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -114,6 +114,9 @@ _SIGS = {
     "dfg_get_frames": (C.c_int, [_V, _I, _I, _I, _I, _I]),
     "dfg_event_record": (C.c_int, [_V, C.c_int]),
     "dfg_event_elapsed": (C.c_int, [_V, C.c_int, C.c_int, _D]),
+    "dfg_measure_gather_rate": (C.c_int, [_V, C.c_longlong, C.c_int, _D]),
+    "dfg_model_rotate": (C.c_int, [_V, _D, C.c_int, C.c_int, _D, _D]),
+    "dfg_model_symmetrize": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, _D, _D]),
 }
 
 _lib = None
@@ -164,6 +167,20 @@ def _csr(lists):
     flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in lists])
                                 if len(lens) else np.zeros(0, np.int32), np.int32)
     return off, flat
+
+
+def _quat5(quat):
+    """An orientation as the five doubles the slice entry points read: a
+    quaternion (q0..q3, weight 1 appended when absent), an angle (2-D: the
+    angle, then zeros) or (phi, beta) (RZ)."""
+    q = np.ascontiguousarray(np.atleast_1d(quat), np.float64).ravel()
+    if q.size == 4:
+        q = np.append(q, 1.)
+    elif q.size in (1, 2):
+        q = np.concatenate([q, np.zeros(5 - q.size)])
+    if q.size != 5:
+        raise ValueError("an orientation is 1 (angle), 2 (phi, beta), 4 or 5 numbers, got %d" % q.size)
+    return q
 
 
 class Context:
@@ -279,6 +296,10 @@ class Context:
         qm = np.ascontiguousarray(quat_mapping, np.int32).ravel()
         t = np.ascontiguousarray(top, np.int32)
         af = np.ascontiguousarray(all_frames, np.int32).ravel()
+        if t.ndim != 2 or t.shape[0] != getattr(self, "num_data", -1):
+            raise ValueError("top must be [num_frames, K] with one row per frame of the context")
+        if qm.size != getattr(self, "num_rot", -1):
+            raise ValueError("quat_mapping must have one entry per orientation")
         self.call("dfg_set_refinement_topk", int(num_coarse), ptr(qm, C.c_int), int(t.shape[1]), ptr(t, C.c_int),
                   int(af.size), ptr(af, C.c_int) if af.size else None)
 
@@ -470,9 +491,7 @@ class Context:
 
     def slice_gen(self, quat, mode=0):
         """Slice at a quaternion (3-D), an angle (2-D) or (phi, beta) (RZ)."""
-        q = np.ascontiguousarray(np.atleast_1d(quat), np.float64)
-        if q.size == 4:
-            q = np.append(q, 1.)
+        q = _quat5(quat)
         out = np.zeros(self.num_pix)
         self.call("dfg_slice_gen", ptr(q, C.c_double), int(mode), ptr(out, C.c_double))
         return out
@@ -480,17 +499,13 @@ class Context:
     def slice_gen_noalloc(self, quat, mode=0):
         """slice_gen through the entry point that allocates no device memory
         (its scratch is a fixed device array of DFG_NOALLOC_MAX_PIXELS)."""
-        q = np.ascontiguousarray(quat, np.float64)
-        if q.size == 4:
-            q = np.append(q, 1.)
+        q = _quat5(quat)
         out = np.zeros(self.num_pix)
         self.call("dfg_slice_gen_noalloc", ptr(q, C.c_double), int(mode), ptr(out, C.c_double))
         return out
 
     def slice_merge(self, quat, view, model2, inter_weight, mode=0):
-        q = np.ascontiguousarray(np.atleast_1d(quat), np.float64)
-        if q.size == 4:
-            q = np.append(q, 1.)
+        q = _quat5(quat)
         v = np.ascontiguousarray(view, np.float64)
         self.call("dfg_slice_merge", ptr(q, C.c_double), int(mode), ptr(v, C.c_double),
                   ptr(model2, C.c_double), ptr(inter_weight, C.c_double))
@@ -535,6 +550,41 @@ class Context:
         ms = C.c_double(0.)
         self.call("dfg_event_elapsed", int(a), int(b), C.byref(ms))
         return ms.value
+
+    def model_rotate(self, model, rot, max_r=0, rotmodel=None):
+        """rotate_model on the GPU: rotmodel (zeros when None) += model
+        interpolated at rot v + c over the cube [-max_r, max_r)^3; returns
+        rotmodel."""
+        m = np.ascontiguousarray(model, np.float64)
+        if m.ndim != 3 or len(set(m.shape)) != 1:
+            raise ValueError("model must be [S, S, S]")
+        r = np.ascontiguousarray(rot, np.float64).reshape(3, 3)
+        out = np.zeros(m.shape) if rotmodel is None else rotmodel
+        if out.shape != m.shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("rotmodel must be a C-contiguous float64 array shaped like model")
+        self.call("dfg_model_rotate", ptr(r, C.c_double), m.shape[0], int(max_r), ptr(m, C.c_double),
+                  ptr(out, C.c_double))
+        return out
+
+    def model_symmetrize(self, group, model, weights, order=0):
+        """In-place point-group (group "S4" / "A5") or axial ("axial", order)
+        symmetrisation of a model and its weights [S, S, S] (float64,
+        C-contiguous)."""
+        g = {"S4": 1, "A5": 2, "axial": 3}[group]
+        for a in (model, weights):
+            if a.ndim != 3 or len(set(a.shape)) != 1 or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("model and weights must be C-contiguous float64 [S, S, S]")
+        if model.shape != weights.shape:
+            raise ValueError("model and weights differ in shape")
+        self.call("dfg_model_symmetrize", g, int(order), model.shape[0], ptr(model, C.c_double),
+                  ptr(weights, C.c_double))
+
+    def measure_gather_rate(self, rows, reps=5):
+        """GB/s of uniformly random 512-byte row reads from a device table of
+        `rows` rows: the ceiling of the E-step / M-step gather pattern."""
+        out = C.c_double(0.)
+        self.call("dfg_measure_gather_rate", int(rows), int(reps), C.byref(out))
+        return out.value
 
     def workload(self):
         out = (C.c_longlong * 11)()

@@ -5,6 +5,7 @@
 nvcc cross-compiles without a GPU; the .so is built in the package directory
 so that it travels with the source tree.
 """
+import glob
 import os
 import shutil
 import subprocess
@@ -13,8 +14,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdfgpu.so")
-SOURCES = ["emc_api.cu", "simulate.cu", "noalloc.cu", "proposal.cu"]
-HEADERS = ["emc_common.cuh", "emc_device.cuh", "emc_ctx.cuh", os.path.join("..", "..", "include", "dragonfly_b200.h")]
+SOURCES = ["emc_api.cu", "simulate.cu", "noalloc.cu", "proposal.cu", "probe.cu"]
+PUBLIC_HEADER = os.path.join(os.path.dirname(HERE), "include", "dragonfly_b200.h")
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
@@ -35,7 +36,10 @@ def _stale():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [__file__]
+    # every source and header under csrc/ (any of them may be included by a
+    # translation unit), the public header and this recipe
+    deps = glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        [PUBLIC_HEADER, __file__]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

@@ -2482,6 +2482,106 @@ extern "C" int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order) 
 	return DFG_OK;
 }
 
+// Model.rotate_model (dragonfly/model.pyx:226-254 -> rotate_model,
+// model.c:381-425): one thread per voxel v of the cube [-max_r, max_r)^3
+// around the centre adds the trilinear interpolation of m at rot v + c to
+// rotmodel[v + c], in the reference's operation order (no contraction).
+namespace dfg {
+__global__ void rotate_model_kernel(const double *__restrict__ rot, const double *__restrict__ m, int s, int max_r,
+                                    double *__restrict__ rotmodel) {
+	const long long side = 2LL * max_r, n = side * side * side;
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const int c = s / 2;
+	const int vx = (int)(i / (side * side)) - max_r, vy = (int)((i / side) % side) - max_r,
+	          vz = (int)(i % side) - max_r;
+	double rv[3];
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		rv[k] = dadd(dadd(dadd(dmul(rot[3 * k], (double)vx), dmul(rot[3 * k + 1], (double)vy)),
+		                  dmul(rot[3 * k + 2], (double)vz)), (double)c);
+	if (rv[0] < 0 || rv[0] >= s - 1 || rv[1] < 0 || rv[1] >= s - 1 || rv[2] < 0 || rv[2] >= s - 1)
+		return;
+	const int x = (int)rv[0], y = (int)rv[1], z = (int)rv[2];
+	const double fx = dsub(rv[0], (double)x), fy = dsub(rv[1], (double)y), fz = dsub(rv[2], (double)z);
+	const double cx = dsub(1., fx), cy = dsub(1., fy), cz = dsub(1., fz);
+	const long long ss = (long long)s * s, x1 = (x + 1) % s, y1 = (y + 1) % s, z1 = (z + 1) % s;
+	double v = dmul(dmul(dmul(cx, cy), cz), m[x * ss + (long long)y * s + z]);
+	v = dadd(v, dmul(dmul(dmul(cx, cy), fz), m[x * ss + (long long)y * s + z1]));
+	v = dadd(v, dmul(dmul(dmul(cx, fy), cz), m[x * ss + y1 * s + z]));
+	v = dadd(v, dmul(dmul(dmul(cx, fy), fz), m[x * ss + y1 * s + z1]));
+	v = dadd(v, dmul(dmul(dmul(fx, cy), cz), m[x1 * ss + (long long)y * s + z]));
+	v = dadd(v, dmul(dmul(dmul(fx, cy), fz), m[x1 * ss + (long long)y * s + z1]));
+	v = dadd(v, dmul(dmul(dmul(fx, fy), cz), m[x1 * ss + y1 * s + z]));
+	v = dadd(v, dmul(dmul(dmul(fx, fy), fz), m[x1 * ss + y1 * s + z1]));
+	double *o = rotmodel + (long long)(vx + c) * ss + (long long)(vy + c) * s + (vz + c);
+	*o = dadd(*o, v);
+}
+}  // namespace dfg
+
+extern "C" int dfg_model_rotate(dfg_ctx *ctx, const double *rot, int size, int max_r, const double *model,
+                                double *rotmodel) {
+	if (!ctx || !rot || !model || !rotmodel)
+		return DFG_ERR_ARG;
+	NEED(size >= 3 && size <= 2048, DFG_ERR_ARG, "model_rotate: size %d out of [3, 2048]", size);
+	if (max_r == 0)
+		max_r = size / 2;   // model.c:385-386
+	NEED(max_r > 0 && max_r <= size / 2, DFG_ERR_ARG, "model_rotate: max_r %d out of [1, size / 2]", max_r);
+	for (int k = 0; k < 9; ++k)
+		NEED(std::isfinite(rot[k]), DFG_ERR_ARG, "model_rotate: rotation entry %d is not finite", k);
+	CK(cudaSetDevice(ctx->device));
+	cudaStream_t st = ctx->stream;
+	const size_t V = (size_t)size * size * size;
+	DevBuf<double> d_rot, d_m, d_out;
+	CK(upload(d_rot, rot, 9, st));
+	CK(upload(d_m, model, V, st));
+	CK(upload(d_out, rotmodel, V, st));
+	const long long n = 8LL * max_r * max_r * max_r;
+	rotate_model_kernel<<<blocks_for(n, 256), 256, 0, st>>>(d_rot.p, d_m.p, size, max_r, d_out.p);
+	CKL("rotate_model_kernel");
+	CK(cudaMemcpyAsync(rotmodel, d_out.p, V * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	return DFG_OK;
+}
+
+extern "C" int dfg_model_symmetrize(dfg_ctx *ctx, int group, int order, int size, double *model,
+                                    double *weights) {
+	if (!ctx || !model || !weights)
+		return DFG_ERR_ARG;
+	NEED(group >= 1 && group <= 3, DFG_ERR_ARG, "model_symmetrize: group must be 1 (S4), 2 (A5) or 3 (axial)");
+	NEED(group != 3 || (order >= 1 && order <= 1024), DFG_ERR_ARG, "model_symmetrize: axial order %d", order);
+	NEED(size >= 3 && size <= 2048, DFG_ERR_ARG, "model_symmetrize: size %d out of [3, 2048]", size);
+	CK(cudaSetDevice(ctx->device));
+	cudaStream_t st = ctx->stream;
+	std::vector<double> r;
+	if (group == 1)
+		r = octahedral_rotations();
+	else if (group == 2)
+		r = icosahedral_rotations();
+	else
+		for (int i = 0; i < order; ++i) {   // symmetrize_axial, model.c:540-549
+			const double angle = 2. * M_PI * i / order, c = std::cos(angle), sn = std::sin(angle);
+			const double R[9] = {c, -sn, 0., sn, c, 0., 0., 0., 1.};
+			r.insert(r.end(), R, R + 9);
+		}
+	const long long V = (long long)size * size * size;
+	DevBuf<double> d_rot, d_m, d_w;
+	DevBuf<double2> d_acc;
+	CK(upload(d_rot, r.data(), r.size(), st));
+	CK(upload(d_m, model, (size_t)V, st));
+	CK(upload(d_w, weights, (size_t)V, st));
+	CK(d_acc.ensure((size_t)V));
+	symmetrize_kernel<<<blocks_for(V, 256), 256, 0, st>>>(d_m.p, d_w.p, size, d_rot.p, (int)(r.size() / 9), d_acc.p);
+	CKL("symmetrize_kernel");
+	symmetrize_finish_kernel<<<blocks_for(V, 256), 256, 0, st>>>(d_acc.p, V, d_m.p, d_w.p);
+	CKL("symmetrize_finish_kernel");
+	CK(cudaMemcpyAsync(model, d_m.p, (size_t)V * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaMemcpyAsync(weights, d_w.p, (size_t)V * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	return DFG_OK;
+}
+
 // Queues update_model's kernels; the squared change lands in scalars[3].
 static int update_enqueue(dfg_ctx *ctx, double alpha) {
 	cudaStream_t st = ctx->stream;

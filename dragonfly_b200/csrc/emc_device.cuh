@@ -392,6 +392,61 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
 // ---------------------------------------------------------------------------
 // (c) per-frame maximum, pruning, normalisation and frame reductions
 // ---------------------------------------------------------------------------
+// Asynchronous 16-byte global -> shared copies (cp.async, L2 only). Each
+// lane copies and later reads its own bytes, so completion of the lane's own
+// groups (cp.async.wait_group) is all the synchronisation needed; the waits
+// are hardware waits on copies already issued and always end.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Rows of a frame's log-likelihoods in flight per warp in the normalisation
+// (a ring of NORM_RING 1-KB rows in shared memory per warp).
+constexpr int NORM_RING = 6;
+
+// Streams rows 0 .. RT-1 of one lane's LW doubles (row k at src + k * stride)
+// through the lane's slots of a shared-memory ring, NORM_RING - 1 rows ahead
+// of the one being consumed, and calls f(rt, v) for each row in order.
+template <typename F>
+__device__ __forceinline__ void stream_rows(const double *__restrict__ src, size_t stride, int RT,
+                                            double *ring, int lane, F &&f) {
+	static_assert(LW % 2 == 0, "rows are copied 16 bytes at a time");
+	double *mine = ring + lane * LW;
+	auto issue = [&](int rt) {
+		const double *g = src + (size_t)rt * stride;
+		double *d = mine + (rt % NORM_RING) * TILE;
+#pragma unroll
+		for (int k = 0; k < LW; k += 2)
+			cp_async16(d + k, g + k);
+	};
+#pragma unroll
+	for (int k = 0; k < NORM_RING - 1; ++k) {
+		if (k < RT)
+			issue(k);
+		cp_async_commit();
+	}
+	for (int rt = 0; rt < RT; ++rt) {
+		if (rt + NORM_RING - 1 < RT)
+			issue(rt + NORM_RING - 1);
+		cp_async_commit();
+		cp_async_wait<NORM_RING - 1>();   // the group of row rt has landed
+		double v[LW];
+		const double *d = mine + (rt % NORM_RING) * TILE;
+#pragma unroll
+		for (int k = 0; k < LW; k += 2) {
+			const double2 x = *reinterpret_cast<const double2 *>(d + k);
+			v[k] = x.x;
+			v[k + 1] = x.y;
+		}
+		f(rt, v);
+	}
+	cp_async_wait<0>();
+}
+
 // One warp per frame. The reference visits orientations in ascending order
 // with a running maximum m (max_prob.c:184-203): a pair enters the kept list
 // when pval + 14/beta > m and, when pval > m, the list is pruned to entries
@@ -419,6 +474,9 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
     double *__restrict__ likelihood, double *__restrict__ psum_d, double *__restrict__ quat_norm,
     int *__restrict__ num_prob, double *__restrict__ Pd, uint8_t *__restrict__ tlive, int zero_dead) {
 	constexpr int UNR = LW == 1 ? 4 : 2;
+	// without tile skipping every row of the frame is read, twice: both passes
+	// stream them through a per-warp ring (stream_rows)
+	__shared__ __align__(16) double s_ring[SKIP ? 1 : 8][SKIP ? 1 : NORM_RING * TILE];
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	const size_t tstride = (size_t)Nc * TILE, pstride = (size_t)(Nc + 1) * TILE;
@@ -507,6 +565,21 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 	};
 	double s = 0.;
 	int cnt = 0;
+	if constexpr (!SKIP) {
+		stream_rows(pv, tstride, RT, s_ring[threadIdx.x >> 5], lane, [&](int rt, const double (&v)[LW]) {
+#pragma unroll
+			for (int e = 0; e < LW; ++e) {
+				const int r = rt * TILE + lane * LW + e;
+				if (r < R) {
+					bool kept = (r <= rstar) ? (v[e] > lo) : (dadd(v[e], thr) > m);
+					if (kept) {
+						s += exp(dmul(b, dsub(v[e], m)));
+						cnt++;
+					}
+				}
+			}
+		});
+	} else
 	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
 		double v[UNR][LW];
 		bool dd[UNR];
@@ -552,6 +625,46 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 #pragma unroll
 	for (int k = 0; k < (MULTI ? MAX_MODES : 1); ++k)
 		qn[k] = 0.;
+	// one kept or dropped pair of the second pass: P, the frame sums, and the
+	// stored probability (sign = PROB_MIN gate)
+	auto pair2 = [&](int r, double x, float &out, double &outd) {
+		out = 0.f;
+		outd = 0.;
+		if (r < R) {
+			bool kept = (r <= rstar) ? (x > lo) : (dadd(x, thr) > m);
+			if (kept) {
+				const double y = dmul(b, dsub(x, m));
+				const double P = exp(y) * inv_s;
+				ll += P * (x - sf);
+				if (psum_d_on)
+					pd += P * u[r] * rescale;
+				if (!(P < PROB_MIN)) {
+					inf += P * (y + cinf - logw[r]);
+					if (MULTI) {
+						int mode = r % M;
+#pragma unroll
+						for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
+							if (q == mode)
+								qn[q] += P;
+					}
+				}
+				out = (P > PROB_MIN) ? (float)P : -(float)P;
+				outd = (P > PROB_MIN) ? P : -P;
+			}
+		}
+	};
+	if constexpr (!SKIP) {
+		stream_rows(pv, tstride, RT, s_ring[threadIdx.x >> 5], lane, [&](int rt, const double (&v)[LW]) {
+			float out[LW];
+			double outd[LW];
+#pragma unroll
+			for (int e = 0; e < LW; ++e)
+				pair2(rt * TILE + lane * LW + e, v[e], out[e], outd[e]);
+			st_row(ps + rt * pstride, out);
+			if (Pd != nullptr)
+				st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, outd);
+		});
+	} else
 	for (int rt0 = 0; rt0 < RT; rt0 += UNR) {
 		double v[UNR][LW];
 		bool dd[UNR];
@@ -585,34 +698,8 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 			float out[LW];
 			double outd[LW];
 #pragma unroll
-			for (int e = 0; e < LW; ++e) {
-				const int r = rt * TILE + lane * LW + e;
-				out[e] = 0.f;
-				outd[e] = 0.;
-				if (r < R) {
-					const double x = v[k][e];
-					bool kept = (r <= rstar) ? (x > lo) : (dadd(x, thr) > m);
-					if (kept) {
-						const double y = dmul(b, dsub(x, m));
-						const double P = exp(y) * inv_s;
-						ll += P * (x - sf);
-						if (psum_d_on)
-							pd += P * u[r] * rescale;
-						if (!(P < PROB_MIN)) {
-							inf += P * (y + cinf - logw[r]);
-							if (MULTI) {
-								int mode = r % M;
-#pragma unroll
-								for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
-									if (q == mode)
-										qn[q] += P;
-							}
-						}
-						out[e] = (P > PROB_MIN) ? (float)P : -(float)P;
-						outd[e] = (P > PROB_MIN) ? P : -P;
-					}
-				}
-			}
+			for (int e = 0; e < LW; ++e)
+				pair2(rt * TILE + lane * LW + e, v[k][e], out[e], outd[e]);
 			st_row(ps + rt * pstride, out);
 			if (Pd != nullptr)
 				st_row(Pd + (size_t)dl * TILE + lane * LW + rt * pstride, outd);
@@ -874,8 +961,100 @@ __global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__r
 // the weights are a change to the cached grid: wsign[r] = +1 / -1 adds /
 // subtracts orientation r's weights (its psum_r > 0 state changed, or +1 for
 // every orientation with psum_r > 0 when no grid is cached), 0 adds none.
+// The full merge's scatter with warp aggregation: the 32 lanes of a warp hold
+// 32 consecutive pixels of one orientation (j = g + 4 k is the same for the
+// warp), and neighbouring pixels often fall in the same trilinear cell.
+// Lanes whose cells coincide (__match_any_sync on the cell index) add their
+// corner contributions in registers, in lane order, and the group's lowest
+// lane issues one atomic per corner for the group.
+template <int GEO>
+__device__ __forceinline__ void merge_aggregated(const float (*s_tile)[TILE + 1], const double *s_ps,
+                                                 const double (*s_rot)[9], const int *s_mode, int i, int g, int p,
+                                                 int P, const double *__restrict__ qvals,
+                                                 const double *__restrict__ corr, const uint8_t *__restrict__ mask,
+                                                 long long S, long long V, double *__restrict__ accum,
+                                                 int with_weight, int views_final) {
+	const int lane = threadIdx.x & 31;
+	const bool pix = p < P && mask[p] <= 1;
+	const int pp = pix ? p : 0;
+	const double qx = qvals[3 * (size_t)pp], qy = qvals[3 * (size_t)pp + 1], qz = qvals[3 * (size_t)pp + 2];
+	const double cr = corr[pp];
+	const double center = (double)(S / 2);
+	constexpr int NC = GEO == MT_3D ? 8 : 4;  // corners
+	// corner q's offset from the cell's first voxel (corner_offsets order)
+	auto off = [S](int q) -> long long {
+		if constexpr (GEO == MT_3D)
+			return (long long)(q & 1) + ((q >> 1) & 1) * S + (long long)(q >> 2) * S * S;
+		else
+			return (long long)(q & 1) + (long long)(q >> 1) * S;
+	};
+	for (int k = 0; k < TILE / 4; ++k) {
+		const int j = g + 4 * k;   // the same for every lane of the warp
+		const double ps = s_ps[j];
+		if (!(ps > 0.))
+			continue;
+		double fw[8];
+		long long base = -1;
+		bool ok = false;
+		if (pix) {
+			if constexpr (GEO == MT_3D) {
+				Cell c = locate(s_rot[j], qx, qy, qz, center, S);
+				ok = c.ok;
+				if (ok) {
+					corner_weights(c, fw);
+					base = c.i000;
+				}
+			} else {
+				Cell2 c = locate2d(s_rot[j], qx, qy, center, S);
+				ok = c.ok;
+				if (ok) {
+					corner_weights2(c, fw);
+					base = c.i00;
+				}
+			}
+		}
+		if (!__any_sync(FULL, ok))
+			continue;
+		if (!ok) {
+#pragma unroll
+			for (int q = 0; q < NC; ++q)
+				fw[q] = 0.;
+			base = -1 - lane;    // a group of its own
+		}
+		const double wv = views_final ? (double)s_tile[i][j] / cr : ((double)s_tile[i][j] / ps) / cr;
+		const unsigned grp = __match_any_sync(FULL, base);
+		const int members = __popc(grp);
+		const int most = (int)__reduce_max_sync(FULL, (unsigned)members);
+		const bool lead = ok && (__ffs(grp) - 1) == lane;
+		double *a = accum + 2 * ((size_t)s_mode[j] * V + (ok ? base : 0));
+		// model sums (slot 0), then with_weight the weights (slot 1): the
+		// group's lanes in lane order, summed by the lowest lane
+		for (int h = 0; h < (with_weight ? 2 : 1); ++h) {
+			double v[8];
+#pragma unroll
+			for (int q = 0; q < NC; ++q)
+				v[q] = h == 0 ? fw[q] * wv : fw[q];
+			for (int m = 1; m < most; ++m) {
+				// the group's m-th lane, or this lane when the group is smaller
+				const int src = m < members ? (int)__fns(grp, 0, m + 1) : lane;
+#pragma unroll
+				for (int q = 0; q < NC; ++q) {
+					const double x = __shfl_sync(FULL, h == 0 ? fw[q] * wv : fw[q], src);
+					if (m < members)
+						v[q] += x;
+				}
+			}
+			if (lead) {
+#pragma unroll
+				for (int q = 0; q < NC; ++q)
+					atomicAdd(a + 2 * off(q) + h, v[q]);
+			}
+		}
+	}
+}
+
 template <int GEO, bool INCR = false>
-__global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
+__global__ void __launch_bounds__(256, 3) merge_kernel(const float *__restrict__ T,
                                                      const double *__restrict__ psum_r,
                                                      const double *__restrict__ quats, int M, int R,
                                                      const double *__restrict__ qvals,
@@ -919,6 +1098,11 @@ __global__ void __launch_bounds__(256) merge_kernel(const float *__restrict__ T,
 	}
 	__syncthreads();
 	const int i = t & (PB - 1), g = t >> 6, p = p0 + i;
+	if constexpr (!INCR) {
+		merge_aggregated<GEO>(s_tile, s_ps, s_rot, s_mode, i, g, p, P, qvals, corr, mask, S, V, accum,
+		                      with_weight, views_final);
+		return;
+	}
 	if (p >= P || mask[p] > 1)
 		return;
 	const double qx = qvals[3 * (size_t)p], qy = qvals[3 * (size_t)p + 1], qz = qvals[3 * (size_t)p + 2];

@@ -12,7 +12,10 @@
 // In host code the array's name only stands for it; its device address comes
 // from cudaGetSymbolAddress, looked up once per device with that device
 // current, on the first call on that device (make that first call before any
-// stream capture). All calls share the array: calls that overlap on the GPU
+// stream capture), and kept for the life of the process: the entry point must
+// not be used across a cudaDeviceReset (or another teardown of the device's
+// primary context) in the host process, after which the kept address would
+// point into freed memory. All calls share the array: calls that overlap on the GPU
 // (other threads, other contexts on the same device) race and must be
 // serialised by the caller. Every call writes the quaternion slots and all
 // num_pix output slots before reading them, so nothing has to be cleared.

@@ -5,7 +5,9 @@ model1 is the current intensity [num_modes, size, size, size] (MODEL_3D) or
 size // 2); model2 / inter_weight hold the last iteration's merged model and
 interpolation weights. slice_gen / slice_merge run on the GPU through the C
 ABI (dfg_slice_gen / dfg_slice_merge); the orientation is a quaternion (3-D),
-an angle (2-D) or (phi, beta) (RZ, which uses the detector's detd).
+an angle (2-D) or (phi, beta) (RZ, which uses the detector's detd). The
+volume operations rotate_model and symmetrize_octahedral / icosahedral /
+axial run on the GPU too (dfg_model_rotate, dfg_model_symmetrize).
 """
 import os
 
@@ -26,12 +28,7 @@ _TYPE_CODES = {"MODEL_3D": 0, "MODEL_2D": 1, "MODEL_RZ": 2}
 def _slice_context(det, model):
     """A shared GPU context holding det and this Model's model1, for
     one-slice calls."""
-    global _slice_ctx
-    from ._lib import Context
-    if _slice_ctx is None:
-        _slice_ctx = Context(int(os.environ.get("LOCAL_RANK", "0")))
-        _slice_ctx._det_id = None
-    c = _slice_ctx
+    c = _device_context()
     key = (id(det.qvals), id(det.corr), id(det.raw_mask))
     if c._det_id != key:
         c.set_detector(det.qvals, det.corr, det.raw_mask)
@@ -40,6 +37,17 @@ def _slice_context(det, model):
     c.set_detector_distance(getattr(det, "detd", 0.))
     c.set_model(model.model1)
     return c
+
+
+def _device_context():
+    """The shared GPU context of the one-slice calls, for the volume
+    operations that need no detector (rotation, symmetrisation)."""
+    global _slice_ctx
+    from ._lib import Context
+    if _slice_ctx is None:
+        _slice_ctx = Context(int(os.environ.get("LOCAL_RANK", "0")))
+        _slice_ctx._det_id = None
+    return _slice_ctx
 
 
 class Model:
@@ -204,10 +212,26 @@ class Model:
             m[ym, c] = a
 
     @staticmethod
-    def _unsupported(*args, **kwargs):
-        raise NotImplementedError("point-group / axial symmetrisation and model rotation are not supported")
+    def symmetrize_octahedral(model, weights):
+        """In-place octahedral (S4, 48 rotations) symmetrisation of a volume
+        and its weights on the GPU (model.pyx:175-184 -> model.c:695-729)."""
+        _device_context().model_symmetrize("S4", model, weights)
 
-    symmetrize_octahedral = _unsupported
-    symmetrize_icosahedral = _unsupported
-    symmetrize_axial = _unsupported
-    rotate_model = _unsupported
+    @staticmethod
+    def symmetrize_icosahedral(model, weights):
+        """In-place icosahedral (A5, 60 rotations) symmetrisation on the GPU
+        (model.pyx:186-195 -> model.c:731-757)."""
+        _device_context().model_symmetrize("A5", model, weights)
+
+    @staticmethod
+    def symmetrize_axial(model, weights, order):
+        """In-place order-fold symmetrisation about z on the GPU
+        (model.pyx:197-207 -> model.c:527-571)."""
+        _device_context().model_symmetrize("axial", model, weights, order=int(order))
+
+    @staticmethod
+    def rotate_model(model, rot, max_r=0, rotmodel=None):
+        """Rotated copy of a volume on the GPU (model.pyx:226-254 ->
+        model.c:381-425): rotmodel (zeros when None) += model interpolated at
+        rot v + c for v in [-max_r, max_r)^3 (max_r 0: size // 2)."""
+        return _device_context().model_rotate(model, rot, max_r, rotmodel)

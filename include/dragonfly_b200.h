@@ -225,6 +225,21 @@ DFG_API int dfg_slice_gen(dfg_ctx *ctx, const double *quat, int mode, double *ou
 DFG_API int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const double *view,
                     double *model2, double *inter_weight);
 
+/* Model.rotate_model (dragonfly/model.pyx:226-254 -> rotate_model,
+ * model.c:381-425) on host arrays: for every voxel v of the cube
+ * [-max_r, max_r)^3 around the centre, rotmodel[v + c] += the trilinear
+ * interpolation of model at rot v + c (rot row-major 3x3; max_r 0 means
+ * size / 2; voxels whose rotated position leaves the model get nothing).
+ * model and rotmodel are [size][size][size]; rotmodel is read and updated. */
+DFG_API int dfg_model_rotate(dfg_ctx *ctx, const double *rot, int size, int max_r, const double *model,
+                             double *rotmodel);
+/* Model.symmetrize_octahedral / symmetrize_icosahedral / symmetrize_axial
+ * (dragonfly/model.pyx:175-210 -> model.c:527-757) on host arrays, in place:
+ * weights <- sum over the group of the rotated weights, model <- (sum of the
+ * rotated model x weights) / that sum where it is positive, else 0. group 1 =
+ * S4 (48 rotations), 2 = A5 (60), 3 = the order-fold axial group about z. */
+DFG_API int dfg_model_symmetrize(dfg_ctx *ctx, int group, int order, int size, double *model, double *weights);
+
 /* dfg_slice_gen without any device allocation. No counterpart in the
  * reference: it is for callers that cannot allocate device memory while they
  * run -- an application whose own pool allocator owns the device memory
@@ -233,8 +248,12 @@ DFG_API int dfg_slice_merge(dfg_ctx *ctx, const double *quat, int mode, const do
  * device array of DFG_NOALLOC_MAX_PIXELS doubles (2 MiB plus 64 bytes) that
  * each GPU loading the library holds until exit; detectors with more pixels
  * are rejected with DFG_ERR_ARG. The first call on a device looks the array's
- * address up (make it before any stream capture). All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * address up (make it before any stream capture) and keeps it for the life of
+ * the process: do not use this entry point across a cudaDeviceReset (or any
+ * other teardown of the device's primary context) in the host process, since
+ * the kept address would then point into freed memory. All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
 #define DFG_NOALLOC_MAX_PIXELS 262144
 DFG_API int dfg_slice_gen_noalloc(dfg_ctx *ctx, const double *quat, int mode, double *out);
 
@@ -403,6 +422,15 @@ DFG_API int dfg_reset_phase_times(dfg_ctx *ctx);
  * (tile, frame) pairs of the pair lists (0 without them), out[10] =
  * orientation tiles per block of the pair lists. out must hold 11 values. */
 DFG_API int dfg_get_workload(dfg_ctx *ctx, long long *out);
+
+/* Ceiling of the gather kernels' access pattern on the context's device. No
+ * counterpart in the reference (a measurement helper): reads uniformly random
+ * 512-byte rows (one 16-byte load per lane, eight rows in flight per lane, all
+ * SMs at full occupancy) of a device table of `rows` rows, the shape of the
+ * E-step's log-slice tile [P + 1][128] FP32 or the M-step's probability tile;
+ * writes the best of `reps` timed launches (after one warm-up launch) in GB/s
+ * of row bytes. Allocates the table for the call and frees it. */
+DFG_API int dfg_measure_gather_rate(dfg_ctx *ctx, long long rows, int reps, double *gbs);
 
 #ifdef __cplusplus
 }

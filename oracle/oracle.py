@@ -26,6 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libdragonfly_ref.so")
 LIB_REF_FAST = os.path.join(HERE, "_ref", "libdragonfly_ref_fast.so")
+LIB_LEGACY_FAST = os.path.join(HERE, "_ref", "libdragonfly_legacy_fast.so")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -46,6 +47,10 @@ def _load(path):
 
 def reference_available(fast=False):
     return os.path.exists(LIB_REF_FAST if fast else LIB_REF)
+
+
+def legacy_available():
+    return os.path.exists(LIB_LEGACY_FAST)
 
 
 def _c(a, dt):
@@ -297,6 +302,63 @@ class ReferenceEngine:
         res["rms_change"] = rms
         res["model1"] = self.model1()
         return res
+
+
+class LegacyEngine:
+    """The reference's legacy engine (src/max_emc.c, the `emc` binary's
+    maximize) driven through legacy_driver.c: one iteration of
+    src/recon_emc.c:102-131 per run_iteration (update_beta, maximize,
+    divide-then-Friedel update_model, normalize_scale). It keeps its state in
+    the library's globals, so only one LegacyEngine exists at a time. Used as
+    a timed CPU baseline; OpenMP threads from OMP_NUM_THREADS / num_threads."""
+
+    _live = None
+
+    def __init__(self, prob, num_threads=None):
+        if LegacyEngine._live is not None:
+            raise RuntimeError("one LegacyEngine at a time (the legacy engine keeps global state)")
+        self.lib = L = _load(LIB_LEGACY_FAST)
+        L.leg_create.restype = C.c_int
+        L.leg_create.argtypes = [C.c_int, _dp, _dp, _up, C.c_int, _ip, _ip, _ip, _ip, _ip, C.c_int, _dp, C.c_long,
+                                 _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]
+        L.leg_run_iteration.restype = C.c_double
+        L.leg_run_iteration.argtypes = [C.c_int]
+        L.leg_get_model1.argtypes = [_dp]
+        L.leg_set_scale.argtypes = [_dp]
+        p = self.prob = prob
+        if p.num_modes != 1 or p.model_type != "3d" or p.blacklist is not None:
+            raise ValueError("the legacy driver takes one 3-D mode and no blacklist")
+        if num_threads:
+            omp = C.CDLL(L._name)
+            try:
+                omp.omp_set_num_threads(int(num_threads))
+            except AttributeError:
+                pass
+        rc = L.leg_create(p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, p.num_data, p.ones, p.multi,
+                          p.place_ones, p.place_multi, p.count_multi, p.num_rot, p.quats.reshape(-1), p.size,
+                          p.model1.reshape(-1), p.need_scaling, p.update_scale, p.beta, p.beta_jump,
+                          p.beta_period)
+        if rc != 0:
+            raise RuntimeError("leg_create failed")
+        if p.scale is not None:
+            L.leg_set_scale(p.scale)
+        LegacyEngine._live = self
+
+    def run_iteration(self, iteration):
+        return self.lib.leg_run_iteration(int(iteration))
+
+    def model1(self):
+        out = np.zeros(self.prob.model1.shape)
+        self.lib.leg_get_model1(out.reshape(-1))
+        return out
+
+    def close(self):
+        if LegacyEngine._live is self:
+            self.lib.leg_destroy()
+            LegacyEngine._live = None
+
+    def __del__(self):
+        self.close()
 
 
 class OracleEngine:

@@ -8,7 +8,7 @@ import bench
 
 
 def _fake(a, b, calls):
-    def step(w, inp, n, seed, threads):
+    def step(w, inp, n, seed, threads, **kw):
         calls.append(n)
         return a + b * n
     return step

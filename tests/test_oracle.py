@@ -150,3 +150,33 @@ def test_oracle_results_do_not_depend_on_its_thread_count(oracle_built):
                            text=True, check=True)
         out.append(r.stdout.strip().splitlines()[-1])
     assert out[0] == out[1]
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference sources not compiled here")
+def test_legacy_engine_driver_agrees_with_packaged_engine(oracle_built):
+    """The legacy engine (src/max_emc.c through legacy_driver.c, the second
+    timed CPU baseline) computes the same E-step as the packaged engine when
+    every mask-0 pixel lies inside a positive model: the same average
+    log-likelihood in the first iteration; the model differs only by the
+    legacy update order (divide, then Friedel average: src/recon_emc.c:137-149
+    against recon.pyx:120-140)."""
+    from dragonfly_b200 import synth
+    from oracle.oracle import LegacyEngine, legacy_available
+    if not legacy_available():
+        pytest.skip("legacy engine library not built")
+    d = synth.small_problem(seed=17, det_side=28, size=33, qmax=15., n_atoms=80, atom_radius=6.,
+                            num_div=2, n_frames=160, mean_count=40.)
+    p = EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"],
+                   d["place_multi"], d["count_multi"], d["quats"], d["model_start"], beta=0.3, need_scaling=1,
+                   update_scale=1)
+    ref = ReferenceEngine(p, num_threads=1)
+    leg = LegacyEngine(p)
+    try:
+        a = ref.run_iteration(1)
+        b = leg.run_iteration(1)
+        assert abs(a["avg_likelihood"] - b) <= 1e-10 * abs(b), (a["avg_likelihood"], b)
+        m = leg.model1()
+        assert np.linalg.norm(m - a["model1"]) <= 0.05 * np.linalg.norm(a["model1"])
+    finally:
+        leg.close()
+        ref.close()

@@ -78,3 +78,65 @@ def test_gpu_symmetrised_update_matches_reference(oracle_built, point_group, axi
         assert dev <= 1e-5 and ll <= 1e-6, (dev, ll)
     gpu.close()
     ref.close()
+
+
+def _ref_lib():
+    import ctypes as C
+    from oracle.oracle import LIB_REF
+    lib = C.CDLL(LIB_REF)
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    lib.rotate_model.argtypes = [dp, dp, C.c_int, C.c_int, dp]
+    for n in ("symmetrize_octahedral", "symmetrize_icosahedral"):
+        getattr(lib, n).argtypes = [dp, dp, C.c_int]
+    lib.symmetrize_axial.argtypes = [dp, dp, C.c_int, C.c_int]
+    return lib
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size,max_r", [(33, 0), (34, 10), (21, 3)])
+def test_gpu_rotate_model_matches_reference(oracle_built, size, max_r):
+    """Model.rotate_model on the GPU (dfg_model_rotate) equals the reference's
+    rotate_model (model.c:381-425) bit for bit, added into a given array."""
+    if not reference_available():
+        pytest.skip("reference engine library not built")
+    from dragonfly_b200.model import Model
+    rng = np.random.default_rng(size + max_r)
+    m = rng.random((size,) * 3)
+    q = rng.normal(size=4)
+    rot = np.ascontiguousarray(Model.make_rot_quat(q / np.linalg.norm(q)), np.float64)
+    start = rng.random((size,) * 3)
+    ref = start.copy()
+    _ref_lib().rotate_model(rot, m, size, max_r, ref)
+    out = Model.rotate_model(m, rot, max_r, start.copy())
+    np.testing.assert_array_equal(out, ref)
+    fresh = Model.rotate_model(m, rot, max_r)
+    np.testing.assert_array_equal(fresh, ref - start)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("group", ["octahedral", "icosahedral", "axial"])
+def test_gpu_model_symmetrize_matches_reference(oracle_built, group):
+    """Model.symmetrize_* on the GPU (dfg_model_symmetrize) against the
+    reference's symmetrize_octahedral / icosahedral / axial (model.c:527-757)
+    on the same un-normalised volume and weights. The groups' rotations are
+    summed in another order (and A5's are exact where the reference's table
+    has 11 decimals), so the bound is relative, not bitwise."""
+    if not reference_available():
+        pytest.skip("reference engine library not built")
+    from dragonfly_b200.model import Model
+    rng = np.random.default_rng(7)
+    size = 31
+    m = rng.random((size,) * 3)
+    w = rng.random((size,) * 3) + 0.1
+    a, wa, b, wb = m.copy(), w.copy(), m.copy(), w.copy()
+    lib = _ref_lib()
+    if group == "axial":
+        lib.symmetrize_axial(a, wa, size, 5)
+        Model.symmetrize_axial(b, wb, 5)
+    else:
+        getattr(lib, "symmetrize_" + group)(a, wa, size)
+        getattr(Model, "symmetrize_" + group)(b, wb)
+    tol = 1e-9 if group == "icosahedral" else 1e-13
+    assert rel_l2(wb, wa) <= tol and rel_l2(b, a) <= tol, (rel_l2(wb, wa), rel_l2(b, a))
+    if group != "icosahedral":
+        assert np.all((wa > 0) == (wb > 0))
