@@ -89,6 +89,7 @@ _SIGS = {
     "dfg_pnet_train": (C.c_int, [_V, _I, C.c_int, C.c_double, C.c_ulonglong, _D]),
     "dfg_pnet_topk": (C.c_int, [_V, C.c_int, _I]),
     "dfg_pnet_set_tensor_cores": (C.c_int, [_V, C.c_int]),
+    "dfg_pnet_set_option": (C.c_int, [_V, C.c_char_p, C.c_double]),
     "dfg_pnet_set_targets": (C.c_int, [_V, C.POINTER(C.c_longlong), _I, C.POINTER(C.c_float)]),
     "dfg_pnet_logits": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "dfg_pnet_gradients": (C.c_int, [_V, _I, C.POINTER(C.c_float), _D]),
@@ -724,6 +725,9 @@ class ProposalNet:
         loss = C.c_double(0.)
         self._call("dfg_pnet_train", ptr(lab, C.c_int), int(epochs), float(lr), int(seed), C.byref(loss))
         return loss.value
+
+    def set_option(self, key, value):
+        self._call("dfg_pnet_set_option", key.encode(), float(value))
 
     def set_tensor_cores(self, on):
         """Inference products on the tcgen05 tensor cores (default) or the

@@ -1370,7 +1370,7 @@ static int launch_mstep(dfg_ctx *ctx, const Chunk &ch, bool dense) {
 		const int n_tiles = ctx->K_pad / DN + (ctx->K_pad % DN ? 1 : 0);
 		mstep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
 		    ctx->map_phi, ctx->map_plo, ctx->map_cnt_m, (Nc + DK - 1) / DK, rows, RT, n_tiles, ctx->kpix.p, ctx->K,
-		    P, ctx->T.p, ctx->derr.p);
+		    P, ctx->T.p, ctx->derr.p, ctx->dense_wait_cycles, ctx->dense_withhold);
 		CKL("mstep_dense_kernel");
 		return DFG_OK;
 	}
@@ -1395,7 +1395,7 @@ static int launch_estep(dfg_ctx *ctx, const Chunk &ch, int use_scale, bool bg, c
 		estep_dense_kernel<<<RT * n_tiles, 192, DSMEM_BYTES, st>>>(
 		    ctx->map_hi, ctx->map_lo, ctx->map_cnt, ctx->K_pad / DK, RT, n_tiles, ctx->u.p, ctx->logw.p, R,
 		    ctx->scale.p, ch.d0, Nc, use_scale, ctx->scalars.p, ctx->pval.p, ctx->tmax.p, ctx->targ.p,
-		    ctx->derr.p);
+		    ctx->derr.p, ctx->dense_wait_cycles, ctx->dense_withhold);
 		CKL("estep_dense_kernel");
 		return DFG_OK;
 	}
@@ -3280,6 +3280,16 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 	}
 	if (!strcmp(key, "tile_skip")) {
 		ctx->mstep_skip = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "dense_wait_cycles")) {
+		NEED(value >= 1e4 && value <= 1e11, DFG_ERR_ARG, "dense_wait_cycles must be in [1e4, 1e11]");
+		ctx->dense_wait_cycles = (long long)value;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "dense_withhold_stage")) {
+		NEED(value >= -1 && value < 1e6, DFG_ERR_ARG, "dense_withhold_stage must be -1 or a stage index");
+		ctx->dense_withhold = (int)value;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "mstep_form")) {

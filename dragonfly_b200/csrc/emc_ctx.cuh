@@ -216,6 +216,11 @@ struct dfg_ctx {
 	int K = 0, K_pad = 0, dense_P = -1, cnt_rows = 0;
 	int max_count0 = -1;  // largest count on a mask < 2 pixel; -1 = not known
 	DevBuf<int> kpix, pcol, derr;
+	// failure-detection test hooks of the dense kernels: the clock cycles
+	// after which a pipeline wait gives up, and a stage whose copies are never
+	// issued (-1: none)
+	long long dense_wait_cycles = 2000000000LL;  // about one second, as TC_WAIT_CYCLES
+	int dense_withhold = -1;
 	DevBuf<uint16_t> Ahi, Alo, cnt, Phi, Plo;
 	// counts read by the E-step (256-frame boxes) and the M-step (64-frame boxes)
 	CUtensorMap map_hi, map_lo, map_cnt, map_phi, map_plo, map_cnt_m;

@@ -17,8 +17,10 @@
 //              column = frame), pval = log w_r - u_r s_d + S (FP64) stored in
 //              the sparse form's layout, and the tile maximum with its lowest
 //              orientation index.
-// Every wait on an mbarrier gives up after about a second of clock cycles,
-// sets the error flag and lets the CTA free its TMEM and exit.
+// Every wait on an mbarrier gives up after wait_cycles clock cycles (about a
+// second unless a test shortens it), sets the error flag and lets the CTA
+// free its TMEM and exit. withhold_kb >= 0 is a test hook that never issues
+// that stage's copies, so the waits on it run out (-1 in production).
 #pragma once
 
 #include <cuda.h>
@@ -62,7 +64,7 @@ __global__ void __launch_bounds__(192, 1) estep_dense_kernel(
     const __grid_constant__ CUtensorMap map_cnt, int num_kb, int RT, int n_tiles, const double *__restrict__ u,
     const double *__restrict__ logw, int R, const double *__restrict__ scale, int d0, int Nc, int use_scale,
     const double *__restrict__ scalars, double *__restrict__ pval, double *__restrict__ tmax,
-    int *__restrict__ targ, int *__restrict__ err) {
+    int *__restrict__ targ, int *__restrict__ err, long long wait_cycles, int withhold_kb) {
 	extern __shared__ uint8_t dsm_raw[];
 	uint8_t *sm = (uint8_t *)(((uintptr_t)dsm_raw + 1023) & ~(uintptr_t)1023);
 	double *s_max = (double *)(sm + DSTAGES * DSTAGE_BYTES);
@@ -106,11 +108,13 @@ __global__ void __launch_bounds__(192, 1) estep_dense_kernel(
 			for (int kb = 0; kb < num_kb; ++kb) {
 				const int s = kb % DSTAGES;
 				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
-				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u)) {
+				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u, wait_cycles)) {
 					*abort_flag = 1;
 					atomicExch(err, 1);
 					break;
 				}
+				if (kb == withhold_kb)  // test hook: this stage's copies are never issued
+					continue;
 				uint8_t *st = sm + s * DSTAGE_BYTES;
 				mbar_expect_tx(&full[s], DSTAGE_BYTES);
 				tma_load_2d(st, &map_hi, &full[s], kb * DK, rt * 128);
@@ -121,7 +125,7 @@ __global__ void __launch_bounds__(192, 1) estep_dense_kernel(
 			// on a give-up, let the copies still in flight land before exiting
 			if (*abort_flag)
 				for (int kb = max(0, issued - DSTAGES); kb < issued; ++kb)
-					mbar_wait(&full[kb % DSTAGES], (uint32_t)(kb / DSTAGES) & 1u);
+					mbar_wait(&full[kb % DSTAGES], (uint32_t)(kb / DSTAGES) & 1u, wait_cycles);
 		}
 		__syncwarp();
 	} else if (warp == 1) {
@@ -129,7 +133,7 @@ __global__ void __launch_bounds__(192, 1) estep_dense_kernel(
 			for (int kb = 0; kb < num_kb; ++kb) {
 				const int s = kb % DSTAGES;
 				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
-				if (*abort_flag || !mbar_wait(&full[s], ph)) {
+				if (*abort_flag || !mbar_wait(&full[s], ph, wait_cycles)) {
 					*abort_flag = 1;
 					atomicExch(err, 1);
 					break;
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(192, 1) estep_dense_kernel(
 		const int q = warp & 3, i = q * 32 + lane, r = rt * 128 + i;
 		const bool valid_r = r < R;
 		const double lw = valid_r ? logw[r] : 0., ur = valid_r ? u[r] : 0.;
-		const bool ok = mbar_wait(accum, 0);
+		const bool ok = mbar_wait(accum, 0, wait_cycles);
 		if (!ok) {
 			*abort_flag = 1;
 			atomicExch(err, 1);
@@ -254,7 +258,8 @@ __device__ __forceinline__ void umma_bf16_mn(uint32_t tmem_d, uint64_t adesc, ui
 __global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
     const __grid_constant__ CUtensorMap map_phi, const __grid_constant__ CUtensorMap map_plo,
     const __grid_constant__ CUtensorMap map_cnt, int num_kb, int Nc_pad, int RT, int n_tiles,
-    const int *__restrict__ kpix, int K, int P, float *__restrict__ T, int *__restrict__ err) {
+    const int *__restrict__ kpix, int K, int P, float *__restrict__ T, int *__restrict__ err, long long wait_cycles,
+    int withhold_kb) {
 	extern __shared__ uint8_t dsm_raw[];
 	uint8_t *sm = (uint8_t *)(((uintptr_t)dsm_raw + 1023) & ~(uintptr_t)1023);
 	uint64_t *bars = (uint64_t *)(sm + DSTAGES * DSTAGE_BYTES + DEPI_BYTES);
@@ -295,11 +300,13 @@ __global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
 			for (int kb = 0; kb < num_kb; ++kb) {
 				const int s = kb % DSTAGES;
 				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
-				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u)) {
+				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u, wait_cycles)) {
 					*abort_flag = 1;
 					atomicExch(err, 1);
 					break;
 				}
+				if (kb == withhold_kb)  // test hook: this stage's copies are never issued
+					continue;
 				uint8_t *st = sm + s * DSTAGE_BYTES;
 				const int fy = rt * Nc_pad + kb * DK;  // probability rows of this frame block
 				mbar_expect_tx(&full[s], DSTAGE_BYTES);
@@ -314,7 +321,7 @@ __global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
 			}
 			if (*abort_flag)
 				for (int kb = max(0, issued - DSTAGES); kb < issued; ++kb)
-					mbar_wait(&full[kb % DSTAGES], (uint32_t)(kb / DSTAGES) & 1u);
+					mbar_wait(&full[kb % DSTAGES], (uint32_t)(kb / DSTAGES) & 1u, wait_cycles);
 		}
 		__syncwarp();
 	} else if (warp == 1) {
@@ -322,7 +329,7 @@ __global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
 			for (int kb = 0; kb < num_kb; ++kb) {
 				const int s = kb % DSTAGES;
 				const uint32_t ph = (uint32_t)(kb / DSTAGES) & 1u;
-				if (*abort_flag || !mbar_wait(&full[s], ph)) {
+				if (*abort_flag || !mbar_wait(&full[s], ph, wait_cycles)) {
 					*abort_flag = 1;
 					atomicExch(err, 1);
 					break;
@@ -343,7 +350,7 @@ __global__ void __launch_bounds__(192, 1) mstep_dense_kernel(
 		__syncwarp();
 	} else {
 		const int q = warp & 3, i = q * 32 + lane;
-		const bool ok = mbar_wait(accum, 0);
+		const bool ok = mbar_wait(accum, 0, wait_cycles);
 		if (!ok) {
 			*abort_flag = 1;
 			atomicExch(err, 1);

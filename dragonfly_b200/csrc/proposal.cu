@@ -409,13 +409,16 @@ struct GemmCfg {
 // zero), accumulated in FP32 in TMEM. One CTA per 128 x BN tile: warp 0
 // issues the TMA loads (GSTAGES-deep ring), warp 1 the MMAs (and owns the
 // TMEM allocation), warps 2-5 read their 32 TMEM lanes, add the bias, apply
-// the ReLU and store FP32 rows. Every wait gives up after about a second,
-// sets *err and lets the CTA free its TMEM and exit.
+// the ReLU and store FP32 rows. Every wait gives up after wait_cycles clock
+// cycles (about a second unless a test shortens it), sets *err and lets the
+// CTA free its TMEM and exit; withhold_kb >= 0 is a test hook that never
+// issues that stage's copies (-1 in production).
 template <int BN>
 __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a,
                                                               const __grid_constant__ CUtensorMap map_b, int num_kb,
                                                               int M, int N, const float *__restrict__ bias, int relu,
-                                                              float *__restrict__ C, int ldc, int *__restrict__ err) {
+                                                              float *__restrict__ C, int ldc, int *__restrict__ err,
+                                                              long long wait_cycles, int withhold_kb) {
 	using G = GemmCfg<BN>;
 	extern __shared__ uint8_t gsm_raw[];
 	uint8_t *sm = (uint8_t *)(((uintptr_t)gsm_raw + 1023) & ~(uintptr_t)1023);
@@ -450,11 +453,13 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 			for (int kb = 0; kb < num_kb; ++kb) {
 				const int s = kb % GSTAGES;
 				const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
-				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u)) {
+				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u, wait_cycles)) {
 					*abort_flag = 1;
 					atomicExch(err, 1);
 					break;
 				}
+				if (kb == withhold_kb)  // test hook: this stage's copies are never issued
+					continue;
 				uint8_t *st = sm + s * G::STAGE;
 				mbar_expect_tx(&full[s], G::STAGE);
 				tma_load_2d(st, &map_a, &full[s], kb * GK, mt * 128);
@@ -464,7 +469,7 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 			// on a give-up, let the copies still in flight land before exiting
 			if (*abort_flag)
 				for (int kb = max(0, issued - GSTAGES); kb < issued; ++kb)
-					mbar_wait(&full[kb % GSTAGES], (uint32_t)(kb / GSTAGES) & 1u);
+					mbar_wait(&full[kb % GSTAGES], (uint32_t)(kb / GSTAGES) & 1u, wait_cycles);
 		}
 		__syncwarp();
 	} else if (warp == 1) {
@@ -472,7 +477,7 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 			for (int kb = 0; kb < num_kb; ++kb) {
 				const int s = kb % GSTAGES;
 				const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
-				if (*abort_flag || !mbar_wait(&full[s], ph)) {
+				if (*abort_flag || !mbar_wait(&full[s], ph, wait_cycles)) {
 					*abort_flag = 1;
 					atomicExch(err, 1);
 					break;
@@ -490,7 +495,7 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 	} else {
 		// warp w reads TMEM lanes 32 (w % 4) .. + 31
 		const int q = warp & 3, row = mt * 128 + q * 32 + lane;
-		const bool ok = mbar_wait(accum, 0);
+		const bool ok = mbar_wait(accum, 0, wait_cycles);
 		if (!ok) {
 			*abort_flag = 1;
 			atomicExch(err, 1);
@@ -653,6 +658,10 @@ struct dfg_pnet {
 	bool use_tc = true;
 	DevBuf<__nv_bfloat16> colsb, wbp[NL];
 	DevBuf<int> terr;
+	// failure-detection test hooks of the tensor-core products (as the
+	// context's dense_wait_cycles / dense_withhold_stage options)
+	long long wait_cycles = 2000000000LL;
+	int withhold = -1;
 	// soft targets of the loaded images (dfg_pnet_set_targets)
 	DevBuf<long long> t_off;
 	DevBuf<int> t_cls, iota;
@@ -796,7 +805,8 @@ static int launch_tc_gemm(dfg_pnet *net, const CUtensorMap &ma, const CUtensorMa
                           const float *bias, int relu, float *C) {
 	dim3 grid((M + 127) / 128, (N + BN - 1) / BN);
 	pnet_gemm_tc_kernel<BN><<<grid, 192, GemmCfg<BN>::SMEM, net->stream>>>(ma, mb, num_kb, M, N, bias, relu, C, N,
-	                                                                     net->terr.p);
+	                                                                     net->terr.p, net->wait_cycles,
+	                                                                     net->withhold);
 	PKL("pnet_gemm_tc_kernel");
 	return DFG_OK;
 }
@@ -1049,6 +1059,26 @@ extern "C" int dfg_pnet_set_tensor_cores(dfg_pnet *net, int on) {
 		return DFG_ERR_ARG;
 	net->use_tc = on != 0;
 	return DFG_OK;
+}
+
+extern "C" int dfg_pnet_set_option(dfg_pnet *net, const char *key, double value) {
+	if (!net || !key)
+		return DFG_ERR_ARG;
+	if (!strcmp(key, "tensor_cores"))
+		return dfg_pnet_set_tensor_cores(net, value != 0.);
+	if (!strcmp(key, "wait_cycles")) {
+		if (!(value >= 1e4 && value <= 1e11))
+			return net->fail(DFG_ERR_ARG, "wait_cycles must be in [1e4, 1e11]");
+		net->wait_cycles = (long long)value;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "withhold_stage")) {
+		if (!(value >= -1 && value < 1e6))
+			return net->fail(DFG_ERR_ARG, "withhold_stage must be -1 or a stage index");
+		net->withhold = (int)value;
+		return DFG_OK;
+	}
+	return net->fail(DFG_ERR_ARG, "unknown option %s", key);
 }
 
 extern "C" long long dfg_pnet_num_params(const dfg_pnet *net) {

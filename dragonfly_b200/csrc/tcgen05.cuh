@@ -24,9 +24,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 	             : "memory");
 }
 
-// Waits for the phase of the given parity to complete; false after about a
-// second (the caller then gives up).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Waits for the phase of the given parity to complete; false after `limit`
+// clock cycles (about a second by default; the caller then gives up).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit = TC_WAIT_CYCLES) {
 	const long long t0 = clock64();
 	while (true) {
 		uint32_t done;
@@ -39,7 +39,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
 		    : "memory");
 		if (done)
 			return true;
-		if (clock64() - t0 > TC_WAIT_CYCLES)
+		if (clock64() - t0 > limit)
 			return false;
 	}
 }

@@ -346,6 +346,13 @@ DFG_API int dfg_pnet_set_targets(dfg_pnet *net, const long long *t_off, const in
  * tcgen05 tensor cores with BF16 activations (on = 1, the default) or on the
  * FP32 path that training uses (on = 0). */
 DFG_API int dfg_pnet_set_tensor_cores(dfg_pnet *net, int on);
+/* Network options by name (no counterpart in the reference): "tensor_cores"
+ * (as dfg_pnet_set_tensor_cores) and two failure-detection test hooks of the
+ * tensor-core products, "wait_cycles" (clock cycles after which a pipeline
+ * wait gives up, default 2e9) and "withhold_stage" (a stage whose copies are
+ * never issued, so its waits run out and dfg_pnet_topk / dfg_pnet_logits
+ * return DFG_ERR_CUDA; -1, the default, issues every stage). */
+DFG_API int dfg_pnet_set_option(dfg_pnet *net, const char *key, double value);
 
 /* out[n][K]: the K largest logits' classes of every loaded image, largest first. */
 DFG_API int dfg_pnet_topk(dfg_pnet *net, int K, int *out);
@@ -400,7 +407,12 @@ DFG_API int dfg_save_emc(dfg_ctx *ctx, const char *path);
  * (tile, frame) pairs, orientations in blocks), "block_budget_mb" (device
  * memory for one block of log-slices (and tomograms); without refinement a
  * value > 0 runs the full search in orientation blocks, which it also does
- * when the resident log-slices and tomograms would exceed half the memory). */
+ * when the resident log-slices and tomograms would exceed half the memory),
+ * and two failure-detection test hooks of the tensor-core kernels:
+ * "dense_wait_cycles" (clock cycles after which a pipeline wait gives up,
+ * default 2e9, about a second) and "dense_withhold_stage" (a stage index
+ * whose copies are never issued, so the waits on it run out and the call
+ * returns DFG_ERR_CUDA; -1, the default, issues every stage). */
 DFG_API int dfg_set_option(dfg_ctx *ctx, const char *key, double value);
 /* Phase times in ms summed since the last reset, and launch counts:
  * names[i] = "slice", "estep", "norm", "psum", "mstep", "merge", "update".

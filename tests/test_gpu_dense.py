@@ -88,3 +88,31 @@ def test_autotuner_times_both_forms_and_keeps_the_fastest(oracle_built, case):
         assert np.mean(np.asarray(a["rmax"]) == np.asarray(b["rmax"])) >= RMAX_AGREE
     tuned.close()
     plain.close()
+
+
+@pytest.mark.parametrize("forms", [(1, 0), (0, 1)], ids=["estep", "mstep"])
+def test_dense_pipeline_wait_gives_up_and_the_context_recovers(oracle_built, forms):
+    """Failure detection of the tensor-core kernels without a GPU fault: with
+    one stage's copies withheld (test hook) every wait on that stage runs out
+    after a short limit, the kernels set the error flag, drain their copies,
+    free their TMEM and return, and maximize reports DFG_ERR_CUDA; the next
+    call on the same context, with the hook off, succeeds and matches the
+    oracle."""
+    from dragonfly_b200._lib import DFG_ERR_CUDA, DFGError
+    prob = _synth()
+    gpu = GPUEngine(prob, estep_form=forms[0], mstep_form=forms[1])
+    c = gpu.ctx
+    par = c.params(1, prob.need_scaling, prob.update_scale, prob.known_scale, prob.beta_jump, prob.beta_period,
+                   prob.beta_factor)
+    c.set_option("dense_wait_cycles", 2e7)        # about 10 ms per wait
+    c.set_option("dense_withhold_stage", 1)
+    with pytest.raises(DFGError) as e:
+        c.maximize(par)
+    assert e.value.code == DFG_ERR_CUDA and "gave up" in str(e.value)
+    c.set_option("dense_withhold_stage", -1)
+    c.set_option("dense_wait_cycles", 2e9)
+    a = gpu.run_iteration(1)
+    b = OracleEngine(prob).run_iteration(1)
+    assert rel_l2(a["model1"], b["model1"]) <= MODEL_REL_L2
+    assert np.mean(np.asarray(a["rmax"]) == np.asarray(b["rmax"])) >= RMAX_AGREE
+    gpu.close()

@@ -131,6 +131,29 @@ def test_gpu_tensor_core_inference_matches_oracle(nc):
 
 
 @pytest.mark.gpu
+def test_gpu_tensor_core_wait_gives_up_and_the_network_recovers():
+    """Failure detection of the network's tensor-core products without a GPU
+    fault: with one stage's copies withheld (test hook) the waits on it run
+    out after a short limit and dfg_pnet_logits reports DFG_ERR_CUDA; with the
+    hook off the next call on the same network gives the logits of before."""
+    from dragonfly_b200._lib import DFG_ERR_CUDA, DFGError, ProposalNet
+    rng = np.random.default_rng(6)
+    net = ProposalNet(40, batch=64, seed=5)
+    x = np.log1p(rng.poisson(0.8, (600, 1024)).astype(np.float64)).astype(np.float32)
+    net.set_images(x)
+    z = net.logits()
+    net.set_option("wait_cycles", 2e7)          # about 10 ms per wait
+    net.set_option("withhold_stage", 1)
+    with pytest.raises(DFGError) as e:
+        net.logits()
+    assert e.value.code == DFG_ERR_CUDA and "gave up" in str(e.value)
+    net.set_option("withhold_stage", -1)
+    net.set_option("wait_cycles", 2e9)
+    np.testing.assert_array_equal(net.logits(), z)
+    net.close()
+
+
+@pytest.mark.gpu
 def test_gpu_soft_target_gradients_match_oracle():
     """Soft targets (a distribution over a few classes per image, as the
     full search's probabilities aggregated per coarse cell give them): loss
