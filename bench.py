@@ -505,9 +505,16 @@ def run_ours(args, rank, world, local_rank):
                       "autotuned": {"slice_block": tune["slice_block"],
                                     "estep_form": ["sparse", "dense"][tune["estep_form"]],
                                     "mstep_form": ["sparse", "dense"][tune["mstep_form"]],
+                                    "estep_blocks_per_sm": tune["estep_blocks_per_sm"],
+                                    "mstep_blocks_per_sm": tune["mstep_blocks_per_sm"],
                                     "ms_first_chunk": {k: None if tune[k] is None else round(float(tune[k]), 2)
                                                        for k in ("estep_sparse_ms", "estep_dense_ms",
-                                                                 "mstep_sparse_ms", "mstep_dense_ms")}},
+                                                                 "mstep_sparse_ms", "mstep_dense_ms")},
+                                    "ms_by_blocks_per_sm": {
+                                        "estep": {str(k): round(v, 2)
+                                                  for k, v in tune["estep_ms_by_blocks_per_sm"].items()},
+                                        "mstep": {str(k): round(v, 2)
+                                                  for k, v in tune["mstep_ms_by_blocks_per_sm"].items()}}},
                       "setup_s": setup_s},
            "s_per_iteration": ms_per_step / 1e3,
            "clocks": clocks,
@@ -729,6 +736,7 @@ def run_proposals(args):
     setup_s = time.perf_counter() - t0
     lp = LearnedProposals(c, inp["qvals"], fine, coarse_div=P_["coarse_div"], K=P_["K"], held_out=P_["held_out"],
                           threshold=P_["threshold"], seed=5, pair_lists=True, retrain_epochs=args.retrain_epochs,
+                          K_max=args.proposal_kmax or None, mass=args.proposal_mass or None,
                           retrain_lr=args.retrain_lr)
     t1 = time.perf_counter()
     if args.train_rounds:
@@ -781,7 +789,22 @@ def run_proposals(args):
         t_same = time.perf_counter() - t0
         mf, _, _ = c.model()
         rf = c.frame_results()["rmax"]
+        # further proposal iterations after the retraining: their captured
+        # mass, and the loop's time per iteration amortised over the fallback
+        # (full search + retraining) and every proposal iteration
+        more = []
+        for k in range(args.loop_iterations):
+            q_ = lp.iteration(par(it + 2 + k), 0.)
+            more.append({"mode": q_["mode"], "captured_mass": q_.get("captured_mass"),
+                         "wall_s": q_.get("propose_s", 0.) + q_.get("lists_s", 0.) + q_["iterate_s"] +
+                         q_.get("retrain_s", 0.)})
+        t_loop = f["iterate_s"] + f["retrain_s"] + p_["propose_s"] + p_["lists_s"] + p_["iterate_s"] + \
+            sum(x["wall_s"] for x in more)
+        n_loop = 2 + len(more)
         loop = {"full_search_s": f["iterate_s"], "full_search_phases_ms": full_phases,
+                "more_iterations": more,
+                "amortised_s_per_iteration": t_loop / n_loop,
+                "amortised_speedup_vs_full_search": f["iterate_s"] / (t_loop / n_loop),
                 "full_search_chunks": wl_full["chunks"], "retrain_s": f["retrain_s"],
                 "retrain": "%d epochs (lr %g) on the %d frames against the full search's probabilities per cell" % (
                     lp.retrain_epochs, lp.retrain_lr, N),
@@ -803,9 +826,11 @@ def run_proposals(args):
            "data": "synthetic (seeded; frames simulated on the GPU; model at the truth, true scales, beta 1)",
            "config": {"workload": "learned proposals: 260x257 pnCCD-like detector, 201^3 model, num_div %d (%d "
                                   "orientations), %d frames, median %g photons (lognormal sigma %g); %d coarse "
-                                  "cells (num_div %d), top %d, %g %% held out" % (
+                                  "cells (num_div %d), top %d%s, %g %% held out" % (
                                       w["num_div"], R, N, w["median_photons"], w["fluence_sigma"], lp.nc,
-                                      P_["coarse_div"], P_["K"], 100 * P_["held_out"]),
+                                      P_["coarse_div"], P_["K"],
+                                      "" if lp.mass is None else " and more up to %d until the network's probability "
+                                      "reaches %g" % (lp.K_max, lp.mass), 100 * P_["held_out"]),
                       "setup_s": setup_s, "train_s": train_s,
                       "training": "%d rounds x %d epochs of %d newly simulated frames, lr %g -> %g" % (
                           P_["rounds"], P_["epochs"], P_["train_frames"], P_["lr"], P_["lr_end"]),
@@ -846,6 +871,12 @@ def main():
     ap.add_argument("--retrain-epochs", type=int, default=3,
                     help="proposals --loop: epochs of retraining on the fallback full search's probabilities")
     ap.add_argument("--retrain-lr", type=float, default=1e-3, help="proposals --loop: retraining rate")
+    ap.add_argument("--proposal-kmax", type=int, default=0,
+                    help="proposals: mass-covering proposals with at most this many cells per frame (0: exactly K)")
+    ap.add_argument("--proposal-mass", type=float, default=0.,
+                    help="proposals: the network probability a frame's cells must cover (with --proposal-kmax)")
+    ap.add_argument("--loop-iterations", type=int, default=2,
+                    help="proposals --loop: proposal iterations after the retraining, for the amortised time")
     ap.add_argument("--loop", action="store_true",
                     help="proposals: also run the fallback full search (orientation blocks), retrain on its "
                          "probabilities and compare the next proposal iteration with a full search")

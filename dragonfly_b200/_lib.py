@@ -17,6 +17,9 @@ DFG_OK, DFG_ERR_ARG, DFG_ERR_CUDA, DFG_ERR_STATE, DFG_ERR_NOMEM = range(5)
 PHASES = ("slice", "estep", "norm", "psum", "mstep", "merge", "update")
 
 
+TUNE_REPORT = 18   # DFG_TUNE_REPORT, values of an autotuner report
+
+
 class DFGError(RuntimeError):
     """A call into libdfgpu.so returned an error code."""
 
@@ -88,6 +91,7 @@ _SIGS = {
     "dfg_pnet_get_images": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "dfg_pnet_train": (C.c_int, [_V, _I, C.c_int, C.c_double, C.c_ulonglong, _D]),
     "dfg_pnet_topk": (C.c_int, [_V, C.c_int, _I]),
+    "dfg_pnet_topk_mass": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, _I]),
     "dfg_pnet_set_tensor_cores": (C.c_int, [_V, C.c_int]),
     "dfg_pnet_set_option": (C.c_int, [_V, C.c_char_p, C.c_double]),
     "dfg_pnet_set_targets": (C.c_int, [_V, C.POINTER(C.c_longlong), _I, C.POINTER(C.c_float)]),
@@ -392,23 +396,29 @@ class Context:
 
     @staticmethod
     def _tune_dict(out):
+        opt = lambda v: float(v) if v >= 0 else None
         return dict(slice_ms={b: float(out[i]) for i, b in enumerate((128, 64, 32, 16)) if out[i] >= 0},
-                    estep_sparse_ms=float(out[4]), estep_dense_ms=float(out[5]) if out[5] >= 0 else None,
+                    estep_sparse_ms=float(out[4]), estep_dense_ms=opt(out[5]),
                     slice_block=int(out[6]), estep_form=int(out[7]) & 1, mstep_form=int(out[7]) >> 1,
-                    mstep_sparse_ms=float(out[8]) if out[8] >= 0 else None,
-                    mstep_dense_ms=float(out[9]) if out[9] >= 0 else None)
+                    mstep_sparse_ms=opt(out[8]), mstep_dense_ms=opt(out[9]),
+                    estep_ms_by_blocks_per_sm={b: float(out[10 + i]) for i, b in enumerate((2, 3, 4))
+                                               if out[10 + i] >= 0},
+                    mstep_ms_by_blocks_per_sm={b: float(out[13 + i]) for i, b in enumerate((3, 4, 5))
+                                               if out[13 + i] >= 0},
+                    estep_blocks_per_sm=int(out[16]), mstep_blocks_per_sm=int(out[17]))
 
     def autotune(self, par):
-        """Times the slice blocks and both E-step forms on the current inputs
-        and keeps the fastest (used by later iterations with option
-        autotune). Returns the measurements and the choice."""
-        out = np.zeros(10)
+        """Times the slice blocks, both E-step and M-step forms and the
+        sparse forms' blocks per SM on the current inputs and keeps the
+        fastest (used by later iterations with option autotune). Returns the
+        measurements and the choice."""
+        out = np.zeros(TUNE_REPORT)
         self.call("dfg_autotune", C.byref(par), ptr(out, C.c_double))
         return self._tune_dict(out)
 
     def tune_report(self):
         """The autotuner's last report for the current inputs (None if not tuned)."""
-        out = np.zeros(10)
+        out = np.zeros(TUNE_REPORT)
         if self.lib.dfg_get_autotune_report(self.h, ptr(out, C.c_double)) != DFG_OK:
             return None
         return self._tune_dict(out)
@@ -737,6 +747,14 @@ class ProposalNet:
     def topk(self, K):
         out = np.zeros((self.n_images, int(K)), np.int32)
         self._call("dfg_pnet_topk", int(K), ptr(out, C.c_int))
+        return out
+
+    def topk_mass(self, K_min, K_max, mass):
+        """[n, K_max]: per image the classes by decreasing logit, K_min and
+        then more until their softmax probabilities sum to mass (at most
+        K_max); unused slots -1."""
+        out = np.zeros((self.n_images, int(K_max)), np.int32)
+        self._call("dfg_pnet_topk_mass", int(K_min), int(K_max), float(mass), ptr(out, C.c_int))
         return out
 
     def logits(self):

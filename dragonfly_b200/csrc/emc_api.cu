@@ -410,6 +410,8 @@ extern "C" int dfg_set_refinement_topk(dfg_ctx *ctx, int num_coarse, const int *
 				w[j] = 0u;
 			for (long long t = d * K; t < (d + 1) * K; ++t) {
 				const int c = top[t];
+				if (c == -1)  // an unused slot
+					continue;
 				if (c < 0 || c >= num_coarse) {
 					if (bad[k] < 0)
 						bad[k] = t;
@@ -1376,12 +1378,21 @@ static int launch_mstep(dfg_ctx *ctx, const Chunk &ch, bool dense) {
 	}
 	if (ch.npix > 0) {
 		const long long warps = (long long)RT * ch.npix;
+		const int minb = ctx->tuning ? ctx->tune_mstep_minb
+		                             : (ctx->mstep_minb > 0 ? ctx->mstep_minb : ctx->tuned_mstep_minb);
+#define DFG_MSTEP(SK, MB)                                                                                     \
+	mstep_kernel<SK, MB><<<blocks_for(warps, 8), 256, 0, st>>>(ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p,           \
+	                                                           ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p,  \
+	                                                           ctx->tlive.p)
 		if (tile_skipping(ctx))
-			mstep_kernel<true><<<blocks_for(warps, 8), 256, 0, st>>>(
-			    ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p, ctx->tlive.p);
+			DFG_MSTEP(true, MSTEP_MINB);
+		else if (minb == 3)
+			DFG_MSTEP(false, 3);
+		else if (minb == 5)
+			DFG_MSTEP(false, 5);
 		else
-			mstep_kernel<false><<<blocks_for(warps, 8), 256, 0, st>>>(
-			    ctx->Pst.p, Nc, ch.cs.p, ch.cs_off.p, ch.cs_mid.p, ch.pix.p, ch.npix, P, RT, ctx->T.p, ctx->tlive.p);
+			DFG_MSTEP(false, MSTEP_MINB);
+#undef DFG_MSTEP
 		CKL("mstep_kernel");
 	}
 	return DFG_OK;
@@ -1408,14 +1419,21 @@ static int launch_estep(dfg_ctx *ctx, const Chunk &ch, int use_scale, bool bg, c
 		CKL("estep_bg_kernel");
 		return DFG_OK;
 	}
-#define DFG_ESTEP(REF)                                                                                        \
-	estep_kernel<REF><<<blocks_for(warps, 8), 256, 0, st>>>(                                                  \
+	// blocks per SM: the autotuner's choice (or the option), else the default
+	const int minb = ctx->tuning ? ctx->tune_estep_minb : (ctx->estep_minb > 0 ? ctx->estep_minb
+	                                                                           : ctx->tuned_estep_minb);
+#define DFG_ESTEP(REF, MB)                                                                                    \
+	estep_kernel<REF, MB><<<blocks_for(warps, 8), 256, 0, st>>>(                                              \
 	    ctx->logW.p, ctx->u.p, ctx->logw.p, R, ctx->ph.p, ctx->ph_off.p, ctx->ph_mid.p, ctx->scale.p,          \
 	    ctx->blacklist.p, ch.d0, Nc, use_scale, ctx->scalars.p, P, RT, ctx->pval.p, ctx->tmax.p, ctx->targ.p, rm)
 	if (rm.qmap != nullptr)
-		DFG_ESTEP(true);
+		DFG_ESTEP(true, ESTEP_MINB);
+	else if (minb == 2)
+		DFG_ESTEP(false, 2);
+	else if (minb == 4)
+		DFG_ESTEP(false, 4);
 	else
-		DFG_ESTEP(false);
+		DFG_ESTEP(false, ESTEP_MINB);
 #undef DFG_ESTEP
 	CKL("estep_kernel");
 	return DFG_OK;
@@ -1427,22 +1445,27 @@ static int launch_norm(dfg_ctx *ctx, const Chunk &ch, int psum_d_on, bool bg) {
 	cudaStream_t st = ctx->stream;
 	const int Nc = ch.nc, RT = ctx->RT, R = ctx->R, M = ctx->M;
 	const int zero_dead = (ctx->keep_prob || bg) ? 1 : 0;
-#define DFG_NORM(MUL, SK)                                                                                     \
-	norm_kernel<MUL, SK><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(                                               \
+#define DFG_NORM(MUL, SK, ONE)                                                                                \
+	norm_kernel<MUL, SK, ONE><<<blocks_for(Nc + 1, 8), 256, 0, st>>>(                                          \
 	    ctx->pval.p, ctx->tmax.p, ctx->targ.p, RT, Nc, ch.d0, R, M, ctx->logw.p, ctx->u.p, ctx->beta.p,        \
 	    ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p, ctx->Pst.p, ctx->rmax.p, ctx->max_exp.p, \
 	    ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p, ctx->quat_norm.p, ctx->num_prob.p,       \
 	    bg ? ctx->Pd.p : nullptr, ctx->tlive.p, zero_dead)
 	if (tile_skipping(ctx)) {
 		if (M > 1)
-			DFG_NORM(true, true);
+			DFG_NORM(true, true, false);
 		else
-			DFG_NORM(false, true);
+			DFG_NORM(false, true, false);
+	} else if (bg) {  // the FP64 copy of P: two exp per pair
+		if (M > 1)
+			DFG_NORM(true, false, false);
+		else
+			DFG_NORM(false, false, false);
 	} else {
 		if (M > 1)
-			DFG_NORM(true, false);
+			DFG_NORM(true, false, true);
 		else
-			DFG_NORM(false, false);
+			DFG_NORM(false, false, true);
 	}
 #undef DFG_NORM
 	CKL("norm_kernel");
@@ -1527,6 +1550,8 @@ static int build_pairs(dfg_ctx *ctx) {
 			}
 			for (long long j = ctx->h_rel_off[d]; j < ctx->h_rel_off[d + 1]; ++j) {
 				const int c = ctx->h_rel[j];
+				if (c < 0)  // an unused slot of a top-K array
+					continue;
 				for (long long q = coff[c]; q < coff[c + 1]; ++q)
 					if (stamp[ctiles[q]] != (int)d) {
 						stamp[ctiles[q]] = (int)d;
@@ -2212,18 +2237,20 @@ static int max_enqueue(dfg_ctx *ctx, const dfg_iter_params *par) {
 // of two after a warm-up launch) the slice kernel with 128, 64, 32 and 16 orientations per block and
 // both forms of the E-step photon term and of the M-step (sparse gathers,
 // dense tensor-core products where the inputs allow them) on the first frame
-// chunk, and keeps the fastest of each. tune_report: slice ms per block size
-// (-1 if not tried), sparse and dense E-step ms (-1 if refused; the dense one
-// includes the count densification), the chosen block, the chosen forms
-// (E-step + 2 x M-step, 1 = dense), sparse and dense M-step ms.
+// chunk, and keeps the fastest of each; then, where the sparse gathers won,
+// their resident blocks per SM. tune_report: as dfg_autotune's report (the
+// dense E-step time includes the count densification).
 static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 	NEED(ctx->P > 0 && ctx->N > 0 && ctx->num_rot > 0 && ctx->S > 0, DFG_ERR_STATE,
 	     "autotune: set detector, frames, quaternions and model first");
-	double rep[10] = {-1., -1., -1., -1., -1., -1., -1., -1., -1., -1.};
+	double rep[DFG_TUNE_REPORT];
+	std::fill(rep, rep + DFG_TUNE_REPORT, -1.);
 	const bool dense_ok = dense_refusal(ctx, par) == nullptr;
 	const bool save_timing = ctx->timing;
 	ctx->timing = false;
 	ctx->tuning = true;
+	ctx->tune_estep_minb = ESTEP_MINB;
+	ctx->tune_mstep_minb = MSTEP_MINB;
 	ctx->tune_form = ctx->tune_mform = dense_ok ? 1 : 0;
 	int rc = max_prepare(ctx, par);
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -2297,6 +2324,36 @@ static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 		rc = timed([&] { return launch_mstep(ctx, c0, false); }, rep[8]);
 	if (rc == DFG_OK && dense_ok)
 		rc = timed([&] { return launch_mstep(ctx, c0, true); }, rep[9]);
+	// resident blocks per SM of the sparse gathers (the plain 3-D path), when
+	// the sparse form is the faster; the chunk's probabilities are still those
+	// of its normalisation above
+	const bool plain = !bg && rm.qmap == nullptr && !tile_skipping(ctx);
+	const bool e_sparse = !(dense_ok && rep[5] >= 0. && rep[5] < rep[4]);
+	const bool m_sparse = !(dense_ok && rep[9] >= 0. && (rep[8] < 0. || rep[9] < rep[8]));
+	int e_minb = ESTEP_MINB, m_minb = MSTEP_MINB;
+	if (rc == DFG_OK && plain && e_sparse) {
+		const int cand[3] = {2, 3, 4};
+		for (int i = 0; i < 3 && rc == DFG_OK; ++i) {
+			ctx->tune_estep_minb = cand[i];
+			rc = timed([&] { return launch_estep(ctx, c0, use_scale, bg, rm, false); }, rep[10 + i]);
+		}
+		for (int i = 0; i < 3; ++i)
+			if (rep[10 + i] >= 0. && rep[10 + i] < rep[10 + (e_minb - 2)])
+				e_minb = cand[i];
+		ctx->tune_estep_minb = ESTEP_MINB;
+		// the last variant overwrote the chunk's log-likelihoods with equal values
+	}
+	if (rc == DFG_OK && plain && m_sparse && c0.npix > 0) {
+		const int cand[3] = {3, 4, 5};
+		for (int i = 0; i < 3 && rc == DFG_OK; ++i) {
+			ctx->tune_mstep_minb = cand[i];
+			rc = timed([&] { return launch_mstep(ctx, c0, false); }, rep[13 + i]);
+		}
+		for (int i = 0; i < 3; ++i)
+			if (rep[13 + i] >= 0. && rep[13 + i] < rep[13 + (m_minb - 3)])
+				m_minb = cand[i];
+		ctx->tune_mstep_minb = MSTEP_MINB;
+	}
 	if (rc == DFG_OK && dense_ok) {
 		int derr = 0;
 		CK(cudaMemcpy(&derr, ctx->derr.p, sizeof(int), cudaMemcpyDeviceToHost));
@@ -2314,10 +2371,14 @@ static int run_autotune(dfg_ctx *ctx, const dfg_iter_params *par) {
 	ctx->tuned_ob = best_ob;
 	ctx->tuned_form = (dense_ok && rep[5] >= 0. && rep[5] < rep[4]) ? 1 : 0;
 	ctx->tuned_mform = (dense_ok && rep[9] >= 0. && (rep[8] < 0. || rep[9] < rep[8])) ? 1 : 0;
+	ctx->tuned_estep_minb = e_minb;
+	ctx->tuned_mstep_minb = m_minb;
 	ctx->tuned = true;
 	rep[6] = best_ob;
 	rep[7] = ctx->tuned_form + 2 * ctx->tuned_mform;
-	std::copy(rep, rep + 10, ctx->tune_report);
+	rep[16] = e_minb;
+	rep[17] = m_minb;
+	std::copy(rep, rep + DFG_TUNE_REPORT, ctx->tune_report);
 	return DFG_OK;
 }
 
@@ -2325,7 +2386,7 @@ extern "C" int dfg_get_autotune_report(dfg_ctx *ctx, double *report) {
 	if (!ctx || !report)
 		return DFG_ERR_ARG;
 	NEED(ctx->tuned, DFG_ERR_STATE, "not tuned for the current inputs");
-	std::copy(ctx->tune_report, ctx->tune_report + 10, report);
+	std::copy(ctx->tune_report, ctx->tune_report + DFG_TUNE_REPORT, report);
 	return DFG_OK;
 }
 
@@ -2337,7 +2398,7 @@ extern "C" int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *re
 	if (int rc = run_autotune(ctx, par))
 		return rc;
 	if (report)
-		std::copy(ctx->tune_report, ctx->tune_report + 10, report);
+		std::copy(ctx->tune_report, ctx->tune_report + DFG_TUNE_REPORT, report);
 	return DFG_OK;
 }
 
@@ -3280,6 +3341,18 @@ extern "C" int dfg_set_option(dfg_ctx *ctx, const char *key, double value) {
 	}
 	if (!strcmp(key, "tile_skip")) {
 		ctx->mstep_skip = value != 0.;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "estep_blocks_per_sm")) {
+		NEED(value == 0 || value == 2 || value == 3 || value == 4, DFG_ERR_ARG,
+		     "estep_blocks_per_sm must be 0 (tuned / default), 2, 3 or 4");
+		ctx->estep_minb = (int)value;
+		return DFG_OK;
+	}
+	if (!strcmp(key, "mstep_blocks_per_sm")) {
+		NEED(value == 0 || value == 3 || value == 4 || value == 5, DFG_ERR_ARG,
+		     "mstep_blocks_per_sm must be 0 (tuned / default), 3, 4 or 5");
+		ctx->mstep_minb = (int)value;
 		return DFG_OK;
 	}
 	if (!strcmp(key, "dense_wait_cycles")) {

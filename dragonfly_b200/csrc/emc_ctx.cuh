@@ -212,7 +212,11 @@ struct dfg_ctx {
 	// it chose for the current inputs; tuning / tune_* while it measures
 	bool autotune = false, tuned = false, tuning = false;
 	int tuned_ob = 0, tuned_form = 0, tuned_mform = 0, tune_form = 0, tune_mform = 0;
-	double tune_report[10] = {};
+	// blocks per SM of the sparse E-step and M-step (0: the build's default;
+	// options estep_blocks_per_sm / mstep_blocks_per_sm override the tuner)
+	int estep_minb = 0, mstep_minb = 0, tuned_estep_minb = 0, tuned_mstep_minb = 0;
+	int tune_estep_minb = 0, tune_mstep_minb = 0;
+	double tune_report[DFG_TUNE_REPORT] = {};
 	int K = 0, K_pad = 0, dense_P = -1, cnt_rows = 0;
 	int max_count0 = -1;  // largest count on a mask < 2 pixel; -1 = not known
 	DevBuf<int> kpix, pcol, derr;

@@ -276,8 +276,8 @@ __device__ __forceinline__ void refine_skip_tile(double *__restrict__ tmax, int 
 	}
 }
 
-template <bool REFINE>
-__global__ void __launch_bounds__(256, ESTEP_MINB) estep_kernel(
+template <bool REFINE, int MINB = ESTEP_MINB>
+__global__ void __launch_bounds__(256, MINB) estep_kernel(
     const float *__restrict__ logW, const double *__restrict__ u, const double *__restrict__ logw, int R,
     const uint32_t *__restrict__ ph, const long long *__restrict__ ph_off, const long long *__restrict__ ph_mid,
     const double *__restrict__ scale, const uint8_t *__restrict__ blacklist, int d0, int Nc, int use_scale,
@@ -464,7 +464,16 @@ __device__ __forceinline__ void stream_rows(const double *__restrict__ src, size
 #ifndef DFG_NORM_MINB
 #define DFG_NORM_MINB 4
 #endif
-template <bool MULTI, bool SKIP>
+// ONE (without tile skipping or the FP64 copy): one exp per kept pair. The
+// first pass stores E = exp(beta (pval - max)) in FP32 in Pst and sums, per
+// frame and in FP64, E, E pval, E u_r, E (y - log w_r) and E per mode; the
+// second pass reads E back, writes P = E / p_norm with the sign gate and takes
+// the pairs with P < PROB_MIN (which info and quat_norm leave out) back out of
+// those sums. Then likelihood = sum E pval / p_norm - sum_fact, psum_d =
+// rescale sum E u_r / p_norm and info = (sum' E (y - log w_r) + (log M -
+// log p_norm) sum' E) / p_norm over the pairs with P >= PROB_MIN -- the
+// reference's per-pair sums (max_update.c:96-130), regrouped.
+template <bool MULTI, bool SKIP, bool ONE = false>
 __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
     const double *__restrict__ pval, const double *__restrict__ tmax, const int *__restrict__ targ, int RT,
     int Nc, int d0, int R, int M, const double *__restrict__ logw, const double *__restrict__ u,
@@ -563,6 +572,117 @@ __global__ void __launch_bounds__(256, DFG_NORM_MINB) norm_kernel(
 		const double t = tmax[(size_t)rt * Nc + dl];
 		return !(t > lo) && !(dadd(t, thr) > m);
 	};
+	if constexpr (ONE) {
+		static_assert(!SKIP, "the one-exp form reads every row");
+		double s = 0., sx = 0., su = 0., sy = 0.;
+		double qe[MULTI ? MAX_MODES : 1];
+#pragma unroll
+		for (int k = 0; k < (MULTI ? MAX_MODES : 1); ++k)
+			qe[k] = 0.;
+		int cnt = 0;
+		stream_rows(pv, tstride, RT, s_ring[threadIdx.x >> 5], lane, [&](int rt, const double (&v)[LW]) {
+			float out[LW];
+#pragma unroll
+			for (int e = 0; e < LW; ++e) {
+				const int r = rt * TILE + lane * LW + e;
+				out[e] = 0.f;
+				if (r < R) {
+					const double x = v[e];
+					const bool kept = (r <= rstar) ? (x > lo) : (dadd(x, thr) > m);
+					if (kept) {
+						const double y = dmul(b, dsub(x, m));
+						const double E = exp(y);
+						s += E;
+						sx += E * x;
+						if (psum_d_on)
+							su += E * u[r];
+						sy += E * (y - logw[r]);
+						if (MULTI) {
+							const int mode = r % M;
+#pragma unroll
+							for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
+								if (q == mode)
+									qe[q] += E;
+						}
+						cnt++;
+						out[e] = (float)E;   // kept pairs have y > -14: a normal FP32 value
+					}
+				}
+			}
+			st_row(ps + rt * pstride, out);
+		});
+		s = warp_sum(s);
+		for (int o = 16; o > 0; o >>= 1)
+			cnt += __shfl_xor_sync(FULL, cnt, o);
+		const double inv_s = 1. / s;
+		const float inv_sf = (float)inv_s;
+		// second pass: this lane's own FP32 values of the first pass, four rows
+		// in flight
+		double ys = 0., es = 0.;
+		double qs[MULTI ? MAX_MODES : 1];
+#pragma unroll
+		for (int k = 0; k < (MULTI ? MAX_MODES : 1); ++k)
+			qs[k] = 0.;
+		constexpr int R2 = 4;
+		for (int rt0 = 0; rt0 < RT; rt0 += R2) {
+			float ev[R2][LW];
+#pragma unroll
+			for (int k = 0; k < R2; ++k)
+				if (rt0 + k < RT)
+					ld_row_rw(ps + (rt0 + k) * pstride, ev[k]);
+#pragma unroll
+			for (int k = 0; k < R2; ++k) {
+				const int rt = rt0 + k;
+				if (rt >= RT)
+					break;
+				float out[LW];
+#pragma unroll
+				for (int e = 0; e < LW; ++e) {
+					const float E = ev[k][e];
+					const float P = E * inv_sf;
+					out[e] = (P > (float)PROB_MIN) ? P : -P;
+					if (E > 0.f && (double)E * inv_s < PROB_MIN) {
+						// a kept pair that info and quat_norm leave out
+						const int r = rt * TILE + lane * LW + e;
+						es += (double)E;
+						ys += (double)E * ((double)logf(E) - logw[r]);
+						if (MULTI) {
+							const int mode = r % M;
+#pragma unroll
+							for (int q = 0; q < (MULTI ? MAX_MODES : 1); ++q)
+								if (q == mode)
+									qs[q] += (double)E;
+						}
+					}
+				}
+				st_row(ps + rt * pstride, out);
+			}
+		}
+		sx = warp_sum(sx);
+		su = warp_sum(su);
+		sy = warp_sum(sy);
+		ys = warp_sum(ys);
+		es = warp_sum(es);
+		const double rescale = scalars[0], sf = sum_fact[d];
+		const double cinf = log((double)M) - log(s);
+		if (MULTI) {
+			for (int k = 0; k < M && k < MAX_MODES; ++k) {
+				const double v = warp_sum(qe[k]) - warp_sum(qs[k]);
+				if (lane == 0)
+					quat_norm[(size_t)d * M + k] = v * inv_s;
+			}
+		}
+		if (lane == 0) {
+			rmax[d] = rstar;
+			max_exp[d] = m;
+			p_norm[d] = s;
+			likelihood[d] = sx * inv_s - sf;
+			info[d] = ((sy - ys) + cinf * (s - es)) * inv_s;
+			psum_d[d] = psum_d_on ? rescale * su * inv_s : 0.;
+			num_prob[d] = cnt;
+		}
+		return;
+	}
 	double s = 0.;
 	int cnt = 0;
 	if constexpr (!SKIP) {
@@ -787,8 +907,8 @@ __global__ void psum_r_reduce_kernel(const double *__restrict__ part, int nsplit
 // pairing). No atomics; pixels are visited heaviest first for balance.
 constexpr int MSTEP_MINB = LW == 4 ? 4 : 6;
 
-template <bool SKIP>
-__global__ void __launch_bounds__(256, MSTEP_MINB) mstep_kernel(const float *__restrict__ Pst, int Nc,
+template <bool SKIP, int MINB = MSTEP_MINB>
+__global__ void __launch_bounds__(256, MINB) mstep_kernel(const float *__restrict__ Pst, int Nc,
                                                      const uint32_t *__restrict__ cs,
                                                      const long long *__restrict__ cs_off,
                                                      const long long *__restrict__ cs_mid,

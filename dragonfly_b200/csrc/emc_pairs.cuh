@@ -341,9 +341,10 @@ __global__ void __launch_bounds__(256) mstep_pairs_kernel(const float *__restric
 // tiles [t0, t0 + nt) for one frame chunk from their log-likelihoods (pval,
 // the chunk's dense layout) and the per-frame results of the first pass
 // (max_exp = maximum, rmax = its first orientation, p_norm = kept sum): the
-// kept rule and P = exp(beta (x - max)) x (1 / p_norm) exactly as
-// norm_kernel forms them, sign = PROB_MIN gate. One warp per (tile, frame);
-// warp index Nc of a tile writes the chunk's zero row.
+// kept rule and P exactly as the one-exp normalisation forms them (E =
+// exp(beta (x - max)) rounded to FP32, times 1 / p_norm in FP32), sign =
+// PROB_MIN gate. One warp per (tile, frame); warp index Nc of a tile writes
+// the chunk's zero row.
 __global__ void __launch_bounds__(256) prob_block_kernel(const double *__restrict__ pval, int t0, int nt, int Nc,
                                                          int d0, int R, const double *__restrict__ beta,
                                                          const double *__restrict__ max_exp,
@@ -374,15 +375,15 @@ __global__ void __launch_bounds__(256) prob_block_kernel(const double *__restric
 		const double thr = PDIFF_THRESH / b;
 		const double lo = dsub(m, thr);
 		const int rstar = rmax[d];
-		const double inv_s = 1. / s;
+		const float inv_sf = (float)(1. / s);
 #pragma unroll
 		for (int e = 0; e < LW; ++e) {
 			const int r = rt * TILE + lane * LW + e;
 			if (r < R) {
 				const bool kept = (r <= rstar) ? (x[e] > lo) : (dadd(x[e], thr) > m);
 				if (kept) {
-					const double P = exp(dmul(b, dsub(x[e], m))) * inv_s;
-					out[e] = (P > PROB_MIN) ? (float)P : -(float)P;
+					const float P = (float)exp(dmul(b, dsub(x[e], m))) * inv_sf;
+					out[e] = (P > (float)PROB_MIN) ? P : -P;
 				}
 			}
 		}

@@ -351,16 +351,36 @@ __global__ void frame_image_kernel(const uint32_t *__restrict__ ph, const long l
 		img[(size_t)dl * IMG * IMG + k] = log1pf(s[k]);
 }
 
-// The K largest logits of each row, in decreasing order (first index on
-// ties); one warp per row, K rounds of a warp-wide arg-max.
-__global__ void topk_kernel(const float *__restrict__ z, int B, int n, int K, int *__restrict__ out) {
+// The largest logits of each row, in decreasing order (first index on ties;
+// one warp per row, one warp-wide arg-max per pick): K_min picks, then more
+// until the picks' softmax probabilities (over the whole row) sum to `mass`,
+// at most K_max; unused slots of out [B][K_max] are -1. K_min = K_max gives
+// the plain top-K.
+__global__ void topk_kernel(const float *__restrict__ z, int B, int n, int K_min, int K_max, float mass,
+                            int *__restrict__ out) {
 	const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
 	if (b >= B)
 		return;
 	const float *r = z + (size_t)b * n;
-	float last = INFINITY;
+	// softmax normaliser of the row: its maximum and sum of exp(z - max)
+	float zmax = -INFINITY;
+	for (int j = lane; j < n; j += 32)
+		zmax = fmaxf(zmax, r[j]);
+	for (int o = 16; o > 0; o >>= 1)
+		zmax = fmaxf(zmax, __shfl_xor_sync(FULL, zmax, o));
+	float den = 0.f;
+	for (int j = lane; j < n; j += 32)
+		den += __expf(r[j] - zmax);
+	for (int o = 16; o > 0; o >>= 1)
+		den += __shfl_xor_sync(FULL, den, o);
+	float last = INFINITY, cum = 0.f;
 	int last_i = -1;
-	for (int k = 0; k < K; ++k) {
+	for (int k = 0; k < K_max; ++k) {
+		if (k >= K_min && cum >= mass) {   // covered: the rest of the row stays out
+			if (lane == 0)
+				out[(size_t)b * K_max + k] = -1;
+			continue;
+		}
 		float m = -INFINITY;
 		int mi = n;
 		for (int j = lane; j < n; j += 32) {
@@ -381,7 +401,8 @@ __global__ void topk_kernel(const float *__restrict__ z, int B, int n, int K, in
 			}
 		}
 		if (lane == 0)
-			out[(size_t)b * K + k] = mi < n ? mi : -1;
+			out[(size_t)b * K_max + k] = mi < n ? mi : -1;
+		cum += mi < n ? __expf(m - zmax) / den : 0.f;
 		last = m;
 		last_i = mi;
 	}
@@ -1288,22 +1309,29 @@ static int check_tc(dfg_pnet *net) {
 	return DFG_OK;
 }
 
-extern "C" int dfg_pnet_topk(dfg_pnet *net, int K, int *out) {
-	if (!net || K < 1 || K > net->num_classes || !out)
+extern "C" int dfg_pnet_topk_mass(dfg_pnet *net, int K_min, int K_max, double mass, int *out) {
+	if (!net || K_min < 1 || K_max < K_min || K_max > net->num_classes || !out || !(mass >= 0.))
 		return DFG_ERR_ARG;
 	PK(cudaSetDevice(net->device));
 	DevBuf<int> d;  // every image's picks, read back once
-	PK(d.ensure((size_t)net->n_images * K));
+	PK(d.ensure((size_t)net->n_images * K_max));
 	if (int rc = for_batches(net, [&](long long b0, int m) -> int {
-		    topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(net->act[NL].p, m, net->num_classes, K,
-		                                                                 d.p + (size_t)b0 * K);
+		    topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(
+		        net->act[NL].p, m, net->num_classes, K_min, K_max, (float)mass, d.p + (size_t)b0 * K_max);
 		    PKL("topk_kernel");
 		    return DFG_OK;
 	    }))
 		return rc;
-	PK(cudaMemcpyAsync(out, d.p, (size_t)net->n_images * K * sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+	PK(cudaMemcpyAsync(out, d.p, (size_t)net->n_images * K_max * sizeof(int), cudaMemcpyDeviceToHost,
+	                   net->stream));
 	PK(cudaStreamSynchronize(net->stream));
 	return check_tc(net);
+}
+
+extern "C" int dfg_pnet_topk(dfg_pnet *net, int K, int *out) {
+	if (!net || K < 1 || !out)
+		return DFG_ERR_ARG;
+	return dfg_pnet_topk_mass(net, K, K, 2., out);
 }
 
 extern "C" int dfg_pnet_logits(dfg_pnet *net, float *out) {

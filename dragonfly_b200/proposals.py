@@ -82,7 +82,11 @@ class LearnedProposals:
         fine: the context's orientation list [R, 5] (ideally from
             ``sort_by_coarse``).
         coarse_div: num_div of the coarse orientation set (the classes).
-        K: coarse cells kept per frame.
+        K: coarse cells kept per frame (the least, with mass).
+        K_max, mass: mass-covering proposals: after its K best cells a frame
+            keeps further cells, by decreasing network probability, until
+            the network's probabilities of its cells sum to mass, at most
+            K_max (None: exactly K cells per frame).
         held_out: share of frames searched in full and watched each iteration.
         threshold: mean captured probability mass below which the next
             iteration searches in full and the network is retrained.
@@ -97,13 +101,15 @@ class LearnedProposals:
     """
 
     def __init__(self, ctx, qvals, fine, coarse_div=4, K=16, held_out=0.01, threshold=0.99, batch=256, seed=0,
-                 pair_lists=False, zoom=0.3, retrain_epochs=3, retrain_lr=1e-3):
+                 pair_lists=False, zoom=0.3, retrain_epochs=3, retrain_lr=1e-3, K_max=None, mass=None):
         from ._lib import Context, ProposalNet
         self.ctx = ctx
         ctx.set_option("pair_lists", 1 if pair_lists else 0)
         self.coarse = quat_gen(coarse_div)
         self.nc = self.coarse.shape[0]
         self.K = int(K)
+        self.K_max = int(K_max) if K_max is not None else self.K
+        self.mass = None if mass is None else float(mass)
         self.held_out = float(held_out)
         self.threshold = float(threshold)
         self.qmap = np.ascontiguousarray(ctx.voronoi_subset(self.coarse, fine), np.int32)
@@ -168,9 +174,12 @@ class LearnedProposals:
         return self.net.train(None, epochs=epochs, lr=lr, seed=int(self.rng.integers(1 << 30)))
 
     def propose(self):
-        """Top-K coarse cells of every frame of the context."""
+        """Proposed coarse cells of every frame of the context: [N, K] (or
+        [N, K_max] with -1 in unused slots for mass-covering proposals)."""
         self.net.load_frames(self.ctx)
-        return self.net.topk(self.K)
+        if self.mass is None:
+            return self.net.topk(self.K)
+        return self.net.topk_mass(self.K, self.K_max, self.mass)
 
     def iteration(self, par, alpha=0.):
         """One iteration: proposal-restricted (held-out frames in full and
@@ -215,12 +224,14 @@ class LearnedProposals:
         n_watch = max(1, int(round(self.held_out * N)))
         watch = np.sort(self.rng.choice(N, n_watch, replace=False)).astype(np.int32)
         ctx.set_refinement_topk(self.nc, self.qmap, top, watch)
-        ctx.set_watch(watch, top[watch])
+        ctx.set_watch(watch, [row[row >= 0] for row in top[watch]])
         t2 = time.perf_counter()
         out = dict(ctx.run_iteration(par, alpha))
         t3 = time.perf_counter()
         mass = ctx.watch_mass()
-        frac = (self.K * (N - n_watch) + self.nc * n_watch) / float(self.nc * N)
+        per_frame = (top >= 0).sum(1)
+        per_frame[watch] = self.nc
+        frac = float(per_frame.sum()) / float(self.nc * N)
         info = dict(mode="proposal", captured_mass=float(mass.mean()), min_mass=float(mass.min()),
                     evaluated_fraction=frac, propose_s=t1 - t0, lists_s=t2 - t1, iterate_s=t3 - t2)
         self.full_next = bool(mass.mean() < self.threshold)

@@ -157,8 +157,9 @@ DFG_API int dfg_set_symmetry(dfg_ctx *ctx, int point_group, int axial_order);
 DFG_API int dfg_set_refinement(dfg_ctx *ctx, int num_coarse, const int *quat_mapping,
                                const long long *rel_off, const int *rel_quat);
 /* The same from a top-K array: frame d's relevant coarse orientations are
- * top[d * K .. d * K + K), except for the n_all frames in all_frames, which
- * evaluate every orientation (learned proposals with held-out frames). */
+ * top[d * K .. d * K + K) (entries -1 are unused slots), except for the n_all
+ * frames in all_frames, which evaluate every orientation (learned proposals
+ * with held-out frames). */
 DFG_API int dfg_set_refinement_topk(dfg_ctx *ctx, int num_coarse, const int *quat_mapping, int K, const int *top,
                                     int n_all, const int *all_frames);
 
@@ -275,11 +276,18 @@ DFG_API int dfg_run_iteration(dfg_ctx *ctx, const dfg_iter_params *par, double a
  * the first frame chunk, and keeps the fastest of each for later iterations
  * when option autotune is 1 (with option autotune, dfg_maximize /
  * dfg_run_iteration tune by themselves whenever the inputs changed).
- * report[10] (may be NULL): slice ms per block size (-1: not tried), sparse
- * and dense E-step ms (-1: form refused), the chosen block, the chosen forms
- * (E-step + 2 x M-step, 1 = dense), sparse and dense M-step ms. */
+ * When the sparse forms win it also times the sparse E-step at 2, 3 and 4
+ * resident blocks per SM and the sparse M-step at 3, 4 and 5 (launch bounds:
+ * registers per thread traded against warps in flight) and keeps the fastest.
+ * report[DFG_TUNE_REPORT] (may be NULL): [0-3] slice ms per block size (-1:
+ * not tried), [4-5] sparse and dense E-step ms (-1: form refused), [6] the
+ * chosen block, [7] the chosen forms (E-step + 2 x M-step, 1 = dense), [8-9]
+ * sparse and dense M-step ms, [10-12] sparse E-step ms at 2, 3, 4 blocks per
+ * SM, [13-15] sparse M-step ms at 3, 4, 5 blocks per SM (-1: not timed),
+ * [16] and [17] the chosen E-step and M-step blocks per SM. */
+#define DFG_TUNE_REPORT 18
 DFG_API int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *report);
-/* The last autotuner report (10 values) for the current inputs
+/* The last autotuner report (DFG_TUNE_REPORT values) for the current inputs
  * (DFG_ERR_STATE if none). */
 DFG_API int dfg_get_autotune_report(dfg_ctx *ctx, double *report);
 
@@ -356,6 +364,11 @@ DFG_API int dfg_pnet_set_option(dfg_pnet *net, const char *key, double value);
 
 /* out[n][K]: the K largest logits' classes of every loaded image, largest first. */
 DFG_API int dfg_pnet_topk(dfg_pnet *net, int K, int *out);
+/* Mass-covering proposals (no counterpart in the reference): out[n][K_max],
+ * per image the classes in decreasing order of their logits, K_min of them
+ * and then more until their softmax probabilities sum to `mass`, at most
+ * K_max; unused slots are -1. */
+DFG_API int dfg_pnet_topk_mass(dfg_pnet *net, int K_min, int K_max, double mass, int *out);
 DFG_API int dfg_pnet_logits(dfg_pnet *net, float *out);
 /* Mean loss and gradients (flat, as the parameters) on the first
  * min(n, batch) loaded images with labels; the parameters are not changed. */
@@ -408,7 +421,10 @@ DFG_API int dfg_save_emc(dfg_ctx *ctx, const char *path);
  * memory for one block of log-slices (and tomograms); without refinement a
  * value > 0 runs the full search in orientation blocks, which it also does
  * when the resident log-slices and tomograms would exceed half the memory),
- * and two failure-detection test hooks of the tensor-core kernels:
+ * "estep_blocks_per_sm" / "mstep_blocks_per_sm" (resident blocks per SM of
+ * the sparse E-step, 2-4, and M-step, 3-5; 0, the default, takes the
+ * autotuner's choice or the build's default), and two failure-detection test
+ * hooks of the tensor-core kernels:
  * "dense_wait_cycles" (clock cycles after which a pipeline wait gives up,
  * default 2e9, about a second) and "dense_withhold_stage" (a stage index
  * whose copies are never issued, so the waits on it run out and the call

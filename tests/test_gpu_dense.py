@@ -78,6 +78,13 @@ def test_autotuner_times_both_forms_and_keeps_the_fastest(oracle_built, case):
     assert rep["estep_form"] == int(rep["estep_dense_ms"] < rep["estep_sparse_ms"])
     assert rep["mstep_sparse_ms"] > 0 and rep["mstep_dense_ms"] > 0
     assert rep["mstep_form"] == int(rep["mstep_dense_ms"] < rep["mstep_sparse_ms"])
+    # where the sparse gathers win, their resident blocks per SM are tuned too
+    if rep["estep_form"] == 0:
+        t = rep["estep_ms_by_blocks_per_sm"]
+        assert set(t) == {2, 3, 4} and rep["estep_blocks_per_sm"] == min(t, key=t.get)
+    if rep["mstep_form"] == 0:
+        t = rep["mstep_ms_by_blocks_per_sm"]
+        assert set(t) == {3, 4, 5} and rep["mstep_blocks_per_sm"] == min(t, key=t.get)
     # iterations with the tuned choice agree with the plain sparse form
     plain = GPUEngine(prob)
     orc = OracleEngine(prob)

@@ -7,7 +7,9 @@ network gains over proposals without it (random cells). A fallback full
 search retrains the network on its probabilities per coarse cell; the next
 proposal iterations then capture more than the threshold and each must stay
 within 1e-3 (model) and 99 % (most likely orientations) of a full search
-from the same state."""
+from the same state. The proposals are mass-covering: at least K cells per
+frame, more (up to K_max) where the network's probabilities of the frame's
+cells fall short of a target mass."""
 import os
 import time
 
@@ -39,12 +41,16 @@ def test_learned_proposals_against_full_search(pair_lists):
         c.calc_beta(1., 0)
     # a 64 x 64 detector and 420 classes: the whole detector as the image and
     # a larger rate than the production detector's 3240 classes want
+    # at least 24 cells per frame, more where the network is unsure, until
+    # its probabilities of the frame's cells reach 0.9995 (at most 64)
     lp = LearnedProposals(restr, d["qvals"], fine, coarse_div=2, K=24, held_out=0.02, threshold=0.99, seed=1,
-                          pair_lists=pair_lists, zoom=1.0, retrain_epochs=int(os.environ.get("RETRAIN_EPOCHS", "40")))
+                          pair_lists=pair_lists, zoom=1.0, retrain_epochs=int(os.environ.get("RETRAIN_EPOCHS", "40")),
+                          K_max=64, mass=0.9995)
     loss = lp.train_simulated(d["model_true"], n_frames=30000, epochs=4, lr=2e-3)
     # the network's gain: top-K hit rate of the true orientations' cells
     cells = full.voronoi_subset(quat_gen(2), np.pad(d["frame_quats"][:, :4], ((0, 0), (0, 1))))
-    top = lp.propose()
+    lp.net.load_frames(restr)
+    top = lp.net.topk(lp.K)
     hit = float(np.mean([cells[i] in top[i] for i in range(len(cells))]))
     chance = lp.K / lp.nc
     print("training loss %.3f; top-%d hit rate %.3f (random cells %.3f)" % (loss, lp.K, hit, chance))
@@ -71,13 +77,12 @@ def test_learned_proposals_against_full_search(pair_lists):
                                                  agree, 1e3 * (t1 - t0), 1e3 * (t2 - t1)))
         if b["mode"] == "proposal":
             masses.append(b["captured_mass"])
-            assert b["evaluated_fraction"] < 0.2
+            assert b["evaluated_fraction"] < 0.25
             if b["captured_mass"] >= lp.threshold:
                 devs.append(dev)
-                # target 1e-3; measured 1.4-1.7e-3 with 0.9987-0.9990 of the
-                # probability captured (the rest is renormalised into the
-                # proposals), most likely orientations 99.98-100 %
-                assert dev <= float(os.environ.get("PROPOSAL_MODEL_TOL", "2e-3")) and agree >= 0.99, (dev, agree)
+                # the bar: within 1e-3 of a full search from the same state,
+                # most likely orientations >= 99 %
+                assert dev <= 1e-3 and agree >= 0.99, (dev, agree)
             else:
                 assert lp.full_next          # the next iteration falls back to full search
     # a full search retrains the network on these frames' own most likely

@@ -131,6 +131,37 @@ def test_gpu_tensor_core_inference_matches_oracle(nc):
 
 
 @pytest.mark.gpu
+def test_gpu_mass_covering_topk_matches_the_logits():
+    """dfg_pnet_topk_mass: per image the classes by decreasing logit, K_min
+    of them and then more until their softmax probabilities reach the mass,
+    at most K_max, -1 in the unused slots; the plain top-K is its prefix."""
+    from dragonfly_b200._lib import ProposalNet
+    rng = np.random.default_rng(8)
+    net = ProposalNet(420, batch=64, seed=5)
+    x = np.log1p(rng.poisson(0.8, (500, 1024)).astype(np.float64)).astype(np.float32)
+    net.set_images(x)
+    z = net.logits().astype(np.float64)
+    p = np.exp(z - z.max(1, keepdims=True))
+    p /= p.sum(1, keepdims=True)
+    K_min, K_max, mass = 4, 40, 0.5
+    sel = net.topk_mass(K_min, K_max, mass)
+    top = net.topk(K_max)
+    np.testing.assert_array_equal(net.topk(K_min), top[:, :K_min])
+    for i in range(len(x)):
+        n = int((sel[i] >= 0).sum())
+        assert K_min <= n <= K_max and np.all(sel[i, n:] == -1)
+        np.testing.assert_array_equal(sel[i, :n], top[i, :n])
+        cum = np.cumsum(p[i, top[i]])
+        # the first count at or after K_min whose cumulative probability
+        # reaches the mass (FP32 sums on the device: a 1e-5 margin)
+        if n < K_max:
+            assert cum[n - 1] >= mass - 1e-5
+        if n > K_min:
+            assert cum[n - 2] < mass + 1e-5
+    net.close()
+
+
+@pytest.mark.gpu
 def test_gpu_tensor_core_wait_gives_up_and_the_network_recovers():
     """Failure detection of the network's tensor-core products without a GPU
     fault: with one stage's copies withheld (test hook) the waits on it run
