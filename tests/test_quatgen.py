@@ -25,9 +25,12 @@ def test_quat_gen_invariants(n):
     np.testing.assert_allclose(np.linalg.norm(q[:, :4], axis=1), 1., rtol=0, atol=1e-14)
     assert abs(q[:, 4].sum() - 1.) < 1e-12
     assert (q[:, 4] > 0).all()
-    dots = np.abs(q[:, :4] @ q[:, :4].T)
-    np.fill_diagonal(dots, 0.)
-    assert dots.max() < 1. - 1e-9
+    # q and -q (or a repeat) would coincide after fixing the sign of the
+    # first non-zero component
+    c = q[:, :4].copy()
+    first = np.argmax(np.abs(c) > 1e-12, axis=1)
+    c *= np.sign(c[np.arange(len(c)), first])[:, None]
+    assert np.unique(np.round(c, 9), axis=0).shape[0] == len(c)
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
