@@ -779,6 +779,7 @@ def run_proposals(args):
         m0, _, _ = c.model()
         s0 = c.frame_params()["scale"]
         p_ = lp.proposal_iteration(par(it + 1), 0.)
+        p_fallback = lp.full_next
         mp, _, _ = c.model()
         rp = c.frame_results()["rmax"].copy()
         c.set_model(m0)
@@ -810,7 +811,7 @@ def run_proposals(args):
                     lp.retrain_epochs, lp.retrain_lr, N),
                 "proposal_after_retrain": {"captured_mass": p_["captured_mass"], "min_mass": p_["min_mass"],
                                            "wall_s": p_["propose_s"] + p_["lists_s"] + p_["iterate_s"],
-                                           "fallback_next": lp.full_next},
+                                           "fallback_next": p_fallback},
                 "vs_full_search_same_state": {"model_rel_l2": float(np.linalg.norm(mp - mf) / np.linalg.norm(mf)),
                                               "rmax_agreement": float(np.mean(rp == rf)),
                                               "full_search_s": t_same}}
