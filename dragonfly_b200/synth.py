@@ -235,6 +235,35 @@ def small_problem(seed=0, det_side=64, size=75, qmax=37., n_atoms=300, atom_radi
                 frame_quats=fr['quats'])
 
 
+def two_detector_problem(seed=0, size=33, qmax=15., n_atoms=80, atom_radius=6., num_div=2,
+                         n_frames=(160, 120), mean_count=(40., 25.), phi_sigma=0.):
+    """One model seen by two detectors of different geometry (Iterate with an
+    in_detector_list): a 28 x 28 flat detector with a radius-3 hole and a
+    20 x 24 detector farther out (detd 40) with a radius-2 hole, x and y
+    polarised, each with its own frames (n_frames, mean_count per detector;
+    lognormal per-frame fluence when phi_sigma > 0).
+
+    Returns (dets, shared): dets a list of two dicts (qvals, corr, mask and
+    the sparse frames, frame_quats, phi), shared a dict of quats (num_div,
+    equal weights), model_start (uniform [0, 1) from the seed) and
+    model_true."""
+    rng = np.random.default_rng(seed)
+    intens = gaussian_atom_intensity(n_atoms, atom_radius, size, rng)
+    geo = [flat_detector(28, 28, qmax, size, hole_radius=3.),
+           flat_detector(20, 24, qmax * 0.8, size, hole_radius=2., detd=40., pol='y')]
+    scale0 = mean_count[0] / model_mean_count(intens, geo[0][0], geo[0][1], geo[0][2], rng)
+    dets = []
+    for k, (qvals, corr, mask, detd, _) in enumerate(geo):
+        m = intens * (mean_count[k] / model_mean_count(intens, qvals, corr, mask, rng))
+        phi = np.exp(rng.normal(0., phi_sigma, n_frames[k])) if phi_sigma > 0 else None
+        fr = sample_frames(m, qvals, corr, mask, n_frames[k], rng, phi=phi)
+        dets.append(dict(qvals=qvals, corr=corr, mask=mask, detd=detd, frame_quats=fr["quats"], phi=fr["phi"],
+                         **{key: fr[key] for key in ("ones", "multi", "place_ones", "place_multi", "count_multi")}))
+    quats = quat_gen(num_div)
+    quats[:, 4] = 1. / quats.shape[0]
+    return dets, dict(quats=quats, model_start=rng.random((1, size, size, size)), model_true=intens * scale0)
+
+
 def small_problem_2d(seed=0, det_side=48, n_blobs=30, num_rot=90, n_frames=600, mean_count=80.,
                      hole_radius=3.):
     """A 2-D reconstruction (recon_type = 2d): a det_side^2 flat detector in

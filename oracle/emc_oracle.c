@@ -272,31 +272,44 @@ typedef struct {
 /* Orientations per sub-block of the parallel merge. */
 #define ORC_MERGE_SUB 64
 
-/* Scratch of merge_block: per (orientation, pixel) geometry, and per
- * (orientation, grid plane) the pixels with corners on that plane. */
+/* Scratch of merge_block: per (orientation, detector, pixel) geometry, and
+ * per (orientation, detector, grid plane) the pixels with corners on that
+ * plane. */
 typedef struct {
-	merge_rec *rec;     /* [ORC_MERGE_SUB][num_pix] */
-	int *idx;           /* [ORC_MERGE_SUB][2 * num_pix] */
-	long *off;          /* [ORC_MERGE_SUB][planes + 1] */
+	merge_rec *rec;     /* [ORC_MERGE_SUB][num_det][max_pix] */
+	int *idx;           /* [ORC_MERGE_SUB][num_det][2 * max_pix] */
+	long *off;          /* [ORC_MERGE_SUB][num_det][planes + 1] */
 	double *acc;        /* [M * V][2]: weight, model2 */
 	long planes;        /* M * size */
+	int num_det, max_pix;
 } merge_scratch;
 
+/* One detector of a maximize call: its geometry and, per block of
+ * orientations, its slices. */
+typedef struct {
+	int num_pix;
+	const double *qvals, *corr;
+	const uint8_t *mask;
+	double *views;      /* [blk][num_pix] */
+} det_view;
+
 /* slice_merge3d (model.c:171-244) for orientations r0 .. r1-1 in ascending
- * order, as the sequential loop of merge_tomogram (max_update.c:18-40) does.
- * The additions to every voxel happen in the order of that loop (orientation,
+ * order and, per orientation, the detectors in ascending order, as the
+ * sequential loop of merge_tomogram (max_update.c:18-40) does. The additions
+ * to every voxel happen in the order of that loop (orientation, detector,
  * pixel, corner), so the sums are bit-identical to it at any thread count:
- * the geometry of each (orientation, pixel) is computed in parallel over
- * orientations and listed under the two grid planes (mode * size + x and
+ * the geometry of each (orientation, detector, pixel) is computed in parallel
+ * over orientations and listed under the two grid planes (mode * size + x and
  * x + 1) its corners lie on; then the planes are shared out among the threads
- * and each walks its planes' lists in orientation and pixel order. The sums go
- * to acc, (weight, model2) interleaved per voxel so that one cache line holds
- * both. */
-static void merge_block(int r0, int r1, int M, const double *quats, const double *psum_r, const double *views,
-                        double *acc, long size, int num_pix, const double *qvals,
-                        const double *corr, const uint8_t *mask, merge_scratch *ms) {
+ * and each walks its planes' lists in orientation, detector and pixel order.
+ * A detector merges an orientation only where its psum_r is positive
+ * (max_update.c:34-36). The sums go to acc, (weight, model2) interleaved per
+ * voxel so that one cache line holds both. */
+static void merge_block(int r0, int r1, int M, int R, const double *quats, const double *psum_r,
+                        const det_view *dv, double *acc, long size, merge_scratch *ms) {
 	const long vol = size * size * size, s2 = size * size;
 	const long planes = ms->planes;
+	const int K = ms->num_det, P = ms->max_pix;
 	int s0;
 	for (s0 = r0; s0 < r1; s0 += ORC_MERGE_SUB) {
 		const int s1 = s0 + ORC_MERGE_SUB < r1 ? s0 + ORC_MERGE_SUB : r1;
@@ -304,77 +317,86 @@ static void merge_block(int r0, int r1, int M, const double *quats, const double
 		long j;
 		#pragma omp parallel for schedule(dynamic, 1)
 		for (r = s0; r < s1; ++r) {
-			merge_rec *out = &ms->rec[(long)(r - s0) * num_pix];
-			int *idx = &ms->idx[(long)(r - s0) * 2 * num_pix];
-			long *off = &ms->off[(long)(r - s0) * (planes + 1)];
-			const double *slice = &views[(long)(r - r0) * num_pix];
-			double rot[3][3], pos[3];
-			long t, x, y, z, p;
-			for (p = 0; p <= planes; ++p)
-				off[p] = 0;
-			if (!(psum_r[r] > 0.))
-				continue;
+			int k;
+			double rot[3][3];
 			orc_make_rot_quat(&quats[(r / M) * 5], rot);
-			for (t = 0; t < num_pix; ++t) {
-				long pl;
-				out[t].base = -1;
-				if (mask[t] > 1)
+			for (k = 0; k < K; ++k) {
+				const long set = (long)(r - s0) * K + k;
+				merge_rec *out = &ms->rec[set * P];
+				int *idx = &ms->idx[set * 2 * P];
+				long *off = &ms->off[set * (planes + 1)];
+				const det_view *v = &dv[k];
+				const double *slice = &v->views[(long)(r - r0) * v->num_pix];
+				double pos[3];
+				long t, x, y, z, p;
+				for (p = 0; p <= planes; ++p)
+					off[p] = 0;
+				if (!(psum_r[(long)k * R + r] > 0.))
 					continue;
-				rotate_pixel(rot, &qvals[t * 3], (double)(size / 2), pos);
-				x = (long)pos[0];
-				y = (long)pos[1];
-				z = (long)pos[2];
-				if (x < 0 || x > size - 2 || y < 0 || y > size - 2 || z < 0 || z > size - 2)
-					continue;
-				out[t].base = (long)(r % M) * vol + x * s2 + y * size + z;
-				out[t].fx = pos[0] - x;
-				out[t].fy = pos[1] - y;
-				out[t].fz = pos[2] - z;
-				out[t].w = slice[t] / corr[t];
-				/* corners 0-3 lie on plane pl, 4-7 on pl + 1 (x + 1 <= size - 1) */
-				pl = (long)(r % M) * size + x;
-				off[pl + 1]++;
-				off[pl + 2]++;
+				for (t = 0; t < v->num_pix; ++t) {
+					long pl;
+					out[t].base = -1;
+					if (v->mask[t] > 1)
+						continue;
+					rotate_pixel(rot, &v->qvals[t * 3], (double)(size / 2), pos);
+					x = (long)pos[0];
+					y = (long)pos[1];
+					z = (long)pos[2];
+					if (x < 0 || x > size - 2 || y < 0 || y > size - 2 || z < 0 || z > size - 2)
+						continue;
+					out[t].base = (long)(r % M) * vol + x * s2 + y * size + z;
+					out[t].fx = pos[0] - x;
+					out[t].fy = pos[1] - y;
+					out[t].fz = pos[2] - z;
+					out[t].w = slice[t] / v->corr[t];
+					/* corners 0-3 lie on plane pl, 4-7 on pl + 1 (x + 1 <= size - 1) */
+					pl = (long)(r % M) * size + x;
+					off[pl + 1]++;
+					off[pl + 2]++;
+				}
+				for (p = 0; p < planes; ++p)
+					off[p + 1] += off[p];
+				for (t = 0; t < v->num_pix; ++t) {
+					long pl;
+					if (out[t].base < 0)
+						continue;
+					pl = out[t].base / s2;
+					idx[off[pl]++] = (int)t;
+					idx[off[pl + 1]++] = (int)t;
+				}
+				/* the fill advanced each start to the next plane's: shift back */
+				for (p = planes; p > 0; --p)
+					off[p] = off[p - 1];
+				off[0] = 0;
 			}
-			for (p = 0; p < planes; ++p)
-				off[p + 1] += off[p];
-			for (t = 0; t < num_pix; ++t) {
-				long pl;
-				if (out[t].base < 0)
-					continue;
-				pl = out[t].base / s2;
-				idx[off[pl]++] = (int)t;
-				idx[off[pl + 1]++] = (int)t;
-			}
-			/* the fill advanced each start to the next plane's: shift back */
-			for (p = planes; p > 0; --p)
-				off[p] = off[p - 1];
-			off[0] = 0;
 		}
 		#pragma omp parallel for schedule(dynamic, 1)
 		for (j = 0; j < planes; ++j) {
-			int rr;
-			for (rr = s0; rr < s1; ++rr) {
-				const merge_rec *rec = &ms->rec[(long)(rr - s0) * num_pix];
-				const int *idx = &ms->idx[(long)(rr - s0) * 2 * num_pix];
-				const long *off = &ms->off[(long)(rr - s0) * (planes + 1)];
-				long i, k;
-				for (i = off[j]; i < off[j + 1]; ++i) {
-					const merge_rec *e = &rec[idx[i]];
-					const long b = e->base;
-					const int upper = b / s2 != j;     /* j is the plane of corners 4-7 */
-					const double fx = e->fx, fy = e->fy, fz = e->fz, w = e->w;
-					const double cx = 1. - fx, cy = 1. - fy, cz = 1. - fz;
-					const long id[8] = {b, b + 1, b + size, b + size + 1,
-					                    b + s2, b + s2 + 1, b + s2 + size, b + s2 + size + 1};
-					const double fw[8] = {cx * cy * cz, cx * cy * fz, cx * fy * cz, cx * fy * fz,
-					                      fx * cy * cz, fx * cy * fz, fx * fy * cz, fx * fy * fz};
-					for (k = upper ? 4 : 0; k < (upper ? 8 : 4); ++k) {
-						acc[2 * id[k]] += fw[k];
-						acc[2 * id[k] + 1] += fw[k] * w;
+			int rr, k;
+			for (rr = s0; rr < s1; ++rr)
+				for (k = 0; k < K; ++k) {
+					const long set = (long)(rr - s0) * K + k;
+					const merge_rec *rec = &ms->rec[set * P];
+					const int *idx = &ms->idx[set * 2 * P];
+					const long *off = &ms->off[set * (planes + 1)];
+					long i;
+					int c;
+					for (i = off[j]; i < off[j + 1]; ++i) {
+						const merge_rec *e = &rec[idx[i]];
+						const long b = e->base;
+						const int upper = b / s2 != j;     /* j is the plane of corners 4-7 */
+						const double fx = e->fx, fy = e->fy, fz = e->fz, w = e->w;
+						const double cx = 1. - fx, cy = 1. - fy, cz = 1. - fz;
+						const long id[8] = {b, b + 1, b + size, b + size + 1,
+						                    b + s2, b + s2 + 1, b + s2 + size, b + s2 + size + 1};
+						const double fw[8] = {cx * cy * cz, cx * cy * fz, cx * fy * cz, cx * fy * fz,
+						                      fx * cy * cz, fx * cy * fz, fx * fy * cz, fx * fy * fz};
+						for (c = upper ? 4 : 0; c < (upper ? 8 : 4); ++c) {
+							acc[2 * id[c]] += fw[c];
+							acc[2 * id[c] + 1] += fw[c] * w;
+						}
 					}
 				}
-			}
 		}
 	}
 }
@@ -385,39 +407,60 @@ static void merge_block(int r0, int r1, int M, const double *quats, const double
  * ascending order); this restatement keeps each of those orders and
  * parallelises only across independent frames or orientations, so its results
  * do not depend on the thread count. The merge into model2 adds to every voxel
- * in orientation order, as with one reference thread (merge_block). */
-double orc_maximize(int num_pix, const double *qvals, const double *corr, const uint8_t *mask,
-                    int num_data, const int *ones, const int *multi, const int *place_ones,
-                    const int *place_multi, const int *count_multi,
-                    int num_rot, int num_modes, const double *quats,
-                    long size, const double *model1,
-                    double *scale, const double *beta, const double *sum_fact, const int *fcounts,
-                    const uint8_t *blacklist, double mean_count,
-                    int need_scaling, int update_scale, int known_scale, int iteration,
-                    double *model2, double *weight, double *u, double *psum_r,
-                    int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
-                    double *psum_d, double *quat_norm, int *num_prob, double *scalars_out) {
-	const int M = num_modes, R = num_modes * num_rot;
+ * in orientation order, as with one reference thread (merge_block).
+ *
+ * Several detectors (Iterate with in_detector_list, iterate.pyx:432-456):
+ * frame d is seen by detector det_of[d]; u, the rescale factor, psum_r and
+ * the tomograms are per detector (max_prob.c:31-42, 56-60; max_update.c:
+ * 55-128, 153-229) and every frame's likelihood uses its own detector's
+ * slice, u and rescale (max_prob.c:96-106, 122-127). */
+double orc_maximize_dets(int num_det, const int *num_pix, const double *const *qvals,
+                         const double *const *corr, const uint8_t *const *mask, const int *det_of,
+                         int num_data, const int *ones, const int *multi, const int *place_ones,
+                         const int *place_multi, const int *count_multi,
+                         int num_rot, int num_modes, const double *quats,
+                         long size, const double *model1,
+                         double *scale, const double *beta, const double *sum_fact, const int *fcounts,
+                         const uint8_t *blacklist, const double *mean_count,
+                         int need_scaling, int update_scale, int known_scale, int iteration,
+                         double *model2, double *weight, double *u, double *psum_r,
+                         int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
+                         double *psum_d, double *quat_norm, int *num_prob, double *rescale,
+                         double *scalars_out) {
+	const int M = num_modes, R = num_modes * num_rot, K = num_det;
 	const long vol = size * size * size, center = size / 2;
 	long *ones_off = malloc((size_t)(num_data + 1) * sizeof(long));
 	long *multi_off = malloc((size_t)(num_data + 1) * sizeof(long));
-	long blk = ORC_BLOCK_DOUBLES / (num_pix > 0 ? num_pix : 1);
-	double *views;
+	long blk, tot_pix = 0;
+	det_view *dv = calloc((size_t)K, sizeof(det_view));
 	merge_scratch ms;
 	kept_list *lists = calloc((size_t)num_data, sizeof(kept_list));
-	double total = 0., rescale, avg_ll = 0., mutual_info = 0.;
+	double avg_ll = 0., mutual_info = 0.;
 	const int use_scale = need_scaling && (iteration > 1 || known_scale);
-	int d, r, r0;
+	int d, r, r0, k;
 
+	ms.max_pix = 1;
+	for (k = 0; k < K; ++k) {
+		dv[k].num_pix = num_pix[k];
+		dv[k].qvals = qvals[k];
+		dv[k].corr = corr[k];
+		dv[k].mask = mask[k];
+		tot_pix += num_pix[k];
+		if (num_pix[k] > ms.max_pix)
+			ms.max_pix = num_pix[k];
+	}
+	blk = ORC_BLOCK_DOUBLES / (tot_pix > 0 ? tot_pix : 1);
 	if (blk < 1)
 		blk = 1;
 	if (blk > R)
 		blk = R;
-	views = malloc((size_t)blk * num_pix * sizeof(double));
+	for (k = 0; k < K; ++k)
+		dv[k].views = malloc((size_t)blk * (num_pix[k] > 0 ? num_pix[k] : 1) * sizeof(double));
+	ms.num_det = K;
 	ms.planes = (long)M * size;
-	ms.rec = malloc((size_t)ORC_MERGE_SUB * num_pix * sizeof(merge_rec));
-	ms.idx = malloc((size_t)ORC_MERGE_SUB * 2 * num_pix * sizeof(int));
-	ms.off = malloc((size_t)ORC_MERGE_SUB * (ms.planes + 1) * sizeof(long));
+	ms.rec = malloc((size_t)ORC_MERGE_SUB * K * ms.max_pix * sizeof(merge_rec));
+	ms.idx = malloc((size_t)ORC_MERGE_SUB * K * 2 * ms.max_pix * sizeof(int));
+	ms.off = malloc((size_t)ORC_MERGE_SUB * K * (ms.planes + 1) * sizeof(long));
 	ms.acc = calloc((size_t)2 * M * vol, sizeof(double));
 	ones_off[0] = multi_off[0] = 0;
 	for (d = 0; d < num_data; ++d) {
@@ -438,52 +481,64 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 #define ROTIND(r) ((r) / M)
 #define MODE(r) ((r) % M)
 
-	/* calculate_rescale (max_prob.c:3-64): u_r = sum of W over mask==0 pixels */
+	/* calculate_rescale (max_prob.c:3-64): u_r = sum of W over mask==0 pixels,
+	 * per detector */
 	#pragma omp parallel for schedule(dynamic, 4)
 	for (r = 0; r < R; ++r) {
-		int t;
-		double *view = malloc((size_t)num_pix * sizeof(double)), acc = 0.;
-		orc_slice_gen3d(&quats[ROTIND(r) * 5], MODE(r), view, num_pix, qvals, corr, size, center, model1);
-		for (t = 0; t < num_pix; ++t)
-			if (mask[t] < 1)
-				acc += view[t];
-		u[r] = acc;
-		free(view);
+		int t, kk;
+		for (kk = 0; kk < K; ++kk) {
+			double *view = malloc((size_t)(num_pix[kk] > 0 ? num_pix[kk] : 1) * sizeof(double)), acc = 0.;
+			orc_slice_gen3d(&quats[ROTIND(r) * 5], MODE(r), view, num_pix[kk], qvals[kk], corr[kk], size, center,
+			                model1);
+			for (t = 0; t < num_pix[kk]; ++t)
+				if (mask[kk][t] < 1)
+					acc += view[t];
+			u[(long)kk * R + r] = acc;
+			free(view);
+		}
 	}
-	for (r = 0; r < R; ++r)
-		total += quats[ROTIND(r) * 5 + 4] * u[r];
-	rescale = mean_count / total * M;
+	for (k = 0; k < K; ++k) {
+		double total = 0.;
+		for (r = 0; r < R; ++r)
+			total += quats[ROTIND(r) * 5 + 4] * u[(long)k * R + r];
+		rescale[k] = mean_count[k] / total * M;
+	}
 
 	/* calculate_prob (max_prob.c:66-213): per frame, orientations in order */
 	for (r0 = 0; r0 < R; r0 += (int)blk) {
 		int r1 = r0 + (int)blk < R ? r0 + (int)blk : R;
 		#pragma omp parallel for schedule(dynamic, 1)
 		for (r = r0; r < r1; ++r) {
-			int t;
-			double *view = &views[(long)(r - r0) * num_pix];
-			orc_slice_gen3d(&quats[ROTIND(r) * 5], MODE(r), view, num_pix, qvals, corr, size, center, model1);
-			for (t = 0; t < num_pix; ++t)
-				view[t] = log(view[t]);
+			int t, kk;
+			for (kk = 0; kk < K; ++kk) {
+				double *view = &dv[kk].views[(long)(r - r0) * num_pix[kk]];
+				orc_slice_gen3d(&quats[ROTIND(r) * 5], MODE(r), view, num_pix[kk], qvals[kk], corr[kk], size,
+				                center, model1);
+				for (t = 0; t < num_pix[kk]; ++t)
+					view[t] = log(view[t]);
+			}
 		}
 		#pragma omp parallel for schedule(dynamic, 16)
 		for (d = 0; d < num_data; ++d) {
 			int rr;
 			long i;
+			const int kd = det_of[d];
+			const uint8_t *mk = mask[kd];
 			if (blacklist[d])
 				continue;
 			for (rr = r0; rr < r1; ++rr) {
-				const double *view = &views[(long)(rr - r0) * num_pix];
+				const double *view = &dv[kd].views[(long)(rr - r0) * num_pix[kd]];
 				const double w = quats[ROTIND(rr) * 5 + 4];
 				double pval, thr;
 				if (use_scale)
-					pval = log(w) - u[rr] * scale[d];
+					pval = log(w) - u[(long)kd * R + rr] * scale[d];
 				else
-					pval = log(w) - u[rr] * rescale;
+					pval = log(w) - u[(long)kd * R + rr] * rescale[kd];
 				for (i = ones_off[d]; i < ones_off[d + 1]; ++i)
-					if (mask[place_ones[i]] < 1)
+					if (mk[place_ones[i]] < 1)
 						pval += view[place_ones[i]];
 				for (i = multi_off[d]; i < multi_off[d + 1]; ++i)
-					if (mask[place_multi[i]] < 1)
+					if (mk[place_multi[i]] < 1)
 						pval += count_multi[i] * view[place_multi[i]];
 				thr = ORC_PDIFF_THRESH / beta[d];
 				if (pval + thr > max_exp[d])
@@ -502,25 +557,26 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 	 * over the frame's kept orientations in ascending order. */
 	#pragma omp parallel for schedule(dynamic, 16)
 	for (d = 0; d < num_data; ++d) {
-		int k;
+		int kk;
 		double s = 0.;
 		kept_list *l = &lists[d];
+		const int kd = det_of[d];
 		if (max_exp[d] == ORC_MAX_EXP_START)
 			rmax[d] = -1;
-		for (k = 0; k < l->n; ++k)
-			s += exp(beta[d] * (l->val[k] - max_exp[d]));
+		for (kk = 0; kk < l->n; ++kk)
+			s += exp(beta[d] * (l->val[kk] - max_exp[d]));
 		p_norm[d] = s;
 		if (blacklist[d])
 			continue;
-		for (k = 0; k < l->n; ++k) {
-			const int rr = l->pos[k];
+		for (kk = 0; kk < l->n; ++kk) {
+			const int rr = l->pos[kk];
 			const double w = quats[ROTIND(rr) * 5 + 4];
-			double temp = l->val[k];
+			double temp = l->val[kk];
 			double P = exp(beta[d] * (temp - max_exp[d])) / p_norm[d];
-			l->val[k] = P;
+			l->val[kk] = P;
 			likelihood[d] += P * (temp - sum_fact[d]);
 			if (need_scaling && update_scale)
-				psum_d[d] += P * u[rr] * rescale;
+				psum_d[d] += P * u[(long)kd * R + rr] * rescale[kd];
 			if (P < ORC_PROB_MIN)
 				continue;
 			if (M > 1)
@@ -536,9 +592,10 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 		int r1 = r0 + (int)blk < R ? r0 + (int)blk : R;
 		#pragma omp parallel for schedule(dynamic, 1)
 		for (r = r0; r < r1; ++r) {
-			double *view = &views[(long)(r - r0) * num_pix], pr = 0.;
-			int dd, t;
+			int dd, t, kk;
 			long i;
+			for (kk = 0; kk < K; ++kk)
+				psum_r[(long)kk * R + r] = 0.;
 			for (dd = 0; dd < num_data; ++dd) {
 				int ind;
 				if (blacklist[dd])
@@ -546,13 +603,17 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 				ind = list_find(&lists[dd], r);
 				if (ind < 0)
 					continue;
-				pr += need_scaling ? lists[dd].val[ind] * scale[dd] : lists[dd].val[ind];
+				psum_r[(long)det_of[dd] * R + r] += need_scaling ? lists[dd].val[ind] * scale[dd]
+				                                                 : lists[dd].val[ind];
 			}
-			psum_r[r] = pr;
-			memset(view, 0, (size_t)num_pix * sizeof(double));
+			for (kk = 0; kk < K; ++kk)
+				memset(&dv[kk].views[(long)(r - r0) * num_pix[kk]], 0, (size_t)num_pix[kk] * sizeof(double));
 			for (dd = 0; dd < num_data; ++dd) {
 				int ind;
 				double P;
+				const int kd = det_of[dd];
+				const uint8_t *mk = mask[kd];
+				double *view = &dv[kd].views[(long)(r - r0) * num_pix[kd]];
 				if (blacklist[dd])
 					continue;
 				ind = list_find(&lists[dd], r);
@@ -562,17 +623,21 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 				if (!(P > ORC_PROB_MIN))
 					continue;
 				for (i = ones_off[dd]; i < ones_off[dd + 1]; ++i)
-					if (mask[place_ones[i]] < 2)
+					if (mk[place_ones[i]] < 2)
 						view[place_ones[i]] += P;
 				for (i = multi_off[dd]; i < multi_off[dd + 1]; ++i)
-					if (mask[place_multi[i]] < 2)
+					if (mk[place_multi[i]] < 2)
 						view[place_multi[i]] += count_multi[i] * P;
 			}
-			if (pr > 0.)
-				for (t = 0; t < num_pix; ++t)
-					view[t] /= pr;
+			for (kk = 0; kk < K; ++kk) {
+				const double pr = psum_r[(long)kk * R + r];
+				double *view = &dv[kk].views[(long)(r - r0) * num_pix[kk]];
+				if (pr > 0.)
+					for (t = 0; t < num_pix[kk]; ++t)
+						view[t] /= pr;
+			}
 		}
-		merge_block(r0, r1, M, quats, psum_r, views, ms.acc, size, num_pix, qvals, corr, mask, &ms);
+		merge_block(r0, r1, M, R, quats, psum_r, dv, ms.acc, size, &ms);
 	}
 
 	for (r0 = 0; r0 < M; ++r0) {
@@ -602,9 +667,8 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 	if (num_prob != NULL)
 		for (d = 0; d < num_data; ++d)
 			num_prob[d] = lists[d].n;
-	scalars_out[0] = rescale;
-	scalars_out[1] = mutual_info;
-	scalars_out[2] = avg_ll;
+	scalars_out[0] = mutual_info;
+	scalars_out[1] = avg_ll;
 
 	if (g_keep_prob) {      /* retained for orc_kept_prob until the next call */
 		orc_free_kept();
@@ -618,7 +682,9 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 		}
 		free(lists);
 	}
-	free(views);
+	for (k = 0; k < K; ++k)
+		free(dv[k].views);
+	free(dv);
 	free(ms.rec);
 	free(ms.idx);
 	free(ms.off);
@@ -628,6 +694,31 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
 #undef ROTIND
 #undef MODE
 	return avg_ll;
+}
+
+double orc_maximize(int num_pix, const double *qvals, const double *corr, const uint8_t *mask,
+                    int num_data, const int *ones, const int *multi, const int *place_ones,
+                    const int *place_multi, const int *count_multi,
+                    int num_rot, int num_modes, const double *quats,
+                    long size, const double *model1,
+                    double *scale, const double *beta, const double *sum_fact, const int *fcounts,
+                    const uint8_t *blacklist, double mean_count,
+                    int need_scaling, int update_scale, int known_scale, int iteration,
+                    double *model2, double *weight, double *u, double *psum_r,
+                    int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
+                    double *psum_d, double *quat_norm, int *num_prob, double *scalars_out) {
+	/* one detector: every frame is detector 0's */
+	int *det_of = calloc((size_t)(num_data > 0 ? num_data : 1), sizeof(int));
+	double sc[2], avg;
+	avg = orc_maximize_dets(1, &num_pix, &qvals, &corr, &mask, det_of, num_data, ones, multi, place_ones,
+	                        place_multi, count_multi, num_rot, num_modes, quats, size, model1, scale, beta,
+	                        sum_fact, fcounts, blacklist, &mean_count, need_scaling, update_scale, known_scale,
+	                        iteration, model2, weight, u, psum_r, rmax, info, likelihood, max_exp, p_norm,
+	                        psum_d, quat_norm, num_prob, &scalars_out[0], sc);
+	scalars_out[1] = sc[0];
+	scalars_out[2] = sc[1];
+	free(det_of);
+	return avg;
 }
 
 double orc_update_model(long size, int num_modes, double *model1, double *model2, double *weight,

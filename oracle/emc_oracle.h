@@ -68,6 +68,27 @@ double orc_maximize(int num_pix, const double *qvals, const double *corr, const 
                     int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
                     double *psum_d, double *quat_norm, int *num_prob, double *scalars_out);
 
+/* orc_maximize for several detectors (Iterate with in_detector_list,
+ * iterate.pyx:432-456): detector k has num_pix[k] pixels with qvals[k]
+ * [num_pix][3], corr[k] and mask[k]; frame d is seen by detector det_of[d];
+ * mean_count [K] per detector. Per-detector outputs: u and psum_r [K*M*R]
+ * (detector-major), rescale [K]; scalars_out [2]: mutual_info,
+ * avg_likelihood. The merge adds, per orientation, the detectors in
+ * ascending order (max_update.c:34-36). */
+double orc_maximize_dets(int num_det, const int *num_pix, const double *const *qvals,
+                         const double *const *corr, const uint8_t *const *mask, const int *det_of,
+                         int num_data, const int *ones, const int *multi, const int *place_ones,
+                         const int *place_multi, const int *count_multi,
+                         int num_rot, int num_modes, const double *quats,
+                         long size, const double *model1,
+                         double *scale, const double *beta, const double *sum_fact, const int *fcounts,
+                         const uint8_t *blacklist, const double *mean_count,
+                         int need_scaling, int update_scale, int known_scale, int iteration,
+                         double *model2, double *weight, double *u, double *psum_r,
+                         int *rmax, double *info, double *likelihood, double *max_exp, double *p_norm,
+                         double *psum_d, double *quat_norm, int *num_prob, double *rescale,
+                         double *scalars_out);
+
 /* With on != 0, orc_maximize keeps its per-frame probability lists (kept
  * orientations in ascending order and their normalised probabilities P) until
  * the next call; orc_kept_prob(d, pos, val) copies frame d's list into pos /

@@ -174,7 +174,12 @@ class ReferenceEngine:
         L.ref_get_frame_prob.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.ref_set_refinement.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_set_friedel_detd.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.ref_add_detector.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _up, C.c_int, _ip, _ip, _ip, _ip, _ip,
+                                       C.c_void_p, C.c_void_p]
+        L.ref_get_u_det.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.ref_get_det_scalars.argtypes = [C.c_void_p, _dp, _dp]
         self.save_prob = False
+        self.extra = []
         self.prob = p = prob
         self._scale_buf = p.scale
         self._bl_buf = p.blacklist
@@ -195,6 +200,33 @@ class ReferenceEngine:
     def __del__(self):
         self.close()
 
+    def add_detector(self, det):
+        """Another detector and the frames it sees (see ref_add_detector):
+        det is an EMCProblem whose detector and frames are used (its scale and
+        blacklist, if any, give those frames' values); its frames follow the
+        frames so far."""
+        self.extra.append(det)
+        self.lib.ref_add_detector(
+            self.h, det.num_pix, det.qvals.reshape(-1), det.corr, det.mask, det.num_data, det.ones, det.multi,
+            det.place_ones, det.place_multi, det.count_multi,
+            None if det.scale is None else det.scale.ctypes.data,
+            None if det.blacklist is None else det.blacklist.ctypes.data)
+
+    @property
+    def num_data(self):
+        return self.prob.num_data + sum(d.num_data for d in self.extra)
+
+    @property
+    def num_det(self):
+        return 1 + len(self.extra)
+
+    @property
+    def blacklist(self):
+        if self.prob.blacklist is None and all(d.blacklist is None for d in self.extra):
+            return None
+        return np.concatenate([q.blacklist if q.blacklist is not None else np.zeros(q.num_data, np.uint8)
+                               for q in [self.prob] + self.extra])
+
     def _arr(self, fn, shape, dt=np.float64):
         out = np.zeros(shape, dtype=dt)
         fn(self.h, out.reshape(-1))
@@ -205,7 +237,7 @@ class ReferenceEngine:
         return self._arr(self.lib.ref_get_model1, p.model1.shape)
 
     def iter_arrays(self):
-        n = self.prob.num_data
+        n = self.num_data
         fc = np.zeros(n, np.int32)
         sf, sc, be, bs = (np.zeros(n) for _ in range(4))
         self.lib.ref_get_iter_arrays(self.h, fc, sf, sc, be, bs)
@@ -255,7 +287,7 @@ class ReferenceEngine:
         self.lib.ref_set_save_prob(self.h, int(bool(on)))
 
     def _sparse_prob(self):
-        n = self.prob.num_data
+        n = self.num_data
         counts = np.array([self.lib.ref_get_frame_prob(self.h, d, None, None) for d in range(n)], np.int64)
         off = np.zeros(n + 1, np.int64)
         off[1:] = np.cumsum(counts)
@@ -270,7 +302,7 @@ class ReferenceEngine:
         p = self.prob
         L = self.lib
         avg_ll = L.ref_maximize(self.h, int(iteration))
-        n = p.num_data
+        n = self.num_data
         res = IterationResult()
         if self.save_prob:
             res["sparse_prob"] = self._sparse_prob()
@@ -284,6 +316,13 @@ class ReferenceEngine:
         L.ref_get_scalars(self.h, sc)
         res["rescale"], res["mean_count"], res["mutual_info"] = sc[0], sc[1], sc[2]
         res["avg_likelihood"] = avg_ll
+        if self.extra:
+            K = self.num_det
+            res["u_det"] = np.zeros((K, p.num_modes * p.num_rot))
+            for k in range(K):
+                L.ref_get_u_det(self.h, k, res["u_det"][k])
+            res["rescale_det"], res["mean_count_det"] = np.zeros(K), np.zeros(K)
+            L.ref_get_det_scalars(self.h, res["rescale_det"], res["mean_count_det"])
         res["model2_sum"] = self._arr(L.ref_get_model2, p.model1.shape)
         res["inter_weight"] = self._arr(L.ref_get_weight, p.model1.shape)
         rms = L.ref_update_model(self.h)
@@ -294,7 +333,7 @@ class ReferenceEngine:
         if p.need_scaling and p.model_type == "3d":   # recon.pyx:102-103
             scale = it["scale"]
             model1 = self.model1()
-            rms, _ = normalize_scale(scale, p.blacklist, model1, rms)
+            rms, _ = normalize_scale(scale, self.blacklist, model1, rms)
             L.ref_set_scale(self.h, scale)
             L.ref_set_model1(self.h, model1.reshape(-1))
             L.ref_set_rms(self.h, rms)
@@ -362,9 +401,11 @@ class LegacyEngine:
 
 
 class OracleEngine:
-    """Our own C restatement (emc_oracle.c), same interface as ReferenceEngine."""
+    """Our own C restatement (emc_oracle.c), same interface as ReferenceEngine.
+    extra: more detectors, each an EMCProblem whose detector and frames are
+    used (as ReferenceEngine.add_detector); their frames follow prob's."""
 
-    def __init__(self, prob):
+    def __init__(self, prob, extra=()):
         self.lib = L = _load(LIB_ORACLE)
         L.orc_maximize.restype = C.c_double
         L.orc_maximize.argtypes = [C.c_int, _dp, _dp, _up, C.c_int, _ip, _ip, _ip, _ip, _ip,
@@ -382,22 +423,44 @@ class OracleEngine:
         L.orc_set_keep_prob.argtypes = [C.c_int]
         L.orc_kept_prob.restype = C.c_int
         L.orc_kept_prob.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        PP = C.POINTER(C.c_void_p)
+        L.orc_maximize_dets.restype = C.c_double
+        L.orc_maximize_dets.argtypes = [C.c_int, _ip, PP, PP, PP, _ip, C.c_int, _ip, _ip, _ip, _ip, _ip,
+                                        C.c_int, C.c_int, _dp, C.c_long, _dp,
+                                        _dp, _dp, _dp, _ip, _up, _dp,
+                                        C.c_int, C.c_int, C.c_int, C.c_int,
+                                        _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _dp, _dp]
         self.save_prob = False
         self.prob = p = prob
-        n = p.num_data
-        self.fcounts = np.zeros(n, np.int32)
-        self.sum_fact = np.zeros(n)
-        mc = C.c_double(0.)
-        L.orc_frame_stats(n, p.ones, p.multi, p.place_ones, p.place_multi, p.count_multi,
-                          p.mask, self.fcounts, self.sum_fact, C.byref(mc))
-        self.mean_count = mc.value
+        self.dets = dets = [p] + list(extra)
+        # per detector: fcounts, sum_fact over its mask (calc_frame_counts,
+        # calc_sum_fact, iterate.c:3-117), mean_count over its frames
+        fcs, sfs, mcs = [], [], []
+        for q in dets:
+            fc, sf, mc = np.zeros(q.num_data, np.int32), np.zeros(q.num_data), C.c_double(0.)
+            L.orc_frame_stats(q.num_data, q.ones, q.multi, q.place_ones, q.place_multi, q.count_multi,
+                              q.mask, fc, sf, C.byref(mc))
+            fcs.append(fc)
+            sfs.append(sf)
+            mcs.append(mc.value)
+        n = sum(q.num_data for q in dets)
+        self.fcounts = np.concatenate(fcs)
+        self.sum_fact = np.concatenate(sfs)
+        self.mean_count_det = np.array(mcs)
+        self.mean_count = mcs[0]
+        self.det_of = np.concatenate([np.full(q.num_data, k, np.int32) for k, q in enumerate(dets)])
         self.beta_start = np.zeros(n)
+        # calc_beta's empirical start uses detector 0's mean count (iterate.c:72-73)
         L.orc_calc_beta(n, p.beta, p.need_scaling, self.mean_count, self.fcounts, self.beta_start)
         self.beta = np.zeros(n)
-        self.blacklist = p.blacklist if p.blacklist is not None else np.zeros(n, np.uint8)
-        self.scale = (p.scale.copy() if p.scale is not None else np.ones(n)) if p.need_scaling \
-            else np.ones(n)
+        self.blacklist = np.concatenate([q.blacklist if q.blacklist is not None else np.zeros(q.num_data, np.uint8)
+                                         for q in dets])
+        self.scale = np.concatenate([q.scale.copy() if q.scale is not None else np.ones(q.num_data)
+                                     for q in dets]) if p.need_scaling else np.ones(n)
         self._model1 = p.model1.copy()
+        if len(dets) > 1:
+            self.frames = {k: np.concatenate([getattr(q, k) for q in dets]).astype(np.int32)
+                           for k in ("ones", "multi", "place_ones", "place_multi", "count_multi")}
 
     def model1(self):
         return self._model1.copy()
@@ -410,7 +473,7 @@ class OracleEngine:
 
     def _sparse_prob(self):
         L = self.lib
-        n = self.prob.num_data
+        n = self.det_of.size
         counts = np.array([max(L.orc_kept_prob(d, None, None), 0) for d in range(n)], np.int64)
         off = np.zeros(n + 1, np.int64)
         off[1:] = np.cumsum(counts)
@@ -440,30 +503,50 @@ class OracleEngine:
     def run_iteration(self, iteration):
         p = self.prob
         L = self.lib
-        n, M = p.num_data, p.num_modes
+        n, M, K = self.det_of.size, p.num_modes, len(self.dets)
         self.update_beta(iteration)
         shape = self._model1.shape
         model2 = np.zeros(shape)
         weight = np.zeros(shape)
-        u = np.zeros(M * p.num_rot)
-        psum_r = np.zeros(M * p.num_rot)
+        u = np.zeros((K, M * p.num_rot))
+        psum_r = np.zeros((K, M * p.num_rot))
         rmax = np.zeros(n, np.int32)
         info, ll, mx, pn, pd = (np.zeros(n) for _ in range(5))
         qn = np.zeros((n, M))
         nprob = np.zeros(n, np.int32)
-        sc = np.zeros(3)
         L.orc_set_keep_prob(int(self.save_prob))
-        avg_ll = L.orc_maximize(
-            p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, n, p.ones, p.multi, p.place_ones,
-            p.place_multi, p.count_multi, p.num_rot, M, p.quats.reshape(-1), p.size,
-            self._model1.reshape(-1), self.scale, self.beta, self.sum_fact, self.fcounts,
-            self.blacklist, self.mean_count, p.need_scaling, p.update_scale, p.known_scale,
-            int(iteration), model2.reshape(-1), weight.reshape(-1), u, psum_r, rmax, info, ll,
-            mx, pn, pd, qn.reshape(-1), nprob, sc)
+        if K == 1:
+            sc = np.zeros(3)
+            avg_ll = L.orc_maximize(
+                p.num_pix, p.qvals.reshape(-1), p.corr, p.mask, n, p.ones, p.multi, p.place_ones,
+                p.place_multi, p.count_multi, p.num_rot, M, p.quats.reshape(-1), p.size,
+                self._model1.reshape(-1), self.scale, self.beta, self.sum_fact, self.fcounts,
+                self.blacklist, self.mean_count, p.need_scaling, p.update_scale, p.known_scale,
+                int(iteration), model2.reshape(-1), weight.reshape(-1), u[0], psum_r[0], rmax, info, ll,
+                mx, pn, pd, qn.reshape(-1), nprob, sc)
+            rescale_det, mi = sc[:1], sc[1]
+        else:
+            PA = C.c_void_p * K
+            qv = PA(*[q.qvals.ctypes.data for q in self.dets])
+            co = PA(*[q.corr.ctypes.data for q in self.dets])
+            mk = PA(*[q.mask.ctypes.data for q in self.dets])
+            npix = np.array([q.num_pix for q in self.dets], np.int32)
+            f = self.frames
+            rescale_det, sc = np.zeros(K), np.zeros(2)
+            avg_ll = L.orc_maximize_dets(
+                K, npix, qv, co, mk, self.det_of, n, f["ones"], f["multi"], f["place_ones"], f["place_multi"],
+                f["count_multi"], p.num_rot, M, p.quats.reshape(-1), p.size, self._model1.reshape(-1), self.scale,
+                self.beta, self.sum_fact, self.fcounts, self.blacklist, self.mean_count_det, p.need_scaling,
+                p.update_scale, p.known_scale, int(iteration), model2.reshape(-1), weight.reshape(-1),
+                u.reshape(-1), psum_r.reshape(-1), rmax, info, ll, mx, pn, pd, qn.reshape(-1), nprob,
+                rescale_det, sc)
+            mi = sc[0]
         res = IterationResult(rmax=rmax, info=info, likelihood=ll, max_exp=mx, p_norm=pn,
-                              psum_d=pd, u=u, psum_r=psum_r, quat_norm=qn, num_prob=nprob,
-                              rescale=sc[0], mutual_info=sc[1], avg_likelihood=avg_ll,
+                              psum_d=pd, u=u[0], psum_r=psum_r[0], quat_norm=qn, num_prob=nprob,
+                              rescale=rescale_det[0], mutual_info=mi, avg_likelihood=avg_ll,
                               mean_count=self.mean_count, beta=self.beta.copy())
+        if K > 1:
+            res.update(u_det=u, psum_r_det=psum_r, rescale_det=rescale_det, mean_count_det=self.mean_count_det)
         if self.save_prob:
             res["sparse_prob"] = self._sparse_prob()
             L.orc_set_keep_prob(0)
@@ -473,7 +556,7 @@ class OracleEngine:
                                  weight.reshape(-1), p.alpha)
         res["model2"] = model2
         if p.need_scaling:
-            rms, _ = normalize_scale(self.scale, p.blacklist, self._model1, rms)
+            rms, _ = normalize_scale(self.scale, self.blacklist if K > 1 else p.blacklist, self._model1, rms)
             res["scale"] = self.scale.copy()
         res["rms_change"] = rms
         res["model1"] = self.model1()

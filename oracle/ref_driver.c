@@ -34,6 +34,13 @@ typedef struct ref_engine {
 	struct max_data *mdata;
 	int det_mapping[1];
 	double avg_likelihood;
+	double beta_start;          /* calc_beta's argument, for ref_add_detector */
+	/* more detectors (ref_add_detector): all detectors contiguous (detector 0
+	 * a copy of det), their datasets linked after dset, one per detector */
+	struct detector *dets;
+	struct dataset **extra;
+	int *det_map;
+	int n_extra;
 } ref_engine;
 
 static void *dup_mem(const void *src, size_t bytes) {
@@ -45,7 +52,7 @@ static void *dup_mem(const void *src, size_t bytes) {
 
 /* Frees the per-call arrays that maximize() allocates on the common struct
  * (maximize.c:58-97). The reference itself leaks them on every call. */
-static void free_common(struct max_data *c, int num_data) {
+static void free_common(struct max_data *c, int num_data, int num_det) {
 	int d;
 	if (c->rmax == NULL)
 		return;
@@ -59,7 +66,8 @@ static void free_common(struct max_data *c, int num_data) {
 	}
 	free(c->prob); free(c->place_prob);
 	if (c->u != NULL) {
-		free(c->u[0]);
+		for (d = 0; d < num_det; ++d)
+			free(c->u[d]);
 		free(c->u);
 	}
 	free(c->max_exp); free(c->p_norm); free(c->offset_prob);
@@ -165,6 +173,7 @@ ref_engine *ref_create(int num_pix, const double *qvals, const double *corr, con
 		for (d = 0; d < num_data; ++d)
 			e->iter.scale[d] = scale != NULL ? scale[d] : 1.;
 	}
+	e->beta_start = beta_start;
 	calc_beta(beta_start, &e->iter);
 
 	e->mdata = calloc(1, sizeof(struct max_data));
@@ -198,7 +207,7 @@ double ref_maximize(ref_engine *e, int iteration) {
 		slice_gen = &slice_gen3d;
 		slice_merge = &slice_merge3d;
 	}
-	free_common(e->mdata, it->tot_num_data);
+	free_common(e->mdata, it->tot_num_data, it->num_det);
 	e->mdata->iter = it;
 	e->mdata->within_openmp = 0;
 	e->avg_likelihood = maximize(e->mdata);
@@ -247,10 +256,107 @@ double ref_update_model(ref_engine *e) {
 
 void ref_set_refinement(ref_engine *e, const int *quat_mapping, const long long *rel_off, const int *rel_quat);
 
+static void copy_or_zero(void *dst, const void *src, size_t bytes);
+
+/* One more detector with one dataset of frames seen by it, appended after the
+ * frames so far (Iterate.set_data with a dataset list whose files name
+ * several detectors, iterate.pyx:241-266 and _gen_detlist :432-456; the new
+ * detector gets the next index). The per-frame arrays are formed again as
+ * set_data / parse_scale / parse_blacklist / calc_beta form them; scale and
+ * blacklist give the new frames' values (NULL: 1 and 0). */
+void ref_add_detector(ref_engine *e, int num_pix, const double *qvals, const double *corr, const uint8_t *mask,
+                      int num_data, const int *ones, const int *multi, const int *place_ones,
+                      const int *place_multi, const int *count_multi, const double *scale,
+                      const uint8_t *blacklist) {
+	struct iterate *it = &e->iter;
+	const int K = it->num_det + 1, old_n = it->tot_num_data, n = old_n + num_data;
+	struct detector *dets = calloc((size_t)K, sizeof(struct detector));
+	struct dataset *ds = calloc(1, sizeof(struct dataset)), *curr;
+	long d, ones_total = 0, multi_total = 0;
+	int k;
+
+	memcpy(dets, it->det, (size_t)(K - 1) * sizeof(struct detector));
+	dets[K - 1].num_pix = num_pix;
+	dets[K - 1].qvals = dup_mem(qvals, (size_t)num_pix * 3 * sizeof(double));
+	dets[K - 1].corr = dup_mem(corr, (size_t)num_pix * sizeof(double));
+	dets[K - 1].raw_mask = dup_mem(mask, (size_t)num_pix);
+	dets[K - 1].detd = e->det.detd;
+	free(e->dets);
+	e->dets = dets;
+	it->det = dets;
+
+	ds->ftype = SPARSE;
+	ds->num_data = num_data;
+	ds->num_pix = num_pix;
+	ds->num_offset = old_n;
+	ds->ones = dup_mem(ones, (size_t)num_data * sizeof(int));
+	ds->multi = dup_mem(multi, (size_t)num_data * sizeof(int));
+	ds->ones_accum = malloc((size_t)(num_data > 0 ? num_data : 1) * sizeof(long));
+	ds->multi_accum = malloc((size_t)(num_data > 0 ? num_data : 1) * sizeof(long));
+	for (d = 0; d < num_data; ++d) {
+		ds->ones_accum[d] = ones_total;
+		ds->multi_accum[d] = multi_total;
+		ones_total += ones[d];
+		multi_total += multi[d];
+	}
+	ds->ones_total = ones_total;
+	ds->multi_total = multi_total;
+	ds->place_ones = dup_mem(place_ones, (size_t)ones_total * sizeof(int));
+	ds->place_multi = dup_mem(place_multi, (size_t)multi_total * sizeof(int));
+	ds->count_multi = dup_mem(count_multi, (size_t)multi_total * sizeof(int));
+	e->extra = realloc(e->extra, (size_t)(e->n_extra + 1) * sizeof(struct dataset *));
+	e->extra[e->n_extra++] = ds;
+	for (curr = &e->dset; curr->next != NULL; curr = curr->next)
+		;
+	curr->next = ds;
+	/* every dataset's detector in the new array (calc_frame_counts reads it) */
+	e->dset.det = &dets[0];
+	for (k = 0; k < e->n_extra; ++k)
+		e->extra[k]->det = &dets[k + 1];
+
+	free(e->det_map);
+	e->det_map = malloc((size_t)K * sizeof(int));
+	for (k = 0; k < K; ++k)
+		e->det_map[k] = k;
+	it->det_mapping = e->det_map;
+	it->num_det = K;
+	it->num_dfiles = K;
+	it->tot_num_data = n;
+
+	free(it->fcounts); it->fcounts = NULL;
+	free(it->mean_count); it->mean_count = NULL;
+	free(it->rescale); it->rescale = NULL;
+	calc_frame_counts(it);
+	it->blacklist = realloc(it->blacklist, (size_t)(n > 0 ? n : 1));
+	for (d = 0; d < num_data; ++d)
+		it->blacklist[old_n + d] = blacklist != NULL ? blacklist[d] : 0;
+	free(it->sum_fact); it->sum_fact = NULL;
+	calc_sum_fact(it);
+	if (e->par.need_scaling) {
+		it->scale = realloc(it->scale, (size_t)(n > 0 ? n : 1) * sizeof(double));
+		for (d = 0; d < num_data; ++d)
+			it->scale[old_n + d] = scale != NULL ? scale[d] : 1.;
+	}
+	free(it->beta); it->beta = NULL;
+	free(it->beta_start); it->beta_start = NULL;
+	calc_beta(e->beta_start, it);
+}
+
+/* Per-detector results of the last maximize: u [num_rot_p] of detector k,
+ * and rescale / mean_count of every detector. */
+void ref_get_u_det(ref_engine *e, int k, double *o) {
+	copy_or_zero(o, e->mdata->u != NULL ? e->mdata->u[k] : NULL, (size_t)e->quat.num_rot_p * sizeof(double));
+}
+
+void ref_get_det_scalars(ref_engine *e, double *rescale, double *mean_count) {
+	memcpy(rescale, e->iter.rescale, (size_t)e->iter.num_det * sizeof(double));
+	memcpy(mean_count, e->iter.mean_count, (size_t)e->iter.num_det * sizeof(double));
+}
+
 void ref_destroy(ref_engine *e) {
 	if (e == NULL)
 		return;
-	free_common(e->mdata, e->iter.tot_num_data);
+	free_common(e->mdata, e->iter.tot_num_data, e->iter.num_det);
 	free(e->mdata);
 	free(e->det.qvals); free(e->det.corr); free(e->det.raw_mask);
 	free(e->dset.ones); free(e->dset.multi); free(e->dset.ones_accum); free(e->dset.multi_accum);
@@ -262,6 +368,17 @@ void ref_destroy(ref_engine *e) {
 	free(e->iter.beta); free(e->iter.beta_start);
 	free(e->det.background); free(e->det.powder); free(e->iter.bgscale);
 	ref_set_refinement(e, NULL, NULL, NULL);
+	for (int k = 0; k < e->n_extra; ++k) {
+		struct dataset *ds = e->extra[k];
+		struct detector *dt = &e->dets[k + 1];
+		free(ds->ones); free(ds->multi); free(ds->ones_accum); free(ds->multi_accum);
+		free(ds->place_ones); free(ds->place_multi); free(ds->count_multi);
+		free(ds);
+		free(dt->qvals); free(dt->corr); free(dt->raw_mask);
+	}
+	free(e->extra);
+	free(e->dets);
+	free(e->det_map);
 	free(e);
 }
 

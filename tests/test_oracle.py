@@ -180,3 +180,51 @@ def test_legacy_engine_driver_agrees_with_packaged_engine(oracle_built):
     finally:
         leg.close()
         ref.close()
+
+
+def _two_detector_problems(seed, **kw):
+    from dragonfly_b200 import synth
+    dets, sh = synth.two_detector_problem(seed=seed)
+    probs = []
+    for k, d in enumerate(dets):
+        scale = None
+        if kw.get("known_scale"):
+            scale = np.random.default_rng(seed + k).uniform(0.5, 1.5, d["ones"].size)
+        probs.append(EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"],
+                                d["place_multi"], d["count_multi"], sh["quats"], sh["model_start"], scale=scale,
+                                **kw))
+    return probs
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference sources not compiled here")
+@pytest.mark.parametrize("seed,prob_kw", [
+    (21, dict(beta=1.)),
+    (22, dict(beta=0.05, beta_jump=2., beta_period=1, need_scaling=1, update_scale=1)),
+    (23, dict(beta=0.3, need_scaling=1, update_scale=0, known_scale=1)),
+])
+def test_oracle_two_detectors_match_live_reference(seed, prob_kw, oracle_built):
+    """Two detectors of different geometry and pixel count, each with its own
+    dataset (the reference's in_detector_list: u, rescale, psum_r and the
+    tomograms per detector, merges per orientation in detector order): the
+    oracle against the reference engine run with both detectors, bit for
+    bit, over three iterations."""
+    p0, p1 = _two_detector_problems(seed, **prob_kw)
+    ref = ReferenceEngine(p0, num_threads=1)
+    ref.add_detector(p1)
+    orc = OracleEngine(p0, extra=[p1])
+    assert ref.num_data == orc.det_of.size == p0.num_data + p1.num_data
+    for it in (1, 2, 3):
+        a = ref.run_iteration(it)
+        b = orc.run_iteration(it)
+        for k in ("avg_likelihood", "mutual_info", "rms_change"):
+            assert a[k] == b[k], k
+        np.testing.assert_array_equal(a["rescale_det"], b["rescale_det"])
+        np.testing.assert_array_equal(a["mean_count_det"], b["mean_count_det"])
+        np.testing.assert_array_equal(a["u_det"], b["u_det"])
+        for k in ("rmax", "info", "likelihood", "max_exp", "p_norm", "psum_d", "model1", "model2", "beta"):
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+        if p0.need_scaling:
+            np.testing.assert_array_equal(a["scale"], b["scale"])
+    # the two detectors see different things: their rescale factors differ
+    assert abs(b["rescale_det"][0] - b["rescale_det"][1]) > 1e-3 * abs(b["rescale_det"][0])
+    ref.close()
