@@ -79,6 +79,13 @@ _SIGS = {
     "dfg_batch_set_lanes": (C.c_int, [_V, C.c_int]),
     "dfg_batch_stats": (C.c_int, [_V, C.POINTER(C.c_long)]),
     "dfg_batch_destroy": (None, [_V]),
+    "dfg_group_create": (C.c_int, [C.POINTER(_V), C.c_int, C.POINTER(_V)]),
+    "dfg_group_destroy": (None, [_V]),
+    "dfg_group_last_error": (C.c_char_p, [_V]),
+    "dfg_group_maximize": (C.c_int, [_V, C.POINTER(IterParams), _D]),
+    "dfg_group_update_model": (C.c_int, [_V, C.c_double, _D]),
+    "dfg_group_normalize_scale": (C.c_int, [_V, _D]),
+    "dfg_group_run_iteration": (C.c_int, [_V, C.POINTER(IterParams), C.c_double, _D]),
     "dfg_pnet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_V)]),
     "dfg_pnet_destroy": (None, [_V]),
     "dfg_pnet_last_error": (C.c_char_p, [_V]),
@@ -646,6 +653,67 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             self.lib.dfg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DetectorGroup:
+    """Several detectors in one reconstruction (dfg_group_*): one Context per
+    detector holding that detector and the frames it sees, all with the same
+    orientations, model and parameters. The model lives in member 0."""
+
+    def __init__(self, contexts):
+        self.lib = load()
+        self.contexts = list(contexts)
+        arr = (_V * len(self.contexts))(*[c.h for c in self.contexts])
+        h = _V()
+        rc = self.lib.dfg_group_create(arr, len(self.contexts), C.byref(h))
+        if rc != DFG_OK:
+            raise DFGError(rc, "dfg_group_create failed")
+        self.h = h
+
+    def call(self, name, *args):
+        rc = getattr(self.lib, name)(self.h, *args)
+        if rc != DFG_OK:
+            raise DFGError(rc, "%s: %s" % (name, self.lib.dfg_group_last_error(self.h).decode()))
+
+    def maximize(self, par):
+        ll = C.c_double(0.)
+        self.call("dfg_group_maximize", C.byref(par), C.byref(ll))
+        return ll.value
+
+    def update_model(self, alpha=0.):
+        rms = C.c_double(0.)
+        self.call("dfg_group_update_model", float(alpha), C.byref(rms))
+        return rms.value
+
+    def normalize_scale(self):
+        m = C.c_double(0.)
+        self.call("dfg_group_normalize_scale", C.byref(m))
+        return m.value
+
+    def run_iteration(self, par, alpha=0.):
+        """As Context.run_iteration, over all detectors."""
+        out = np.zeros(5)
+        self.call("dfg_group_run_iteration", C.byref(par), float(alpha), ptr(out, C.c_double))
+        return dict(zip(("avg_likelihood", "rms_change", "mutual_info", "rescale", "mean_scale"), out.tolist()))
+
+    def model(self):
+        return self.contexts[0].model()
+
+    def frame_results(self):
+        """Per-frame results of all members, member 0's frames first."""
+        parts = [c.frame_results() for c in self.contexts]
+        return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dfg_group_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -3064,6 +3064,229 @@ extern "C" int dfg_run_iteration_host(dfg_ctx *ctx, const dfg_iter_params *par, 
 }
 
 // ---------------------------------------------------------------------------
+// several detectors in one reconstruction
+// ---------------------------------------------------------------------------
+// Iterate with an in_detector_list (iterate.pyx:432-456): member k is a
+// context holding detector k and the frames it sees. The reference's
+// per-detector quantities (u, rescale, psum_r, the tomograms: max_prob.c:
+// 31-60, max_update.c:33-36, 55-128, 153-229) live in the members; what the
+// detectors share is the model: the merged sums of every member are added
+// into member 0's (the reference merges all detectors into one model2 /
+// inter_weight), member 0 updates the model and every member gets a copy.
+// Frame-wide quantities (average log-likelihood, mutual information, the
+// mean scale of normalize_scale) are taken over the frames of all members.
+struct dfg_group {
+	std::vector<dfg_ctx *> m;
+	std::string err;
+	bool have_results = false;
+	double avg_ll = 0., mutual_info = 0., rms = 0.;
+	int fail(int code, const char *fmt, ...) {
+		char buf[1024];
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(buf, sizeof(buf), fmt, ap);
+		va_end(ap);
+		err = buf;
+		return code;
+	}
+};
+
+#define GNEED(cond, code, ...)                  \
+	do {                                        \
+		if (!(cond))                            \
+			return g->fail(code, __VA_ARGS__);  \
+	} while (0)
+#define GCK(call)                                                                                   \
+	do {                                                                                            \
+		cudaError_t e_ = (call);                                                                    \
+		if (e_ != cudaSuccess)                                                                      \
+			return g->fail(DFG_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+	} while (0)
+
+extern "C" void dfg_group_destroy(dfg_group *g) { delete g; }
+
+extern "C" const char *dfg_group_last_error(const dfg_group *g) { return g ? g->err.c_str() : "null group"; }
+
+extern "C" int dfg_group_create(dfg_ctx *const *members, int n, dfg_group **out) {
+	if (!members || n < 1 || !out)
+		return DFG_ERR_ARG;
+	*out = nullptr;
+	for (int i = 0; i < n; ++i)
+		if (!members[i])
+			return DFG_ERR_ARG;
+	dfg_group *g = new dfg_group;
+	g->m.assign(members, members + n);
+	*out = g;
+	return DFG_OK;
+}
+
+// The members must agree on everything but their detector and frames.
+static int group_check(dfg_group *g) {
+	dfg_ctx *a = g->m[0];
+	for (size_t k = 0; k < g->m.size(); ++k) {
+		dfg_ctx *c = g->m[k];
+		GNEED(c->device == a->device, DFG_ERR_ARG, "detector %d: another device", (int)k);
+		GNEED(c->P > 0 && c->N > 0, DFG_ERR_STATE, "detector %d: set detector and frames", (int)k);
+		GNEED(c->S > 0 && c->S == a->S && c->M == a->M && c->model_type == a->model_type, DFG_ERR_ARG,
+		      "detector %d: the model must have the same shape and type as detector 0's", (int)k);
+		GNEED(c->num_rot == a->num_rot, DFG_ERR_ARG, "detector %d: another orientation count", (int)k);
+		GNEED(c->refine == a->refine, DFG_ERR_ARG, "detector %d: refinement on some detectors only", (int)k);
+		// the background-aware updates couple the detectors (scalemax over
+		// all frames, mean_count averaged over the detectors: max_update.c:
+		// 350-356); not built for several detectors
+		GNEED(!c->with_bg || g->m.size() == 1, DFG_ERR_ARG,
+		      "background-aware updates with several detectors are not supported");
+		for (size_t j = 0; j < k; ++j)
+			GNEED(g->m[j] != c, DFG_ERR_ARG, "detector %d repeats detector %d", (int)k, (int)j);
+	}
+	return DFG_OK;
+}
+
+extern "C" int dfg_group_maximize(dfg_group *g, const dfg_iter_params *par, double *avg_likelihood) {
+	if (!g || !par)
+		return DFG_ERR_ARG;
+	if (int rc = group_check(g))
+		return rc;
+	dfg_ctx *m0 = g->m[0];
+	GCK(cudaSetDevice(m0->device));
+	// every member's iteration on its own stream
+	for (size_t k = 0; k < g->m.size(); ++k) {
+		dfg_ctx *c = g->m[k];
+		if (int rc = max_prepare(c, par))
+			return g->fail(rc, "detector %d: %s", (int)k, c->err.c_str());
+		if (int rc = max_enqueue(c, par))
+			return g->fail(rc, "detector %d: %s", (int)k, c->err.c_str());
+	}
+	double sum_mi = 0., sum_ll = 0.;
+	long long n = 0;
+	std::vector<double> h(3 * g->m.size());
+	for (size_t k = 0; k < g->m.size(); ++k) {
+		dfg_ctx *c = g->m[k];
+		int derr = 0;
+		GCK(cudaMemcpyAsync(&h[3 * k], c->scalars.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+		if (c->dense_active || c->m_dense_active)
+			GCK(cudaMemcpyAsync(&derr, c->derr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+		GCK(cudaStreamSynchronize(c->stream));
+		phase_collect(c);
+		GNEED(derr == 0, DFG_ERR_CUDA, "detector %d: dense E-step / M-step: a pipeline wait gave up", (int)k);
+		max_finish(c, &h[3 * k]);
+		sum_mi += h[3 * k + 1];
+		sum_ll += h[3 * k + 2];
+		n += c->N;
+	}
+	// one model: the other members' merged sums added into member 0's
+	const long long mv = (long long)m0->M * m0->V;
+	for (size_t k = 1; k < g->m.size(); ++k) {
+		add_into_kernel<<<blocks_for(mv, 256), 256, 0, m0->stream>>>(m0->model2.p, g->m[k]->model2.p, mv);
+		add_into_kernel<<<blocks_for(mv, 256), 256, 0, m0->stream>>>(m0->weight.p, g->m[k]->weight.p, mv);
+		GCK(cudaGetLastError());
+	}
+	GCK(cudaStreamSynchronize(m0->stream));
+	g->mutual_info = sum_mi / (double)n;
+	g->avg_ll = sum_ll / (double)n;
+	g->have_results = true;
+	if (avg_likelihood)
+		*avg_likelihood = g->avg_ll;
+	return DFG_OK;
+}
+
+// member 0's model to the others (after an update or a scale normalisation)
+static int group_share_model(dfg_group *g) {
+	dfg_ctx *m0 = g->m[0];
+	const size_t n = (size_t)m0->M * m0->V;
+	for (size_t k = 1; k < g->m.size(); ++k)
+		GCK(cudaMemcpyAsync(g->m[k]->model1.p, m0->model1.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
+		                    m0->stream));
+	GCK(cudaStreamSynchronize(m0->stream));
+	return DFG_OK;
+}
+
+extern "C" int dfg_group_update_model(dfg_group *g, double alpha, double *rms_change) {
+	if (!g)
+		return DFG_ERR_ARG;
+	GNEED(g->have_results, DFG_ERR_STATE, "update_model: run dfg_group_maximize first");
+	dfg_ctx *m0 = g->m[0];
+	if (int rc = dfg_update_model(m0, alpha, &g->rms))
+		return g->fail(rc, "%s", m0->err.c_str());
+	if (int rc = group_share_model(g))
+		return rc;
+	if (rms_change)
+		*rms_change = g->rms;
+	return DFG_OK;
+}
+
+// normalize_scale over the frames of all detectors (iterate.pyx:361-384):
+// the mean of the good frames' scale factors divides each member's factors;
+// member 0's model (mode 0) is multiplied by it and shared.
+extern "C" int dfg_group_normalize_scale(dfg_group *g, double *mean_scale) {
+	if (!g)
+		return DFG_ERR_ARG;
+	if (int rc = group_check(g))
+		return rc;
+	dfg_ctx *m0 = g->m[0];
+	GCK(cudaSetDevice(m0->device));
+	double tot[2] = {0., 0.};
+	for (dfg_ctx *c : g->m) {
+		GCK(c->scalars.ensure(8));
+		scale_sum_kernel<<<1, 1024, 0, c->stream>>>(c->scale.p, c->blacklist.p, c->N, c->scalars.p + 4);
+		GCK(cudaGetLastError());
+		double h[2];
+		GCK(cudaMemcpyAsync(h, c->scalars.p + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+		GCK(cudaStreamSynchronize(c->stream));
+		tot[0] += h[0];
+		tot[1] += h[1];
+	}
+	GNEED(tot[1] > 0, DFG_ERR_STATE, "normalize_scale: no good frames");
+	for (size_t k = 0; k < g->m.size(); ++k) {
+		dfg_ctx *c = g->m[k];
+		GCK(cudaMemcpyAsync(c->scalars.p + 4, tot, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+		const long long V = k == 0 ? m0->V : 0;  // the model once, in member 0
+		const long long nn = std::max<long long>(V, c->N);
+		apply_scale_norm_kernel<<<blocks_for(nn, 256), 256, 0, c->stream>>>(c->scale.p, c->blacklist.p, c->N,
+		                                                                   c->model1.p, nullptr, V, c->scalars.p + 4);
+		GCK(cudaGetLastError());
+		GCK(cudaStreamSynchronize(c->stream));
+	}
+	if (int rc = group_share_model(g))
+		return rc;
+	const double mean = tot[0] / tot[1];
+	g->rms *= mean;
+	for (dfg_ctx *c : g->m)
+		c->rms = g->rms;
+	if (mean_scale)
+		*mean_scale = mean;
+	return DFG_OK;
+}
+
+// One iteration over all detectors: maximize, update_model and, when
+// need_scaling (volumes only, recon.pyx:102-103), normalize_scale. out[5]:
+// average log-likelihood, rms change, mutual information, detector 0's
+// rescale factor, mean scale (1 without normalisation).
+extern "C" int dfg_group_run_iteration(dfg_group *g, const dfg_iter_params *par, double alpha, double *out) {
+	if (!g || !par)
+		return DFG_ERR_ARG;
+	if (int rc = dfg_group_maximize(g, par, nullptr))
+		return rc;
+	if (int rc = dfg_group_update_model(g, alpha, nullptr))
+		return rc;
+	double mean = 1.;
+	if (iteration_normalizes(g->m[0], par))
+		if (int rc = dfg_group_normalize_scale(g, &mean))
+			return rc;
+	if (out) {
+		out[0] = g->avg_ll;
+		out[1] = g->rms;
+		out[2] = g->mutual_info;
+		out[3] = g->m[0]->rescale;
+		out[4] = mean;
+	}
+	return DFG_OK;
+}
+
+#undef GNEED
+#undef GCK
+
+// ---------------------------------------------------------------------------
 // results
 // ---------------------------------------------------------------------------
 template <typename T>

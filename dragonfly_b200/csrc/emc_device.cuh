@@ -1639,6 +1639,13 @@ __global__ void __launch_bounds__(1024) scale_sum_kernel(const double *__restric
 	}
 }
 
+// a[i] += b[i]: one detector's merged sums into the shared model's.
+__global__ void add_into_kernel(double *__restrict__ a, const double *__restrict__ b, long long n) {
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+		a[i] += b[i];
+}
+
 // phi /= mean for good frames; model1 of mode 0 *= mean (iterate.pyx:372-382);
 // mean = sums[0] / sums[1] (sum and count of good frames' phi); nothing
 // changes without good frames (the host reports that case).

@@ -427,7 +427,7 @@ struct GemmCfg {
 
 // C[M][N] = act(A B^T + bias) for A [M][K] and B [N][K] in BF16 (K a multiple
 // of 64; both read by TMA with the 128-byte swizzle, rows past M or N read as
-// zero), accumulated in FP32 in TMEM. One CTA per 128 x BN tile: warp 0
+// zero; bias may be null), accumulated in FP32 in TMEM. One CTA per 128 x BN tile: warp 0
 // issues the TMA loads (GSTAGES-deep ring), warp 1 the MMAs (and owns the
 // TMEM allocation), warps 2-5 read their 32 TMEM lanes, add the bias, apply
 // the ReLU and store FP32 rows. Every wait gives up after wait_cycles clock
@@ -439,8 +439,16 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
                                                               const __grid_constant__ CUtensorMap map_b, int num_kb,
                                                               int M, int N, const float *__restrict__ bias, int relu,
                                                               float *__restrict__ C, int ldc, int *__restrict__ err,
-                                                              long long wait_cycles, int withhold_kb) {
+                                                              long long wait_cycles, int withhold_kb,
+                                                              int kb_split = 0) {
 	using G = GemmCfg<BN>;
+	// split-k (kb_split > 0): CTA z takes K blocks [z kb_split, +kb_split)
+	// and writes its partial product to C + z M ldc (every split has at
+	// least one block: the grid has ceil(num_kb / kb_split) of them)
+	const int kb0 = kb_split > 0 ? (int)blockIdx.z * kb_split : 0;
+	const int nkb = kb_split > 0 ? min(kb_split, num_kb - kb0) : num_kb;
+	if (kb_split > 0)
+		C += (size_t)blockIdx.z * M * ldc;
 	extern __shared__ uint8_t gsm_raw[];
 	uint8_t *sm = (uint8_t *)(((uintptr_t)gsm_raw + 1023) & ~(uintptr_t)1023);
 	uint64_t *bars = (uint64_t *)(sm + GSTAGES * G::STAGE);
@@ -471,7 +479,7 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 	if (warp == 0) {
 		if (lane == 0) {
 			int issued = 0;
-			for (int kb = 0; kb < num_kb; ++kb) {
+			for (int kb = 0; kb < nkb; ++kb) {
 				const int s = kb % GSTAGES;
 				const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
 				if (*abort_flag || !mbar_wait(&empty[s], ph ^ 1u, wait_cycles)) {
@@ -483,8 +491,8 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 					continue;
 				uint8_t *st = sm + s * G::STAGE;
 				mbar_expect_tx(&full[s], G::STAGE);
-				tma_load_2d(st, &map_a, &full[s], kb * GK, mt * 128);
-				tma_load_2d(st + G::A_BYTES, &map_b, &full[s], kb * GK, nt * BN);
+				tma_load_2d(st, &map_a, &full[s], (kb0 + kb) * GK, mt * 128);
+				tma_load_2d(st + G::A_BYTES, &map_b, &full[s], (kb0 + kb) * GK, nt * BN);
 				issued = kb + 1;
 			}
 			// on a give-up, let the copies still in flight land before exiting
@@ -495,7 +503,7 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 		__syncwarp();
 	} else if (warp == 1) {
 		if (lane == 0) {
-			for (int kb = 0; kb < num_kb; ++kb) {
+			for (int kb = 0; kb < nkb; ++kb) {
 				const int s = kb % GSTAGES;
 				const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
 				if (*abort_flag || !mbar_wait(&full[s], ph, wait_cycles)) {
@@ -531,7 +539,7 @@ __global__ void __launch_bounds__(192, 1) pnet_gemm_tc_kernel(const __grid_const
 					for (int j = 0; j < 16; ++j) {
 						const int col = nt * BN + c * 16 + j;
 						if (col < N) {
-							const float x = v[j] + bias[col];
+							const float x = bias != nullptr ? v[j] + bias[col] : v[j];
 							C[(size_t)row * ldc + col] = relu ? fmaxf(x, 0.f) : x;
 						}
 					}
@@ -658,6 +666,44 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int *__r
 		lab_out[e] = lab[idx[e]];
 }
 
+// Y[c][r] = bf16(X[r][c]) for r < rows, 0 for rows <= r < rows_p: a 32 x 32
+// tile through shared memory per block (coalesced reads of X's rows and
+// writes of Y's rows). Grid: ceil(cols / 32) x ceil(rows_p / 32), 32 x 8
+// threads.
+template <typename T>
+__global__ void transpose_bf16_kernel(const T *__restrict__ X, long long rows, int cols, long long rows_p,
+                                      __nv_bfloat16 *__restrict__ Y) {
+	__shared__ float tile[32][33];
+	const int c0 = blockIdx.x * 32;
+	const long long r0 = (long long)blockIdx.y * 32;
+	for (int k = threadIdx.y; k < 32; k += 8) {
+		const long long r = r0 + k;
+		const int c = c0 + threadIdx.x;
+		float v = 0.f;
+		if (r < rows && c < cols)
+			v = (float)X[r * cols + c];
+		tile[k][threadIdx.x] = v;
+	}
+	__syncthreads();
+	for (int k = threadIdx.y; k < 32; k += 8) {
+		const int c = c0 + k;
+		const long long r = r0 + threadIdx.x;
+		if (c < cols && r < rows_p)
+			Y[(size_t)c * rows_p + r] = __float2bfloat16(tile[threadIdx.x][k]);
+	}
+}
+
+// Wt[k][c] = W[c][k] for a BF16 weight matrix W [cout][K], c padded with
+// zeros to coutp: the B operand of the input-gradient product.
+__global__ void transpose_pad_weights_kernel(const __nv_bfloat16 *__restrict__ W, int cout, int K, int coutp,
+                                             __nv_bfloat16 *__restrict__ Wt) {
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= (long long)K * coutp)
+		return;
+	const int k = (int)(i / coutp), c = (int)(i % coutp);
+	Wt[i] = c < cout ? W[(size_t)c * K + k] : __float2bfloat16(0.f);
+}
+
 struct dfg_pnet {
 	int device = 0;
 	cudaStream_t stream = nullptr;
@@ -678,6 +724,13 @@ struct dfg_pnet {
 	// tensor-core inference: BF16 operands with K padded to 64, error flag
 	bool use_tc = true;
 	DevBuf<__nv_bfloat16> colsb, wbp[NL];
+	// tensor-core training (mixed precision): every layer's BF16 input rows
+	// of the training batch (kept for its weight gradient), the transposed
+	// operands of the gradient products, BF16 output gradients, transposed
+	// padded weights and split-k partials
+	bool tc_train = true;
+	DevBuf<__nv_bfloat16> colsbl[NL], dyt, colst, dyb, wtp[NL];
+	DevBuf<float> tsplit;
 	DevBuf<int> terr;
 	// failure-detection test hooks of the tensor-core products (as the
 	// context's dense_wait_cycles / dense_withhold_stage options)
@@ -942,6 +995,189 @@ static int backward(dfg_pnet *net, const float *X, const int *lab, int n, const 
 	return DFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// tensor-core training: mixed precision (BF16 operands, FP32 accumulation)
+// ---------------------------------------------------------------------------
+// C[M][N] (row stride N) = A[M][Kp] B[N][Kp]^T (+ bias, ReLU) on the tensor
+// cores; when the (M, N) tiles alone would leave most SMs idle, the K blocks
+// are split over a third grid dimension and the partial products summed in
+// split order (deterministic).
+static long long round128(long long m) { return (m + 127) / 128 * 128; }
+
+static int tc_product(dfg_pnet *net, const __nv_bfloat16 *A, long long M, int Kp, const __nv_bfloat16 *B, int N,
+                      float *C, const float *bias, int relu) {
+	// A holds round128(M) rows (the rows past M are never stored), so that
+	// every 128-row box lies inside the tensor
+	const int BN = N <= 32 ? 32 : (N <= 64 ? 64 : 256);
+	const int num_kb = Kp / GK;
+	const long long tiles = ((M + 127) / 128) * (long long)((N + BN - 1) / BN);
+	int S = (int)std::max<long long>(1, std::min<long long>(num_kb, 296 / std::max<long long>(1, tiles)));
+	const int kbs = (num_kb + S - 1) / S;
+	S = (num_kb + kbs - 1) / kbs;  // every split holds at least one K block
+	if (S > 1 && (size_t)S * M * N > net->tsplit.n)
+		PK(net->tsplit.ensure((size_t)S * M * N));
+	CUtensorMap ma, mb;
+	if (int rc = pnet_map(net, &ma, A, round128(M), Kp, 128))
+		return rc;
+	if (int rc = pnet_map(net, &mb, B, N, Kp, BN))
+		return rc;
+	float *out = S > 1 ? net->tsplit.p : C;
+	const float *b = S > 1 ? nullptr : bias;
+	const int rl = S > 1 ? 0 : relu;
+	dim3 grid((unsigned)((M + 127) / 128), (unsigned)((N + BN - 1) / BN), (unsigned)S);
+#define DFG_TC(BNV)                                                                                           \
+	pnet_gemm_tc_kernel<BNV><<<grid, 192, GemmCfg<BNV>::SMEM, net->stream>>>(                                 \
+	    ma, mb, num_kb, (int)M, N, b, rl, out, N, net->terr.p, net->wait_cycles, net->withhold, S > 1 ? kbs : 0)
+	if (BN == 32)
+		DFG_TC(32);
+	else if (BN == 64)
+		DFG_TC(64);
+	else
+		DFG_TC(256);
+#undef DFG_TC
+	PKL("pnet_gemm_tc_kernel");
+	if (S > 1) {
+		sum_splits_kernel<<<grid_for(M * N), 256, 0, net->stream>>>(net->tsplit.p, S, M * N, C);
+		PKL("sum_splits_kernel");
+		if (bias != nullptr) {
+			bias_act_kernel<<<grid_for(M * N), 256, 0, net->stream>>>(C, M, N, bias, relu);
+			PKL("bias_act_kernel");
+		}
+	}
+	return DFG_OK;
+}
+
+// The BF16 copies of the current weights the tensor-core products read: K
+// padded to 64 (forward) and transposed with the outputs padded to 64 (input
+// gradients).
+static int refresh_tc_weights(dfg_pnet *net) {
+	if (int rc = pad_weights(net))
+		return rc;
+	for (int l = 1; l < NL; ++l) {
+		const LayerShape &sh = net->L[l];
+		const int K = sh.fan_in(), cp = kpad64(sh.cout);
+		transpose_pad_weights_kernel<<<grid_for((long long)K * cp), 256, 0, net->stream>>>(net->wb[l].p, sh.cout,
+		                                                                                    K, cp, net->wtp[l].p);
+		PKL("transpose_pad_weights_kernel");
+	}
+	return DFG_OK;
+}
+
+// Training forward pass of n <= batch images: layer 0 as the FP32 path (its
+// im2col rows kept for its weight gradient), layers 1-5 as tensor-core
+// products of BF16 input rows (kept per layer) and the padded weights;
+// FP32 outputs in act.
+static int forward_train_tc(dfg_pnet *net, const float *X, int n) {
+	cudaStream_t st = net->stream;
+	const LayerShape &s0 = net->L[0];
+	const long long rows0 = net->rows(0, n);
+	im2col_kernel<<<grid_for(rows0 * 9 * s0.cin), 256, 0, st>>>(X, n, s0.hin, s0.cin, s0.stride, s0.hout,
+	                                                           net->cols[0].p);
+	PKL("im2col_kernel");
+	conv0_kernel<<<grid_for((long long)n * IMG * IMG), 256, 0, st>>>(X, n, net->wb[0].p, net->b[0].p, net->act[1].p);
+	PKL("conv0_kernel");
+	for (int l = 1; l < NL; ++l) {
+		const LayerShape &s = net->L[l];
+		const long long rows = net->rows(l, n);
+		const int K = s.fan_in(), Kp = kpad64(K);
+		const float *in = net->act[l].p;
+		if (s.kind == 0) {
+			im2col_bf16_kernel<<<grid_for(rows * Kp / 8), 256, 0, st>>>(in, n, s.hin, s.cin, s.stride, s.hout, Kp,
+			                                                            net->colsbl[l].p);
+			PKL("im2col_bf16_kernel");
+		} else {
+			rows_bf16_kernel<<<grid_for(rows * Kp), 256, 0, st>>>(in, rows, K, Kp, net->colsbl[l].p);
+			PKL("rows_bf16_kernel");
+		}
+		if (int rc = tc_product(net, net->colsbl[l].p, rows, Kp, net->wbp[l].p, s.cout, net->act[l + 1].p,
+		                        net->b[l].p, l < NL - 1))
+			return rc;
+	}
+	return DFG_OK;
+}
+
+// Gradients of the training forward pass: per layer the FP32 output
+// gradient (ReLU mask, bias gradient as the FP32 path), then in BF16 on the
+// tensor cores the weight gradient dW = dY^T X (dY and the layer's BF16
+// input rows transposed so that the batch's rows are the reduction, split-k)
+// and the input gradient dX = dY W (dY rows against the transposed weights);
+// layer 0's weight gradient (K = 9) stays on the FP32 path.
+static int backward_tc(dfg_pnet *net, const float *X, const int *lab, int n, const int *img) {
+	cudaStream_t st = net->stream;
+	(void)X;
+	if (lab != nullptr) {
+		softmax_xent_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(net->act[NL].p, lab, n, net->num_classes,
+		                                                          net->dact[NL].p, net->loss.p);
+		PKL("softmax_xent_kernel");
+	} else {
+		softmax_xent_soft_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(
+		    net->act[NL].p, img, net->t_off.p, net->t_cls.p, net->t_w.p, n, net->num_classes, net->dact[NL].p,
+		    net->loss.p);
+		PKL("softmax_xent_soft_kernel");
+	}
+	for (int l = NL - 1; l >= 0; --l) {
+		const LayerShape &s = net->L[l];
+		const long long rows = net->rows(l, n);
+		float *dY = net->dact[l + 1].p;
+		if (l < NL - 1) {
+			relu_back_kernel<<<grid_for(rows * s.cout), 256, 0, st>>>(dY, net->act[l + 1].p, rows * s.cout);
+			PKL("relu_back_kernel");
+		}
+		bias_grad_kernel<<<s.cout, 256, 0, st>>>(dY, rows, s.cout, net->gb[l].p);
+		PKL("bias_grad_kernel");
+		if (l == 0) {
+			if (int rc = gemm_wgrad(net, s.cout, 9 * s.cin, (int)rows, dY, net->cols[0].p, net->gw[0].p))
+				return rc;
+			continue;
+		}
+		const int K = s.fan_in(), Kp = kpad64(K), cp = kpad64(s.cout);
+		const long long rows_p = (rows + 63) / 64 * 64;
+		// dW [cout][K] = dY^T X: both operands with the batch rows as the reduction
+		dim3 tb(32, 8);
+		transpose_bf16_kernel<float><<<dim3((s.cout + 31) / 32, (unsigned)(rows_p / 32)), tb, 0, st>>>(
+		    dY, rows, s.cout, rows_p, net->dyt.p);
+		PKL("transpose_bf16_kernel");
+		transpose_bf16_kernel<__nv_bfloat16><<<dim3((Kp + 31) / 32, (unsigned)(rows_p / 32)), tb, 0, st>>>(
+		    net->colsbl[l].p, rows, Kp, rows_p, net->colst.p);
+		PKL("transpose_bf16_kernel");
+		if (int rc = tc_product(net, net->dyt.p, s.cout, (int)rows_p, net->colst.p, K, net->gw[l].p, nullptr, 0))
+			return rc;
+		// dX = dY W: dY rows in BF16 (outputs padded to 64) against W^T
+		rows_bf16_kernel<<<grid_for(rows * cp), 256, 0, st>>>(dY, rows, s.cout, cp, net->dyb.p);
+		PKL("rows_bf16_kernel");
+		if (s.kind == 0) {
+			if (int rc = tc_product(net, net->dyb.p, rows, cp, net->wtp[l].p, K, net->dcols[l].p, nullptr, 0))
+				return rc;
+			const long long nx = (long long)n * s.hin * s.hin * s.cin;
+			col2im_kernel<<<grid_for(nx), 256, 0, st>>>(net->dcols[l].p, n, s.hin, s.cin, s.stride, s.hout,
+			                                             net->dact[l].p);
+			PKL("col2im_kernel");
+		} else {
+			if (int rc = tc_product(net, net->dyb.p, rows, cp, net->wtp[l].p, K, net->dact[l].p, nullptr, 0))
+				return rc;
+		}
+	}
+	return DFG_OK;
+}
+
+static int check_tc_flag(dfg_pnet *net);
+
+// Loss and gradients of one training batch: on the tensor cores (BF16
+// operands from the current weights) or on the FP32 path. The products'
+// pipeline flag is read by the caller at its next synchronisation.
+static int train_pass(dfg_pnet *net, const float *X, const int *lab, int m, const int *img) {
+	if (net->tc_train) {
+		if (int rc = refresh_tc_weights(net))
+			return rc;
+		if (int rc = forward_train_tc(net, X, m))
+			return rc;
+		return backward_tc(net, X, lab, m, img);
+	}
+	if (int rc = forward(net, X, m))
+		return rc;
+	return backward(net, X, lab, m, img);
+}
+
 static int adam_step(dfg_pnet *net, float lr) {
 	const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
 	net->step++;
@@ -1060,6 +1296,31 @@ extern "C" int dfg_pnet_create(int device, int num_classes, int batch, unsigned 
 	}
 	if (net->colsb.ensure((size_t)cb) != cudaSuccess || net->terr.ensure(1) != cudaSuccess)
 		return bad(DFG_ERR_NOMEM);
+	// tensor-core training: per layer the BF16 input rows of a training batch
+	// and the transposed padded weights; the transposed output gradients (the
+	// output count padded to 128 rows, zero past it), transposed input rows
+	// and BF16 output gradients of the largest layer
+	{
+		long long dyt = 0, colst = 0, dyb = 0;
+		for (int l = 1; l < NL; ++l) {
+			const LayerShape &sh = net->L[l];
+			const int K = sh.fan_in(), Kp = kpad64(K), cp = kpad64(sh.cout);
+			const long long rows = net->rows(l, batch), rows_p = (rows + 63) / 64 * 64;
+			if (net->colsbl[l].ensure((size_t)round128(rows) * Kp) != cudaSuccess ||
+			    net->wtp[l].ensure((size_t)K * cp) != cudaSuccess)
+				return bad(DFG_ERR_NOMEM);
+			dyt = std::max(dyt, round128(sh.cout) * rows_p);
+			colst = std::max(colst, (long long)Kp * rows_p);
+			dyb = std::max(dyb, round128(rows) * cp);
+		}
+		if (net->dyt.ensure((size_t)dyt) != cudaSuccess || net->colst.ensure((size_t)colst) != cudaSuccess ||
+		    net->dyb.ensure((size_t)dyb) != cudaSuccess)
+			return bad(DFG_ERR_NOMEM);
+		cudaMemsetAsync(net->dyt.p, 0, (size_t)dyt * sizeof(__nv_bfloat16), net->stream);
+		for (int l = 1; l < NL; ++l)
+			cudaMemsetAsync(net->colsbl[l].p, 0, net->colsbl[l].n * sizeof(__nv_bfloat16), net->stream);
+		cudaMemsetAsync(net->dyb.p, 0, (size_t)dyb * sizeof(__nv_bfloat16), net->stream);
+	}
 	cudaMemsetAsync(net->terr.p, 0, sizeof(int), net->stream);
 	if (net->loss_acc.ensure(1) != cudaSuccess)
 		return bad(DFG_ERR_NOMEM);
@@ -1087,6 +1348,10 @@ extern "C" int dfg_pnet_set_option(dfg_pnet *net, const char *key, double value)
 		return DFG_ERR_ARG;
 	if (!strcmp(key, "tensor_cores"))
 		return dfg_pnet_set_tensor_cores(net, value != 0.);
+	if (!strcmp(key, "tensor_core_training")) {
+		net->tc_train = value != 0.;
+		return DFG_OK;
+	}
 	if (!strcmp(key, "wait_cycles")) {
 		if (!(value >= 1e4 && value <= 1e11))
 			return net->fail(DFG_ERR_ARG, "wait_cycles must be in [1e4, 1e11]");
@@ -1257,9 +1522,7 @@ extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, doub
 			    net->images.p, net->perm.p + b0, m, IMG * IMG, net->xbatch.p, labels ? net->lab_all.p : nullptr,
 			    net->labels.p);
 			PKL("gather_rows_kernel");
-			if (int rc = forward(net, net->xbatch.p, m))
-				return rc;
-			if (int rc = backward(net, net->xbatch.p, labels ? net->labels.p : nullptr, m, net->perm.p + b0))
+			if (int rc = train_pass(net, net->xbatch.p, labels ? net->labels.p : nullptr, m, net->perm.p + b0))
 				return rc;
 			if (int rc = adam_step(net, (float)lr))
 				return rc;
@@ -1269,6 +1532,9 @@ extern "C" int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, doub
 		double sum = 0.;
 		PK(cudaMemcpyAsync(&sum, net->loss_acc.p, sizeof(double), cudaMemcpyDeviceToHost, st));
 		PK(cudaStreamSynchronize(st));
+		if (net->tc_train)
+			if (int rc = check_tc_flag(net))
+				return rc;
 		last = sum / (double)n;
 	}
 	if (mean_loss)
@@ -1299,6 +1565,10 @@ static int for_batches(dfg_pnet *net, F fn) {
 static int check_tc(dfg_pnet *net) {
 	if (!net->use_tc)
 		return DFG_OK;
+	return check_tc_flag(net);
+}
+
+static int check_tc_flag(dfg_pnet *net) {
 	int e = 0;
 	PK(cudaMemcpyAsync(&e, net->terr.p, sizeof(int), cudaMemcpyDeviceToHost, net->stream));
 	PK(cudaStreamSynchronize(net->stream));
@@ -1361,9 +1631,7 @@ extern "C" int dfg_pnet_gradients(dfg_pnet *net, const int *labels, float *grads
 	const int m = (int)std::min<long long>(net->batch, net->n_images);
 	if (labels)
 		PK(cudaMemcpyAsync(net->labels.p, labels, m * sizeof(int), cudaMemcpyHostToDevice, net->stream));
-	if (int rc = forward(net, net->images.p, m))
-		return rc;
-	if (int rc = backward(net, net->images.p, labels ? net->labels.p : nullptr, m, net->iota.p))
+	if (int rc = train_pass(net, net->images.p, labels ? net->labels.p : nullptr, m, net->iota.p))
 		return rc;
 	size_t o = 0;
 	for (int l = 0; l < NL; ++l) {
@@ -1377,6 +1645,9 @@ extern "C" int dfg_pnet_gradients(dfg_pnet *net, const int *labels, float *grads
 	std::vector<float> loss((size_t)m);
 	PK(cudaMemcpyAsync(loss.data(), net->loss.p, m * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
 	PK(cudaStreamSynchronize(net->stream));
+	if (net->tc_train)
+		if (int rc = check_tc_flag(net))
+			return rc;
 	double s = 0.;
 	for (float v : loss)
 		s += v;

@@ -3,8 +3,10 @@ dragonfly/iterate.pyx:21-592).
 
 Holds the detector(s), the photon datasets, orientations, model, parameters
 and the per-frame arrays (fcounts, scale, beta, beta_start, sum_fact,
-blacklist) on the host; EMCRecon uploads them to the GPU. Supports one unique
-detector (the reference's multi-detector lists are not supported).
+blacklist) on the host; EMCRecon uploads them to the GPU. Several detectors
+(in_detector_list) map each dataset to one of the unique detectors as the
+reference's _gen_detlist does (iterate.pyx:432-456); the frames seen by
+detector k are member_frames(k) / member_index(k).
 """
 import configparser
 import ctypes
@@ -38,14 +40,17 @@ def ln_factorial(c):
     return _libm.lgamma(float(c) + 1.0)
 
 
-def frame_stats(dsets, mask):
+def frame_stats(dsets, mask, det_mapping=None, num_det=1):
     """fcounts, sum_fact and mean_count over mask == 0 pixels (calc_frame_counts
-    and calc_sum_fact, dragonfly/src/iterate.c:3-117; ln c! = lgamma(c + 1))."""
+    and calc_sum_fact, dragonfly/src/iterate.c:3-117; ln c! = lgamma(c + 1)).
+    mask: one array, or one per detector with det_mapping giving each
+    dataset's detector; mean_count is then per detector (an array)."""
     fc, sf = [], []
-    for d in dsets:
+    for i, d in enumerate(dsets):
+        m = mask if det_mapping is None else mask[det_mapping[i]]
         n = d.num_data
-        good1 = mask[d.place_ones] < 1
-        good_m = mask[d.place_multi] < 1
+        good1 = m[d.place_ones] < 1
+        good_m = m[d.place_multi] < 1
         fid1 = np.repeat(np.arange(n), d.ones)
         fidm = np.repeat(np.arange(n), d.multi)
         f = np.bincount(fid1[good1], minlength=n).astype(np.int64)
@@ -58,7 +63,16 @@ def frame_stats(dsets, mask):
         fc.append(f.astype(np.int32))
         sf.append(s)
     fcounts = np.concatenate(fc)
-    mean_count = float(np.cumsum(fcounts.astype(np.float64))[-1] / fcounts.size) if fcounts.size else 0.
+    if det_mapping is None:
+        mean_count = float(np.cumsum(fcounts.astype(np.float64))[-1] / fcounts.size) if fcounts.size else 0.
+        return fcounts, np.concatenate(sf), mean_count
+    # per detector: the sequential sum over its frames in dataset order
+    # (cumsum adds in order, as the reference's loop), then / count
+    mean_count = np.zeros(num_det)
+    for k in range(num_det):
+        parts = [f for i, f in enumerate(fc) if det_mapping[i] == k]
+        v = np.concatenate(parts).astype(np.float64) if parts else np.zeros(0)
+        mean_count[k] = np.cumsum(v)[-1] / v.size if v.size else 0.
     return fcounts, np.concatenate(sf), mean_count
 
 
@@ -107,27 +121,32 @@ class Iterate:
         det_fname, det_flist = chained("in_detector_file"), chained("in_detector_list")
         if det_fname is not None and det_flist is not None:
             raise ValueError("Both in_detector_file and in_detector_list specified. Pick one.")
-        if det_flist is not None:
-            raise NotImplementedError("multiple detectors (in_detector_list) are not supported")
-        if det_fname is None:
+        if det_fname is not None:
+            dets = [CDetector(op.join(folder, det_fname), norm=True, rtype=rtype)]
+        elif det_flist is not None:
+            with open(op.join(folder, det_flist)) as f:
+                dets = [CDetector(op.join(folder, ln.strip()), norm=True, rtype=rtype) for ln in f.readlines()]
+        else:
             raise ValueError("Need either in_detector_file or in_detector_list.")
-        det = CDetector(op.join(folder, det_fname), norm=True, rtype=rtype)
 
         ph_fname, ph_flist = chained("in_photons_file"), chained("in_photons_list")
         if ph_fname is not None and ph_flist is not None:
             raise ValueError("Both in_photons_file and in_photons_list specified. Pick one.")
         if ph_fname is not None:
-            frames = CDataset(op.join(folder, ph_fname), det)
+            if len(dets) > 1:
+                print("WARNING: Multiple detectors but only one photons file. Using first detector")
+            frames = CDataset(op.join(folder, ph_fname), dets[0])
         elif ph_flist is not None:
-            with open(ph_flist) as f:
-                fnames = [op.join(folder, ln.strip()) for ln in f if ln.strip()]
-            frames = CDataset(fnames[0], det)
-            for fn in fnames[1:]:
-                frames.append(CDataset(fn, det))
+            with open(op.join(folder, ph_flist)) as f:
+                fnames = [op.join(folder, ln.strip()) for ln in f.readlines()]
+            # file i is seen by detector i with a detector list, else by the one
+            frames = CDataset(fnames[0], dets[0])
+            for i, fn in enumerate(fnames[1:], 1):
+                frames.append(CDataset(fn, dets[i] if len(dets) > 1 else dets[0]))
         else:
             raise ValueError("Need either in_photons_file or in_photons_list.")
-        # per-pixel background (iterate.pyx:109-127); one detector here, so a
-        # background list must have one entry
+        # per-pixel background (iterate.pyx:109-127): one file, or a list with
+        # one entry per detector
         bg_file = config.get(section_name, "background_file", fallback=None)
         bg_list = config.get(section_name, "background_list", fallback=None)
         if bg_file is not None and bg_list is not None:
@@ -136,12 +155,14 @@ class Iterate:
             bg_list = op.join(folder, bg_list)
             with open(bg_list) as f:
                 lines = [ln.strip() for ln in f if ln.strip()]
-            if len(lines) != 1:
-                raise ValueError("Background list has %d entries but there are 1 unique detectors" % len(lines))
-            det.parse_background(op.join(op.dirname(bg_list), lines[0]))
+            if len(lines) != len(dets):
+                raise ValueError("Background list has %d entries but there are %d unique detectors"
+                                 % (len(lines), len(dets)))
+            for det, ln in zip(dets, lines):
+                det.parse_background(op.join(op.dirname(bg_list), ln))
         elif bg_file is not None:
-            det.parse_background(op.join(folder, bg_file))
-        self.dets = [det]
+            for det in dets:
+                det.parse_background(op.join(folder, bg_file))
         self.set_data(frames)
 
         quat = Quaternion()
@@ -176,8 +197,9 @@ class Iterate:
                 quat.voronoi_subset(param.coarse_div)
             self.parse_rel_quat(probs_file, quat.num_rot_coarse)
 
-        model = Model(self.calculate_size(det.qmax()), param.num_modes, rtype)
-        model_mean = self.mean_count[0] / (det.raw_mask == 0).sum() * 2.
+        qmax = max(det.qmax() for det in self.dets)
+        model = Model(self.calculate_size(qmax), param.num_modes, rtype)
+        model_mean = self.mean_count[0] / (self.dets[0].raw_mask == 0).sum() * 2.
         model.allocate(model_file, model_mean, fixed_seed=bool(param.fixed_seed))
         self.set_model(model)
         if param.need_scaling == 1:
@@ -210,22 +232,43 @@ class Iterate:
         self.calc_beta()
 
     def _attach(self, in_dset):
+        """Iterate.set_data's bookkeeping (iterate.pyx:241-266): frame
+        offsets, the unique detectors and each dataset's detector
+        (_gen_detlist, iterate.pyx:432-456: unique detector file names in
+        sorted order; datasets without a detector use the first), frame
+        counts, sum_fact and per-detector mean counts."""
         self.data = in_dset
         dsets = list(in_dset)
-        if not self.dets:
-            self.dets = [in_dset.det]
-        for d in dsets:
-            if d.det is not None and d.det is not self.dets[0] and d.det.num_pix != self.dets[0].num_pix:
-                raise NotImplementedError("multiple detectors are not supported")
+        dets = [d.det if d.det is not None else (self.dets[0] if self.dets else None) for d in dsets]
+        if dets[0] is None:
+            raise AttributeError("Set a detector for the dataset")
+        # one key per distinct detector: its file name, else the object
+        keys = [dt.fname if dt.fname else "<%d>" % id(dt) for dt in dets]
+        uniq, first, mapping = np.unique(np.array(keys, dtype=object), return_index=True, return_inverse=True)
+        self.dets = [dets[i] for i in first]
+        self._det_mapping = np.asarray(mapping, np.int32).ravel()
         self.tot_num_data = sum(d.num_data for d in dsets)
-        fc, sf, mc = frame_stats(dsets, self.dets[0].raw_mask)
+        fc, sf, mc = frame_stats(dsets, [dt.raw_mask for dt in self.dets], self._det_mapping, len(self.dets))
         self.fcounts, self.sum_fact = fc, sf
-        self.mean_count = np.array([mc])
-        self.rescale = np.zeros(1)
+        self.mean_count = mc
+        self.rescale = np.zeros(len(self.dets))
         self.blacklist = np.zeros(self.tot_num_data, np.uint8)
 
+    def member_index(self, k):
+        """Global indices of the frames seen by detector k, in frame order."""
+        ds = list(self.data)
+        off = np.concatenate([[0], np.cumsum([d.num_data for d in ds])])
+        parts = [np.arange(off[i], off[i + 1]) for i in range(len(ds)) if self._det_mapping[i] == k]
+        return np.concatenate(parts).astype(np.int64) if parts else np.zeros(0, np.int64)
+
+    def member_frames(self, k):
+        """The datasets seen by detector k as one set of sparse arrays."""
+        ds = [d for i, d in enumerate(self.data) if self._det_mapping[i] == k]
+        cat = lambda key: np.concatenate([getattr(d, key) for d in ds]).astype(np.int32)
+        return tuple(cat(key) for key in ("ones", "multi", "place_ones", "place_multi", "count_multi"))
+
     def merged_frames(self):
-        """The linked datasets as one set of sparse arrays."""
+        """The linked datasets as one set of sparse arrays (one detector)."""
         ds = list(self.data)
         cat = lambda k: np.concatenate([getattr(d, k) for d in ds]).astype(np.int32)
         return tuple(cat(k) for k in ("ones", "multi", "place_ones", "place_multi", "count_multi"))
@@ -383,4 +426,6 @@ class Iterate:
 
     @property
     def det_mapping(self):
-        return np.zeros(self.num_dfiles, np.int32)
+        if self.data is None:
+            return None
+        return self._det_mapping.copy()

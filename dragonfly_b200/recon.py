@@ -40,6 +40,11 @@ class EMCRecon:
         self.num_threads = num_threads if num_threads > 0 else (os.cpu_count() or 1)
         self.device = int(os.environ.get("LOCAL_RANK", "0")) if device is None else device
         self.ctx = None
+        # several detectors: one context per detector (ctx is the first, which
+        # holds the model), run together as a DetectorGroup
+        self.ctxs = []
+        self.group = None
+        self._index = []
         self._iter = None
         self.refinement = 0
         self.within_openmp = 0
@@ -67,30 +72,41 @@ class EMCRecon:
             raise NotImplementedError("point-group and axial symmetries apply to 3-D models")
         if itr.params.nonrot_modes:
             raise NotImplementedError("non-rotating modes are not supported")
-        from ._lib import Context
-        if self.ctx is None:
-            self.ctx = Context(self.device)
-        c = self.ctx
-        det = itr.dets[0]
-        c.set_detector(det.qvals, det.corr, det.raw_mask)
-        c.set_frames(*itr.merged_frames())
-        # background-aware updates (max_update.c:232-543, max_scale.c:21-288)
-        c.set_background(det.background if det.with_bg else None)
-        c.set_quaternions(itr.quat.quats)
-        # 2-D: angles in quats[:, 0], images [modes, S, S], Friedel average
-        # when params.friedel_sym (recon.pyx:118-119)
-        c.set_model_type(1 if two_d else 0, itr.params.friedel_sym if two_d else 0)
-        c.set_model(itr.model.model1)
-        # refinement (max_prob.c:110-120 with src/iterate.c:103-130)
-        if itr.params.refine:
-            if itr.quat.quat_mapping is None or itr.rel_quat is None:
-                raise ValueError("refinement needs quat.voronoi_subset() and Iterate.parse_rel_quat()")
-            c.set_refinement(itr.quat.num_rot_coarse, itr.quat.quat_mapping, itr.rel_quat)
-            self.refinement = 1
-        # update_model's symmetries (recon.pyx:120-134)
+        from ._lib import Context, DetectorGroup
+        K = itr.num_det
+        if K > 1 and any(d.with_bg for d in itr.dets):
+            raise NotImplementedError("background-aware updates with several detectors are not supported")
+        while len(self.ctxs) < K:
+            self.ctxs.append(Context(self.device))
+        while len(self.ctxs) > K:
+            self.ctxs.pop().close()
+        self.ctx = self.ctxs[0]
+        self._index = [itr.member_index(k) for k in range(K)]
+        if itr.params.refine and (itr.quat.quat_mapping is None or itr.rel_quat is None):
+            raise ValueError("refinement needs quat.voronoi_subset() and Iterate.parse_rel_quat()")
         pg = 2 if itr.quat.icosahedral_flag else (1 if itr.quat.octahedral_flag else 0)
-        if not two_d:
-            c.set_symmetry(pg, itr.params.axial_sym if itr.params.axial_sym > 1 else 0)
+        for k, c in enumerate(self.ctxs):
+            det = itr.dets[k]
+            c.set_detector(det.qvals, det.corr, det.raw_mask)
+            c.set_frames(*itr.member_frames(k))
+            # background-aware updates (max_update.c:232-543, max_scale.c:21-288)
+            c.set_background(det.background if det.with_bg else None)
+            c.set_quaternions(itr.quat.quats)
+            # 2-D: angles in quats[:, 0], images [modes, S, S], Friedel average
+            # when params.friedel_sym (recon.pyx:118-119)
+            c.set_model_type(1 if two_d else 0, itr.params.friedel_sym if two_d else 0)
+            c.set_model(itr.model.model1)
+            # refinement (max_prob.c:110-120 with src/iterate.c:103-130)
+            if itr.params.refine:
+                c.set_refinement(itr.quat.num_rot_coarse, itr.quat.quat_mapping,
+                                 [itr.rel_quat[i] for i in self._index[k]])
+                self.refinement = 1
+            # update_model's symmetries (recon.pyx:120-134)
+            if not two_d:
+                c.set_symmetry(pg, itr.params.axial_sym if itr.params.axial_sym > 1 else 0)
+        if self.group is not None:
+            self.group.close()
+        self.group = DetectorGroup(self.ctxs) if K > 1 else None
         itr.quat.divide(0, 1, itr.params.num_modes, itr.params.nonrot_modes)
         itr.params.rank, itr.params.num_proc = 0, 1
         self._iter = itr
@@ -107,30 +123,37 @@ class EMCRecon:
         stime = time.time()
         if par.iteration == 1:
             self.write_log_file_header()
-        c = self.ctx
-        c.set_model(itr.model.model1)
-        c.set_blacklist(itr.blacklist)
-        c.set_beta_start(itr.beta_start)
-        if par.need_scaling:
-            c.set_scale(itr.scale)
-            if itr.dets[0].with_bg:
-                c.set_bgscale(itr.bgscale)
+        for c, idx in zip(self.ctxs, self._index):
+            c.set_model(itr.model.model1)
+            c.set_blacklist(itr.blacklist[idx])
+            c.set_beta_start(itr.beta_start[idx])
+            if par.need_scaling:
+                c.set_scale(itr.scale[idx])
+                if itr.dets[0].with_bg:
+                    c.set_bgscale(itr.bgscale[idx])
+            # the per-frame probability lists are formed only when they are
+            # saved (combine_information_omp, max_prob.c:294-325)
+            c.set_option("keep_prob", 1 if par.save_prob else 0)
         beta_mean = self.update_beta()
-        p = c.params(par.iteration, par.need_scaling, par.update_scale, par.known_scale, par.beta_jump,
-                     par.beta_period, par.beta_factor)
-        # the per-frame probability lists are formed only when they are saved
-        # (combine_information_omp, max_prob.c:294-325)
-        c.set_option("keep_prob", 1 if par.save_prob else 0)
-        likelihood = c.maximize(p)
+        p = self.ctx.params(par.iteration, par.need_scaling, par.update_scale, par.known_scale, par.beta_jump,
+                            par.beta_period, par.beta_factor)
+        if self.group is not None:
+            likelihood = self.group.maximize(p)
+        else:
+            likelihood = self.ctx.maximize(p)
         self.update_model()
         # recon.pyx:102-103: volumes only
         if par.need_scaling == 1 and itr.model.mtype == "MODEL_3D":
             itr.normalize_scale()
-        fp = c.frame_params()
-        itr.beta[itr.blacklist == 0] = fp["beta"][itr.blacklist == 0]
-        sc = c.scalars()
-        itr.rescale[0] = sc["rescale"]
-        itr.mutual_info = sc["mutual_info"]
+        beta = self._gather(lambda c: c.frame_params()["beta"])
+        itr.beta[itr.blacklist == 0] = beta[itr.blacklist == 0]
+        for k, c in enumerate(self.ctxs):
+            itr.rescale[k] = c.scalars()["rescale"]
+        if self.group is not None:
+            n = itr.tot_num_data
+            itr.mutual_info = float(sum(c.scalars()["mutual_info"] * c.num_data for c in self.ctxs) / n)
+        else:
+            itr.mutual_info = self.ctx.scalars()["mutual_info"]
         itr.likelihood = likelihood
         self._results = {}
         if par.rank == 0:
@@ -146,13 +169,27 @@ class EMCRecon:
         When need_scaling, the scale update of maximize is copied too."""
         itr = self._iter
         c = self.ctx
-        itr.rms_change = c.update_model(itr.params.alpha)
+        if self.group is not None:
+            itr.rms_change = self.group.update_model(itr.params.alpha)
+        else:
+            itr.rms_change = c.update_model(itr.params.alpha)
         m1, m2, w = c.model()
         itr.model.model1 = m1
         itr.model.model2 = m2
         itr.model.inter_weight = w
         if itr.params.need_scaling:
-            itr.scale = c.frame_params()["scale"]
+            itr.scale = self._gather(lambda cc: cc.frame_params()["scale"])
+
+    def _gather(self, fn, dtype=None):
+        """Per-frame values of every detector's context in global frame
+        order."""
+        if len(self.ctxs) == 1:
+            return fn(self.ctx)
+        parts = [fn(c) for c in self.ctxs]
+        out = np.zeros((self._iter.tot_num_data,) + parts[0].shape[1:], dtype or parts[0].dtype)
+        for idx, a in zip(self._index, parts):
+            out[idx] = a
+        return out
 
     def update_beta(self):
         """Mean of beta_d = min(1, beta_start_d * factor) over good frames
@@ -167,9 +204,13 @@ class EMCRecon:
         return float(beta.sum() / (itr.tot_num_data - itr.num_blacklist))
 
     def free(self):
-        if self.ctx is not None:
-            self.ctx.close()
-            self.ctx = None
+        if self.group is not None:
+            self.group.close()
+            self.group = None
+        for c in self.ctxs:
+            c.close()
+        self.ctxs = []
+        self.ctx = None
 
     # -- output ----------------------------------------------------------------
     def write_log_file_header(self):
@@ -259,7 +300,12 @@ class EMCRecon:
     # -- results ---------------------------------------------------------------
     def _frame(self, key):
         if key not in self._results:
-            self._results.update(self.ctx.frame_results())
+            if len(self.ctxs) > 1:
+                parts = [c.frame_results() for c in self.ctxs]
+                for k in parts[0]:
+                    self._results[k] = self._gather(lambda c, k=k: parts[self.ctxs.index(c)][k])
+            else:
+                self._results.update(self.ctx.frame_results())
         return self._results[key]
 
     @property
@@ -296,7 +342,7 @@ class EMCRecon:
 
     @property
     def quat_norm(self):
-        return self.ctx.quat_norm()
+        return self._gather(lambda c: c.quat_norm())
 
     @property
     def num_prob(self):
@@ -306,15 +352,21 @@ class EMCRecon:
         if self._iter is not None and self._iter.params.save_prob:
             off = self._sparse()[0]
             return np.diff(off).astype(np.int32)
-        return np.zeros(self.ctx.num_data, np.int32)
+        return np.zeros(self._iter.tot_num_data, np.int32)
 
     @property
     def u(self):
-        return [self.ctx.orientation_results()[0]]
+        """u_r per detector (max_prob.c:31-42)."""
+        return [c.orientation_results()[0] for c in self.ctxs]
 
     @property
     def psum_r(self):
+        """psum_r of the first detector (per detector: psum_r_det)."""
         return self.ctx.orientation_results()[1]
+
+    @property
+    def psum_r_det(self):
+        return [c.orientation_results()[1] for c in self.ctxs]
 
     @property
     def model(self):
@@ -326,7 +378,23 @@ class EMCRecon:
 
     def _sparse(self):
         if "sparse" not in self._results:
-            self._results["sparse"] = self.ctx.sparse_prob()
+            if len(self.ctxs) == 1:
+                self._results["sparse"] = self.ctx.sparse_prob()
+            else:
+                # every frame's list from its detector's context, in global
+                # frame order
+                n = self._iter.tot_num_data
+                lists = [None] * n
+                for c, idx in zip(self.ctxs, self._index):
+                    off, place, prob = c.sparse_prob()
+                    for j, d in enumerate(idx):
+                        lists[d] = (place[off[j]:off[j + 1]], prob[off[j]:off[j + 1]])
+                counts = np.array([a.size for a, _ in lists], np.int64)
+                off = np.zeros(n + 1, np.int64)
+                np.cumsum(counts, out=off[1:])
+                place = np.concatenate([a for a, _ in lists]).astype(np.int32) if n else np.zeros(0, np.int32)
+                prob = np.concatenate([b for _, b in lists]) if n else np.zeros(0)
+                self._results["sparse"] = (off, place, prob)
         return self._results["sparse"]
 
     @property

@@ -291,6 +291,36 @@ DFG_API int dfg_autotune(dfg_ctx *ctx, const dfg_iter_params *par, double *repor
  * (DFG_ERR_STATE if none). */
 DFG_API int dfg_get_autotune_report(dfg_ctx *ctx, double *report);
 
+/* ---- several detectors in one reconstruction -----------------------------
+ * Replaces the reference's num_det loops (Iterate with in_detector_list,
+ * dragonfly/iterate.pyx:432-456; calculate_rescale and calculate_prob,
+ * dragonfly/src/max_prob.c:31-60, 96-106; calc_psum_r, update_tomogram_nobg
+ * and merge_tomogram, dragonfly/src/max_update.c:18-40, 55-128, 153-229).
+ * Member k is a context holding detector k and the frames seen by it, with
+ * the same orientations, model (shape, type, values), parameters and
+ * refinement setting as the others; member 0 also holds the model update's
+ * symmetries. The per-detector quantities (u, rescale, psum_r, tomograms)
+ * stay in the members; every member's merged sums are added into member 0's
+ * (one model2 / inter_weight, as in the reference), member 0 updates the
+ * model and the others receive a copy. Averages (log-likelihood, mutual
+ * information) and normalize_scale's mean scale are taken over the frames of
+ * all detectors. Background-aware updates with several detectors return
+ * DFG_ERR_ARG. Per-frame results: dfg_get_frame_results on each member (its
+ * frames in its own order); the model: dfg_get_model on member 0. */
+typedef struct dfg_group dfg_group;
+DFG_API int dfg_group_create(dfg_ctx *const *members, int n, dfg_group **out);
+DFG_API void dfg_group_destroy(dfg_group *group);
+DFG_API const char *dfg_group_last_error(const dfg_group *group);
+/* maximize() over all detectors (maximize.c:8-56 with num_det > 1). */
+DFG_API int dfg_group_maximize(dfg_group *group, const dfg_iter_params *par, double *avg_likelihood);
+/* EMCRecon.update_model (recon.pyx:112-149) on the shared model. */
+DFG_API int dfg_group_update_model(dfg_group *group, double alpha, double *rms_change);
+/* Iterate.normalize_scale (iterate.pyx:361-384) over all detectors' frames. */
+DFG_API int dfg_group_normalize_scale(dfg_group *group, double *mean_scale);
+/* One iteration as dfg_run_iteration; out[5]: average log-likelihood, rms
+ * change, mutual information, detector 0's rescale factor, mean scale. */
+DFG_API int dfg_group_run_iteration(dfg_group *group, const dfg_iter_params *par, double alpha, double *out);
+
 /* ---- batches of independent reconstructions -------------------------------
  * Several contexts on one GPU (different detectors, frames, orientation sets,
  * models and modes) iterated together: dfg_batch_run runs dfg_run_iteration
@@ -352,14 +382,18 @@ DFG_API int dfg_pnet_train(dfg_pnet *net, const int *labels, int epochs, double 
 DFG_API int dfg_pnet_set_targets(dfg_pnet *net, const long long *t_off, const int *t_cls, const float *t_w);
 /* Inference products (dfg_pnet_topk, dfg_pnet_logits) of layers 1-5 on the
  * tcgen05 tensor cores with BF16 activations (on = 1, the default) or on the
- * FP32 path that training uses (on = 0). */
+ * FP32 path (on = 0). */
 DFG_API int dfg_pnet_set_tensor_cores(dfg_pnet *net, int on);
 /* Network options by name (no counterpart in the reference): "tensor_cores"
- * (as dfg_pnet_set_tensor_cores) and two failure-detection test hooks of the
- * tensor-core products, "wait_cycles" (clock cycles after which a pipeline
- * wait gives up, default 2e9) and "withhold_stage" (a stage whose copies are
- * never issued, so its waits run out and dfg_pnet_topk / dfg_pnet_logits
- * return DFG_ERR_CUDA; -1, the default, issues every stage). */
+ * (as dfg_pnet_set_tensor_cores); "tensor_core_training" (1, the default:
+ * dfg_pnet_train and dfg_pnet_gradients compute the products of layers 1-5,
+ * forward, weight and input gradients, on the tcgen05 tensor cores with BF16
+ * operands and FP32 accumulation; 0: on the FP32 path, FP32 activations and
+ * gradients against BF16 weights); and two failure-detection test hooks of
+ * the tensor-core products, "wait_cycles" (clock cycles after which a
+ * pipeline wait gives up, default 2e9) and "withhold_stage" (a stage whose
+ * copies are never issued, so its waits run out and the call returns
+ * DFG_ERR_CUDA; -1, the default, issues every stage). */
 DFG_API int dfg_pnet_set_option(dfg_pnet *net, const char *key, double value);
 
 /* out[n][K]: the K largest logits' classes of every loaded image, largest first. */

@@ -77,10 +77,15 @@ def logits(params, images, num_classes, round_activations=False):
     return a
 
 
-def loss_and_grads(params, images, labels, num_classes, round_weights=True, targets=None):
+def loss_and_grads(params, images, labels, num_classes, round_weights=True, targets=None, mixed=False):
     """Mean softmax cross-entropy of the images [B][1024] and its gradient
     with respect to the flat parameters; against the labels, or (targets
-    [B][classes], rows summing to 1) against soft targets."""
+    [B][classes], rows summing to 1) against soft targets. mixed: the
+    roundings of mixed-precision training on the tensor cores -- the inputs
+    of layers 1-5 rounded to BF16 in the forward products and in their
+    weight gradients, the output gradients of layers 1-5 rounded to BF16 in
+    their weight and input gradients (bias gradients and layer 0 from the
+    unrounded values)."""
     L = layers(num_classes)
     P = unflatten(params, num_classes)
     B = images.shape[0]
@@ -88,11 +93,12 @@ def loss_and_grads(params, images, labels, num_classes, round_weights=True, targ
     acts, colss = [x], []
     for l, ((kind, cin, cout, hin, s, ho), (w, b)) in enumerate(zip(L, P)):
         wr = bf16(w) if round_weights else w
+        a_in = bf16(acts[-1]) if (mixed and l > 0) else acts[-1]
         if kind == 0:
-            cols = im2col(acts[-1], s, ho)
+            cols = im2col(a_in, s, ho)
             y = (cols @ wr.T + b).reshape(B, ho, ho, cout)
         else:
-            cols = acts[-1].reshape(B, -1)
+            cols = a_in.reshape(B, -1)
             y = cols @ wr.T + b
         colss.append(cols)
         acts.append(np.maximum(y, 0.) if l < len(L) - 1 else y)
@@ -113,8 +119,10 @@ def loss_and_grads(params, images, labels, num_classes, round_weights=True, targ
         if l < len(L) - 1:
             dy = dy * (acts[l + 1] > 0)
         d2 = dy.reshape(-1, cout)
-        gw = d2.T @ colss[l]
         gb = d2.sum(0)
+        if mixed and l > 0:
+            d2 = bf16(d2)
+        gw = d2.T @ colss[l]
         grads[l] = (gw, gb)
         if l > 0:
             dc = d2 @ wr

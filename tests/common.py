@@ -46,3 +46,21 @@ def compare_iteration(a, b, prob, it, check_model=True, model_before=None, scale
     if prob.need_scaling:
         assert out["scale_rel"] <= SCALE_REL, msg
     return out
+
+
+def two_detector_problems(seed, **kw):
+    """Two EMCProblems sharing orientations and model, each with its own
+    detector (different geometry and pixel count) and frames
+    (synth.two_detector_problem); kw are EMCProblem parameters; with
+    known_scale each detector's frames get seeded uniform [0.5, 1.5) scales."""
+    from dragonfly_b200 import synth
+    dets, sh = synth.two_detector_problem(seed=seed)
+    probs = []
+    for k, d in enumerate(dets):
+        scale = None
+        if kw.get("known_scale"):
+            scale = np.random.default_rng(seed + k).uniform(0.5, 1.5, d["ones"].size)
+        probs.append(EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"],
+                                d["place_multi"], d["count_multi"], sh["quats"], sh["model_start"], scale=scale,
+                                **kw))
+    return probs

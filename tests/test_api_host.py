@@ -187,3 +187,60 @@ def test_make_rot_quat_and_quaternion_api():
     # voronoi_subset runs on the GPU: tests/test_refinement.py
     q2 = Quaternion(num_rot=36, point_group="1")
     assert q2.quats.shape == (36, 5)
+
+
+def test_iterate_detector_list(tmp_path, oracle_built):
+    """in_detector_list / in_photons_list (iterate.pyx:61-101, 432-456):
+    file i is seen by detector i; the unique detectors are ordered by file
+    name, so here the second file's detector is detector 0. Frame counts,
+    sum_fact and the per-detector mean counts as the oracle forms them for
+    each detector's frames; the model is sized by the largest qmax."""
+    dets, sh = synth.two_detector_problem(seed=7)
+    names = ["det_z.npz", "det_a.npz"]
+    for k, dd in enumerate(dets):
+        det = Detector()
+        det.qvals, det.corr, det.raw_mask = dd["qvals"], dd["corr"], dd["mask"]
+        det.detd, det.ewald_rad = dd["detd"], 1.
+        det.write(str(tmp_path / names[k]))
+        write_emc(str(tmp_path / ("photons%d.emc" % k)), dd["qvals"].shape[0], dd["ones"], dd["multi"],
+                  dd["place_ones"], dd["place_multi"], dd["count_multi"])
+    (tmp_path / "dets.txt").write_text("\n".join(names) + "\n")
+    (tmp_path / "photons.txt").write_text("photons0.emc\nphotons1.emc\n")
+    cfg = tmp_path / "config.ini"
+    cfg.write_text("""[emc]
+in_photons_list = photons.txt
+in_detector_list = dets.txt
+num_div = 2
+output_folder = out/
+log_file = out/EMC.log
+beta = 0.5
+""")
+    itr = Iterate(str(cfg))
+    n0, n1 = dets[0]["ones"].size, dets[1]["ones"].size
+    assert itr.num_det == 2 and itr.tot_num_data == n0 + n1
+    np.testing.assert_array_equal(itr.det_mapping, [1, 0])
+    assert itr.dets[0].fname.endswith("det_a.npz") and itr.dets[1].fname.endswith("det_z.npz")
+    np.testing.assert_array_equal(itr.member_index(0), np.arange(n0, n0 + n1))
+    np.testing.assert_array_equal(itr.member_index(1), np.arange(n0))
+    for k, key in enumerate(("ones", "multi", "place_ones", "place_multi", "count_multi")):
+        np.testing.assert_array_equal(itr.member_frames(0)[k], dets[1][key])
+    fcs, mcs = [], []
+    for dd in dets:
+        p = EMCProblem_from(dd, sh)
+        orc = OracleEngine(p)
+        fcs.append(orc.fcounts)
+        mcs.append(orc.mean_count)
+    np.testing.assert_array_equal(itr.fcounts, np.concatenate(fcs))
+    assert itr.mean_count[0] == mcs[1] and itr.mean_count[1] == mcs[0]
+    qmax = max(np.linalg.norm(dd["qvals"], axis=1).max() for dd in dets)
+    assert itr.model.size == Iterate.calculate_size(qmax)
+    # a single photons file with a detector list uses the first detector
+    cfg.write_text(cfg.read_text().replace("in_photons_list = photons.txt", "in_photons_file = photons0.emc"))
+    itr1 = Iterate(str(cfg))
+    assert itr1.num_det == 1 and itr1.dets[0].fname.endswith("det_z.npz")
+
+
+def EMCProblem_from(dd, sh):
+    from oracle.oracle import EMCProblem
+    return EMCProblem(dd["qvals"], dd["corr"], dd["mask"], dd["ones"], dd["multi"], dd["place_ones"],
+                      dd["place_multi"], dd["count_multi"], sh["quats"], sh["model_start"])

@@ -11,7 +11,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from common import CASES, load_case
+from common import CASES, load_case, two_detector_problems
 from oracle.oracle import EMCProblem, OracleEngine, ReferenceEngine, reference_available
 
 
@@ -182,20 +182,6 @@ def test_legacy_engine_driver_agrees_with_packaged_engine(oracle_built):
         ref.close()
 
 
-def _two_detector_problems(seed, **kw):
-    from dragonfly_b200 import synth
-    dets, sh = synth.two_detector_problem(seed=seed)
-    probs = []
-    for k, d in enumerate(dets):
-        scale = None
-        if kw.get("known_scale"):
-            scale = np.random.default_rng(seed + k).uniform(0.5, 1.5, d["ones"].size)
-        probs.append(EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"],
-                                d["place_multi"], d["count_multi"], sh["quats"], sh["model_start"], scale=scale,
-                                **kw))
-    return probs
-
-
 @pytest.mark.skipif(not reference_available(), reason="reference sources not compiled here")
 @pytest.mark.parametrize("seed,prob_kw", [
     (21, dict(beta=1.)),
@@ -208,7 +194,7 @@ def test_oracle_two_detectors_match_live_reference(seed, prob_kw, oracle_built):
     tomograms per detector, merges per orientation in detector order): the
     oracle against the reference engine run with both detectors, bit for
     bit, over three iterations."""
-    p0, p1 = _two_detector_problems(seed, **prob_kw)
+    p0, p1 = two_detector_problems(seed, **prob_kw)
     ref = ReferenceEngine(p0, num_threads=1)
     ref.add_detector(p1)
     orc = OracleEngine(p0, extra=[p1])

@@ -76,6 +76,7 @@ def test_gpu_gradients_match_oracle():
     rng = np.random.default_rng(1)
     nc = 40
     net = ProposalNet(nc, batch=8, seed=3)
+    net.set_option("tensor_core_training", 0)   # the FP32 path
     p = net.params().astype(np.float64)
     x = np.log1p(rng.poisson(0.5, (8, 1024)).astype(np.float64))
     y = rng.integers(0, nc, 8)
@@ -91,6 +92,64 @@ def test_gpu_gradients_match_oracle():
             a, b = g[o:o + n].astype(np.float64), g_ref[o:o + n]
             o += n
             assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b) + 1e-9, (kind, cin, cout, n)
+    net.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nc,batch", [(40, 8), (420, 64)])
+def test_gpu_tensor_core_gradients_match_oracle(nc, batch):
+    """Mixed-precision training: the forward products of layers 1-5 and their
+    weight and input gradients on the tcgen05 tensor cores (BF16 activations,
+    output gradients and weights; FP32 accumulation, the weight gradients
+    split over the batch rows), layer 0, the biases and the loss in FP32.
+    Against the oracle with the same roundings (loss_and_grads(mixed=True)):
+    the loss and every layer's gradients. Activations summed in FP32 on the
+    GPU and in FP64 by the oracle (relative differences of order 1e-6) round
+    to different BF16 neighbours now and then, and those flips move the
+    gradients: the bound per layer is twice the oracle's own change under a
+    1e-6 relative perturbation of the weights (measured here; 1e-4 to 3e-2 on
+    these inputs), at least 5e-3. Against the unrounded oracle the BF16
+    roundings themselves account for 0.01 % to 10 % per layer (largest
+    towards the input, where five products' roundings have added up), with
+    the direction kept."""
+    from dragonfly_b200._lib import ProposalNet
+    rng = np.random.default_rng(11)
+    net = ProposalNet(nc, batch=batch, seed=3)
+    p = net.params().astype(np.float64)
+    x = np.log1p(rng.poisson(0.5, (batch, 1024)).astype(np.float64))
+    y = rng.integers(0, nc, batch)
+    net.set_images(x)
+    g, loss = net.gradients(y)
+    x64 = x.astype(np.float32).astype(np.float64)
+    loss_mix, g_mix = loss_and_grads(p, x64, y, nc, mixed=True)
+    loss_ref, g_ref = loss_and_grads(p, x64, y, nc)
+    # the mixed-precision gradients' own sensitivity to rounding flips
+    sens = np.zeros_like(g_mix)
+    for seed in (1, 2):
+        pr = p * (1. + 1e-6 * np.random.default_rng(seed).standard_normal(p.size))
+        sens = np.maximum(sens, np.abs(loss_and_grads(pr, x64, y, nc, mixed=True)[1] - g_mix))
+    print("loss: tensor cores %.6f, mixed-precision oracle %.6f, oracle %.6f" % (loss, loss_mix, loss_ref))
+    assert abs(loss - loss_mix) <= 5e-4 * abs(loss_mix), (loss, loss_mix)
+    o, errs = 0, []
+    for kind, cin, cout, *_ in layers(nc):
+        fan = 9 * cin if kind == 0 else cin
+        for n in (cout * fan, cout):
+            a, m, b = g[o:o + n].astype(np.float64), g_mix[o:o + n], g_ref[o:o + n]
+            sv = np.linalg.norm(sens[o:o + n]) / np.linalg.norm(m)
+            o += n
+            cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+            errs.append((kind, cout, n, np.linalg.norm(a - m) / np.linalg.norm(m), sv,
+                         np.linalg.norm(a - b) / np.linalg.norm(b), cos))
+    for r in errs:
+        print("layer kind %d cout %4d size %7d: vs mixed-precision oracle %.2e (its flip sensitivity %.2e), "
+              "vs oracle %.2e, cosine %.6f" % r)
+    for kind, cout, n, e_mix, sv, e_ref, cos in errs:
+        assert e_mix <= max(2. * sv, 5e-3), (kind, cout, n, e_mix, sv)
+        assert e_ref <= 0.15 and cos >= 0.99, (kind, cout, n, e_ref, cos)
+    # the FP32 path on the same network stays at its own bar
+    net.set_option("tensor_core_training", 0)
+    g32, _ = net.gradients(y)
+    assert np.linalg.norm(g32 - g_ref) <= 1e-4 * np.linalg.norm(g_ref)
     net.close()
 
 
@@ -193,6 +252,7 @@ def test_gpu_soft_target_gradients_match_oracle():
     rng = np.random.default_rng(2)
     nc = 40
     net = ProposalNet(nc, batch=8, seed=4)
+    net.set_option("tensor_core_training", 0)   # the FP32 path
     p = net.params().astype(np.float64)
     x = np.log1p(rng.poisson(0.5, (8, 1024)).astype(np.float64))
     net.set_images(x)
@@ -211,7 +271,9 @@ def test_gpu_soft_target_gradients_match_oracle():
     loss_ref, g_ref = loss_and_grads(p, x.astype(np.float32).astype(np.float64), None, nc, targets=T)
     assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref), (loss, loss_ref)
     assert np.linalg.norm(g - g_ref) <= 1e-4 * np.linalg.norm(g_ref), np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
-    # training against the targets lowers their cross-entropy
+    # training against the targets (on the tensor cores) lowers their
+    # cross-entropy
+    net.set_option("tensor_core_training", 1)
     l1 = net.train(epochs=20, lr=1e-3)
     assert l1 < loss, (l1, loss)
     with pytest.raises(RuntimeError):
