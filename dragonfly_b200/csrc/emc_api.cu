@@ -1678,17 +1678,15 @@ static int ensure_pair_buffers(dfg_ctx *ctx, const dfg_iter_params *par) {
 	CK(ctx->p_norm.ensure(N));
 	CK(ctx->psum_d.ensure(N));
 	CK(ctx->quat_norm.ensure(N * ctx->M));
-	// per-pair buffers with 10 % headroom (the live pairs change with every
-	// new restriction); the block buffer, sized from the memory left, gives
-	// way when they grow
+	// the per-pair buffer (FP64 sums, the probabilities written over them)
+	// with 10 % headroom (the live pairs change with every new restriction);
+	// the block buffer, sized from the memory left, gives way when it grows
 	const size_t need = (size_t)std::max<long long>(ctx->npairs, 1) * TILE;
-	if (ctx->raw.n < need || ctx->Pq.n < need) {
+	if (ctx->raw.n < need) {
 		ctx->blk.release();
 		ctx->blk_tiles = 0;
 		ctx->raw.release();
-		ctx->Pq.release();
 		CK(ctx->raw.ensure(need + need / 10));
-		CK(ctx->Pq.ensure(need + need / 10));
 	}
 	// one orientation block: (P + 1) x 128 floats per tile (log-slices with
 	// their zero row; the tomograms use P rows of the same space)
@@ -1786,19 +1784,19 @@ static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
 	norm_pairs_kernel<<<blocks_for((long long)N * 32, 256), 256, 0, st>>>(
 	    ctx->raw.p, ctx->frame_off.p, ctx->frame_pair.p, ctx->pair_tile.p, N, R, ctx->logw.p, ctx->u.p,
 	    ctx->scale.p, use_scale, ctx->beta.p, ctx->sum_fact.p, ctx->blacklist.p, psum_d_on, ctx->scalars.p,
-	    ctx->Pq.p, ctx->rmax.p, ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p,
+	    (float *)ctx->raw.p, ctx->rmax.p, ctx->max_exp.p, ctx->p_norm.p, ctx->info.p, ctx->likelihood.p, ctx->psum_d.p,
 	    ctx->num_prob.p);
 	CKL("norm_pairs_kernel");
 	const int nw = (int)ctx->h_watch.size();
 	if (nw > 0) {
 		captured_mass_pairs_kernel<<<blocks_for((long long)nw * 32, 256), 256, 0, st>>>(
-		    ctx->Pq.p, ctx->frame_off.p, ctx->frame_pair.p, ctx->pair_tile.p, ctx->qmap.p, ctx->watch_local.p, nw,
+		    (float *)ctx->raw.p, ctx->frame_off.p, ctx->frame_pair.p, ctx->pair_tile.p, ctx->qmap.p, ctx->watch_local.p, nw,
 		    ctx->watch_bits.p, ctx->rwords, ctx->watch_mass.p);
 		CKL("captured_mass_pairs_kernel");
 	}
 	phase_end(ctx, PH_NORM, nw > 0 ? 2 : 1);
 	phase_begin(ctx, PH_PSUM);
-	psum_pairs_kernel<<<RT, 256, 0, st>>>(ctx->Pq.p, ctx->tile_off.p, ctx->pair_frame.p, ctx->scale.p,
+	psum_pairs_kernel<<<RT, 256, 0, st>>>((float *)ctx->raw.p, ctx->tile_off.p, ctx->pair_frame.p, ctx->scale.p,
 	                                      par->need_scaling, R, ctx->psum_r.p);
 	CKL("psum_pairs_kernel");
 	phase_end(ctx, PH_PSUM, 1);
@@ -1812,7 +1810,7 @@ static int max_enqueue_pairs(dfg_ctx *ctx, const dfg_iter_params *par) {
 		CK(cudaMemsetAsync(ctx->blk.p, 0, (size_t)nt * P * TILE * sizeof(float), st));
 		const long long q0 = ctx->h_tile_off[t0], nq = ctx->h_tile_off[t0 + nt] - q0;
 		if (nq > 0) {
-			mstep_pairs_kernel<<<blocks_for(nq, 8), 256, 0, st>>>(ctx->Pq.p, t0, q0, nq, ctx->pair_tile.p,
+			mstep_pairs_kernel<<<blocks_for(nq, 8), 256, 0, st>>>((float *)ctx->raw.p, t0, q0, nq, ctx->pair_tile.p,
 			                                                       ctx->pair_frame.p, ctx->mw.p, ctx->mw_off.p, P,
 			                                                       ctx->blk.p);
 			CKL("mstep_pairs_kernel");
@@ -1882,8 +1880,7 @@ static int blocked_prepare(dfg_ctx *ctx, const dfg_iter_params *par) {
 	ctx->R_pad = ctx->RT * TILE;
 	ctx->logW.release();
 	ctx->T.release();
-	ctx->raw.release();  // per-pair buffers of the pair lists
-	ctx->Pq.release();
+	ctx->raw.release();  // per-pair buffer of the pair lists
 	dense_release(ctx);
 	const size_t N = (size_t)ctx->N, P = (size_t)ctx->P;
 	CK(ctx->u.ensure((size_t)ctx->R_pad));

@@ -258,7 +258,7 @@ struct dfg_ctx {
 	DevBuf<long long> tile_off, frame_off;
 	DevBuf<int> pair_tile, pair_frame, frame_pair;
 	DevBuf<double> raw;
-	DevBuf<float> Pq, blk, blkT;  // blkT: tomograms of the blocked full search
+	DevBuf<float> blk, blkT;  // blkT: tomograms of the blocked full search
 	bool blocked = false;         // the last full search ran in orientation blocks
 	DevBuf<signed char> wsign;  // per orientation: weight change of the merge
 	int blk_tiles = 0;

@@ -6,8 +6,10 @@
 // pair_tile[q] and frame pair_frame[q], the pairs of tile t are
 // [tile_off[t], tile_off[t + 1]) in ascending frame order, and frame d lists
 // its pairs in ascending tile order in frame_pair[frame_off[d] ..]. Per pair:
-// the FP64 photon sums of the tile's 128 orientations (raw) and their FP32
-// probabilities (Pq, sign = PROB_MIN gate as Pst). With the orientations split
+// the FP64 photon sums of the tile's 128 orientations (raw, 1 KB) and their
+// FP32 probabilities (Pq, sign = PROB_MIN gate as Pst), which the
+// normalisation writes over the first half of the same row once it has read
+// it (so a pair costs 1 KB, not 1.5). With the orientations split
 // into blocks of whole tiles, one block-sized buffer holds the block's
 // log-slices during the E-step and its tomograms during the M-step, so the
 // full log-slice and tomogram arrays (4 B x R x P each) are never resident.
@@ -24,6 +26,10 @@
 #include "emc_device.cuh"
 
 namespace dfg {
+
+// floats from one pair's probabilities to the next: they live in the first
+// half of the pair's FP64 row of raw
+constexpr int PQ_STRIDE = 2 * TILE;
 
 // Photon sums of the 4 (LW) orientations of one lane over one frame's E-step
 // lists (the loop of estep_kernel): compensated FP32, formed in FP64.
@@ -119,12 +125,15 @@ __global__ void __launch_bounds__(256, ESTEP_MINB) estep_pairs_kernel(
 // warp per frame, three passes over the frame's pairs (maximum and its lowest
 // orientation, kept sum, probabilities and frame sums). The log-likelihood is
 // x = log w_r - u_r s_d + raw, as the E-step forms it in the dense layout.
+// Pq aliases raw (PQ_STRIDE): a pair's row belongs to one frame, and the last
+// pass stores its probabilities only after every lane of the warp has read
+// the row.
 __global__ void __launch_bounds__(256) norm_pairs_kernel(
-    const double *__restrict__ raw, const long long *__restrict__ frame_off, const int *__restrict__ frame_pair,
+    const double *raw, const long long *__restrict__ frame_off, const int *__restrict__ frame_pair,
     const int *__restrict__ pair_tile, int N, int R, const double *__restrict__ logw, const double *__restrict__ u,
     const double *__restrict__ scale, int use_scale, const double *__restrict__ beta,
     const double *__restrict__ sum_fact, const uint8_t *__restrict__ blacklist, int psum_d_on,
-    const double *__restrict__ scalars, float *__restrict__ Pq, int *__restrict__ rmax,
+    const double *__restrict__ scalars, float *Pq, int *__restrict__ rmax,
     double *__restrict__ max_exp, double *__restrict__ p_norm, double *__restrict__ info,
     double *__restrict__ likelihood, double *__restrict__ psum_d, int *__restrict__ num_prob) {
 	const int d = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -173,7 +182,7 @@ __global__ void __launch_bounds__(256) norm_pairs_kernel(
 		for (int e = 0; e < LW; ++e)
 			zero[e] = 0.f;
 		for (long long k = k0; k < k1; ++k)
-			st_row(Pq + (size_t)frame_pair[k] * TILE + lane * LW, zero);
+			st_row(Pq + (size_t)frame_pair[k] * PQ_STRIDE + lane * LW, zero);
 		if (lane == 0) {
 			rmax[d] = -1;
 			max_exp[d] = MAX_EXP_START;
@@ -236,7 +245,8 @@ __global__ void __launch_bounds__(256) norm_pairs_kernel(
 				}
 			}
 		}
-		st_row(Pq + (size_t)frame_pair[k] * TILE + lane * LW, out);
+		__syncwarp();  // every lane has read the row that the stores overwrite
+		st_row(Pq + (size_t)frame_pair[k] * PQ_STRIDE + lane * LW, out);
 	}
 	ll = warp_sum(ll);
 	pd = warp_sum(pd);
@@ -268,7 +278,7 @@ __global__ void __launch_bounds__(256) psum_pairs_kernel(const float *__restrict
 		acc[k] = 0.;
 	for (long long q = tile_off[rt] + w; q < tile_off[rt + 1]; q += 8) {
 		float v[LW];
-		ld_row(Pq + (size_t)q * TILE + lane * LW, v);
+		ld_row(Pq + (size_t)q * PQ_STRIDE + lane * LW, v);
 		const double f = need_scaling ? scale[pair_frame[q]] : 1.;
 #pragma unroll
 		for (int k = 0; k < LW; ++k)
@@ -307,7 +317,7 @@ __global__ void __launch_bounds__(256) mstep_pairs_kernel(const float *__restric
 		return;
 	const long long q = q0 + w;
 	float v[LW];
-	ld_row(Pq + (size_t)q * TILE + lane * LW, v);
+	ld_row(Pq + (size_t)q * PQ_STRIDE + lane * LW, v);
 	bool any = false;
 #pragma unroll
 	for (int k = 0; k < LW; ++k) {
@@ -408,7 +418,7 @@ __global__ void __launch_bounds__(256) captured_mass_pairs_kernel(
 		const int q = frame_pair[k];
 		const int r0 = pair_tile[q] * TILE + lane * LW;
 		float v[LW];
-		ld_row(Pq + (size_t)q * TILE + lane * LW, v);
+		ld_row(Pq + (size_t)q * PQ_STRIDE + lane * LW, v);
 #pragma unroll
 		for (int e = 0; e < LW; ++e) {
 			const double p = fabs((double)v[e]);
