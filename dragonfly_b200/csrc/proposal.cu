@@ -145,14 +145,15 @@ __global__ void im2col_kernel(const float *__restrict__ X, int B, int H, int C, 
 // dX[b][y][x][c] = sum of dcols over the (ho, wo, ky, kx) that read it.
 __global__ void col2im_kernel(const float *__restrict__ dcols, int B, int H, int C, int s, int Ho,
                               float *__restrict__ dX) {
-	const long long n = (long long)B * H * H * C;
-	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-		const int c = (int)(e % C);
-		long long r = e / C;
-		const int x = (int)(r % H);
-		r /= H;
-		const int y = (int)(r % H);
-		const int b = (int)(r / H);
+	// 32-bit index arithmetic (B H H C < 2^31 for every layer and batch)
+	const unsigned n = (unsigned)B * H * H * C;
+	for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+		const int c = (int)(e % (unsigned)C);
+		unsigned r = e / (unsigned)C;
+		const int x = (int)(r % (unsigned)H);
+		r /= (unsigned)H;
+		const int y = (int)(r % (unsigned)H);
+		const int b = (int)(r / (unsigned)H);
 		float acc = 0.f;
 		for (int ky = 0; ky < 3; ++ky) {
 			const int yy = y + 1 - ky;
@@ -185,13 +186,26 @@ __global__ void bias_act_kernel(float *__restrict__ Y, long long rows, int cols,
 	}
 }
 
-// out[e] = sum over z of part[z n + e], z in order.
-__global__ void sum_splits_kernel(const float *__restrict__ part, int S, long long n, float *__restrict__ out) {
-	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-		float acc = 0.f;
-		for (int z = 0; z < S; ++z)
+// out[e] = sum over z of part[z n + e]: block (32, 8) per 32 elements, row y
+// of the block adds the splits y, y + 8, ... in order and the 8 rows are
+// added in order (deterministic; the 8 rows keep loads in flight when S is
+// large and n small).
+__global__ void __launch_bounds__(256) sum_splits_kernel(const float *__restrict__ part, int S, long long n,
+                                                         float *__restrict__ out) {
+	__shared__ float s[8][32];
+	const long long e = (long long)blockIdx.x * 32 + threadIdx.x;
+	float acc = 0.f;
+	if (e < n)
+		for (int z = threadIdx.y; z < S; z += 8)
 			acc += part[z * n + e];
-		out[e] = acc;
+	s[threadIdx.y][threadIdx.x] = acc;
+	__syncthreads();
+	if (threadIdx.y == 0 && e < n) {
+		float t = 0.f;
+#pragma unroll
+		for (int k = 0; k < 8; ++k)
+			t += s[k][threadIdx.x];
+		out[e] = t;
 	}
 }
 
@@ -221,22 +235,103 @@ __global__ void relu_back_kernel(float *__restrict__ dY, const float *__restrict
 
 // db[c] = sum_r dY[r][c]: one block per column, a fixed-order tree over
 // per-thread strided partial sums.
-__global__ void __launch_bounds__(256) bias_grad_kernel(const float *__restrict__ dY, long long rows, int cols,
-                                                        float *__restrict__ db) {
+// Column sums of dY [rows][cols] (bias gradients), first stage: block b adds
+// its rows [b chunk, (b + 1) chunk) into part[b][cols]. With cols dividing
+// 256, thread t keeps column t % cols and every (256 / cols)-th row from
+// t / cols on, so each step reads 256 consecutive floats (coalesced); the
+// threads of a column are then added in thread order. Otherwise thread t
+// keeps columns t, t + 256, ... over all the block's rows. Fixed order
+// throughout: the sums are deterministic.
+__global__ void __launch_bounds__(256) colsum_part_kernel(const float *__restrict__ dY, long long rows, int cols,
+                                                          long long chunk, float *__restrict__ part) {
 	__shared__ float s[256];
-	const int c = blockIdx.x;
-	float acc = 0.f;
-	for (long long r = threadIdx.x; r < rows; r += 256)
-		acc += dY[r * cols + c];
-	s[threadIdx.x] = acc;
-	__syncthreads();
-	for (int h = 128; h > 0; h >>= 1) {
-		if (threadIdx.x < h)
-			s[threadIdx.x] += s[threadIdx.x + h];
+	const long long r0 = (long long)blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
+	float *out = part + (size_t)blockIdx.x * cols;
+	if (256 % cols == 0) {
+		const int c = threadIdx.x % cols, j = threadIdx.x / cols, step = 256 / cols;
+		float acc = 0.f;
+		for (long long r = r0 + j; r < r1; r += step)
+			acc += dY[r * cols + c];
+		s[threadIdx.x] = acc;
 		__syncthreads();
+		if (threadIdx.x < cols) {
+			float t = 0.f;
+			for (int k = 0; k < step; ++k)
+				t += s[k * cols + threadIdx.x];
+			out[threadIdx.x] = t;
+		}
+	} else {
+		for (int c = threadIdx.x; c < cols; c += 256) {
+			float acc = 0.f;
+			for (long long r = r0; r < r1; ++r)
+				acc += dY[r * cols + c];
+			out[c] = acc;
+		}
 	}
-	if (threadIdx.x == 0)
-		db[c] = s[0];
+}
+
+// out[c] = sum over b < nb of part[b][c], b in order.
+__global__ void colsum_final_kernel(const float *__restrict__ part, int nb, int cols, float *__restrict__ out) {
+	const int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= cols)
+		return;
+	float t = 0.f;
+	for (int b = 0; b < nb; ++b)
+		t += part[(size_t)b * cols + c];
+	out[c] = t;
+}
+
+// Layer 0's weight and bias gradients (cout 32, K = 9 taps of one channel),
+// first stage: block b takes rows [b chunk, (b + 1) chunk) of dY [rows][32]
+// and the FP32 im2col rows X [rows][9]; thread t keeps output channel t % 32
+// over every 8th row from t / 32 on (each step reads 256 consecutive floats
+// of dY; the 9 taps of a row are read by the 32 threads of its channel group
+// from the same 36 bytes). part[b][c][0 .. 8] = weight sums, [9] = bias sum,
+// the 8 row phases added in order.
+__global__ void __launch_bounds__(256) wgrad0_part_kernel(const float *__restrict__ dY, const float *__restrict__ X,
+                                                          long long rows, long long chunk, float *__restrict__ part) {
+	__shared__ float s[8][32][10];
+	const int c = threadIdx.x & 31, j = threadIdx.x >> 5;
+	const long long r0 = (long long)blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
+	float acc[10];
+#pragma unroll
+	for (int k = 0; k < 10; ++k)
+		acc[k] = 0.f;
+	for (long long r = r0 + j; r < r1; r += 8) {
+		const float g = dY[r * 32 + c];
+		const float *x = X + r * 9;
+#pragma unroll
+		for (int k = 0; k < 9; ++k)
+			acc[k] += g * x[k];
+		acc[9] += g;
+	}
+#pragma unroll
+	for (int k = 0; k < 10; ++k)
+		s[j][c][k] = acc[k];
+	__syncthreads();
+	for (int e = threadIdx.x; e < 320; e += 256) {
+		const int cc = e / 10, k = e % 10;
+		float t = 0.f;
+		for (int jj = 0; jj < 8; ++jj)
+			t += s[jj][cc][k];
+		part[(size_t)blockIdx.x * 320 + e] = t;
+	}
+}
+
+// Second stage: gw[c][k] and gb[c] from the blocks' partial sums, in block order.
+__global__ void wgrad0_final_kernel(const float *__restrict__ part, int nb, float *__restrict__ gw,
+                                    float *__restrict__ gb) {
+	const int e = threadIdx.x;  // c * 10 + k
+	if (e >= 320)
+		return;
+	float t = 0.f;
+	for (int b = 0; b < nb; ++b)
+		t += part[(size_t)b * 320 + e];
+	const int c = e / 10, k = e % 10;
+	if (k < 9)
+		gw[c * 9 + k] = t;
+	else
+		gb[c] = t;
 }
 
 // Softmax cross-entropy per row (one warp per row): loss[b] =
@@ -644,10 +739,11 @@ __global__ void pad_rows_bf16_kernel(const __nv_bfloat16 *__restrict__ W, long l
 // X [rows][K] FP32 -> [rows][Kp] BF16 with zero columns K .. Kp - 1.
 __global__ void rows_bf16_kernel(const float *__restrict__ X, long long rows, int K, int Kp,
                                  __nv_bfloat16 *__restrict__ out) {
-	const long long n = rows * Kp;
-	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-		const int k = (int)(e % Kp);
-		out[e] = __float2bfloat16_rn(k < K ? X[(e / Kp) * K + k] : 0.f);
+	// 32-bit index arithmetic (rows Kp < 2^31 for every layer and batch)
+	const unsigned n = (unsigned)(rows * Kp);
+	for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+		const unsigned r = e / (unsigned)Kp, k = e - r * (unsigned)Kp;
+		out[e] = __float2bfloat16_rn((int)k < K ? X[(size_t)r * K + k] : 0.f);
 	}
 }
 
@@ -716,6 +812,7 @@ struct dfg_pnet {
 	DevBuf<float> act[NL + 1], dact[NL + 1], cols[4], dcols[4], loss, xbatch;
 	DevBuf<int> labels, idx, perm, lab_all;
 	DevBuf<float> wsplit;  // split-k partial weight gradients
+	DevBuf<float> gpart;   // per-block partial sums of the bias and layer-0 gradients
 	DevBuf<double> loss_acc;
 	DevBuf<float> images;
 	long long n_images = 0;
@@ -805,8 +902,37 @@ static int gemm_wgrad(dfg_pnet *net, int M, int N, int K, const float *A, const 
 	                                                                      net->wsplit.p, N, chunk,
 	                                                                      (long long)M * N);
 	PKL("gemm_kernel");
-	sum_splits_kernel<<<grid_for((long long)M * N), 256, 0, net->stream>>>(net->wsplit.p, S, (long long)M * N, C);
+	sum_splits_kernel<<<(unsigned)(((long long)M * N + 31) / 32), dim3(32, 8), 0, net->stream>>>(net->wsplit.p, S,
+	                                                                                          (long long)M * N, C);
 	PKL("sum_splits_kernel");
+	return DFG_OK;
+}
+
+// Bias gradients db[c] = sum over rows of dY[r][c] (two-stage, deterministic).
+static int bias_grad(dfg_pnet *net, const float *dY, long long rows, int cols, float *db) {
+	const long long chunk = std::max<long long>(64, (rows + 295) / 296);
+	const int nb = (int)((rows + chunk - 1) / chunk);
+	if ((size_t)nb * cols > net->gpart.n)
+		PK(net->gpart.ensure((size_t)nb * cols));
+	colsum_part_kernel<<<nb, 256, 0, net->stream>>>(dY, rows, cols, chunk, net->gpart.p);
+	PKL("colsum_part_kernel");
+	colsum_final_kernel<<<(cols + 255) / 256, 256, 0, net->stream>>>(net->gpart.p, nb, cols, db);
+	PKL("colsum_final_kernel");
+	return DFG_OK;
+}
+
+// Layer 0's weight and bias gradients from its FP32 im2col rows (K = 9).
+static int wgrad0(dfg_pnet *net, const float *dY, const float *X, long long rows, float *gw, float *gb) {
+	if (net->L[0].cout != 32 || net->L[0].fan_in() != 9)
+		return net->fail(DFG_ERR_STATE, "layer 0 must map 1 channel to 32 (3 x 3)");
+	const long long chunk = std::max<long long>(64, (rows + 295) / 296);
+	const int nb = (int)((rows + chunk - 1) / chunk);
+	if ((size_t)nb * 320 > net->gpart.n)
+		PK(net->gpart.ensure((size_t)nb * 320));
+	wgrad0_part_kernel<<<nb, 256, 0, net->stream>>>(dY, X, rows, chunk, net->gpart.p);
+	PKL("wgrad0_part_kernel");
+	wgrad0_final_kernel<<<1, 320, 0, net->stream>>>(net->gpart.p, nb, gw, gb);
+	PKL("wgrad0_final_kernel");
 	return DFG_OK;
 }
 
@@ -967,9 +1093,14 @@ static int backward(dfg_pnet *net, const float *X, const int *lab, int n, const 
 			relu_back_kernel<<<grid_for(rows * s.cout), 256, 0, st>>>(dY, net->act[l + 1].p, rows * s.cout);
 			PKL("relu_back_kernel");
 		}
-		bias_grad_kernel<<<s.cout, 256, 0, st>>>(dY, rows, s.cout, net->gb[l].p);
-		PKL("bias_grad_kernel");
 		const float *in = l == 0 ? X : net->act[l].p;
+		if (l == 0) {
+			if (int rc = wgrad0(net, dY, net->cols[0].p, rows, net->gw[0].p, net->gb[0].p))
+				return rc;
+			continue;
+		}
+		if (int rc = bias_grad(net, dY, rows, s.cout, net->gb[l].p))
+			return rc;
 		if (s.kind == 0) {
 			if (int rc = gemm_wgrad(net, s.cout, 9 * s.cin, (int)rows, dY, net->cols[l].p, net->gw[l].p))
 				return rc;
@@ -1037,7 +1168,7 @@ static int tc_product(dfg_pnet *net, const __nv_bfloat16 *A, long long M, int Kp
 #undef DFG_TC
 	PKL("pnet_gemm_tc_kernel");
 	if (S > 1) {
-		sum_splits_kernel<<<grid_for(M * N), 256, 0, net->stream>>>(net->tsplit.p, S, M * N, C);
+		sum_splits_kernel<<<(unsigned)((M * N + 31) / 32), dim3(32, 8), 0, net->stream>>>(net->tsplit.p, S, M * N, C);
 		PKL("sum_splits_kernel");
 		if (bias != nullptr) {
 			bias_act_kernel<<<grid_for(M * N), 256, 0, net->stream>>>(C, M, N, bias, relu);
@@ -1123,13 +1254,13 @@ static int backward_tc(dfg_pnet *net, const float *X, const int *lab, int n, con
 			relu_back_kernel<<<grid_for(rows * s.cout), 256, 0, st>>>(dY, net->act[l + 1].p, rows * s.cout);
 			PKL("relu_back_kernel");
 		}
-		bias_grad_kernel<<<s.cout, 256, 0, st>>>(dY, rows, s.cout, net->gb[l].p);
-		PKL("bias_grad_kernel");
 		if (l == 0) {
-			if (int rc = gemm_wgrad(net, s.cout, 9 * s.cin, (int)rows, dY, net->cols[0].p, net->gw[0].p))
+			if (int rc = wgrad0(net, dY, net->cols[0].p, rows, net->gw[0].p, net->gb[0].p))
 				return rc;
 			continue;
 		}
+		if (int rc = bias_grad(net, dY, rows, s.cout, net->gb[l].p))
+			return rc;
 		const int K = s.fan_in(), Kp = kpad64(K), cp = kpad64(s.cout);
 		const long long rows_p = (rows + 63) / 64 * 64;
 		// dW [cout][K] = dY^T X: both operands with the batch rows as the reduction

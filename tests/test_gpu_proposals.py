@@ -44,9 +44,9 @@ def test_learned_proposals_against_full_search(pair_lists):
     # at least 24 cells per frame, more where the network is unsure, until
     # its probabilities of the frame's cells reach 0.999999 (at most 128).
     # Measured on this case (one B200), after the first full search and the
-    # retraining on it: the model within 6.6-7.7e-4 of a full search from the
-    # same state, most likely orientations 99.975 %, 16.7 % of the pairs
-    # evaluated, captured mass 0.9995-0.9998. At 0.99999 the retrained
+    # retraining on it: the model within 6.6-8.4e-4 of a full search from the
+    # same state, most likely orientations 99.88-99.975 %, 16.7-18 % of the
+    # pairs evaluated, captured mass 0.9995-0.9998. At 0.99999 the retrained
     # network's proposals hold 11.6-12.2 % of the pairs and the model stays
     # 1.0-1.3e-3 away (so does a fixed 24 cells, 7.6 %, at 0.9985-0.999
     # captured mass): an orientation whose probability comes mostly from
