@@ -143,6 +143,47 @@ __global__ void im2col_kernel(const float *__restrict__ X, int B, int H, int C, 
 }
 
 // dX[b][y][x][c] = sum of dcols over the (ho, wo, ky, kx) that read it.
+// col2im_kernel for C a multiple of 4 and stride S (1 or 2): four channels
+// per thread (16-byte loads and stores), the taps added in the same order.
+template <int S>
+__global__ void col2im4_kernel(const float *__restrict__ dcols, int B, int H, int C, int Ho,
+                               float *__restrict__ dX) {
+	const unsigned C4 = (unsigned)C >> 2;
+	const unsigned n = (unsigned)B * H * H * C4;
+	for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+		const unsigned c4 = e % C4;
+		unsigned r = e / C4;
+		const int x = (int)(r % (unsigned)H);
+		r /= (unsigned)H;
+		const int y = (int)(r % (unsigned)H);
+		const int b = (int)(r / (unsigned)H);
+		float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+		for (int ky = 0; ky < 3; ++ky) {
+			const int yy = y + 1 - ky;
+			if (yy < 0 || (S == 2 && (yy & 1)))
+				continue;
+			const int ho = yy / S;
+			if (ho >= Ho)
+				continue;
+			for (int kx = 0; kx < 3; ++kx) {
+				const int xx = x + 1 - kx;
+				if (xx < 0 || (S == 2 && (xx & 1)))
+					continue;
+				const int wo = xx / S;
+				if (wo >= Ho)
+					continue;
+				const float4 v = *reinterpret_cast<const float4 *>(
+				    dcols + ((((size_t)b * Ho + ho) * Ho + wo) * 9 + ky * 3 + kx) * C + 4 * c4);
+				acc.x += v.x;
+				acc.y += v.y;
+				acc.z += v.z;
+				acc.w += v.w;
+			}
+		}
+		*reinterpret_cast<float4 *>(dX + (size_t)e * 4) = acc;
+	}
+}
+
 __global__ void col2im_kernel(const float *__restrict__ dcols, int B, int H, int C, int s, int Ho,
                               float *__restrict__ dX) {
 	// 32-bit index arithmetic (B H H C < 2^31 for every layer and batch)
@@ -500,6 +541,149 @@ __global__ void topk_kernel(const float *__restrict__ z, int B, int n, int K_min
 		cum += mi < n ? __expf(m - zmax) / den : 0.f;
 		last = m;
 		last_i = mi;
+	}
+}
+
+// Order-preserving key of a finite float (larger float, larger key); -0 and
+// +0 share a key, as they compare equal.
+__device__ __forceinline__ uint32_t order_key(float v) {
+	const uint32_t b = v == 0.f ? 0u : __float_as_uint(v);
+	return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// topk_kernel's picks for K_max <= SELK, one warp per row, without a row scan
+// per pick: a radix select (four passes of 8 bits, a per-warp histogram in
+// shared memory) finds the K_max-th largest key, the K_max largest entries
+// (ties at the boundary by ascending index) are compacted into shared memory
+// in index order, sorted by (value descending, index ascending) with a
+// bitonic network, and the mass rule is applied to them in that order with
+// topk_kernel's arithmetic, so the output is the same.
+constexpr int SELK = 256;
+__global__ void __launch_bounds__(256) topk_select_kernel(const float *__restrict__ z, int B, int n, int K_min,
+                                                          int K_max, float mass, int *__restrict__ out) {
+	__shared__ uint32_t s_hist[8][256];
+	__shared__ uint32_t s_key[8][SELK];
+	__shared__ int s_idx[8][SELK];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int b = blockIdx.x * 8 + w;
+	if (b >= B)
+		return;
+	const float *r = z + (size_t)b * n;
+	uint32_t *hist = s_hist[w], *key = s_key[w];
+	int *idx = s_idx[w];
+	// softmax normaliser, as topk_kernel
+	float zmax = -INFINITY;
+	for (int j = lane; j < n; j += 32)
+		zmax = fmaxf(zmax, r[j]);
+	for (int o = 16; o > 0; o >>= 1)
+		zmax = fmaxf(zmax, __shfl_xor_sync(FULL, zmax, o));
+	float den = 0.f;
+	for (int j = lane; j < n; j += 32)
+		den += __expf(r[j] - zmax);
+	for (int o = 16; o > 0; o >>= 1)
+		den += __shfl_xor_sync(FULL, den, o);
+	// radix select of the K_max-th largest key
+	uint32_t prefix = 0;
+	int need = K_max;
+	for (int shift = 24; shift >= 0; shift -= 8) {
+		for (int k = lane; k < 256; k += 32)
+			hist[k] = 0;
+		__syncwarp();
+		const uint32_t hi_mask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
+		for (int j = lane; j < n; j += 32) {
+			const uint32_t u = order_key(r[j]);
+			if ((u & hi_mask) == (prefix & hi_mask))
+				atomicAdd(&hist[(u >> shift) & 255u], 1u);
+		}
+		__syncwarp();
+		// lane L holds digits 255 - 8 L down to 248 - 8 L
+		int lsum = 0;
+#pragma unroll
+		for (int q = 0; q < 8; ++q)
+			lsum += (int)hist[255 - 8 * lane - q];
+		int incl = lsum;
+		for (int o = 1; o < 32; o <<= 1) {
+			const int t = __shfl_up_sync(FULL, incl, o);
+			if (lane >= o)
+				incl += t;
+		}
+		const unsigned hit = __ballot_sync(FULL, incl >= need);
+		const int src = __ffs(hit) - 1;  // need <= the group's count, so some lane crosses
+		int d = 0, above = 0;
+		if (lane == src) {
+			int c = incl - lsum;
+			for (int q = 0; q < 8; ++q) {
+				const int dig = 255 - 8 * lane - q, h = (int)hist[dig];
+				if (c + h >= need) {
+					d = dig;
+					above = c;
+					break;
+				}
+				c += h;
+			}
+		}
+		d = __shfl_sync(FULL, d, src);
+		above = __shfl_sync(FULL, above, src);
+		need -= above;
+		prefix |= (uint32_t)d << shift;
+		__syncwarp();
+	}
+	// the entries above the boundary key, and the first `need` at it by index,
+	// compacted in index order
+	int base = 0, ties = 0;
+	for (int j0 = 0; j0 < n; j0 += 32) {
+		const int j = j0 + lane;
+		const uint32_t u = j < n ? order_key(r[j]) : 0u;
+		const bool tie = j < n && u == prefix;
+		const unsigned tm = __ballot_sync(FULL, tie);
+		const int trank = ties + __popc(tm & ((1u << lane) - 1u));
+		const bool sel = j < n && (u > prefix || (tie && trank < need));
+		const unsigned sm = __ballot_sync(FULL, sel);
+		if (sel) {
+			const int pos = base + __popc(sm & ((1u << lane) - 1u));
+			key[pos] = u;
+			idx[pos] = j;
+		}
+		base += __popc(sm);
+		ties += __popc(tm);
+	}
+	int P = 1;
+	while (P < K_max)
+		P <<= 1;
+	for (int k = K_max + lane; k < P; k += 32) {  // pads sort last
+		key[k] = 0u;
+		idx[k] = 0x7fffffff;
+	}
+	__syncwarp();
+	for (int k = 2; k <= P; k <<= 1)
+		for (int jj = k >> 1; jj > 0; jj >>= 1) {
+			for (int i = lane; i < P; i += 32) {
+				const int ixj = i ^ jj;
+				if (ixj > i) {
+					const uint32_t ka = key[i], kb = key[ixj];
+					const int ia = idx[i], ib = idx[ixj];
+					const bool a_first = ka > kb || (ka == kb && ia < ib);
+					if (((i & k) == 0) != a_first) {
+						key[i] = kb;
+						key[ixj] = ka;
+						idx[i] = ib;
+						idx[ixj] = ia;
+					}
+				}
+			}
+			__syncwarp();
+		}
+	if (lane == 0) {
+		float cum = 0.f;
+		for (int k = 0; k < K_max; ++k) {
+			if (k >= K_min && cum >= mass) {
+				out[(size_t)b * K_max + k] = -1;
+				continue;
+			}
+			const int i = idx[k];
+			out[(size_t)b * K_max + k] = i;
+			cum += __expf(r[i] - zmax) / den;
+		}
 	}
 }
 
@@ -908,6 +1092,23 @@ static int gemm_wgrad(dfg_pnet *net, int M, int N, int K, const float *A, const 
 	return DFG_OK;
 }
 
+// dX [B][H][H][C] from the column gradients of a 3 x 3 convolution.
+static int col2im(dfg_pnet *net, const float *dcols, int B, int H, int C, int s, int Ho, float *dX) {
+	cudaStream_t st = net->stream;
+	if (C % 4 == 0 && (s == 1 || s == 2)) {
+		const long long n4 = (long long)B * H * H * (C / 4);
+		if (s == 1)
+			col2im4_kernel<1><<<grid_for(n4), 256, 0, st>>>(dcols, B, H, C, Ho, dX);
+		else
+			col2im4_kernel<2><<<grid_for(n4), 256, 0, st>>>(dcols, B, H, C, Ho, dX);
+		PKL("col2im4_kernel");
+		return DFG_OK;
+	}
+	col2im_kernel<<<grid_for((long long)B * H * H * C), 256, 0, st>>>(dcols, B, H, C, s, Ho, dX);
+	PKL("col2im_kernel");
+	return DFG_OK;
+}
+
 // Bias gradients db[c] = sum over rows of dY[r][c] (two-stage, deterministic).
 static int bias_grad(dfg_pnet *net, const float *dY, long long rows, int cols, float *db) {
 	const long long chunk = std::max<long long>(64, (rows + 295) / 296);
@@ -1109,10 +1310,8 @@ static int backward(dfg_pnet *net, const float *X, const int *lab, int n, const 
 				                                                        s.cout, net->wb[l].p, 9 * s.cin, 0.f,
 				                                                        net->dcols[l].p, 9 * s.cin))
 					return rc;
-				const long long nx = (long long)n * s.hin * s.hin * s.cin;
-				col2im_kernel<<<grid_for(nx), 256, 0, st>>>(net->dcols[l].p, n, s.hin, s.cin, s.stride, s.hout,
-				                                             net->dact[l].p);
-				PKL("col2im_kernel");
+				if (int rc = col2im(net, net->dcols[l].p, n, s.hin, s.cin, s.stride, s.hout, net->dact[l].p))
+					return rc;
 			}
 		} else {
 			if (int rc = gemm_wgrad(net, s.cout, s.cin, n, dY, in, net->gw[l].p))
@@ -1279,10 +1478,8 @@ static int backward_tc(dfg_pnet *net, const float *X, const int *lab, int n, con
 		if (s.kind == 0) {
 			if (int rc = tc_product(net, net->dyb.p, rows, cp, net->wtp[l].p, K, net->dcols[l].p, nullptr, 0))
 				return rc;
-			const long long nx = (long long)n * s.hin * s.hin * s.cin;
-			col2im_kernel<<<grid_for(nx), 256, 0, st>>>(net->dcols[l].p, n, s.hin, s.cin, s.stride, s.hout,
-			                                             net->dact[l].p);
-			PKL("col2im_kernel");
+			if (int rc = col2im(net, net->dcols[l].p, n, s.hin, s.cin, s.stride, s.hout, net->dact[l].p))
+				return rc;
 		} else {
 			if (int rc = tc_product(net, net->dyb.p, rows, cp, net->wtp[l].p, K, net->dact[l].p, nullptr, 0))
 				return rc;
@@ -1717,9 +1914,15 @@ extern "C" int dfg_pnet_topk_mass(dfg_pnet *net, int K_min, int K_max, double ma
 	DevBuf<int> d;  // every image's picks, read back once
 	PK(d.ensure((size_t)net->n_images * K_max));
 	if (int rc = for_batches(net, [&](long long b0, int m) -> int {
-		    topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(
-		        net->act[NL].p, m, net->num_classes, K_min, K_max, (float)mass, d.p + (size_t)b0 * K_max);
-		    PKL("topk_kernel");
+		    if (K_max <= SELK) {
+			    topk_select_kernel<<<(m + 7) / 8, 256, 0, net->stream>>>(
+			        net->act[NL].p, m, net->num_classes, K_min, K_max, (float)mass, d.p + (size_t)b0 * K_max);
+			    PKL("topk_select_kernel");
+		    } else {
+			    topk_kernel<<<(m * 32 + 255) / 256, 256, 0, net->stream>>>(
+			        net->act[NL].p, m, net->num_classes, K_min, K_max, (float)mass, d.p + (size_t)b0 * K_max);
+			    PKL("topk_kernel");
+		    }
 		    return DFG_OK;
 	    }))
 		return rc;

@@ -208,6 +208,14 @@ def test_gpu_mass_covering_topk_matches_the_logits():
     sel = net.topk_mass(K_min, K_max, mass)
     top = net.topk(K_max)
     np.testing.assert_array_equal(net.topk(K_min), top[:, :K_min])
+    # up to 256 picks come from the radix-select kernel, more from the
+    # per-pick arg-max kernel: the two agree, and with a stable sort of the
+    # logits (value descending, index ascending)
+    wide = net.topk(300)
+    np.testing.assert_array_equal(wide[:, :K_max], top)
+    np.testing.assert_array_equal(net.topk(256), wide[:, :256])
+    ref = np.argsort(-z, axis=1, kind="stable")[:, :256]
+    np.testing.assert_array_equal(net.topk(256), ref)
     for i in range(len(x)):
         n = int((sel[i] >= 0).sum())
         assert K_min <= n <= K_max and np.all(sel[i, n:] == -1)
