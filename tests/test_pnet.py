@@ -235,7 +235,10 @@ def test_gpu_tensor_core_wait_gives_up_and_the_network_recovers():
     """Failure detection of the network's tensor-core products without a GPU
     fault: with one stage's copies withheld (test hook) the waits on it run
     out after a short limit and dfg_pnet_logits reports DFG_ERR_CUDA; with the
-    hook off the next call on the same network gives the logits of before."""
+    hook off the next call on the same network gives the logits of before.
+    Training on the tensor cores reports the same at the end of its epoch
+    (its products are invalid, so the weights are put back before the
+    network is used again)."""
     from dragonfly_b200._lib import DFG_ERR_CUDA, DFGError, ProposalNet
     rng = np.random.default_rng(6)
     net = ProposalNet(40, batch=64, seed=5)
@@ -247,9 +250,15 @@ def test_gpu_tensor_core_wait_gives_up_and_the_network_recovers():
     with pytest.raises(DFGError) as e:
         net.logits()
     assert e.value.code == DFG_ERR_CUDA and "gave up" in str(e.value)
+    p0 = net.params()
+    with pytest.raises(DFGError) as e:
+        net.train(np.arange(600) % 40, epochs=1, lr=1e-3)
+    assert e.value.code == DFG_ERR_CUDA and "gave up" in str(e.value)
     net.set_option("withhold_stage", -1)
     net.set_option("wait_cycles", 2e9)
+    net.set_params(p0)
     np.testing.assert_array_equal(net.logits(), z)
+    net.train(np.arange(600) % 40, epochs=1, lr=1e-3)   # the products run to the end again
     net.close()
 
 
