@@ -845,7 +845,10 @@ def run_proposals(args):
                            "rule": "t(R) linear in R through the two measured subsets"},
            "speedup_vs_full_search": full_ms / ms if full_ms else None,
            "loop": loop,
-           "effective_pairs_per_s": R * N / (ms / 1e3)}
+           "effective_pairs_per_s": R * N / (ms / 1e3),
+           # the (orientation, frame) pairs the proposal iteration evaluates:
+           # every orientation of each live (tile, frame) pair
+           "evaluated_pairs_per_s": wl["live_pairs"] * 128 / (it_ms / 1e3)}
     print(json.dumps(out))
     lp.close()
     c.close()
