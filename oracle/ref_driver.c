@@ -35,6 +35,7 @@ typedef struct ref_engine {
 	int det_mapping[1];
 	double avg_likelihood;
 	double beta_start;          /* calc_beta's argument, for ref_add_detector */
+	int num_threads;            /* OpenMP threads of this engine's calls (<= 0: the default) */
 	/* more detectors (ref_add_detector): all detectors contiguous (detector 0
 	 * a copy of det), their datasets linked after dset, one per detector */
 	struct detector *dets;
@@ -84,8 +85,10 @@ ref_engine *ref_create(int num_pix, const double *qvals, const double *corr, con
                        const double *scale, const uint8_t *blacklist, int num_threads) {
 	long d, ones_total = 0, multi_total = 0;
 	ref_engine *e = calloc(1, sizeof(ref_engine));
-	if (num_threads > 0)
-		omp_set_num_threads(num_threads);
+	/* the thread count applies to this engine's calls only (ref_maximize,
+	 * ref_update_model): setting it for the process would also slow every
+	 * later OpenMP region of the caller (the oracle's among them) */
+	e->num_threads = num_threads;
 
 	/* Detector (detector.pyx:61-74) */
 	e->det.num_pix = num_pix;
@@ -210,7 +213,13 @@ double ref_maximize(ref_engine *e, int iteration) {
 	free_common(e->mdata, it->tot_num_data, it->num_det);
 	e->mdata->iter = it;
 	e->mdata->within_openmp = 0;
-	e->avg_likelihood = maximize(e->mdata);
+	{
+		const int prev = omp_get_max_threads();
+		if (e->num_threads > 0)
+			omp_set_num_threads(e->num_threads);
+		e->avg_likelihood = maximize(e->mdata);
+		omp_set_num_threads(prev);
+	}
 	return e->avg_likelihood;
 }
 
