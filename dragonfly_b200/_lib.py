@@ -809,7 +809,8 @@ class ProposalNet:
 
     def set_tensor_cores(self, on):
         """Inference products on the tcgen05 tensor cores (default) or the
-        FP32 path training uses."""
+        FP32 path (CUDA-core products, FP32 activations). Training has its
+        own switch, set_option("tensor_core_training", 0 or 1)."""
         self._call("dfg_pnet_set_tensor_cores", 1 if on else 0)
 
     def topk(self, K):
