@@ -234,8 +234,22 @@ beta = 0.5
     assert itr.mean_count[0] == mcs[1] and itr.mean_count[1] == mcs[0]
     qmax = max(np.linalg.norm(dd["qvals"], axis=1).max() for dd in dets)
     assert itr.model.size == Iterate.calculate_size(qmax)
+    # a background list needs one entry per detector (iterate.pyx:109-127),
+    # in the detector list's order (det_z first), whatever their sorted order
+    for k, dd in enumerate(dets):
+        np.savez(str(tmp_path / ("bg%d.npz" % k)), background=np.full(dd["qvals"].shape[0], 0.1 * (k + 1)))
+    (tmp_path / "bg1.txt").write_text("bg0.npz\n")
+    (tmp_path / "bg2.txt").write_text("bg0.npz\nbg1.npz\n")
+    base = cfg.read_text()
+    cfg.write_text(base + "background_list = bg1.txt\n")
+    with pytest.raises(ValueError, match="Background list has 1 entries but there are 2 unique detectors"):
+        Iterate(str(cfg))
+    cfg.write_text(base + "background_list = bg2.txt\n")
+    itr2 = Iterate(str(cfg))
+    assert all(d.with_bg for d in itr2.dets)
+    assert itr2.dets[0].background[0] == 0.2 and itr2.dets[1].background[0] == 0.1
     # a single photons file with a detector list uses the first detector
-    cfg.write_text(cfg.read_text().replace("in_photons_list = photons.txt", "in_photons_file = photons0.emc"))
+    cfg.write_text(base.replace("in_photons_list = photons.txt", "in_photons_file = photons0.emc"))
     itr1 = Iterate(str(cfg))
     assert itr1.num_det == 1 and itr1.dets[0].fname.endswith("det_z.npz")
 
