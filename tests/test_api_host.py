@@ -234,6 +234,9 @@ beta = 0.5
     assert itr.mean_count[0] == mcs[1] and itr.mean_count[1] == mcs[0]
     qmax = max(np.linalg.norm(dd["qvals"], axis=1).max() for dd in dets)
     assert itr.model.size == Iterate.calculate_size(qmax)
+    # calc_beta's empirical start uses detector 0's mean count (iterate.c:72-73)
+    itr.calc_beta()
+    np.testing.assert_allclose(itr.beta_start, np.exp(-6.5 * (itr.mean_count[0] * 1e-5) ** 0.15), rtol=1e-14)
     # a background list needs one entry per detector (iterate.pyx:109-127),
     # in the detector list's order (det_z first), whatever their sorted order
     for k, dd in enumerate(dets):
