@@ -9,9 +9,14 @@ so it runs only where they are present:
 
     python tests/golden/make_golden.py
 
+    python tests/golden/make_golden.py detectors2     # only the named cases
+
 Each case file <name>.npz holds the inputs and, per iteration, the outputs:
 scalars, per-frame arrays and the SHA-256 of model1's bytes (bit-exact pin),
 plus the final model1. quat_gen.npz holds the reference's quat_gen lists.
+detectors2.npz is a reconstruction with two detectors (each with its own
+dataset; inputs of detector k under d<k>_*), run through the reference with
+both detectors (ref_add_detector).
 """
 import hashlib
 import os
@@ -148,13 +153,53 @@ def run_case(name, spec):
     print("wrote", path, os.path.getsize(path) // 1024, "KB")
 
 
-def main():
+def run_two_detectors(name="detectors2", seed=5, iters=3):
+    """Two detectors of different geometry, scale updates on (the reference's
+    in_detector_list: per-detector u, rescale, psum_r and tomograms)."""
+    dets, sh = synth.two_detector_problem(seed=seed)
+    kw = dict(beta=0.05, beta_jump=1.41421356, beta_period=2, need_scaling=1, update_scale=1)
+    probs = [EMCProblem(d["qvals"], d["corr"], d["mask"], d["ones"], d["multi"], d["place_ones"],
+                        d["place_multi"], d["count_multi"], sh["quats"], sh["model_start"], **kw) for d in dets]
+    eng = ReferenceEngine(probs[0], num_threads=1)
+    eng.add_detector(probs[1])
+    out = dict(quats=probs[0].quats, model_start=probs[0].model1, iters=np.array(iters),
+               prob_params=np.array([1, 1, 0, 0., kw["beta"], kw["beta_jump"], kw["beta_period"], 1.]))
+    for k, p in enumerate(probs):
+        for key in ("qvals", "corr", "mask", "ones", "multi", "place_ones", "place_multi", "count_multi"):
+            out["d%d_%s" % (k, key)] = getattr(p, key)
+    it0 = eng.iter_arrays()
+    out["fcounts"], out["sum_fact"], out["beta_start"] = it0["fcounts"], it0["sum_fact"], it0["beta_start"]
+    for it in range(1, iters + 1):
+        r = eng.run_iteration(it)
+        k = "it%d_" % it
+        out[k + "scalars"] = np.array([r["avg_likelihood"], r["mutual_info"], r["rms_change"]])
+        out[k + "rescale_det"] = r["rescale_det"]
+        out[k + "mean_count_det"] = r["mean_count_det"]
+        out[k + "u_det"] = r["u_det"]
+        for key in ("rmax", "info", "likelihood", "max_exp", "p_norm", "psum_d", "beta", "scale"):
+            out[k + key] = r[key]
+        out[k + "model_sha256"] = np.array(model_hash(r["model1"]))
+        out[k + "model2_sum_sha256"] = np.array(model_hash(r["model2_sum"]))
+        out[k + "weight_sha256"] = np.array(model_hash(r["inter_weight"]))
+        if it == iters:
+            out["final_model1"] = r["model1"]
+    eng.close()
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path) // 1024, "KB")
+
+
+def main(names=None):
     for name, spec in CASES.items():
-        run_case(name, spec)
-    qg = {"num_div_%d" % n: quat_gen_reference(n) for n in (1, 2, 3, 4)}
-    np.savez_compressed(os.path.join(HERE, "quat_gen.npz"), **qg)
-    print("wrote quat_gen.npz")
+        if names is None or name in names:
+            run_case(name, spec)
+    if names is None or "detectors2" in names:
+        run_two_detectors()
+    if names is None or "quat_gen" in names:
+        qg = {"num_div_%d" % n: quat_gen_reference(n) for n in (1, 2, 3, 4)}
+        np.savez_compressed(os.path.join(HERE, "quat_gen.npz"), **qg)
+        print("wrote quat_gen.npz")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -214,3 +214,35 @@ def test_oracle_two_detectors_match_live_reference(seed, prob_kw, oracle_built):
     # the two detectors see different things: their rescale factors differ
     assert abs(b["rescale_det"][0] - b["rescale_det"][1]) > 1e-3 * abs(b["rescale_det"][0])
     ref.close()
+
+
+def test_oracle_matches_two_detector_golden(oracle_built):
+    """The two-detector fixture (tests/golden/detectors2.npz, made by the
+    reference engine run with both detectors): the oracle bit for bit, three
+    iterations with scale updates."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "detectors2.npz"))
+    pp = g["prob_params"]
+    kw = dict(need_scaling=int(pp[0]), update_scale=int(pp[1]), known_scale=int(pp[2]), alpha=pp[3],
+              beta=pp[4], beta_jump=pp[5], beta_period=int(pp[6]), beta_factor=pp[7])
+    probs = [EMCProblem(*(g["d%d_%s" % (k, key)] for key in ("qvals", "corr", "mask", "ones", "multi",
+                                                             "place_ones", "place_multi", "count_multi")),
+                        g["quats"], g["model_start"], **kw) for k in (0, 1)]
+    eng = OracleEngine(probs[0], extra=probs[1:])
+    np.testing.assert_array_equal(eng.fcounts, g["fcounts"])
+    np.testing.assert_array_equal(eng.sum_fact, g["sum_fact"])
+    np.testing.assert_array_equal(eng.beta_start, g["beta_start"])
+    for it in range(1, int(g["iters"]) + 1):
+        r = eng.run_iteration(it)
+        k = "it%d_" % it
+        sc = g[k + "scalars"]
+        assert (r["avg_likelihood"], r["mutual_info"], r["rms_change"]) == tuple(sc)
+        np.testing.assert_array_equal(r["rescale_det"], g[k + "rescale_det"])
+        np.testing.assert_array_equal(r["mean_count_det"], g[k + "mean_count_det"])
+        np.testing.assert_array_equal(r["u_det"], g[k + "u_det"])
+        for key in ("rmax", "info", "likelihood", "max_exp", "p_norm", "psum_d", "beta", "scale"):
+            np.testing.assert_array_equal(r[key], g[k + key], err_msg=key)
+        assert sha(r["model2_sum"]) == str(g[k + "model2_sum_sha256"])
+        assert sha(r["inter_weight"]) == str(g[k + "weight_sha256"])
+        assert sha(r["model1"]) == str(g[k + "model_sha256"])
+    np.testing.assert_array_equal(r["model1"], g["final_model1"])
